@@ -1,0 +1,331 @@
+/*
+ * pnanovdb_b200.h - C ABI of the B200 Gaussian -> NanoVDB (node2) voxelizer.
+ *
+ * Drop-in boundary: libpnanovdbcompute.so exports pnanovdb_get_raster() and
+ * pnanovdb_get_compute(), whose tables are layout-compatible with the
+ * reference's pnanovdb_raster_t (nanovdb_editor/putil/Raster.h:58-174) and
+ * pnanovdb_compute_t (nanovdb_editor/putil/Compute.h:784-853), so the
+ * reference's ctypes binding (pymodule/nanovdb_editor/raster.py:14-168,
+ * compute.py:109-217) binds them unchanged.  Vulkan handles are replaced by
+ * headless CUDA ones: a queue is a CUDA stream on one device and a
+ * pnanovdb_compute_buffer_t is a device pointer plus a size.
+ *
+ * Below the drop-in table are the library's own vox_* entry points (device
+ * pointers in, node2 grid out), which the table is built on and which the
+ * Python autograd path calls directly.
+ *
+ * Calling convention: cdecl (PNANOVDB_ABI is empty on Linux,
+ * nanovdb_editor/putil/Reflect.h:28-32).  No exceptions cross this boundary;
+ * failures return PNANOVDB_FALSE / NULL / a negative vox status and log.
+ */
+#ifndef PNANOVDB_B200_H
+#define PNANOVDB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef PNANOVDB_ABI
+#define PNANOVDB_ABI
+#endif
+#ifndef PNANOVDB_API
+#define PNANOVDB_API __attribute__((visibility("default")))
+#endif
+
+typedef uint32_t pnanovdb_uint32_t;
+typedef uint64_t pnanovdb_uint64_t;
+typedef int32_t pnanovdb_int32_t;
+typedef int32_t pnanovdb_bool_t; /* bound as c_int32 by raster.py:126 */
+#define PNANOVDB_TRUE 1
+#define PNANOVDB_FALSE 0
+
+/* --------------------------------------------------------------- arrays -- */
+/* nanovdb_editor/putil/Compute.h:765-771 */
+typedef struct pnanovdb_compute_array_t
+{
+    void* data;
+    pnanovdb_uint64_t element_size;
+    pnanovdb_uint64_t element_count;
+    const char* filepath;
+} pnanovdb_compute_array_t;
+
+/* headless device buffer (replaces the opaque Vulkan buffer of
+ * nanovdb_editor/putil/Compute.h:101) */
+typedef struct pnanovdb_compute_buffer_t
+{
+    void* device_ptr;
+    pnanovdb_uint64_t size_bytes;
+} pnanovdb_compute_buffer_t;
+
+/* a queue: one CUDA stream on one device (replaces Compute.h's Vulkan queue) */
+typedef struct pnanovdb_compute_queue_t pnanovdb_compute_queue_t;
+typedef struct pnanovdb_compute_device_t pnanovdb_compute_device_t;
+
+/* nanovdb_editor/putil/Compute.h:546-551, :561-564 */
+typedef struct pnanovdb_compute_profiler_entry_t
+{
+    const char* label;
+    float cpu_delta_time;
+    float gpu_delta_time;
+} pnanovdb_compute_profiler_entry_t;
+typedef void(PNANOVDB_ABI* pnanovdb_profiler_report_t)(void* userdata, pnanovdb_uint64_t capture_id,
+                                                       pnanovdb_uint32_t num_entries,
+                                                       pnanovdb_compute_profiler_entry_t* entries);
+
+/* ------------------------------------------------------ compute table -- */
+/* Layout of nanovdb_editor/putil/Compute.h:566-661: 1 + 33 pointers.  The
+ * entries this library implements are named; the rest are NULL. */
+typedef struct pnanovdb_compute_device_interface_t
+{
+    const void* interface_pnanovdb_reflect_data_type;
+    void* (PNANOVDB_ABI* create_device_manager)(pnanovdb_bool_t enable_validation_on_debug_build);
+    void(PNANOVDB_ABI* destroy_device_manager)(void* manager);
+    pnanovdb_bool_t(PNANOVDB_ABI* enumerate_devices)(void* manager, pnanovdb_uint32_t device_index, void* p_desc);
+    pnanovdb_compute_device_t*(PNANOVDB_ABI* create_device)(void* manager, const void* desc);
+    void(PNANOVDB_ABI* destroy_device)(void* manager, pnanovdb_compute_device_t* device);
+    void* reserved_get_memory_stats;
+    void* reserved_semaphore[4];
+    pnanovdb_compute_queue_t*(PNANOVDB_ABI* get_device_queue)(const pnanovdb_compute_device_t* device);
+    pnanovdb_compute_queue_t*(PNANOVDB_ABI* get_compute_queue)(const pnanovdb_compute_device_t* device);
+    int(PNANOVDB_ABI* flush)(pnanovdb_compute_queue_t* queue, pnanovdb_uint64_t* flushed_frame, void* wait_semaphore,
+                             void* signal_semaphore);
+    void* reserved_frames[2];
+    void(PNANOVDB_ABI* wait_idle)(pnanovdb_compute_queue_t* queue);
+    void* reserved_interface[2];
+    void* reserved_swapchain[5];
+    void* reserved_encoder[6];
+    void* reserved_profiler[3];
+    pnanovdb_uint32_t(PNANOVDB_ABI* get_device_index)(const pnanovdb_compute_device_t* device);
+} pnanovdb_compute_device_interface_t;
+
+/* nanovdb_editor/putil/Compute.h:734-745 */
+typedef struct pnanovdb_compute_shader_interface_t
+{
+    const void* interface_pnanovdb_reflect_data_type;
+    void* reserved[3];
+} pnanovdb_compute_shader_interface_t;
+
+/* nanovdb_editor/putil/Compute.h:784-853 */
+typedef struct pnanovdb_compute_t
+{
+    const void* interface_pnanovdb_reflect_data_type;
+    void* module;
+    const void* compiler;
+    pnanovdb_compute_shader_interface_t shader_interface;
+    pnanovdb_compute_device_interface_t device_interface;
+    pnanovdb_compute_array_t*(PNANOVDB_ABI* load_nanovdb)(const char* filepath);
+    pnanovdb_bool_t(PNANOVDB_ABI* save_nanovdb)(pnanovdb_compute_array_t* array, const char* filepath);
+    void* reserved_shader[5]; /* create_shader_context .. dispatch_shader */
+    void* reserved_dispatch[2];
+    pnanovdb_compute_array_t*(PNANOVDB_ABI* create_array)(size_t element_size, pnanovdb_uint64_t element_count,
+                                                          const void* data);
+    void(PNANOVDB_ABI* destroy_array)(pnanovdb_compute_array_t* array);
+    void*(PNANOVDB_ABI* map_array)(pnanovdb_compute_array_t* array);
+    void(PNANOVDB_ABI* unmap_array)(pnanovdb_compute_array_t* array);
+    void* reserved_print_range;
+    void* reserved_from_image;
+    pnanovdb_compute_array_t*(PNANOVDB_ABI* duplicate_array)(pnanovdb_compute_array_t* array);
+} pnanovdb_compute_t;
+
+/* ------------------------------------------------------- raster table -- */
+typedef struct pnanovdb_raster_context_t pnanovdb_raster_context_t;
+typedef struct pnanovdb_raster_gaussian_data_t pnanovdb_raster_gaussian_data_t;
+
+/* nanovdb_editor/putil/Raster.h:26-34 */
+typedef struct pnanovdb_raster_shader_params_t
+{
+    float eps2d;
+    float min_radius_2d;
+    pnanovdb_uint32_t tile_size;
+    pnanovdb_int32_t sh_degree_override;
+    pnanovdb_uint32_t sh_stride_rgbrgbrgb_override;
+    const void* data_type;
+    const char* name;
+} pnanovdb_raster_shader_params_t;
+
+/* index of gaussian_frag_color's parameter block in shader_params_arrays
+ * (nanovdb_editor/putil/Raster.h:216-235); its first two 32-bit words are
+ * cull_scale (float) and use_default (bool32), gaussian_frag_color.slang:21-28 */
+#define PNANOVDB_RASTER_SHADER_GAUSSIAN_FRAG_COLOR 1
+
+/* nanovdb_editor/putil/Raster.h:58-174, field order preserved */
+typedef struct pnanovdb_raster_t
+{
+    const void* interface_pnanovdb_reflect_data_type;
+    const pnanovdb_compute_t* compute;
+    pnanovdb_raster_context_t*(PNANOVDB_ABI* create_context)(const pnanovdb_compute_t* compute,
+                                                             pnanovdb_compute_queue_t* queue);
+    void(PNANOVDB_ABI* destroy_context)(const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue,
+                                        pnanovdb_raster_context_t* context);
+    pnanovdb_raster_gaussian_data_t*(PNANOVDB_ABI* create_gaussian_data)(
+        const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue, pnanovdb_raster_context_t* context,
+        pnanovdb_compute_array_t* means, pnanovdb_compute_array_t* quaternions, pnanovdb_compute_array_t* scales,
+        pnanovdb_compute_array_t* colors, pnanovdb_compute_array_t* sh_0, pnanovdb_compute_array_t* sh_n,
+        pnanovdb_compute_array_t* opacities, pnanovdb_compute_array_t** shader_params_arrays,
+        pnanovdb_raster_shader_params_t* raster_params);
+    void(PNANOVDB_ABI* upload_gaussian_data)(const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue,
+                                             pnanovdb_raster_context_t* context, pnanovdb_raster_gaussian_data_t* data);
+    void(PNANOVDB_ABI* destroy_gaussian_data)(const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue,
+                                              pnanovdb_raster_gaussian_data_t* data);
+    void(PNANOVDB_ABI* raster_gaussian_2d)(const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue,
+                                           pnanovdb_raster_context_t* context, pnanovdb_raster_gaussian_data_t* data,
+                                           void* color_2d, pnanovdb_uint32_t image_width,
+                                           pnanovdb_uint32_t image_height, const void* view, const void* projection,
+                                           const pnanovdb_raster_shader_params_t* shader_params,
+                                           pnanovdb_uint32_t composite);
+    void(PNANOVDB_ABI* raster_gaussian_3d)(const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue,
+                                           pnanovdb_raster_context_t* context, float voxel_size,
+                                           pnanovdb_raster_gaussian_data_t* data,
+                                           pnanovdb_compute_buffer_t* nanovdb_out,
+                                           pnanovdb_uint64_t nanovdb_word_count, void* userdata);
+    pnanovdb_compute_array_t*(PNANOVDB_ABI* raster_to_nanovdb)(
+        const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue, float voxel_size,
+        pnanovdb_compute_array_t* means, pnanovdb_compute_array_t* quaternions, pnanovdb_compute_array_t* scales,
+        pnanovdb_compute_array_t* colors, pnanovdb_compute_array_t* sh_0, pnanovdb_compute_array_t* sh_n,
+        pnanovdb_compute_array_t* opacities, pnanovdb_compute_array_t** shader_params_arrays,
+        pnanovdb_profiler_report_t profiler_report, void* userdata);
+    pnanovdb_bool_t(PNANOVDB_ABI* raster_file)(struct pnanovdb_raster_t* raster, const pnanovdb_compute_t* compute,
+                                               pnanovdb_compute_queue_t* queue, const char* filename,
+                                               float voxel_size, pnanovdb_compute_array_t** nanovdb_arr,
+                                               pnanovdb_raster_gaussian_data_t** gaussian_data,
+                                               pnanovdb_raster_context_t** raster_context,
+                                               pnanovdb_compute_array_t** shader_params_arrays,
+                                               pnanovdb_raster_shader_params_t* raster_params,
+                                               pnanovdb_profiler_report_t profiler_report, void* userdata);
+    pnanovdb_bool_t(PNANOVDB_ABI* raster_to_nanovdb_from_arrays)(struct pnanovdb_raster_t* raster,
+                                                                 const pnanovdb_compute_t* compute,
+                                                                 pnanovdb_compute_queue_t* queue, float voxel_size,
+                                                                 pnanovdb_compute_array_t** arrays_gaussian,
+                                                                 pnanovdb_uint32_t array_count,
+                                                                 pnanovdb_compute_array_t** out_nanovdb_arr);
+    pnanovdb_bool_t(PNANOVDB_ABI* create_gaussian_data_from_arrays)(
+        struct pnanovdb_raster_t* raster, const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue,
+        pnanovdb_compute_array_t** arrays_gaussian, pnanovdb_uint32_t array_count,
+        pnanovdb_raster_gaussian_data_t** gaussian_data, pnanovdb_raster_shader_params_t* raster_params,
+        pnanovdb_raster_context_t** raster_context);
+    pnanovdb_bool_t(PNANOVDB_ABI* create_gaussian_data_from_desc)(
+        struct pnanovdb_raster_t* raster, const pnanovdb_compute_t* compute, pnanovdb_compute_queue_t* queue,
+        const void* desc, const char* name, pnanovdb_raster_gaussian_data_t** gaussian_data,
+        pnanovdb_raster_shader_params_t* raster_params, pnanovdb_raster_context_t** raster_context);
+} pnanovdb_raster_t;
+
+/* replaces raster/Raster.cpp:822-840 */
+PNANOVDB_API pnanovdb_raster_t* pnanovdb_get_raster(void);
+/* replaces the compute table the reference builds in compute/Compute.cpp */
+PNANOVDB_API pnanovdb_compute_t* pnanovdb_get_compute(void);
+
+/* ------------------------------------------------------ grid container -- */
+/* The grid buffer this library produces.  The reference returns a NanoVDB
+ * grid whose GridData/TreeData headers come from PNanoVDB.h, which the
+ * reference does not vendor; this header stands in for them and everything
+ * from node2_offset on is the reference's node2 layout: the root node
+ * (541728 B) followed by every node at its node2 maximum size in node_idx
+ * order (upper 274464 B, lower 34336 B, leaf 128 B; PNanoVDBExt.h:49-64),
+ * child links as byte offsets relative to the parent.  The blind data that
+ * grid_build_blindmetadata.slang appends follow: the bbox (two int32x3,
+ * inclusive voxel coordinates) and per-value arrays indexed by value index
+ * (two background slots first): RGBA8 as the reference computes it, float
+ * density = sum of per-pair alpha in (voxel key, Gaussian id) order, and
+ * Vec3f colour = alpha-weighted mean RGB. */
+#define VOX_GRID_MAGIC 0x32454E58564F5642ull /* "BVOXNE2" */
+#define VOX_GRID_HEADER_BYTES 256u
+
+typedef struct vox_grid_header_t
+{
+    uint64_t magic;
+    uint32_t version;
+    uint32_t header_bytes;
+    uint64_t grid_bytes;
+    uint64_t node2_offset;
+    uint64_t node2_bytes;
+    uint32_t upper_count;
+    uint32_t lower_count;
+    uint32_t leaf_count;
+    uint32_t node_order; /* 0: one fragment window, 1: reference 256K x 8M windows */
+    uint64_t value_count; /* 2 + active voxels */
+    uint64_t bbox_offset;
+    uint64_t rgba8_offset;
+    uint64_t density_offset;
+    uint64_t color_offset;
+    float voxel_size;
+    int32_t bbox[6];
+    uint32_t pad0;
+    uint64_t pair_count;
+    uint64_t candidate_count;
+    uint8_t reserved[256 - 144];
+} vox_grid_header_t;
+
+/* --------------------------------------------------- vox_* entry points -- */
+typedef struct vox_context_t vox_context_t;
+
+/* flags for vox_voxelize */
+#define VOX_FLAG_RAW_INPUTS 1u     /* log scales, logit opacities, raw quaternions, SH0 colours */
+#define VOX_FLAG_WINDOW_ORDER 2u   /* node_idx order of the reference's fragment windows */
+
+/* status codes */
+#define VOX_OK 0
+#define VOX_ERR_ARGS -1
+#define VOX_ERR_CUDA -2
+#define VOX_ERR_MEMORY -3
+#define VOX_ERR_RANGE -4      /* voxel coordinate outside [-65536, 65535] */
+#define VOX_ERR_FOOTPRINT -5  /* one Gaussian covers >= 2^31 candidate voxels */
+#define VOX_ERR_TIMEOUT -6    /* a bounded device wait expired */
+#define VOX_ERR_SIZE -7       /* caller buffer too small */
+
+typedef struct vox_gaussians_t
+{
+    const float* means;     /* [n][3] */
+    const float* quats;     /* [n][4] w, x, y, z */
+    const float* scales;    /* [n][3] (log scales with VOX_FLAG_RAW_INPUTS) */
+    const float* opacities; /* [n] (logits with VOX_FLAG_RAW_INPUTS) */
+    const float* colors;    /* [n][3] RGB (SH0 coefficients with VOX_FLAG_RAW_INPUTS) */
+    int64_t count;
+} vox_gaussians_t;
+
+typedef struct vox_stats_t
+{
+    int64_t gaussians, candidates, pairs, voxels, uppers, lowers, leaves, value_count;
+    int64_t grid_bytes;
+    int32_t key_bits;
+    int32_t sort_passes;
+    float ms_prep, ms_emit, ms_sort, ms_build, ms_accumulate, ms_total;
+} vox_stats_t;
+
+/* One context per caller thread; it owns a CUDA stream on `device` and a
+ * device arena that grows to the largest workload seen. */
+PNANOVDB_API vox_context_t* vox_context_create(int device);
+PNANOVDB_API void vox_context_destroy(vox_context_t* ctx);
+PNANOVDB_API void* vox_context_stream(vox_context_t* ctx);
+PNANOVDB_API const char* vox_last_error(vox_context_t* ctx);
+
+/* Voxelizes device-resident Gaussians (the path of raster_gaussian_3d,
+ * raster/Raster.cpp:420-558).  On success *grid (device) points at the
+ * context-owned grid buffer (valid until the next call) and *grid_bytes is
+ * its size.  cull_scale <= 0 selects 0.05 (gaussian_frag_color.slang:205). */
+PNANOVDB_API int vox_voxelize(vox_context_t* ctx, const vox_gaussians_t* gaussians, float voxel_size,
+                              float cull_scale, uint32_t flags, void** grid, uint64_t* grid_bytes);
+
+/* Same from host arrays, with the grid copied to host memory (`out`,
+ * `out_capacity` bytes); copies are counted in the call. */
+PNANOVDB_API int vox_voxelize_host(vox_context_t* ctx, const vox_gaussians_t* gaussians, float voxel_size,
+                                   float cull_scale, uint32_t flags, void* out, uint64_t out_capacity,
+                                   uint64_t* grid_bytes);
+
+/* Copies the grid of the last vox_voxelize / vox_voxelize_host call to host
+ * memory (`capacity` bytes). */
+PNANOVDB_API int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity);
+
+/* Sorted (voxel, Gaussian) pairs of the last vox_voxelize call: hierarchical
+ * 64-bit keys (root_n << 36 | upper_n << 21 | lower_n << 9 | leaf_n) and
+ * Gaussian ids, in (key, id) order, copied to host memory. */
+PNANOVDB_API int vox_copy_pairs(vox_context_t* ctx, uint64_t* keys, uint32_t* ids, int64_t capacity);
+
+PNANOVDB_API void vox_get_stats(vox_context_t* ctx, vox_stats_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PNANOVDB_B200_H */

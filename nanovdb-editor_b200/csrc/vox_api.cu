@@ -1,0 +1,716 @@
+// vox_api.cu - host orchestration of the voxelization pipeline and the C ABI
+// (pnanovdb_get_raster / pnanovdb_get_compute drop-in tables and vox_*).
+//
+// The reference drives raster_gaussian_3d from the host as a loop of
+// 256K-prim x 8M-fragment windows with a per-window queue flush and a
+// frame-lagged readback of the fragment total (raster/Raster.cpp:420-558,
+// raster/GridBuild.cpp:830-942).  Here one call runs the whole chain on one
+// CUDA stream with three small read-backs (candidate count, pair count, node
+// counts) that size the buffers; buffers persist in the context and only
+// grow, so repeated calls allocate nothing.
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "pnanovdb_b200.h"
+#include "vox_device.cuh"
+#include "vox_internal.h"
+#include "vox_raster.h"
+
+using namespace vox;
+
+namespace
+{
+
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+struct Timers
+{
+    cudaEvent_t ev[8] = {};
+};
+
+} // namespace
+
+struct vox_context_t
+{
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    std::string last_error;
+    std::vector<DevBuf*> bufs;
+    // device buffers
+    DevBuf recs, footprints, frag_off, root_bits, root_prefix, root_of_rank, lower_bits, lower_prefix, lower_cell;
+    DevBuf scan_status, emit_status, run_status;
+    DevBuf keys, ids, keys_alt, ids_alt, sort_ws;
+    DevBuf vox_start, leaf_vstart, lower_lstart, lower_rank;
+    DevBuf lower_origin, lower_upper_n, upper_head, upper_scan, lower_parent, upper_root_n, upper_lostart;
+    DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
+    DevBuf order; // 9 node order arrays
+    DevBuf grid;
+    DevBuf scal; // device scalars
+    DevBuf hier_keys;
+    uint64_t* hscal = nullptr; // pinned mirror
+    Epochs scan_epochs, emit_epochs, run_epochs;
+    uint64_t pair_cap = 0;
+    int key64 = 0;
+    int sorted_in_alt = 0;
+    vox_stats_t stats{};
+    Timers timers;
+    SortTuning tuning;
+    // last result
+    int64_t last_P = 0;
+    uint64_t last_grid_bytes = 0;
+};
+
+// device scalar slots (u64 each)
+enum
+{
+    SC_F = 0,
+    SC_NROOT,
+    SC_NLOWER,
+    SC_P,
+    SC_V,
+    SC_L,
+    SC_LO,
+    SC_U,
+    SC_ERR, // int in the low half
+    SC_BBOX, // 3 words (6 int32)
+    SC_COUNT = SC_BBOX + 3,
+    SC_SCRATCH = 16
+};
+
+static void set_error(vox_context_t* ctx, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx)
+        ctx->last_error = buf;
+    fprintf(stderr, "[pnanovdb_b200] %s\n", buf);
+}
+
+static bool ensure(vox_context_t* ctx, DevBuf& b, size_t bytes)
+{
+    if (bytes == 0)
+        bytes = 256;
+    if (b.cap >= bytes)
+        return true;
+    if (b.p)
+        cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = bytes + bytes / 8 + 256;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        set_error(ctx, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+        b.p = nullptr;
+        return false;
+    }
+    b.cap = want;
+    return true;
+}
+
+static int check_cuda(vox_context_t* ctx, const char* where)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+    {
+        set_error(ctx, "CUDA error at %s: %s", where, cudaGetErrorString(e));
+        return VOX_ERR_CUDA;
+    }
+    return VOX_OK;
+}
+
+static int sync_scalars(vox_context_t* ctx, const char* where)
+{
+    cudaMemcpyAsync(ctx->hscal, ctx->scal.p, sizeof(uint64_t) * SC_COUNT, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+    {
+        set_error(ctx, "CUDA error at %s: %s", where, cudaGetErrorString(e));
+        return VOX_ERR_CUDA;
+    }
+    int err = (int)(ctx->hscal[SC_ERR] & 0xffffffffu);
+    if (err & ERR_LOOKBACK)
+    {
+        set_error(ctx, "%s: a bounded device wait expired", where);
+        return VOX_ERR_TIMEOUT;
+    }
+    if (err & ERR_RANGE)
+    {
+        set_error(ctx, "%s: voxel coordinates outside [-65536, 65535] (root key range of the node2 grid)", where);
+        return VOX_ERR_RANGE;
+    }
+    if (err & ERR_FOOTPRINT)
+    {
+        set_error(ctx, "%s: a Gaussian's bounding box covers 2^31 or more voxels", where);
+        return VOX_ERR_FOOTPRINT;
+    }
+    return VOX_OK;
+}
+
+static int bits_for(uint64_t n)
+{
+    int b = 0;
+    while ((1ull << b) < n)
+        b++;
+    return b;
+}
+
+static float elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+// ---------------------------------------------------------------------------
+// the pipeline
+// ---------------------------------------------------------------------------
+static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float voxel_size, float cull_scale,
+                        uint32_t flags)
+{
+    if (!ctx || !gs || gs->count < 0 || !(voxel_size > 0.f))
+    {
+        set_error(ctx, "vox_voxelize: invalid arguments");
+        return VOX_ERR_ARGS;
+    }
+    if (gs->count > 0 && (!gs->means || !gs->quats || !gs->scales || !gs->opacities || !gs->colors))
+    {
+        set_error(ctx, "vox_voxelize: missing attribute array");
+        return VOX_ERR_ARGS;
+    }
+    if (flags & VOX_FLAG_WINDOW_ORDER)
+    {
+        set_error(ctx, "vox_voxelize: reference window node order is not available in this build");
+        return VOX_ERR_ARGS;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int64_t G = gs->count;
+    memset(&ctx->stats, 0, sizeof(ctx->stats));
+    ctx->stats.gaussians = G;
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    int* d_err = (int*)(sc + SC_ERR);
+    uint32_t* d_counter = (uint32_t*)(sc + SC_SCRATCH);
+    cudaEventRecord(ctx->timers.ev[0], s);
+
+    // ---------------------------------------------------------------- prep
+    const float cull = cull_scale > 0.f ? cull_scale : 0.05f;
+    if (!ensure(ctx, ctx->recs, sizeof(GaussRec) * (size_t)(G + 1)) ||
+        !ensure(ctx, ctx->footprints, sizeof(uint64_t) * (size_t)(G + 1)) ||
+        !ensure(ctx, ctx->frag_off, sizeof(uint64_t) * (size_t)(G + 1)) ||
+        !ensure(ctx, ctx->root_bits, sizeof(uint64_t) * 512) || !ensure(ctx, ctx->root_prefix, sizeof(uint64_t) * 512) ||
+        !ensure(ctx, ctx->root_of_rank, sizeof(uint32_t) * 32768) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(G > 512 ? G : 512) * 2))
+        return VOX_ERR_MEMORY;
+    GaussRec* recs = (GaussRec*)ctx->recs.p;
+    uint64_t* footprints = (uint64_t*)ctx->footprints.p;
+    uint64_t* frag_off = (uint64_t*)ctx->frag_off.p;
+    uint64_t* root_bits = (uint64_t*)ctx->root_bits.p;
+    uint64_t* root_prefix = (uint64_t*)ctx->root_prefix.p;
+    cudaMemsetAsync(root_bits, 0, sizeof(uint64_t) * 512, s);
+    PrepParams P;
+    P.means = gs->means;
+    P.quats = gs->quats;
+    P.scales = gs->scales;
+    P.opac = gs->opacities;
+    P.colors = gs->colors;
+    P.count = G;
+    P.raw = (flags & VOX_FLAG_RAW_INPUTS) ? 1 : 0;
+    P.voxel_size = voxel_size;
+    P.cull_scale = cull;
+    launch_prep(P, recs, footprints, root_bits, d_err, s);
+    uint64_t* scan_status = (uint64_t*)ctx->scan_status.p;
+    size_t scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    scan_exclusive_u64(footprints, frag_off, G, 0, sc + SC_F, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
+                       d_counter, d_err, ctx->num_sms, s);
+    scan_exclusive_u64(root_bits, root_prefix, 512, 1, sc + SC_NROOT, scan_status,
+                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    launch_invert_bits(root_bits, root_prefix, 512, (uint32_t*)ctx->root_of_rank.p, s);
+    int rc = sync_scalars(ctx, "prep");
+    if (rc)
+        return rc;
+    const uint64_t F = ctx->hscal[SC_F];
+    const uint64_t NR = ctx->hscal[SC_NROOT];
+    ctx->stats.candidates = (int64_t)F;
+
+    // ------------------------------------------------------- lower ranks
+    const int64_t lwords = (int64_t)(NR > 0 ? NR : 1) * 512;
+    if (!ensure(ctx, ctx->lower_bits, sizeof(uint64_t) * lwords) ||
+        !ensure(ctx, ctx->lower_prefix, sizeof(uint64_t) * lwords) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(lwords > G ? lwords : G) * 2))
+        return VOX_ERR_MEMORY;
+    scan_status = (uint64_t*)ctx->scan_status.p;
+    scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    uint64_t* lower_bits = (uint64_t*)ctx->lower_bits.p;
+    uint64_t* lower_prefix = (uint64_t*)ctx->lower_prefix.p;
+    cudaMemsetAsync(lower_bits, 0, sizeof(uint64_t) * lwords, s);
+    launch_mark_lower(recs, G, root_bits, root_prefix, lower_bits, s);
+    scan_exclusive_u64(lower_bits, lower_prefix, lwords, 1, sc + SC_NLOWER, scan_status,
+                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    rc = sync_scalars(ctx, "lower ranks");
+    if (rc)
+        return rc;
+    const uint64_t NL = ctx->hscal[SC_NLOWER];
+    if (!ensure(ctx, ctx->lower_cell, sizeof(uint32_t) * (NL + 1)))
+        return VOX_ERR_MEMORY;
+    launch_invert_bits(lower_bits, lower_prefix, lwords, (uint32_t*)ctx->lower_cell.p, s);
+    const int key_bits = 21 + bits_for(NL > 1 ? NL : 2);
+    const int key64 = key_bits > 32 ? 1 : 0;
+    ctx->key64 = key64;
+    ctx->stats.key_bits = key_bits;
+    cudaEventRecord(ctx->timers.ev[1], s);
+
+    // ---------------------------------------------------------------- emit
+    RankTables T{ root_bits, root_prefix, lower_bits, lower_prefix };
+    const size_t kb = key64 ? 8 : 4;
+    uint64_t cap = ctx->pair_cap;
+    if (cap == 0)
+        cap = F / 3 + 1024;
+    if (cap > F)
+        cap = F > 0 ? F : 1;
+    int64_t P_pairs = 0;
+    for (int attempt = 0; attempt < 2; attempt++)
+    {
+        int64_t etiles = emit_tile_count(F);
+        if (!ensure(ctx, ctx->keys, kb * cap) || !ensure(ctx, ctx->ids, 4 * cap) ||
+            !ensure(ctx, ctx->emit_status, sizeof(uint64_t) * (size_t)(etiles + 1)))
+            return VOX_ERR_MEMORY;
+        EmitParams E;
+        E.recs = recs;
+        E.frag_off = frag_off;
+        E.G = G;
+        E.F = F;
+        E.voxel_size = voxel_size;
+        E.cap = cap;
+        E.status = (uint64_t*)ctx->emit_status.p;
+        E.epoch = ctx->emit_epochs.next(E.status, ctx->emit_status.cap / sizeof(uint64_t), s);
+        E.counter = d_counter;
+        E.total = sc + SC_P;
+        E.err = d_err;
+        if (key64)
+            launch_emit_u64(E, T, (uint64_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, ctx->num_sms, s);
+        else
+            launch_emit_u32(E, T, (uint32_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, ctx->num_sms, s);
+        rc = sync_scalars(ctx, "emit");
+        if (rc)
+            return rc;
+        P_pairs = (int64_t)ctx->hscal[SC_P];
+        if ((uint64_t)P_pairs <= cap)
+            break;
+        cap = (uint64_t)P_pairs + P_pairs / 16 + 1024;
+        // clear the capacity flag and retry once with the exact size
+        cudaMemsetAsync(d_err, 0, sizeof(int), s);
+    }
+    if ((uint64_t)P_pairs > cap)
+    {
+        set_error(ctx, "emit: pair buffer overflow");
+        return VOX_ERR_MEMORY;
+    }
+    if ((uint64_t)P_pairs >= 0xFFFFFFF0ull)
+    {
+        set_error(ctx, "emit: %lld pairs exceed the 32-bit pair index range", (long long)P_pairs);
+        return VOX_ERR_SIZE;
+    }
+    ctx->pair_cap = cap;
+    ctx->stats.pairs = P_pairs;
+    ctx->last_P = P_pairs;
+    cudaEventRecord(ctx->timers.ev[2], s);
+
+    // ---------------------------------------------------------------- sort
+    if (!ensure(ctx, ctx->keys_alt, kb * (size_t)(P_pairs + 1)) || !ensure(ctx, ctx->ids_alt, 4 * (size_t)(P_pairs + 1)) ||
+        !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(P_pairs, (int)kb)))
+        return VOX_ERR_MEMORY;
+    int in_alt;
+    if (key64)
+        in_alt = sort_pairs_u64((uint64_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, (uint64_t*)ctx->keys_alt.p,
+                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, d_err, ctx->num_sms, s,
+                                ctx->tuning);
+    else
+        in_alt = sort_pairs_u32((uint32_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, (uint32_t*)ctx->keys_alt.p,
+                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, d_err, ctx->num_sms, s,
+                                ctx->tuning);
+    ctx->sorted_in_alt = in_alt;
+    ctx->stats.sort_passes = (key_bits + ctx->tuning.digit_bits - 1) / ctx->tuning.digit_bits;
+    const void* skeys = in_alt ? ctx->keys_alt.p : ctx->keys.p;
+    const uint32_t* sids = (const uint32_t*)(in_alt ? ctx->ids_alt.p : ctx->ids.p);
+    cudaEventRecord(ctx->timers.ev[3], s);
+
+    // ---------------------------------------------------------------- runs
+    const int64_t rtiles = runs_tile_count(P_pairs);
+    if (!ensure(ctx, ctx->vox_start, 4 * (size_t)(P_pairs + 2)) || !ensure(ctx, ctx->leaf_vstart, 4 * (size_t)(P_pairs + 2)) ||
+        !ensure(ctx, ctx->lower_lstart, 4 * (size_t)(NL + 2)) || !ensure(ctx, ctx->lower_rank, 4 * (size_t)(NL + 2)) ||
+        !ensure(ctx, ctx->run_status, sizeof(uint64_t) * 3 * (size_t)(rtiles + 1)))
+        return VOX_ERR_MEMORY;
+    RunParams Rp;
+    Rp.P = P_pairs;
+    Rp.vox_start = (uint32_t*)ctx->vox_start.p;
+    Rp.leaf_vstart = (uint32_t*)ctx->leaf_vstart.p;
+    Rp.lower_lstart = (uint32_t*)ctx->lower_lstart.p;
+    Rp.lower_rank = (uint32_t*)ctx->lower_rank.p;
+    Rp.counts = sc + SC_V;
+    Rp.status = (uint64_t*)ctx->run_status.p;
+    Rp.epoch = ctx->run_epochs.next(Rp.status, ctx->run_status.cap / sizeof(uint64_t), s);
+    Rp.counter = d_counter;
+    Rp.err = d_err;
+    if (P_pairs == 0)
+    {
+        cudaMemsetAsync(Rp.vox_start, 0, 4, s);
+        cudaMemsetAsync(Rp.leaf_vstart, 0, 4, s);
+        cudaMemsetAsync(Rp.lower_lstart, 0, 4, s);
+    }
+    launch_runs(Rp, skeys, key64, s);
+    rc = sync_scalars(ctx, "runs");
+    if (rc)
+        return rc;
+    const int64_t V = (int64_t)ctx->hscal[SC_V], L = (int64_t)ctx->hscal[SC_L], Lo = (int64_t)ctx->hscal[SC_LO];
+
+    // ---------------------------------------------------------- node tables
+    if (!ensure(ctx, ctx->lower_origin, 12 * (size_t)(Lo + 1)) || !ensure(ctx, ctx->lower_upper_n, 4 * (size_t)(Lo + 1)) ||
+        !ensure(ctx, ctx->upper_head, 8 * (size_t)(Lo + 1)) || !ensure(ctx, ctx->upper_scan, 8 * (size_t)(Lo + 1)) ||
+        !ensure(ctx, ctx->lower_parent, 4 * (size_t)(Lo + 1)) || !ensure(ctx, ctx->upper_root_n, 4 * (size_t)(Lo + 1)) ||
+        !ensure(ctx, ctx->upper_lostart, 4 * (size_t)(Lo + 2)) || !ensure(ctx, ctx->leaf_lower, 4 * (size_t)(L + 1)) ||
+        !ensure(ctx, ctx->leaf_lower_n, 4 * (size_t)(L + 1)) || !ensure(ctx, ctx->leaf_mask, 64 * (size_t)(L + 1)) ||
+        !ensure(ctx, ctx->leaf_origin, 12 * (size_t)(L + 1)) ||
+        !ensure(ctx, ctx->order, 8 * 3 * (size_t)((Lo + 1) * 2 + (L + 1))) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(Lo + 1) * 2))
+        return VOX_ERR_MEMORY;
+    scan_status = (uint64_t*)ctx->scan_status.p;
+    scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    NodeParams N;
+    N.Lo = Lo;
+    N.L = L;
+    N.lower_rank = (const uint32_t*)ctx->lower_rank.p;
+    N.lower_cell = (const uint32_t*)ctx->lower_cell.p;
+    N.root_of_rank = (const uint32_t*)ctx->root_of_rank.p;
+    N.lower_lstart = (const uint32_t*)ctx->lower_lstart.p;
+    N.leaf_vstart = (const uint32_t*)ctx->leaf_vstart.p;
+    N.vox_start = (const uint32_t*)ctx->vox_start.p;
+    N.lower_origin = (int32_t*)ctx->lower_origin.p;
+    N.lower_upper_n = (uint32_t*)ctx->lower_upper_n.p;
+    N.upper_head = (uint64_t*)ctx->upper_head.p;
+    N.upper_scan = (uint64_t*)ctx->upper_scan.p;
+    N.lower_parent = (uint32_t*)ctx->lower_parent.p;
+    N.upper_root_n = (uint32_t*)ctx->upper_root_n.p;
+    N.upper_lostart = (uint32_t*)ctx->upper_lostart.p;
+    N.upper_count = sc + SC_U;
+    N.leaf_lower = (uint32_t*)ctx->leaf_lower.p;
+    N.leaf_lower_n = (uint32_t*)ctx->leaf_lower_n.p;
+    N.leaf_mask = (uint64_t*)ctx->leaf_mask.p;
+    N.leaf_origin = (int32_t*)ctx->leaf_origin.p;
+    N.bbox = (int32_t*)(sc + SC_BBOX);
+    uint64_t* ord = (uint64_t*)ctx->order.p;
+    N.upper_idx = ord;
+    N.upper_addr = ord + (Lo + 1);
+    N.upper_vidx = ord + 2 * (Lo + 1);
+    N.lower_idx = ord + 3 * (Lo + 1);
+    N.lower_addr = ord + 4 * (Lo + 1);
+    N.lower_vidx = ord + 5 * (Lo + 1);
+    N.leaf_idx = ord + 6 * (Lo + 1);
+    N.leaf_addr = ord + 6 * (Lo + 1) + (L + 1);
+    N.leaf_vidx = ord + 6 * (Lo + 1) + 2 * (L + 1);
+    {
+        int32_t bb[6] = { 0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, (int32_t)0x80000000, (int32_t)0x80000000,
+                          (int32_t)0x80000000 };
+        cudaMemcpyAsync(N.bbox, bb, sizeof(bb), cudaMemcpyHostToDevice, s);
+    }
+    launch_lower_info(N, s);
+    scan_exclusive_u64(N.upper_head, N.upper_scan, Lo, 0, sc + SC_SCRATCH + 1, scan_status,
+                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    launch_upper_info(N, s);
+    launch_leaf_tables(N, skeys, key64, s);
+    rc = sync_scalars(ctx, "node tables");
+    if (rc)
+        return rc;
+    const uint64_t U = Lo > 0 ? ctx->hscal[SC_U] : 0;
+    launch_canonical_order(N, U, s);
+
+    // --------------------------------------------------------- grid buffer
+    const uint64_t node2_bytes = n2_node_bytes(0) + U * n2_node_bytes(1) + (uint64_t)Lo * n2_node_bytes(2) +
+                                 (uint64_t)L * n2_node_bytes(3);
+    const uint64_t value_count = 2 + (uint64_t)V;
+    auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
+    const uint64_t off_node2 = VOX_GRID_HEADER_BYTES;
+    const uint64_t off_bbox = al(off_node2 + node2_bytes);
+    const uint64_t off_rgba = al(off_bbox + 32);
+    const uint64_t off_dens = al(off_rgba + 4 * value_count);
+    const uint64_t off_col = al(off_dens + 4 * value_count);
+    const uint64_t grid_bytes = al(off_col + 12 * value_count);
+    if (!ensure(ctx, ctx->grid, grid_bytes))
+        return VOX_ERR_MEMORY;
+    uint8_t* grid = (uint8_t*)ctx->grid.p;
+    cudaMemsetAsync(grid, 0, grid_bytes, s);
+    launch_write_nodes(N, U, grid + off_node2, s);
+    cudaEventRecord(ctx->timers.ev[4], s);
+    AccumParams A;
+    A.recs = recs;
+    A.keys = skeys;
+    A.voxel_size = voxel_size;
+    A.rgba8 = (uint32_t*)(grid + off_rgba);
+    A.density = (float*)(grid + off_dens);
+    A.color = (float*)(grid + off_col);
+    launch_accumulate(A, N, sids, key64, s);
+    cudaEventRecord(ctx->timers.ev[5], s);
+    rc = sync_scalars(ctx, "accumulate");
+    if (rc)
+        return rc;
+    rc = check_cuda(ctx, "accumulate");
+    if (rc)
+        return rc;
+
+    vox_grid_header_t h;
+    memset(&h, 0, sizeof(h));
+    h.magic = VOX_GRID_MAGIC;
+    h.version = 1;
+    h.header_bytes = VOX_GRID_HEADER_BYTES;
+    h.grid_bytes = grid_bytes;
+    h.node2_offset = off_node2;
+    h.node2_bytes = node2_bytes;
+    h.upper_count = (uint32_t)U;
+    h.lower_count = (uint32_t)Lo;
+    h.leaf_count = (uint32_t)L;
+    h.node_order = (flags & VOX_FLAG_WINDOW_ORDER) ? 1u : 0u;
+    h.value_count = value_count;
+    h.bbox_offset = off_bbox;
+    h.rgba8_offset = off_rgba;
+    h.density_offset = off_dens;
+    h.color_offset = off_col;
+    h.voxel_size = voxel_size;
+    memcpy(h.bbox, &ctx->hscal[SC_BBOX], sizeof(h.bbox));
+    if (V == 0)
+        memset(h.bbox, 0, sizeof(h.bbox));
+    h.pair_count = (uint64_t)P_pairs;
+    h.candidate_count = F;
+    memcpy(ctx->hscal + SC_SCRATCH * 2, &h, sizeof(h));
+    cudaMemcpyAsync(grid, ctx->hscal + SC_SCRATCH * 2, sizeof(h), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(grid + off_bbox, h.bbox, sizeof(h.bbox), cudaMemcpyHostToDevice, s);
+    cudaEventRecord(ctx->timers.ev[6], s);
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+        return check_cuda(ctx, "finalize");
+
+    ctx->last_grid_bytes = grid_bytes;
+    vox_stats_t& st = ctx->stats;
+    st.voxels = V;
+    st.uppers = (int64_t)U;
+    st.lowers = Lo;
+    st.leaves = L;
+    st.value_count = (int64_t)value_count;
+    st.grid_bytes = (int64_t)grid_bytes;
+    st.ms_prep = elapsed(ctx->timers.ev[0], ctx->timers.ev[1]);
+    st.ms_emit = elapsed(ctx->timers.ev[1], ctx->timers.ev[2]);
+    st.ms_sort = elapsed(ctx->timers.ev[2], ctx->timers.ev[3]);
+    st.ms_build = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]);
+    st.ms_accumulate = elapsed(ctx->timers.ev[4], ctx->timers.ev[5]);
+    st.ms_total = elapsed(ctx->timers.ev[0], ctx->timers.ev[6]);
+    return VOX_OK;
+}
+
+// hierarchical key of a compact key: rank -> cell -> (root_n, upper_n)
+__global__ void k_export_keys(const void* keys, int key64, const uint32_t* lower_cell, const uint32_t* root_of_rank,
+                              int64_t n, uint64_t* out)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    uint64_t k = key64 ? ((const uint64_t*)keys)[i] : (uint64_t)((const uint32_t*)keys)[i];
+    uint32_t cell = lower_cell[k >> 21];
+    uint64_t rn = root_of_rank[cell >> 15];
+    out[i] = (rn << 36) | ((uint64_t)(cell & 32767u) << 21) | (k & ((1ull << 21) - 1ull));
+}
+
+// ---------------------------------------------------------------------------
+// vox_* C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+vox_context_t* vox_context_create(int device)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0)
+    {
+        cudaGetLastError();
+        set_error(nullptr, "vox_context_create: no CUDA device");
+        return nullptr;
+    }
+    if (device < 0 || device >= count)
+        device = 0;
+    vox_context_t* ctx = new vox_context_t();
+    ctx->device = device;
+    cudaSetDevice(device);
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost((void**)&ctx->hscal, sizeof(uint64_t) * SC_SCRATCH * 8) != cudaSuccess)
+    {
+        set_error(nullptr, "vox_context_create: stream / pinned allocation failed");
+        delete ctx;
+        return nullptr;
+    }
+    for (auto& e : ctx->timers.ev)
+        cudaEventCreate(&e);
+    return ctx;
+}
+
+void vox_context_destroy(vox_context_t* ctx)
+{
+    if (!ctx)
+        return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    DevBuf* all[] = { &ctx->recs, &ctx->footprints, &ctx->frag_off, &ctx->root_bits, &ctx->root_prefix,
+                      &ctx->root_of_rank, &ctx->lower_bits, &ctx->lower_prefix, &ctx->lower_cell, &ctx->scan_status,
+                      &ctx->emit_status, &ctx->run_status, &ctx->keys, &ctx->ids, &ctx->keys_alt, &ctx->ids_alt,
+                      &ctx->sort_ws, &ctx->vox_start, &ctx->leaf_vstart, &ctx->lower_lstart, &ctx->lower_rank,
+                      &ctx->lower_origin, &ctx->lower_upper_n, &ctx->upper_head, &ctx->upper_scan,
+                      &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
+                      &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
+                      &ctx->hier_keys };
+    for (DevBuf* b : all)
+        if (b->p)
+            cudaFree(b->p);
+    for (auto& e : ctx->timers.ev)
+        if (e)
+            cudaEventDestroy(e);
+    if (ctx->hscal)
+        cudaFreeHost(ctx->hscal);
+    if (ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+void* vox_context_stream(vox_context_t* ctx)
+{
+    return ctx ? (void*)ctx->stream : nullptr;
+}
+
+const char* vox_last_error(vox_context_t* ctx)
+{
+    return ctx ? ctx->last_error.c_str() : "no context";
+}
+
+int vox_voxelize(vox_context_t* ctx, const vox_gaussians_t* gaussians, float voxel_size, float cull_scale,
+                 uint32_t flags, void** grid, uint64_t* grid_bytes)
+{
+    int rc = run_voxelize(ctx, gaussians, voxel_size, cull_scale, flags);
+    if (rc)
+        return rc;
+    if (grid)
+        *grid = ctx->grid.p;
+    if (grid_bytes)
+        *grid_bytes = ctx->last_grid_bytes;
+    return VOX_OK;
+}
+
+int vox_voxelize_host(vox_context_t* ctx, const vox_gaussians_t* gaussians, float voxel_size, float cull_scale,
+                      uint32_t flags, void* out, uint64_t out_capacity, uint64_t* grid_bytes)
+{
+    if (!ctx || !gaussians)
+        return VOX_ERR_ARGS;
+    cudaSetDevice(ctx->device);
+    const int64_t n = gaussians->count;
+    DevBuf& in = ctx->hier_keys; // reused as the attribute upload area between calls
+    const size_t per = 16 * sizeof(float);
+    if (!ensure(ctx, in, per * (size_t)(n + 1)))
+        return VOX_ERR_MEMORY;
+    float* d = (float*)in.p;
+    vox_gaussians_t dg;
+    dg.count = n;
+    dg.means = d;
+    dg.quats = d + 3 * n;
+    dg.scales = d + 7 * n;
+    dg.opacities = d + 10 * n;
+    dg.colors = d + 11 * n;
+    if (n > 0)
+    {
+        cudaMemcpyAsync((void*)dg.means, gaussians->means, 12 * n, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.quats, gaussians->quats, 16 * n, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.scales, gaussians->scales, 12 * n, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.opacities, gaussians->opacities, 4 * n, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.colors, gaussians->colors, 12 * n, cudaMemcpyHostToDevice, ctx->stream);
+    }
+    int rc = run_voxelize(ctx, &dg, voxel_size, cull_scale, flags);
+    if (rc)
+        return rc;
+    if (grid_bytes)
+        *grid_bytes = ctx->last_grid_bytes;
+    if (!out)
+        return VOX_OK;
+    if (out_capacity < ctx->last_grid_bytes)
+    {
+        set_error(ctx, "vox_voxelize_host: output capacity %llu < grid size %llu", (unsigned long long)out_capacity,
+                  (unsigned long long)ctx->last_grid_bytes);
+        return VOX_ERR_SIZE;
+    }
+    cudaMemcpyAsync(out, ctx->grid.p, ctx->last_grid_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return check_cuda(ctx, "vox_voxelize_host copy");
+    return VOX_OK;
+}
+
+int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity)
+{
+    if (!ctx || !out)
+        return VOX_ERR_ARGS;
+    if (capacity < ctx->last_grid_bytes)
+        return VOX_ERR_SIZE;
+    cudaSetDevice(ctx->device);
+    cudaMemcpyAsync(out, ctx->grid.p, ctx->last_grid_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return check_cuda(ctx, "vox_copy_grid");
+    return VOX_OK;
+}
+
+int vox_copy_pairs(vox_context_t* ctx, uint64_t* keys, uint32_t* ids, int64_t capacity)
+{
+    if (!ctx)
+        return VOX_ERR_ARGS;
+    const int64_t P = ctx->last_P;
+    if (capacity < P)
+        return VOX_ERR_SIZE;
+    if (P == 0)
+        return VOX_OK;
+    cudaSetDevice(ctx->device);
+    DevBuf tmp;
+    if (!ensure(ctx, tmp, 8 * (size_t)P))
+        return VOX_ERR_MEMORY;
+    const void* skeys = ctx->sorted_in_alt ? ctx->keys_alt.p : ctx->keys.p;
+    const void* sids = ctx->sorted_in_alt ? ctx->ids_alt.p : ctx->ids.p;
+    k_export_keys<<<(unsigned)((P + 255) / 256), 256, 0, ctx->stream>>>(
+        skeys, ctx->key64, (const uint32_t*)ctx->lower_cell.p, (const uint32_t*)ctx->root_of_rank.p, P,
+        (uint64_t*)tmp.p);
+    if (keys)
+        cudaMemcpyAsync(keys, tmp.p, 8 * (size_t)P, cudaMemcpyDeviceToHost, ctx->stream);
+    if (ids)
+        cudaMemcpyAsync(ids, sids, 4 * (size_t)P, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(tmp.p);
+    if (e != cudaSuccess)
+        return check_cuda(ctx, "vox_copy_pairs");
+    return VOX_OK;
+}
+
+void vox_get_stats(vox_context_t* ctx, vox_stats_t* out)
+{
+    if (ctx && out)
+        *out = ctx->stats;
+}
+
+} // extern "C"

@@ -1,0 +1,439 @@
+// vox_device.cuh - device-side building blocks of the Gaussian -> node2 path.
+//
+// Floating-point contract: every operation that decides topology or an RGBA8
+// byte is a single IEEE operation with round-to-nearest and no contraction
+// (VOX_F* macros -> __f*_rn), so results are bit-identical to the host
+// restatement of the reference shaders.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "vox_detmath.h"
+
+namespace vox
+{
+
+// ------------------------------------------------------------------------
+// node2 layout (nanovdb_editor/PNanoVDBExt.h:49-81), offsets in 64-bit words
+// ------------------------------------------------------------------------
+constexpr uint32_t N2_OFF_NODE_IDX = 0;
+constexpr uint32_t N2_OFF_VALUE_IDX = 1;
+__host__ __device__ constexpr uint32_t n2_off_value_prefix(int t)
+{
+    return t == 0 ? 258u : t == 1 ? 258u : t == 2 ? 34u : 6u;
+}
+__host__ __device__ constexpr uint32_t n2_off_value_mask(int t)
+{
+    return t == 0 ? 386u : t == 1 ? 386u : t == 2 ? 50u : 8u;
+}
+__host__ __device__ constexpr uint32_t n2_off_child_prefix(int t)
+{
+    return t == 0 ? 898u : t == 1 ? 898u : t == 2 ? 114u : 6u;
+}
+__host__ __device__ constexpr uint32_t n2_off_child_mask(int t)
+{
+    return t == 0 ? 1026u : t == 1 ? 1026u : t == 2 ? 130u : 8u;
+}
+constexpr uint32_t N2_OFF_KEY_PREFIX_ROOT = 1538;
+constexpr uint32_t N2_OFF_KEY_MASK_ROOT = 1666;
+__host__ __device__ constexpr uint32_t n2_off_children(int t)
+{
+    return t == 0 ? 2180u : t == 1 ? 1538u : t == 2 ? 194u : 16u;
+}
+__host__ __device__ constexpr uint64_t n2_node_bytes(int t)
+{
+    return t == 0 ? 541728ull : t == 1 ? 274464ull : t == 2 ? 34336ull : 128ull;
+}
+constexpr uint64_t N2_END_KEY = 1ull << 63;
+
+// n = coordinate -> child slot (PNanoVDBExt.h:93-101)
+__device__ __forceinline__ uint32_t root_n_of(int32_t x, int32_t y, int32_t z)
+{
+    return ((((uint32_t)x & 0x1FFFFu) >> 12) << 10) | ((((uint32_t)y & 0x1FFFFu) >> 12) << 5) |
+           (((uint32_t)z & 0x1FFFFu) >> 12);
+}
+__device__ __forceinline__ uint32_t upper_n_of(int32_t x, int32_t y, int32_t z)
+{
+    return ((((uint32_t)x & 0xFFFu) >> 7) << 10) | ((((uint32_t)y & 0xFFFu) >> 7) << 5) | (((uint32_t)z & 0xFFFu) >> 7);
+}
+__device__ __forceinline__ uint32_t lower_n_of(int32_t x, int32_t y, int32_t z)
+{
+    return ((((uint32_t)x & 0x7Fu) >> 3) << 8) | ((((uint32_t)y & 0x7Fu) >> 3) << 4) | (((uint32_t)z & 0x7Fu) >> 3);
+}
+__device__ __forceinline__ uint32_t leaf_n_of(int32_t x, int32_t y, int32_t z)
+{
+    return (((uint32_t)x & 7u) << 6) | (((uint32_t)y & 7u) << 3) | ((uint32_t)z & 7u);
+}
+
+// ------------------------------------------------------------------------
+// per-Gaussian record, written once by the prep kernel (128 B, 16B aligned)
+// ------------------------------------------------------------------------
+struct __align__(16) GaussRec
+{
+    float4 q0; // pos.xyz, inv_ls = 1/ls
+    float4 q1; // rinv[0][0..2], rinv[1][0]
+    float4 q2; // rinv[1][1..2], rinv[2][0..1]
+    float4 q3; // rinv[2][2], inv_s.xyz = 1/s (clamped scale)
+    int4 q4;   // bbox min xyz, valid
+    int4 q5;   // bbox range xyz (max + 1 - min), unused
+    float4 q6; // opacity, ls, e = 1 / (0.1 |s| / voxel_size), |s|
+    float4 q7; // rgb, culled (1.f if |s| > cull scale)
+};
+
+struct PrepParams
+{
+    const float* means;   // 3G
+    const float* quats;   // 4G, w x y z (raw or normalised)
+    const float* scales;  // 3G (log-scale when raw)
+    const float* opac;    // G (logit when raw)
+    const float* colors;  // 3G RGB (SH0 when raw)
+    int64_t count;
+    int raw;              // 1: apply the host preprocessing of raster/RasterUtils.cpp:59-117
+    float voxel_size;
+    float cull_scale;     // > 0
+};
+
+// dot with the reference's fixed evaluation order (a.x*b.x + a.y*b.y) + a.z*b.z
+__device__ __forceinline__ float dot3_rn(float ax, float ay, float az, float bx, float by, float bz)
+{
+    return VOX_FADD(VOX_FADD(VOX_FMUL(ax, bx), VOX_FMUL(ay, by)), VOX_FMUL(az, bz));
+}
+
+__device__ __forceinline__ bool finite_f(float v)
+{
+    return v == v && VOX_FSUB(v, v) == 0.f;
+}
+
+// Builds the record of one Gaussian (gaussian_prim.slang:47-144 and the
+// per-Gaussian prologue of gaussian_frag_alloc.slang / gaussian_frag_color.slang).
+// Returns the bbox footprint (0 when the Gaussian emits nothing).
+__device__ __forceinline__ uint64_t make_record(const PrepParams& P, int64_t g, GaussRec& R, int32_t bmax[3])
+{
+    float pos[3] = { P.means[3 * g + 0], P.means[3 * g + 1], P.means[3 * g + 2] };
+    float qw = P.quats[4 * g + 0], qx = P.quats[4 * g + 1], qy = P.quats[4 * g + 2], qz = P.quats[4 * g + 3];
+    float s[3] = { P.scales[3 * g + 0], P.scales[3 * g + 1], P.scales[3 * g + 2] };
+    float op = P.opac[g];
+    float rgb[3] = { P.colors[3 * g + 0], P.colors[3 * g + 1], P.colors[3 * g + 2] };
+    if (P.raw)
+    {
+        // raster/RasterUtils.cpp:59-117
+        float ss = VOX_FADD(VOX_FADD(VOX_FADD(VOX_FMUL(qx, qx), VOX_FMUL(qy, qy)), VOX_FMUL(qz, qz)), VOX_FMUL(qw, qw));
+        float mi = VOX_FDIV(1.f, VOX_FSQRT(ss));
+        qx = VOX_FMUL(qx, mi);
+        qy = VOX_FMUL(qy, mi);
+        qz = VOX_FMUL(qz, mi);
+        qw = VOX_FMUL(qw, mi);
+        for (int a = 0; a < 3; a++)
+            s[a] = vox_expf_cr(s[a]);
+        const float c0 = 0.28209479177387814f;
+        for (int a = 0; a < 3; a++)
+            rgb[a] = VOX_FADD(VOX_FMUL(c0, rgb[a]), 0.5f);
+        op = VOX_FDIV(1.f, VOX_FADD(1.f, vox_expf_cr(-op)));
+    }
+    const float vs = P.voxel_size;
+    const float vs_inv = VOX_FDIV(1.f, vs);
+
+    bool ok = finite_f(op) && finite_f(qx) && finite_f(qy) && finite_f(qz) && finite_f(qw);
+    for (int a = 0; a < 3; a++)
+        ok = ok && finite_f(pos[a]) && finite_f(s[a]) && s[a] > 0.f;
+    float lg = ok ? vox_logf(VOX_FDIV(op, 0.01f)) : 0.f;
+    float ls = VOX_FSQRT(VOX_FMUL(2.f, lg));
+    const float min_scale = VOX_FMUL(0.125f, vs);
+    for (int a = 0; a < 3; a++)
+        s[a] = s[a] > min_scale ? s[a] : min_scale;
+    ok = ok && lg > 0.f && finite_f(ls);
+
+    // rotation rows (gaussian_prim.slang:83-90); inverse rows are the transpose
+    float r[3][3];
+    r[0][0] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(qy, qy), VOX_FMUL(qz, qz))));
+    r[0][1] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(qx, qy), VOX_FMUL(qz, qw)));
+    r[0][2] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(qx, qz), VOX_FMUL(qy, qw)));
+    r[1][0] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(qx, qy), VOX_FMUL(qz, qw)));
+    r[1][1] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(qx, qx), VOX_FMUL(qz, qz))));
+    r[1][2] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(qy, qz), VOX_FMUL(qx, qw)));
+    r[2][0] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(qx, qz), VOX_FMUL(qy, qw)));
+    r[2][1] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(qy, qz), VOX_FMUL(qx, qw)));
+    r[2][2] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(qx, qx), VOX_FMUL(qy, qy))));
+
+    // bbox of the 8 transformed box corners.  Each output coordinate is
+    // fl(fl(t0 + t1) + t2) + pos with t_a = +-fl(fl(s_a * ls) * r_ra); rounding
+    // is monotone, so the corner minimum / maximum is reached with every
+    // t_a = -|.| / +|.|, identical to the reference's 8-corner loop.
+    int32_t bmin[3];
+    uint64_t footprint = 0;
+    if (ok)
+    {
+        float u[3] = { VOX_FMUL(s[0], ls), VOX_FMUL(s[1], ls), VOX_FMUL(s[2], ls) };
+        footprint = 1;
+        for (int a = 0; a < 3; a++)
+        {
+            float m = VOX_FADD(VOX_FADD(fabsf(VOX_FMUL(u[0], r[a][0])), fabsf(VOX_FMUL(u[1], r[a][1]))),
+                               fabsf(VOX_FMUL(u[2], r[a][2])));
+            float lo = VOX_FMUL(VOX_FSUB(pos[a], m), vs_inv);
+            float hi = VOX_FMUL(VOX_FADD(pos[a], m), vs_inv);
+            bmin[a] = (int32_t)floorf(lo);
+            bmax[a] = (int32_t)floorf(hi);
+            footprint *= (uint64_t)(int64_t)(bmax[a] + 1 - bmin[a]);
+        }
+    }
+    else
+    {
+        bmin[0] = bmin[1] = bmin[2] = 0;
+        bmax[0] = bmax[1] = bmax[2] = -1;
+    }
+
+    float scale1d = VOX_FSQRT(dot3_rn(s[0], s[1], s[2], s[0], s[1], s[2]));
+    float vrs = VOX_FDIV(VOX_FMUL(0.1f, scale1d), vs);
+    float e = VOX_FDIV(1.f, vrs);
+    float culled = scale1d > P.cull_scale ? 1.f : 0.f;
+
+    R.q0 = make_float4(pos[0], pos[1], pos[2], VOX_FDIV(1.f, ls));
+    R.q1 = make_float4(r[0][0], r[1][0], r[2][0], r[0][1]);
+    R.q2 = make_float4(r[1][1], r[2][1], r[0][2], r[1][2]);
+    R.q3 = make_float4(r[2][2], VOX_FDIV(1.f, s[0]), VOX_FDIV(1.f, s[1]), VOX_FDIV(1.f, s[2]));
+    R.q4 = make_int4(bmin[0], bmin[1], bmin[2], ok ? 1 : 0);
+    R.q5 = make_int4(bmax[0] + 1 - bmin[0], bmax[1] + 1 - bmin[1], bmax[2] + 1 - bmin[2], 0);
+    R.q6 = make_float4(op, ls, e, scale1d);
+    R.q7 = make_float4(rgb[0], rgb[1], rgb[2], culled);
+    return footprint;
+}
+
+// inverse rotation rows from the record: rinv[row][axis]
+struct RInv
+{
+    float m[3][3];
+};
+__device__ __forceinline__ RInv rinv_of(const GaussRec& R)
+{
+    RInv o;
+    o.m[0][0] = R.q1.x;
+    o.m[0][1] = R.q1.y;
+    o.m[0][2] = R.q1.z;
+    o.m[1][0] = R.q1.w;
+    o.m[1][1] = R.q2.x;
+    o.m[1][2] = R.q2.y;
+    o.m[2][0] = R.q2.z;
+    o.m[2][1] = R.q2.w;
+    o.m[2][2] = R.q3.x;
+    return o;
+}
+
+// Local AABB of a voxel in the Gaussian's unit-sphere space
+// (gaussian_frag_alloc.slang:84-131).  The reference transforms the 8 voxel
+// corners; every local coordinate is fl(fl(fl(p_x + p_y) + p_z) * inv_ls) * inv_s
+// with p_a = fl(c_a * rinv[row][a]) and c_a one of two corner values per axis.
+// Rounded addition and multiplication by a positive constant are monotone, so
+// the corner minimum (maximum) is the same expression over the per-axis
+// minimum (maximum) products - bit-identical to the 8-corner loop.
+struct Aabb
+{
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ void axis_corners(float vs, float pos, int32_t i, float& c0, float& c1)
+{
+    float v0 = (float)i;
+    float v1 = VOX_FADD(v0, 1.f);
+    c0 = VOX_FSUB(VOX_FMUL(v0, vs), pos);
+    c1 = VOX_FSUB(VOX_FMUL(v1, vs), pos);
+}
+
+__device__ __forceinline__ void minmax_prod(float c0, float c1, float r, float& mn, float& mx)
+{
+    float p0 = VOX_FMUL(c0, r), p1 = VOX_FMUL(c1, r);
+    mn = p0 < p1 ? p0 : p1;
+    mx = p0 < p1 ? p1 : p0;
+}
+
+__device__ __forceinline__ Aabb voxel_local_aabb(const GaussRec& R, const RInv& M, float vs, int32_t i, int32_t j,
+                                                 int32_t k)
+{
+    float cx0, cx1, cy0, cy1, cz0, cz1;
+    axis_corners(vs, R.q0.x, i, cx0, cx1);
+    axis_corners(vs, R.q0.y, j, cy0, cy1);
+    axis_corners(vs, R.q0.z, k, cz0, cz1);
+    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
+    Aabb b;
+#pragma unroll
+    for (int row = 0; row < 3; row++)
+    {
+        float xn, xx, yn, yx, zn, zx;
+        minmax_prod(cx0, cx1, M.m[row][0], xn, xx);
+        minmax_prod(cy0, cy1, M.m[row][1], yn, yx);
+        minmax_prod(cz0, cz1, M.m[row][2], zn, zx);
+        float lo = VOX_FADD(VOX_FADD(xn, yn), zn);
+        float hi = VOX_FADD(VOX_FADD(xx, yx), zx);
+        b.lo[row] = VOX_FMUL(VOX_FMUL(lo, R.q0.w), inv_s[row]);
+        b.hi[row] = VOX_FMUL(VOX_FMUL(hi, R.q0.w), inv_s[row]);
+    }
+    return b;
+}
+
+// dist2 test of gaussian_frag_alloc.slang:132-162
+__device__ __forceinline__ bool aabb_hits_unit_sphere(const Aabb& b)
+{
+    float d2 = 1.f;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        if (0.f < b.lo[a])
+            d2 = VOX_FSUB(d2, VOX_FMUL(b.lo[a], b.lo[a]));
+        else if (0.f > b.hi[a])
+            d2 = VOX_FSUB(d2, VOX_FMUL(b.hi[a], b.hi[a]));
+    }
+    return d2 > 0.f;
+}
+
+// Alpha of a passing (voxel, Gaussian) pair (gaussian_frag_color.slang:184-213).
+// The reference takes the maximum of op * exp(-ls * |p|^2) over a 4x4x4
+// lattice p = w * hi + (1 - w) * lo.  |p|^2 = fl(fl(x^2 + y^2) + z^2) is
+// monotone in each per-axis square and exp (vox_expf_cr) is monotone, so the
+// maximum is the lattice point with the per-axis smallest square.
+__device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
+{
+    const float third = VOX_FDIV(1.f, 3.f);
+    float m[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        float best = 0.f;
+#pragma unroll
+        for (int s = 0; s < 4; s++)
+        {
+            float w = VOX_FMUL(third, (float)s);
+            float ow = VOX_FSUB(1.f, w);
+            float p = VOX_FADD(VOX_FMUL(w, b.hi[a]), VOX_FMUL(ow, b.lo[a]));
+            float sq = VOX_FMUL(p, p);
+            best = (s == 0 || sq < best) ? sq : best;
+        }
+        m[a] = best;
+    }
+    float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
+    float a = VOX_FMUL(R.q6.x, vox_expf_cr(-VOX_FMUL(R.q6.y, d)));
+    a = a > 0.f ? a : 0.f;
+    a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), R.q6.z));
+    if (R.q7.w != 0.f)
+        a = 0.f;
+    return a;
+}
+
+__device__ __forceinline__ uint32_t pack_rgba8(const GaussRec& R, float a)
+{
+    float ch[4] = { R.q7.x, R.q7.y, R.q7.z, a };
+    uint32_t out = 0;
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+    {
+        float v = ch[c] < 1.f ? ch[c] : 1.f;
+        v = 0.f > v ? 0.f : v;
+        out |= ((uint32_t)VOX_FMUL(255.f, v)) << (8 * c);
+    }
+    return out;
+}
+
+// ------------------------------------------------------------------------
+// decoupled look-back status words: [63:56] epoch, [55] inclusive flag,
+// [54:0] value.  Epoch 0 means "not yet written in this use".
+// ------------------------------------------------------------------------
+constexpr uint64_t LB_VALUE_MASK = (1ull << 55) - 1ull;
+constexpr uint64_t LB_INCL = 1ull << 55;
+constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
+
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p)
+{
+    uint64_t v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Publishes `aggregate` for `tile`, walks predecessors and returns the
+// exclusive prefix.  Every wait is bounded; on timeout *err is set and the
+// partial prefix is returned (the host treats the call as failed).
+__device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_t tile, uint64_t aggregate,
+                                                       uint32_t epoch, int* err, size_t stride = 1)
+{
+    const uint64_t tag = (uint64_t)epoch << 56;
+    if (tile == 0)
+    {
+        st_release_u64(&status[0], tag | LB_INCL | (aggregate & LB_VALUE_MASK));
+        return 0;
+    }
+    st_release_u64(&status[tile * stride], tag | (aggregate & LB_VALUE_MASK));
+    uint64_t excl = 0;
+    int64_t p = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (p >= 0)
+    {
+        uint64_t s = ld_acquire_u64(&status[(uint64_t)p * stride]);
+        if ((s >> 56) != epoch)
+        {
+            if (++spins > LB_SPIN_LIMIT)
+            {
+                atomicExch(err, 1);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        excl += s & LB_VALUE_MASK;
+        if (s & LB_INCL)
+            break;
+        p--;
+    }
+    st_release_u64(&status[tile * stride], tag | LB_INCL | ((excl + aggregate) & LB_VALUE_MASK));
+    return excl;
+}
+
+// ------------------------------------------------------------------------
+// warp / block scans
+// ------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t warp_incl_scan_u64(uint64_t v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        uint64_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o)
+            v += t;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one u64 per thread (blockDim.x a multiple of
+// 32, <= 1024).  s_warp must hold 33 words.  All threads must call it.
+__device__ __forceinline__ uint64_t block_excl_scan_u64(uint64_t v, uint64_t* s_warp, uint64_t& total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    uint64_t incl = warp_incl_scan_u64(v);
+    if (lane == 31)
+        s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0)
+    {
+        uint64_t w = lane < nwarps ? s_warp[lane] : 0;
+        uint64_t wi = warp_incl_scan_u64(w);
+        if (lane < nwarps)
+            s_warp[lane] = wi - w;
+        if (lane == nwarps - 1)
+            s_warp[32] = wi;
+    }
+    __syncthreads();
+    total = s_warp[32];
+    uint64_t r = s_warp[warp] + incl - v;
+    __syncthreads();
+    return r;
+}
+
+// device error word bits
+constexpr int ERR_LOOKBACK = 1;
+constexpr int ERR_RANGE = 2;      // voxel coordinate outside [-65536, 65535]
+constexpr int ERR_FOOTPRINT = 4;  // one Gaussian's bbox above 2^31 fragments
+constexpr int ERR_CAPACITY = 8;   // pair buffer too small (host retries)
+
+} // namespace vox

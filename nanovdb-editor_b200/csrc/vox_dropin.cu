@@ -1,0 +1,528 @@
+// vox_dropin.cu - the reference-compatible function tables:
+// pnanovdb_get_raster() (raster/Raster.cpp:822-840, RasterUtils.cpp) and a
+// headless pnanovdb_get_compute() whose array functions follow
+// nanovdb_editor/putil/Compute.h:838-843.  Every raster entry is a thin
+// wrapper over vox_voxelize / vox_voxelize_host.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "pnanovdb_b200.h"
+
+// ------------------------------------------------------------- queue / device
+struct pnanovdb_compute_device_t
+{
+    int index;
+    pnanovdb_compute_queue_t* queue;
+};
+struct pnanovdb_compute_queue_t
+{
+    int device;
+};
+
+struct pnanovdb_raster_context_t
+{
+    vox_context_t* vox;
+};
+
+struct pnanovdb_raster_gaussian_data_t
+{
+    int64_t n = 0;
+    std::vector<float> means, quats, scales, colors, opacities; // activated
+    float cull_scale = 0.05f;
+    int raw = 0;          // attributes still in the on-disk convention (VOX_FLAG_RAW_INPUTS)
+    float* dev = nullptr; // device copy after upload_gaussian_data
+    int device = 0;
+};
+
+static int queue_device(pnanovdb_compute_queue_t* q)
+{
+    return q ? q->device : 0;
+}
+
+static void log_err(const char* msg)
+{
+    fprintf(stderr, "[pnanovdb_b200] %s\n", msg);
+}
+
+// cull scale from gaussian_frag_color's parameter block (gaussian_frag_color.slang:205-213)
+static float cull_from_params(pnanovdb_compute_array_t** shader_params_arrays)
+{
+    if (!shader_params_arrays)
+        return 0.05f;
+    pnanovdb_compute_array_t* a = shader_params_arrays[PNANOVDB_RASTER_SHADER_GAUSSIAN_FRAG_COLOR];
+    if (!a || !a->data || a->element_size * a->element_count < 8)
+        return 0.05f;
+    float cull;
+    uint32_t use_default;
+    memcpy(&cull, a->data, 4);
+    memcpy(&use_default, (const char*)a->data + 4, 4);
+    if (use_default || cull == 0.f)
+        return 0.05f;
+    return cull;
+}
+
+// ------------------------------------------------------------------ arrays
+static pnanovdb_compute_array_t* PNANOVDB_ABI array_create(size_t element_size, pnanovdb_uint64_t element_count,
+                                                           const void* data)
+{
+    pnanovdb_compute_array_t* a = (pnanovdb_compute_array_t*)calloc(1, sizeof(pnanovdb_compute_array_t));
+    if (!a)
+        return nullptr;
+    size_t bytes = element_size * element_count;
+    a->data = malloc(bytes ? bytes : 1);
+    if (!a->data)
+    {
+        free(a);
+        return nullptr;
+    }
+    if (data && bytes)
+        memcpy(a->data, data, bytes);
+    else if (bytes)
+        memset(a->data, 0, bytes);
+    a->element_size = element_size;
+    a->element_count = element_count;
+    return a;
+}
+static void PNANOVDB_ABI array_destroy(pnanovdb_compute_array_t* a)
+{
+    if (!a)
+        return;
+    free(a->data);
+    free(a);
+}
+static void* PNANOVDB_ABI array_map(pnanovdb_compute_array_t* a)
+{
+    return a ? a->data : nullptr;
+}
+static void PNANOVDB_ABI array_unmap(pnanovdb_compute_array_t*)
+{
+}
+static pnanovdb_compute_array_t* PNANOVDB_ABI array_duplicate(pnanovdb_compute_array_t* a)
+{
+    return a ? array_create(a->element_size, a->element_count, a->data) : nullptr;
+}
+static pnanovdb_compute_array_t* PNANOVDB_ABI load_grid(const char* path)
+{
+    FILE* f = fopen(path, "rb");
+    if (!f)
+        return nullptr;
+    fseek(f, 0, SEEK_END);
+    long bytes = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    pnanovdb_compute_array_t* a = array_create(4, (uint64_t)(bytes + 3) / 4, nullptr);
+    if (a && fread(a->data, 1, (size_t)bytes, f) != (size_t)bytes)
+    {
+        array_destroy(a);
+        a = nullptr;
+    }
+    fclose(f);
+    return a;
+}
+static pnanovdb_bool_t PNANOVDB_ABI save_grid(pnanovdb_compute_array_t* a, const char* path)
+{
+    if (!a || !path)
+        return PNANOVDB_FALSE;
+    FILE* f = fopen(path, "wb");
+    if (!f)
+        return PNANOVDB_FALSE;
+    size_t bytes = a->element_size * a->element_count;
+    bool ok = fwrite(a->data, 1, bytes, f) == bytes;
+    fclose(f);
+    return ok ? PNANOVDB_TRUE : PNANOVDB_FALSE;
+}
+
+// ---------------------------------------------------------- device interface
+static int g_manager_token = 0;
+static void* PNANOVDB_ABI dev_create_manager(pnanovdb_bool_t)
+{
+    return &g_manager_token;
+}
+static void PNANOVDB_ABI dev_destroy_manager(void*)
+{
+}
+static pnanovdb_bool_t PNANOVDB_ABI dev_enumerate(void*, pnanovdb_uint32_t index, void*)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return PNANOVDB_FALSE;
+    }
+    return (int)index < n ? PNANOVDB_TRUE : PNANOVDB_FALSE;
+}
+static pnanovdb_compute_device_t* PNANOVDB_ABI dev_create(void*, const void*)
+{
+    pnanovdb_compute_device_t* d = new pnanovdb_compute_device_t();
+    d->index = 0;
+    d->queue = new pnanovdb_compute_queue_t();
+    d->queue->device = 0;
+    return d;
+}
+static void PNANOVDB_ABI dev_destroy(void*, pnanovdb_compute_device_t* d)
+{
+    if (!d)
+        return;
+    delete d->queue;
+    delete d;
+}
+static pnanovdb_compute_queue_t* PNANOVDB_ABI dev_queue(const pnanovdb_compute_device_t* d)
+{
+    return d ? d->queue : nullptr;
+}
+static int PNANOVDB_ABI dev_flush(pnanovdb_compute_queue_t*, pnanovdb_uint64_t* flushed, void*, void*)
+{
+    if (flushed)
+        *flushed = 0;
+    return 0;
+}
+static void PNANOVDB_ABI dev_wait_idle(pnanovdb_compute_queue_t* q)
+{
+    cudaSetDevice(queue_device(q));
+    cudaDeviceSynchronize();
+}
+static pnanovdb_uint32_t PNANOVDB_ABI dev_index(const pnanovdb_compute_device_t* d)
+{
+    return d ? (pnanovdb_uint32_t)d->index : 0u;
+}
+
+// ------------------------------------------------------------------- raster
+// one cached vox context per device for the one-shot entry points
+static std::mutex g_oneshot_mutex;
+static vox_context_t* g_oneshot[64] = {};
+
+static vox_context_t* oneshot_context(int device)
+{
+    if (device < 0 || device >= 64)
+        device = 0;
+    if (!g_oneshot[device])
+        g_oneshot[device] = vox_context_create(device);
+    return g_oneshot[device];
+}
+
+static pnanovdb_raster_context_t* PNANOVDB_ABI r_create_context(const pnanovdb_compute_t*,
+                                                                  pnanovdb_compute_queue_t* queue)
+{
+    vox_context_t* v = vox_context_create(queue_device(queue));
+    if (!v)
+        return nullptr;
+    pnanovdb_raster_context_t* c = new pnanovdb_raster_context_t();
+    c->vox = v;
+    return c;
+}
+static void PNANOVDB_ABI r_destroy_context(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
+                                           pnanovdb_raster_context_t* c)
+{
+    if (!c)
+        return;
+    vox_context_destroy(c->vox);
+    delete c;
+}
+
+static bool copy_floats(std::vector<float>& dst, pnanovdb_compute_array_t* a, int64_t count)
+{
+    if (!a || !a->data || a->element_size != 4 || (int64_t)a->element_count < count)
+        return false;
+    dst.assign((const float*)a->data, (const float*)a->data + count);
+    return true;
+}
+
+static pnanovdb_raster_gaussian_data_t* PNANOVDB_ABI r_create_gaussian_data(
+    const pnanovdb_compute_t*, pnanovdb_compute_queue_t* queue, pnanovdb_raster_context_t*,
+    pnanovdb_compute_array_t* means, pnanovdb_compute_array_t* quaternions, pnanovdb_compute_array_t* scales,
+    pnanovdb_compute_array_t* colors, pnanovdb_compute_array_t* sh_0, pnanovdb_compute_array_t*,
+    pnanovdb_compute_array_t* opacities, pnanovdb_compute_array_t** shader_params_arrays,
+    pnanovdb_raster_shader_params_t*)
+{
+    if (!means || means->element_size != 4)
+    {
+        log_err("create_gaussian_data: means must be float32");
+        return nullptr;
+    }
+    pnanovdb_raster_gaussian_data_t* d = new pnanovdb_raster_gaussian_data_t();
+    d->n = (int64_t)(means->element_count / 3);
+    d->device = queue_device(queue);
+    bool ok = copy_floats(d->means, means, 3 * d->n) && copy_floats(d->quats, quaternions, 4 * d->n) &&
+              copy_floats(d->scales, scales, 3 * d->n) && copy_floats(d->opacities, opacities, d->n);
+    if (ok && colors)
+        ok = copy_floats(d->colors, colors, 3 * d->n);
+    else if (ok && sh_0)
+    {
+        ok = copy_floats(d->colors, sh_0, 3 * d->n);
+        for (auto& c : d->colors)
+            c = 0.28209479177387814f * c + 0.5f;
+    }
+    if (!ok)
+    {
+        log_err("create_gaussian_data: attribute arrays must be float32 with 3/4/3/3/1 values per Gaussian");
+        delete d;
+        return nullptr;
+    }
+    d->cull_scale = cull_from_params(shader_params_arrays);
+    return d;
+}
+
+static void PNANOVDB_ABI r_upload_gaussian_data(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
+                                                pnanovdb_raster_context_t* ctx, pnanovdb_raster_gaussian_data_t* d)
+{
+    if (!d)
+        return;
+    (void)ctx;
+    cudaSetDevice(d->device);
+    if (d->dev)
+        cudaFree(d->dev);
+    d->dev = nullptr;
+    size_t floats = (size_t)d->n * 14;
+    if (cudaMalloc(&d->dev, floats * 4 + 4) != cudaSuccess)
+    {
+        cudaGetLastError();
+        log_err("upload_gaussian_data: cudaMalloc failed");
+        d->dev = nullptr;
+        return;
+    }
+    int64_t n = d->n;
+    cudaMemcpy(d->dev, d->means.data(), 12 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d->dev + 3 * n, d->quats.data(), 16 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d->dev + 7 * n, d->scales.data(), 12 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d->dev + 10 * n, d->opacities.data(), 4 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d->dev + 11 * n, d->colors.data(), 12 * n, cudaMemcpyHostToDevice);
+}
+
+static void PNANOVDB_ABI r_destroy_gaussian_data(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
+                                                 pnanovdb_raster_gaussian_data_t* d)
+{
+    if (!d)
+        return;
+    if (d->dev)
+    {
+        cudaSetDevice(d->device);
+        cudaFree(d->dev);
+    }
+    delete d;
+}
+
+static void PNANOVDB_ABI r_raster_gaussian_2d(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
+                                              pnanovdb_raster_context_t*, pnanovdb_raster_gaussian_data_t*, void*,
+                                              pnanovdb_uint32_t, pnanovdb_uint32_t, const void*, const void*,
+                                              const pnanovdb_raster_shader_params_t*, pnanovdb_uint32_t)
+{
+    log_err("raster_gaussian_2d: the screen-space splatting path is not provided by this library");
+}
+
+// raster/Raster.cpp:420-558: device Gaussians -> grid in the caller's device buffer
+static void PNANOVDB_ABI r_raster_gaussian_3d(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
+                                              pnanovdb_raster_context_t* ctx, float voxel_size,
+                                              pnanovdb_raster_gaussian_data_t* d, pnanovdb_compute_buffer_t* out,
+                                              pnanovdb_uint64_t word_count, void*)
+{
+    if (!ctx || !d || !out || !out->device_ptr)
+    {
+        log_err("raster_gaussian_3d: missing context, data or output buffer");
+        return;
+    }
+    if (!d->dev)
+        r_upload_gaussian_data(nullptr, nullptr, ctx, d);
+    if (!d->dev)
+        return;
+    vox_gaussians_t g;
+    int64_t n = d->n;
+    g.count = n;
+    g.means = d->dev;
+    g.quats = d->dev + 3 * n;
+    g.scales = d->dev + 7 * n;
+    g.opacities = d->dev + 10 * n;
+    g.colors = d->dev + 11 * n;
+    void* grid = nullptr;
+    uint64_t bytes = 0;
+    if (vox_voxelize(ctx->vox, &g, voxel_size, d->cull_scale, d->raw ? VOX_FLAG_RAW_INPUTS : 0u, &grid, &bytes) !=
+        VOX_OK)
+        return;
+    uint64_t cap = word_count * 4ull;
+    if (out->size_bytes && out->size_bytes < cap)
+        cap = out->size_bytes;
+    if (bytes > cap)
+    {
+        log_err("raster_gaussian_3d: output buffer too small for the grid");
+        return;
+    }
+    cudaMemcpyAsync(out->device_ptr, grid, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)vox_context_stream(ctx->vox));
+    cudaStreamSynchronize((cudaStream_t)vox_context_stream(ctx->vox));
+}
+
+static pnanovdb_compute_array_t* run_host(int device, const vox_gaussians_t* g, float voxel_size, float cull,
+                                          uint32_t flags, pnanovdb_profiler_report_t report, void* userdata)
+{
+    std::lock_guard<std::mutex> lock(g_oneshot_mutex);
+    vox_context_t* v = oneshot_context(device);
+    if (!v)
+        return nullptr;
+    uint64_t bytes = 0;
+    if (vox_voxelize_host(v, g, voxel_size, cull, flags, nullptr, 0, &bytes) != VOX_OK)
+        return nullptr;
+    pnanovdb_compute_array_t* a = array_create(4, (bytes + 3) / 4, nullptr);
+    if (!a)
+        return nullptr;
+    if (vox_copy_grid(v, a->data, bytes) != VOX_OK)
+    {
+        array_destroy(a);
+        return nullptr;
+    }
+    if (report)
+    {
+        vox_stats_t st;
+        vox_get_stats(v, &st);
+        pnanovdb_compute_profiler_entry_t e[5] = { { "prep", 0.f, st.ms_prep * 1e-3f },
+                                                   { "emit", 0.f, st.ms_emit * 1e-3f },
+                                                   { "sort", 0.f, st.ms_sort * 1e-3f },
+                                                   { "build", 0.f, st.ms_build * 1e-3f },
+                                                   { "accumulate", 0.f, st.ms_accumulate * 1e-3f } };
+        report(userdata, 0, 5, e);
+    }
+    return a;
+}
+
+static pnanovdb_compute_array_t* PNANOVDB_ABI r_raster_to_nanovdb(
+    const pnanovdb_compute_t*, pnanovdb_compute_queue_t* queue, float voxel_size, pnanovdb_compute_array_t* means,
+    pnanovdb_compute_array_t* quaternions, pnanovdb_compute_array_t* scales, pnanovdb_compute_array_t* colors,
+    pnanovdb_compute_array_t* sh_0, pnanovdb_compute_array_t* sh_n, pnanovdb_compute_array_t* opacities,
+    pnanovdb_compute_array_t** shader_params_arrays, pnanovdb_profiler_report_t profiler_report, void* userdata)
+{
+    pnanovdb_raster_gaussian_data_t* d = r_create_gaussian_data(nullptr, queue, nullptr, means, quaternions, scales,
+                                                                colors, sh_0, sh_n, opacities, shader_params_arrays,
+                                                                nullptr);
+    if (!d)
+        return nullptr;
+    vox_gaussians_t g;
+    g.count = d->n;
+    g.means = d->means.data();
+    g.quats = d->quats.data();
+    g.scales = d->scales.data();
+    g.opacities = d->opacities.data();
+    g.colors = d->colors.data();
+    pnanovdb_compute_array_t* a = run_host(queue_device(queue), &g, voxel_size, d->cull_scale, 0u, profiler_report,
+                                           userdata);
+    r_destroy_gaussian_data(nullptr, nullptr, d);
+    return a;
+}
+
+static pnanovdb_bool_t PNANOVDB_ABI r_from_arrays(pnanovdb_raster_t*, const pnanovdb_compute_t*,
+                                                  pnanovdb_compute_queue_t* queue, float voxel_size,
+                                                  pnanovdb_compute_array_t** arrays, pnanovdb_uint32_t count,
+                                                  pnanovdb_compute_array_t** out)
+{
+    if (!out || !arrays || count < 5u)
+        return PNANOVDB_FALSE;
+    *out = nullptr;
+    pnanovdb_compute_array_t *m = arrays[0], *o = arrays[1], *q = arrays[2], *s = arrays[3], *c = arrays[4];
+    if (!m || !o || !q || !s || !c || m->element_size != 4 || o->element_size != 4 || q->element_size != 4 ||
+        s->element_size != 4 || c->element_size != 4)
+    {
+        log_err("raster_to_nanovdb_from_arrays: arrays must be float32 [means, opacities, quaternions, scales, sh_0]");
+        return PNANOVDB_FALSE;
+    }
+    int64_t n = (int64_t)(m->element_count / 3);
+    if ((int64_t)o->element_count < n || (int64_t)q->element_count < 4 * n || (int64_t)s->element_count < 3 * n ||
+        (int64_t)c->element_count < 3 * n)
+    {
+        log_err("raster_to_nanovdb_from_arrays: attribute counts do not match means");
+        return PNANOVDB_FALSE;
+    }
+    // raw inputs: the reference preprocesses them on the host in place
+    // (RasterUtils.cpp:59-117); here the same arithmetic runs inside the prep
+    // kernel and the caller's arrays are left untouched.
+    vox_gaussians_t g;
+    g.count = n;
+    g.means = (const float*)m->data;
+    g.quats = (const float*)q->data;
+    g.scales = (const float*)s->data;
+    g.opacities = (const float*)o->data;
+    g.colors = (const float*)c->data;
+    *out = run_host(queue_device(queue), &g, voxel_size, 0.05f, VOX_FLAG_RAW_INPUTS, nullptr, nullptr);
+    return *out ? PNANOVDB_TRUE : PNANOVDB_FALSE;
+}
+
+static pnanovdb_bool_t PNANOVDB_ABI r_create_from_arrays(pnanovdb_raster_t*, const pnanovdb_compute_t*,
+                                                         pnanovdb_compute_queue_t*, pnanovdb_compute_array_t**,
+                                                         pnanovdb_uint32_t, pnanovdb_raster_gaussian_data_t**,
+                                                         pnanovdb_raster_shader_params_t*,
+                                                         pnanovdb_raster_context_t**);
+static pnanovdb_bool_t PNANOVDB_ABI r_raster_file(pnanovdb_raster_t*, const pnanovdb_compute_t*,
+                                                  pnanovdb_compute_queue_t*, const char*, float,
+                                                  pnanovdb_compute_array_t**, pnanovdb_raster_gaussian_data_t**,
+                                                  pnanovdb_raster_context_t**, pnanovdb_compute_array_t**,
+                                                  pnanovdb_raster_shader_params_t*, pnanovdb_profiler_report_t,
+                                                  void*);
+
+static pnanovdb_bool_t PNANOVDB_ABI r_create_from_desc(pnanovdb_raster_t*, const pnanovdb_compute_t*,
+                                                       pnanovdb_compute_queue_t*, const void*, const char*,
+                                                       pnanovdb_raster_gaussian_data_t**,
+                                                       pnanovdb_raster_shader_params_t*, pnanovdb_raster_context_t**)
+{
+    log_err("create_gaussian_data_from_desc: editor descriptors are not provided by this library");
+    return PNANOVDB_FALSE;
+}
+
+#include "vox_npz.inl"
+
+extern "C" {
+
+pnanovdb_compute_t* pnanovdb_get_compute(void)
+{
+    static pnanovdb_compute_t t;
+    static bool init = false;
+    if (!init)
+    {
+        memset(&t, 0, sizeof(t));
+        t.device_interface.create_device_manager = dev_create_manager;
+        t.device_interface.destroy_device_manager = dev_destroy_manager;
+        t.device_interface.enumerate_devices = dev_enumerate;
+        t.device_interface.create_device = dev_create;
+        t.device_interface.destroy_device = dev_destroy;
+        t.device_interface.get_device_queue = dev_queue;
+        t.device_interface.get_compute_queue = dev_queue;
+        t.device_interface.flush = dev_flush;
+        t.device_interface.wait_idle = dev_wait_idle;
+        t.device_interface.get_device_index = dev_index;
+        t.load_nanovdb = load_grid;
+        t.save_nanovdb = save_grid;
+        t.create_array = array_create;
+        t.destroy_array = array_destroy;
+        t.map_array = array_map;
+        t.unmap_array = array_unmap;
+        t.duplicate_array = array_duplicate;
+        init = true;
+    }
+    return &t;
+}
+
+pnanovdb_raster_t* pnanovdb_get_raster(void)
+{
+    static pnanovdb_raster_t r;
+    static bool init = false;
+    if (!init)
+    {
+        memset(&r, 0, sizeof(r));
+        r.compute = pnanovdb_get_compute();
+        r.create_context = r_create_context;
+        r.destroy_context = r_destroy_context;
+        r.create_gaussian_data = r_create_gaussian_data;
+        r.upload_gaussian_data = r_upload_gaussian_data;
+        r.destroy_gaussian_data = r_destroy_gaussian_data;
+        r.raster_gaussian_2d = r_raster_gaussian_2d;
+        r.raster_gaussian_3d = r_raster_gaussian_3d;
+        r.raster_to_nanovdb = r_raster_to_nanovdb;
+        r.raster_file = r_raster_file;
+        r.raster_to_nanovdb_from_arrays = r_from_arrays;
+        r.create_gaussian_data_from_arrays = r_create_from_arrays;
+        r.create_gaussian_data_from_desc = r_create_from_desc;
+        init = true;
+    }
+    return &r;
+}
+
+} // extern "C"

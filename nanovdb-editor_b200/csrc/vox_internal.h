@@ -1,0 +1,78 @@
+// vox_internal.h - interfaces between the CUDA translation units of the
+// Gaussian -> node2 library.  Not part of the public C ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vox
+{
+
+// Bump allocator over one device arena; grows (re-allocates) between calls only.
+struct Arena
+{
+    char* base = nullptr;
+    size_t cap = 0;
+    size_t used = 0;
+    void reset()
+    {
+        used = 0;
+    }
+    template <class T>
+    T* take(size_t count, size_t align = 256)
+    {
+        size_t off = (used + align - 1) / align * align;
+        size_t bytes = count * sizeof(T);
+        if (off + bytes > cap)
+            return nullptr;
+        used = off + bytes;
+        return reinterpret_cast<T*>(base + off);
+    }
+};
+
+// Look-back bookkeeping: each user owns a status region and an epoch counter
+// so that regions need no clearing between uses (epoch wraps every 255 uses,
+// at which point the region is cleared once).
+struct Epochs
+{
+    // A region seen for the first time (new allocation) or after 255 uses is
+    // cleared once; otherwise stale words carry an older epoch and are ignored.
+    uint32_t next(uint64_t* region, size_t words, cudaStream_t s)
+    {
+        if (value == 255 || value == 0 || region != last_region || words != last_words)
+        {
+            cudaMemsetAsync(region, 0, words * sizeof(uint64_t), s);
+            value = 0;
+            last_region = region;
+            last_words = words;
+        }
+        return ++value;
+    }
+    uint32_t value = 0;
+    uint64_t* last_region = nullptr;
+    size_t last_words = 0;
+};
+
+// ---------------------------------------------------------------- scan ----
+// exclusive scan of n u64 values (mode 0) or of popcounts of n u64 words
+// (mode 1); out may alias in; *total receives the sum.
+size_t scan_status_words(int64_t n);
+void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, uint64_t* total, uint64_t* status,
+                        uint32_t epoch, uint32_t* counter, int* err, int num_sms, cudaStream_t s);
+
+// ---------------------------------------------------------------- sort ----
+struct SortTuning
+{
+    int digit_bits = 8; // radix bits per pass (<= 8)
+};
+size_t sort_workspace_bytes(int64_t n, int key_bytes);
+// Stable LSD sort of (key, value) pairs by key bits [0, key_bits).  Uses
+// keys_alt / vals_alt as ping-pong buffers; returns 0 if the result is in
+// keys / vals and 1 if it is in keys_alt / vals_alt.
+int sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
+                   void* workspace, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
+int sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
+                   void* workspace, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
+
+} // namespace vox

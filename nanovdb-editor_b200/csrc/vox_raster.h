@@ -1,0 +1,105 @@
+// vox_raster.h - kernel parameter blocks and launchers of vox_raster.cu.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "vox_device.cuh"
+
+namespace vox
+{
+
+struct RankTables
+{
+    const uint64_t* root_bits;    // 512 words: touched root tiles by root_n
+    const uint64_t* root_prefix;  // exclusive popcount prefix per word
+    const uint64_t* lower_bits;   // roots * 512 words: touched lower cells (root rank, upper_n)
+    const uint64_t* lower_prefix;
+};
+
+struct EmitParams
+{
+    const GaussRec* recs;
+    const uint64_t* frag_off; // exclusive scan of footprints
+    int64_t G;
+    uint64_t F;
+    float voxel_size;
+    uint64_t cap;
+    uint64_t* status;
+    uint32_t epoch;
+    uint32_t* counter;
+    uint64_t* total;
+    int* err;
+};
+
+struct RunParams
+{
+    int64_t P;
+    uint32_t* vox_start;    // [V + 1]
+    uint32_t* leaf_vstart;  // [L + 1]
+    uint32_t* lower_lstart; // [Lo + 1]
+    uint32_t* lower_rank;   // [Lo]
+    uint64_t* counts;       // V, L, Lo
+    uint64_t* status;       // 3 per tile
+    uint32_t epoch;
+    uint32_t* counter;
+    int* err;
+};
+
+struct NodeParams
+{
+    int64_t Lo, L;
+    const uint32_t* lower_rank;
+    const uint32_t* lower_cell;   // lower rank -> cell (root rank << 15 | upper_n)
+    const uint32_t* root_of_rank; // root rank -> root_n
+    const uint32_t* lower_lstart;
+    const uint32_t* leaf_vstart;
+    const uint32_t* vox_start;
+    int32_t* lower_origin;
+    uint32_t* lower_upper_n;
+    uint64_t* upper_head;
+    uint64_t* upper_scan;
+    uint32_t* lower_parent;
+    uint32_t* upper_root_n;
+    uint32_t* upper_lostart;
+    uint64_t* upper_count;
+    uint32_t* leaf_lower;
+    uint32_t* leaf_lower_n;
+    uint64_t* leaf_mask;
+    int32_t* leaf_origin;
+    int32_t* bbox;
+    uint64_t *upper_idx, *upper_addr, *upper_vidx;
+    uint64_t *lower_idx, *lower_addr, *lower_vidx;
+    uint64_t *leaf_idx, *leaf_addr, *leaf_vidx;
+};
+
+struct AccumParams
+{
+    const GaussRec* recs;
+    const void* keys;
+    float voxel_size;
+    uint32_t* rgba8;
+    float* density;
+    float* color;
+};
+
+void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* root_bits, int* err,
+                 cudaStream_t s);
+void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits, const uint64_t* root_prefix,
+                       uint64_t* lower_bits, cudaStream_t s);
+void launch_invert_bits(const uint64_t* bits, const uint64_t* prefix, int64_t words, uint32_t* out, cudaStream_t s);
+void launch_emit_u32(const EmitParams& E, const RankTables& T, uint32_t* out_k, uint32_t* out_i, int num_sms,
+                     cudaStream_t s);
+void launch_emit_u64(const EmitParams& E, const RankTables& T, uint64_t* out_k, uint32_t* out_i, int num_sms,
+                     cudaStream_t s);
+int64_t emit_tile_count(uint64_t F);
+void launch_runs(const RunParams& Rp, const void* keys, int key64, cudaStream_t s);
+int64_t runs_tile_count(int64_t P);
+void launch_lower_info(const NodeParams& N, cudaStream_t s);
+void launch_upper_info(const NodeParams& N, cudaStream_t s);
+void launch_leaf_tables(const NodeParams& N, const void* keys, int key64, cudaStream_t s);
+void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s);
+void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* node2, cudaStream_t s);
+void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s);
+
+} // namespace vox

@@ -1,0 +1,185 @@
+"""Low-level binding of the library's vox_* entry points (include/pnanovdb_b200.h).
+
+``VoxContext.voxelize`` takes CUDA tensors (device pointers, no copies) and
+returns the grid as a ``NodeGrid`` on the host or leaves it on the device;
+``voxelize_host`` takes numpy arrays and times host<->device copies inside
+the call (the end-to-end path of ``raster_to_nanovdb``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, Structure, byref, c_char_p, c_float, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+from .exceptions import PipelineError
+from .grid import NodeGrid
+from .utils import load_library
+
+FLAG_RAW_INPUTS = 1
+FLAG_WINDOW_ORDER = 2
+
+STATUS = {
+    0: "ok",
+    -1: "invalid arguments",
+    -2: "CUDA error",
+    -3: "out of device memory",
+    -4: "voxel coordinate outside [-65536, 65535]",
+    -5: "Gaussian bbox covers 2^31 or more voxels",
+    -6: "bounded device wait expired",
+    -7: "buffer too small",
+}
+
+
+class vox_gaussians_t(Structure):
+    _fields_ = [
+        ("means", c_void_p),
+        ("quats", c_void_p),
+        ("scales", c_void_p),
+        ("opacities", c_void_p),
+        ("colors", c_void_p),
+        ("count", c_int64),
+    ]
+
+
+class vox_stats_t(Structure):
+    _fields_ = [
+        ("gaussians", c_int64),
+        ("candidates", c_int64),
+        ("pairs", c_int64),
+        ("voxels", c_int64),
+        ("uppers", c_int64),
+        ("lowers", c_int64),
+        ("leaves", c_int64),
+        ("value_count", c_int64),
+        ("grid_bytes", c_int64),
+        ("key_bits", c_int32),
+        ("sort_passes", c_int32),
+        ("ms_prep", c_float),
+        ("ms_emit", c_float),
+        ("ms_sort", c_float),
+        ("ms_build", c_float),
+        ("ms_accumulate", c_float),
+        ("ms_total", c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def _lib():
+    lib = load_library("pnanovdbcompute")
+    if not getattr(lib, "_vox_bound", False):
+        lib.vox_context_create.restype = c_void_p
+        lib.vox_context_create.argtypes = [c_int]
+        lib.vox_context_destroy.argtypes = [c_void_p]
+        lib.vox_context_stream.restype = c_void_p
+        lib.vox_context_stream.argtypes = [c_void_p]
+        lib.vox_last_error.restype = c_char_p
+        lib.vox_last_error.argtypes = [c_void_p]
+        lib.vox_voxelize.restype = c_int
+        lib.vox_voxelize.argtypes = [c_void_p, POINTER(vox_gaussians_t), c_float, c_float, c_uint32, POINTER(c_void_p), POINTER(c_uint64)]
+        lib.vox_voxelize_host.restype = c_int
+        lib.vox_voxelize_host.argtypes = [c_void_p, POINTER(vox_gaussians_t), c_float, c_float, c_uint32, c_void_p, c_uint64, POINTER(c_uint64)]
+        lib.vox_copy_grid.restype = c_int
+        lib.vox_copy_grid.argtypes = [c_void_p, c_void_p, c_uint64]
+        lib.vox_copy_pairs.restype = c_int
+        lib.vox_copy_pairs.argtypes = [c_void_p, c_void_p, c_void_p, c_int64]
+        lib.vox_get_stats.argtypes = [c_void_p, POINTER(vox_stats_t)]
+        lib._vox_bound = True
+    return lib
+
+
+def _ptr(t) -> int:
+    if t is None:
+        return 0
+    if hasattr(t, "data_ptr"):
+        return int(t.data_ptr())
+    return int(t.ctypes.data)
+
+
+class VoxContext:
+    """One CUDA stream + persistent device buffers on one device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib()
+        self.handle = self.lib.vox_context_create(int(device))
+        if not self.handle:
+            raise PipelineError("vox_context_create failed (no CUDA device?)")
+        self.last_grid_bytes = 0
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.vox_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.vox_context_stream(self.handle) or 0)
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.lib.vox_last_error(self.handle).decode(errors="replace")
+            raise PipelineError(f"{what}: {STATUS.get(rc, rc)}: {msg}")
+
+    @staticmethod
+    def _gauss(means, quats, scales, opacities, colors) -> vox_gaussians_t:
+        n = int(means.shape[0]) if len(means.shape) > 1 else int(means.shape[0]) // 3
+        g = vox_gaussians_t()
+        g.means, g.quats, g.scales, g.opacities, g.colors = (
+            _ptr(means),
+            _ptr(quats),
+            _ptr(scales),
+            _ptr(opacities),
+            _ptr(colors),
+        )
+        g.count = n
+        return g
+
+    def voxelize(self, means, quats, scales, opacities, colors, voxel_size, cull_scale=0.05, flags=0):
+        """Device tensors in (contiguous float32 CUDA tensors); returns (device ptr, bytes).
+
+        The caller must have finished producing the inputs (e.g. torch.cuda.synchronize()).
+        """
+        g = self._gauss(means, quats, scales, opacities, colors)
+        ptr = c_void_p()
+        nbytes = c_uint64()
+        rc = self.lib.vox_voxelize(self.handle, byref(g), float(voxel_size), float(cull_scale), int(flags), byref(ptr), byref(nbytes))
+        self._check(rc, "vox_voxelize")
+        self.last_grid_bytes = int(nbytes.value)
+        return int(ptr.value or 0), int(nbytes.value)
+
+    def voxelize_host(self, means, quats, scales, opacities, colors, voxel_size, cull_scale=0.05, flags=0) -> NodeGrid:
+        """numpy float32 arrays in, host grid out (copies counted in the call)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (means, quats, scales, opacities, colors)]
+        g = self._gauss(*arrs)
+        nbytes = c_uint64()
+        rc = self.lib.vox_voxelize_host(self.handle, byref(g), float(voxel_size), float(cull_scale), int(flags), None, 0, byref(nbytes))
+        self._check(rc, "vox_voxelize_host")
+        self.last_grid_bytes = int(nbytes.value)
+        return self.grid()
+
+    def grid(self) -> NodeGrid:
+        out = np.empty(self.last_grid_bytes, dtype=np.uint8)
+        self._check(self.lib.vox_copy_grid(self.handle, out.ctypes.data, out.nbytes), "vox_copy_grid")
+        return NodeGrid(out)
+
+    def pairs(self):
+        st = self.stats()
+        n = int(st["pairs"])
+        keys = np.empty(n, dtype=np.uint64)
+        ids = np.empty(n, dtype=np.uint32)
+        self._check(self.lib.vox_copy_pairs(self.handle, keys.ctypes.data, ids.ctypes.data, n), "vox_copy_pairs")
+        return keys, ids
+
+    def stats(self) -> dict:
+        st = vox_stats_t()
+        self.lib.vox_get_stats(self.handle, byref(st))
+        return st.as_dict()

@@ -1,0 +1,145 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/libvox_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker; never by the product.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import c_float, c_int, c_int64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libvox_oracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref_shaders.so")
+
+COUNT_NAMES = ["G", "G_valid", "F", "P", "V", "upper", "lower", "leaf", "value_count", "node2_bytes", "windows", "error"]
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    else:
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def build_ref() -> str | None:
+    """Compiles the reference's shaders as C++ when the reference checkout exists."""
+    script = os.path.join(HERE, "ref_shaders", "build_ref.sh")
+    subprocess.run(["sh", script], check=True, stdout=subprocess.DEVNULL)
+    return REF_PATH if os.path.exists(REF_PATH) else None
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.ov_run.restype = c_void_p
+        L.ov_run.argtypes = [c_int64] + [c_void_p] * 5 + [c_float, c_float, c_int, c_int]
+        L.ov_destroy.argtypes = [c_void_p]
+        L.ov_counts.argtypes = [c_void_p, c_void_p]
+        L.ov_node2_bytes.restype = c_int64
+        L.ov_node2_bytes.argtypes = [c_void_p, c_void_p]
+        L.ov_pairs.argtypes = [c_void_p, c_void_p, c_void_p]
+        L.ov_values.argtypes = [c_void_p] + [c_void_p] * 5
+        L.ov_voxels.argtypes = [c_void_p, c_void_p, c_void_p]
+        L.ov_bbox.argtypes = [c_void_p, c_void_p]
+        L.ov_node_table.argtypes = [c_void_p] + [c_void_p] * 4
+        L.ov_preprocess.argtypes = [c_int64] + [c_void_p] * 8
+        L.ov_prim_bbox.restype = c_int
+        L.ov_prim_bbox.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_float, c_void_p, c_void_p]
+        L.ov_frag_test.restype = c_int
+        L.ov_frag_test.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_float, c_void_p, c_void_p, c_void_p]
+        L.ov_frag_rgba.restype = ctypes.c_uint32
+        L.ov_frag_rgba.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_void_p, c_float, c_float, c_void_p, c_void_p]
+        L.ov_hier_key.restype = ctypes.c_uint64
+        L.ov_hier_key.argtypes = [ctypes.c_int32] * 3
+        _LIB = L
+    return _LIB
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def preprocess(raw):
+    """A2 restatement: raw [means, logit, quats, log scales, sh0, sh_n] -> activated dict."""
+    means, logit, quats, log_s, sh0 = (_f32(raw[i]) for i in range(5))
+    n = means.reshape(-1, 3).shape[0]
+    q = np.empty((n, 4), np.float32)
+    s = np.empty((n, 3), np.float32)
+    o = np.empty(n, np.float32)
+    c = np.empty((n, 3), np.float32)
+    lib().ov_preprocess(n, quats.ctypes.data, log_s.ctypes.data, logit.ctypes.data, sh0.ctypes.data, q.ctypes.data, s.ctypes.data, o.ctypes.data, c.ctypes.data)
+    return {"means": means.reshape(n, 3), "quats": q, "scales": s, "opacities": o, "colors": c}
+
+
+class OracleResult:
+    def __init__(self, cloud, voxel_size, cull_scale=0.0, window_mode=0, nthreads=None):
+        L = lib()
+        self._keep = [_f32(cloud[k]) for k in ("means", "quats", "scales", "colors", "opacities")]
+        n = self._keep[0].reshape(-1, 3).shape[0]
+        nthreads = nthreads or max(1, min(16, os.cpu_count() or 1))
+        self.h = L.ov_run(n, *[a.ctypes.data for a in self._keep], float(voxel_size), float(cull_scale), int(window_mode), int(nthreads))
+        cnt = np.zeros(12, np.int64)
+        L.ov_counts(self.h, cnt.ctypes.data)
+        self.counts = dict(zip(COUNT_NAMES, cnt.tolist()))
+
+    def close(self):
+        if self.h:
+            lib().ov_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def node2(self) -> np.ndarray:
+        out = np.empty(self.counts["node2_bytes"], np.uint8)
+        lib().ov_node2_bytes(self.h, out.ctypes.data)
+        return out
+
+    def pairs(self):
+        P = self.counts["P"]
+        k = np.empty(P, np.uint64)
+        i = np.empty(P, np.uint32)
+        lib().ov_pairs(self.h, k.ctypes.data, i.ctypes.data)
+        return k, i
+
+    def values(self):
+        vc = self.counts["value_count"]
+        rgba = np.empty(vc, np.uint32)
+        d = np.empty(vc, np.float32)
+        c = np.empty((vc, 3), np.float32)
+        d64 = np.empty(vc, np.float64)
+        c64 = np.empty((vc, 3), np.float64)
+        lib().ov_values(self.h, rgba.ctypes.data, d.ctypes.data, c.ctypes.data, d64.ctypes.data, c64.ctypes.data)
+        return {"rgba8": rgba, "density": d, "color": c, "density64": d64, "color64": c64}
+
+    def voxels(self):
+        V = self.counts["V"]
+        ijk = np.empty((V, 3), np.int32)
+        vidx = np.empty(V, np.uint64)
+        lib().ov_voxels(self.h, ijk.ctypes.data, vidx.ctypes.data)
+        return ijk, vidx
+
+    def bbox(self):
+        b = np.empty(6, np.int32)
+        lib().ov_bbox(self.h, b.ctypes.data)
+        return b
+
+
+def hier_key(i, j, k) -> int:
+    return int(lib().ov_hier_key(int(i), int(j), int(k)))

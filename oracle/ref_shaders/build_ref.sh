@@ -1,0 +1,31 @@
+#!/bin/sh
+# Builds oracle/_ref/libref_shaders.so: the reference's per-thread raster
+# shaders compiled as C++ straight from the reference checkout.  Test
+# infrastructure only; the outputs are git-ignored and nothing in the product
+# links them.  The only source change is mechanical and made on the fly:
+# Slang attributes / system-value semantics are stripped and the `.xxx`
+# scalar swizzle is spelled as a float3 broadcast.  Skips (exit 0) when the
+# reference checkout is absent.
+set -e
+REF="${VOX_REFERENCE_DIR:-/root/reference}"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/../_ref"
+if [ ! -d "$REF/raster/shaders" ]; then
+    echo "reference checkout not found at $REF; skipping oracle/_ref"
+    exit 0
+fi
+mkdir -p "$OUT"
+for s in gaussian_prim gaussian_frag_alloc gaussian_frag_color fanout_scatter_prim_idxs fanout_compute_fragment_idxs; do
+    sed -e '/^#define PNANOVDB_/d' \
+        -e '/^#include "PNanoVDB/d' \
+        -e 's/\[require([^]]*)\]//g' \
+        -e 's/\[shader("compute")\]//g' \
+        -e 's/\[numthreads([^]]*)\]//g' \
+        -e 's/ : SV_Group[A-Za-z]*//g' \
+        -e 's/\([A-Za-z_][A-Za-z_0-9.]*\)\.xxx/float3(\1)/g' \
+        "$REF/raster/shaders/$s.slang" > "$OUT/$s.inc"
+done
+${CXX:-g++} -O2 -fPIC -std=c++17 -ffp-contract=off -w -Wno-narrowing \
+    -I"$HERE" -I"$HERE/../../include" -I"$OUT" \
+    -shared -o "$OUT/libref_shaders.so" "$HERE/ref_driver.cpp"
+echo "built $OUT/libref_shaders.so"

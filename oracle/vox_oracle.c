@@ -1,0 +1,1053 @@
+/*
+ * vox_oracle.c - CPU restatement of the reference's Gaussian -> node2 path.
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+ * bench's CPU-baseline leg as the checker.  Never part of the product path.
+ *
+ * Every function restates the reference file:line it follows; the shader
+ * arithmetic is written literally (8 corners, 64 alpha samples) so that it is
+ * independent of the product kernels' optimised formulation.  Floating-point
+ * evaluation order: one IEEE operation at a time, no FMA (built with
+ * -ffp-contract=off); dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z; the shader's
+ * exp is vox_expf_cr (monotone), log and pow are vox_logf / vox_powf, all from
+ * vox_detmath.h.
+ */
+#include "vox_oracle.h"
+#include "vox_detmath.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------ */
+/* node2 layout constants (nanovdb_editor/PNanoVDBExt.h:49-81)              */
+/* ------------------------------------------------------------------------ */
+static const uint32_t N2_OFF_VALUE_PREFIX[4] = { 258, 258, 34, 6 };
+static const uint32_t N2_OFF_VALUE_MASK[4] = { 386, 386, 50, 8 };
+static const uint32_t N2_OFF_CHILD_PREFIX[4] = { 898, 898, 114, 6 };
+static const uint32_t N2_OFF_CHILD_MASK[4] = { 1026, 1026, 130, 8 };
+static const uint32_t N2_OFF_KEY_PREFIX_ROOT = 1538;
+static const uint32_t N2_OFF_KEY_MASK_ROOT = 1666;
+static const uint32_t N2_OFF_CHILDREN[4] = { 2180, 1538, 194, 16 };
+static const uint32_t N2_MAX_SIZE[4] = { 541728, 274464, 34336, 128 };
+static const uint32_t N2_IJK_MASK[4] = { 0x1FFFF, 0xFFF, 0x7F, 0x7 };
+static const uint32_t N2_FANOUT_BITS[4] = { 5, 5, 4, 3 };
+static const uint32_t N2_TILEDIM_BITS[4] = { 12, 7, 3, 0 };
+static const uint32_t N2_FANOUT[4] = { 32768, 32768, 4096, 512 };
+static const uint64_t N2_END_KEY = 1ull << 63;
+
+/* PNanoVDBExt.h:93-101 */
+static uint32_t n2_coord_to_n(int type, int32_t x, int32_t y, int32_t z)
+{
+    uint32_t m = N2_IJK_MASK[type], t = N2_TILEDIM_BITS[type], b = N2_FANOUT_BITS[type];
+    return ((((uint32_t)x & m) >> t) << (b + b)) | ((((uint32_t)y & m) >> t) << b) | (((uint32_t)z & m) >> t);
+}
+
+/* hierarchical order key: root_n | upper_n | lower_n | leaf_n (51 bits) */
+uint64_t ov_hier_key(int32_t i, int32_t j, int32_t k)
+{
+    return ((uint64_t)n2_coord_to_n(0, i, j, k) << 36) | ((uint64_t)n2_coord_to_n(1, i, j, k) << 21) |
+           ((uint64_t)n2_coord_to_n(2, i, j, k) << 9) | (uint64_t)n2_coord_to_n(3, i, j, k);
+}
+
+/* ------------------------------------------------------------------------ */
+/* A2 preprocessing: raster/RasterUtils.cpp:59-117                           */
+/* ------------------------------------------------------------------------ */
+void ov_preprocess(int64_t n, const float* quat_raw, const float* log_scale, const float* opacity_logit,
+                   const float* sh0, float* quat_out, float* scale_out, float* opacity_out, float* color_out)
+{
+    for (int64_t p = 0; p < n; p++)
+    {
+        /* :61-73 quaternion stored w,x,y,z */
+        float x = quat_raw[4 * p + 1], y = quat_raw[4 * p + 2], z = quat_raw[4 * p + 3], w = quat_raw[4 * p + 0];
+        float ss = VOX_FADD(VOX_FADD(VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(y, y)), VOX_FMUL(z, z)), VOX_FMUL(w, w));
+        float magn_inv = VOX_FDIV(1.f, VOX_FSQRT(ss));
+        quat_out[4 * p + 1] = VOX_FMUL(x, magn_inv);
+        quat_out[4 * p + 2] = VOX_FMUL(y, magn_inv);
+        quat_out[4 * p + 3] = VOX_FMUL(z, magn_inv);
+        quat_out[4 * p + 0] = VOX_FMUL(w, magn_inv);
+        /* :81-88 */
+        for (int a = 0; a < 3; a++)
+            scale_out[3 * p + a] = vox_expf_cr(log_scale[3 * p + a]);
+        /* :95-105 */
+        const float c0 = 0.28209479177387814f;
+        for (int a = 0; a < 3; a++)
+            color_out[3 * p + a] = VOX_FADD(VOX_FMUL(c0, sh0[3 * p + a]), 0.5f);
+        /* :112-117 */
+        opacity_out[p] = VOX_FDIV(1.f, VOX_FADD(1.f, vox_expf_cr(-opacity_logit[p])));
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* per-Gaussian setup shared by gaussian_prim / frag_alloc / frag_color      */
+/* ------------------------------------------------------------------------ */
+typedef struct
+{
+    float pos[3];
+    float q[4]; /* x, y, z, w as the shader reads them (gaussian_prim.slang:53-56) */
+    float s[3]; /* clamped scale */
+    float op;
+    float ls;
+    float rgb[3];
+    int valid;
+    int32_t bmin[3], bmax[3];
+    uint64_t footprint;
+} prim_t;
+
+static float dot3(const float* a, const float* b)
+{
+    return VOX_FADD(VOX_FADD(VOX_FMUL(a[0], b[0]), VOX_FMUL(a[1], b[1])), VOX_FMUL(a[2], b[2]));
+}
+
+/* rotation rows, gaussian_prim.slang:83-90 (forward) */
+static void rot_rows(const float* q, float r[3][3])
+{
+    float x = q[0], y = q[1], z = q[2], w = q[3];
+    r[0][0] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, y), VOX_FMUL(z, z))));
+    r[0][1] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, y), VOX_FMUL(z, w)));
+    r[0][2] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, z), VOX_FMUL(y, w)));
+    r[1][0] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, y), VOX_FMUL(z, w)));
+    r[1][1] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(z, z))));
+    r[1][2] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(y, z), VOX_FMUL(x, w)));
+    r[2][0] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, z), VOX_FMUL(y, w)));
+    r[2][1] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, z), VOX_FMUL(x, w)));
+    r[2][2] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(y, y))));
+}
+/* inverse rows, gaussian_frag_alloc.slang:106-114 */
+static void rot_inv_rows(const float* q, float r[3][3])
+{
+    float x = q[0], y = q[1], z = q[2], w = q[3];
+    r[0][0] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, y), VOX_FMUL(z, z))));
+    r[0][1] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, y), VOX_FMUL(z, w)));
+    r[0][2] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, z), VOX_FMUL(y, w)));
+    r[1][0] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, y), VOX_FMUL(z, w)));
+    r[1][1] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(z, z))));
+    r[1][2] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, z), VOX_FMUL(x, w)));
+    r[2][0] = VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, z), VOX_FMUL(y, w)));
+    r[2][1] = VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(y, z), VOX_FMUL(x, w)));
+    r[2][2] = VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(y, y))));
+}
+
+static int ov_isfinite(float v)
+{
+    return v == v && v - v == 0.f;
+}
+
+/* gaussian_prim.slang:47-144.  Gaussians whose opacity is not above the 0.01
+ * cutoff (sqrt(2 log(op/0.01)) undefined or zero) emit nothing: a deliberate
+ * fix of the reference's NaN cutoff radius for those inputs. */
+static void prim_setup(prim_t* P, const float* mean, const float* quat_wxyz, const float* scale, float opacity,
+                       const float* color, float vs)
+{
+    float vs_inv = VOX_FDIV(1.f, vs); /* GridBuild.cpp:780 */
+    P->pos[0] = mean[0];
+    P->pos[1] = mean[1];
+    P->pos[2] = mean[2];
+    P->q[0] = quat_wxyz[1];
+    P->q[1] = quat_wxyz[2];
+    P->q[2] = quat_wxyz[3];
+    P->q[3] = quat_wxyz[0];
+    P->op = opacity;
+    if (color)
+    {
+        P->rgb[0] = color[0];
+        P->rgb[1] = color[1];
+        P->rgb[2] = color[2];
+    }
+    int ok = ov_isfinite(opacity);
+    for (int a = 0; a < 3; a++)
+        ok = ok && ov_isfinite(mean[a]) && ov_isfinite(scale[a]) && scale[a] > 0.f;
+    for (int a = 0; a < 4; a++)
+        ok = ok && ov_isfinite(quat_wxyz[a]);
+    float lg = ok ? vox_logf(VOX_FDIV(opacity, 0.01f)) : 0.f;
+    P->ls = VOX_FSQRT(VOX_FMUL(2.f, lg));
+    const float min_scale = VOX_FMUL(0.125f, vs); /* :67-68 */
+    for (int a = 0; a < 3; a++)
+        P->s[a] = scale[a] > min_scale ? scale[a] : min_scale;
+    P->valid = ok && lg > 0.f && ov_isfinite(P->ls);
+    P->footprint = 0;
+    if (!P->valid)
+    {
+        P->bmin[0] = P->bmin[1] = P->bmin[2] = 0;
+        P->bmax[0] = P->bmax[1] = P->bmax[2] = -1;
+        return;
+    }
+    float r[3][3];
+    rot_rows(P->q, r);
+    for (int v = 0; v < 8; v++)
+    {
+        float c[3];
+        c[0] = (v & 1) ? 1.f : -1.f;
+        c[1] = (v & 2) ? 1.f : -1.f;
+        c[2] = (v & 4) ? 1.f : -1.f;
+        for (int a = 0; a < 3; a++)
+        {
+            c[a] = VOX_FMUL(c[a], P->s[a]);
+            c[a] = VOX_FMUL(c[a], P->ls);
+        }
+        float p[3] = { dot3(c, r[0]), dot3(c, r[1]), dot3(c, r[2]) };
+        int32_t ijk[3];
+        for (int a = 0; a < 3; a++)
+        {
+            p[a] = VOX_FADD(p[a], P->pos[a]);
+            ijk[a] = (int32_t)floorf(VOX_FMUL(p[a], vs_inv));
+        }
+        for (int a = 0; a < 3; a++)
+        {
+            if (v == 0 || ijk[a] < P->bmin[a])
+                P->bmin[a] = ijk[a];
+            if (v == 0 || ijk[a] > P->bmax[a])
+                P->bmax[a] = ijk[a];
+        }
+    }
+    P->footprint = (uint64_t)(P->bmax[0] + 1 - P->bmin[0]) * (uint64_t)(P->bmax[1] + 1 - P->bmin[1]) *
+                   (uint64_t)(P->bmax[2] + 1 - P->bmin[2]);
+}
+
+/* gaussian_frag_alloc.slang:84-162: returns 1 when dist2 > 0 */
+static int frag_test(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float* vmin, float* vmax)
+{
+    float inv_ls = VOX_FDIV(1.f, P->ls);
+    float inv_s[3] = { VOX_FDIV(1.f, P->s[0]), VOX_FDIV(1.f, P->s[1]), VOX_FDIV(1.f, P->s[2]) };
+    for (int v = 0; v < 8; v++)
+    {
+        float vp[3] = { (float)ijk[0], (float)ijk[1], (float)ijk[2] };
+        if (v & 1)
+            vp[0] = VOX_FADD(vp[0], 1.f);
+        if (v & 2)
+            vp[1] = VOX_FADD(vp[1], 1.f);
+        if (v & 4)
+            vp[2] = VOX_FADD(vp[2], 1.f);
+        float lp[3];
+        for (int a = 0; a < 3; a++)
+            lp[a] = VOX_FSUB(VOX_FMUL(vp[a], vs), P->pos[a]);
+        float l[3] = { dot3(lp, rinv[0]), dot3(lp, rinv[1]), dot3(lp, rinv[2]) };
+        for (int a = 0; a < 3; a++)
+        {
+            l[a] = VOX_FMUL(l[a], inv_ls);
+            l[a] = VOX_FMUL(l[a], inv_s[a]);
+            if (v == 0 || l[a] < vmin[a])
+                vmin[a] = l[a];
+            if (v == 0 || l[a] > vmax[a])
+                vmax[a] = l[a];
+        }
+    }
+    float dist2 = 1.f;
+    for (int a = 0; a < 3; a++)
+    {
+        if (0.f < vmin[a])
+            dist2 = VOX_FSUB(dist2, VOX_FMUL(vmin[a], vmin[a]));
+        else if (0.f > vmax[a])
+            dist2 = VOX_FSUB(dist2, VOX_FMUL(vmax[a], vmax[a]));
+    }
+    return dist2 > 0.f;
+}
+
+/* gaussian_frag_color.slang:184-217: alpha after the opacity transform and
+ * the cull, plus the packed RGBA8 */
+static uint32_t frag_rgba(const prim_t* P, float vs, float cull_scale, const float* vmin, const float* vmax,
+                          float* alpha_out)
+{
+    float a = 0.f;
+    const float third = VOX_FDIV(1.f, 3.f);
+    for (int s = 0; s < 64; s++)
+    {
+        float w[3] = { VOX_FMUL(third, (float)((s >> 4) & 3)), VOX_FMUL(third, (float)((s >> 2) & 3)),
+                       VOX_FMUL(third, (float)(s & 3)) };
+        float lp[3];
+        for (int c = 0; c < 3; c++)
+            lp[c] = VOX_FADD(VOX_FMUL(w[c], vmax[c]), VOX_FMUL(VOX_FSUB(1.f, w[c]), vmin[c]));
+        float d = dot3(lp, lp);
+        float v = VOX_FMUL(P->op, vox_expf_cr(-VOX_FMUL(P->ls, d)));
+        a = v > a ? v : a;
+    }
+    float scale1d = VOX_FSQRT(dot3(P->s, P->s));
+    float vrs = VOX_FDIV(VOX_FMUL(0.1f, scale1d), vs);
+    a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), VOX_FDIV(1.f, vrs)));
+    float cull = cull_scale > 0.f ? cull_scale : 0.05f;
+    if (scale1d > cull)
+        a = 0.f;
+    *alpha_out = a;
+    float ch[4] = { P->rgb[0], P->rgb[1], P->rgb[2], a };
+    uint32_t out = 0;
+    for (int c = 0; c < 4; c++)
+    {
+        float v = ch[c] < 1.f ? ch[c] : 1.f;
+        v = 0.f > v ? 0.f : v;
+        out |= ((uint32_t)VOX_FMUL(255.f, v)) << (8 * c);
+    }
+    return out;
+}
+
+/* FP64 restatement of the same alpha (lattice of 64 samples, cull), computed
+ * from the float inputs in double with the C library's exp/log/pow. */
+static double frag_alpha64(const prim_t* P, double vs, double cull_scale, const int32_t* ijk)
+{
+    double q[4] = { P->q[0], P->q[1], P->q[2], P->q[3] };
+    double x = q[0], y = q[1], z = q[2], w = q[3];
+    double r[3][3] = { { 1 - 2 * (y * y + z * z), 2 * (x * y + z * w), 2 * (x * z - y * w) },
+                       { 2 * (x * y - z * w), 1 - 2 * (x * x + z * z), 2 * (y * z + x * w) },
+                       { 2 * (x * z + y * w), 2 * (y * z - x * w), 1 - 2 * (x * x + y * y) } };
+    double ls = sqrt(2.0 * log((double)P->op / 0.01));
+    double s[3] = { P->s[0], P->s[1], P->s[2] };
+    double vmin[3], vmax[3];
+    for (int v = 0; v < 8; v++)
+    {
+        double lp[3] = { (ijk[0] + ((v & 1) ? 1 : 0)) * vs - P->pos[0], (ijk[1] + ((v & 2) ? 1 : 0)) * vs - P->pos[1],
+                         (ijk[2] + ((v & 4) ? 1 : 0)) * vs - P->pos[2] };
+        for (int a = 0; a < 3; a++)
+        {
+            double l = (lp[0] * r[a][0] + lp[1] * r[a][1] + lp[2] * r[a][2]) / ls / s[a];
+            if (v == 0 || l < vmin[a])
+                vmin[a] = l;
+            if (v == 0 || l > vmax[a])
+                vmax[a] = l;
+        }
+    }
+    double al = 0.0;
+    for (int sidx = 0; sidx < 64; sidx++)
+    {
+        double wv[3] = { ((sidx >> 4) & 3) / 3.0, ((sidx >> 2) & 3) / 3.0, (sidx & 3) / 3.0 };
+        double d = 0.0;
+        for (int c = 0; c < 3; c++)
+        {
+            double t = wv[c] * vmax[c] + (1.0 - wv[c]) * vmin[c];
+            d += t * t;
+        }
+        double v = (double)P->op * exp(-ls * d);
+        al = v > al ? v : al;
+    }
+    double scale1d = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    double vrs = 0.1 * scale1d / vs;
+    al = 1.0 - pow(1.0 - al, 1.0 / vrs);
+    /* the cull decision follows the float pass so both see the same pair set */
+    float s1f = VOX_FSQRT(dot3(P->s, P->s));
+    float cullf = cull_scale > 0 ? (float)cull_scale : 0.05f;
+    if (s1f > cullf)
+        al = 0.0;
+    return al;
+}
+
+int ov_prim_bbox(const float* mean, const float* quat_wxyz, const float* scale, float opacity, float voxel_size,
+                 int32_t* bbox6, uint64_t* footprint)
+{
+    prim_t P;
+    prim_setup(&P, mean, quat_wxyz, scale, opacity, NULL, voxel_size);
+    for (int a = 0; a < 3; a++)
+    {
+        bbox6[a] = P.bmin[a];
+        bbox6[3 + a] = P.bmax[a];
+    }
+    *footprint = P.footprint;
+    return P.valid;
+}
+
+int ov_frag_test(const float* mean, const float* quat_wxyz, const float* scale, float opacity, float voxel_size,
+                 const int32_t* ijk, float* vmin3, float* vmax3)
+{
+    prim_t P;
+    prim_setup(&P, mean, quat_wxyz, scale, opacity, NULL, voxel_size);
+    if (!P.valid)
+        return 0;
+    float rinv[3][3];
+    rot_inv_rows(P.q, rinv);
+    return frag_test(&P, rinv, voxel_size, ijk, vmin3, vmax3);
+}
+
+uint32_t ov_frag_rgba(const float* mean, const float* quat_wxyz, const float* scale, float opacity,
+                      const float* color, float voxel_size, float cull_scale, const int32_t* ijk, float* alpha_out)
+{
+    prim_t P;
+    prim_setup(&P, mean, quat_wxyz, scale, opacity, color, voxel_size);
+    float rinv[3][3], vmin[3], vmax[3];
+    rot_inv_rows(P.q, rinv);
+    frag_test(&P, rinv, voxel_size, ijk, vmin, vmax);
+    return frag_rgba(&P, voxel_size, cull_scale, vmin, vmax, alpha_out);
+}
+
+/* ------------------------------------------------------------------------ */
+/* incremental node2 build (raster/GridBuild.cpp:361-506 +                   */
+/* grid_build_{set_masks,count_new,scatter_new,finalize}.slang)              */
+/* ------------------------------------------------------------------------ */
+typedef struct
+{
+    int type;
+    int32_t parent;
+    uint32_t n;
+    int32_t origin[3];
+    int32_t* child;     /* dense child node index per n (-1 none); non-leaf */
+    uint64_t* vmask;    /* leaf value mask (8 words) */
+} node_t;
+
+typedef struct
+{
+    /* inputs */
+    int64_t G;
+    float vs, cull;
+    prim_t* prims;
+    /* pairs in emission (Gaussian-major) order, later sorted */
+    uint64_t* keys;
+    uint32_t* ids;
+    int32_t* pijk; /* ijk per pair, emission order */
+    int64_t P, Pcap;
+    /* tree */
+    node_t* nodes;
+    int64_t nn, ncap;
+    /* results */
+    int64_t counts[OV_COUNT_N];
+    uint8_t* node2;
+    int64_t node2_bytes;
+    uint64_t* value_idx_node; /* per node */
+    int64_t V;
+    int32_t* vox_ijk;
+    uint64_t* vox_vidx;
+    uint32_t* rgba;
+    float* dens;
+    float* col;
+    double* dens64;
+    double* col64;
+    int32_t bbox[6];
+} ov_state_t;
+
+static int32_t new_node(ov_state_t* S, int type, int32_t parent, uint32_t n, const int32_t* origin)
+{
+    if (S->nn == S->ncap)
+    {
+        S->ncap = S->ncap ? 2 * S->ncap : 1024;
+        S->nodes = (node_t*)realloc(S->nodes, sizeof(node_t) * S->ncap);
+    }
+    node_t* N = &S->nodes[S->nn];
+    N->type = type;
+    N->parent = parent;
+    N->n = n;
+    N->origin[0] = origin[0];
+    N->origin[1] = origin[1];
+    N->origin[2] = origin[2];
+    N->child = NULL;
+    N->vmask = NULL;
+    if (type < 3)
+    {
+        N->child = (int32_t*)malloc(sizeof(int32_t) * N2_FANOUT[type]);
+        for (uint32_t i = 0; i < N2_FANOUT[type]; i++)
+            N->child[i] = -1;
+    }
+    else
+    {
+        N->vmask = (uint64_t*)calloc(8, sizeof(uint64_t));
+    }
+    return (int32_t)(S->nn++);
+}
+
+typedef struct
+{
+    int32_t node;
+    uint32_t n;
+    int32_t ijk[3];
+} mark_t;
+
+static int mark_cmp(const void* a, const void* b)
+{
+    const mark_t* x = (const mark_t*)a;
+    const mark_t* y = (const mark_t*)b;
+    if (x->node != y->node)
+        return x->node < y->node ? -1 : 1;
+    if (x->n != y->n)
+        return x->n < y->n ? -1 : 1;
+    return 0;
+}
+
+/* one fragment window: levels root -> upper -> lower -> leaf (GridBuild.cpp:412-505).
+ * New children are appended in (parent node_idx, n) order, which is the order
+ * grid_build_scatter_new.slang:107-170 allocates them in. */
+static void insert_window(ov_state_t* S, const int32_t* ijk, int64_t count)
+{
+    mark_t* marks = (mark_t*)malloc(sizeof(mark_t) * (count ? count : 1));
+    for (int level = 0; level < 3; level++)
+    {
+        int64_t m = 0;
+        for (int64_t f = 0; f < count; f++)
+        {
+            const int32_t* c = &ijk[3 * f];
+            int32_t node = 0;
+            for (int t = 0; t < level; t++)
+                node = S->nodes[node].child[n2_coord_to_n(t, c[0], c[1], c[2])];
+            uint32_t n = n2_coord_to_n(level, c[0], c[1], c[2]);
+            if (S->nodes[node].child[n] < 0)
+            {
+                marks[m].node = node;
+                marks[m].n = n;
+                marks[m].ijk[0] = c[0];
+                marks[m].ijk[1] = c[1];
+                marks[m].ijk[2] = c[2];
+                m++;
+            }
+        }
+        qsort(marks, (size_t)m, sizeof(mark_t), mark_cmp);
+        for (int64_t i = 0; i < m; i++)
+        {
+            if (i > 0 && marks[i].node == marks[i - 1].node && marks[i].n == marks[i - 1].n)
+                continue;
+            uint32_t tile = 1u << N2_TILEDIM_BITS[level]; /* child covers 2^tiledim voxels per axis */
+            int32_t origin[3];
+            for (int a = 0; a < 3; a++)
+                origin[a] = marks[i].ijk[a] & ~(int32_t)(tile - 1u);
+            int32_t child = new_node(S, level + 1, marks[i].node, marks[i].n, origin);
+            S->nodes[marks[i].node].child[marks[i].n] = child;
+        }
+    }
+    /* leaf value bits */
+    for (int64_t f = 0; f < count; f++)
+    {
+        const int32_t* c = &ijk[3 * f];
+        int32_t node = 0;
+        for (int t = 0; t < 3; t++)
+            node = S->nodes[node].child[n2_coord_to_n(t, c[0], c[1], c[2])];
+        uint32_t n = n2_coord_to_n(3, c[0], c[1], c[2]);
+        S->nodes[node].vmask[n >> 6] |= 1ull << (n & 63);
+    }
+    free(marks);
+}
+
+/* ------------------------------------------------------------------------ */
+/* threaded fragment test for one window                                     */
+/* ------------------------------------------------------------------------ */
+typedef struct
+{
+    ov_state_t* S;
+    const int64_t* pidx;      /* prim index per prim in batch */
+    const uint64_t* off;      /* exclusive fragment offset within batch */
+    int64_t nprim;
+    uint64_t f0, f1;          /* fragment range of this worker */
+    int32_t* out_ijk;
+    uint32_t* out_id;
+    int64_t out_n, out_cap;
+} wjob_t;
+
+static int64_t upper_bound_u64(const uint64_t* a, int64_t n, uint64_t v)
+{
+    int64_t lo = 0, hi = n;
+    while (lo < hi)
+    {
+        int64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+static void* window_worker(void* arg)
+{
+    wjob_t* J = (wjob_t*)arg;
+    ov_state_t* S = J->S;
+    if (J->f0 >= J->f1)
+        return NULL;
+    /* prim containing fragment f0: last prim with off <= f0 (zero-footprint prims are skipped) */
+    int64_t p = upper_bound_u64(J->off, J->nprim, J->f0) - 1;
+    uint64_t f = J->f0;
+    while (f < J->f1 && p < J->nprim)
+    {
+        const prim_t* P = &S->prims[J->pidx[p]];
+        uint64_t pend = J->off[p] + P->footprint;
+        if (P->footprint == 0 || f >= pend)
+        {
+            p++;
+            continue;
+        }
+        float rinv[3][3];
+        rot_inv_rows(P->q, rinv);
+        int32_t Ry = P->bmax[1] + 1 - P->bmin[1], Rz = P->bmax[2] + 1 - P->bmin[2];
+        uint64_t stop = pend < J->f1 ? pend : J->f1;
+        for (; f < stop; f++)
+        {
+            int32_t r = (int32_t)(f - J->off[p]);
+            /* gaussian_frag_alloc.slang:55-58 */
+            int32_t ijk[3] = { r / (Rz * Ry) + P->bmin[0], (r / Rz) % Ry + P->bmin[1], r % Rz + P->bmin[2] };
+            float vmin[3], vmax[3];
+            if (frag_test(P, rinv, S->vs, ijk, vmin, vmax))
+            {
+                if (J->out_n == J->out_cap)
+                {
+                    J->out_cap = J->out_cap ? 2 * J->out_cap : 4096;
+                    J->out_ijk = (int32_t*)realloc(J->out_ijk, sizeof(int32_t) * 3 * J->out_cap);
+                    J->out_id = (uint32_t*)realloc(J->out_id, sizeof(uint32_t) * J->out_cap);
+                }
+                memcpy(&J->out_ijk[3 * J->out_n], ijk, 12);
+                J->out_id[J->out_n] = (uint32_t)J->pidx[p];
+                J->out_n++;
+            }
+        }
+        p++;
+    }
+    return NULL;
+}
+
+/* stable LSD radix sort of (key, id) by key, 11-bit digits */
+static void radix_sort_pairs(uint64_t* keys, uint32_t* ids, int64_t n, int key_bits)
+{
+    uint64_t* k2 = (uint64_t*)malloc(sizeof(uint64_t) * (n ? n : 1));
+    uint32_t* i2 = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    int64_t* hist = (int64_t*)malloc(sizeof(int64_t) * 2048);
+    for (int sh = 0; sh < key_bits; sh += 11)
+    {
+        memset(hist, 0, sizeof(int64_t) * 2048);
+        for (int64_t i = 0; i < n; i++)
+            hist[(keys[i] >> sh) & 2047]++;
+        int64_t s = 0;
+        for (int d = 0; d < 2048; d++)
+        {
+            int64_t c = hist[d];
+            hist[d] = s;
+            s += c;
+        }
+        for (int64_t i = 0; i < n; i++)
+        {
+            int64_t dst = hist[(keys[i] >> sh) & 2047]++;
+            k2[dst] = keys[i];
+            i2[dst] = ids[i];
+        }
+        memcpy(keys, k2, sizeof(uint64_t) * n);
+        memcpy(ids, i2, sizeof(uint32_t) * n);
+    }
+    free(k2);
+    free(i2);
+    free(hist);
+}
+
+/* ------------------------------------------------------------------------ */
+/* values: gaussian_frag_color.slang:182-246 (R mode, max of packed RGBA8)   */
+/* plus the float density / colour sums in (key, id) order                   */
+/* ------------------------------------------------------------------------ */
+typedef struct
+{
+    ov_state_t* S;
+    const int64_t* vstart; /* pair start per voxel (V + 1 entries) */
+    int64_t v0, v1;
+} vjob_t;
+
+static void* values_worker(void* arg)
+{
+    vjob_t* J = (vjob_t*)arg;
+    ov_state_t* S = J->S;
+    for (int64_t v = J->v0; v < J->v1; v++)
+    {
+        uint64_t vi = S->vox_vidx[v];
+        const int32_t* ijk = &S->vox_ijk[3 * v];
+        uint32_t rgba = 0;
+        float dsum = 0.f, csum[3] = { 0.f, 0.f, 0.f };
+        double dsum64 = 0.0, csum64[3] = { 0.0, 0.0, 0.0 };
+        for (int64_t p = J->vstart[v]; p < J->vstart[v + 1]; p++)
+        {
+            const prim_t* P = &S->prims[S->ids[p]];
+            float rinv[3][3], vmin[3], vmax[3], a;
+            rot_inv_rows(P->q, rinv);
+            frag_test(P, rinv, S->vs, ijk, vmin, vmax);
+            uint32_t c = frag_rgba(P, S->vs, S->cull, vmin, vmax, &a);
+            rgba = c > rgba ? c : rgba; /* InterlockedMax, :239-246 */
+            dsum = VOX_FADD(dsum, a);
+            for (int ch = 0; ch < 3; ch++)
+                csum[ch] = VOX_FADD(csum[ch], VOX_FMUL(a, P->rgb[ch]));
+            double a64 = frag_alpha64(P, (double)S->vs, (double)S->cull, ijk);
+            dsum64 += a64;
+            for (int ch = 0; ch < 3; ch++)
+                csum64[ch] += a64 * (double)P->rgb[ch];
+        }
+        S->rgba[vi] = rgba;
+        S->dens[vi] = dsum;
+        S->dens64[vi] = dsum64;
+        for (int ch = 0; ch < 3; ch++)
+        {
+            S->col[3 * vi + ch] = dsum > 0.f ? VOX_FDIV(csum[ch], dsum) : 0.f;
+            S->col64[3 * vi + ch] = dsum64 > 0.0 ? csum64[ch] / dsum64 : 0.0;
+        }
+    }
+    return NULL;
+}
+
+static int popc64(uint64_t x)
+{
+    return __builtin_popcountll(x);
+}
+
+/* mask prefix sums, grid_build_count_new.slang:49-88: field (w & 3) of word
+ * (w >> 2) holds popcount(mask[0 .. w-1]); field 0 of word 0 holds the total. */
+static void write_prefix(uint64_t* words, const uint64_t* mask, uint32_t nwords)
+{
+    uint64_t sum = 0;
+    for (uint32_t w = 0; w < nwords; w++)
+    {
+        sum += (uint64_t)popc64(mask[w]);
+        uint32_t wi = (w + 1) & (nwords - 1);
+        uint64_t* dst = &words[wi >> 2];
+        *dst &= ~(0xFFFFull << ((wi & 3) * 16));
+        *dst |= (sum & 0xFFFF) << ((wi & 3) * 16);
+    }
+}
+
+static void serialize(ov_state_t* S)
+{
+    int64_t nn = S->nn;
+    uint64_t* addr = (uint64_t*)malloc(sizeof(uint64_t) * nn);
+    uint64_t total = 0;
+    for (int64_t i = 0; i < nn; i++)
+    {
+        addr[i] = total;
+        total += N2_MAX_SIZE[S->nodes[i].type];
+    }
+    S->node2_bytes = (int64_t)total;
+    S->node2 = (uint8_t*)calloc(total, 1);
+    S->value_idx_node = (uint64_t*)malloc(sizeof(uint64_t) * nn);
+    uint64_t vsum = 2; /* two background values, grid_build_count_new.slang:103-106 */
+    for (int64_t i = 0; i < nn; i++)
+    {
+        S->value_idx_node[i] = vsum;
+        if (S->nodes[i].type == 3)
+            for (int w = 0; w < 8; w++)
+                vsum += (uint64_t)popc64(S->nodes[i].vmask[w]);
+    }
+    for (int64_t i = 0; i < nn; i++)
+    {
+        node_t* N = &S->nodes[i];
+        uint64_t* W = (uint64_t*)(S->node2 + addr[i]);
+        int t = N->type;
+        W[0] = (uint64_t)i;
+        W[1] = S->value_idx_node[i];
+        if (t == 3)
+        {
+            memcpy(&W[N2_OFF_VALUE_MASK[3]], N->vmask, 64);
+            write_prefix(&W[N2_OFF_VALUE_PREFIX[3]], N->vmask, 8);
+            continue;
+        }
+        uint32_t fan = N2_FANOUT[t], nw = fan >> 6;
+        uint64_t* cm = &W[N2_OFF_CHILD_MASK[t]];
+        for (uint32_t n = 0; n < fan; n++)
+            if (N->child[n] >= 0)
+                cm[n >> 6] |= 1ull << (n & 63);
+        write_prefix(&W[N2_OFF_CHILD_PREFIX[t]], cm, nw);
+        uint64_t* ch = &W[N2_OFF_CHILDREN[t]];
+        if (t == 0)
+        {
+            for (uint32_t e = 0; e < 2u * fan; e++)
+                ch[e] = N2_END_KEY; /* GridBuild.cpp:178-183 */
+        }
+        uint32_t rank = 0;
+        for (uint32_t n = 0; n < fan; n++)
+            if (N->child[n] >= 0)
+                ch[rank++] = addr[N->child[n]] - addr[i];
+        if (t == 0)
+        {
+            /* keys, grid_build_blindmetadata.slang:104-201 */
+            uint64_t* km = &W[N2_OFF_KEY_MASK_ROOT];
+            memcpy(km, cm, 8 * nw);
+            write_prefix(&W[N2_OFF_KEY_PREFIX_ROOT], km, nw);
+            uint32_t child_count = rank, kidx = 0;
+            for (uint32_t n = 0; n < fan; n++)
+            {
+                if (N->child[n] < 0)
+                    continue;
+                int32_t x = (int32_t)(((n >> 10) & 0x1F) << 12), y = (int32_t)(((n >> 5) & 0x1F) << 12),
+                        z = (int32_t)((n & 0x1F) << 12);
+                const int32_t half = 65536;
+                x = x >= half ? x - 2 * half : x;
+                y = y >= half ? y - 2 * half : y;
+                z = z >= half ? z - 2 * half : z;
+                uint64_t key = (uint64_t)((uint32_t)z >> 12) | ((uint64_t)((uint32_t)y >> 12) << 21) |
+                               ((uint64_t)((uint32_t)x >> 12) << 42);
+                ch[child_count + kidx++] = key;
+            }
+        }
+    }
+    free(addr);
+}
+
+void* ov_run(int64_t n, const float* means, const float* quats_wxyz, const float* scales, const float* colors,
+             const float* opacities, float voxel_size, float cull_scale, int window_mode, int nthreads)
+{
+    if (nthreads < 1)
+        nthreads = 1;
+    ov_state_t* S = (ov_state_t*)calloc(1, sizeof(ov_state_t));
+    S->G = n;
+    S->vs = voxel_size;
+    S->cull = cull_scale;
+    S->prims = (prim_t*)malloc(sizeof(prim_t) * (n ? n : 1));
+    int64_t valid = 0;
+    uint64_t F = 0;
+    for (int64_t g = 0; g < n; g++)
+    {
+        prim_setup(&S->prims[g], &means[3 * g], &quats_wxyz[4 * g], &scales[3 * g], opacities[g],
+                   colors ? &colors[3 * g] : NULL, voxel_size);
+        valid += S->prims[g].valid;
+        F += S->prims[g].footprint;
+        if (S->prims[g].valid)
+        {
+            for (int a = 0; a < 3; a++)
+                if (S->prims[g].bmin[a] < -65536 || S->prims[g].bmax[a] > 65535)
+                    S->counts[OV_ERROR] = 1; /* root key range, grid_build_blindmetadata.slang:182-192 */
+            if (S->prims[g].footprint >= (1ull << 31))
+                S->counts[OV_ERROR] = 2;
+        }
+    }
+    S->counts[OV_G] = n;
+    S->counts[OV_G_VALID] = valid;
+    S->counts[OV_F] = (int64_t)F;
+    if (S->counts[OV_ERROR])
+        return S;
+
+    int32_t origin0[3] = { 0, 0, 0 };
+    new_node(S, 0, -1, 0, origin0);
+
+    int64_t batch = window_mode ? OV_PRIM_BATCH : (n ? n : 1);
+    uint64_t wsize = window_mode ? OV_WINDOW : ~0ull;
+    int64_t windows = 0;
+    int64_t* pidx = (int64_t*)malloc(sizeof(int64_t) * (batch ? batch : 1));
+    uint64_t* off = (uint64_t*)malloc(sizeof(uint64_t) * (batch ? batch : 1));
+    wjob_t* jobs = (wjob_t*)calloc((size_t)nthreads, sizeof(wjob_t));
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+    for (int64_t b0 = 0; b0 < n; b0 += batch)
+    {
+        int64_t nb = (n - b0) < batch ? (n - b0) : batch;
+        uint64_t fsum = 0;
+        for (int64_t p = 0; p < nb; p++)
+        {
+            pidx[p] = b0 + p;
+            off[p] = fsum;
+            fsum += S->prims[b0 + p].footprint;
+        }
+        for (uint64_t w0 = 0, w1 = 0; w0 < fsum; w0 = w1)
+        {
+            w1 = (fsum - w0) < wsize ? fsum : w0 + wsize;
+            uint64_t span = w1 - w0;
+            for (int t = 0; t < nthreads; t++)
+            {
+                jobs[t].S = S;
+                jobs[t].pidx = pidx;
+                jobs[t].off = off;
+                jobs[t].nprim = nb;
+                jobs[t].f0 = w0 + span * (uint64_t)t / (uint64_t)nthreads;
+                jobs[t].f1 = w0 + span * (uint64_t)(t + 1) / (uint64_t)nthreads;
+                jobs[t].out_n = 0;
+                pthread_create(&th[t], NULL, window_worker, &jobs[t]);
+            }
+            int64_t wcount = 0;
+            for (int t = 0; t < nthreads; t++)
+            {
+                pthread_join(th[t], NULL);
+                wcount += jobs[t].out_n;
+            }
+            int32_t* wijk = (int32_t*)malloc(sizeof(int32_t) * 3 * (wcount ? wcount : 1));
+            int64_t pos = 0;
+            if (S->P + wcount > S->Pcap)
+            {
+                S->Pcap = (S->P + wcount) * 2;
+                S->keys = (uint64_t*)realloc(S->keys, sizeof(uint64_t) * S->Pcap);
+                S->ids = (uint32_t*)realloc(S->ids, sizeof(uint32_t) * S->Pcap);
+            }
+            for (int t = 0; t < nthreads; t++)
+            {
+                for (int64_t i = 0; i < jobs[t].out_n; i++)
+                {
+                    const int32_t* c = &jobs[t].out_ijk[3 * i];
+                    memcpy(&wijk[3 * pos], c, 12);
+                    S->keys[S->P + pos] = ov_hier_key(c[0], c[1], c[2]);
+                    S->ids[S->P + pos] = jobs[t].out_id[i];
+                    pos++;
+                }
+            }
+            S->P += wcount;
+            insert_window(S, wijk, wcount);
+            free(wijk);
+            windows++;
+        }
+    }
+    for (int t = 0; t < nthreads; t++)
+    {
+        free(jobs[t].out_ijk);
+        free(jobs[t].out_id);
+    }
+    free(jobs);
+    free(pidx);
+    free(off);
+
+    radix_sort_pairs(S->keys, S->ids, S->P, 51);
+
+    /* voxel runs in key order */
+    int64_t V = 0;
+    for (int64_t p = 0; p < S->P; p++)
+        if (p == 0 || S->keys[p] != S->keys[p - 1])
+            V++;
+    S->V = V;
+    int64_t* vstart = (int64_t*)malloc(sizeof(int64_t) * (V + 1));
+    S->vox_ijk = (int32_t*)malloc(sizeof(int32_t) * 3 * (V ? V : 1));
+    S->vox_vidx = (uint64_t*)malloc(sizeof(uint64_t) * (V ? V : 1));
+
+    serialize(S);
+
+    int64_t vi = 0;
+    for (int64_t p = 0; p < S->P; p++)
+    {
+        if (p == 0 || S->keys[p] != S->keys[p - 1])
+            vstart[vi++] = p;
+    }
+    vstart[V] = S->P;
+    /* ijk back from a pair: recompute from the Gaussian's emission is not
+     * needed; decode the hierarchical key through the tree instead */
+    for (int64_t v = 0; v < V; v++)
+    {
+        uint64_t key = S->keys[vstart[v]];
+        uint32_t rn = (uint32_t)(key >> 36) & 0x7FFF, un = (uint32_t)(key >> 21) & 0x7FFF,
+                 ln = (uint32_t)(key >> 9) & 0xFFF, vn = (uint32_t)key & 0x1FF;
+        int32_t up = S->nodes[0].child[rn];
+        int32_t lo = S->nodes[up].child[un];
+        int32_t lf = S->nodes[lo].child[ln];
+        node_t* L = &S->nodes[lf];
+        int32_t* c = &S->vox_ijk[3 * v];
+        c[0] = L->origin[0] + (int32_t)((vn >> 6) & 7);
+        c[1] = L->origin[1] + (int32_t)((vn >> 3) & 7);
+        c[2] = L->origin[2] + (int32_t)(vn & 7);
+        uint64_t below = 0;
+        for (uint32_t w = 0; w < (vn >> 6); w++)
+            below += (uint64_t)popc64(L->vmask[w]);
+        below += (uint64_t)popc64(L->vmask[vn >> 6] & ((1ull << (vn & 63)) - 1ull));
+        S->vox_vidx[v] = S->value_idx_node[lf] + below;
+    }
+
+    int64_t value_count = 2 + V;
+    S->rgba = (uint32_t*)calloc((size_t)value_count, sizeof(uint32_t));
+    S->dens = (float*)calloc((size_t)value_count, sizeof(float));
+    S->col = (float*)calloc((size_t)value_count * 3, sizeof(float));
+    S->dens64 = (double*)calloc((size_t)value_count, sizeof(double));
+    S->col64 = (double*)calloc((size_t)value_count * 3, sizeof(double));
+    vjob_t* vj = (vjob_t*)malloc(sizeof(vjob_t) * nthreads);
+    for (int t = 0; t < nthreads; t++)
+    {
+        vj[t].S = S;
+        vj[t].vstart = vstart;
+        vj[t].v0 = V * t / nthreads;
+        vj[t].v1 = V * (t + 1) / nthreads;
+        pthread_create(&th[t], NULL, values_worker, &vj[t]);
+    }
+    for (int t = 0; t < nthreads; t++)
+        pthread_join(th[t], NULL);
+    free(vj);
+    free(th);
+    free(vstart);
+
+    /* bbox of active voxels (grid_build_compute_bbox.slang) */
+    for (int a = 0; a < 3; a++)
+    {
+        S->bbox[a] = 0x7FFFFFFF;
+        S->bbox[3 + a] = (int32_t)0x80000000;
+    }
+    for (int64_t v = 0; v < V; v++)
+        for (int a = 0; a < 3; a++)
+        {
+            int32_t c = S->vox_ijk[3 * v + a];
+            S->bbox[a] = c < S->bbox[a] ? c : S->bbox[a];
+            S->bbox[3 + a] = c > S->bbox[3 + a] ? c : S->bbox[3 + a];
+        }
+
+    int64_t cnt[4] = { 0, 0, 0, 0 };
+    for (int64_t i = 0; i < S->nn; i++)
+        cnt[S->nodes[i].type]++;
+    S->counts[OV_P] = S->P;
+    S->counts[OV_V] = V;
+    S->counts[OV_UPPER] = cnt[1];
+    S->counts[OV_LOWER] = cnt[2];
+    S->counts[OV_LEAF] = cnt[3];
+    S->counts[OV_VALUE_COUNT] = value_count;
+    S->counts[OV_NODE2_BYTES] = S->node2_bytes;
+    S->counts[OV_WINDOWS] = windows;
+    return S;
+}
+
+void ov_destroy(void* h)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    if (!S)
+        return;
+    for (int64_t i = 0; i < S->nn; i++)
+    {
+        free(S->nodes[i].child);
+        free(S->nodes[i].vmask);
+    }
+    free(S->nodes);
+    free(S->prims);
+    free(S->keys);
+    free(S->ids);
+    free(S->pijk);
+    free(S->node2);
+    free(S->value_idx_node);
+    free(S->vox_ijk);
+    free(S->vox_vidx);
+    free(S->rgba);
+    free(S->dens);
+    free(S->col);
+    free(S->dens64);
+    free(S->col64);
+    free(S);
+}
+
+void ov_counts(void* h, int64_t* out)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    memcpy(out, S->counts, sizeof(S->counts));
+}
+
+int64_t ov_node2_bytes(void* h, uint8_t* dst)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    if (dst && S->node2)
+        memcpy(dst, S->node2, (size_t)S->node2_bytes);
+    return S->node2_bytes;
+}
+
+void ov_pairs(void* h, uint64_t* keys, uint32_t* ids)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    memcpy(keys, S->keys, sizeof(uint64_t) * S->P);
+    memcpy(ids, S->ids, sizeof(uint32_t) * S->P);
+}
+
+void ov_values(void* h, uint32_t* rgba8, float* density, float* color, double* density64, double* color64)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    int64_t vc = 2 + S->V;
+    if (rgba8)
+        memcpy(rgba8, S->rgba, sizeof(uint32_t) * vc);
+    if (density)
+        memcpy(density, S->dens, sizeof(float) * vc);
+    if (color)
+        memcpy(color, S->col, sizeof(float) * 3 * vc);
+    if (density64)
+        memcpy(density64, S->dens64, sizeof(double) * vc);
+    if (color64)
+        memcpy(color64, S->col64, sizeof(double) * 3 * vc);
+}
+
+void ov_voxels(void* h, int32_t* ijk, uint64_t* value_idx)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    memcpy(ijk, S->vox_ijk, sizeof(int32_t) * 3 * S->V);
+    memcpy(value_idx, S->vox_vidx, sizeof(uint64_t) * S->V);
+}
+
+void ov_bbox(void* h, int32_t* out6)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    memcpy(out6, S->bbox, sizeof(S->bbox));
+}
+
+void ov_node_table(void* h, int32_t* type, int32_t* parent, int32_t* n_in_parent, int32_t* origin3)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    for (int64_t i = 0; i < S->nn; i++)
+    {
+        type[i] = S->nodes[i].type;
+        parent[i] = S->nodes[i].parent;
+        n_in_parent[i] = (int32_t)S->nodes[i].n;
+        memcpy(&origin3[3 * i], S->nodes[i].origin, 12);
+    }
+}

@@ -1,0 +1,106 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Bit-exact: sorted (voxel key, Gaussian id) pairs, the node2 region (masks,
+prefix sums, child offsets, node counts, value indices, root keys), the
+active-voxel bbox, RGBA8 values and the float32 density / colour sums (same
+per-pair arithmetic, same sequential order).  Against the FP64 oracle the
+float density and colour agree to 1e-5 of the grid's maximum density.
+"""
+
+import numpy as np
+import pytest
+
+from nanovdb_editor import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL_REL_MAX = 1e-5  # |f32 - f64| <= 1e-5 * max |density f64|
+
+
+def _check(vox_ctx, oracle_mod, cloud, vs, cull=0.05):
+    g = vox_ctx.voxelize_host(cloud["means"], cloud["quats"], cloud["scales"], cloud["opacities"], cloud["colors"], vs, cull)
+    ref = oracle_mod.OracleResult(cloud, vs, cull, window_mode=0)
+    c = ref.counts
+    assert c["error"] == 0
+    got = g.counts
+    assert got["pairs"] == c["P"]
+    assert got["candidates"] == c["F"]
+    assert got["voxels"] == c["V"]
+    assert (got["upper"], got["lower"], got["leaf"]) == (c["upper"], c["lower"], c["leaf"])
+    k_ref, i_ref = ref.pairs()
+    k_got, i_got = vox_ctx.pairs()
+    np.testing.assert_array_equal(k_got, k_ref)
+    np.testing.assert_array_equal(i_got, i_ref)
+    n2 = ref.node2()
+    assert g.node2.shape == n2.shape
+    if not np.array_equal(g.node2, n2):
+        bad = np.nonzero(g.node2.view(np.uint64) != n2.view(np.uint64))[0]
+        pytest.fail(f"node2 differs in {bad.size} words, first word index {bad[:8]}")
+    if c["V"]:
+        np.testing.assert_array_equal(g.bbox, ref.bbox())
+    v = ref.values()
+    np.testing.assert_array_equal(g.rgba8, v["rgba8"])
+    np.testing.assert_array_equal(g.density, v["density"])
+    np.testing.assert_array_equal(g.color, v["color"])
+    dmax = float(np.abs(v["density64"]).max()) if c["V"] else 1.0
+    err_d = float(np.abs(g.density.astype(np.float64) - v["density64"]).max()) if c["V"] else 0.0
+    assert err_d <= TOL_REL_MAX * max(dmax, 1e-30), (err_d, dmax)
+    w = v["density64"] > 1e-3 * dmax
+    if w.any():
+        err_c = float(np.abs(g.color.astype(np.float64)[w] - v["color64"][w]).max())
+        assert err_c <= 1e-4, err_c
+    ref.close()
+    return g, c
+
+
+def test_pytest_cloud(vox_ctx, oracle_mod):
+    # pytests/test_pipelines.py:313-336 / :497-506: element_count > 0 at voxel 1/8
+    cloud = W.pytest_cloud()
+    g, c = _check(vox_ctx, oracle_mod, cloud, 1.0 / 8.0)
+    assert c["V"] > 0 and g.header["grid_bytes"] > 0
+
+
+@pytest.mark.parametrize("n,seed", [(1, 0), (7, 1), (200, 2), (5000, 3)])
+def test_plain_small(vox_ctx, oracle_mod, n, seed):
+    _check(vox_ctx, oracle_mod, W.plain_cloud(n, seed), 0.01)
+
+
+def test_cluster_small(vox_ctx, oracle_mod):
+    _check(vox_ctx, oracle_mod, W.cluster_cloud(20_000, 4, clusters=8), 0.002)
+
+
+def test_plain_100k(vox_ctx, oracle_mod):
+    # the 100k-Gaussian workload at voxel 0.01, in full
+    _check(vox_ctx, oracle_mod, W.plain_cloud(100_000, 0), 0.01)
+
+
+def test_empty_cloud(vox_ctx):
+    z = np.zeros((0, 3), np.float32)
+    g = vox_ctx.voxelize_host(z, np.zeros((0, 4), np.float32), z, np.zeros(0, np.float32), z, 0.01)
+    assert g.counts["voxels"] == 0 and g.counts["pairs"] == 0
+    assert g.value_count == 2
+
+
+def test_transparent_gaussians_emit_nothing(vox_ctx, oracle_mod):
+    cloud = W.plain_cloud(64, 5)
+    cloud["opacities"][:] = 0.009  # below the 0.01 cutoff of gaussian_prim.slang:65
+    g = vox_ctx.voxelize_host(cloud["means"], cloud["quats"], cloud["scales"], cloud["opacities"], cloud["colors"], 0.01)
+    assert g.counts["pairs"] == 0
+
+
+def test_out_of_range_rejected(vox_ctx):
+    from nanovdb_editor.exceptions import PipelineError
+
+    cloud = W.plain_cloud(16, 6)
+    cloud["means"][0] = [700.0, 0.0, 0.0]  # 70000 voxels at 0.01 > 65535
+    with pytest.raises(PipelineError):
+        vox_ctx.voxelize_host(cloud["means"], cloud["quats"], cloud["scales"], cloud["opacities"], cloud["colors"], 0.01)
+    # the context stays usable
+    ok = W.plain_cloud(16, 7)
+    g = vox_ctx.voxelize_host(ok["means"], ok["quats"], ok["scales"], ok["opacities"], ok["colors"], 0.01)
+    assert g.counts["voxels"] > 0
+
+
+def test_cull_scale_parameter(vox_ctx, oracle_mod):
+    cloud = W.plain_cloud(2000, 8)
+    _check(vox_ctx, oracle_mod, cloud, 0.01, cull=0.02)
