@@ -1,0 +1,341 @@
+"""Benchmark: Gaussian -> NanoVDB (node2) voxelization on B200.
+
+Workload (one step = one full voxelization of one cloud): 2M Gaussians drawn
+from 64 surface-like clusters (cluster_cloud), voxel size 0.002, float32
+attributes in the raw on-disk convention (log scales, logit opacities, SH0).
+Data: seeded synthetic (the reference publishes no dataset for this path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value   Gaussians/s with inputs resident in HBM (vox_voxelize on device
+        pointers), per-step CUDA events on the library's stream, L2 flushed
+        between steps; whole job over N ranks (weak scaling: each rank
+        voxelizes its own cloud).
+e2e     same metric through the reference-facing C ABI with host buffers
+        (pnanovdb_raster_t.raster_to_nanovdb_from_arrays: pinned host inputs
+        in, host grid out, copies inside the timed call).
+roofline  achieved HBM GB/s of the dominant kernel stage from its algorithmic
+        bytes and its CUDA-event duration, against MEASURED_PEAKS.json.
+cpu_baseline  the CPU oracle (C restatement of the reference path; the
+        reference's Vulkan path is unavailable on this box) on a bounded
+        sample of the same workload on all host cores.
+--impl reference  times that CPU implementation alone (rank 0).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "nanovdb-editor_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Gaussians/s voxelized: plain vs batched vs fwd+bwd at 1e-5 rel; % of HBM peak"
+UNIT = "Gaussians/s"
+WORKLOAD = {"workload": "plain_forward_2M_clusters64_vs0.002", "gaussians": 2_000_000, "clusters": 64, "voxel_size": 0.002}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device_index=0):
+        self.proc = None
+        self.out = []
+        self.device_index = device_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(steps=1, target_s=15.0):
+    """Oracle (float outputs only) on a bounded sample of the workload, all host cores."""
+    import oracle as oracle_py
+    from nanovdb_editor import workloads as W
+
+    oracle_py.build()
+    cores = os.cpu_count() or 1
+    vs = WORKLOAD["voxel_size"]
+    n = 20_000
+    rate = None
+    sample = None
+    for _ in range(4):
+        cloud = W.cluster_cloud(n, 1, clusters=max(1, int(64 * n / 2_000_000)) or 1)
+        t0 = time.perf_counter()
+        r = oracle_py.OracleResult(cloud, vs, 0.05, window_mode=1 | 2, nthreads=cores)
+        dt = time.perf_counter() - t0
+        ok = r.counts["error"] == 0
+        r.close()
+        rate = n / dt if ok else None
+        sample = f"{n} Gaussians of the 2M-cluster distribution (density-preserving subset: {max(1, int(64 * n / 2_000_000))} clusters), voxel 0.002, {dt:.1f}s"
+        if dt > target_s / 4 or n >= 400_000:
+            break
+        n = int(min(400_000, n * max(2.0, target_s / max(dt, 1e-3) / 2)))
+    return {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    res = []
+    for _ in range(max(1, args.steps)):
+        res.append(cpu_baseline())
+    vals = [r["value"] for r in res if r["value"]]
+    v = statistics.median(vals) if vals else None
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": dict(WORKLOAD, note="CPU restatement of the reference path (the reference's Vulkan path cannot run here)"),
+        "cpu_baseline": {"kind": "port", "cores": res[-1]["cores"], "sample": res[-1]["sample"], "value": v, "unit": UNIT},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--gaussians", type=int, default=WORKLOAD["gaussians"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    from ctypes import POINTER, byref, c_float, c_uint32, pointer
+
+    from nanovdb_editor import workloads as W
+    from nanovdb_editor.compute import Compute, pnanovdb_ComputeArray
+    from nanovdb_editor.raster import Raster
+    from nanovdb_editor.vox import FLAG_RAW_INPUTS, VoxContext
+
+    G = args.gaussians
+    vs = WORKLOAD["voxel_size"]
+    cloud = W.cluster_cloud(G, 1 + rank, clusters=64)
+    raw = cloud.raw_arrays()  # [means, logit, quats, log_s, sh0, sh_n]
+    dev = [torch.from_numpy(a).cuda() for a in raw[:5]]
+    ctx = VoxContext(local)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    ext_stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step():
+        # inputs resident in HBM: means, quats, log scales, logits, SH0
+        ctx.voxelize(dev[0], dev[2], dev[3], dev[1], dev[4], vs, 0.05, FLAG_RAW_INPUTS)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    times, stats = [], []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            start.record(ext_stream)
+            step()
+            end.record(ext_stream)
+            end.synchronize()
+            times.append(start.elapsed_time(end))
+            stats.append(ctx.stats())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = sum(times) / len(times)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * G / (ms * 1e-3)
+
+    # ---- e2e through the reference-facing C ABI with host buffers
+    comp = Compute(device_index=local)
+    raster = Raster(comp)
+    pinned = [torch.from_numpy(a).pin_memory() for a in raw]
+    arrays = []
+    for t in pinned:
+        arr = pnanovdb_ComputeArray()
+        arr.data = t.data_ptr()
+        arr.element_size = 4
+        arr.element_count = t.numel()
+        arrays.append(arr)
+    h2d = sum(int(t.numel()) * 4 for t in pinned[:5])
+    out = raster.raster_to_nanovdb_from_arrays(vs, arrays)  # warm
+    comp.destroy_array(out)
+    e2e_times, d2h = [], 0
+    if dist:
+        dist.barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = raster.raster_to_nanovdb_from_arrays(vs, arrays)
+        e2e_times.append(time.perf_counter() - t0)
+        d2h = int(out.element_size * out.element_count)
+        comp.destroy_array(out)
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * G / e2e_s
+
+    # ---- roofline of the dominant stage
+    st = stats[-1]
+    P = st["pairs"]
+    passes = st["sort_passes"]
+    kb = 8 if st["key_bits"] > 32 else 4
+    A = 56
+    # algorithmic bytes per stage (definitions in DESIGN.md)
+    stage_bytes = {
+        "emit": G * 128 + P * (kb + 4),  # read Gaussian records, write (key, id)
+        "sort": P * (kb + (kb + 4) * 2 * passes),  # histogram read + per pass read/write (key, id)
+        "accumulate": P * (kb + 4) + G * 128 + st["voxels"] * 20,
+        "prep": G * (A + 128 + 8),
+    }
+    stage_ms = {
+        "emit": float(np.mean([s["ms_emit"] for s in stats])),
+        "sort": float(np.mean([s["ms_sort"] for s in stats])),
+        "accumulate": float(np.mean([s["ms_accumulate"] for s in stats])),
+        "prep": float(np.mean([s["ms_prep"] for s in stats])),
+        "build": float(np.mean([s["ms_build"] for s in stats])),
+    }
+    dom = max(("emit", "sort", "accumulate"), key=lambda k: stage_ms[k])
+    peak, peak_kind = load_peaks()
+    achieved = stage_bytes[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dom)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        clk = clocks.summary()
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, gaussians=G, parallelism=f"replicas{world}" if world > 1 else "single", l2="256 MB flush between steps; pair working set >> L2", inputs="raw (log-scale, logit, SH0)"),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind},
+            "stages_ms": stage_ms,
+            "counts": {k: st[k] for k in ("candidates", "pairs", "voxels", "uppers", "lowers", "leaves", "key_bits", "sort_passes")},
+            "pairs_per_s": world * P / (ms * 1e-3),
+            "voxels_per_s": world * st["voxels"] / (ms * 1e-3),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -292,6 +292,7 @@ typedef struct vox_stats_t
     int32_t key_bits;
     int32_t sort_passes;
     float ms_prep, ms_emit, ms_sort, ms_build, ms_accumulate, ms_total;
+    int64_t kernel_launches; /* kernels this library launched in the call */
 } vox_stats_t;
 
 /* One context per caller thread; it owns a CUDA stream on `device` and a

@@ -205,6 +205,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     const int64_t G = gs->count;
     memset(&ctx->stats, 0, sizeof(ctx->stats));
     ctx->stats.gaussians = G;
+    const int64_t launches0 = launch_count();
     if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
@@ -521,6 +522,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     st.ms_build = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]);
     st.ms_accumulate = elapsed(ctx->timers.ev[4], ctx->timers.ev[5]);
     st.ms_total = elapsed(ctx->timers.ev[0], ctx->timers.ev[6]);
+    st.kernel_launches = launch_count() - launches0;
     return VOX_OK;
 }
 

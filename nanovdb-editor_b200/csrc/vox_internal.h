@@ -9,6 +9,10 @@
 namespace vox
 {
 
+// number of kernels this library has launched (all contexts, all threads)
+int64_t launch_count();
+void count_launch();
+
 // Bump allocator over one device arena; grows (re-allocates) between calls only.
 struct Arena
 {

@@ -715,7 +715,7 @@ void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint
 {
     if (P.count <= 0)
         return;
-    k_prep<<<(unsigned)((P.count + 255) / 256), 256, 0, s>>>(P, recs, footprints, (unsigned long long*)root_bits, err);
+    { k_prep<<<(unsigned)((P.count + 255) / 256), 256, 0, s>>>(P, recs, footprints, (unsigned long long*)root_bits, err); count_launch(); }
 }
 
 void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits, const uint64_t* root_prefix,
@@ -723,15 +723,15 @@ void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bit
 {
     if (G <= 0)
         return;
-    k_mark_lower<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(recs, G, root_bits, root_prefix,
-                                                           (unsigned long long*)lower_bits);
+    { k_mark_lower<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(recs, G, root_bits, root_prefix,
+                                                           (unsigned long long*)lower_bits); count_launch(); }
 }
 
 void launch_invert_bits(const uint64_t* bits, const uint64_t* prefix, int64_t words, uint32_t* out, cudaStream_t s)
 {
     if (words <= 0)
         return;
-    k_invert_bits<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(bits, prefix, words, out);
+    { k_invert_bits<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(bits, prefix, words, out); count_launch(); }
 }
 
 template <class K>
@@ -754,7 +754,7 @@ static void launch_emit_t(const EmitParams& E, const RankTables& T, K* out_k, ui
     if (grid > tiles)
         grid = tiles;
     cudaMemsetAsync(E.counter, 0, sizeof(uint32_t), s);
-    k_emit<K><<<(unsigned)grid, EMIT_BLOCK, smem, s>>>(E, T, out_k, out_i);
+    { k_emit<K><<<(unsigned)grid, EMIT_BLOCK, smem, s>>>(E, T, out_k, out_i); count_launch(); }
 }
 void launch_emit_u32(const EmitParams& E, const RankTables& T, uint32_t* out_k, uint32_t* out_i, int num_sms,
                      cudaStream_t s)
@@ -778,9 +778,9 @@ void launch_runs(const RunParams& Rp, const void* keys, int key64, cudaStream_t 
     cudaMemsetAsync(Rp.counter, 0, sizeof(uint32_t), s);
     int64_t tiles = (Rp.P + RUN_TILE - 1) / RUN_TILE;
     if (key64)
-        k_runs<uint64_t><<<(unsigned)tiles, RUN_BLOCK, 0, s>>>(Rp, (const uint64_t*)keys);
+        { k_runs<uint64_t><<<(unsigned)tiles, RUN_BLOCK, 0, s>>>(Rp, (const uint64_t*)keys); count_launch(); }
     else
-        k_runs<uint32_t><<<(unsigned)tiles, RUN_BLOCK, 0, s>>>(Rp, (const uint32_t*)keys);
+        { k_runs<uint32_t><<<(unsigned)tiles, RUN_BLOCK, 0, s>>>(Rp, (const uint32_t*)keys); count_launch(); }
 }
 int64_t runs_tile_count(int64_t P)
 {
@@ -791,25 +791,25 @@ void launch_lower_info(const NodeParams& N, cudaStream_t s)
 {
     if (N.Lo <= 0)
         return;
-    k_lower_info<<<(unsigned)((N.Lo + 255) / 256), 256, 0, s>>>(N);
+    { k_lower_info<<<(unsigned)((N.Lo + 255) / 256), 256, 0, s>>>(N); count_launch(); }
 }
 void launch_upper_info(const NodeParams& N, cudaStream_t s)
 {
     if (N.Lo <= 0)
         return;
-    k_upper_info<<<(unsigned)((N.Lo + 255) / 256), 256, 0, s>>>(N);
+    { k_upper_info<<<(unsigned)((N.Lo + 255) / 256), 256, 0, s>>>(N); count_launch(); }
 }
 void launch_leaf_tables(const NodeParams& N, const void* keys, int key64, cudaStream_t s)
 {
     if (N.L <= 0)
         return;
-    k_leaf_lower<<<(unsigned)((N.Lo + 255) / 256), 256, 0, s>>>(N);
-    k_leaf_lower_n<<<(unsigned)((N.L + 255) / 256), 256, 0, s>>>(N, keys, key64);
+    { k_leaf_lower<<<(unsigned)((N.Lo + 255) / 256), 256, 0, s>>>(N); count_launch(); }
+    { k_leaf_lower_n<<<(unsigned)((N.L + 255) / 256), 256, 0, s>>>(N, keys, key64); count_launch(); }
     unsigned blocks = (unsigned)((N.L * 32 + 255) / 256);
     if (key64)
-        k_leaf_masks<uint64_t><<<blocks, 256, 0, s>>>(N, (const uint64_t*)keys);
+        { k_leaf_masks<uint64_t><<<blocks, 256, 0, s>>>(N, (const uint64_t*)keys); count_launch(); }
     else
-        k_leaf_masks<uint32_t><<<blocks, 256, 0, s>>>(N, (const uint32_t*)keys);
+        { k_leaf_masks<uint32_t><<<blocks, 256, 0, s>>>(N, (const uint32_t*)keys); count_launch(); }
 }
 void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s)
 {
@@ -820,17 +820,17 @@ void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s)
         m = N.Lo;
     if (m <= 0)
         return;
-    k_canonical_order<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(N, U);
+    { k_canonical_order<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(N, U); count_launch(); }
 }
 void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* node2, cudaStream_t s)
 {
-    k_write_root<<<1, 1024, 0, s>>>(N, U, node2);
+    { k_write_root<<<1, 1024, 0, s>>>(N, U, node2); count_launch(); }
     if (U)
-        k_write_upper<<<(unsigned)U, 512, 0, s>>>(N, node2);
+        { k_write_upper<<<(unsigned)U, 512, 0, s>>>(N, node2); count_launch(); }
     if (N.Lo)
-        k_write_lower<<<(unsigned)N.Lo, 256, 0, s>>>(N, node2);
+        { k_write_lower<<<(unsigned)N.Lo, 256, 0, s>>>(N, node2); count_launch(); }
     if (N.L)
-        k_write_leaf<<<(unsigned)((N.L * 16 + 255) / 256), 256, 0, s>>>(N, node2);
+        { k_write_leaf<<<(unsigned)((N.L * 16 + 255) / 256), 256, 0, s>>>(N, node2); count_launch(); }
 }
 void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s)
 {
@@ -838,9 +838,9 @@ void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t
         return;
     unsigned blocks = (unsigned)((N.L * 32 + 255) / 256);
     if (key64)
-        k_accumulate<uint64_t><<<blocks, 256, 0, s>>>(A, N, ids);
+        { k_accumulate<uint64_t><<<blocks, 256, 0, s>>>(A, N, ids); count_launch(); }
     else
-        k_accumulate<uint32_t><<<blocks, 256, 0, s>>>(A, N, ids);
+        { k_accumulate<uint32_t><<<blocks, 256, 0, s>>>(A, N, ids); count_launch(); }
 }
 
 } // namespace vox

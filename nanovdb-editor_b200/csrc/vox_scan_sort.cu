@@ -6,6 +6,7 @@
 // counter, publish their tile aggregate, then walk back over predecessors'
 // published (aggregate | inclusive) words.  All waits are bounded
 // (LB_SPIN_LIMIT); a timeout sets the device error word and the call fails.
+#include <atomic>
 #include <cstdio>
 #include <cuda_runtime.h>
 
@@ -14,6 +15,16 @@
 
 namespace vox
 {
+
+static std::atomic<int64_t> g_launches{ 0 };
+int64_t launch_count()
+{
+    return g_launches.load(std::memory_order_relaxed);
+}
+void count_launch()
+{
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
 
 // ===================================================================== scan
 constexpr int SCAN_BLOCK = 256;
@@ -80,7 +91,7 @@ void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, 
     }
     cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-    k_scan_excl<<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(in, out, n, mode, total, status, epoch, counter, err);
+    { k_scan_excl<<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(in, out, n, mode, total, status, epoch, counter, err); count_launch(); }
 }
 
 // ===================================================================== sort
@@ -398,8 +409,8 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     int hist_grid = num_sms * 2;
     if ((int64_t)hist_grid > w.tiles)
         hist_grid = (int)w.tiles;
-    k_sort_hist<K><<<hist_grid, SORT_BLOCK, 0, s>>>(keys, n, passes, bits, w.hist);
-    k_sort_bases<<<1, 256, 0, s>>>(w.hist, w.base, w.portions, passes);
+    { k_sort_hist<K><<<hist_grid, SORT_BLOCK, 0, s>>>(keys, n, passes, bits, w.hist); count_launch(); }
+    { k_sort_bases<<<1, 256, 0, s>>>(w.hist, w.base, w.portions, passes); count_launch(); }
     const size_t smem = sizeof(SortSmem<K>);
     cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     K* src_k = keys;
@@ -409,8 +420,8 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     for (int p = 0; p < passes; p++)
     {
         cudaMemsetAsync(w.status, 0, sizeof(uint32_t) * (size_t)w.tiles * 256, s);
-        k_onesweep<K><<<(unsigned)w.tiles, SORT_BLOCK, smem, s>>>(src_k, src_v, dst_k, dst_v, n, p * bits, bits,
-                                                                   w.base, p, w.status, w.counters + p, err);
+        { k_onesweep<K><<<(unsigned)w.tiles, SORT_BLOCK, smem, s>>>(src_k, src_v, dst_k, dst_v, n, p * bits, bits,
+                                                                   w.base, p, w.status, w.counters + p, err); count_launch(); }
         K* tk = src_k;
         src_k = dst_k;
         dst_k = tk;

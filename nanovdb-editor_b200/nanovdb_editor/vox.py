@@ -62,6 +62,7 @@ class vox_stats_t(Structure):
         ("ms_build", c_float),
         ("ms_accumulate", c_float),
         ("ms_total", c_float),
+        ("kernel_launches", c_int64),
     ]
 
     def as_dict(self) -> dict:

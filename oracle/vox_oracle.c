@@ -386,6 +386,7 @@ typedef struct
     /* inputs */
     int64_t G;
     float vs, cull;
+    int skip_f64; /* timing runs: only the float outputs the product computes */
     prim_t* prims;
     /* pairs in emission (Gaussian-major) order, later sorted */
     uint64_t* keys;
@@ -650,7 +651,7 @@ static void* values_worker(void* arg)
             dsum = VOX_FADD(dsum, a);
             for (int ch = 0; ch < 3; ch++)
                 csum[ch] = VOX_FADD(csum[ch], VOX_FMUL(a, P->rgb[ch]));
-            double a64 = frag_alpha64(P, (double)S->vs, (double)S->cull, ijk);
+            double a64 = S->skip_f64 ? 0.0 : frag_alpha64(P, (double)S->vs, (double)S->cull, ijk);
             dsum64 += a64;
             for (int ch = 0; ch < 3; ch++)
                 csum64[ch] += a64 * (double)P->rgb[ch];
@@ -772,6 +773,8 @@ void* ov_run(int64_t n, const float* means, const float* quats_wxyz, const float
     S->G = n;
     S->vs = voxel_size;
     S->cull = cull_scale;
+    S->skip_f64 = (window_mode & OV_MODE_NO_F64) != 0;
+    window_mode &= OV_MODE_WINDOWS;
     S->prims = (prim_t*)malloc(sizeof(prim_t) * (n ? n : 1));
     int64_t valid = 0;
     uint64_t F = 0;

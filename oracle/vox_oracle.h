@@ -52,6 +52,10 @@ enum
 void ov_preprocess(int64_t n, const float* quat_raw, const float* log_scale, const float* opacity_logit,
                    const float* sh0, float* quat_out, float* scale_out, float* opacity_out, float* color_out);
 
+/* mode bits of ov_run */
+#define OV_MODE_WINDOWS 1 /* reference 256K-prim x 8M-fragment windows (else one window) */
+#define OV_MODE_NO_F64 2  /* skip the FP64 values (timed CPU-baseline runs) */
+
 /* Full forward.  window_mode 1 = reference 256K-prim x 8M-fragment windows,
  * 0 = one window (canonical hierarchical node order).  cull_scale <= 0 selects
  * the shader default 0.05 (gaussian_frag_color.slang:205-213). */
