@@ -61,8 +61,9 @@ struct vox_context_t
     DevBuf scal; // device scalars
     DevBuf hier_keys;
     uint64_t* hscal = nullptr; // pinned mirror
-    Epochs scan_epochs, emit_epochs, run_epochs;
+    Epochs scan_epochs, emit_epochs, run_epochs, sort_epochs;
     uint64_t pair_cap = 0;
+    int check_sort = 0; // VOX_CHECK_SORT=1: validate key order after every sort
     int key64 = 0;
     int sorted_in_alt = 0;
     vox_stats_t stats{};
@@ -160,6 +161,12 @@ static int sync_scalars(vox_context_t* ctx, const char* where)
     {
         set_error(ctx, "%s: a Gaussian's bounding box covers 2^31 or more voxels", where);
         return VOX_ERR_FOOTPRINT;
+    }
+    if (err & (ERR_ORDER | ERR_BOUNDS))
+    {
+        set_error(ctx, "%s: internal consistency check failed (%s%s)", where, (err & ERR_ORDER) ? "keys out of order " : "",
+                  (err & ERR_BOUNDS) ? "index out of range" : "");
+        return VOX_ERR_CUDA;
     }
     return VOX_OK;
 }
@@ -344,16 +351,30 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     int in_alt;
     if (key64)
         in_alt = sort_pairs_u64((uint64_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, (uint64_t*)ctx->keys_alt.p,
-                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, d_err, ctx->num_sms, s,
+                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, &ctx->sort_epochs, d_err, ctx->num_sms, s,
                                 ctx->tuning);
     else
         in_alt = sort_pairs_u32((uint32_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, (uint32_t*)ctx->keys_alt.p,
-                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, d_err, ctx->num_sms, s,
+                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, &ctx->sort_epochs, d_err, ctx->num_sms, s,
                                 ctx->tuning);
     ctx->sorted_in_alt = in_alt;
     ctx->stats.sort_passes = (key_bits + ctx->tuning.digit_bits - 1) / ctx->tuning.digit_bits;
     const void* skeys = in_alt ? ctx->keys_alt.p : ctx->keys.p;
     const uint32_t* sids = (const uint32_t*)(in_alt ? ctx->ids_alt.p : ctx->ids.p);
+    if (ctx->check_sort)
+    {
+        check_sorted(skeys, P_pairs, key64, sc + SC_SCRATCH + 2, ctx->num_sms, s);
+        rc = sync_scalars(ctx, "sort");
+        if (rc)
+            return rc;
+        uint64_t descents = 0;
+        cudaMemcpy(&descents, sc + SC_SCRATCH + 2, sizeof(uint64_t), cudaMemcpyDeviceToHost);
+        if (descents)
+        {
+            set_error(ctx, "sort: %llu keys out of order", (unsigned long long)descents);
+            return VOX_ERR_CUDA;
+        }
+    }
     cudaEventRecord(ctx->timers.ev[3], s);
 
     // ---------------------------------------------------------------- runs
@@ -373,6 +394,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     Rp.epoch = ctx->run_epochs.next(Rp.status, ctx->run_status.cap / sizeof(uint64_t), s);
     Rp.counter = d_counter;
     Rp.err = d_err;
+    Rp.lower_cap = NL + 2;
     if (P_pairs == 0)
     {
         cudaMemsetAsync(Rp.vox_start, 0, 4, s);
@@ -568,6 +590,8 @@ vox_context_t* vox_context_create(int device)
     }
     for (auto& e : ctx->timers.ev)
         cudaEventCreate(&e);
+    const char* chk = getenv("VOX_CHECK_SORT");
+    ctx->check_sort = (chk && chk[0] == '1') ? 1 : 0;
     return ctx;
 }
 

@@ -435,5 +435,7 @@ constexpr int ERR_LOOKBACK = 1;
 constexpr int ERR_RANGE = 2;      // voxel coordinate outside [-65536, 65535]
 constexpr int ERR_FOOTPRINT = 4;  // one Gaussian's bbox above 2^31 fragments
 constexpr int ERR_CAPACITY = 8;   // pair buffer too small (host retries)
+constexpr int ERR_ORDER = 16;     // keys found out of order after the sort
+constexpr int ERR_BOUNDS = 32;    // an index check failed; the access was skipped
 
 } // namespace vox

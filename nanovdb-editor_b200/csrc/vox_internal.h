@@ -75,8 +75,12 @@ size_t sort_workspace_bytes(int64_t n, int key_bytes);
 // keys_alt / vals_alt as ping-pong buffers; returns 0 if the result is in
 // keys / vals and 1 if it is in keys_alt / vals_alt.
 int sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
 int sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
+size_t sort_status_words(int64_t n);
+
+// counts keys[i] < keys[i - 1] into *descents (validation)
+void check_sorted(const void* keys, int64_t n, int key64, uint64_t* descents, int num_sms, cudaStream_t s);
 
 } // namespace vox

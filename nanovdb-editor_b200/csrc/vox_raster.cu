@@ -187,6 +187,11 @@ __global__ void __launch_bounds__(EMIT_BLOCK) k_emit(EmitParams E, RankTables T,
             while (c < cend)
             {
                 // Gaussian g owns [frag_off[g], frag_off[g] + footprint)
+                if (g >= E.G)
+                {
+                    atomicOr(E.err, ERR_BOUNDS);
+                    break;
+                }
                 const GaussRec R = E.recs[g];
                 const uint64_t gbeg = E.frag_off[g];
                 const uint64_t gend = gbeg + (uint64_t)R.q5.x * (uint64_t)R.q5.y * (uint64_t)R.q5.z;
@@ -313,8 +318,15 @@ __global__ void __launch_bounds__(RUN_BLOCK) k_runs(RunParams Rp, const K* __res
         uint32_t f = fl[t];
         if (f & 4u)
         {
-            Rp.lower_lstart[lo] = (uint32_t)l;
-            Rp.lower_rank[lo] = (uint32_t)((uint64_t)keys[idx] >> 21);
+            // distinct lower ranks never exceed the touched-cell count; more
+            // heads mean the keys are not sorted: report, never write past it
+            if (lo + 1 < Rp.lower_cap)
+            {
+                Rp.lower_lstart[lo] = (uint32_t)l;
+                Rp.lower_rank[lo] = (uint32_t)((uint64_t)keys[idx] >> 21);
+            }
+            else
+                atomicOr(Rp.err, ERR_ORDER);
             lo++;
         }
         if (f & 2u)
@@ -331,7 +343,8 @@ __global__ void __launch_bounds__(RUN_BLOCK) k_runs(RunParams Rp, const K* __res
         {
             Rp.vox_start[v] = (uint32_t)P;
             Rp.leaf_vstart[l] = (uint32_t)v;
-            Rp.lower_lstart[lo] = (uint32_t)l;
+            if (lo < Rp.lower_cap)
+                Rp.lower_lstart[lo] = (uint32_t)l;
             Rp.counts[0] = v;
             Rp.counts[1] = l;
             Rp.counts[2] = lo;

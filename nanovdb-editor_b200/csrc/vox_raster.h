@@ -44,6 +44,7 @@ struct RunParams
     uint32_t epoch;
     uint32_t* counter;
     int* err;
+    uint64_t lower_cap;     // entries of lower_lstart / lower_rank (heads beyond it are an error)
 };
 
 struct NodeParams

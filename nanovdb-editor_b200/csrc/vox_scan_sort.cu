@@ -95,28 +95,23 @@ void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, 
 }
 
 // ===================================================================== sort
-// Tile: SORT_BLOCK threads x SORT_ITEMS keys.  Keys are processed in
-// portions of at most 2^29 keys so that 32-bit look-back words (2 flag bits,
-// 30-bit count) never overflow; each portion's digit bases come from the
-// up-front histogram pass.
+// Tile: SORT_BLOCK threads x SORT_ITEMS keys.  One up-front pass computes the
+// digit histograms of every pass (global counts are permutation-invariant);
+// each scatter pass then finds, per digit, the count in earlier tiles with a
+// decoupled look-back over 64-bit epoch-tagged words (55-bit counts).
 constexpr int SORT_BLOCK = 512;
 constexpr int SORT_WARPS = SORT_BLOCK / 32;
 constexpr int SORT_ITEMS = 16;
 constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
-constexpr int SORT_TILES_PER_PORTION = 1 << 16;
-constexpr int64_t SORT_PORTION = (int64_t)SORT_TILE * SORT_TILES_PER_PORTION; // 2^29
 constexpr int SORT_MAX_PASSES = 8;
-constexpr uint32_t ST_AGG = 1u << 30;
-constexpr uint32_t ST_INCL = 2u << 30;
-constexpr uint32_t ST_VAL = (1u << 30) - 1u;
 
 struct SortWs
 {
-    uint32_t* hist;      // [portions][passes][256]
-    uint64_t* base;      // [portions][passes][256]
-    uint32_t* status;    // [tiles][256]
-    uint32_t* counters;  // [passes]
-    int64_t tiles, portions;
+    uint32_t* hist;     // [passes][256]
+    uint64_t* base;     // [passes][256]
+    uint32_t* counters; // [passes]
+    uint64_t* status;   // [tiles][256]
+    int64_t tiles;
 };
 
 static size_t align256(size_t x)
@@ -128,17 +123,14 @@ static SortWs carve(void* ws, int64_t n)
 {
     SortWs w;
     w.tiles = (n + SORT_TILE - 1) / SORT_TILE;
-    w.portions = (n + SORT_PORTION - 1) / SORT_PORTION;
-    if (w.portions < 1)
-        w.portions = 1;
     char* p = (char*)ws;
     w.hist = (uint32_t*)p;
-    p += align256(sizeof(uint32_t) * w.portions * SORT_MAX_PASSES * 256);
+    p += align256(sizeof(uint32_t) * SORT_MAX_PASSES * 256);
     w.base = (uint64_t*)p;
-    p += align256(sizeof(uint64_t) * w.portions * SORT_MAX_PASSES * 256);
+    p += align256(sizeof(uint64_t) * SORT_MAX_PASSES * 256);
     w.counters = (uint32_t*)p;
     p += align256(sizeof(uint32_t) * SORT_MAX_PASSES);
-    w.status = (uint32_t*)p;
+    w.status = (uint64_t*)p;
     return w;
 }
 
@@ -146,12 +138,13 @@ size_t sort_workspace_bytes(int64_t n, int key_bytes)
 {
     (void)key_bytes;
     int64_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
-    int64_t portions = (n + SORT_PORTION - 1) / SORT_PORTION;
-    if (portions < 1)
-        portions = 1;
-    return align256(sizeof(uint32_t) * portions * SORT_MAX_PASSES * 256) +
-           align256(sizeof(uint64_t) * portions * SORT_MAX_PASSES * 256) + align256(sizeof(uint32_t) * SORT_MAX_PASSES) +
-           align256(sizeof(uint32_t) * (tiles + 1) * 256);
+    return align256(sizeof(uint32_t) * SORT_MAX_PASSES * 256) + align256(sizeof(uint64_t) * SORT_MAX_PASSES * 256) +
+           align256(sizeof(uint32_t) * SORT_MAX_PASSES) + align256(sizeof(uint64_t) * (tiles + 1) * 256);
+}
+
+size_t sort_status_words(int64_t n)
+{
+    return (size_t)((n + SORT_TILE - 1) / SORT_TILE + 1) * 256;
 }
 
 template <class K>
@@ -160,7 +153,8 @@ __device__ __forceinline__ uint32_t digit_of(K k, int shift, uint32_t mask)
     return (uint32_t)(k >> shift) & mask;
 }
 
-// up-front histogram of every pass's digit, per portion
+// up-front histogram of every pass's digit (per-CTA shared counters, then
+// one global atomic per bin); counts fit 32 bits for n < 2^32
 template <class K>
 __global__ void __launch_bounds__(SORT_BLOCK) k_sort_hist(const K* keys, int64_t n, int passes, int bits,
                                                             uint32_t* hist)
@@ -170,75 +164,28 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_sort_hist(const K* keys, int64_t
     for (int i = threadIdx.x; i < SORT_MAX_PASSES * 256; i += blockDim.x)
         s_h[i] = 0;
     __syncthreads();
-    int64_t cur_portion = -1;
-    const int64_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
-    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x)
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (int64_t)gridDim.x * blockDim.x)
     {
-        int64_t portion = t / SORT_TILES_PER_PORTION;
-        if (portion != cur_portion)
-        {
-            __syncthreads();
-            if (cur_portion >= 0)
-            {
-                for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
-                {
-                    if (s_h[i])
-                        atomicAdd(&hist[cur_portion * SORT_MAX_PASSES * 256 + i], s_h[i]);
-                    s_h[i] = 0;
-                }
-            }
-            cur_portion = portion;
-            __syncthreads();
-        }
-        int64_t b = t * SORT_TILE;
-        for (int i = threadIdx.x; i < SORT_TILE; i += blockDim.x)
-        {
-            int64_t idx = b + i;
-            if (idx < n)
-            {
-                K k = keys[idx];
-                for (int p = 0; p < passes; p++)
-                    atomicAdd(&s_h[p * 256 + digit_of(k, p * bits, mask)], 1u);
-            }
-        }
+        K k = keys[idx];
+        for (int p = 0; p < passes; p++)
+            atomicAdd(&s_h[p * 256 + digit_of(k, p * bits, mask)], 1u);
     }
     __syncthreads();
-    if (cur_portion >= 0)
-        for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
-            if (s_h[i])
-                atomicAdd(&hist[cur_portion * SORT_MAX_PASSES * 256 + i], s_h[i]);
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
+        if (s_h[i])
+            atomicAdd(&hist[i], s_h[i]);
 }
 
-// base[portion][pass][d] = sum_{d' < d} total[pass][d'] + sum_{p' < portion} hist[p'][pass][d]
-__global__ void k_sort_bases(const uint32_t* hist, uint64_t* base, int64_t portions, int passes)
+// base[pass][d] = sum_{d' < d} hist[pass][d']
+__global__ void k_sort_bases(const uint32_t* hist, uint64_t* base, int passes)
 {
     __shared__ uint64_t s_warp[33];
     const int d = threadIdx.x; // 256 threads
     for (int p = 0; p < passes; p++)
     {
-        uint64_t tot = 0;
-        for (int64_t q = 0; q < portions; q++)
-            tot += hist[q * SORT_MAX_PASSES * 256 + p * 256 + d];
         uint64_t all;
-        uint64_t excl = block_excl_scan_u64(tot, s_warp, all);
-        uint64_t run = excl;
-        for (int64_t q = 0; q < portions; q++)
-        {
-            base[q * SORT_MAX_PASSES * 256 + p * 256 + d] = run;
-            run += hist[q * SORT_MAX_PASSES * 256 + p * 256 + d];
-        }
+        base[p * 256 + d] = block_excl_scan_u64((uint64_t)hist[p * 256 + d], s_warp, all);
     }
-}
-
-__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v)
-{
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p)
-{
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
 }
 
 template <class K>
@@ -257,7 +204,7 @@ template <class K>
 __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                                                            K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                                                            int64_t n, int shift, int bits, const uint64_t* base,
-                                                           int pass, uint32_t* status, uint32_t* counter, int* err)
+                                                           uint64_t* status, uint32_t epoch, uint32_t* counter, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
@@ -272,8 +219,6 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
     __syncthreads();
     const int64_t tile = S.tile;
     const int64_t tile_base = tile * SORT_TILE;
-    const int64_t portion = tile / SORT_TILES_PER_PORTION;
-    const int64_t ptile = tile % SORT_TILES_PER_PORTION;
     const int tile_count = (int)min((int64_t)SORT_TILE, n - tile_base);
 
     // load: warp-contiguous chunks, item-major within a warp (stable order = (item, lane))
@@ -329,42 +274,11 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
     {
         S.digit_excl[threadIdx.x] = (uint32_t)dexcl;
         const int d = threadIdx.x;
-        uint64_t excl = 0;
         if (d < radix)
         {
-            uint32_t* st = status + (size_t)tile * 256 + d;
-            if (ptile == 0)
-            {
-                st_release_u32(st, ST_INCL | ((uint32_t)total & ST_VAL));
-            }
-            else
-            {
-                st_release_u32(st, ST_AGG | ((uint32_t)total & ST_VAL));
-                int64_t p = tile - 1;
-                const int64_t pfirst = portion * SORT_TILES_PER_PORTION;
-                uint32_t spins = 0;
-                while (p >= pfirst)
-                {
-                    uint32_t sv = ld_acquire_u32(status + (size_t)p * 256 + d);
-                    uint32_t flag = sv & ~ST_VAL;
-                    if (flag == 0)
-                    {
-                        if (++spins > LB_SPIN_LIMIT)
-                        {
-                            atomicExch(err, ERR_LOOKBACK);
-                            break;
-                        }
-                        __nanosleep(20);
-                        continue;
-                    }
-                    excl += sv & ST_VAL;
-                    if (flag == ST_INCL)
-                        break;
-                    p--;
-                }
-                st_release_u32(st, ST_INCL | ((uint32_t)(excl + total) & ST_VAL));
-            }
-            S.gbase[d] = base[portion * SORT_MAX_PASSES * 256 + pass * 256 + d] + excl - dexcl;
+            // count of digit d in all earlier tiles
+            uint64_t excl = lookback_exclusive(status + d, (uint64_t)tile, total, epoch, err, 256);
+            S.gbase[d] = base[d] + excl - dexcl;
         }
     }
     __syncthreads();
@@ -378,8 +292,13 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
         {
             uint32_t d = digit_of(k[i], shift, mask);
             uint32_t pos = S.digit_excl[d] + S.warp_hist[warp][d] + rank[i];
-            S.keys[pos] = k[i];
-            S.vals[pos] = v[i];
+            if (pos < (uint32_t)SORT_TILE)
+            {
+                S.keys[pos] = k[i];
+                S.vals[pos] = v[i];
+            }
+            else
+                atomicOr(err, ERR_BOUNDS);
         }
     }
     __syncthreads();
@@ -388,14 +307,20 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
         K kk = S.keys[i];
         uint32_t d = digit_of(kk, shift, mask);
         uint64_t dst = S.gbase[d] + (uint64_t)i;
-        keys_out[dst] = kk;
-        vals_out[dst] = S.vals[i];
+        if (dst < (uint64_t)n)
+        {
+            keys_out[dst] = kk;
+            vals_out[dst] = S.vals[i];
+        }
+        else
+            atomicOr(err, ERR_BOUNDS);
     }
 }
 
 template <class K>
 static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                           void* workspace, int* err, int num_sms, cudaStream_t s, const SortTuning& tune)
+                           void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s,
+                           const SortTuning& tune)
 {
     if (n <= 1 || key_bits <= 0)
         return 0;
@@ -404,24 +329,26 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     if (passes > SORT_MAX_PASSES)
         passes = SORT_MAX_PASSES;
     SortWs w = carve(workspace, n);
-    cudaMemsetAsync(w.hist, 0, sizeof(uint32_t) * w.portions * SORT_MAX_PASSES * 256, s);
+    cudaMemsetAsync(w.hist, 0, sizeof(uint32_t) * SORT_MAX_PASSES * 256, s);
     cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * SORT_MAX_PASSES, s);
-    int hist_grid = num_sms * 2;
-    if ((int64_t)hist_grid > w.tiles)
-        hist_grid = (int)w.tiles;
-    { k_sort_hist<K><<<hist_grid, SORT_BLOCK, 0, s>>>(keys, n, passes, bits, w.hist); count_launch(); }
-    { k_sort_bases<<<1, 256, 0, s>>>(w.hist, w.base, w.portions, passes); count_launch(); }
+    int64_t hist_grid = (int64_t)num_sms * 4;
+    int64_t need = (n + SORT_BLOCK - 1) / SORT_BLOCK;
+    if (hist_grid > need)
+        hist_grid = need;
+    { k_sort_hist<K><<<(unsigned)hist_grid, SORT_BLOCK, 0, s>>>(keys, n, passes, bits, w.hist); count_launch(); }
+    { k_sort_bases<<<1, 256, 0, s>>>(w.hist, w.base, passes); count_launch(); }
     const size_t smem = sizeof(SortSmem<K>);
     cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     K* src_k = keys;
     uint32_t* src_v = vals;
     K* dst_k = keys_alt;
     uint32_t* dst_v = vals_alt;
+    const size_t words = sort_status_words(n);
     for (int p = 0; p < passes; p++)
     {
-        cudaMemsetAsync(w.status, 0, sizeof(uint32_t) * (size_t)w.tiles * 256, s);
+        uint32_t epoch = epochs->next(w.status, words, s);
         { k_onesweep<K><<<(unsigned)w.tiles, SORT_BLOCK, smem, s>>>(src_k, src_v, dst_k, dst_v, n, p * bits, bits,
-                                                                   w.base, p, w.status, w.counters + p, err); count_launch(); }
+                                                                   w.base + p * 256, w.status, epoch, w.counters + p, err); count_launch(); }
         K* tk = src_k;
         src_k = dst_k;
         dst_k = tk;
@@ -433,14 +360,49 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
 }
 
 int sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, int* err, int num_sms, cudaStream_t s, const SortTuning& tune)
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune)
 {
-    return sort_pairs_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, key_bits, workspace, err, num_sms, s, tune);
+    return sort_pairs_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, key_bits, workspace, epochs, err, num_sms, s,
+                                     tune);
 }
 int sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, int* err, int num_sms, cudaStream_t s, const SortTuning& tune)
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune)
 {
-    return sort_pairs_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, key_bits, workspace, err, num_sms, s, tune);
+    return sort_pairs_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, key_bits, workspace, epochs, err, num_sms, s,
+                                     tune);
 }
 
+} // namespace vox
+
+namespace vox
+{
+// counts adjacent pairs with keys[i] < keys[i - 1] (a read-only validation pass)
+template <class K>
+__global__ void k_check_sorted(const K* keys, int64_t n, unsigned long long* descents)
+{
+    unsigned long long local = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        local += keys[i] < keys[i - 1] ? 1ull : 0ull;
+    for (int o = 16; o > 0; o >>= 1)
+        local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local)
+        atomicAdd(descents, local);
+}
+
+void check_sorted(const void* keys, int64_t n, int key64, uint64_t* descents, int num_sms, cudaStream_t s)
+{
+    cudaMemsetAsync(descents, 0, sizeof(uint64_t), s);
+    if (n <= 1)
+        return;
+    if (key64)
+    {
+        k_check_sorted<uint64_t><<<num_sms * 4, 256, 0, s>>>((const uint64_t*)keys, n, (unsigned long long*)descents);
+        count_launch();
+    }
+    else
+    {
+        k_check_sorted<uint32_t><<<num_sms * 4, 256, 0, s>>>((const uint32_t*)keys, n, (unsigned long long*)descents);
+        count_launch();
+    }
+}
 } // namespace vox
