@@ -169,6 +169,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--gaussians", type=int, default=WORKLOAD["gaussians"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer C-ABI measurement (profiling runs)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -241,36 +242,39 @@ def main():
     value = world * G / (ms * 1e-3)
 
     # ---- e2e through the reference-facing C ABI with host buffers
-    comp = Compute(device_index=local)
-    raster = Raster(comp)
-    pinned = [torch.from_numpy(a).pin_memory() for a in raw]
-    arrays = []
-    for t in pinned:
-        arr = pnanovdb_ComputeArray()
-        arr.data = t.data_ptr()
-        arr.element_size = 4
-        arr.element_count = t.numel()
-        arrays.append(arr)
-    h2d = sum(int(t.numel()) * 4 for t in pinned[:5])
-    out = raster.raster_to_nanovdb_from_arrays(vs, arrays)  # warm
-    comp.destroy_array(out)
-    e2e_times, d2h = [], 0
-    if dist:
-        dist.barrier()
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        out = raster.raster_to_nanovdb_from_arrays(vs, arrays)
-        e2e_times.append(time.perf_counter() - t0)
-        d2h = int(out.element_size * out.element_count)
+    e2e = None
+    if not args.no_e2e:
+        comp = Compute(device_index=local)
+        raster = Raster(comp)
+        pinned = [torch.from_numpy(a).pin_memory() for a in raw]
+        arrays = []
+        for t in pinned:
+            arr = pnanovdb_ComputeArray()
+            arr.data = t.data_ptr()
+            arr.element_size = 4
+            arr.element_count = t.numel()
+            arrays.append(arr)
+        h2d = sum(int(t.numel()) * 4 for t in pinned[:5])
+        out = raster.raster_to_nanovdb_from_arrays(vs, arrays)  # warm
         comp.destroy_array(out)
-    e2e_s = sum(e2e_times) / len(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * G / e2e_s
+        e2e_times, d2h = [], 0
+        if dist:
+            dist.barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = raster.raster_to_nanovdb_from_arrays(vs, arrays)
+            e2e_times.append(time.perf_counter() - t0)
+            d2h = int(out.element_size * out.element_count)
+            comp.destroy_array(out)
+        e2e_s = sum(e2e_times) / len(e2e_times)
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_value = world * G / e2e_s
+        e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3}
 
     # ---- roofline of the dominant stage
     st = stats[-1]
@@ -320,7 +324,7 @@ def main():
             "dtype": "f32",
             "data": "synthetic",
             "config": dict(WORKLOAD, gaussians=G, parallelism=f"replicas{world}" if world > 1 else "single", l2="256 MB flush between steps; pair working set >> L2", inputs="raw (log-scale, logit, SH0)"),
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+            "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind},
             "stages_ms": stage_ms,

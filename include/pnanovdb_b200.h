@@ -326,6 +326,25 @@ PNANOVDB_API int vox_copy_pairs(vox_context_t* ctx, uint64_t* keys, uint32_t* id
 
 PNANOVDB_API void vox_get_stats(vox_context_t* ctx, vox_stats_t* out);
 
+/* ---------------------------------------------------- parallel primitives --
+ * The primitives the path is built on, on device pointers, ordered on the
+ * context's stream and synchronised before returning. */
+
+/* replaces pnanovdb_parallel_primitives_t::global_scan_uint64
+ * (nanovdb_editor/putil/ParallelPrimitives.h:41-47, raster/ParallelPrimitives.cpp:151-310):
+ * scan of n u64 values d_in -> d_out (may alias), inclusive when `inclusive`
+ * is non-zero (the reference's scan is inclusive), else exclusive; *d_total
+ * (device) receives the sum. */
+PNANOVDB_API int vox_global_scan_u64(vox_context_t* ctx, const uint64_t* d_in, uint64_t* d_out, int64_t n,
+                                     int inclusive, uint64_t* d_total);
+
+/* replaces pnanovdb_parallel_primitives_t::radix_sort_key64
+ * (nanovdb_editor/putil/ParallelPrimitives.h:77-84, raster/ParallelPrimitives.cpp:685-869):
+ * stable sort of n (64-bit key, 32-bit value) device pairs in place by key
+ * bits [0, key_bit_count). */
+PNANOVDB_API int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n,
+                                      uint32_t key_bit_count);
+
 #ifdef __cplusplus
 }
 #endif

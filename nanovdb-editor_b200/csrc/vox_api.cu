@@ -60,6 +60,7 @@ struct vox_context_t
     DevBuf grid;
     DevBuf scal; // device scalars
     DevBuf hier_keys;
+    DevBuf prim_keys_alt, prim_vals_alt; // ping-pong buffers of vox_radix_sort_key64
     uint64_t* hscal = nullptr; // pinned mirror
     Epochs scan_epochs, emit_epochs, run_epochs, sort_epochs;
     uint64_t pair_cap = 0;
@@ -608,7 +609,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->lower_origin, &ctx->lower_upper_n, &ctx->upper_head, &ctx->upper_scan,
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
-                      &ctx->hier_keys };
+                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt };
     for (DevBuf* b : all)
         if (b->p)
             cudaFree(b->p);
@@ -737,6 +738,51 @@ void vox_get_stats(vox_context_t* ctx, vox_stats_t* out)
 {
     if (ctx && out)
         *out = ctx->stats;
+}
+
+int vox_global_scan_u64(vox_context_t* ctx, const uint64_t* d_in, uint64_t* d_out, int64_t n, int inclusive,
+                        uint64_t* d_total)
+{
+    if (!ctx || n < 0 || (n > 0 && (!d_in || !d_out)) || !d_total)
+        return VOX_ERR_ARGS;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(n > 512 ? n : 512) * 2))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    uint64_t* status = (uint64_t*)ctx->scan_status.p;
+    scan_exclusive_u64(d_in, d_out, n, inclusive ? 2 : 0, d_total, status,
+                       ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s),
+                       (uint32_t*)(sc + SC_SCRATCH), (int*)(sc + SC_ERR), ctx->num_sms, s);
+    return sync_scalars(ctx, "vox_global_scan_u64");
+}
+
+int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, uint32_t key_bit_count)
+{
+    if (!ctx || n < 0 || (n > 0 && (!d_keys || !d_vals)) || key_bit_count > 64)
+        return VOX_ERR_ARGS;
+    if (n <= 1 || key_bit_count == 0)
+        return VOX_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) ||
+        !ensure(ctx, ctx->prim_keys_alt, 8 * (size_t)n) || !ensure(ctx, ctx->prim_vals_alt, 4 * (size_t)n) ||
+        !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(n, 8)))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    SortTuning t = ctx->tuning;
+    int in_alt = sort_pairs_u64(d_keys, d_vals, (uint64_t*)ctx->prim_keys_alt.p, (uint32_t*)ctx->prim_vals_alt.p, n,
+                                (int)key_bit_count, ctx->sort_ws.p, &ctx->sort_epochs, (int*)(sc + SC_ERR),
+                                ctx->num_sms, s, t);
+    if (in_alt)
+    {
+        cudaMemcpyAsync(d_keys, ctx->prim_keys_alt.p, 8 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d_vals, ctx->prim_vals_alt.p, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    }
+    return sync_scalars(ctx, "vox_radix_sort_key64");
 }
 
 } // extern "C"

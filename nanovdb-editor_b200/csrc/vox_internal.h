@@ -59,8 +59,9 @@ struct Epochs
 };
 
 // ---------------------------------------------------------------- scan ----
-// exclusive scan of n u64 values (mode 0) or of popcounts of n u64 words
-// (mode 1); out may alias in; *total receives the sum.
+// scan of n u64 values; mode bit 0: scan popcounts of the words instead of the
+// values, bit 1: inclusive instead of exclusive.  out may alias in; *total
+// receives the sum.
 size_t scan_status_words(int64_t n);
 void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, uint64_t* total, uint64_t* status,
                         uint32_t epoch, uint32_t* counter, int* err, int num_sms, cudaStream_t s);

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_excl(const uint64_t* in, ui
     {
         int64_t idx = base + i;
         uint64_t x = idx < n ? in[idx] : 0ull;
-        if (mode == 1)
+        if (mode & 1)
             x = (uint64_t)__popcll(x);
         v[i] = x;
         sum += x;
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_excl(const uint64_t* in, ui
         int64_t idx = base + i;
         if (idx < n)
         {
-            out[idx] = run;
+            out[idx] = (mode & 2) ? run + v[i] : run;
             run += v[i];
             if (idx == n - 1)
                 *total = run;

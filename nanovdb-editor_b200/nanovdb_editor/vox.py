@@ -88,6 +88,10 @@ def _lib():
         lib.vox_copy_pairs.restype = c_int
         lib.vox_copy_pairs.argtypes = [c_void_p, c_void_p, c_void_p, c_int64]
         lib.vox_get_stats.argtypes = [c_void_p, POINTER(vox_stats_t)]
+        lib.vox_global_scan_u64.restype = c_int
+        lib.vox_global_scan_u64.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]
+        lib.vox_radix_sort_key64.restype = c_int
+        lib.vox_radix_sort_key64.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_uint32]
         lib._vox_bound = True
     return lib
 
@@ -184,3 +188,13 @@ class VoxContext:
         st = vox_stats_t()
         self.lib.vox_get_stats(self.handle, byref(st))
         return st.as_dict()
+
+    def global_scan_u64(self, d_in, d_out, d_total, inclusive: bool = True) -> None:
+        """Scan of CUDA uint64 tensors (the reference's global_scan_uint64 is inclusive)."""
+        n = int(d_in.numel())
+        self._check(self.lib.vox_global_scan_u64(self.handle, _ptr(d_in), _ptr(d_out), n, 1 if inclusive else 0, _ptr(d_total)), "vox_global_scan_u64")
+
+    def radix_sort_key64(self, d_keys, d_vals, key_bits: int = 64) -> None:
+        """Stable in-place sort of CUDA (uint64 key, uint32 value) tensors by key bits [0, key_bits)."""
+        n = int(d_keys.numel())
+        self._check(self.lib.vox_radix_sort_key64(self.handle, _ptr(d_keys), _ptr(d_vals), n, int(key_bits)), "vox_radix_sort_key64")
