@@ -345,6 +345,27 @@ PNANOVDB_API int vox_global_scan_u64(vox_context_t* ctx, const uint64_t* d_in, u
 PNANOVDB_API int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n,
                                       uint32_t key_bit_count);
 
+/* Scan that allocates nothing.  No counterpart in the reference.
+ *
+ * Same result as vox_global_scan_u64, for callers that cannot let a library
+ * allocate device memory: hosts whose device memory is owned by their own
+ * allocator (a framework's caching pool holding the free memory, where an
+ * extra cudaMalloc can fail or fragment it) and loops where the implicit
+ * device synchronisation of cudaMalloc / cudaFree is not acceptable.  It
+ * needs no vox_context_t and calls no cudaMalloc, cudaFree or other
+ * allocating routine: its look-back scratch is a fixed 64 KiB device array
+ * inside the library (held by every GPU that loads the library until exit),
+ * which limits n to VOX_NOALLOC_SCAN_MAX; larger n returns VOX_ERR_SIZE.
+ *
+ * The first call on each device looks up that array's device address, so
+ * make it before any stream capture.  All calls share the one array: calls
+ * whose work overlaps on the GPU (concurrent streams or threads) race and
+ * must be serialised by the caller.  The call is ordered on `stream`
+ * (cudaStream_t, may be 0) and returns after the scan has completed. */
+#define VOX_NOALLOC_SCAN_MAX (1ll << 24)
+PNANOVDB_API int vox_global_scan_u64_noalloc(const uint64_t* d_in, uint64_t* d_out, int64_t n, int inclusive,
+                                             uint64_t* d_total, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
