@@ -50,12 +50,13 @@ struct vox_context_t
     std::string last_error;
     std::vector<DevBuf*> bufs;
     // device buffers
-    DevBuf recs, footprints, frag_off, root_bits, root_prefix, root_of_rank, lower_bits, lower_prefix, lower_cell;
+    DevBuf recs, footprints, frag_off, columns, col_off, root_bits, root_prefix, root_of_rank, lower_bits, lower_prefix, lower_cell;
     DevBuf scan_status, emit_status, run_status;
     DevBuf keys, ids, keys_alt, ids_alt, sort_ws;
     DevBuf vox_start, leaf_vstart, lower_lstart, lower_rank;
     DevBuf lower_origin, lower_upper_n, upper_head, upper_scan, lower_parent, upper_root_n, upper_lostart;
     DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
+    DevBuf vox_leaf, vox_n, rank_to_lower;
     DevBuf order; // 9 node order arrays
     DevBuf grid;
     DevBuf scal; // device scalars
@@ -65,6 +66,7 @@ struct vox_context_t
     Epochs scan_epochs, emit_epochs, run_epochs, sort_epochs;
     uint64_t pair_cap = 0;
     int check_sort = 0; // VOX_CHECK_SORT=1: validate key order after every sort
+    int check_emit = 0; // VOX_CHECK_EMIT=1: test the candidates the column bound skips
     int key64 = 0;
     int sorted_in_alt = 0;
     vox_stats_t stats{};
@@ -87,6 +89,7 @@ enum
     SC_LO,
     SC_U,
     SC_ERR, // int in the low half
+    SC_NC,  // emission columns
     SC_BBOX, // 3 words (6 int32)
     SC_COUNT = SC_BBOX + 3,
     SC_SCRATCH = 16
@@ -227,6 +230,8 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     if (!ensure(ctx, ctx->recs, sizeof(GaussRec) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->footprints, sizeof(uint64_t) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->frag_off, sizeof(uint64_t) * (size_t)(G + 1)) ||
+        !ensure(ctx, ctx->columns, sizeof(uint64_t) * (size_t)(G + 1)) ||
+        !ensure(ctx, ctx->col_off, sizeof(uint64_t) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->root_bits, sizeof(uint64_t) * 512) || !ensure(ctx, ctx->root_prefix, sizeof(uint64_t) * 512) ||
         !ensure(ctx, ctx->root_of_rank, sizeof(uint32_t) * 32768) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(G > 512 ? G : 512) * 2))
@@ -234,6 +239,8 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     GaussRec* recs = (GaussRec*)ctx->recs.p;
     uint64_t* footprints = (uint64_t*)ctx->footprints.p;
     uint64_t* frag_off = (uint64_t*)ctx->frag_off.p;
+    uint64_t* columns = (uint64_t*)ctx->columns.p;
+    uint64_t* col_off = (uint64_t*)ctx->col_off.p;
     uint64_t* root_bits = (uint64_t*)ctx->root_bits.p;
     uint64_t* root_prefix = (uint64_t*)ctx->root_prefix.p;
     cudaMemsetAsync(root_bits, 0, sizeof(uint64_t) * 512, s);
@@ -247,10 +254,12 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     P.raw = (flags & VOX_FLAG_RAW_INPUTS) ? 1 : 0;
     P.voxel_size = voxel_size;
     P.cull_scale = cull;
-    launch_prep(P, recs, footprints, root_bits, d_err, s);
+    launch_prep(P, recs, footprints, columns, root_bits, d_err, s);
     uint64_t* scan_status = (uint64_t*)ctx->scan_status.p;
     size_t scan_words = ctx->scan_status.cap / sizeof(uint64_t);
     scan_exclusive_u64(footprints, frag_off, G, 0, sc + SC_F, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
+                       d_counter, d_err, ctx->num_sms, s);
+    scan_exclusive_u64(columns, col_off, G, 0, sc + SC_NC, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
                        d_counter, d_err, ctx->num_sms, s);
     scan_exclusive_u64(root_bits, root_prefix, 512, 1, sc + SC_NROOT, scan_status,
                        ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
@@ -260,6 +269,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         return rc;
     const uint64_t F = ctx->hscal[SC_F];
     const uint64_t NR = ctx->hscal[SC_NROOT];
+    const uint64_t NC = ctx->hscal[SC_NC];
     ctx->stats.candidates = (int64_t)F;
 
     // ------------------------------------------------------- lower ranks
@@ -300,15 +310,15 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     int64_t P_pairs = 0;
     for (int attempt = 0; attempt < 2; attempt++)
     {
-        int64_t etiles = emit_tile_count(F);
+        int64_t etiles = emit_tile_count(NC);
         if (!ensure(ctx, ctx->keys, kb * cap) || !ensure(ctx, ctx->ids, 4 * cap) ||
             !ensure(ctx, ctx->emit_status, sizeof(uint64_t) * (size_t)(etiles + 1)))
             return VOX_ERR_MEMORY;
         EmitParams E;
         E.recs = recs;
-        E.frag_off = frag_off;
+        E.col_off = col_off;
         E.G = G;
-        E.F = F;
+        E.NC = NC;
         E.voxel_size = voxel_size;
         E.cap = cap;
         E.status = (uint64_t*)ctx->emit_status.p;
@@ -316,6 +326,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         E.counter = d_counter;
         E.total = sc + SC_P;
         E.err = d_err;
+        E.check = ctx->check_emit;
         if (key64)
             launch_emit_u64(E, T, (uint64_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, ctx->num_sms, s);
         else
@@ -382,11 +393,14 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     const int64_t rtiles = runs_tile_count(P_pairs);
     if (!ensure(ctx, ctx->vox_start, 4 * (size_t)(P_pairs + 2)) || !ensure(ctx, ctx->leaf_vstart, 4 * (size_t)(P_pairs + 2)) ||
         !ensure(ctx, ctx->lower_lstart, 4 * (size_t)(NL + 2)) || !ensure(ctx, ctx->lower_rank, 4 * (size_t)(NL + 2)) ||
-        !ensure(ctx, ctx->run_status, sizeof(uint64_t) * 3 * (size_t)(rtiles + 1)))
+        !ensure(ctx, ctx->run_status, sizeof(uint64_t) * 3 * (size_t)(rtiles + 1)) ||
+        !ensure(ctx, ctx->vox_leaf, 4 * (size_t)(P_pairs + 2)) || !ensure(ctx, ctx->vox_n, 2 * (size_t)(P_pairs + 2)))
         return VOX_ERR_MEMORY;
     RunParams Rp;
     Rp.P = P_pairs;
     Rp.vox_start = (uint32_t*)ctx->vox_start.p;
+    Rp.vox_leaf = (uint32_t*)ctx->vox_leaf.p;
+    Rp.vox_n = (uint16_t*)ctx->vox_n.p;
     Rp.leaf_vstart = (uint32_t*)ctx->leaf_vstart.p;
     Rp.lower_lstart = (uint32_t*)ctx->lower_lstart.p;
     Rp.lower_rank = (uint32_t*)ctx->lower_rank.p;
@@ -414,7 +428,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         !ensure(ctx, ctx->lower_parent, 4 * (size_t)(Lo + 1)) || !ensure(ctx, ctx->upper_root_n, 4 * (size_t)(Lo + 1)) ||
         !ensure(ctx, ctx->upper_lostart, 4 * (size_t)(Lo + 2)) || !ensure(ctx, ctx->leaf_lower, 4 * (size_t)(L + 1)) ||
         !ensure(ctx, ctx->leaf_lower_n, 4 * (size_t)(L + 1)) || !ensure(ctx, ctx->leaf_mask, 64 * (size_t)(L + 1)) ||
-        !ensure(ctx, ctx->leaf_origin, 12 * (size_t)(L + 1)) ||
+        !ensure(ctx, ctx->leaf_origin, 12 * (size_t)(L + 1)) || !ensure(ctx, ctx->rank_to_lower, 4 * (size_t)(NL + 1)) ||
         !ensure(ctx, ctx->order, 8 * 3 * (size_t)((Lo + 1) * 2 + (L + 1))) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(Lo + 1) * 2))
         return VOX_ERR_MEMORY;
@@ -431,6 +445,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     N.vox_start = (const uint32_t*)ctx->vox_start.p;
     N.lower_origin = (int32_t*)ctx->lower_origin.p;
     N.lower_upper_n = (uint32_t*)ctx->lower_upper_n.p;
+    N.rank_to_lower = (uint32_t*)ctx->rank_to_lower.p;
     N.upper_head = (uint64_t*)ctx->upper_head.p;
     N.upper_scan = (uint64_t*)ctx->upper_scan.p;
     N.lower_parent = (uint32_t*)ctx->lower_parent.p;
@@ -483,17 +498,23 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         return VOX_ERR_MEMORY;
     uint8_t* grid = (uint8_t*)ctx->grid.p;
     cudaMemsetAsync(grid, 0, grid_bytes, s);
-    launch_write_nodes(N, U, grid + off_node2, s);
+    cudaMemsetAsync(N.leaf_mask, 0, 64 * (size_t)L, s);
     cudaEventRecord(ctx->timers.ev[4], s);
     AccumParams A;
     A.recs = recs;
     A.keys = skeys;
     A.voxel_size = voxel_size;
+    A.V = V;
+    A.rank_to_lower = N.rank_to_lower;
+    A.vox_leaf = (const uint32_t*)ctx->vox_leaf.p;
+    A.vox_n = (const uint16_t*)ctx->vox_n.p;
     A.rgba8 = (uint32_t*)(grid + off_rgba);
     A.density = (float*)(grid + off_dens);
     A.color = (float*)(grid + off_col);
     launch_accumulate(A, N, sids, key64, s);
     cudaEventRecord(ctx->timers.ev[5], s);
+    launch_leaf_bbox(N, s);
+    launch_write_nodes(N, U, grid + off_node2, s);
     rc = sync_scalars(ctx, "accumulate");
     if (rc)
         return rc;
@@ -593,6 +614,8 @@ vox_context_t* vox_context_create(int device)
         cudaEventCreate(&e);
     const char* chk = getenv("VOX_CHECK_SORT");
     ctx->check_sort = (chk && chk[0] == '1') ? 1 : 0;
+    const char* chk_emit = getenv("VOX_CHECK_EMIT");
+    ctx->check_emit = (chk_emit && chk_emit[0] == '1') ? 1 : 0;
     return ctx;
 }
 
@@ -602,13 +625,14 @@ void vox_context_destroy(vox_context_t* ctx)
         return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf* all[] = { &ctx->recs, &ctx->footprints, &ctx->frag_off, &ctx->root_bits, &ctx->root_prefix,
+    DevBuf* all[] = { &ctx->recs, &ctx->footprints, &ctx->frag_off, &ctx->columns, &ctx->col_off, &ctx->root_bits, &ctx->root_prefix,
                       &ctx->root_of_rank, &ctx->lower_bits, &ctx->lower_prefix, &ctx->lower_cell, &ctx->scan_status,
                       &ctx->emit_status, &ctx->run_status, &ctx->keys, &ctx->ids, &ctx->keys_alt, &ctx->ids_alt,
                       &ctx->sort_ws, &ctx->vox_start, &ctx->leaf_vstart, &ctx->lower_lstart, &ctx->lower_rank,
                       &ctx->lower_origin, &ctx->lower_upper_n, &ctx->upper_head, &ctx->upper_scan,
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
+                      &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
                       &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt };
     for (DevBuf* b : all)
         if (b->p)

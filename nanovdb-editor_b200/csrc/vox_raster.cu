@@ -25,7 +25,7 @@ namespace vox
 {
 
 // ------------------------------------------------------------------ prep ----
-__global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint64_t* footprints,
+__global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint64_t* footprints, uint64_t* columns,
                                               unsigned long long* root_bits, int* err)
 {
     int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint
     }
     recs[g] = R;
     footprints[g] = fp;
+    columns[g] = fp ? (uint64_t)R.q5.x * (uint64_t)R.q5.y : 0ull;
     if (fp)
     {
         // root tiles (4096^3 voxels) spanned by the bbox
@@ -65,12 +66,6 @@ __global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint
                     atomicOr(&root_bits[rn >> 6], 1ull << (rn & 63));
                 }
     }
-}
-
-__device__ __forceinline__ uint64_t bit_rank(const uint64_t* bits, const uint64_t* prefix, uint64_t idx)
-{
-    uint64_t w = bits[idx >> 6];
-    return prefix[idx >> 6] + (uint64_t)__popcll(w & ((1ull << (idx & 63)) - 1ull));
 }
 
 __global__ void __launch_bounds__(256) k_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits,
@@ -111,244 +106,117 @@ __global__ void k_invert_bits(const uint64_t* bits, const uint64_t* prefix, int6
     }
 }
 
-// ------------------------------------------------------------------ emit ----
-constexpr int EMIT_BLOCK = 256;
-constexpr int EMIT_CPT = 16;
-constexpr int EMIT_TILE = EMIT_BLOCK * EMIT_CPT;
-
-__device__ __forceinline__ int64_t upper_bound_u64(const uint64_t* a, int64_t lo, int64_t hi, uint64_t v)
-{
-    while (lo < hi)
-    {
-        int64_t mid = (lo + hi) >> 1;
-        if (a[mid] <= v)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
-template <class K>
-__device__ __forceinline__ K compact_key(const RankTables& T, int32_t x, int32_t y, int32_t z)
-{
-    uint64_t rr = bit_rank(T.root_bits, T.root_prefix, root_n_of(x, y, z));
-    uint64_t cell = rr * 32768ull + upper_n_of(x, y, z);
-    uint64_t lr = bit_rank(T.lower_bits, T.lower_prefix, cell);
-    return (K)((lr << 21) | ((uint64_t)lower_n_of(x, y, z) << 9) | (uint64_t)leaf_n_of(x, y, z));
-}
-
-template <class K>
-struct EmitSmem
-{
-    K stage_k[EMIT_TILE];
-    uint32_t stage_i[EMIT_TILE];
-    K out_k[EMIT_TILE];
-    uint32_t out_i[EMIT_TILE];
-    uint64_t s_warp[33];
-    uint64_t gofs;
-    int64_t g_lo, g_hi;
-    uint32_t tile;
-};
-
-template <class K>
-__global__ void __launch_bounds__(EMIT_BLOCK) k_emit(EmitParams E, RankTables T, K* __restrict__ out_k,
-                                                       uint32_t* __restrict__ out_i)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    EmitSmem<K>& S = *reinterpret_cast<EmitSmem<K>*>(smem_raw);
-    const uint64_t F = E.F;
-    const int64_t ntiles = (int64_t)((F + EMIT_TILE - 1) / EMIT_TILE);
-    while (true)
-    {
-        if (threadIdx.x == 0)
-        {
-            uint32_t t = atomicAdd(E.counter, 1u);
-            S.tile = t;
-            if ((int64_t)t < ntiles)
-            {
-                uint64_t c0 = (uint64_t)t * EMIT_TILE;
-                uint64_t c1 = min(c0 + EMIT_TILE, F) - 1;
-                S.g_lo = upper_bound_u64(E.frag_off, 0, E.G, c0) - 1;
-                S.g_hi = upper_bound_u64(E.frag_off, S.g_lo, E.G, c1);
-            }
-        }
-        __syncthreads();
-        const int64_t tile = S.tile;
-        if (tile >= ntiles)
-            break;
-        const uint64_t cbeg = (uint64_t)tile * EMIT_TILE + (uint64_t)threadIdx.x * EMIT_CPT;
-        const uint64_t cend = min(cbeg + EMIT_CPT, F);
-        uint32_t cnt = 0;
-        if (cbeg < cend)
-        {
-            int64_t g = upper_bound_u64(E.frag_off, S.g_lo, S.g_hi, cbeg) - 1;
-            uint64_t c = cbeg;
-            while (c < cend)
-            {
-                // Gaussian g owns [frag_off[g], frag_off[g] + footprint)
-                if (g >= E.G)
-                {
-                    atomicOr(E.err, ERR_BOUNDS);
-                    break;
-                }
-                const GaussRec R = E.recs[g];
-                const uint64_t gbeg = E.frag_off[g];
-                const uint64_t gend = gbeg + (uint64_t)R.q5.x * (uint64_t)R.q5.y * (uint64_t)R.q5.z;
-                if (!R.q4.w || c >= gend)
-                {
-                    g++;
-                    continue;
-                }
-                const RInv M = rinv_of(R);
-                const uint32_t ry = (uint32_t)R.q5.y, rz = (uint32_t)R.q5.z;
-                uint32_t r = (uint32_t)(c - gbeg);
-                // fragment decode, x slowest / z fastest (gaussian_frag_alloc.slang:55-58)
-                int32_t i = (int32_t)(r / (rz * ry)), j = (int32_t)((r / rz) % ry), k = (int32_t)(r % rz);
-                const uint64_t stop = min(cend, gend);
-                for (; c < stop; c++)
-                {
-                    int32_t x = R.q4.x + i, y = R.q4.y + j, z = R.q4.z + k;
-                    Aabb b = voxel_local_aabb(R, M, E.voxel_size, x, y, z);
-                    if (aabb_hits_unit_sphere(b))
-                    {
-                        S.stage_k[threadIdx.x * EMIT_CPT + cnt] = compact_key<K>(T, x, y, z);
-                        S.stage_i[threadIdx.x * EMIT_CPT + cnt] = (uint32_t)g;
-                        cnt++;
-                    }
-                    if (++k == (int32_t)rz)
-                    {
-                        k = 0;
-                        if (++j == (int32_t)ry)
-                        {
-                            j = 0;
-                            ++i;
-                        }
-                    }
-                }
-            }
-        }
-        uint64_t tile_total;
-        uint64_t texcl = block_excl_scan_u64(cnt, S.s_warp, tile_total);
-        if (threadIdx.x == 0)
-            S.gofs = lookback_exclusive(E.status, (uint64_t)tile, tile_total, E.epoch, E.err);
-        for (uint32_t m = 0; m < cnt; m++)
-        {
-            S.out_k[texcl + m] = S.stage_k[threadIdx.x * EMIT_CPT + m];
-            S.out_i[texcl + m] = S.stage_i[threadIdx.x * EMIT_CPT + m];
-        }
-        __syncthreads();
-        const uint64_t gofs = S.gofs;
-        for (uint32_t m = threadIdx.x; m < (uint32_t)tile_total; m += EMIT_BLOCK)
-        {
-            uint64_t dst = gofs + m;
-            if (dst < E.cap)
-            {
-                out_k[dst] = S.out_k[m];
-                out_i[dst] = S.out_i[m];
-            }
-        }
-        if (threadIdx.x == 0 && tile == ntiles - 1)
-        {
-            *E.total = gofs + tile_total;
-            if (gofs + tile_total > E.cap)
-                atomicOr(E.err, ERR_CAPACITY);
-        }
-        __syncthreads();
-    }
-}
-
 // ------------------------------------------------------------------ runs ----
+// Unique-key run detection over the sorted keys.  Warp-contiguous loads
+// (element = warp chunk + item * 32 + lane), heads found against the
+// previous key (shuffle across lanes, carried across items), counted with
+// ballots, three exclusive counts (voxels, leaves, lower nodes) across the
+// tile and across tiles with a decoupled look-back.
 constexpr int RUN_BLOCK = 256;
-constexpr int RUN_ITEMS = 8;
+constexpr int RUN_ITEMS = 16;
+constexpr int RUN_WARPS = RUN_BLOCK / 32;
 constexpr int RUN_TILE = RUN_BLOCK * RUN_ITEMS;
 
 template <class K>
 __global__ void __launch_bounds__(RUN_BLOCK) k_runs(RunParams Rp, const K* __restrict__ keys)
 {
-    __shared__ uint64_t s_warp[33];
+    __shared__ uint32_t s_wtot[3][RUN_WARPS];
     __shared__ uint64_t s_ex[3];
     __shared__ uint32_t s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0)
         s_tile = atomicAdd(Rp.counter, 1u);
     __syncthreads();
     const uint64_t tile = s_tile;
     const int64_t P = Rp.P;
-    const int64_t base = (int64_t)tile * RUN_TILE + (int64_t)threadIdx.x * RUN_ITEMS;
-    K prev = (base > 0 && base - 1 < P) ? keys[base - 1] : (K)0;
-    uint32_t fl[RUN_ITEMS];
-    uint64_t cv = 0, cl = 0, clo = 0;
+    const int64_t wbase = (int64_t)tile * RUN_TILE + (int64_t)warp * (32 * RUN_ITEMS);
+    K k[RUN_ITEMS];
+    uint32_t bv[RUN_ITEMS], bl[RUN_ITEMS], blo[RUN_ITEMS];
+    K carry = (wbase > 0 && wbase - 1 < P) ? keys[wbase - 1] : (K)0;
+    uint32_t tv = 0, tl = 0, tlo = 0;
 #pragma unroll
-    for (int t = 0; t < RUN_ITEMS; t++)
+    for (int i = 0; i < RUN_ITEMS; i++)
     {
-        int64_t idx = base + t;
-        uint32_t f = 0;
-        if (idx < P)
-        {
-            K k = keys[idx];
-            bool first = idx == 0;
-            bool hv = first || k != prev;
-            bool hl = first || (k >> 9) != (prev >> 9);
-            bool hlo = first || (k >> 21) != (prev >> 21);
-            f = (hv ? 1u : 0u) | (hl ? 2u : 0u) | (hlo ? 4u : 0u);
-            prev = k;
-        }
-        fl[t] = f;
-        cv += f & 1u;
-        cl += (f >> 1) & 1u;
-        clo += (f >> 2) & 1u;
+        const int64_t idx = wbase + i * 32 + lane;
+        const bool valid = idx < P;
+        k[i] = valid ? keys[idx] : (K)0;
+        K prev = __shfl_up_sync(0xffffffffu, k[i], 1);
+        if (lane == 0)
+            prev = carry;
+        carry = __shfl_sync(0xffffffffu, k[i], 31);
+        const bool first = idx == 0;
+        const bool hv = valid && (first || k[i] != prev);
+        const bool hl = valid && (first || (k[i] >> 9) != (prev >> 9));
+        const bool hlo = valid && (first || (k[i] >> 21) != (prev >> 21));
+        bv[i] = __ballot_sync(0xffffffffu, hv);
+        bl[i] = __ballot_sync(0xffffffffu, hl);
+        blo[i] = __ballot_sync(0xffffffffu, hlo);
+        tv += __popc(bv[i]);
+        tl += __popc(bl[i]);
+        tlo += __popc(blo[i]);
     }
-    uint64_t tv, tl, tlo;
-    uint64_t ev = block_excl_scan_u64(cv, s_warp, tv);
-    uint64_t el = block_excl_scan_u64(cl, s_warp, tl);
-    uint64_t elo = block_excl_scan_u64(clo, s_warp, tlo);
+    if (lane == 0)
+    {
+        s_wtot[0][warp] = tv;
+        s_wtot[1][warp] = tl;
+        s_wtot[2][warp] = tlo;
+    }
+    __syncthreads();
     if (threadIdx.x < 3)
     {
-        uint64_t agg = threadIdx.x == 0 ? tv : (threadIdx.x == 1 ? tl : tlo);
+        uint64_t agg = 0;
+        for (int w = 0; w < RUN_WARPS; w++)
+            agg += s_wtot[threadIdx.x][w];
         s_ex[threadIdx.x] = lookback_exclusive(Rp.status + threadIdx.x, tile, agg, Rp.epoch, Rp.err, 3);
     }
     __syncthreads();
-    uint64_t v = s_ex[0] + ev, l = s_ex[1] + el, lo = s_ex[2] + elo;
-#pragma unroll
-    for (int t = 0; t < RUN_ITEMS; t++)
+    uint64_t v = s_ex[0], l = s_ex[1], lo = s_ex[2];
+    for (int w = 0; w < warp; w++)
     {
-        int64_t idx = base + t;
-        if (idx >= P)
-            break;
-        uint32_t f = fl[t];
-        if (f & 4u)
+        v += s_wtot[0][w];
+        l += s_wtot[1][w];
+        lo += s_wtot[2][w];
+    }
+    const uint32_t le = (lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1u);
+#pragma unroll
+    for (int i = 0; i < RUN_ITEMS; i++)
+    {
+        const int64_t idx = wbase + i * 32 + lane;
+        // inclusive counts at this element: heads up to and including it
+        const uint64_t vi = v + __popc(bv[i] & le), li = l + __popc(bl[i] & le), loi = lo + __popc(blo[i] & le);
+        if ((blo[i] >> lane) & 1u)
         {
             // distinct lower ranks never exceed the touched-cell count; more
             // heads mean the keys are not sorted: report, never write past it
-            if (lo + 1 < Rp.lower_cap)
+            if (loi < Rp.lower_cap)
             {
-                Rp.lower_lstart[lo] = (uint32_t)l;
-                Rp.lower_rank[lo] = (uint32_t)((uint64_t)keys[idx] >> 21);
+                Rp.lower_lstart[loi - 1] = (uint32_t)(li - 1);
+                Rp.lower_rank[loi - 1] = (uint32_t)((uint64_t)k[i] >> 21);
             }
             else
                 atomicOr(Rp.err, ERR_ORDER);
-            lo++;
         }
-        if (f & 2u)
+        if ((bl[i] >> lane) & 1u)
+            Rp.leaf_vstart[li - 1] = (uint32_t)(vi - 1);
+        if ((bv[i] >> lane) & 1u)
         {
-            Rp.leaf_vstart[l] = (uint32_t)v;
-            l++;
-        }
-        if (f & 1u)
-        {
-            Rp.vox_start[v] = (uint32_t)idx;
-            v++;
+            Rp.vox_start[vi - 1] = (uint32_t)idx;
+            Rp.vox_leaf[vi - 1] = (uint32_t)(li - 1);
+            Rp.vox_n[vi - 1] = (uint16_t)((uint32_t)k[i] & 511u);
         }
         if (idx == P - 1)
         {
-            Rp.vox_start[v] = (uint32_t)P;
-            Rp.leaf_vstart[l] = (uint32_t)v;
-            if (lo < Rp.lower_cap)
-                Rp.lower_lstart[lo] = (uint32_t)l;
-            Rp.counts[0] = v;
-            Rp.counts[1] = l;
-            Rp.counts[2] = lo;
+            Rp.vox_start[vi] = (uint32_t)P;
+            Rp.leaf_vstart[li] = (uint32_t)vi;
+            if (loi < Rp.lower_cap)
+                Rp.lower_lstart[loi] = (uint32_t)li;
+            Rp.counts[0] = vi;
+            Rp.counts[1] = li;
+            Rp.counts[2] = loi;
         }
+        v += __popc(bv[i]);
+        l += __popc(bl[i]);
+        lo += __popc(blo[i]);
     }
 }
 
@@ -379,6 +247,7 @@ __global__ void k_lower_info(NodeParams N)
     N.lower_origin[3 * lo + 1] = o[1];
     N.lower_origin[3 * lo + 2] = o[2];
     N.lower_upper_n[lo] = un;
+    N.rank_to_lower[N.lower_rank[lo]] = (uint32_t)lo;
     bool head = lo == 0 || (N.lower_cell[N.lower_rank[lo - 1]] >> 15) != rr;
     N.upper_head[lo] = head ? 1ull : 0ull;
 }
@@ -431,58 +300,59 @@ __global__ void k_canonical_order(NodeParams N, uint64_t U)
     }
 }
 
-// leaf value masks (+ bbox of active voxels, grid_build_compute_bbox.slang)
+// per leaf: lower_n in its parent and origin
 template <class K>
-__global__ void __launch_bounds__(256) k_leaf_masks(NodeParams N, const K* __restrict__ keys)
+__global__ void __launch_bounds__(256) k_leaf_info(NodeParams N, const K* __restrict__ keys)
 {
-    const int lane = threadIdx.x & 31;
-    int64_t l = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= N.L)
         return;
-    uint32_t v0 = N.leaf_vstart[l], v1 = N.leaf_vstart[l + 1];
-    uint64_t m[8] = { 0, 0, 0, 0, 0, 0, 0, 0 };
-    int32_t mn[3] = { 8, 8, 8 }, mx[3] = { -1, -1, -1 };
-    K key0 = keys[N.vox_start[v0]];
-    for (uint32_t v = v0 + lane; v < v1; v += 32)
+    const K key0 = keys[N.vox_start[N.leaf_vstart[l]]];
+    const uint32_t ln = (uint32_t)((uint64_t)key0 >> 9) & 4095u;
+    const uint32_t lo = N.leaf_lower[l];
+    N.leaf_lower_n[l] = ln;
+    N.leaf_origin[3 * l + 0] = N.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8;
+    N.leaf_origin[3 * l + 1] = N.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8;
+    N.leaf_origin[3 * l + 2] = N.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8;
+}
+
+// bbox of the active voxels from the leaf masks (grid_build_compute_bbox.slang)
+__global__ void __launch_bounds__(256) k_leaf_bbox(NodeParams N)
+{
+    __shared__ int32_t s_bb[6];
+    if (threadIdx.x < 6)
+        s_bb[threadIdx.x] = threadIdx.x < 3 ? 0x7FFFFFFF : (int32_t)0x80000000;
+    __syncthreads();
+    int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < N.L)
     {
-        uint32_t n = (uint32_t)keys[N.vox_start[v]] & 511u;
-        m[n >> 6] |= 1ull << (n & 63);
-        int32_t c[3] = { (int32_t)(n >> 6), (int32_t)((n >> 3) & 7), (int32_t)(n & 7) };
+        int32_t mn[3] = { 8, 8, 8 }, mx[3] = { -1, -1, -1 };
+        for (int w = 0; w < 8; w++)
+        {
+            uint64_t m = N.leaf_mask[8 * l + w];
+            while (m)
+            {
+                int n = w * 64 + __ffsll((long long)m) - 1;
+                m &= m - 1;
+                int32_t c[3] = { n >> 6, (n >> 3) & 7, n & 7 };
+                for (int a = 0; a < 3; a++)
+                {
+                    mn[a] = min(mn[a], c[a]);
+                    mx[a] = max(mx[a], c[a]);
+                }
+            }
+        }
         for (int a = 0; a < 3; a++)
         {
-            mn[a] = min(mn[a], c[a]);
-            mx[a] = max(mx[a], c[a]);
+            atomicMin(&s_bb[a], N.leaf_origin[3 * l + a] + mn[a]);
+            atomicMax(&s_bb[3 + a], N.leaf_origin[3 * l + a] + mx[a]);
         }
     }
-#pragma unroll
-    for (int w = 0; w < 8; w++)
-        for (int o = 16; o > 0; o >>= 1)
-            m[w] |= __shfl_xor_sync(0xffffffffu, m[w], o);
-    for (int a = 0; a < 3; a++)
-        for (int o = 16; o > 0; o >>= 1)
-        {
-            mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
-            mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
-        }
-    if (lane < 8)
-        N.leaf_mask[8 * l + lane] = m[lane];
-    if (lane == 0)
-    {
-        // leaf origin from its lower node and lower_n
-        uint32_t ln = (uint32_t)((uint64_t)key0 >> 9) & 4095u;
-        uint32_t lo = N.leaf_lower[l];
-        int32_t o[3] = { N.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8,
-                         N.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8,
-                         N.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8 };
-        N.leaf_origin[3 * l + 0] = o[0];
-        N.leaf_origin[3 * l + 1] = o[1];
-        N.leaf_origin[3 * l + 2] = o[2];
-        for (int a = 0; a < 3; a++)
-        {
-            atomicMin(&N.bbox[a], o[a] + mn[a]);
-            atomicMax(&N.bbox[3 + a], o[a] + mx[a]);
-        }
-    }
+    __syncthreads();
+    if (threadIdx.x < 3)
+        atomicMin(&N.bbox[threadIdx.x], s_bb[threadIdx.x]);
+    else if (threadIdx.x < 6)
+        atomicMax(&N.bbox[threadIdx.x], s_bb[threadIdx.x]);
 }
 
 // leaf -> lower index (leaves of lower lo are [lower_lstart[lo], lower_lstart[lo+1]))
@@ -669,66 +539,114 @@ __global__ void __launch_bounds__(256) k_write_leaf(NodeParams N, uint8_t* node2
     ((uint64_t*)(node2 + N.leaf_addr[l]))[w] = val;
 }
 
-__global__ void k_leaf_lower_n(NodeParams N, const void* keys_v, int key64)
-{
-    int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= N.L)
-        return;
-    uint64_t key = key64 ? ((const uint64_t*)keys_v)[N.vox_start[N.leaf_vstart[l]]]
-                         : (uint64_t)((const uint32_t*)keys_v)[N.vox_start[N.leaf_vstart[l]]];
-    N.leaf_lower_n[l] = (uint32_t)(key >> 9) & 4095u;
-}
-
 // ------------------------------------------------------------- accumulate ----
-// one warp per leaf, one lane per voxel; each lane walks its voxel's pairs in
-// (key, id) order so the float sums have a fixed sequential order
-template <class K>
-__global__ void __launch_bounds__(256) k_accumulate(AccumParams A, NodeParams N, const uint32_t* __restrict__ ids)
+// A CTA owns 256 consecutive voxels (one per thread) and walks their pairs,
+// which are contiguous in the sorted array, in chunks: every thread computes
+// the alpha of one pair at a time (balanced across lanes) into shared memory,
+// then each voxel's thread sums its own pairs sequentially in (key, id)
+// order, so the float sums have the same fixed order as a serial loop.  The
+// voxel's bit is set in its leaf mask on the way.
+constexpr int ACC_BLOCK = 256;
+constexpr int ACC_CHUNK = 2048;
+
+struct AccSmem
 {
-    const int lane = threadIdx.x & 31;
-    int64_t l = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (l >= N.L)
+    float a[ACC_CHUNK];
+    float ar[ACC_CHUNK], ag[ACC_CHUNK], ab[ACC_CHUNK];
+    uint32_t rgba[ACC_CHUNK];
+    uint32_t vstart[ACC_BLOCK + 1];
+};
+
+template <class K>
+__global__ void __launch_bounds__(ACC_BLOCK) k_accumulate(AccumParams A, NodeParams N, const uint32_t* __restrict__ ids)
+{
+    __shared__ AccSmem S;
+    const int64_t v0 = (int64_t)blockIdx.x * ACC_BLOCK;
+    const int64_t V = A.V;
+    if (v0 >= V)
         return;
-    const uint32_t v0 = N.leaf_vstart[l], v1 = N.leaf_vstart[l + 1];
-    const int32_t ox = N.leaf_origin[3 * l + 0], oy = N.leaf_origin[3 * l + 1], oz = N.leaf_origin[3 * l + 2];
-    const uint64_t vbase = N.leaf_vidx[l];
+    const int64_t nv = min((int64_t)ACC_BLOCK, V - v0);
+    for (int t = threadIdx.x; t <= nv; t += ACC_BLOCK)
+        S.vstart[t] = N.vox_start[v0 + t];
+    __syncthreads();
+    const uint32_t pa = S.vstart[0], pb = S.vstart[nv];
     const K* keys = (const K*)A.keys;
-    for (uint32_t v = v0 + lane; v < v1; v += 32)
+    const int t = threadIdx.x;
+    const bool mine = t < nv;
+    const uint32_t my0 = mine ? S.vstart[t] : 0u, my1 = mine ? S.vstart[t + 1] : 0u;
+    uint32_t rgba = 0;
+    float dsum = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    for (uint32_t pc = pa; pc < pb; pc += ACC_CHUNK)
     {
-        const uint32_t p0 = N.vox_start[v], p1 = N.vox_start[v + 1];
-        const uint32_t n = (uint32_t)keys[p0] & 511u;
-        const int32_t x = ox + (int32_t)(n >> 6), y = oy + (int32_t)((n >> 3) & 7), z = oz + (int32_t)(n & 7);
-        uint32_t rgba = 0;
-        float dsum = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-        for (uint32_t p = p0; p < p1; p++)
+        const uint32_t len = min((uint32_t)ACC_CHUNK, pb - pc);
+        for (uint32_t e = threadIdx.x; e < len; e += ACC_BLOCK)
         {
+            const uint32_t p = pc + e;
+            const uint64_t key = (uint64_t)keys[p];
+            const uint32_t lo = A.rank_to_lower[key >> 21];
+            const uint32_t ln = (uint32_t)(key >> 9) & 4095u, vn = (uint32_t)key & 511u;
+            const int32_t x = N.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8 + (int32_t)(vn >> 6);
+            const int32_t y = N.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8 + (int32_t)((vn >> 3) & 7);
+            const int32_t z = N.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8 + (int32_t)(vn & 7);
             const GaussRec R = A.recs[ids[p]];
             const RInv M = rinv_of(R);
-            Aabb b = voxel_local_aabb(R, M, A.voxel_size, x, y, z);
-            float a = pair_alpha(R, b);
-            uint32_t c = pack_rgba8(R, a);
-            rgba = c > rgba ? c : rgba;
-            dsum = VOX_FADD(dsum, a);
-            c0 = VOX_FADD(c0, VOX_FMUL(a, R.q7.x));
-            c1 = VOX_FADD(c1, VOX_FMUL(a, R.q7.y));
-            c2 = VOX_FADD(c2, VOX_FMUL(a, R.q7.z));
+            const float vs = A.voxel_size;
+            float cx0, cx1, cy0, cy1, cz0, cz1;
+            axis_corners(vs, R.q0.x, x, cx0, cx1);
+            axis_corners(vs, R.q0.y, y, cy0, cy1);
+            axis_corners(vs, R.q0.z, z, cz0, cz1);
+            const float a8 = pair_alpha(R, aabb_from_corners(R, M, cx0, cx1, cy0, cy1, cz0, cz1));
+            // float channels: corner offsets rounded once from double
+            float sx0, sx1, sy0, sy1, sz0, sz1;
+            axis_corners_stable(vs, R.q0.x, x, sx0, sx1);
+            axis_corners_stable(vs, R.q0.y, y, sy0, sy1);
+            axis_corners_stable(vs, R.q0.z, z, sz0, sz1);
+            const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
+            const float a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
+            S.a[e] = a;
+            S.ar[e] = VOX_FMUL(a, R.q7.x);
+            S.ag[e] = VOX_FMUL(a, R.q7.y);
+            S.ab[e] = VOX_FMUL(a, R.q7.z);
+            S.rgba[e] = pack_rgba8(R, a8);
         }
-        const uint64_t vi = vbase + (v - v0);
+        __syncthreads();
+        if (mine)
+        {
+            const uint32_t q0 = max(my0, pc), q1 = min(my1, pc + len);
+            for (uint32_t p = q0; p < q1; p++)
+            {
+                const uint32_t e = p - pc;
+                rgba = S.rgba[e] > rgba ? S.rgba[e] : rgba;
+                dsum = VOX_FADD(dsum, S.a[e]);
+                c0 = VOX_FADD(c0, S.ar[e]);
+                c1 = VOX_FADD(c1, S.ag[e]);
+                c2 = VOX_FADD(c2, S.ab[e]);
+            }
+        }
+        __syncthreads();
+    }
+    if (mine)
+    {
+        const int64_t v = v0 + t;
+        const uint32_t l = A.vox_leaf[v];
+        const uint32_t n = A.vox_n[v];
+        const uint64_t vi = N.leaf_vidx[l] + (uint64_t)(v - N.leaf_vstart[l]);
         A.rgba8[vi] = rgba;
         A.density[vi] = dsum;
         A.color[3 * vi + 0] = dsum > 0.f ? VOX_FDIV(c0, dsum) : 0.f;
         A.color[3 * vi + 1] = dsum > 0.f ? VOX_FDIV(c1, dsum) : 0.f;
         A.color[3 * vi + 2] = dsum > 0.f ? VOX_FDIV(c2, dsum) : 0.f;
+        atomicOr((unsigned long long*)&N.leaf_mask[8 * (uint64_t)l + (n >> 6)], 1ull << (n & 63));
     }
 }
 
 // =================================================================== launch
-void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* root_bits, int* err,
-                 cudaStream_t s)
+void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* columns, uint64_t* root_bits,
+                 int* err, cudaStream_t s)
 {
     if (P.count <= 0)
         return;
-    { k_prep<<<(unsigned)((P.count + 255) / 256), 256, 0, s>>>(P, recs, footprints, (unsigned long long*)root_bits, err); count_launch(); }
+    { k_prep<<<(unsigned)((P.count + 255) / 256), 256, 0, s>>>(P, recs, footprints, columns, (unsigned long long*)root_bits, err); count_launch(); }
 }
 
 void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits, const uint64_t* root_prefix,
@@ -747,42 +665,6 @@ void launch_invert_bits(const uint64_t* bits, const uint64_t* prefix, int64_t wo
     { k_invert_bits<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(bits, prefix, words, out); count_launch(); }
 }
 
-template <class K>
-static void launch_emit_t(const EmitParams& E, const RankTables& T, K* out_k, uint32_t* out_i, int num_sms,
-                          cudaStream_t s)
-{
-    if (E.F == 0)
-    {
-        cudaMemsetAsync(E.total, 0, sizeof(uint64_t), s);
-        return;
-    }
-    const size_t smem = sizeof(EmitSmem<K>);
-    cudaFuncSetAttribute(k_emit<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_emit<K>, EMIT_BLOCK, smem);
-    if (per_sm < 1)
-        per_sm = 1;
-    int64_t tiles = (int64_t)((E.F + EMIT_TILE - 1) / EMIT_TILE);
-    int64_t grid = (int64_t)num_sms * per_sm;
-    if (grid > tiles)
-        grid = tiles;
-    cudaMemsetAsync(E.counter, 0, sizeof(uint32_t), s);
-    { k_emit<K><<<(unsigned)grid, EMIT_BLOCK, smem, s>>>(E, T, out_k, out_i); count_launch(); }
-}
-void launch_emit_u32(const EmitParams& E, const RankTables& T, uint32_t* out_k, uint32_t* out_i, int num_sms,
-                     cudaStream_t s)
-{
-    launch_emit_t<uint32_t>(E, T, out_k, out_i, num_sms, s);
-}
-void launch_emit_u64(const EmitParams& E, const RankTables& T, uint64_t* out_k, uint32_t* out_i, int num_sms,
-                     cudaStream_t s)
-{
-    launch_emit_t<uint64_t>(E, T, out_k, out_i, num_sms, s);
-}
-int64_t emit_tile_count(uint64_t F)
-{
-    return (int64_t)((F + EMIT_TILE - 1) / EMIT_TILE);
-}
 
 void launch_runs(const RunParams& Rp, const void* keys, int key64, cudaStream_t s)
 {
@@ -817,12 +699,17 @@ void launch_leaf_tables(const NodeParams& N, const void* keys, int key64, cudaSt
     if (N.L <= 0)
         return;
     { k_leaf_lower<<<(unsigned)((N.Lo + 255) / 256), 256, 0, s>>>(N); count_launch(); }
-    { k_leaf_lower_n<<<(unsigned)((N.L + 255) / 256), 256, 0, s>>>(N, keys, key64); count_launch(); }
-    unsigned blocks = (unsigned)((N.L * 32 + 255) / 256);
+    unsigned blocks = (unsigned)((N.L + 255) / 256);
     if (key64)
-        { k_leaf_masks<uint64_t><<<blocks, 256, 0, s>>>(N, (const uint64_t*)keys); count_launch(); }
+        { k_leaf_info<uint64_t><<<blocks, 256, 0, s>>>(N, (const uint64_t*)keys); count_launch(); }
     else
-        { k_leaf_masks<uint32_t><<<blocks, 256, 0, s>>>(N, (const uint32_t*)keys); count_launch(); }
+        { k_leaf_info<uint32_t><<<blocks, 256, 0, s>>>(N, (const uint32_t*)keys); count_launch(); }
+}
+void launch_leaf_bbox(const NodeParams& N, cudaStream_t s)
+{
+    if (N.L <= 0)
+        return;
+    { k_leaf_bbox<<<(unsigned)((N.L + 255) / 256), 256, 0, s>>>(N); count_launch(); }
 }
 void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s)
 {
@@ -847,13 +734,13 @@ void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* node2, cudaStr
 }
 void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s)
 {
-    if (N.L <= 0)
+    if (A.V <= 0)
         return;
-    unsigned blocks = (unsigned)((N.L * 32 + 255) / 256);
+    unsigned blocks = (unsigned)((A.V + ACC_BLOCK - 1) / ACC_BLOCK);
     if (key64)
-        { k_accumulate<uint64_t><<<blocks, 256, 0, s>>>(A, N, ids); count_launch(); }
+        { k_accumulate<uint64_t><<<blocks, ACC_BLOCK, 0, s>>>(A, N, ids); count_launch(); }
     else
-        { k_accumulate<uint32_t><<<blocks, 256, 0, s>>>(A, N, ids); count_launch(); }
+        { k_accumulate<uint32_t><<<blocks, ACC_BLOCK, 0, s>>>(A, N, ids); count_launch(); }
 }
 
 } // namespace vox

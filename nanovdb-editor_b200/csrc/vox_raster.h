@@ -20,9 +20,9 @@ struct RankTables
 struct EmitParams
 {
     const GaussRec* recs;
-    const uint64_t* frag_off; // exclusive scan of footprints
+    const uint64_t* col_off; // exclusive scan of per-Gaussian column counts (bbox range x * range y)
     int64_t G;
-    uint64_t F;
+    uint64_t NC;             // total columns
     float voxel_size;
     uint64_t cap;
     uint64_t* status;
@@ -30,6 +30,7 @@ struct EmitParams
     uint32_t* counter;
     uint64_t* total;
     int* err;
+    int check; // also test the candidates the column bound skips (validation)
 };
 
 struct RunParams
@@ -45,6 +46,8 @@ struct RunParams
     uint32_t* counter;
     int* err;
     uint64_t lower_cap;     // entries of lower_lstart / lower_rank (heads beyond it are an error)
+    uint32_t* vox_leaf;     // [V] leaf index of each voxel
+    uint16_t* vox_n;        // [V] leaf_n (position in the leaf) of each voxel
 };
 
 struct NodeParams
@@ -58,6 +61,7 @@ struct NodeParams
     const uint32_t* vox_start;
     int32_t* lower_origin;
     uint32_t* lower_upper_n;
+    uint32_t* rank_to_lower; // [touched lower cells] lower rank -> lower node index
     uint64_t* upper_head;
     uint64_t* upper_scan;
     uint32_t* lower_parent;
@@ -79,13 +83,17 @@ struct AccumParams
     const GaussRec* recs;
     const void* keys;
     float voxel_size;
+    int64_t V;
+    const uint32_t* rank_to_lower; // lower rank -> lower node index
+    const uint32_t* vox_leaf;
+    const uint16_t* vox_n;
     uint32_t* rgba8;
     float* density;
     float* color;
 };
 
-void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* root_bits, int* err,
-                 cudaStream_t s);
+void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* columns, uint64_t* root_bits,
+                 int* err, cudaStream_t s);
 void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits, const uint64_t* root_prefix,
                        uint64_t* lower_bits, cudaStream_t s);
 void launch_invert_bits(const uint64_t* bits, const uint64_t* prefix, int64_t words, uint32_t* out, cudaStream_t s);
@@ -93,12 +101,13 @@ void launch_emit_u32(const EmitParams& E, const RankTables& T, uint32_t* out_k, 
                      cudaStream_t s);
 void launch_emit_u64(const EmitParams& E, const RankTables& T, uint64_t* out_k, uint32_t* out_i, int num_sms,
                      cudaStream_t s);
-int64_t emit_tile_count(uint64_t F);
+int64_t emit_tile_count(uint64_t NC);
 void launch_runs(const RunParams& Rp, const void* keys, int key64, cudaStream_t s);
 int64_t runs_tile_count(int64_t P);
 void launch_lower_info(const NodeParams& N, cudaStream_t s);
 void launch_upper_info(const NodeParams& N, cudaStream_t s);
 void launch_leaf_tables(const NodeParams& N, const void* keys, int key64, cudaStream_t s);
+void launch_leaf_bbox(const NodeParams& N, cudaStream_t s);
 void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s);
 void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* node2, cudaStream_t s);
 void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s);

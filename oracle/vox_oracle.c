@@ -207,7 +207,16 @@ static void prim_setup(prim_t* P, const float* mean, const float* quat_wxyz, con
 }
 
 /* gaussian_frag_alloc.slang:84-162: returns 1 when dist2 > 0 */
+/* stable = 1: corner offsets v * vs - mu computed in double and rounded once
+ * (used for the float density / colour channels only, not the reference test) */
+static int frag_test_ex(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float* vmin,
+                        float* vmax, int stable);
 static int frag_test(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float* vmin, float* vmax)
+{
+    return frag_test_ex(P, rinv, vs, ijk, vmin, vmax, 0);
+}
+static int frag_test_ex(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float* vmin,
+                        float* vmax, int stable)
 {
     float inv_ls = VOX_FDIV(1.f, P->ls);
     float inv_s[3] = { VOX_FDIV(1.f, P->s[0]), VOX_FDIV(1.f, P->s[1]), VOX_FDIV(1.f, P->s[2]) };
@@ -222,7 +231,8 @@ static int frag_test(const prim_t* P, const float rinv[3][3], float vs, const in
             vp[2] = VOX_FADD(vp[2], 1.f);
         float lp[3];
         for (int a = 0; a < 3; a++)
-            lp[a] = VOX_FSUB(VOX_FMUL(vp[a], vs), P->pos[a]);
+            lp[a] = stable ? (float)((double)vp[a] * (double)vs - (double)P->pos[a])
+                           : VOX_FSUB(VOX_FMUL(vp[a], vs), P->pos[a]);
         float l[3] = { dot3(lp, rinv[0]), dot3(lp, rinv[1]), dot3(lp, rinv[2]) };
         for (int a = 0; a < 3; a++)
         {
@@ -646,8 +656,12 @@ static void* values_worker(void* arg)
             float rinv[3][3], vmin[3], vmax[3], a;
             rot_inv_rows(P->q, rinv);
             frag_test(P, rinv, S->vs, ijk, vmin, vmax);
-            uint32_t c = frag_rgba(P, S->vs, S->cull, vmin, vmax, &a);
+            float a8;
+            uint32_t c = frag_rgba(P, S->vs, S->cull, vmin, vmax, &a8);
             rgba = c > rgba ? c : rgba; /* InterlockedMax, :239-246 */
+            /* float channels: the same alpha from corner offsets rounded once from double */
+            frag_test_ex(P, rinv, S->vs, ijk, vmin, vmax, 1);
+            frag_rgba(P, S->vs, S->cull, vmin, vmax, &a);
             dsum = VOX_FADD(dsum, a);
             for (int ch = 0; ch < 3; ch++)
                 csum[ch] = VOX_FADD(csum[ch], VOX_FMUL(a, P->rgb[ch]));

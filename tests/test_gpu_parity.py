@@ -104,3 +104,49 @@ def test_out_of_range_rejected(vox_ctx):
 def test_cull_scale_parameter(vox_ctx, oracle_mod):
     cloud = W.plain_cloud(2000, 8)
     _check(vox_ctx, oracle_mod, cloud, 0.01, cull=0.02)
+
+
+def test_far_from_origin(vox_ctx, oracle_mod):
+    # coordinates near the root-key limit: v * vs rounds coarsely in float
+    cloud = W.plain_cloud(3000, 9)
+    cloud["means"] += np.float32(640.0)
+    _check(vox_ctx, oracle_mod, cloud, 0.01)
+
+
+def test_needles_and_discs(vox_ctx, oracle_mod):
+    cloud = W.plain_cloud(3000, 10)
+    cloud["scales"][:1000, 0] *= 40.0  # needles
+    cloud["scales"][1000:2000, :2] *= 15.0  # discs
+    cloud["scales"][2000:, :] *= 0.05  # below the voxel/8 clamp
+    _check(vox_ctx, oracle_mod, cloud, 0.01)
+
+
+def test_column_bound_never_skips_a_passing_voxel(oracle_mod):
+    """VOX_CHECK_EMIT=1 also tests every candidate the per-column bound skips
+    and fails the call if one of them passes the reference test."""
+    import os
+
+    from nanovdb_editor.vox import VoxContext
+
+    os.environ["VOX_CHECK_EMIT"] = "1"
+    try:
+        ctx = VoxContext(0)
+    finally:
+        del os.environ["VOX_CHECK_EMIT"]
+    try:
+        clouds = [
+            (W.plain_cloud(20_000, 12), 0.01),
+            (W.cluster_cloud(50_000, 13, clusters=16), 0.002),
+            (W.pytest_cloud(), 1.0 / 8.0),
+        ]
+        far = W.plain_cloud(5000, 14)
+        far["means"] -= np.float32(600.0)
+        clouds.append((far, 0.01))
+        needles = W.plain_cloud(5000, 15)
+        needles["scales"][:, 2] *= 20.0
+        clouds.append((needles, 0.01))
+        for cloud, vs in clouds:
+            g = ctx.voxelize_host(cloud["means"], cloud["quats"], cloud["scales"], cloud["opacities"], cloud["colors"], vs)
+            assert g.counts["pairs"] > 0
+    finally:
+        ctx.close()
