@@ -264,6 +264,11 @@ typedef struct vox_context_t vox_context_t;
 /* flags for vox_voxelize */
 #define VOX_FLAG_RAW_INPUTS 1u     /* log scales, logit opacities, raw quaternions, SH0 colours */
 #define VOX_FLAG_WINDOW_ORDER 2u   /* node_idx order of the reference's fragment windows */
+/* differentiable channels: density = sum over the pairs of
+ * K = max(op exp(-|S^-1 R^T (x - mu)|^2 / 2) - 0.01, 0) at the voxel centre x,
+ * colour = sum K rgb (premultiplied); RGBA8 stays the reference's
+ * (gaussian_frag_color.slang:182-246).  Keeps what vox_backward needs. */
+#define VOX_FLAG_DIFFERENTIABLE 4u
 
 /* status codes */
 #define VOX_OK 0
@@ -293,6 +298,8 @@ typedef struct vox_stats_t
     int32_t sort_passes;
     float ms_prep, ms_emit, ms_sort, ms_build, ms_accumulate, ms_total;
     int64_t kernel_launches; /* kernels this library launched in the call */
+    float ms_backward;       /* last vox_backward */
+    int32_t reserved0;
 } vox_stats_t;
 
 /* One context per caller thread; it owns a CUDA stream on `device` and a
@@ -316,7 +323,7 @@ PNANOVDB_API int vox_voxelize_host(vox_context_t* ctx, const vox_gaussians_t* ga
                                    uint64_t* grid_bytes);
 
 /* Copies the grid of the last vox_voxelize / vox_voxelize_host call to host
- * memory (`capacity` bytes). */
+ * or device memory (`capacity` bytes). */
 PNANOVDB_API int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity);
 
 /* Sorted (voxel, Gaussian) pairs of the last vox_voxelize call: hierarchical
@@ -325,6 +332,23 @@ PNANOVDB_API int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity)
 PNANOVDB_API int vox_copy_pairs(vox_context_t* ctx, uint64_t* keys, uint32_t* ids, int64_t capacity);
 
 PNANOVDB_API void vox_get_stats(vox_context_t* ctx, vox_stats_t* out);
+
+/* Coordinates (i, j, k) of the active voxels of the last grid, row r for value
+ * index r + 2, written to DEVICE memory d_ijk [capacity][3] (capacity >= V). */
+PNANOVDB_API int vox_voxel_coords(vox_context_t* ctx, int32_t* d_ijk, int64_t capacity);
+
+/* Adjoint of the differentiable channels of the context's last call, which
+ * must have been a successful vox_voxelize with VOX_FLAG_DIFFERENTIABLE (the
+ * reference has no adjoint; this differentiates the forward above).
+ * `gaussians`: the forward's inputs (device).  grad_density [value_count] and
+ * grad_color [value_count][3] are dL/d channel, indexed like the grid's
+ * channels (either may be NULL = zero).  Outputs (device, any may be NULL):
+ * dL/d means [n][3], quats [n][4] (w, x, y, z), scales [n][3], opacities [n],
+ * colors [n][3], with respect to the inputs as given (with VOX_FLAG_RAW_INPUTS:
+ * the raw quaternion before normalisation, log scales, opacity logits, SH0). */
+PNANOVDB_API int vox_backward(vox_context_t* ctx, const vox_gaussians_t* gaussians, const float* grad_density,
+                              const float* grad_color, float* grad_means, float* grad_quats, float* grad_scales,
+                              float* grad_opacities, float* grad_colors);
 
 /* ---------------------------------------------------- parallel primitives --
  * The primitives the path is built on, on device pointers, ordered on the

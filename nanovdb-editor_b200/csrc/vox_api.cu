@@ -57,6 +57,7 @@ struct vox_context_t
     DevBuf lower_origin, lower_upper_n, upper_head, upper_scan, lower_parent, upper_root_n, upper_lostart;
     DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
     DevBuf vox_leaf, vox_n, rank_to_lower;
+    DevBuf emit_keys, emit_ids, leaf_slot, bwd_acc; // differentiable calls
     DevBuf order; // 9 node order arrays
     DevBuf grid;
     DevBuf scal; // device scalars
@@ -75,6 +76,14 @@ struct vox_context_t
     // last result
     int64_t last_P = 0;
     uint64_t last_grid_bytes = 0;
+    // state the adjoint of the last differentiable call reads
+    bool diff_ready = false;
+    int64_t last_G = 0;
+    int64_t last_V = -1; // -1: no successful call yet
+    uint64_t last_value_count = 0;
+    uint32_t last_flags = 0;
+    float last_voxel_size = 0.f;
+    NodeParams last_N{};
 };
 
 // device scalar slots (u64 each)
@@ -211,6 +220,9 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         set_error(ctx, "vox_voxelize: reference window node order is not available in this build");
         return VOX_ERR_ARGS;
     }
+    ctx->diff_ready = false;
+    ctx->last_V = -1;
+    const bool diff = (flags & VOX_FLAG_DIFFERENTIABLE) != 0;
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     const int64_t G = gs->count;
@@ -354,6 +366,14 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     ctx->pair_cap = cap;
     ctx->stats.pairs = P_pairs;
     ctx->last_P = P_pairs;
+    if (diff)
+    {
+        // the adjoint walks the pairs in emission order (sorted by Gaussian id)
+        if (!ensure(ctx, ctx->emit_keys, kb * (size_t)(P_pairs + 1)) || !ensure(ctx, ctx->emit_ids, 4 * (size_t)(P_pairs + 1)))
+            return VOX_ERR_MEMORY;
+        cudaMemcpyAsync(ctx->emit_keys.p, ctx->keys.p, kb * (size_t)P_pairs, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(ctx->emit_ids.p, ctx->ids.p, 4 * (size_t)P_pairs, cudaMemcpyDeviceToDevice, s);
+    }
     cudaEventRecord(ctx->timers.ev[2], s);
 
     // ---------------------------------------------------------------- sort
@@ -432,6 +452,8 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         !ensure(ctx, ctx->order, 8 * 3 * (size_t)((Lo + 1) * 2 + (L + 1))) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(Lo + 1) * 2))
         return VOX_ERR_MEMORY;
+    if (diff && !ensure(ctx, ctx->leaf_slot, 4 * 4096 * (size_t)(Lo + 1)))
+        return VOX_ERR_MEMORY;
     scan_status = (uint64_t*)ctx->scan_status.p;
     scan_words = ctx->scan_status.cap / sizeof(uint64_t);
     NodeParams N;
@@ -454,6 +476,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     N.upper_count = sc + SC_U;
     N.leaf_lower = (uint32_t*)ctx->leaf_lower.p;
     N.leaf_lower_n = (uint32_t*)ctx->leaf_lower_n.p;
+    N.leaf_slot = diff ? (uint32_t*)ctx->leaf_slot.p : nullptr;
     N.leaf_mask = (uint64_t*)ctx->leaf_mask.p;
     N.leaf_origin = (int32_t*)ctx->leaf_origin.p;
     N.bbox = (int32_t*)(sc + SC_BBOX);
@@ -511,6 +534,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     A.rgba8 = (uint32_t*)(grid + off_rgba);
     A.density = (float*)(grid + off_dens);
     A.color = (float*)(grid + off_col);
+    A.smooth = diff ? 1 : 0;
     launch_accumulate(A, N, sids, key64, s);
     cudaEventRecord(ctx->timers.ev[5], s);
     launch_leaf_bbox(N, s);
@@ -567,7 +591,107 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     st.ms_accumulate = elapsed(ctx->timers.ev[4], ctx->timers.ev[5]);
     st.ms_total = elapsed(ctx->timers.ev[0], ctx->timers.ev[6]);
     st.kernel_launches = launch_count() - launches0;
+    ctx->last_G = G;
+    ctx->last_V = V;
+    ctx->last_value_count = value_count;
+    ctx->last_flags = flags;
+    ctx->last_voxel_size = voxel_size;
+    ctx->last_N = N;
+    ctx->diff_ready = diff;
     return VOX_OK;
+}
+
+static int run_backward(vox_context_t* ctx, const vox_gaussians_t* gs, const float* grad_density,
+                        const float* grad_color, float* d_means, float* d_quats, float* d_scales, float* d_opacities,
+                        float* d_colors)
+{
+    if (!ctx || !gs)
+    {
+        set_error(ctx, "vox_backward: invalid arguments");
+        return VOX_ERR_ARGS;
+    }
+    if (!ctx->diff_ready)
+    {
+        set_error(ctx, "vox_backward: the context's last call was not a successful VOX_FLAG_DIFFERENTIABLE voxelization");
+        return VOX_ERR_ARGS;
+    }
+    if (gs->count != ctx->last_G)
+    {
+        set_error(ctx, "vox_backward: %lld Gaussians, the forward had %lld", (long long)gs->count, (long long)ctx->last_G);
+        return VOX_ERR_ARGS;
+    }
+    const int64_t G = gs->count;
+    if (G > 0 && (!gs->means || !gs->quats || !gs->scales || !gs->opacities || !gs->colors))
+    {
+        set_error(ctx, "vox_backward: missing attribute array");
+        return VOX_ERR_ARGS;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int64_t launches0 = launch_count();
+    if (!ensure(ctx, ctx->bwd_acc, sizeof(double) * BWD_NACC * (size_t)(G + 1)))
+        return VOX_ERR_MEMORY;
+    cudaEventRecord(ctx->timers.ev[0], s);
+    cudaMemsetAsync(ctx->bwd_acc.p, 0, sizeof(double) * BWD_NACC * (size_t)G, s);
+    cudaMemsetAsync((uint64_t*)ctx->scal.p + SC_ERR, 0, sizeof(uint64_t), s);
+    const NodeParams& N = ctx->last_N;
+    BwdParams B;
+    B.recs = (const GaussRec*)ctx->recs.p;
+    B.keys = ctx->emit_keys.p;
+    B.ids = (const uint32_t*)ctx->emit_ids.p;
+    B.P = ctx->last_P;
+    B.G = G;
+    B.rank_to_lower = N.rank_to_lower;
+    B.leaf_slot = N.leaf_slot;
+    B.leaf_vidx = N.leaf_vidx;
+    B.leaf_mask = N.leaf_mask;
+    B.lower_origin = N.lower_origin;
+    B.grad_density = grad_density;
+    B.grad_color = grad_color;
+    B.voxel_size = ctx->last_voxel_size;
+    B.acc = (double*)ctx->bwd_acc.p;
+    if (grad_density || grad_color)
+        launch_bwd_pairs(B, ctx->key64, s);
+    BwdFinalParams F;
+    F.acc = B.acc;
+    F.G = G;
+    F.means = gs->means;
+    F.quats = gs->quats;
+    F.scales = gs->scales;
+    F.opacities = gs->opacities;
+    F.colors = gs->colors;
+    F.raw = (ctx->last_flags & VOX_FLAG_RAW_INPUTS) ? 1 : 0;
+    F.voxel_size = ctx->last_voxel_size;
+    F.d_means = d_means;
+    F.d_quats = d_quats;
+    F.d_scales = d_scales;
+    F.d_opacities = d_opacities;
+    F.d_colors = d_colors;
+    launch_bwd_finalize(F, s);
+    cudaEventRecord(ctx->timers.ev[1], s);
+    int rc = sync_scalars(ctx, "backward");
+    if (rc)
+        return rc;
+    rc = check_cuda(ctx, "backward");
+    if (rc)
+        return rc;
+    ctx->stats.ms_backward = elapsed(ctx->timers.ev[0], ctx->timers.ev[1]);
+    ctx->stats.kernel_launches = launch_count() - launches0;
+    return VOX_OK;
+}
+
+// coordinates of the active voxels by value index (minus the 2 background slots)
+__global__ void k_voxel_coords(int64_t V, const uint32_t* vox_leaf, const uint16_t* vox_n, const int32_t* leaf_origin,
+                               const uint32_t* leaf_vstart, const uint64_t* leaf_vidx, int32_t* out)
+{
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V)
+        return;
+    const uint32_t l = vox_leaf[v], n = vox_n[v];
+    const uint64_t slot = leaf_vidx[l] + (uint64_t)(v - leaf_vstart[l]) - 2;
+    out[3 * slot + 0] = leaf_origin[3 * l + 0] + (int32_t)(n >> 6);
+    out[3 * slot + 1] = leaf_origin[3 * l + 1] + (int32_t)((n >> 3) & 7);
+    out[3 * slot + 2] = leaf_origin[3 * l + 2] + (int32_t)(n & 7);
 }
 
 // hierarchical key of a compact key: rank -> cell -> (root_n, upper_n)
@@ -657,6 +781,13 @@ const char* vox_last_error(vox_context_t* ctx)
     return ctx ? ctx->last_error.c_str() : "no context";
 }
 
+int vox_backward(vox_context_t* ctx, const vox_gaussians_t* gaussians, const float* grad_density, const float* grad_color,
+                 float* grad_means, float* grad_quats, float* grad_scales, float* grad_opacities, float* grad_colors)
+{
+    return run_backward(ctx, gaussians, grad_density, grad_color, grad_means, grad_quats, grad_scales, grad_opacities,
+                        grad_colors);
+}
+
 int vox_voxelize(vox_context_t* ctx, const vox_gaussians_t* gaussians, float voxel_size, float cull_scale,
                  uint32_t flags, void** grid, uint64_t* grid_bytes)
 {
@@ -723,9 +854,32 @@ int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity)
     if (capacity < ctx->last_grid_bytes)
         return VOX_ERR_SIZE;
     cudaSetDevice(ctx->device);
-    cudaMemcpyAsync(out, ctx->grid.p, ctx->last_grid_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    // host or device destination (unified addressing)
+    cudaMemcpyAsync(out, ctx->grid.p, ctx->last_grid_bytes, cudaMemcpyDefault, ctx->stream);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return check_cuda(ctx, "vox_copy_grid");
+    return VOX_OK;
+}
+
+int vox_voxel_coords(vox_context_t* ctx, int32_t* d_ijk, int64_t capacity)
+{
+    if (!ctx || (!d_ijk && capacity > 0))
+        return VOX_ERR_ARGS;
+    if (ctx->last_V < 0)
+    {
+        set_error(ctx, "vox_voxel_coords: no grid");
+        return VOX_ERR_ARGS;
+    }
+    const int64_t V = ctx->last_V;
+    if (capacity < V)
+        return VOX_ERR_SIZE;
+    if (V == 0)
+        return VOX_OK;
+    cudaSetDevice(ctx->device);
+    const NodeParams& N = ctx->last_N;
+    { k_voxel_coords<<<(unsigned)((V + 255) / 256), 256, 0, ctx->stream>>>(V, (const uint32_t*)ctx->vox_leaf.p, (const uint16_t*)ctx->vox_n.p, N.leaf_origin, N.leaf_vstart, N.leaf_vidx, d_ijk); count_launch(); }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return check_cuda(ctx, "vox_voxel_coords");
     return VOX_OK;
 }
 

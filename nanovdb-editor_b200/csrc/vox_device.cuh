@@ -423,6 +423,37 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
     return a;
 }
 
+// Differentiable channels (VOX_FLAG_DIFFERENTIABLE).  The reference alpha
+// (4^3-lattice maximum, opacity transform, cull) jumps where a voxel enters or
+// leaves the pair set, so these channels use the centre-sampled kernel
+//   K = max(op * exp(-|z|^2 / 2) - 0.01, 0),  z = S^-1 R^T (x - mu),
+// x the voxel centre, over the same pairs.  K vanishes on the 0.01-opacity
+// ellipsoid the pair test is built on (radius ls = sqrt(2 log(op / 0.01)),
+// gaussian_prim.slang:65), so the channels are continuous in every parameter.
+// Centre offsets are rounded once from double (stable far from the origin).
+constexpr float SMOOTH_TAU = 0.01f;
+struct SmoothTerms
+{
+    float d[3], z[3], E, e;
+};
+__device__ __forceinline__ float smooth_kernel(const GaussRec& R, const RInv& M, float vs, int32_t x, int32_t y,
+                                               int32_t z, SmoothTerms& t)
+{
+    const int32_t c[3] = { x, y, z };
+    const float mu[3] = { R.q0.x, R.q0.y, R.q0.z };
+    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+        t.d[a] = (float)VOX_DSUB(VOX_DMUL(VOX_DADD((double)c[a], 0.5), (double)vs), (double)mu[a]);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+        t.z[r] = VOX_FMUL(dot3_rn(t.d[0], t.d[1], t.d[2], M.m[r][0], M.m[r][1], M.m[r][2]), inv_s[r]);
+    const float q = dot3_rn(t.z[0], t.z[1], t.z[2], t.z[0], t.z[1], t.z[2]);
+    t.E = vox_expf_cr(VOX_FMUL(-0.5f, q));
+    t.e = VOX_FMUL(R.q6.x, t.E);
+    return t.e > SMOOTH_TAU ? VOX_FSUB(t.e, SMOOTH_TAU) : 0.f;
+}
+
 __device__ __forceinline__ uint32_t pack_rgba8(const GaussRec& R, float a)
 {
     float ch[4] = { R.q7.x, R.q7.y, R.q7.z, a };

@@ -311,6 +311,8 @@ __global__ void __launch_bounds__(256) k_leaf_info(NodeParams N, const K* __rest
     const uint32_t ln = (uint32_t)((uint64_t)key0 >> 9) & 4095u;
     const uint32_t lo = N.leaf_lower[l];
     N.leaf_lower_n[l] = ln;
+    if (N.leaf_slot)
+        N.leaf_slot[(uint64_t)lo * 4096u + ln] = (uint32_t)l;
     N.leaf_origin[3 * l + 0] = N.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8;
     N.leaf_origin[3 * l + 1] = N.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8;
     N.leaf_origin[3 * l + 2] = N.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8;
@@ -596,13 +598,22 @@ __global__ void __launch_bounds__(ACC_BLOCK) k_accumulate(AccumParams A, NodePar
             axis_corners(vs, R.q0.y, y, cy0, cy1);
             axis_corners(vs, R.q0.z, z, cz0, cz1);
             const float a8 = pair_alpha(R, aabb_from_corners(R, M, cx0, cx1, cy0, cy1, cz0, cz1));
-            // float channels: corner offsets rounded once from double
-            float sx0, sx1, sy0, sy1, sz0, sz1;
-            axis_corners_stable(vs, R.q0.x, x, sx0, sx1);
-            axis_corners_stable(vs, R.q0.y, y, sy0, sy1);
-            axis_corners_stable(vs, R.q0.z, z, sz0, sz1);
-            const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
-            const float a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
+            float a;
+            if (A.smooth)
+            {
+                SmoothTerms st;
+                a = smooth_kernel(R, M, vs, x, y, z, st);
+            }
+            else
+            {
+                // float channels: corner offsets rounded once from double
+                float sx0, sx1, sy0, sy1, sz0, sz1;
+                axis_corners_stable(vs, R.q0.x, x, sx0, sx1);
+                axis_corners_stable(vs, R.q0.y, y, sy0, sy1);
+                axis_corners_stable(vs, R.q0.z, z, sz0, sz1);
+                const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
+                a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
+            }
             S.a[e] = a;
             S.ar[e] = VOX_FMUL(a, R.q7.x);
             S.ag[e] = VOX_FMUL(a, R.q7.y);
@@ -633,9 +644,19 @@ __global__ void __launch_bounds__(ACC_BLOCK) k_accumulate(AccumParams A, NodePar
         const uint64_t vi = N.leaf_vidx[l] + (uint64_t)(v - N.leaf_vstart[l]);
         A.rgba8[vi] = rgba;
         A.density[vi] = dsum;
-        A.color[3 * vi + 0] = dsum > 0.f ? VOX_FDIV(c0, dsum) : 0.f;
-        A.color[3 * vi + 1] = dsum > 0.f ? VOX_FDIV(c1, dsum) : 0.f;
-        A.color[3 * vi + 2] = dsum > 0.f ? VOX_FDIV(c2, dsum) : 0.f;
+        if (A.smooth)
+        {
+            // premultiplied colour (linear in the per-pair weights)
+            A.color[3 * vi + 0] = c0;
+            A.color[3 * vi + 1] = c1;
+            A.color[3 * vi + 2] = c2;
+        }
+        else
+        {
+            A.color[3 * vi + 0] = dsum > 0.f ? VOX_FDIV(c0, dsum) : 0.f;
+            A.color[3 * vi + 1] = dsum > 0.f ? VOX_FDIV(c1, dsum) : 0.f;
+            A.color[3 * vi + 2] = dsum > 0.f ? VOX_FDIV(c2, dsum) : 0.f;
+        }
         atomicOr((unsigned long long*)&N.leaf_mask[8 * (uint64_t)l + (n >> 6)], 1ull << (n & 63));
     }
 }

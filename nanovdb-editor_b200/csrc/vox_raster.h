@@ -70,6 +70,7 @@ struct NodeParams
     uint64_t* upper_count;
     uint32_t* leaf_lower;
     uint32_t* leaf_lower_n;
+    uint32_t* leaf_slot; // optional [lower runs * 4096]: (lower run, lower_n) -> leaf index
     uint64_t* leaf_mask;
     int32_t* leaf_origin;
     int32_t* bbox;
@@ -90,7 +91,41 @@ struct AccumParams
     uint32_t* rgba8;
     float* density;
     float* color;
+    int smooth; // differentiable channels (smooth_kernel, premultiplied colour)
 };
+
+// per-Gaussian adjoint sums: [0] dL/d op, [1..3] U, [4..6] W, [7..15] Q[r][a], [16..18] dL/d rgb
+constexpr int BWD_NACC = 19;
+
+struct BwdParams
+{
+    const GaussRec* recs;
+    const void* keys;    // compact keys in emission order (sorted by Gaussian id)
+    const uint32_t* ids; // Gaussian ids in emission order
+    int64_t P, G;
+    const uint32_t* rank_to_lower;
+    const uint32_t* leaf_slot;
+    const uint64_t* leaf_vidx;
+    const uint64_t* leaf_mask;
+    const int32_t* lower_origin;
+    const float* grad_density; // [value_count] or null
+    const float* grad_color;   // [value_count][3] or null
+    float voxel_size;
+    double* acc;               // [G][BWD_NACC], zeroed
+};
+
+struct BwdFinalParams
+{
+    const double* acc;
+    int64_t G;
+    const float *means, *quats, *scales, *opacities, *colors; // the forward's inputs
+    int raw;
+    float voxel_size;
+    float *d_means, *d_quats, *d_scales, *d_opacities, *d_colors; // any may be null
+};
+
+void launch_bwd_pairs(const BwdParams& B, int key64, cudaStream_t s);
+void launch_bwd_finalize(const BwdFinalParams& F, cudaStream_t s);
 
 void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* columns, uint64_t* root_bits,
                  int* err, cudaStream_t s);

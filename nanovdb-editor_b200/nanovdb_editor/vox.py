@@ -19,6 +19,7 @@ from .utils import load_library
 
 FLAG_RAW_INPUTS = 1
 FLAG_WINDOW_ORDER = 2
+FLAG_DIFFERENTIABLE = 4
 
 STATUS = {
     0: "ok",
@@ -63,6 +64,8 @@ class vox_stats_t(Structure):
         ("ms_accumulate", c_float),
         ("ms_total", c_float),
         ("kernel_launches", c_int64),
+        ("ms_backward", c_float),
+        ("reserved0", c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -90,6 +93,10 @@ def _lib():
         lib.vox_get_stats.argtypes = [c_void_p, POINTER(vox_stats_t)]
         lib.vox_global_scan_u64.restype = c_int
         lib.vox_global_scan_u64.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]
+        lib.vox_voxel_coords.restype = c_int
+        lib.vox_voxel_coords.argtypes = [c_void_p, c_void_p, c_int64]
+        lib.vox_backward.restype = c_int
+        lib.vox_backward.argtypes = [c_void_p, POINTER(vox_gaussians_t)] + [c_void_p] * 7
         lib.vox_radix_sort_key64.restype = c_int
         lib.vox_radix_sort_key64.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_uint32]
         lib._vox_bound = True
@@ -113,6 +120,7 @@ class VoxContext:
         if not self.handle:
             raise PipelineError("vox_context_create failed (no CUDA device?)")
         self.last_grid_bytes = 0
+        self.generation = 0  # counts forward calls; the adjoint belongs to the latest
 
     def close(self):
         if getattr(self, "handle", None):
@@ -156,6 +164,7 @@ class VoxContext:
         g = self._gauss(means, quats, scales, opacities, colors)
         ptr = c_void_p()
         nbytes = c_uint64()
+        self.generation += 1
         rc = self.lib.vox_voxelize(self.handle, byref(g), float(voxel_size), float(cull_scale), int(flags), byref(ptr), byref(nbytes))
         self._check(rc, "vox_voxelize")
         self.last_grid_bytes = int(nbytes.value)
@@ -166,10 +175,28 @@ class VoxContext:
         arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (means, quats, scales, opacities, colors)]
         g = self._gauss(*arrs)
         nbytes = c_uint64()
+        self.generation += 1
         rc = self.lib.vox_voxelize_host(self.handle, byref(g), float(voxel_size), float(cull_scale), int(flags), None, 0, byref(nbytes))
         self._check(rc, "vox_voxelize_host")
         self.last_grid_bytes = int(nbytes.value)
         return self.grid()
+
+    def backward(self, means, quats, scales, opacities, colors, grad_density, grad_color, out):
+        """Adjoint of the last differentiable voxelize (device tensors).  `out` maps
+        means/quats/scales/opacities/colors to float32 CUDA tensors (or None)."""
+        g = self._gauss(means, quats, scales, opacities, colors)
+        rc = self.lib.vox_backward(
+            self.handle, byref(g), _ptr(grad_density), _ptr(grad_color),
+            *[_ptr(out.get(k)) for k in ("means", "quats", "scales", "opacities", "colors")])
+        self._check(rc, "vox_backward")
+
+    def voxel_coords(self, dst) -> None:
+        """Writes the active voxels' (i, j, k) into a CUDA int32 tensor [V, 3], row r = value index r + 2."""
+        self._check(self.lib.vox_voxel_coords(self.handle, _ptr(dst), int(dst.shape[0]) if dst.dim() > 1 else int(dst.numel()) // 3), "vox_voxel_coords")
+
+    def grid_device(self, dst) -> None:
+        """Copies the last grid into a CUDA uint8 tensor of at least last_grid_bytes."""
+        self._check(self.lib.vox_copy_grid(self.handle, _ptr(dst), int(dst.numel())), "vox_copy_grid")
 
     def grid(self) -> NodeGrid:
         out = np.empty(self.last_grid_bytes, dtype=np.uint8)

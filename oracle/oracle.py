@@ -17,6 +17,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libvox_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libref_shaders.so")
 
+OV_MODE_WINDOWS = 1
+OV_MODE_NO_F64 = 2
+OV_MODE_SMOOTH = 4
+
 COUNT_NAMES = ["G", "G_valid", "F", "P", "V", "upper", "lower", "leaf", "value_count", "node2_bytes", "windows", "error"]
 
 
@@ -64,6 +68,12 @@ def lib():
         L.ov_frag_rgba.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_void_p, c_float, c_float, c_void_p, c_void_p]
         L.ov_hier_key.restype = ctypes.c_uint64
         L.ov_hier_key.argtypes = [ctypes.c_int32] * 3
+        L.ov_lookup.restype = c_int64
+        L.ov_lookup.argtypes = [c_void_p] + [ctypes.c_int32] * 3
+        L.ov_smooth_grad64.restype = c_int
+        L.ov_smooth_grad64.argtypes = [c_void_p] + [c_void_p] * 5 + [c_int] + [c_void_p] * 7
+        L.ov_smooth_loss64.restype = ctypes.c_double
+        L.ov_smooth_loss64.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
         _LIB = L
     return _LIB
 
@@ -139,6 +149,39 @@ class OracleResult:
         b = np.empty(6, np.int32)
         lib().ov_bbox(self.h, b.ctypes.data)
         return b
+
+    def lookup(self, i, j, k) -> int:
+        return int(lib().ov_lookup(self.h, int(i), int(j), int(k)))
+
+    def smooth_grad64(self, params, raw, grad_density, grad_color=None):
+        """FP64 adjoint of the smooth channels.  params: dict means/quats/scales/
+        opacities/colors as passed to the product (raw: quats before normalisation,
+        log-scales, opacity logits, SH0).  grad arrays are indexed by value index."""
+        arrs = [_f32(params[k]) for k in ("means", "quats", "scales", "opacities", "colors")]
+        n = arrs[0].reshape(-1, 3).shape[0]
+        gd = np.ascontiguousarray(grad_density, np.float64)
+        gc = None if grad_color is None else np.ascontiguousarray(grad_color, np.float64)
+        out = {
+            "means": np.zeros((n, 3)),
+            "quats": np.zeros((n, 4)),
+            "scales": np.zeros((n, 3)),
+            "opacities": np.zeros(n),
+            "colors": np.zeros((n, 3)),
+        }
+        rc = lib().ov_smooth_grad64(
+            self.h, *[a.ctypes.data for a in arrs], int(bool(raw)), gd.ctypes.data, None if gc is None else gc.ctypes.data,
+            *[out[k].ctypes.data for k in ("means", "quats", "scales", "opacities", "colors")])
+        if rc != 0:
+            raise RuntimeError("oracle adjoint failed")
+        return out
+
+    def smooth_loss64(self, theta, raw, grad_density, grad_color=None):
+        """FP64 contribution of one Gaussian theta = [mean3, quat wxyz4, scale3, opacity, colour3]."""
+        t = np.ascontiguousarray(theta, np.float64)
+        gd = np.ascontiguousarray(grad_density, np.float64)
+        gc = None if grad_color is None else np.ascontiguousarray(grad_color, np.float64)
+        return float(lib().ov_smooth_loss64(self.h, t.ctypes.data, int(bool(raw)), gd.ctypes.data,
+                                            None if gc is None else gc.ctypes.data))
 
 
 def hier_key(i, j, k) -> int:

@@ -397,6 +397,7 @@ typedef struct
     int64_t G;
     float vs, cull;
     int skip_f64; /* timing runs: only the float outputs the product computes */
+    int smooth;   /* OV_MODE_SMOOTH: differentiable density / colour channels */
     prim_t* prims;
     /* pairs in emission (Gaussian-major) order, later sorted */
     uint64_t* keys;
@@ -628,6 +629,137 @@ static void radix_sort_pairs(uint64_t* keys, uint32_t* ids, int64_t n, int key_b
     free(hist);
 }
 
+
+/* ------------------------------------------------------------------------ */
+/* Differentiable (smooth) channels.  The reference's alpha (max over a 4^3  */
+/* lattice, opacity transform, cull) is discontinuous at the pair-set        */
+/* boundary and piecewise in every parameter, so the differentiable channels */
+/* use the centre-sampled kernel                                             */
+/*   K = max(op * exp(-|S^-1 R^T (x - mu)|^2 / 2) - 0.01, 0)                 */
+/* over the same pair set: K vanishes where the voxel centre leaves the      */
+/* 0.01-opacity ellipsoid the reference test is built on (its radius         */
+/* ls = sqrt(2 log(op / 0.01)), gaussian_prim.slang:65), so the channel is   */
+/* continuous.  density = sum K, colour = sum K * rgb (premultiplied).       */
+/* ------------------------------------------------------------------------ */
+#define OV_SMOOTH_TAU 0.01f
+#define OV_SH_C0 0.28209479177387814
+
+/* float kernel, bit-identical to the device: centre offsets rounded once
+ * from double, u = dot(d, rinv row), z = u * (1 / s), |z|^2 in dot order */
+static float smooth_k_f32(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk)
+{
+    float d[3];
+    for (int a = 0; a < 3; a++)
+        d[a] = (float)(((double)ijk[a] + 0.5) * (double)vs - (double)P->pos[a]);
+    float z[3];
+    for (int r = 0; r < 3; r++)
+        z[r] = VOX_FMUL(dot3(d, rinv[r]), VOX_FDIV(1.f, P->s[r]));
+    float q = dot3(z, z);
+    float e = VOX_FMUL(P->op, vox_expf_cr(VOX_FMUL(-0.5f, q)));
+    return e > OV_SMOOTH_TAU ? VOX_FSUB(e, OV_SMOOTH_TAU) : 0.f;
+}
+
+typedef struct
+{
+    double mu[3];
+    double q[4];  /* x, y, z, w after normalisation (raw inputs) */
+    double qnorm; /* |q| of the raw quaternion (1 for activated inputs) */
+    double R[3][3];
+    double s[3], s_act[3];
+    int clamped[3];
+    double op, rgb[3];
+    int raw;
+} g64_t;
+
+static void g64_rot(g64_t* g)
+{
+    double x = g->q[0], y = g->q[1], z = g->q[2], w = g->q[3];
+    g->R[0][0] = 1 - 2 * (y * y + z * z);
+    g->R[0][1] = 2 * (x * y - z * w);
+    g->R[0][2] = 2 * (x * z + y * w);
+    g->R[1][0] = 2 * (x * y + z * w);
+    g->R[1][1] = 1 - 2 * (x * x + z * z);
+    g->R[1][2] = 2 * (y * z - x * w);
+    g->R[2][0] = 2 * (x * z - y * w);
+    g->R[2][1] = 2 * (y * z + x * w);
+    g->R[2][2] = 1 - 2 * (x * x + y * y);
+}
+
+/* FP64 Gaussian from the caller's parameters: raw = (quaternion as given,
+ * log-scale, opacity logit, SH0) as raster/RasterUtils.cpp:59-117 activates
+ * them; otherwise (normalised quaternion, scale, opacity, rgb). */
+static void g64_setup(g64_t* g, const double* mean, const double* q_wxyz, const double* scale, double opac,
+                      const double* col, int raw, double vs)
+{
+    g->raw = raw;
+    for (int a = 0; a < 3; a++)
+        g->mu[a] = mean[a];
+    double x = q_wxyz[1], y = q_wxyz[2], z = q_wxyz[3], w = q_wxyz[0];
+    double n = raw ? sqrt(x * x + y * y + z * z + w * w) : 1.0;
+    g->qnorm = n;
+    g->q[0] = x / n;
+    g->q[1] = y / n;
+    g->q[2] = z / n;
+    g->q[3] = w / n;
+    g64_rot(g);
+    const double min_scale = 0.125 * vs;
+    for (int a = 0; a < 3; a++)
+    {
+        g->s_act[a] = raw ? exp(scale[a]) : scale[a];
+        g->clamped[a] = !(g->s_act[a] > min_scale);
+        g->s[a] = g->clamped[a] ? min_scale : g->s_act[a];
+    }
+    g->op = raw ? 1.0 / (1.0 + exp(-opac)) : opac;
+    for (int c = 0; c < 3; c++)
+        g->rgb[c] = raw ? OV_SH_C0 * col[c] + 0.5 : col[c];
+}
+
+/* FP64 Gaussian from the float activated record (value comparison only) */
+static void g64_from_prim(g64_t* g, const prim_t* P)
+{
+    g->raw = 0;
+    for (int a = 0; a < 3; a++)
+    {
+        g->mu[a] = P->pos[a];
+        g->s[a] = g->s_act[a] = P->s[a];
+        g->clamped[a] = 0;
+    }
+    for (int a = 0; a < 4; a++)
+        g->q[a] = P->q[a];
+    g->qnorm = 1.0;
+    g64_rot(g);
+    g->op = P->op;
+    for (int c = 0; c < 3; c++)
+        g->rgb[c] = P->rgb[c];
+}
+
+typedef struct
+{
+    double d[3], z[3], E, e;
+} smooth_terms_t;
+
+static double smooth64(const g64_t* g, double vs, const int32_t* ijk, smooth_terms_t* t)
+{
+    double d[3], z[3], q = 0.0;
+    for (int a = 0; a < 3; a++)
+        d[a] = ((double)ijk[a] + 0.5) * vs - g->mu[a];
+    for (int r = 0; r < 3; r++)
+    {
+        double u = g->R[0][r] * d[0] + g->R[1][r] * d[1] + g->R[2][r] * d[2];
+        z[r] = u / g->s[r];
+        q += z[r] * z[r];
+    }
+    double E = exp(-0.5 * q), e = g->op * E;
+    if (t)
+    {
+        memcpy(t->d, d, sizeof(d));
+        memcpy(t->z, z, sizeof(z));
+        t->E = E;
+        t->e = e;
+    }
+    return e > (double)OV_SMOOTH_TAU ? e - (double)OV_SMOOTH_TAU : 0.0;
+}
+
 /* ------------------------------------------------------------------------ */
 /* values: gaussian_frag_color.slang:182-246 (R mode, max of packed RGBA8)   */
 /* plus the float density / colour sums in (key, id) order                   */
@@ -659,6 +791,23 @@ static void* values_worker(void* arg)
             float a8;
             uint32_t c = frag_rgba(P, S->vs, S->cull, vmin, vmax, &a8);
             rgba = c > rgba ? c : rgba; /* InterlockedMax, :239-246 */
+            if (S->smooth)
+            {
+                float k = smooth_k_f32(P, rinv, S->vs, ijk);
+                dsum = VOX_FADD(dsum, k);
+                for (int ch = 0; ch < 3; ch++)
+                    csum[ch] = VOX_FADD(csum[ch], VOX_FMUL(k, P->rgb[ch]));
+                if (!S->skip_f64)
+                {
+                    g64_t g;
+                    g64_from_prim(&g, P);
+                    double k64 = smooth64(&g, (double)S->vs, ijk, NULL);
+                    dsum64 += k64;
+                    for (int ch = 0; ch < 3; ch++)
+                        csum64[ch] += k64 * g.rgb[ch];
+                }
+                continue;
+            }
             /* float channels: the same alpha from corner offsets rounded once from double */
             frag_test_ex(P, rinv, S->vs, ijk, vmin, vmax, 1);
             frag_rgba(P, S->vs, S->cull, vmin, vmax, &a);
@@ -675,6 +824,13 @@ static void* values_worker(void* arg)
         S->dens64[vi] = dsum64;
         for (int ch = 0; ch < 3; ch++)
         {
+            if (S->smooth)
+            {
+                /* premultiplied colour: linear in the per-pair weights */
+                S->col[3 * vi + ch] = csum[ch];
+                S->col64[3 * vi + ch] = csum64[ch];
+                continue;
+            }
             S->col[3 * vi + ch] = dsum > 0.f ? VOX_FDIV(csum[ch], dsum) : 0.f;
             S->col64[3 * vi + ch] = dsum64 > 0.0 ? csum64[ch] / dsum64 : 0.0;
         }
@@ -788,6 +944,7 @@ void* ov_run(int64_t n, const float* means, const float* quats_wxyz, const float
     S->vs = voxel_size;
     S->cull = cull_scale;
     S->skip_f64 = (window_mode & OV_MODE_NO_F64) != 0;
+    S->smooth = (window_mode & OV_MODE_SMOOTH) != 0;
     window_mode &= OV_MODE_WINDOWS;
     S->prims = (prim_t*)malloc(sizeof(prim_t) * (n ? n : 1));
     int64_t valid = 0;
@@ -1067,4 +1224,200 @@ void ov_node_table(void* h, int32_t* type, int32_t* parent, int32_t* n_in_parent
         n_in_parent[i] = (int32_t)S->nodes[i].n;
         memcpy(&origin3[3 * i], S->nodes[i].origin, 12);
     }
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP64 adjoint of the smooth channels and the per-Gaussian FP64 loss used  */
+/* for finite differences.                                                   */
+/* ------------------------------------------------------------------------ */
+int64_t ov_lookup(void* h, int32_t i, int32_t j, int32_t k)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    if (!S || S->nn == 0 || i < -65536 || i > 65535 || j < -65536 || j > 65535 || k < -65536 || k > 65535)
+        return -1;
+    uint64_t key = ov_hier_key(i, j, k);
+    uint32_t rn = (uint32_t)(key >> 36) & 0x7FFF, un = (uint32_t)(key >> 21) & 0x7FFF,
+             ln = (uint32_t)(key >> 9) & 0xFFF, vn = (uint32_t)key & 0x1FF;
+    int32_t up = S->nodes[0].child[rn];
+    if (up < 0)
+        return -1;
+    int32_t lo = S->nodes[up].child[un];
+    if (lo < 0)
+        return -1;
+    int32_t lf = S->nodes[lo].child[ln];
+    if (lf < 0)
+        return -1;
+    const node_t* L = &S->nodes[lf];
+    if (!((L->vmask[vn >> 6] >> (vn & 63)) & 1ull))
+        return -1;
+    uint64_t below = 0;
+    for (uint32_t w = 0; w < (vn >> 6); w++)
+        below += (uint64_t)popc64(L->vmask[w]);
+    below += (uint64_t)popc64(L->vmask[vn >> 6] & ((1ull << (vn & 63)) - 1ull));
+    return (int64_t)(S->value_idx_node[lf] + below);
+}
+
+/* chain the per-Gaussian sums to the caller's parameters */
+static void g64_finalize(const g64_t* g, const double U[3], const double W[3], const double Q[3][3], double dop,
+                         const double drgb[3], double* d_mean, double* d_quat_wxyz, double* d_scale, double* d_opac,
+                         double* d_col)
+{
+    for (int a = 0; a < 3; a++)
+        d_mean[a] = -(g->R[a][0] * U[0] + g->R[a][1] * U[1] + g->R[a][2] * U[2]);
+    for (int r = 0; r < 3; r++)
+    {
+        double ds = g->clamped[r] ? 0.0 : -W[r] / g->s[r];
+        d_scale[r] = g->raw ? ds * g->s_act[r] : ds;
+    }
+    /* u_r = sum_a R[a][r] d_a, so dL/dR[a][r] = Q[r][a] */
+    double G[3][3];
+    for (int a = 0; a < 3; a++)
+        for (int r = 0; r < 3; r++)
+            G[a][r] = Q[r][a];
+    double x = g->q[0], y = g->q[1], z = g->q[2], w = g->q[3];
+    double dx = 2 * y * (G[0][1] + G[1][0]) + 2 * z * (G[0][2] + G[2][0]) + 2 * w * (G[2][1] - G[1][2]) -
+                4 * x * (G[1][1] + G[2][2]);
+    double dy = 2 * x * (G[0][1] + G[1][0]) + 2 * w * (G[0][2] - G[2][0]) + 2 * z * (G[1][2] + G[2][1]) -
+                4 * y * (G[0][0] + G[2][2]);
+    double dz = 2 * w * (G[1][0] - G[0][1]) + 2 * x * (G[0][2] + G[2][0]) + 2 * y * (G[1][2] + G[2][1]) -
+                4 * z * (G[0][0] + G[1][1]);
+    double dw = 2 * z * (G[1][0] - G[0][1]) + 2 * y * (G[0][2] - G[2][0]) + 2 * x * (G[2][1] - G[1][2]);
+    if (g->raw)
+    {
+        /* q_n = q / |q| */
+        double dot = x * dx + y * dy + z * dz + w * dw;
+        dx = (dx - x * dot) / g->qnorm;
+        dy = (dy - y * dot) / g->qnorm;
+        dz = (dz - z * dot) / g->qnorm;
+        dw = (dw - w * dot) / g->qnorm;
+    }
+    d_quat_wxyz[0] = dw;
+    d_quat_wxyz[1] = dx;
+    d_quat_wxyz[2] = dy;
+    d_quat_wxyz[3] = dz;
+    *d_opac = g->raw ? dop * g->op * (1.0 - g->op) : dop;
+    for (int c = 0; c < 3; c++)
+        d_col[c] = g->raw ? OV_SH_C0 * drgb[c] : drgb[c];
+}
+
+int ov_smooth_grad64(void* h, const float* means, const float* quats_wxyz, const float* scales, const float* opacities,
+                     const float* colors, int raw, const double* grad_density, const double* grad_color,
+                     double* d_means, double* d_quats, double* d_scales, double* d_opacities, double* d_colors)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    if (!S || S->counts[OV_ERROR])
+        return -1;
+    const int64_t G = S->G;
+    double* acc = (double*)calloc((size_t)(G ? G : 1) * 19, sizeof(double));
+    const double vs = (double)S->vs;
+    int64_t v = -1;
+    for (int64_t p = 0; p < S->P; p++)
+    {
+        if (p == 0 || S->keys[p] != S->keys[p - 1])
+            v++;
+        const uint32_t gid = S->ids[p];
+        const int32_t* ijk = &S->vox_ijk[3 * v];
+        const uint64_t vi = S->vox_vidx[v];
+        double mean[3], q[4], sc[3], col[3];
+        for (int a = 0; a < 3; a++)
+        {
+            mean[a] = means[3 * gid + a];
+            sc[a] = scales[3 * gid + a];
+            col[a] = colors[3 * gid + a];
+        }
+        for (int a = 0; a < 4; a++)
+            q[a] = quats_wxyz[4 * gid + a];
+        g64_t g;
+        g64_setup(&g, mean, q, sc, (double)opacities[gid], col, raw, vs);
+        smooth_terms_t t;
+        double K = smooth64(&g, vs, ijk, &t);
+        if (!(t.e > (double)OV_SMOOTH_TAU))
+            continue;
+        double* A = &acc[19 * (int64_t)gid];
+        const double gd = grad_density ? grad_density[vi] : 0.0;
+        double gc[3] = { 0.0, 0.0, 0.0 };
+        if (grad_color)
+            for (int c = 0; c < 3; c++)
+                gc[c] = grad_color[3 * vi + c];
+        const double GK = gd + gc[0] * g.rgb[0] + gc[1] * g.rgb[1] + gc[2] * g.rgb[2];
+        A[0] += GK * t.E; /* dop */
+        for (int r = 0; r < 3; r++)
+        {
+            double dz = -GK * t.e * t.z[r];
+            double du = dz / g.s[r];
+            A[1 + r] += du;           /* U */
+            A[4 + r] += dz * t.z[r];  /* W */
+            for (int a = 0; a < 3; a++)
+                A[7 + 3 * r + a] += du * t.d[a]; /* Q[r][a] */
+        }
+        for (int c = 0; c < 3; c++)
+            A[16 + c] += K * gc[c];
+    }
+    for (int64_t gid = 0; gid < G; gid++)
+    {
+        const double* A = &acc[19 * gid];
+        double mean[3], q[4], sc[3], col[3];
+        for (int a = 0; a < 3; a++)
+        {
+            mean[a] = means[3 * gid + a];
+            sc[a] = scales[3 * gid + a];
+            col[a] = colors[3 * gid + a];
+        }
+        for (int a = 0; a < 4; a++)
+            q[a] = quats_wxyz[4 * gid + a];
+        g64_t g;
+        g64_setup(&g, mean, q, sc, (double)opacities[gid], col, raw, vs);
+        double Q[3][3];
+        for (int r = 0; r < 3; r++)
+            for (int a = 0; a < 3; a++)
+                Q[r][a] = A[7 + 3 * r + a];
+        g64_finalize(&g, &A[1], &A[4], (const double(*)[3])Q, A[0], &A[16], &d_means[3 * gid], &d_quats[4 * gid],
+                     &d_scales[3 * gid], &d_opacities[gid], &d_colors[3 * gid]);
+    }
+    free(acc);
+    return 0;
+}
+
+/* L_g(theta) = sum over voxels of grad_density * K + grad_color . K rgb for one
+ * Gaussian given in FP64 (theta = mean[3], quat wxyz[4], scale[3], opacity,
+ * colour[3]); every voxel of the kernel's support box is visited, so the
+ * value does not depend on the pair set. */
+double ov_smooth_loss64(void* h, const double* theta, int raw, const double* grad_density, const double* grad_color)
+{
+    ov_state_t* S = (ov_state_t*)h;
+    const double vs = (double)S->vs;
+    g64_t g;
+    g64_setup(&g, &theta[0], &theta[3], &theta[7], theta[10], &theta[11], raw, vs);
+    if (!(g.op > (double)OV_SMOOTH_TAU))
+        return 0.0;
+    const double ls2 = 2.0 * log(g.op / (double)OV_SMOOTH_TAU);
+    int32_t lo[3], hi[3];
+    for (int a = 0; a < 3; a++)
+    {
+        double ext = 0.0;
+        for (int r = 0; r < 3; r++)
+            ext += g.R[a][r] * g.R[a][r] * g.s[r] * g.s[r];
+        ext = sqrt(ls2 * ext);
+        lo[a] = (int32_t)floor((g.mu[a] - ext) / vs) - 1;
+        hi[a] = (int32_t)floor((g.mu[a] + ext) / vs) + 1;
+    }
+    double L = 0.0;
+    int32_t ijk[3];
+    for (ijk[0] = lo[0]; ijk[0] <= hi[0]; ijk[0]++)
+        for (ijk[1] = lo[1]; ijk[1] <= hi[1]; ijk[1]++)
+            for (ijk[2] = lo[2]; ijk[2] <= hi[2]; ijk[2]++)
+            {
+                double K = smooth64(&g, vs, ijk, NULL);
+                if (K == 0.0)
+                    continue;
+                int64_t vi = ov_lookup(h, ijk[0], ijk[1], ijk[2]);
+                if (vi < 0)
+                    continue;
+                double t = grad_density ? grad_density[vi] : 0.0;
+                if (grad_color)
+                    t += grad_color[3 * vi] * g.rgb[0] + grad_color[3 * vi + 1] * g.rgb[1] +
+                         grad_color[3 * vi + 2] * g.rgb[2];
+                L += K * t;
+            }
+    return L;
 }

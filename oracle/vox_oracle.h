@@ -55,6 +55,9 @@ void ov_preprocess(int64_t n, const float* quat_raw, const float* log_scale, con
 /* mode bits of ov_run */
 #define OV_MODE_WINDOWS 1 /* reference 256K-prim x 8M-fragment windows (else one window) */
 #define OV_MODE_NO_F64 2  /* skip the FP64 values (timed CPU-baseline runs) */
+#define OV_MODE_SMOOTH 4  /* differentiable channels: density = sum of
+                             K = max(op exp(-|S^-1 R^T (x - mu)|^2 / 2) - 0.01, 0)
+                             at voxel centres over the pair set, colour = sum K rgb */
 
 /* Full forward.  window_mode 1 = reference 256K-prim x 8M-fragment windows,
  * 0 = one window (canonical hierarchical node order).  cull_scale <= 0 selects
@@ -81,6 +84,20 @@ uint32_t ov_frag_rgba(const float* mean, const float* quat_wxyz, const float* sc
                       const float* color, float voxel_size, float cull_scale, const int32_t* ijk, float* alpha_out);
 
 uint64_t ov_hier_key(int32_t i, int32_t j, int32_t k);
+
+/* value index of an active voxel, -1 when inactive */
+int64_t ov_lookup(void* h, int32_t i, int32_t j, int32_t k);
+/* FP64 adjoint of the smooth channels over the pair set: gradients of
+ * L = sum_v grad_density[v] density[v] + grad_color[v] . colour[v] with respect
+ * to the inputs as given (raw = 1: quaternion before normalisation, log-scale,
+ * opacity logit, SH0 - raster/RasterUtils.cpp:59-117; raw = 0: activated
+ * values).  grad arrays are indexed by value index (2 + V entries). */
+int ov_smooth_grad64(void* h, const float* means, const float* quats_wxyz, const float* scales, const float* opacities,
+                     const float* colors, int raw, const double* grad_density, const double* grad_color,
+                     double* d_means, double* d_quats, double* d_scales, double* d_opacities, double* d_colors);
+/* FP64 contribution of one Gaussian (theta = mean[3], quat wxyz[4], scale[3],
+ * opacity, colour[3], raw as above) to L, summed over its kernel's support */
+double ov_smooth_loss64(void* h, const double* theta, int raw, const double* grad_density, const double* grad_color);
 
 #ifdef __cplusplus
 }
