@@ -133,6 +133,135 @@ def cpu_baseline(steps=1, target_s=15.0):
     return {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
 
 
+FWD_BWD = {"workload": "fwd_bwd_500k_clusters64_vs0.004", "gaussians": 500_000, "clusters": 64, "voxel_size": 0.004}
+
+
+def measure_fwd_bwd(ctx, torch, rank, steps, warmup, flush):
+    """Plain forward vs forward + adjoint on the 500K-Gaussian differentiable
+    workload (cluster distribution, voxel 0.004), upstream dL/dvoxel ~ N(0, 1)
+    on the active voxels; CUDA events on the library's stream, L2 flushed."""
+    from nanovdb_editor import workloads as W
+    from nanovdb_editor.vox import FLAG_DIFFERENTIABLE, FLAG_RAW_INPUTS
+
+    G = FWD_BWD["gaussians"]
+    vs = FWD_BWD["voxel_size"]
+    raw = W.cluster_cloud(G, 101 + rank, clusters=FWD_BWD["clusters"]).raw_arrays()
+    dev = [torch.from_numpy(a).cuda() for a in raw[:5]]
+    ins = (dev[0], dev[2], dev[3], dev[1], dev[4])  # means, quats, log scales, logits, SH0
+    out = {k: torch.empty_like(t) for k, t in zip(("means", "quats", "scales", "opacities", "colors"), ins)}
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    ev0, ev1, ev2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    ctx.voxelize(*ins, vs, 0.05, FLAG_RAW_INPUTS | FLAG_DIFFERENTIABLE)
+    vc = int(ctx.stats()["value_count"])
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    gd = torch.randn(vc, device="cuda", generator=gen)
+    gc = torch.randn((vc, 3), device="cuda", generator=gen)
+    gd[:2] = 0
+    gc[:2] = 0
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        res = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0.record(ext)
+            fn()
+            ev2.record(ext)
+            ev2.synchronize()
+            res.append(ev0.elapsed_time(ev2))
+        return float(np.mean(res))
+
+    plain_ms = timed(lambda: ctx.voxelize(*ins, vs, 0.05, FLAG_RAW_INPUTS))
+    fwd_ms = timed(lambda: ctx.voxelize(*ins, vs, 0.05, FLAG_RAW_INPUTS | FLAG_DIFFERENTIABLE))
+    bwd_only = []
+
+    def fwd_bwd():
+        ctx.voxelize(*ins, vs, 0.05, FLAG_RAW_INPUTS | FLAG_DIFFERENTIABLE)
+        ctx.backward(*ins, gd, gc, out)
+        bwd_only.append(ctx.stats()["ms_backward"])
+
+    fb_ms = timed(fwd_bwd)
+    st = ctx.stats()
+    return {
+        "workload": FWD_BWD["workload"],
+        "gaussians": G,
+        "pairs": int(st["pairs"]),
+        "voxels": int(st["voxels"]),
+        "plain_forward_ms": plain_ms,
+        "differentiable_forward_ms": fwd_ms,
+        "backward_ms": float(np.mean(bwd_only[-steps:])),
+        "fwd_bwd_ms": fb_ms,
+        "fwd_bwd_over_plain": fb_ms / plain_ms,
+        "fwd_bwd_gaussians_per_s": G / (fb_ms * 1e-3),
+        "plain_gaussians_per_s": G / (plain_ms * 1e-3),
+        "tolerance": "1e-5 of each gradient family's max vs the FP64 adjoint (tests/test_gpu_adjoint.py)",
+    }
+
+
+BATCHED = {"workload": "batched_256_clouds_1k-200k_vs0.002-0.02", "clouds": 256, "min_n": 1_000, "max_n": 200_000}
+
+
+def measure_batched(ctx, torch, rank, steps, warmup, flush):
+    """Uneven batch (256 clouds, log-uniform 1k-200k Gaussians, 1-16 clusters,
+    voxel size log-uniform in [0.002, 0.02]): one vox_voxelize_batch call vs the
+    plain form, one vox_voxelize call per cloud back to back; inputs resident in
+    HBM, CUDA events on the library's stream around the whole batch."""
+    from nanovdb_editor import workloads as W
+    from nanovdb_editor.vox import FLAG_RAW_INPUTS
+
+    clouds, start, vs = W.batch_clouds(BATCHED["clouds"], 3 + rank, BATCHED["min_n"], BATCHED["max_n"])
+    allc = W.concat(clouds)
+    raw = allc.raw_arrays()
+    dev = [torch.from_numpy(a).cuda() for a in raw[:5]]
+    ins = (dev[0], dev[2], dev[3], dev[1], dev[4])
+    G = int(start[-1])
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        res = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0.record(ext)
+            fn()
+            ev1.record(ext)
+            ev1.synchronize()
+            res.append(ev0.elapsed_time(ev1))
+        return float(np.mean(res))
+
+    def batched():
+        ctx.voxelize_batch(*ins, start, vs, 0.05, FLAG_RAW_INPUTS)
+
+    views = [tuple(t[int(a):int(b)] for t in ins) for a, b in zip(start[:-1], start[1:])]
+
+    def plain():
+        for v, x in zip(views, vs):
+            ctx.voxelize(*v, float(x), 0.05, FLAG_RAW_INPUTS)
+
+    b_ms = timed(batched)
+    st = ctx.stats()
+    p_ms = timed(plain)
+    return {
+        "workload": BATCHED["workload"],
+        "clouds": len(clouds),
+        "gaussians": G,
+        "pairs": int(st["pairs"]),
+        "voxels": int(st["voxels"]),
+        "batched_ms": b_ms,
+        "plain_loop_ms": p_ms,
+        "batched_gaussians_per_s": G / (b_ms * 1e-3),
+        "plain_loop_gaussians_per_s": G / (p_ms * 1e-3),
+        "batched_over_plain": p_ms / b_ms,
+        "parity": "every cloud's grid byte-identical to its single-cloud grid (tests/test_gpu_batch.py)",
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -170,6 +299,7 @@ def main():
     ap.add_argument("--gaussians", type=int, default=WORKLOAD["gaussians"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer C-ABI measurement (profiling runs)")
+    ap.add_argument("--no-forms", action="store_true", help="skip the forward+backward and batched forms")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -304,6 +434,11 @@ def main():
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get(dom)
 
+    forms = {}
+    if not args.no_forms:
+        forms["fwd_bwd"] = measure_fwd_bwd(ctx, torch, rank, args.steps, args.warmup, flush)
+        forms["batched"] = measure_batched(ctx, torch, rank, args.steps, args.warmup, flush)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu = cpu_baseline()
@@ -332,6 +467,7 @@ def main():
             "pairs_per_s": world * P / (ms * 1e-3),
             "voxels_per_s": world * st["voxels"] / (ms * 1e-3),
             "clocks": clk,
+            "forms": forms,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

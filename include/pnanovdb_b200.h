@@ -322,6 +322,22 @@ PNANOVDB_API int vox_voxelize_host(vox_context_t* ctx, const vox_gaussians_t* ga
                                    float cull_scale, uint32_t flags, void* out, uint64_t out_capacity,
                                    uint64_t* grid_bytes);
 
+/* Batched form: `clouds` independent clouds in one call, cloud b = Gaussians
+ * [cloud_start[b], cloud_start[b + 1]) of `gaussians` with its own voxel size
+ * voxel_sizes[b] (host arrays, clouds + 1 and clouds entries).  The cloud
+ * index is the most significant part of every sort key, so one emit / sort /
+ * build / accumulate chain serves all clouds.  *grids (device, context-owned)
+ * holds one self-contained grid per cloud, cloud b at byte offset
+ * grid_offsets[b] (host, clouds + 1 entries, the last = total bytes); each is
+ * laid out exactly as the single-cloud grid.  value_offsets (host, clouds + 1,
+ * may be NULL) receives where each cloud's values start when the clouds'
+ * value arrays are concatenated (the layout of vox_backward's upstream arrays
+ * after a batched call). */
+#define VOX_MAX_CLOUDS 4096
+PNANOVDB_API int vox_voxelize_batch(vox_context_t* ctx, const vox_gaussians_t* gaussians, int64_t clouds,
+                                    const int64_t* cloud_start, const float* voxel_sizes, float cull_scale,
+                                    uint32_t flags, void** grids, uint64_t* grid_offsets, uint64_t* value_offsets);
+
 /* Copies the grid of the last vox_voxelize / vox_voxelize_host call to host
  * or device memory (`capacity` bytes). */
 PNANOVDB_API int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity);
@@ -333,8 +349,10 @@ PNANOVDB_API int vox_copy_pairs(vox_context_t* ctx, uint64_t* keys, uint32_t* id
 
 PNANOVDB_API void vox_get_stats(vox_context_t* ctx, vox_stats_t* out);
 
-/* Coordinates (i, j, k) of the active voxels of the last grid, row r for value
- * index r + 2, written to DEVICE memory d_ijk [capacity][3] (capacity >= V). */
+/* Coordinates (i, j, k) of the active voxels of the last call, row r for value
+ * index r (clouds' value arrays back to back after a batched call; the two
+ * background rows of every cloud are not written), to DEVICE memory
+ * d_ijk [capacity][3], capacity >= the total value count. */
 PNANOVDB_API int vox_voxel_coords(vox_context_t* ctx, int32_t* d_ijk, int64_t capacity);
 
 /* Adjoint of the differentiable channels of the context's last call, which

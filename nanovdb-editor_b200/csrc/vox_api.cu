@@ -58,6 +58,7 @@ struct vox_context_t
     DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
     DevBuf vox_leaf, vox_n, rank_to_lower;
     DevBuf emit_keys, emit_ids, leaf_slot, bwd_acc; // differentiable calls
+    DevBuf cloud_start, cloud_vs, clouds;           // batched calls: inputs, per-cloud layout
     DevBuf order; // 9 node order arrays
     DevBuf grid;
     DevBuf scal; // device scalars
@@ -84,6 +85,8 @@ struct vox_context_t
     uint32_t last_flags = 0;
     float last_voxel_size = 0.f;
     NodeParams last_N{};
+    const float* last_cloud_vs = nullptr;
+    std::vector<uint64_t> h_grid_off, h_value_base; // per cloud, last call
 };
 
 // device scalar slots (u64 each)
@@ -99,6 +102,7 @@ enum
     SC_U,
     SC_ERR, // int in the low half
     SC_NC,  // emission columns
+    SC_GRID_BYTES,
     SC_BBOX, // 3 words (6 int32)
     SC_COUNT = SC_BBOX + 3,
     SC_SCRATCH = 16
@@ -202,13 +206,26 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b)
 // ---------------------------------------------------------------------------
 // the pipeline
 // ---------------------------------------------------------------------------
+// B clouds: Gaussians [h_start[b], h_start[b + 1]) with voxel size h_vs[b]
+// (h_start / h_vs null: one cloud with voxel_size)
 static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float voxel_size, float cull_scale,
-                        uint32_t flags)
+                        uint32_t flags, int64_t B = 1, const int64_t* h_start = nullptr, const float* h_vs = nullptr)
 {
-    if (!ctx || !gs || gs->count < 0 || !(voxel_size > 0.f))
+    if (!ctx || !gs || gs->count < 0 || B < 1 || B > VOX_MAX_CLOUDS || (!h_vs && !(voxel_size > 0.f)))
     {
         set_error(ctx, "vox_voxelize: invalid arguments");
         return VOX_ERR_ARGS;
+    }
+    if (h_start)
+    {
+        bool ok = h_start[0] == 0 && h_start[B] == gs->count && h_vs;
+        for (int64_t b = 0; ok && b < B; b++)
+            ok = h_start[b] <= h_start[b + 1] && h_vs[b] > 0.f;
+        if (!ok)
+        {
+            set_error(ctx, "vox_voxelize_batch: cloud_start must rise from 0 to the Gaussian count and every voxel size be > 0");
+            return VOX_ERR_ARGS;
+        }
     }
     if (gs->count > 0 && (!gs->means || !gs->quats || !gs->scales || !gs->opacities || !gs->colors))
     {
@@ -244,10 +261,20 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         !ensure(ctx, ctx->frag_off, sizeof(uint64_t) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->columns, sizeof(uint64_t) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->col_off, sizeof(uint64_t) * (size_t)(G + 1)) ||
-        !ensure(ctx, ctx->root_bits, sizeof(uint64_t) * 512) || !ensure(ctx, ctx->root_prefix, sizeof(uint64_t) * 512) ||
-        !ensure(ctx, ctx->root_of_rank, sizeof(uint32_t) * 32768) ||
-        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(G > 512 ? G : 512) * 2))
+        !ensure(ctx, ctx->root_bits, sizeof(uint64_t) * 512 * B) || !ensure(ctx, ctx->root_prefix, sizeof(uint64_t) * 512 * B) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(G > 512 * B ? G : 512 * B) * 2))
         return VOX_ERR_MEMORY;
+    const int64_t* d_cloud_start = nullptr;
+    const float* d_cloud_vs = nullptr;
+    if (h_start)
+    {
+        if (!ensure(ctx, ctx->cloud_start, sizeof(int64_t) * (B + 1)) || !ensure(ctx, ctx->cloud_vs, sizeof(float) * B))
+            return VOX_ERR_MEMORY;
+        cudaMemcpyAsync(ctx->cloud_start.p, h_start, sizeof(int64_t) * (B + 1), cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(ctx->cloud_vs.p, h_vs, sizeof(float) * B, cudaMemcpyHostToDevice, s);
+        d_cloud_start = (const int64_t*)ctx->cloud_start.p;
+        d_cloud_vs = (const float*)ctx->cloud_vs.p;
+    }
     GaussRec* recs = (GaussRec*)ctx->recs.p;
     uint64_t* footprints = (uint64_t*)ctx->footprints.p;
     uint64_t* frag_off = (uint64_t*)ctx->frag_off.p;
@@ -255,7 +282,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     uint64_t* col_off = (uint64_t*)ctx->col_off.p;
     uint64_t* root_bits = (uint64_t*)ctx->root_bits.p;
     uint64_t* root_prefix = (uint64_t*)ctx->root_prefix.p;
-    cudaMemsetAsync(root_bits, 0, sizeof(uint64_t) * 512, s);
+    cudaMemsetAsync(root_bits, 0, sizeof(uint64_t) * 512 * B, s);
     PrepParams P;
     P.means = gs->means;
     P.quats = gs->quats;
@@ -266,6 +293,9 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     P.raw = (flags & VOX_FLAG_RAW_INPUTS) ? 1 : 0;
     P.voxel_size = voxel_size;
     P.cull_scale = cull;
+    P.cloud_start = d_cloud_start;
+    P.cloud_vs = d_cloud_vs;
+    P.clouds = B;
     launch_prep(P, recs, footprints, columns, root_bits, d_err, s);
     uint64_t* scan_status = (uint64_t*)ctx->scan_status.p;
     size_t scan_words = ctx->scan_status.cap / sizeof(uint64_t);
@@ -273,14 +303,16 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
                        d_counter, d_err, ctx->num_sms, s);
     scan_exclusive_u64(columns, col_off, G, 0, sc + SC_NC, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
                        d_counter, d_err, ctx->num_sms, s);
-    scan_exclusive_u64(root_bits, root_prefix, 512, 1, sc + SC_NROOT, scan_status,
+    scan_exclusive_u64(root_bits, root_prefix, 512 * B, 1, sc + SC_NROOT, scan_status,
                        ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
-    launch_invert_bits(root_bits, root_prefix, 512, (uint32_t*)ctx->root_of_rank.p, s);
     int rc = sync_scalars(ctx, "prep");
     if (rc)
         return rc;
     const uint64_t F = ctx->hscal[SC_F];
     const uint64_t NR = ctx->hscal[SC_NROOT];
+    if (!ensure(ctx, ctx->root_of_rank, sizeof(uint32_t) * (NR + 1)))
+        return VOX_ERR_MEMORY;
+    launch_invert_bits(root_bits, root_prefix, 512 * B, (uint32_t*)ctx->root_of_rank.p, s);
     const uint64_t NC = ctx->hscal[SC_NC];
     ctx->stats.candidates = (int64_t)F;
 
@@ -332,6 +364,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         E.G = G;
         E.NC = NC;
         E.voxel_size = voxel_size;
+        E.cloud_vs = d_cloud_vs;
         E.cap = cap;
         E.status = (uint64_t*)ctx->emit_status.p;
         E.epoch = ctx->emit_epochs.next(E.status, ctx->emit_status.cap / sizeof(uint64_t), s);
@@ -454,6 +487,11 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         return VOX_ERR_MEMORY;
     if (diff && !ensure(ctx, ctx->leaf_slot, 4 * 4096 * (size_t)(Lo + 1)))
         return VOX_ERR_MEMORY;
+    // per-cloud tables: 3 x (B + 1) u32 starts, L u32 leaf clouds, 9 x (B + 1) u64 layout words, 6 B i32 bbox
+    const size_t cl_u32 = 3 * (size_t)(B + 1), cl_u64 = 9 * (size_t)(B + 1);
+    const size_t cl_bytes = 8 * cl_u64 + 4 * (cl_u32 + (size_t)L + 6 * (size_t)B) + 64;
+    if (!ensure(ctx, ctx->clouds, cl_bytes))
+        return VOX_ERR_MEMORY;
     scan_status = (uint64_t*)ctx->scan_status.p;
     scan_words = ctx->scan_status.cap / sizeof(uint64_t);
     NodeParams N;
@@ -479,7 +517,6 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     N.leaf_slot = diff ? (uint32_t*)ctx->leaf_slot.p : nullptr;
     N.leaf_mask = (uint64_t*)ctx->leaf_mask.p;
     N.leaf_origin = (int32_t*)ctx->leaf_origin.p;
-    N.bbox = (int32_t*)(sc + SC_BBOX);
     uint64_t* ord = (uint64_t*)ctx->order.p;
     N.upper_idx = ord;
     N.upper_addr = ord + (Lo + 1);
@@ -491,32 +528,50 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     N.leaf_addr = ord + 6 * (Lo + 1) + (L + 1);
     N.leaf_vidx = ord + 6 * (Lo + 1) + 2 * (L + 1);
     {
-        int32_t bb[6] = { 0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, (int32_t)0x80000000, (int32_t)0x80000000,
-                          (int32_t)0x80000000 };
-        cudaMemcpyAsync(N.bbox, bb, sizeof(bb), cudaMemcpyHostToDevice, s);
+        CloudParams& C = N.C;
+        uint64_t* w64 = (uint64_t*)ctx->clouds.p;
+        C.B = B;
+        C.vstart = w64;
+        C.grid_off = w64 + (B + 1);
+        C.value_base = w64 + 2 * (B + 1);
+        C.node2_bytes = w64 + 3 * (B + 1);
+        C.bbox_off = w64 + 4 * (B + 1);
+        C.rgba_off = w64 + 5 * (B + 1);
+        C.dens_off = w64 + 6 * (B + 1);
+        C.col_off = w64 + 7 * (B + 1);
+        uint32_t* w32 = (uint32_t*)(w64 + cl_u64);
+        C.upper_start = w32;
+        C.lower_start = w32 + (B + 1);
+        C.leaf_start = w32 + 2 * (B + 1);
+        C.leaf_cloud = w32 + cl_u32;
+        C.bbox = (int32_t*)(w32 + cl_u32 + L);
+        C.cloud_vs = d_cloud_vs;
+        C.voxel_size = voxel_size;
+        C.cloud_start = d_cloud_start;
+        C.frag_off = frag_off;
+        C.F_total = sc + SC_F;
+        C.G = G;
+        C.P = P_pairs;
+        C.V = V;
+        C.node_order = (flags & VOX_FLAG_WINDOW_ORDER) ? 1u : 0u;
+        cudaMemsetAsync(C.upper_start, 0, 4 * cl_u32, s); // clouds without nodes start at 0
     }
     launch_lower_info(N, s);
     scan_exclusive_u64(N.upper_head, N.upper_scan, Lo, 0, sc + SC_SCRATCH + 1, scan_status,
                        ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
     launch_upper_info(N, s);
     launch_leaf_tables(N, skeys, key64, s);
+    launch_cloud_layout(N, s);
+    cudaMemcpyAsync(sc + SC_GRID_BYTES, N.C.grid_off + B, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
     rc = sync_scalars(ctx, "node tables");
     if (rc)
         return rc;
     const uint64_t U = Lo > 0 ? ctx->hscal[SC_U] : 0;
+    const uint64_t grid_bytes = ctx->hscal[SC_GRID_BYTES];
     launch_canonical_order(N, U, s);
 
     // --------------------------------------------------------- grid buffer
-    const uint64_t node2_bytes = n2_node_bytes(0) + U * n2_node_bytes(1) + (uint64_t)Lo * n2_node_bytes(2) +
-                                 (uint64_t)L * n2_node_bytes(3);
-    const uint64_t value_count = 2 + (uint64_t)V;
-    auto al = [](uint64_t x) { return (x + 255) / 256 * 256; };
-    const uint64_t off_node2 = VOX_GRID_HEADER_BYTES;
-    const uint64_t off_bbox = al(off_node2 + node2_bytes);
-    const uint64_t off_rgba = al(off_bbox + 32);
-    const uint64_t off_dens = al(off_rgba + 4 * value_count);
-    const uint64_t off_col = al(off_dens + 4 * value_count);
-    const uint64_t grid_bytes = al(off_col + 12 * value_count);
+    // every cloud's grid: header, node2 region, bbox, RGBA8, density, colour
     if (!ensure(ctx, ctx->grid, grid_bytes))
         return VOX_ERR_MEMORY;
     uint8_t* grid = (uint8_t*)ctx->grid.p;
@@ -531,50 +586,26 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     A.rank_to_lower = N.rank_to_lower;
     A.vox_leaf = (const uint32_t*)ctx->vox_leaf.p;
     A.vox_n = (const uint16_t*)ctx->vox_n.p;
-    A.rgba8 = (uint32_t*)(grid + off_rgba);
-    A.density = (float*)(grid + off_dens);
-    A.color = (float*)(grid + off_col);
+    A.out = grid;
+    A.cloud_vs = d_cloud_vs;
     A.smooth = diff ? 1 : 0;
     launch_accumulate(A, N, sids, key64, s);
     cudaEventRecord(ctx->timers.ev[5], s);
     launch_leaf_bbox(N, s);
-    launch_write_nodes(N, U, grid + off_node2, s);
+    launch_write_nodes(N, U, grid, s);
+    launch_write_headers(N, grid, s);
+    ctx->h_grid_off.resize((size_t)B + 1);
+    ctx->h_value_base.resize((size_t)B + 1);
+    cudaMemcpyAsync(ctx->h_grid_off.data(), N.C.grid_off, sizeof(uint64_t) * (B + 1), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(ctx->h_value_base.data(), N.C.value_base, sizeof(uint64_t) * (B + 1), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(ctx->timers.ev[6], s);
     rc = sync_scalars(ctx, "accumulate");
     if (rc)
         return rc;
     rc = check_cuda(ctx, "accumulate");
     if (rc)
         return rc;
-
-    vox_grid_header_t h;
-    memset(&h, 0, sizeof(h));
-    h.magic = VOX_GRID_MAGIC;
-    h.version = 1;
-    h.header_bytes = VOX_GRID_HEADER_BYTES;
-    h.grid_bytes = grid_bytes;
-    h.node2_offset = off_node2;
-    h.node2_bytes = node2_bytes;
-    h.upper_count = (uint32_t)U;
-    h.lower_count = (uint32_t)Lo;
-    h.leaf_count = (uint32_t)L;
-    h.node_order = (flags & VOX_FLAG_WINDOW_ORDER) ? 1u : 0u;
-    h.value_count = value_count;
-    h.bbox_offset = off_bbox;
-    h.rgba8_offset = off_rgba;
-    h.density_offset = off_dens;
-    h.color_offset = off_col;
-    h.voxel_size = voxel_size;
-    memcpy(h.bbox, &ctx->hscal[SC_BBOX], sizeof(h.bbox));
-    if (V == 0)
-        memset(h.bbox, 0, sizeof(h.bbox));
-    h.pair_count = (uint64_t)P_pairs;
-    h.candidate_count = F;
-    memcpy(ctx->hscal + SC_SCRATCH * 2, &h, sizeof(h));
-    cudaMemcpyAsync(grid, ctx->hscal + SC_SCRATCH * 2, sizeof(h), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(grid + off_bbox, h.bbox, sizeof(h.bbox), cudaMemcpyHostToDevice, s);
-    cudaEventRecord(ctx->timers.ev[6], s);
-    if (cudaStreamSynchronize(s) != cudaSuccess)
-        return check_cuda(ctx, "finalize");
+    const uint64_t value_count = ctx->h_value_base[(size_t)B];
 
     ctx->last_grid_bytes = grid_bytes;
     vox_stats_t& st = ctx->stats;
@@ -596,6 +627,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     ctx->last_value_count = value_count;
     ctx->last_flags = flags;
     ctx->last_voxel_size = voxel_size;
+    ctx->last_cloud_vs = d_cloud_vs;
     ctx->last_N = N;
     ctx->diff_ready = diff;
     return VOX_OK;
@@ -648,7 +680,10 @@ static int run_backward(vox_context_t* ctx, const vox_gaussians_t* gs, const flo
     B.lower_origin = N.lower_origin;
     B.grad_density = grad_density;
     B.grad_color = grad_color;
+    B.leaf_cloud = N.C.leaf_cloud;
+    B.value_base = N.C.value_base;
     B.voxel_size = ctx->last_voxel_size;
+    B.cloud_vs = ctx->last_cloud_vs;
     B.acc = (double*)ctx->bwd_acc.p;
     if (grad_density || grad_color)
         launch_bwd_pairs(B, ctx->key64, s);
@@ -662,6 +697,8 @@ static int run_backward(vox_context_t* ctx, const vox_gaussians_t* gs, const flo
     F.colors = gs->colors;
     F.raw = (ctx->last_flags & VOX_FLAG_RAW_INPUTS) ? 1 : 0;
     F.voxel_size = ctx->last_voxel_size;
+    F.cloud_vs = ctx->last_cloud_vs;
+    F.recs = (const GaussRec*)ctx->recs.p;
     F.d_means = d_means;
     F.d_quats = d_quats;
     F.d_scales = d_scales;
@@ -680,15 +717,16 @@ static int run_backward(vox_context_t* ctx, const vox_gaussians_t* gs, const flo
     return VOX_OK;
 }
 
-// coordinates of the active voxels by value index (minus the 2 background slots)
+// coordinates of the active voxels by value index (clouds back to back)
 __global__ void k_voxel_coords(int64_t V, const uint32_t* vox_leaf, const uint16_t* vox_n, const int32_t* leaf_origin,
-                               const uint32_t* leaf_vstart, const uint64_t* leaf_vidx, int32_t* out)
+                               const uint32_t* leaf_vstart, const uint64_t* leaf_vidx, const uint32_t* leaf_cloud,
+                               const uint64_t* value_base, int32_t* out)
 {
     int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V)
         return;
     const uint32_t l = vox_leaf[v], n = vox_n[v];
-    const uint64_t slot = leaf_vidx[l] + (uint64_t)(v - leaf_vstart[l]) - 2;
+    const uint64_t slot = value_base[leaf_cloud[l]] + leaf_vidx[l] + (uint64_t)(v - leaf_vstart[l]);
     out[3 * slot + 0] = leaf_origin[3 * l + 0] + (int32_t)(n >> 6);
     out[3 * slot + 1] = leaf_origin[3 * l + 1] + (int32_t)((n >> 3) & 7);
     out[3 * slot + 2] = leaf_origin[3 * l + 2] + (int32_t)(n & 7);
@@ -781,6 +819,27 @@ const char* vox_last_error(vox_context_t* ctx)
     return ctx ? ctx->last_error.c_str() : "no context";
 }
 
+int vox_voxelize_batch(vox_context_t* ctx, const vox_gaussians_t* gaussians, int64_t clouds, const int64_t* cloud_start,
+                       const float* voxel_sizes, float cull_scale, uint32_t flags, void** grids,
+                       uint64_t* grid_offsets, uint64_t* value_offsets)
+{
+    if (!cloud_start || !voxel_sizes)
+    {
+        set_error(ctx, "vox_voxelize_batch: cloud_start and voxel_sizes are required");
+        return VOX_ERR_ARGS;
+    }
+    int rc = run_voxelize(ctx, gaussians, voxel_sizes[0], cull_scale, flags, clouds, cloud_start, voxel_sizes);
+    if (rc)
+        return rc;
+    if (grids)
+        *grids = ctx->grid.p;
+    if (grid_offsets)
+        memcpy(grid_offsets, ctx->h_grid_off.data(), sizeof(uint64_t) * (size_t)(clouds + 1));
+    if (value_offsets)
+        memcpy(value_offsets, ctx->h_value_base.data(), sizeof(uint64_t) * (size_t)(clouds + 1));
+    return VOX_OK;
+}
+
 int vox_backward(vox_context_t* ctx, const vox_gaussians_t* gaussians, const float* grad_density, const float* grad_color,
                  float* grad_means, float* grad_quats, float* grad_scales, float* grad_opacities, float* grad_colors)
 {
@@ -871,13 +930,13 @@ int vox_voxel_coords(vox_context_t* ctx, int32_t* d_ijk, int64_t capacity)
         return VOX_ERR_ARGS;
     }
     const int64_t V = ctx->last_V;
-    if (capacity < V)
+    if (capacity < (int64_t)ctx->last_value_count)
         return VOX_ERR_SIZE;
     if (V == 0)
         return VOX_OK;
     cudaSetDevice(ctx->device);
     const NodeParams& N = ctx->last_N;
-    { k_voxel_coords<<<(unsigned)((V + 255) / 256), 256, 0, ctx->stream>>>(V, (const uint32_t*)ctx->vox_leaf.p, (const uint16_t*)ctx->vox_n.p, N.leaf_origin, N.leaf_vstart, N.leaf_vidx, d_ijk); count_launch(); }
+    { k_voxel_coords<<<(unsigned)((V + 255) / 256), 256, 0, ctx->stream>>>(V, (const uint32_t*)ctx->vox_leaf.p, (const uint16_t*)ctx->vox_n.p, N.leaf_origin, N.leaf_vstart, N.leaf_vidx, N.C.leaf_cloud, N.C.value_base, d_ijk); count_launch(); }
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return check_cuda(ctx, "vox_voxel_coords");
     return VOX_OK;

@@ -47,14 +47,15 @@ __device__ __forceinline__ void pair_adjoint(const BwdParams& B, uint64_t key, u
     for (uint32_t w = 0; w < (vn >> 6); w++)
         below += (uint64_t)__popcll(m[w]);
     below += (uint64_t)__popcll(m[vn >> 6] & ((1ull << (vn & 63)) - 1ull));
-    const uint64_t vi = B.leaf_vidx[l] + below;
+    // value index in the value-concatenated upstream arrays (clouds back to back)
+    const uint64_t vi = B.value_base[B.leaf_cloud[l]] + B.leaf_vidx[l] + below;
     const int32_t x = B.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8 + (int32_t)(vn >> 6);
     const int32_t y = B.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8 + (int32_t)((vn >> 3) & 7);
     const int32_t z = B.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8 + (int32_t)(vn & 7);
     const GaussRec R = B.recs[gid];
     const RInv M = rinv_of(R);
     SmoothTerms t;
-    const float Kw = smooth_kernel(R, M, B.voxel_size, x, y, z, t);
+    const float Kw = smooth_kernel(R, M, rec_vs(R, B.voxel_size, B.cloud_vs), x, y, z, t);
     if (!(t.e > SMOOTH_TAU))
         return;
     const float gd = B.grad_density ? B.grad_density[vi] : 0.f;
@@ -175,7 +176,8 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
           dc[3] = { 0.f, 0.f, 0.f };
     if (any)
     {
-        const double vs = (double)F.voxel_size;
+        const float vsf = rec_vs(F.recs[g], F.voxel_size, F.cloud_vs);
+        const double vs = (double)vsf;
         // rotation of the quaternion as the forward used it (normalised for raw inputs)
         double x = F.quats[4 * g + 1], y = F.quats[4 * g + 2], z = F.quats[4 * g + 3], w = F.quats[4 * g + 0];
         const double n = F.raw ? sqrt(x * x + y * y + z * z + w * w) : 1.0;
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
         const double* W = &a[4];
         for (int k = 0; k < 3; k++)
             dmu[k] = (float)(-(R[k][0] * U[0] + R[k][1] * U[1] + R[k][2] * U[2]));
-        const float min_scale = VOX_FMUL(0.125f, F.voxel_size);
+        const float min_scale = VOX_FMUL(0.125f, vsf);
         for (int r = 0; r < 3; r++)
         {
             const float in = F.scales[3 * g + r];

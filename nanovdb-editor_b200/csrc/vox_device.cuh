@@ -53,6 +53,13 @@ __device__ __forceinline__ uint32_t root_n_of(int32_t x, int32_t y, int32_t z)
     return ((((uint32_t)x & 0x1FFFFu) >> 12) << 10) | ((((uint32_t)y & 0x1FFFFu) >> 12) << 5) |
            (((uint32_t)z & 0x1FFFFu) >> 12);
 }
+// root tile index across clouds: cloud << 15 | root_n.  Ranks of touched root
+// tiles and lower cells are taken in this order, so the cloud is the most
+// significant part of every compact key.
+__device__ __forceinline__ uint64_t root_index(uint32_t cloud, int32_t x, int32_t y, int32_t z)
+{
+    return ((uint64_t)cloud << 15) | root_n_of(x, y, z);
+}
 __device__ __forceinline__ uint32_t upper_n_of(int32_t x, int32_t y, int32_t z)
 {
     return ((((uint32_t)x & 0xFFFu) >> 7) << 10) | ((((uint32_t)y & 0xFFFu) >> 7) << 5) | (((uint32_t)z & 0xFFFu) >> 7);
@@ -84,7 +91,7 @@ struct __align__(16) GaussRec
     float4 q2; // rinv[1][1..2], rinv[2][0..1]
     float4 q3; // rinv[2][2], inv_s.xyz = 1/s (clamped scale)
     int4 q4;   // bbox min xyz, valid
-    int4 q5;   // bbox range xyz (max + 1 - min), unused
+    int4 q5;   // bbox range xyz (max + 1 - min), cloud index
     float4 q6; // opacity, ls, e = 1 / (0.1 |s| / voxel_size), |s|
     float4 q7; // rgb, culled (1.f if |s| > cull scale)
 };
@@ -98,9 +105,16 @@ struct PrepParams
     const float* colors;  // 3G RGB (SH0 when raw)
     int64_t count;
     int raw;              // 1: apply the host preprocessing of raster/RasterUtils.cpp:59-117
-    float voxel_size;
+    float voxel_size;     // every cloud's voxel size when cloud_vs is null
     float cull_scale;     // > 0
+    // batched calls: Gaussians [cloud_start[b], cloud_start[b + 1]) form cloud b
+    // with voxel size cloud_vs[b]; null for one cloud
+    const int64_t* cloud_start;
+    const float* cloud_vs;
+    int64_t clouds;
 };
+
+
 
 // dot with the reference's fixed evaluation order (a.x*b.x + a.y*b.y) + a.z*b.z
 __device__ __forceinline__ float dot3_rn(float ax, float ay, float az, float bx, float by, float bz)
@@ -116,7 +130,7 @@ __device__ __forceinline__ bool finite_f(float v)
 // Builds the record of one Gaussian (gaussian_prim.slang:47-144 and the
 // per-Gaussian prologue of gaussian_frag_alloc.slang / gaussian_frag_color.slang).
 // Returns the bbox footprint (0 when the Gaussian emits nothing).
-__device__ __forceinline__ uint64_t make_record(const PrepParams& P, int64_t g, GaussRec& R, int32_t bmax[3])
+__device__ __forceinline__ uint64_t make_record(const PrepParams& P, int64_t g, float vs, GaussRec& R, int32_t bmax[3])
 {
     float pos[3] = { P.means[3 * g + 0], P.means[3 * g + 1], P.means[3 * g + 2] };
     float qw = P.quats[4 * g + 0], qx = P.quats[4 * g + 1], qy = P.quats[4 * g + 2], qz = P.quats[4 * g + 3];
@@ -139,7 +153,6 @@ __device__ __forceinline__ uint64_t make_record(const PrepParams& P, int64_t g, 
             rgb[a] = VOX_FADD(VOX_FMUL(c0, rgb[a]), 0.5f);
         op = VOX_FDIV(1.f, VOX_FADD(1.f, vox_expf_cr(-op)));
     }
-    const float vs = P.voxel_size;
     const float vs_inv = VOX_FDIV(1.f, vs);
 
     bool ok = finite_f(op) && finite_f(qx) && finite_f(qy) && finite_f(qz) && finite_f(qw);
@@ -201,10 +214,20 @@ __device__ __forceinline__ uint64_t make_record(const PrepParams& P, int64_t g, 
     R.q2 = make_float4(r[1][1], r[2][1], r[0][2], r[1][2]);
     R.q3 = make_float4(r[2][2], VOX_FDIV(1.f, s[0]), VOX_FDIV(1.f, s[1]), VOX_FDIV(1.f, s[2]));
     R.q4 = make_int4(bmin[0], bmin[1], bmin[2], ok ? 1 : 0);
-    R.q5 = make_int4(bmax[0] + 1 - bmin[0], bmax[1] + 1 - bmin[1], bmax[2] + 1 - bmin[2], 0);
+    R.q5 = make_int4(bmax[0] + 1 - bmin[0], bmax[1] + 1 - bmin[1], bmax[2] + 1 - bmin[2], 0); // cloud set by the caller
     R.q6 = make_float4(op, ls, e, scale1d);
     R.q7 = make_float4(rgb[0], rgb[1], rgb[2], culled);
     return footprint;
+}
+
+__device__ __forceinline__ uint32_t rec_cloud(const GaussRec& R)
+{
+    return (uint32_t)R.q5.w;
+}
+// voxel size of the record's cloud
+__device__ __forceinline__ float rec_vs(const GaussRec& R, float vs, const float* cloud_vs)
+{
+    return cloud_vs ? cloud_vs[R.q5.w] : vs;
 }
 
 // inverse rotation rows from the record: rinv[row][axis]

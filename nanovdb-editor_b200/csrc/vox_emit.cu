@@ -41,9 +41,9 @@ __device__ __forceinline__ int64_t upper_bound_u64(const uint64_t* a, int64_t lo
 }
 
 template <class K>
-__device__ __forceinline__ K compact_key(const RankTables& T, int32_t x, int32_t y, int32_t z)
+__device__ __forceinline__ K compact_key(const RankTables& T, uint32_t cloud, int32_t x, int32_t y, int32_t z)
 {
-    uint64_t rr = bit_rank(T.root_bits, T.root_prefix, root_n_of(x, y, z));
+    uint64_t rr = bit_rank(T.root_bits, T.root_prefix, root_index(cloud, x, y, z));
     uint64_t cell = rr * 32768ull + upper_n_of(x, y, z);
     uint64_t lr = bit_rank(T.lower_bits, T.lower_prefix, cell);
     return (K)((lr << 21) | ((uint64_t)lower_n_of(x, y, z) << 9) | (uint64_t)leaf_n_of(x, y, z));
@@ -91,11 +91,11 @@ __device__ __forceinline__ bool test_candidate(const EmitParams& E, const RankTa
     gid = S.col_g[col];
     const GaussRec R = E.recs[gid];
     const RInv M = rinv_of(R);
-    const bool pass = aabb_hits_unit_sphere(voxel_local_aabb(R, M, E.voxel_size, i, j, k));
+    const bool pass = aabb_hits_unit_sphere(voxel_local_aabb(R, M, rec_vs(R, E.voxel_size, E.cloud_vs), i, j, k));
     if (CHECK && pass && (k < S.col_blo[col] || k > S.col_bhi[col]))
         atomicOr(E.err, ERR_BOUNDS); // the column bound would have dropped a passing voxel
     if (pass)
-        key = compact_key<K>(T, i, j, k);
+        key = compact_key<K>(T, rec_cloud(R), i, j, k);
     return pass;
 }
 
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(EMIT_BLOCK) k_emit(EmitParams E, RankTables T,
             const int32_t i = R.q4.x + (int32_t)(lc / (uint32_t)R.q5.y);
             const int32_t j = R.q4.y + (int32_t)(lc % (uint32_t)R.q5.y);
             int32_t klo, khi;
-            column_interval(R, M, E.voxel_size, i, j, klo, khi);
+            column_interval(R, M, rec_vs(R, E.voxel_size, E.cloud_vs), i, j, klo, khi);
             S.col_g[threadIdx.x] = (uint32_t)g;
             S.col_i[threadIdx.x] = i;
             S.col_j[threadIdx.x] = j;

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cuda_runtime.h>
 
+#include "pnanovdb_b200.h"
 #include "vox_device.cuh"
 #include "vox_internal.h"
 #include "vox_raster.h"
@@ -33,7 +34,24 @@ __global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint
         return;
     GaussRec R;
     int32_t bmax[3];
-    uint64_t fp = make_record(P, g, R, bmax);
+    uint32_t cloud = 0;
+    if (P.cloud_start)
+    {
+        // last cloud whose start is <= g
+        int64_t lo = 0, hi = P.clouds;
+        while (lo < hi)
+        {
+            int64_t mid = (lo + hi) >> 1;
+            if (P.cloud_start[mid] <= g)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        cloud = (uint32_t)(lo - 1);
+    }
+    const float vs = P.cloud_vs ? P.cloud_vs[cloud] : P.voxel_size;
+    uint64_t fp = make_record(P, g, vs, R, bmax);
+    R.q5.w = (int32_t)cloud;
     if (fp)
     {
         int e = 0;
@@ -62,7 +80,7 @@ __global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint
             for (int32_t y = R.q4.y >> 12; y <= (bmax[1] >> 12); y++)
                 for (int32_t z = R.q4.z >> 12; z <= (bmax[2] >> 12); z++)
                 {
-                    uint32_t rn = root_n_of(x << 12, y << 12, z << 12);
+                    const uint64_t rn = root_index(cloud, x << 12, y << 12, z << 12);
                     atomicOr(&root_bits[rn >> 6], 1ull << (rn & 63));
                 }
     }
@@ -84,7 +102,7 @@ __global__ void __launch_bounds__(256) k_mark_lower(const GaussRec* recs, int64_
             for (int32_t z = mn[2] >> 7; z <= (mx[2] >> 7); z++)
             {
                 int32_t cx = x << 7, cy = y << 7, cz = z << 7;
-                uint64_t rr = bit_rank(root_bits, root_prefix, root_n_of(cx, cy, cz));
+                uint64_t rr = bit_rank(root_bits, root_prefix, root_index(rec_cloud(R), cx, cy, cz));
                 uint64_t cell = rr * 32768ull + upper_n_of(cx, cy, cz);
                 atomicOr(&lower_bits[cell >> 6], 1ull << (cell & 63));
             }
@@ -273,31 +291,194 @@ __global__ void k_upper_info(NodeParams N)
     }
 }
 
-// canonical (single fragment window) node order: uppers, lowers, leaves, each
-// in hierarchical key order; node addresses follow node_idx order
+// ---------------------------------------------------------------- clouds ----
+__device__ __forceinline__ uint32_t upper_cloud(const NodeParams& N, uint64_t u)
+{
+    return N.upper_root_n[u] >> 15;
+}
+__device__ __forceinline__ uint32_t lower_cloud(const NodeParams& N, uint64_t lo)
+{
+    return N.upper_root_n[N.lower_parent[lo]] >> 15;
+}
+
+// fills start[b] for clouds (prev, cur] with i; the last element closes the table
+__device__ __forceinline__ void fill_starts(uint32_t* start, int64_t i, int64_t n, int64_t prev, int64_t cur, int64_t B)
+{
+    for (int64_t b = prev + 1; b <= cur; b++)
+        start[b] = (uint32_t)i;
+    if (i == n - 1)
+        for (int64_t b = cur + 1; b <= B; b++)
+            start[b] = (uint32_t)n;
+}
+
+// first upper / lower / leaf of every cloud (nodes are ordered by cloud first);
+// the upper count is read on the device
+__global__ void k_cloud_starts(NodeParams N)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t U = (int64_t)*N.upper_count, B = N.C.B;
+    if (t < U)
+        fill_starts(N.C.upper_start, t, U, t ? (int64_t)upper_cloud(N, t - 1) : -1, upper_cloud(N, t), B);
+    if (t < N.Lo)
+        fill_starts(N.C.lower_start, t, N.Lo, t ? (int64_t)lower_cloud(N, t - 1) : -1, lower_cloud(N, t), B);
+    if (t < N.L)
+    {
+        const uint32_t c = lower_cloud(N, N.leaf_lower[t]);
+        N.C.leaf_cloud[t] = c;
+        fill_starts(N.C.leaf_start, t, N.L, t ? (int64_t)lower_cloud(N, N.leaf_lower[t - 1]) : -1, c, B);
+    }
+}
+
+__device__ __forceinline__ uint64_t al256(uint64_t x)
+{
+    return (x + 255) / 256 * 256;
+}
+
+// one CTA: per-cloud node counts -> grid layout, grid offsets and value bases
+// (exclusive scans over the clouds, 1024 at a time)
+__global__ void __launch_bounds__(1024) k_cloud_layout(NodeParams N)
+{
+    __shared__ uint64_t s_warp[33];
+    __shared__ uint64_t s_carry[2];
+    const CloudParams& C = N.C;
+    if (threadIdx.x == 0)
+        s_carry[0] = s_carry[1] = 0;
+    __syncthreads();
+    for (int64_t c0 = 0; c0 < C.B; c0 += blockDim.x)
+    {
+        const int64_t b = c0 + threadIdx.x;
+        uint64_t size = 0, vc = 0;
+        uint64_t node2 = 0, o_bbox = 0, o_rgba = 0, o_dens = 0, o_col = 0;
+        if (b < C.B)
+        {
+            const uint64_t U = C.upper_start[b + 1] - C.upper_start[b];
+            const uint64_t Lo = C.lower_start[b + 1] - C.lower_start[b];
+            const uint64_t L = C.leaf_start[b + 1] - C.leaf_start[b];
+            const uint64_t v0 = C.leaf_start[b] < (uint64_t)N.L ? N.leaf_vstart[C.leaf_start[b]] : (uint64_t)C.V;
+            C.vstart[b] = v0;
+            if (b == C.B - 1)
+                C.vstart[C.B] = (uint64_t)C.V;
+            const uint64_t v1 = C.leaf_start[b + 1] < (uint64_t)N.L ? N.leaf_vstart[C.leaf_start[b + 1]] : (uint64_t)C.V;
+            vc = 2 + (v1 - v0);
+            node2 = n2_node_bytes(0) + U * n2_node_bytes(1) + Lo * n2_node_bytes(2) + L * n2_node_bytes(3);
+            o_bbox = al256(VOX_GRID_HEADER_BYTES + node2);
+            o_rgba = al256(o_bbox + 32);
+            o_dens = al256(o_rgba + 4 * vc);
+            o_col = al256(o_dens + 4 * vc);
+            size = al256(o_col + 12 * vc);
+            for (int a = 0; a < 6; a++)
+                C.bbox[6 * b + a] = a < 3 ? 0x7FFFFFFF : (int32_t)0x80000000;
+        }
+        uint64_t tot_size, tot_vc;
+        const uint64_t ex_size = block_excl_scan_u64(size, s_warp, tot_size);
+        const uint64_t ex_vc = block_excl_scan_u64(vc, s_warp, tot_vc);
+        if (b < C.B)
+        {
+            const uint64_t g = s_carry[0] + ex_size;
+            C.grid_off[b] = g;
+            C.value_base[b] = s_carry[1] + ex_vc;
+            C.node2_bytes[b] = node2;
+            C.bbox_off[b] = g + o_bbox;
+            C.rgba_off[b] = g + o_rgba;
+            C.dens_off[b] = g + o_dens;
+            C.col_off[b] = g + o_col;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            s_carry[0] += tot_size;
+            s_carry[1] += tot_vc;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        C.grid_off[C.B] = s_carry[0];
+        C.value_base[C.B] = s_carry[1];
+    }
+}
+
+// canonical (single fragment window) node order inside every cloud's grid:
+// uppers, lowers, leaves, each in hierarchical key order; node addresses
+// (absolute in the output buffer) follow node_idx order
 __global__ void k_canonical_order(NodeParams N, uint64_t U)
 {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t root_sz = n2_node_bytes(0), up_sz = n2_node_bytes(1), lo_sz = n2_node_bytes(2),
                    lf_sz = n2_node_bytes(3);
+    const CloudParams& C = N.C;
     if (t < (int64_t)U)
     {
-        N.upper_idx[t] = 1 + t;
-        N.upper_addr[t] = root_sz + (uint64_t)t * up_sz;
+        const uint32_t b = upper_cloud(N, t);
+        const uint64_t local = (uint64_t)t - C.upper_start[b];
+        N.upper_idx[t] = 1 + local;
+        N.upper_addr[t] = C.grid_off[b] + VOX_GRID_HEADER_BYTES + root_sz + local * up_sz;
         N.upper_vidx[t] = 2;
     }
     if (t < N.Lo)
     {
-        N.lower_idx[t] = 1 + U + t;
-        N.lower_addr[t] = root_sz + U * up_sz + (uint64_t)t * lo_sz;
+        const uint32_t b = lower_cloud(N, t);
+        const uint64_t Ub = C.upper_start[b + 1] - C.upper_start[b];
+        const uint64_t local = (uint64_t)t - C.lower_start[b];
+        N.lower_idx[t] = 1 + Ub + local;
+        N.lower_addr[t] = C.grid_off[b] + VOX_GRID_HEADER_BYTES + root_sz + Ub * up_sz + local * lo_sz;
         N.lower_vidx[t] = 2;
     }
     if (t < N.L)
     {
-        N.leaf_idx[t] = 1 + U + N.Lo + t;
-        N.leaf_addr[t] = root_sz + U * up_sz + (uint64_t)N.Lo * lo_sz + (uint64_t)t * lf_sz;
-        N.leaf_vidx[t] = 2 + (uint64_t)N.leaf_vstart[t];
+        const uint32_t b = C.leaf_cloud[t];
+        const uint64_t Ub = C.upper_start[b + 1] - C.upper_start[b];
+        const uint64_t Lob = C.lower_start[b + 1] - C.lower_start[b];
+        const uint64_t local = (uint64_t)t - C.leaf_start[b];
+        N.leaf_idx[t] = 1 + Ub + Lob + local;
+        N.leaf_addr[t] = C.grid_off[b] + VOX_GRID_HEADER_BYTES + root_sz + Ub * up_sz + Lob * lo_sz + local * lf_sz;
+        N.leaf_vidx[t] = 2 + ((uint64_t)N.leaf_vstart[t] - C.vstart[b]);
     }
+}
+
+// per cloud: the grid header (vox_grid_header_t) and the bbox blind data
+__global__ void k_write_headers(NodeParams N, uint8_t* out)
+{
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const CloudParams& C = N.C;
+    if (b >= C.B)
+        return;
+    const uint64_t g = C.grid_off[b];
+    vox_grid_header_t h;
+    memset(&h, 0, sizeof(h));
+    const uint64_t vc = 2 + (C.vstart[b + 1] - C.vstart[b]);
+    h.magic = VOX_GRID_MAGIC;
+    h.version = 1;
+    h.header_bytes = VOX_GRID_HEADER_BYTES;
+    h.grid_bytes = C.grid_off[b + 1] - g;
+    h.node2_offset = VOX_GRID_HEADER_BYTES;
+    h.node2_bytes = C.node2_bytes[b];
+    h.upper_count = C.upper_start[b + 1] - C.upper_start[b];
+    h.lower_count = C.lower_start[b + 1] - C.lower_start[b];
+    h.leaf_count = C.leaf_start[b + 1] - C.leaf_start[b];
+    h.node_order = C.node_order;
+    h.value_count = vc;
+    h.bbox_offset = C.bbox_off[b] - g;
+    h.rgba8_offset = C.rgba_off[b] - g;
+    h.density_offset = C.dens_off[b] - g;
+    h.color_offset = C.col_off[b] - g;
+    h.voxel_size = C.cloud_vs ? C.cloud_vs[b] : C.voxel_size;
+    if (vc > 2)
+        for (int a = 0; a < 6; a++)
+            h.bbox[a] = C.bbox[6 * b + a];
+    const uint64_t p0 = C.vstart[b] < (uint64_t)C.V ? N.vox_start[C.vstart[b]] : (uint64_t)C.P;
+    const uint64_t p1 = C.vstart[b + 1] < (uint64_t)C.V ? N.vox_start[C.vstart[b + 1]] : (uint64_t)C.P;
+    h.pair_count = p1 - p0;
+    const int64_t g0 = C.cloud_start ? C.cloud_start[b] : 0, g1 = C.cloud_start ? C.cloud_start[b + 1] : C.G;
+    const uint64_t f0 = g0 < C.G ? C.frag_off[g0] : *C.F_total, f1 = g1 < C.G ? C.frag_off[g1] : *C.F_total;
+    h.candidate_count = f1 - f0;
+    const uint32_t* src = (const uint32_t*)&h;
+    uint32_t* dst = (uint32_t*)(out + g);
+    for (int w = 0; w < (int)(sizeof(h) / 4); w++)
+        dst[w] = src[w];
+    int32_t* bb = (int32_t*)(out + C.bbox_off[b]);
+    for (int a = 0; a < 6; a++)
+        bb[a] = h.bbox[a];
 }
 
 // per leaf: lower_n in its parent and origin
@@ -325,7 +506,12 @@ __global__ void __launch_bounds__(256) k_leaf_bbox(NodeParams N)
     if (threadIdx.x < 6)
         s_bb[threadIdx.x] = threadIdx.x < 3 ? 0x7FFFFFFF : (int32_t)0x80000000;
     __syncthreads();
-    int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t l0 = (int64_t)blockIdx.x * blockDim.x;
+    const int64_t lz = min((int64_t)N.L, l0 + (int64_t)blockDim.x) - 1;
+    // leaves of one cloud reduce in shared memory; a CTA spanning clouds goes to global per leaf
+    const uint32_t cb = N.C.leaf_cloud[l0];
+    const bool one_cloud = N.C.leaf_cloud[lz] == cb;
+    int64_t l = l0 + threadIdx.x;
     if (l < N.L)
     {
         int32_t mn[3] = { 8, 8, 8 }, mx[3] = { -1, -1, -1 };
@@ -344,17 +530,21 @@ __global__ void __launch_bounds__(256) k_leaf_bbox(NodeParams N)
                 }
             }
         }
+        int32_t* bb = one_cloud ? s_bb : N.C.bbox + 6 * (uint64_t)N.C.leaf_cloud[l];
         for (int a = 0; a < 3; a++)
         {
-            atomicMin(&s_bb[a], N.leaf_origin[3 * l + a] + mn[a]);
-            atomicMax(&s_bb[3 + a], N.leaf_origin[3 * l + a] + mx[a]);
+            atomicMin(&bb[a], N.leaf_origin[3 * l + a] + mn[a]);
+            atomicMax(&bb[3 + a], N.leaf_origin[3 * l + a] + mx[a]);
         }
     }
     __syncthreads();
-    if (threadIdx.x < 3)
-        atomicMin(&N.bbox[threadIdx.x], s_bb[threadIdx.x]);
-    else if (threadIdx.x < 6)
-        atomicMax(&N.bbox[threadIdx.x], s_bb[threadIdx.x]);
+    if (one_cloud)
+    {
+        if (threadIdx.x < 3)
+            atomicMin(&N.C.bbox[6 * (uint64_t)cb + threadIdx.x], s_bb[threadIdx.x]);
+        else if (threadIdx.x < 6)
+            atomicMax(&N.C.bbox[6 * (uint64_t)cb + threadIdx.x], s_bb[threadIdx.x]);
+    }
 }
 
 // leaf -> lower index (leaves of lower lo are [lower_lstart[lo], lower_lstart[lo+1]))
@@ -403,17 +593,22 @@ __device__ void write_prefix_block(uint64_t* dst, const uint64_t* s_mask, uint32
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(1024) k_write_root(NodeParams N, uint64_t U, uint8_t* node2)
+// one CTA per cloud: the root of that cloud's grid
+__global__ void __launch_bounds__(1024) k_write_root(NodeParams N, uint8_t* out)
 {
     __shared__ uint64_t s_mask[512];
     __shared__ uint32_t s_scan[513];
-    uint64_t* W = (uint64_t*)node2;
+    const uint64_t b = blockIdx.x;
+    const uint64_t root_addr = N.C.grid_off[b] + VOX_GRID_HEADER_BYTES;
+    uint64_t* W = (uint64_t*)(out + root_addr);
+    const uint32_t u0 = N.C.upper_start[b];
+    const uint64_t U = N.C.upper_start[b + 1] - u0;
     for (int i = threadIdx.x; i < 512; i += blockDim.x)
         s_mask[i] = 0;
     __syncthreads();
     for (uint64_t u = threadIdx.x; u < U; u += blockDim.x)
     {
-        uint32_t rn = N.upper_root_n[u];
+        uint32_t rn = N.upper_root_n[u0 + u] & 32767u;
         atomicOr((unsigned long long*)&s_mask[rn >> 6], 1ull << (rn & 63));
     }
     __syncthreads();
@@ -434,10 +629,10 @@ __global__ void __launch_bounds__(1024) k_write_root(NodeParams N, uint64_t U, u
     {
         uint64_t val = N2_END_KEY;
         if (e < U)
-            val = N.upper_addr[e];
+            val = N.upper_addr[u0 + e] - root_addr;
         else if (e < 2 * U)
         {
-            uint32_t rn = N.upper_root_n[e - U];
+            uint32_t rn = N.upper_root_n[u0 + e - U] & 32767u;
             int32_t x = (int32_t)(((rn >> 10) & 31) << 12), y = (int32_t)(((rn >> 5) & 31) << 12),
                     z = (int32_t)((rn & 31) << 12);
             x = x >= 65536 ? x - 131072 : x;
@@ -592,7 +787,7 @@ __global__ void __launch_bounds__(ACC_BLOCK) k_accumulate(AccumParams A, NodePar
             const int32_t z = N.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8 + (int32_t)(vn & 7);
             const GaussRec R = A.recs[ids[p]];
             const RInv M = rinv_of(R);
-            const float vs = A.voxel_size;
+            const float vs = rec_vs(R, A.voxel_size, A.cloud_vs);
             float cx0, cx1, cy0, cy1, cz0, cz1;
             axis_corners(vs, R.q0.x, x, cx0, cx1);
             axis_corners(vs, R.q0.y, y, cy0, cy1);
@@ -642,20 +837,24 @@ __global__ void __launch_bounds__(ACC_BLOCK) k_accumulate(AccumParams A, NodePar
         const uint32_t l = A.vox_leaf[v];
         const uint32_t n = A.vox_n[v];
         const uint64_t vi = N.leaf_vidx[l] + (uint64_t)(v - N.leaf_vstart[l]);
-        A.rgba8[vi] = rgba;
-        A.density[vi] = dsum;
+        const uint32_t b = N.C.leaf_cloud[l];
+        uint32_t* rgba8 = (uint32_t*)(A.out + N.C.rgba_off[b]);
+        float* density = (float*)(A.out + N.C.dens_off[b]);
+        float* color = (float*)(A.out + N.C.col_off[b]);
+        rgba8[vi] = rgba;
+        density[vi] = dsum;
         if (A.smooth)
         {
             // premultiplied colour (linear in the per-pair weights)
-            A.color[3 * vi + 0] = c0;
-            A.color[3 * vi + 1] = c1;
-            A.color[3 * vi + 2] = c2;
+            color[3 * vi + 0] = c0;
+            color[3 * vi + 1] = c1;
+            color[3 * vi + 2] = c2;
         }
         else
         {
-            A.color[3 * vi + 0] = dsum > 0.f ? VOX_FDIV(c0, dsum) : 0.f;
-            A.color[3 * vi + 1] = dsum > 0.f ? VOX_FDIV(c1, dsum) : 0.f;
-            A.color[3 * vi + 2] = dsum > 0.f ? VOX_FDIV(c2, dsum) : 0.f;
+            color[3 * vi + 0] = dsum > 0.f ? VOX_FDIV(c0, dsum) : 0.f;
+            color[3 * vi + 1] = dsum > 0.f ? VOX_FDIV(c1, dsum) : 0.f;
+            color[3 * vi + 2] = dsum > 0.f ? VOX_FDIV(c2, dsum) : 0.f;
         }
         atomicOr((unsigned long long*)&N.leaf_mask[8 * (uint64_t)l + (n >> 6)], 1ull << (n & 63));
     }
@@ -743,15 +942,27 @@ void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s)
         return;
     { k_canonical_order<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(N, U); count_launch(); }
 }
-void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* node2, cudaStream_t s)
+void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* out, cudaStream_t s)
 {
-    { k_write_root<<<1, 1024, 0, s>>>(N, U, node2); count_launch(); }
+    { k_write_root<<<(unsigned)N.C.B, 1024, 0, s>>>(N, out); count_launch(); }
     if (U)
-        { k_write_upper<<<(unsigned)U, 512, 0, s>>>(N, node2); count_launch(); }
+        { k_write_upper<<<(unsigned)U, 512, 0, s>>>(N, out); count_launch(); }
     if (N.Lo)
-        { k_write_lower<<<(unsigned)N.Lo, 256, 0, s>>>(N, node2); count_launch(); }
+        { k_write_lower<<<(unsigned)N.Lo, 256, 0, s>>>(N, out); count_launch(); }
     if (N.L)
-        { k_write_leaf<<<(unsigned)((N.L * 16 + 255) / 256), 256, 0, s>>>(N, node2); count_launch(); }
+        { k_write_leaf<<<(unsigned)((N.L * 16 + 255) / 256), 256, 0, s>>>(N, out); count_launch(); }
+}
+void launch_cloud_layout(const NodeParams& N, cudaStream_t s)
+{
+    // U <= Lo, so Lo + L threads cover every level
+    const int64_t n = N.Lo > N.L ? N.Lo : N.L;
+    if (n > 0)
+        { k_cloud_starts<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(N); count_launch(); }
+    { k_cloud_layout<<<1, 1024, 0, s>>>(N); count_launch(); }
+}
+void launch_write_headers(const NodeParams& N, uint8_t* out, cudaStream_t s)
+{
+    { k_write_headers<<<(unsigned)((N.C.B + 127) / 128), 128, 0, s>>>(N, out); count_launch(); }
 }
 void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s)
 {

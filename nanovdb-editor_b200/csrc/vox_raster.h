@@ -24,6 +24,7 @@ struct EmitParams
     int64_t G;
     uint64_t NC;             // total columns
     float voxel_size;
+    const float* cloud_vs; // per-cloud voxel sizes (batched calls) or null
     uint64_t cap;
     uint64_t* status;
     uint32_t epoch;
@@ -50,9 +51,33 @@ struct RunParams
     uint16_t* vox_n;        // [V] leaf_n (position in the leaf) of each voxel
 };
 
+// per-cloud layout: every cloud gets its own self-contained grid (header,
+// node2 region, bbox, channels) in one output buffer; nodes, leaves and voxels
+// of all clouds sit in one array per level, ordered by cloud first
+struct CloudParams
+{
+    int64_t B;                   // clouds
+    uint32_t *upper_start, *lower_start, *leaf_start; // [B + 1] first node of each cloud per level
+    uint32_t* leaf_cloud;        // [L]
+    uint64_t* vstart;            // [B + 1] first voxel (run order) of each cloud
+    uint64_t* grid_off;          // [B + 1] byte offset of each cloud's grid; [B] = total bytes
+    uint64_t* value_base;        // [B + 1] first value of each cloud in value-concatenated arrays
+    uint64_t* node2_bytes;       // [B]
+    uint64_t *bbox_off, *rgba_off, *dens_off, *col_off; // [B] byte offsets in the output
+    int32_t* bbox;               // [B][6] active-voxel bbox
+    const float* cloud_vs;       // [B] or null (voxel_size for every cloud)
+    float voxel_size;
+    const int64_t* cloud_start;  // [B + 1] Gaussian ranges (device) or null for one cloud
+    const uint64_t* frag_off;    // exclusive scan of footprints (candidates per cloud)
+    const uint64_t* F_total;
+    int64_t G, P, V;
+    uint32_t node_order;
+};
+
 struct NodeParams
 {
     int64_t Lo, L;
+    CloudParams C;
     const uint32_t* lower_rank;
     const uint32_t* lower_cell;   // lower rank -> cell (root rank << 15 | upper_n)
     const uint32_t* root_of_rank; // root rank -> root_n
@@ -73,7 +98,6 @@ struct NodeParams
     uint32_t* leaf_slot; // optional [lower runs * 4096]: (lower run, lower_n) -> leaf index
     uint64_t* leaf_mask;
     int32_t* leaf_origin;
-    int32_t* bbox;
     uint64_t *upper_idx, *upper_addr, *upper_vidx;
     uint64_t *lower_idx, *lower_addr, *lower_vidx;
     uint64_t *leaf_idx, *leaf_addr, *leaf_vidx;
@@ -88,9 +112,8 @@ struct AccumParams
     const uint32_t* rank_to_lower; // lower rank -> lower node index
     const uint32_t* vox_leaf;
     const uint16_t* vox_n;
-    uint32_t* rgba8;
-    float* density;
-    float* color;
+    uint8_t* out;          // grid buffer: channels at the per-cloud offsets of NodeParams::C
+    const float* cloud_vs; // per-cloud voxel sizes or null
     int smooth; // differentiable channels (smooth_kernel, premultiplied colour)
 };
 
@@ -110,7 +133,10 @@ struct BwdParams
     const int32_t* lower_origin;
     const float* grad_density; // [value_count] or null
     const float* grad_color;   // [value_count][3] or null
+    const uint32_t* leaf_cloud;
+    const uint64_t* value_base; // values of cloud b start at value_base[b] in the grad arrays
     float voxel_size;
+    const float* cloud_vs;
     double* acc;               // [G][BWD_NACC], zeroed
 };
 
@@ -121,6 +147,8 @@ struct BwdFinalParams
     const float *means, *quats, *scales, *opacities, *colors; // the forward's inputs
     int raw;
     float voxel_size;
+    const float* cloud_vs;
+    const GaussRec* recs;
     float *d_means, *d_quats, *d_scales, *d_opacities, *d_colors; // any may be null
 };
 
@@ -143,8 +171,10 @@ void launch_lower_info(const NodeParams& N, cudaStream_t s);
 void launch_upper_info(const NodeParams& N, cudaStream_t s);
 void launch_leaf_tables(const NodeParams& N, const void* keys, int key64, cudaStream_t s);
 void launch_leaf_bbox(const NodeParams& N, cudaStream_t s);
+void launch_cloud_layout(const NodeParams& N, cudaStream_t s);
 void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s);
-void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* node2, cudaStream_t s);
+void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* out, cudaStream_t s);
+void launch_write_headers(const NodeParams& N, uint8_t* out, cudaStream_t s);
 void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s);
 
 } // namespace vox

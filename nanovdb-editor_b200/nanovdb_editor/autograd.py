@@ -83,12 +83,11 @@ def voxelize(means, quats, scales, opacities, colors, voxel_size: float, raw: bo
 
 
 def voxel_coords(vox: VoxContext, value_count: int, device) -> torch.Tensor:
-    """(i, j, k) of the active voxels of the context's last grid, row r = value index r + 2."""
-    V = max(int(value_count) - 2, 0)
-    out = torch.empty((V, 3), dtype=torch.int32, device=device)
-    if V:
+    """(i, j, k) of the active voxels of the context's last (single-cloud) grid, row r = value index r + 2."""
+    out = torch.full((max(int(value_count), 2), 3), -(1 << 31), dtype=torch.int32, device=device)
+    if value_count > 2:
         vox.voxel_coords(out)
-    return out
+    return out[2:]
 
 
 def pack_coords(ijk: torch.Tensor) -> torch.Tensor:

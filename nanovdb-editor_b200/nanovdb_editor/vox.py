@@ -93,6 +93,8 @@ def _lib():
         lib.vox_get_stats.argtypes = [c_void_p, POINTER(vox_stats_t)]
         lib.vox_global_scan_u64.restype = c_int
         lib.vox_global_scan_u64.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]
+        lib.vox_voxelize_batch.restype = c_int
+        lib.vox_voxelize_batch.argtypes = [c_void_p, POINTER(vox_gaussians_t), c_int64, c_void_p, c_void_p, c_float, c_uint32, POINTER(c_void_p), c_void_p, c_void_p]
         lib.vox_voxel_coords.restype = c_int
         lib.vox_voxel_coords.argtypes = [c_void_p, c_void_p, c_int64]
         lib.vox_backward.restype = c_int
@@ -170,6 +172,32 @@ class VoxContext:
         self.last_grid_bytes = int(nbytes.value)
         return int(ptr.value or 0), int(nbytes.value)
 
+    def voxelize_batch(self, means, quats, scales, opacities, colors, cloud_start, voxel_sizes, cull_scale=0.05, flags=0):
+        """Many clouds in one call (device tensors, concatenated).  cloud_start: host
+        int64 [B + 1]; voxel_sizes: host float32 [B].  Returns (device ptr, grid
+        offsets [B + 1], value offsets [B + 1]) - grid b is bytes [off[b], off[b + 1])."""
+        g = self._gauss(means, quats, scales, opacities, colors)
+        cs = np.ascontiguousarray(cloud_start, dtype=np.int64)
+        vs = np.ascontiguousarray(voxel_sizes, dtype=np.float32)
+        B = int(vs.shape[0])
+        if cs.shape[0] != B + 1:
+            raise PipelineError("voxelize_batch: cloud_start needs one more entry than voxel_sizes")
+        goff = np.zeros(B + 1, dtype=np.uint64)
+        voff = np.zeros(B + 1, dtype=np.uint64)
+        ptr = c_void_p()
+        self.generation += 1
+        rc = self.lib.vox_voxelize_batch(self.handle, byref(g), B, cs.ctypes.data, vs.ctypes.data, float(cull_scale), int(flags),
+                                         byref(ptr), goff.ctypes.data, voff.ctypes.data)
+        self._check(rc, "vox_voxelize_batch")
+        self.last_grid_bytes = int(goff[-1])
+        return int(ptr.value or 0), goff, voff
+
+    def grids(self, grid_offsets) -> list:
+        """Host copies of every cloud's grid of the last batched call."""
+        buf = np.empty(self.last_grid_bytes, dtype=np.uint8)
+        self._check(self.lib.vox_copy_grid(self.handle, buf.ctypes.data, buf.nbytes), "vox_copy_grid")
+        return [NodeGrid(buf[int(a) : int(b)]) for a, b in zip(grid_offsets[:-1], grid_offsets[1:])]
+
     def voxelize_host(self, means, quats, scales, opacities, colors, voxel_size, cull_scale=0.05, flags=0) -> NodeGrid:
         """numpy float32 arrays in, host grid out (copies counted in the call)."""
         arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (means, quats, scales, opacities, colors)]
@@ -191,7 +219,8 @@ class VoxContext:
         self._check(rc, "vox_backward")
 
     def voxel_coords(self, dst) -> None:
-        """Writes the active voxels' (i, j, k) into a CUDA int32 tensor [V, 3], row r = value index r + 2."""
+        """Writes the active voxels' (i, j, k) into a CUDA int32 tensor [value_count, 3], row = value index
+        (background rows untouched)."""
         self._check(self.lib.vox_voxel_coords(self.handle, _ptr(dst), int(dst.shape[0]) if dst.dim() > 1 else int(dst.numel()) // 3), "vox_voxel_coords")
 
     def grid_device(self, dst) -> None:

@@ -12,6 +12,9 @@ value distributions the workload definitions name:
                        in-plane and 0.005 along the normal, per-axis scales
                        exp(N(ln 0.003, 0.5)) with anisotropy capped at 20:1.
                        2M Gaussians at voxel 0.002 is the at-scale workload.
+* ``batch_clouds``     uneven batches: log-uniform cloud sizes and voxel sizes,
+                       1-16 clusters per cloud (256 clouds of 1k-200k Gaussians
+                       at voxel 0.002-0.02 is the batched workload).
 * ``pytest_cloud``     the 32-Gaussian cloud of the reference's pipeline test
                        (means N(0, 0.3), opacity logit 0.9, identity quaternions,
                        log-scale -3, SH0 0.5) at voxel 1/8.
@@ -122,6 +125,28 @@ def pytest_cloud(n: int = 32) -> GaussianCloud:
         opacities=(1.0 / (1.0 + np.exp(-logit.astype(np.float64)))).astype(np.float32),
         raw=[means, logit, quats, log_s, sh0, np.zeros(0, dtype=np.float32)],
     )
+
+
+def concat(clouds) -> GaussianCloud:
+    """One cloud of all clouds' Gaussians, in order."""
+    keys = ("means", "quats", "scales", "colors", "opacities")
+    return GaussianCloud(**{k: np.ascontiguousarray(np.concatenate([c[k] for c in clouds], axis=0)) for k in keys})
+
+
+def batch_clouds(count: int = 256, seed: int = 3, min_n: int = 1_000, max_n: int = 200_000,
+                 vs_min: float = 0.002, vs_max: float = 0.02, max_clusters: int = 16):
+    """Uneven batch: `count` clouds of log-uniform size in [min_n, max_n], each a
+    cluster_cloud with 1..max_clusters clusters and its own voxel size,
+    log-uniform in [vs_min, vs_max].  Returns (list of clouds, cloud_start int64
+    [count + 1], voxel_sizes float32 [count])."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(min_n), np.log(max_n), count)).astype(np.int64)
+    clusters = rng.integers(1, max_clusters + 1, count)
+    vs = np.exp(rng.uniform(np.log(vs_min), np.log(vs_max), count)).astype(np.float32)
+    clouds = [cluster_cloud(int(n), int(seed * 100003 + i), clusters=int(c)) for i, (n, c) in enumerate(zip(sizes, clusters))]
+    start = np.zeros(count + 1, dtype=np.int64)
+    start[1:] = np.cumsum(sizes)
+    return clouds, start, vs
 
 
 WORKLOADS = {
