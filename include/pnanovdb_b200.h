@@ -299,7 +299,7 @@ typedef struct vox_stats_t
     float ms_prep, ms_emit, ms_sort, ms_build, ms_accumulate, ms_total;
     int64_t kernel_launches; /* kernels this library launched in the call */
     float ms_backward;       /* last vox_backward */
-    int32_t reserved0;
+    int32_t sort_shape;      /* onesweep tile shape the sort used (tuned) */
 } vox_stats_t;
 
 /* One context per caller thread; it owns a CUDA stream on `device` and a

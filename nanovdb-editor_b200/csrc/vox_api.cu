@@ -424,6 +424,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
                                 ctx->tuning);
     ctx->sorted_in_alt = in_alt;
     ctx->stats.sort_passes = (key_bits + ctx->tuning.digit_bits - 1) / ctx->tuning.digit_bits;
+    ctx->stats.sort_shape = sort_shape_used(P_pairs, key64, ctx->tuning);
     const void* skeys = in_alt ? ctx->keys_alt.p : ctx->keys.p;
     const uint32_t* sids = (const uint32_t*)(in_alt ? ctx->ids_alt.p : ctx->ids.p);
     if (ctx->check_sort)
@@ -1010,7 +1011,7 @@ int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals,
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
     cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
-    SortTuning t = ctx->tuning;
+    SortTuning& t = ctx->tuning;
     int in_alt = sort_pairs_u64(d_keys, d_vals, (uint64_t*)ctx->prim_keys_alt.p, (uint32_t*)ctx->prim_vals_alt.p, n,
                                 (int)key_bit_count, ctx->sort_ws.p, &ctx->sort_epochs, (int*)(sc + SC_ERR),
                                 ctx->num_sms, s, t);

@@ -70,16 +70,26 @@ void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, 
 struct SortTuning
 {
     int digit_bits = 8; // radix bits per pass (<= 8)
+    int shape = -1;     // onesweep tile shape, -1 = tuned: fastest pass 0 per key width and size class
+    int best[2][40];    // tuner's choice per (64-bit keys, floor(log2 n)), -1 = not yet timed
+    SortTuning()
+    {
+        for (auto& r : best)
+            for (int& b : r)
+                b = -1;
+    }
 };
 size_t sort_workspace_bytes(int64_t n, int key_bytes);
 // Stable LSD sort of (key, value) pairs by key bits [0, key_bits).  Uses
 // keys_alt / vals_alt as ping-pong buffers; returns 0 if the result is in
 // keys / vals and 1 if it is in keys_alt / vals_alt.
 int sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, SortTuning& tune);
 int sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune);
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, SortTuning& tune);
 size_t sort_status_words(int64_t n);
+// shape index the sort of n pairs uses under `tune` (-1 before tuning)
+int sort_shape_used(int64_t n, int key64, const SortTuning& tune);
 
 // counts keys[i] < keys[i - 1] into *descents (validation)
 void check_sorted(const void* keys, int64_t n, int key64, uint64_t* descents, int num_sms, cudaStream_t s);

@@ -95,15 +95,19 @@ void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, 
 }
 
 // ===================================================================== sort
-// Tile: SORT_BLOCK threads x SORT_ITEMS keys.  One up-front pass computes the
+// Tile: block threads x items keys (SORT_SHAPES).  One up-front pass computes the
 // digit histograms of every pass (global counts are permutation-invariant);
 // each scatter pass then finds, per digit, the count in earlier tiles with a
 // decoupled look-back over 64-bit epoch-tagged words (55-bit counts).
-constexpr int SORT_BLOCK = 512;
-constexpr int SORT_WARPS = SORT_BLOCK / 32;
-constexpr int SORT_ITEMS = 16;
-constexpr int SORT_TILE = SORT_BLOCK * SORT_ITEMS;
 constexpr int SORT_MAX_PASSES = 8;
+struct SortShapeInfo
+{
+    int block, items, tile;
+};
+constexpr int SORT_NSHAPES = 5;
+constexpr SortShapeInfo SORT_SHAPES[SORT_NSHAPES] = { { 512, 16, 8192 }, { 256, 16, 4096 }, { 256, 12, 3072 },
+                                                      { 256, 8, 2048 }, { 512, 8, 4096 } };
+constexpr int SORT_TILE_MIN = 2048; // status words are sized for the smallest tile
 
 struct SortWs
 {
@@ -122,14 +126,14 @@ static size_t align256(size_t x)
 static SortWs carve(void* ws, int64_t n)
 {
     SortWs w;
-    w.tiles = (n + SORT_TILE - 1) / SORT_TILE;
+    w.tiles = (n + SORT_TILE_MIN - 1) / SORT_TILE_MIN;
     char* p = (char*)ws;
     w.hist = (uint32_t*)p;
     p += align256(sizeof(uint32_t) * SORT_MAX_PASSES * 256);
     w.base = (uint64_t*)p;
     p += align256(sizeof(uint64_t) * SORT_MAX_PASSES * 256);
     w.counters = (uint32_t*)p;
-    p += align256(sizeof(uint32_t) * SORT_MAX_PASSES);
+    p += align256(sizeof(uint32_t) * (SORT_MAX_PASSES + 1));
     w.status = (uint64_t*)p;
     return w;
 }
@@ -137,14 +141,14 @@ static SortWs carve(void* ws, int64_t n)
 size_t sort_workspace_bytes(int64_t n, int key_bytes)
 {
     (void)key_bytes;
-    int64_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
+    int64_t tiles = (n + SORT_TILE_MIN - 1) / SORT_TILE_MIN;
     return align256(sizeof(uint32_t) * SORT_MAX_PASSES * 256) + align256(sizeof(uint64_t) * SORT_MAX_PASSES * 256) +
-           align256(sizeof(uint32_t) * SORT_MAX_PASSES) + align256(sizeof(uint64_t) * (tiles + 1) * 256);
+           align256(sizeof(uint32_t) * (SORT_MAX_PASSES + 1)) + align256(sizeof(uint64_t) * (tiles + 1) * 256);
 }
 
 size_t sort_status_words(int64_t n)
 {
-    return (size_t)((n + SORT_TILE - 1) / SORT_TILE + 1) * 256;
+    return (size_t)((n + SORT_TILE_MIN - 1) / SORT_TILE_MIN + 1) * 256;
 }
 
 template <class K>
@@ -156,7 +160,7 @@ __device__ __forceinline__ uint32_t digit_of(K k, int shift, uint32_t mask)
 // up-front histogram of every pass's digit (per-CTA shared counters, then
 // one global atomic per bin); counts fit 32 bits for n < 2^32
 template <class K>
-__global__ void __launch_bounds__(SORT_BLOCK) k_sort_hist(const K* keys, int64_t n, int passes, int bits,
+__global__ void __launch_bounds__(512) k_sort_hist(const K* keys, int64_t n, int passes, int bits,
                                                             uint32_t* hist)
 {
     __shared__ uint32_t s_h[SORT_MAX_PASSES * 256];
@@ -188,26 +192,31 @@ __global__ void k_sort_bases(const uint32_t* hist, uint64_t* base, int passes)
     }
 }
 
-template <class K>
+// onesweep tile shapes: threads x keys per thread (x minimum resident CTAs,
+// which caps registers); the tuner times one pass of each and keeps the
+// fastest per key width and size class
+template <class K, int BLOCK, int ITEMS>
 struct SortSmem
 {
-    K keys[SORT_TILE];
-    uint32_t vals[SORT_TILE];
-    uint32_t warp_hist[SORT_WARPS][256];
+    K keys[BLOCK * ITEMS];
+    uint32_t vals[BLOCK * ITEMS];
+    uint32_t warp_hist[BLOCK / 32][256];
     uint32_t digit_excl[256];
     uint64_t gbase[256];
     uint64_t s_warp[33];
     uint32_t tile;
 };
 
-template <class K>
-__global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-                                                           K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
-                                                           int64_t n, int shift, int bits, const uint64_t* base,
-                                                           uint64_t* status, uint32_t epoch, uint32_t* counter, int* err)
+template <class K, int BLOCK, int ITEMS, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                                                          K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+                                                          int64_t n, int shift, int bits, const uint64_t* base,
+                                                          uint64_t* status, uint32_t epoch, uint32_t* counter, int* err)
 {
+    constexpr int TILE = BLOCK * ITEMS;
+    constexpr int WARPS = BLOCK / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
+    SortSmem<K, BLOCK, ITEMS>& S = *reinterpret_cast<SortSmem<K, BLOCK, ITEMS>*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t mask = (1u << bits) - 1u;
     const int radix = 1 << bits;
@@ -218,16 +227,16 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
         S.warp_hist[warp][i] = 0;
     __syncthreads();
     const int64_t tile = S.tile;
-    const int64_t tile_base = tile * SORT_TILE;
-    const int tile_count = (int)min((int64_t)SORT_TILE, n - tile_base);
+    const int64_t tile_base = tile * TILE;
+    const int tile_count = (int)min((int64_t)TILE, n - tile_base);
 
     // load: warp-contiguous chunks, item-major within a warp (stable order = (item, lane))
-    K k[SORT_ITEMS];
-    uint32_t v[SORT_ITEMS];
-    uint32_t rank[SORT_ITEMS];
-    const int64_t wbase = tile_base + (int64_t)warp * (32 * SORT_ITEMS);
+    K k[ITEMS];
+    uint32_t v[ITEMS];
+    uint32_t rank[ITEMS];
+    const int64_t wbase = tile_base + (int64_t)warp * (32 * ITEMS);
 #pragma unroll
-    for (int i = 0; i < SORT_ITEMS; i++)
+    for (int i = 0; i < ITEMS; i++)
     {
         int64_t idx = wbase + i * 32 + lane;
         if (idx < n)
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
     }
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int i = 0; i < SORT_ITEMS; i++)
+    for (int i = 0; i < ITEMS; i++)
     {
         int64_t idx = wbase + i * 32 + lane;
         bool valid = idx < n;
@@ -260,7 +269,7 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
     if (threadIdx.x < 256)
     {
         uint32_t run = 0;
-        for (int w = 0; w < SORT_WARPS; w++)
+        for (int w = 0; w < WARPS; w++)
         {
             uint32_t c = S.warp_hist[w][threadIdx.x];
             S.warp_hist[w][threadIdx.x] = run;
@@ -285,14 +294,14 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
 
     // scatter into shared memory in digit order
 #pragma unroll
-    for (int i = 0; i < SORT_ITEMS; i++)
+    for (int i = 0; i < ITEMS; i++)
     {
         int64_t idx = wbase + i * 32 + lane;
         if (idx < n)
         {
             uint32_t d = digit_of(k[i], shift, mask);
             uint32_t pos = S.digit_excl[d] + S.warp_hist[warp][d] + rank[i];
-            if (pos < (uint32_t)SORT_TILE)
+            if (pos < (uint32_t)TILE)
             {
                 S.keys[pos] = k[i];
                 S.vals[pos] = v[i];
@@ -302,7 +311,7 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < tile_count; i += SORT_BLOCK)
+    for (int i = threadIdx.x; i < tile_count; i += BLOCK)
     {
         K kk = S.keys[i];
         uint32_t d = digit_of(kk, shift, mask);
@@ -317,10 +326,43 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const K* __restrict__ k
     }
 }
 
+// one onesweep pass with shape `shape` (SORT_SHAPES)
+template <class K>
+static void onesweep_pass(int shape, const K* src_k, const uint32_t* src_v, K* dst_k, uint32_t* dst_v, int64_t n,
+                          int shift, int bits, const uint64_t* base, uint64_t* status, uint32_t epoch,
+                          uint32_t* counter, int* err, cudaStream_t s)
+{
+    const int64_t tiles = (n + SORT_SHAPES[shape].tile - 1) / SORT_SHAPES[shape].tile;
+#define VOX_ONESWEEP(B, I, M)                                                                                      \
+    {                                                                                                              \
+        const size_t smem = sizeof(SortSmem<K, B, I>);                                                             \
+        cudaFuncSetAttribute(k_onesweep<K, B, I, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+        k_onesweep<K, B, I, M><<<(unsigned)tiles, B, smem, s>>>(src_k, src_v, dst_k, dst_v, n, shift, bits, base, \
+                                                                 status, epoch, counter, err);                     \
+        count_launch();                                                                                            \
+    }
+    switch (shape)
+    {
+    case 0: VOX_ONESWEEP(512, 16, 1) break;
+    case 1: VOX_ONESWEEP(256, 16, 2) break;
+    case 2: VOX_ONESWEEP(256, 12, 3) break;
+    case 3: VOX_ONESWEEP(256, 8, 4) break;
+    default: VOX_ONESWEEP(512, 8, 2) break;
+    }
+#undef VOX_ONESWEEP
+}
+
+static int size_class(int64_t n)
+{
+    int c = 0;
+    while (c < 39 && (1ll << (c + 1)) <= n)
+        c++;
+    return c;
+}
+
 template <class K>
 static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                           void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s,
-                           const SortTuning& tune)
+                           void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, SortTuning& tune)
 {
     if (n <= 1 || key_bits <= 0)
         return 0;
@@ -330,25 +372,54 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
         passes = SORT_MAX_PASSES;
     SortWs w = carve(workspace, n);
     cudaMemsetAsync(w.hist, 0, sizeof(uint32_t) * SORT_MAX_PASSES * 256, s);
-    cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * SORT_MAX_PASSES, s);
+    cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * (SORT_MAX_PASSES + 1), s);
     int64_t hist_grid = (int64_t)num_sms * 4;
-    int64_t need = (n + SORT_BLOCK - 1) / SORT_BLOCK;
+    int64_t need = (n + 511) / 512;
     if (hist_grid > need)
         hist_grid = need;
-    { k_sort_hist<K><<<(unsigned)hist_grid, SORT_BLOCK, 0, s>>>(keys, n, passes, bits, w.hist); count_launch(); }
+    { k_sort_hist<K><<<(unsigned)hist_grid, 512, 0, s>>>(keys, n, passes, bits, w.hist); count_launch(); }
     { k_sort_bases<<<1, 256, 0, s>>>(w.hist, w.base, passes); count_launch(); }
-    const size_t smem = sizeof(SortSmem<K>);
-    cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t words = sort_status_words(n);
+    const int kw = sizeof(K) == 8 ? 1 : 0, sc = size_class(n);
+    int shape = tune.shape >= 0 && tune.shape < SORT_NSHAPES ? tune.shape : tune.best[kw][sc];
+    if (shape < 0)
+    {
+        // tuner: time pass 0 of every shape on this data (the output is rewritten below)
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best_ms = 1e30f;
+        shape = 0;
+        for (int t = 0; t < SORT_NSHAPES; t++)
+        {
+            uint32_t epoch = epochs->next(w.status, words, s);
+            cudaMemsetAsync(w.counters + SORT_MAX_PASSES, 0, sizeof(uint32_t), s);
+            cudaEventRecord(e0, s);
+            onesweep_pass<K>(t, keys, vals, keys_alt, vals_alt, n, 0, bits, w.base, w.status, epoch,
+                             w.counters + SORT_MAX_PASSES, err, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms)
+            {
+                best_ms = ms;
+                shape = t;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        tune.best[kw][sc] = shape;
+    }
     K* src_k = keys;
     uint32_t* src_v = vals;
     K* dst_k = keys_alt;
     uint32_t* dst_v = vals_alt;
-    const size_t words = sort_status_words(n);
     for (int p = 0; p < passes; p++)
     {
         uint32_t epoch = epochs->next(w.status, words, s);
-        { k_onesweep<K><<<(unsigned)w.tiles, SORT_BLOCK, smem, s>>>(src_k, src_v, dst_k, dst_v, n, p * bits, bits,
-                                                                   w.base + p * 256, w.status, epoch, w.counters + p, err); count_launch(); }
+        onesweep_pass<K>(shape, src_k, src_v, dst_k, dst_v, n, p * bits, bits, w.base + p * 256, w.status, epoch,
+                         w.counters + p, err, s);
         K* tk = src_k;
         src_k = dst_k;
         dst_k = tk;
@@ -359,14 +430,21 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     return (passes & 1) ? 1 : 0;
 }
 
+int sort_shape_used(int64_t n, int key64, const SortTuning& tune)
+{
+    if (tune.shape >= 0 && tune.shape < SORT_NSHAPES)
+        return tune.shape;
+    return n > 1 ? tune.best[key64 ? 1 : 0][size_class(n)] : -1;
+}
+
 int sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune)
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, SortTuning& tune)
 {
     return sort_pairs_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, key_bits, workspace, epochs, err, num_sms, s,
                                      tune);
 }
 int sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,
-                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, const SortTuning& tune)
+                   void* workspace, Epochs* epochs, int* err, int num_sms, cudaStream_t s, SortTuning& tune)
 {
     return sort_pairs_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, key_bits, workspace, epochs, err, num_sms, s,
                                      tune);

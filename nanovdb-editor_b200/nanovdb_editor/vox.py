@@ -65,7 +65,7 @@ class vox_stats_t(Structure):
         ("ms_total", c_float),
         ("kernel_launches", c_int64),
         ("ms_backward", c_float),
-        ("reserved0", c_int32),
+        ("sort_shape", c_int32),
     ]
 
     def as_dict(self) -> dict:
