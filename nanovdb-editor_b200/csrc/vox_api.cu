@@ -57,7 +57,11 @@ struct vox_context_t
     DevBuf lower_origin, lower_upper_n, upper_head, upper_scan, lower_parent, upper_root_n, upper_lostart;
     DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
     DevBuf vox_leaf, vox_n, rank_to_lower;
-    DevBuf emit_keys, emit_ids, leaf_slot, bwd_acc; // differentiable calls
+    DevBuf bwd_acc;                                 // differentiable calls
+    // leaf-granular pipeline
+    DevBuf lcols, lcol_off, lc_count, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask;
+    DevBuf s_rgba, s_dens, s_col, s_pairs, cand_cnt, cand_voff, vkeys, vslot, vpairs, pair_off, cand_vbase;
+    DevBuf partials, exp_keys, exp_ids;
     DevBuf cloud_start, cloud_vs, clouds;           // batched calls: inputs, per-cloud layout
     DevBuf order; // 9 node order arrays
     DevBuf grid;
@@ -85,6 +89,8 @@ struct vox_context_t
     uint32_t last_flags = 0;
     float last_voxel_size = 0.f;
     NodeParams last_N{};
+    LeafPassParams last_LP{};
+    uint64_t last_NLC = 0, last_Q = 0;
     const float* last_cloud_vs = nullptr;
     std::vector<uint64_t> h_grid_off, h_value_base; // per cloud, last call
 };
@@ -103,9 +109,13 @@ enum
     SC_ERR, // int in the low half
     SC_NC,  // emission columns
     SC_GRID_BYTES,
+    SC_NLC,  // leaf columns
+    SC_Q,    // (leaf, Gaussian) pairs
+    SC_NCL,  // candidate leaves
+    SC_NVOX, // active voxels from the leaf masks
     SC_BBOX, // 3 words (6 int32)
     SC_COUNT = SC_BBOX + 3,
-    SC_SCRATCH = 16
+    SC_SCRATCH = 24
 };
 
 static void set_error(vox_context_t* ctx, const char* fmt, ...)
@@ -343,93 +353,85 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     ctx->stats.key_bits = key_bits;
     cudaEventRecord(ctx->timers.ev[1], s);
 
-    // ---------------------------------------------------------------- emit
+    // ---------------------------------------------------------- leaf pairs
     RankTables T{ root_bits, root_prefix, lower_bits, lower_prefix };
     const size_t kb = key64 ? 8 : 4;
-    uint64_t cap = ctx->pair_cap;
-    if (cap == 0)
-        cap = F / 3 + 1024;
-    if (cap > F)
-        cap = F > 0 ? F : 1;
-    int64_t P_pairs = 0;
-    for (int attempt = 0; attempt < 2; attempt++)
+    const int leaf_key_bits = 12 + bits_for(NL > 1 ? NL : 2);
+    if (leaf_key_bits > 32)
     {
-        int64_t etiles = emit_tile_count(NC);
-        if (!ensure(ctx, ctx->keys, kb * cap) || !ensure(ctx, ctx->ids, 4 * cap) ||
-            !ensure(ctx, ctx->emit_status, sizeof(uint64_t) * (size_t)(etiles + 1)))
-            return VOX_ERR_MEMORY;
-        EmitParams E;
-        E.recs = recs;
-        E.col_off = col_off;
-        E.G = G;
-        E.NC = NC;
-        E.voxel_size = voxel_size;
-        E.cloud_vs = d_cloud_vs;
-        E.cap = cap;
-        E.status = (uint64_t*)ctx->emit_status.p;
-        E.epoch = ctx->emit_epochs.next(E.status, ctx->emit_status.cap / sizeof(uint64_t), s);
-        E.counter = d_counter;
-        E.total = sc + SC_P;
-        E.err = d_err;
-        E.check = ctx->check_emit;
-        if (key64)
-            launch_emit_u64(E, T, (uint64_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, ctx->num_sms, s);
-        else
-            launch_emit_u32(E, T, (uint32_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, ctx->num_sms, s);
-        rc = sync_scalars(ctx, "emit");
-        if (rc)
-            return rc;
-        P_pairs = (int64_t)ctx->hscal[SC_P];
-        if ((uint64_t)P_pairs <= cap)
-            break;
-        cap = (uint64_t)P_pairs + P_pairs / 16 + 1024;
-        // clear the capacity flag and retry once with the exact size
-        cudaMemsetAsync(d_err, 0, sizeof(int), s);
-    }
-    if ((uint64_t)P_pairs > cap)
-    {
-        set_error(ctx, "emit: pair buffer overflow");
-        return VOX_ERR_MEMORY;
-    }
-    if ((uint64_t)P_pairs >= 0xFFFFFFF0ull)
-    {
-        set_error(ctx, "emit: %lld pairs exceed the 32-bit pair index range", (long long)P_pairs);
+        set_error(ctx, "voxelize: %llu touched lower-node cells (128^3 voxels) exceed the 2^20 leaf keys hold",
+                  (unsigned long long)NL);
         return VOX_ERR_SIZE;
     }
-    ctx->pair_cap = cap;
-    ctx->stats.pairs = P_pairs;
-    ctx->last_P = P_pairs;
-    if (diff)
+    if (!ensure(ctx, ctx->lcols, 8 * (size_t)(G + 1)) || !ensure(ctx, ctx->lcol_off, 8 * (size_t)(G + 1)))
+        return VOX_ERR_MEMORY;
+    uint64_t* lcols = (uint64_t*)ctx->lcols.p;
+    uint64_t* lcol_off = (uint64_t*)ctx->lcol_off.p;
+    launch_leaf_cols(recs, G, lcols, s);
+    scan_exclusive_u64(lcols, lcol_off, G, 0, sc + SC_NLC, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
+                       d_counter, d_err, ctx->num_sms, s);
+    rc = sync_scalars(ctx, "leaf columns");
+    if (rc)
+        return rc;
+    const uint64_t NLC = ctx->hscal[SC_NLC];
+    if (!ensure(ctx, ctx->lc_count, 8 * (size_t)(NLC + 1)) || !ensure(ctx, ctx->lc_off, 8 * (size_t)(NLC + 1)) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words((int64_t)NLC + 1) * 2))
+        return VOX_ERR_MEMORY;
+    scan_status = (uint64_t*)ctx->scan_status.p;
+    scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    LeafEmitParams LE;
+    memset(&LE, 0, sizeof(LE));
+    LE.recs = recs;
+    LE.G = G;
+    LE.lcol_off = lcol_off;
+    LE.NLC = NLC;
+    LE.lc_count = (uint64_t*)ctx->lc_count.p;
+    LE.voxel_size = voxel_size;
+    LE.cloud_vs = d_cloud_vs;
+    LE.check = ctx->check_emit;
+    launch_leaf_emit(LE, T, false, s);
+    uint64_t* lc_off = (uint64_t*)ctx->lc_off.p;
+    scan_exclusive_u64(LE.lc_count, lc_off, (int64_t)NLC, 0, sc + SC_Q, scan_status,
+                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    rc = sync_scalars(ctx, "leaf pairs");
+    if (rc)
+        return rc;
+    const uint64_t Q = ctx->hscal[SC_Q];
+    if (Q >= 0xFFFFFFF0ull)
     {
-        // the adjoint walks the pairs in emission order (sorted by Gaussian id)
-        if (!ensure(ctx, ctx->emit_keys, kb * (size_t)(P_pairs + 1)) || !ensure(ctx, ctx->emit_ids, 4 * (size_t)(P_pairs + 1)))
-            return VOX_ERR_MEMORY;
-        cudaMemcpyAsync(ctx->emit_keys.p, ctx->keys.p, kb * (size_t)P_pairs, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(ctx->emit_ids.p, ctx->ids.p, 4 * (size_t)P_pairs, cudaMemcpyDeviceToDevice, s);
+        set_error(ctx, "voxelize: %llu (leaf, Gaussian) pairs exceed the 32-bit pair index range", (unsigned long long)Q);
+        return VOX_ERR_SIZE;
     }
+    if (!ensure(ctx, ctx->keys, 4 * (size_t)(Q + 1)) || !ensure(ctx, ctx->ids, 4 * (size_t)(Q + 1)) ||
+        !ensure(ctx, ctx->keys_alt, 4 * (size_t)(Q + 1)) || !ensure(ctx, ctx->ids_alt, 4 * (size_t)(Q + 1)) ||
+        !ensure(ctx, ctx->emit_gid, 4 * (size_t)(Q + 1)) ||
+        (ctx->check_emit && !ensure(ctx, ctx->emit_flag, (size_t)(Q + 1))) ||
+        !ensure(ctx, ctx->sort_ws, sort_workspace_bytes((int64_t)Q, 4)) || !ensure(ctx, ctx->lflags, 8 * (size_t)(Q + 1)) ||
+        !ensure(ctx, ctx->lpos, 8 * (size_t)(Q + 1)) || !ensure(ctx, ctx->cand_key, 4 * (size_t)(Q + 1)) ||
+        !ensure(ctx, ctx->cand_start, 4 * (size_t)(Q + 2)) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words((int64_t)Q + 1) * 2))
+        return VOX_ERR_MEMORY;
+    scan_status = (uint64_t*)ctx->scan_status.p;
+    scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    LE.lc_off = lc_off;
+    LE.keys = (uint32_t*)ctx->keys.p;
+    LE.vals = (uint32_t*)ctx->ids.p;
+    LE.emit_gid = (uint32_t*)ctx->emit_gid.p;
+    LE.emit_flag = ctx->check_emit ? (uint8_t*)ctx->emit_flag.p : nullptr;
+    launch_leaf_emit(LE, T, true, s);
     cudaEventRecord(ctx->timers.ev[2], s);
 
-    // ---------------------------------------------------------------- sort
-    if (!ensure(ctx, ctx->keys_alt, kb * (size_t)(P_pairs + 1)) || !ensure(ctx, ctx->ids_alt, 4 * (size_t)(P_pairs + 1)) ||
-        !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(P_pairs, (int)kb)))
-        return VOX_ERR_MEMORY;
-    int in_alt;
-    if (key64)
-        in_alt = sort_pairs_u64((uint64_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, (uint64_t*)ctx->keys_alt.p,
-                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, &ctx->sort_epochs, d_err, ctx->num_sms, s,
-                                ctx->tuning);
-    else
-        in_alt = sort_pairs_u32((uint32_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, (uint32_t*)ctx->keys_alt.p,
-                                (uint32_t*)ctx->ids_alt.p, P_pairs, key_bits, ctx->sort_ws.p, &ctx->sort_epochs, d_err, ctx->num_sms, s,
-                                ctx->tuning);
-    ctx->sorted_in_alt = in_alt;
-    ctx->stats.sort_passes = (key_bits + ctx->tuning.digit_bits - 1) / ctx->tuning.digit_bits;
-    ctx->stats.sort_shape = sort_shape_used(P_pairs, key64, ctx->tuning);
-    const void* skeys = in_alt ? ctx->keys_alt.p : ctx->keys.p;
-    const uint32_t* sids = (const uint32_t*)(in_alt ? ctx->ids_alt.p : ctx->ids.p);
+    // ------------------------------------------ sort by leaf key, candidates
+    const int in_alt = sort_pairs_u32((uint32_t*)ctx->keys.p, (uint32_t*)ctx->ids.p, (uint32_t*)ctx->keys_alt.p,
+                                      (uint32_t*)ctx->ids_alt.p, (int64_t)Q, leaf_key_bits, ctx->sort_ws.p,
+                                      &ctx->sort_epochs, d_err, ctx->num_sms, s, ctx->tuning);
+    ctx->stats.sort_passes = (leaf_key_bits + ctx->tuning.digit_bits - 1) / ctx->tuning.digit_bits;
+    ctx->stats.sort_shape = sort_shape_used((int64_t)Q, 0, ctx->tuning);
+    const uint32_t* lkeys = (const uint32_t*)(in_alt ? ctx->keys_alt.p : ctx->keys.p);
+    const uint32_t* lvals = (const uint32_t*)(in_alt ? ctx->ids_alt.p : ctx->ids.p);
     if (ctx->check_sort)
     {
-        check_sorted(skeys, P_pairs, key64, sc + SC_SCRATCH + 2, ctx->num_sms, s);
+        check_sorted(lkeys, (int64_t)Q, 0, sc + SC_SCRATCH + 2, ctx->num_sms, s);
         rc = sync_scalars(ctx, "sort");
         if (rc)
             return rc;
@@ -441,17 +443,85 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
             return VOX_ERR_CUDA;
         }
     }
+    uint64_t* lflags = (uint64_t*)ctx->lflags.p;
+    uint64_t* lpos = (uint64_t*)ctx->lpos.p;
+    launch_leaf_heads(lkeys, (int64_t)Q, lflags, s);
+    scan_exclusive_u64(lflags, lpos, (int64_t)Q, 0, sc + SC_NCL, scan_status,
+                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    if (Q == 0)
+        cudaMemsetAsync(ctx->cand_start.p, 0, 4, s);
+    launch_leaf_compact(lkeys, (int64_t)Q, lflags, lpos, (uint32_t*)ctx->cand_key.p, (uint32_t*)ctx->cand_start.p, s);
+    rc = sync_scalars(ctx, "candidate leaves");
+    if (rc)
+        return rc;
+    const int64_t NCL = (int64_t)ctx->hscal[SC_NCL];
+    if ((uint64_t)NCL * 512ull >= 0xFFFFFFF0ull)
+    {
+        set_error(ctx, "voxelize: %lld candidate leaves exceed the 2^23 the staging indices hold", (long long)NCL);
+        return VOX_ERR_SIZE;
+    }
     cudaEventRecord(ctx->timers.ev[3], s);
 
-    // ---------------------------------------------------------------- runs
-    const int64_t rtiles = runs_tile_count(P_pairs);
-    if (!ensure(ctx, ctx->vox_start, 4 * (size_t)(P_pairs + 2)) || !ensure(ctx, ctx->leaf_vstart, 4 * (size_t)(P_pairs + 2)) ||
+    // ------------------------------------------------------------ leaf walk
+    const size_t slots = 512 * (size_t)(NCL + 1);
+    if (!ensure(ctx, ctx->cand_mask, 64 * (size_t)(NCL + 1)) || !ensure(ctx, ctx->s_rgba, 4 * slots) ||
+        !ensure(ctx, ctx->s_dens, 4 * slots) || !ensure(ctx, ctx->s_col, 12 * slots) || !ensure(ctx, ctx->s_pairs, 4 * slots) ||
+        !ensure(ctx, ctx->cand_cnt, 8 * (size_t)(NCL + 1)) || !ensure(ctx, ctx->cand_voff, 8 * (size_t)(NCL + 1)) ||
+        !ensure(ctx, ctx->cand_vbase, 8 * (size_t)(NCL + 1)) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(NCL + 1) * 2))
+        return VOX_ERR_MEMORY;
+    scan_status = (uint64_t*)ctx->scan_status.p;
+    scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    LeafPassParams LP;
+    memset(&LP, 0, sizeof(LP));
+    LP.recs = recs;
+    LP.vals = lvals;
+    LP.emit_gid = (const uint32_t*)ctx->emit_gid.p;
+    LP.emit_flag = ctx->check_emit ? (const uint8_t*)ctx->emit_flag.p : nullptr;
+    LP.cand_key = (const uint32_t*)ctx->cand_key.p;
+    LP.cand_start = (const uint32_t*)ctx->cand_start.p;
+    LP.NCL = NCL;
+    LP.lower_cell = (const uint32_t*)ctx->lower_cell.p;
+    LP.root_of_rank = (const uint32_t*)ctx->root_of_rank.p;
+    LP.voxel_size = voxel_size;
+    LP.cloud_vs = d_cloud_vs;
+    LP.smooth = diff ? 1 : 0;
+    LP.cand_mask = (uint64_t*)ctx->cand_mask.p;
+    LP.s_rgba = (uint32_t*)ctx->s_rgba.p;
+    LP.s_dens = (float*)ctx->s_dens.p;
+    LP.s_col = (float*)ctx->s_col.p;
+    LP.s_pairs = (uint32_t*)ctx->s_pairs.p;
+    LP.total_pairs = sc + SC_P;
+    LP.err = d_err;
+    LP.cand_vbase = (const uint64_t*)ctx->cand_vbase.p;
+    LP.cand_voff = (const uint64_t*)ctx->cand_voff.p;
+    LP.key64 = key64;
+    launch_leaf_pass(LP, d_counter, ctx->num_sms, s);
+    cudaEventRecord(ctx->timers.ev[4], s);
+    launch_leaf_popc(LP.cand_mask, NCL, (uint64_t*)ctx->cand_cnt.p, s);
+    scan_exclusive_u64((const uint64_t*)ctx->cand_cnt.p, (uint64_t*)ctx->cand_voff.p, NCL, 0, sc + SC_NVOX, scan_status,
+                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    rc = sync_scalars(ctx, "leaf walk");
+    if (rc)
+        return rc;
+    const int64_t VX = (int64_t)ctx->hscal[SC_NVOX];
+    const int64_t P_pairs = (int64_t)ctx->hscal[SC_P];
+    ctx->stats.pairs = P_pairs;
+    ctx->last_P = P_pairs;
+    if (!ensure(ctx, ctx->vkeys, kb * (size_t)(VX + 1)) || !ensure(ctx, ctx->vslot, 4 * (size_t)(VX + 1)))
+        return VOX_ERR_MEMORY;
+    launch_voxel_keys(LP.cand_mask, LP.cand_key, LP.cand_voff, NCL, ctx->vkeys.p, key64, (uint32_t*)ctx->vslot.p, s);
+    const void* skeys = ctx->vkeys.p;
+
+    // ------------------------------------------- runs over the voxel keys
+    const int64_t rtiles = runs_tile_count(VX);
+    if (!ensure(ctx, ctx->vox_start, 4 * (size_t)(VX + 2)) || !ensure(ctx, ctx->leaf_vstart, 4 * (size_t)(VX + 2)) ||
         !ensure(ctx, ctx->lower_lstart, 4 * (size_t)(NL + 2)) || !ensure(ctx, ctx->lower_rank, 4 * (size_t)(NL + 2)) ||
         !ensure(ctx, ctx->run_status, sizeof(uint64_t) * 3 * (size_t)(rtiles + 1)) ||
-        !ensure(ctx, ctx->vox_leaf, 4 * (size_t)(P_pairs + 2)) || !ensure(ctx, ctx->vox_n, 2 * (size_t)(P_pairs + 2)))
+        !ensure(ctx, ctx->vox_leaf, 4 * (size_t)(VX + 2)) || !ensure(ctx, ctx->vox_n, 2 * (size_t)(VX + 2)))
         return VOX_ERR_MEMORY;
     RunParams Rp;
-    Rp.P = P_pairs;
+    Rp.P = VX;
     Rp.vox_start = (uint32_t*)ctx->vox_start.p;
     Rp.vox_leaf = (uint32_t*)ctx->vox_leaf.p;
     Rp.vox_n = (uint16_t*)ctx->vox_n.p;
@@ -464,7 +534,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     Rp.counter = d_counter;
     Rp.err = d_err;
     Rp.lower_cap = NL + 2;
-    if (P_pairs == 0)
+    if (VX == 0)
     {
         cudaMemsetAsync(Rp.vox_start, 0, 4, s);
         cudaMemsetAsync(Rp.leaf_vstart, 0, 4, s);
@@ -485,8 +555,6 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         !ensure(ctx, ctx->leaf_origin, 12 * (size_t)(L + 1)) || !ensure(ctx, ctx->rank_to_lower, 4 * (size_t)(NL + 1)) ||
         !ensure(ctx, ctx->order, 8 * 3 * (size_t)((Lo + 1) * 2 + (L + 1))) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(Lo + 1) * 2))
-        return VOX_ERR_MEMORY;
-    if (diff && !ensure(ctx, ctx->leaf_slot, 4 * 4096 * (size_t)(Lo + 1)))
         return VOX_ERR_MEMORY;
     // per-cloud tables: 3 x (B + 1) u32 starts, L u32 leaf clouds, 9 x (B + 1) u64 layout words, 6 B i32 bbox
     const size_t cl_u32 = 3 * (size_t)(B + 1), cl_u64 = 9 * (size_t)(B + 1);
@@ -515,7 +583,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     N.upper_count = sc + SC_U;
     N.leaf_lower = (uint32_t*)ctx->leaf_lower.p;
     N.leaf_lower_n = (uint32_t*)ctx->leaf_lower_n.p;
-    N.leaf_slot = diff ? (uint32_t*)ctx->leaf_slot.p : nullptr;
+    N.leaf_slot = nullptr;
     N.leaf_mask = (uint64_t*)ctx->leaf_mask.p;
     N.leaf_origin = (int32_t*)ctx->leaf_origin.p;
     uint64_t* ord = (uint64_t*)ctx->order.p;
@@ -578,19 +646,28 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     uint8_t* grid = (uint8_t*)ctx->grid.p;
     cudaMemsetAsync(grid, 0, grid_bytes, s);
     cudaMemsetAsync(N.leaf_mask, 0, 64 * (size_t)L, s);
-    cudaEventRecord(ctx->timers.ev[4], s);
-    AccumParams A;
-    A.recs = recs;
-    A.keys = skeys;
-    A.voxel_size = voxel_size;
-    A.V = V;
-    A.rank_to_lower = N.rank_to_lower;
-    A.vox_leaf = (const uint32_t*)ctx->vox_leaf.p;
-    A.vox_n = (const uint16_t*)ctx->vox_n.p;
-    A.out = grid;
-    A.cloud_vs = d_cloud_vs;
-    A.smooth = diff ? 1 : 0;
-    launch_accumulate(A, N, sids, key64, s);
+    if (!ensure(ctx, ctx->vpairs, 8 * (size_t)(V + 1)) || !ensure(ctx, ctx->pair_off, 8 * (size_t)(V + 1)) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(V + 1) * 2))
+        return VOX_ERR_MEMORY;
+    scan_status = (uint64_t*)ctx->scan_status.p;
+    scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    ValueParams VA;
+    VA.V = V;
+    VA.vslot = (const uint32_t*)ctx->vslot.p;
+    VA.s_rgba = LP.s_rgba;
+    VA.s_dens = LP.s_dens;
+    VA.s_col = LP.s_col;
+    VA.s_pairs = LP.s_pairs;
+    VA.vpairs = (uint64_t*)ctx->vpairs.p;
+    VA.cand_vbase = (uint64_t*)ctx->cand_vbase.p;
+    VA.vox_leaf = (const uint32_t*)ctx->vox_leaf.p;
+    VA.vox_n = (const uint16_t*)ctx->vox_n.p;
+    VA.out = grid;
+    launch_values(VA, N, s);
+    scan_exclusive_u64(VA.vpairs, (uint64_t*)ctx->pair_off.p, V, 0, sc + SC_SCRATCH + 3, scan_status,
+                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    N.C.pair_off = (const uint64_t*)ctx->pair_off.p;
+    N.C.P = P_pairs;
     cudaEventRecord(ctx->timers.ev[5], s);
     launch_leaf_bbox(N, s);
     launch_write_nodes(N, U, grid, s);
@@ -617,10 +694,10 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     st.value_count = (int64_t)value_count;
     st.grid_bytes = (int64_t)grid_bytes;
     st.ms_prep = elapsed(ctx->timers.ev[0], ctx->timers.ev[1]);
-    st.ms_emit = elapsed(ctx->timers.ev[1], ctx->timers.ev[2]);
-    st.ms_sort = elapsed(ctx->timers.ev[2], ctx->timers.ev[3]);
-    st.ms_build = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]);
-    st.ms_accumulate = elapsed(ctx->timers.ev[4], ctx->timers.ev[5]);
+    st.ms_emit = elapsed(ctx->timers.ev[1], ctx->timers.ev[2]);       // (leaf, Gaussian) pairs
+    st.ms_sort = elapsed(ctx->timers.ev[2], ctx->timers.ev[3]);       // sort + candidate leaves
+    st.ms_accumulate = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]); // leaf walk: test, RGBA8, float sums
+    st.ms_build = elapsed(ctx->timers.ev[4], ctx->timers.ev[6]);      // topology, values, node2
     st.ms_total = elapsed(ctx->timers.ev[0], ctx->timers.ev[6]);
     st.kernel_launches = launch_count() - launches0;
     ctx->last_G = G;
@@ -630,6 +707,10 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     ctx->last_voxel_size = voxel_size;
     ctx->last_cloud_vs = d_cloud_vs;
     ctx->last_N = N;
+    LP.pair_off = N.C.pair_off;
+    ctx->last_LP = LP;
+    ctx->last_NLC = NLC;
+    ctx->last_Q = Q;
     ctx->diff_ready = diff;
     return VOX_OK;
 }
@@ -662,34 +743,29 @@ static int run_backward(vox_context_t* ctx, const vox_gaussians_t* gs, const flo
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     const int64_t launches0 = launch_count();
-    if (!ensure(ctx, ctx->bwd_acc, sizeof(double) * BWD_NACC * (size_t)(G + 1)))
+    const uint64_t Q = ctx->last_Q;
+    if (!ensure(ctx, ctx->partials, sizeof(float) * BWD_NACC * (size_t)(Q + 1)))
         return VOX_ERR_MEMORY;
     cudaEventRecord(ctx->timers.ev[0], s);
-    cudaMemsetAsync(ctx->bwd_acc.p, 0, sizeof(double) * BWD_NACC * (size_t)G, s);
     cudaMemsetAsync((uint64_t*)ctx->scal.p + SC_ERR, 0, sizeof(uint64_t), s);
-    const NodeParams& N = ctx->last_N;
-    BwdParams B;
-    B.recs = (const GaussRec*)ctx->recs.p;
-    B.keys = ctx->emit_keys.p;
-    B.ids = (const uint32_t*)ctx->emit_ids.p;
-    B.P = ctx->last_P;
-    B.G = G;
-    B.rank_to_lower = N.rank_to_lower;
-    B.leaf_slot = N.leaf_slot;
-    B.leaf_vidx = N.leaf_vidx;
-    B.leaf_mask = N.leaf_mask;
-    B.lower_origin = N.lower_origin;
-    B.grad_density = grad_density;
-    B.grad_color = grad_color;
-    B.leaf_cloud = N.C.leaf_cloud;
-    B.value_base = N.C.value_base;
-    B.voxel_size = ctx->last_voxel_size;
-    B.cloud_vs = ctx->last_cloud_vs;
-    B.acc = (double*)ctx->bwd_acc.p;
+    float* partials = (float*)ctx->partials.p;
     if (grad_density || grad_color)
-        launch_bwd_pairs(B, ctx->key64, s);
+    {
+        LeafPassParams LP = ctx->last_LP;
+        LP.grad_density = grad_density;
+        LP.grad_color = grad_color;
+        LP.partials = partials;
+        launch_leaf_backward(LP, (uint32_t*)((uint64_t*)ctx->scal.p + SC_SCRATCH), ctx->num_sms, s);
+    }
+    else
+        cudaMemsetAsync(partials, 0, sizeof(float) * BWD_NACC * (size_t)Q, s);
     BwdFinalParams F;
-    F.acc = B.acc;
+    memset(&F, 0, sizeof(F));
+    F.partials = partials;
+    F.lcol_off = (const uint64_t*)ctx->lcol_off.p;
+    F.lc_off = (const uint64_t*)ctx->lc_off.p;
+    F.NLC = ctx->last_NLC;
+    F.Q = Q;
     F.G = G;
     F.means = gs->means;
     F.quats = gs->quats;
@@ -947,24 +1023,36 @@ int vox_copy_pairs(vox_context_t* ctx, uint64_t* keys, uint32_t* ids, int64_t ca
 {
     if (!ctx)
         return VOX_ERR_ARGS;
+    if (ctx->last_V < 0)
+    {
+        set_error(ctx, "vox_copy_pairs: no grid");
+        return VOX_ERR_ARGS;
+    }
     const int64_t P = ctx->last_P;
     if (capacity < P)
         return VOX_ERR_SIZE;
     if (P == 0)
         return VOX_OK;
     cudaSetDevice(ctx->device);
+    const size_t kb = ctx->key64 ? 8 : 4;
+    if (!ensure(ctx, ctx->exp_keys, kb * (size_t)P) || !ensure(ctx, ctx->exp_ids, 4 * (size_t)P))
+        return VOX_ERR_MEMORY;
+    // replay the leaf walk, writing every passing pair at its voxel's pair offset
+    LeafPassParams LP = ctx->last_LP;
+    LP.out_keys = ctx->exp_keys.p;
+    LP.out_ids = (uint32_t*)ctx->exp_ids.p;
+    launch_leaf_export(LP, (uint32_t*)((uint64_t*)ctx->scal.p + SC_SCRATCH), ctx->num_sms, ctx->stream);
     DevBuf tmp;
     if (!ensure(ctx, tmp, 8 * (size_t)P))
         return VOX_ERR_MEMORY;
-    const void* skeys = ctx->sorted_in_alt ? ctx->keys_alt.p : ctx->keys.p;
-    const void* sids = ctx->sorted_in_alt ? ctx->ids_alt.p : ctx->ids.p;
     k_export_keys<<<(unsigned)((P + 255) / 256), 256, 0, ctx->stream>>>(
-        skeys, ctx->key64, (const uint32_t*)ctx->lower_cell.p, (const uint32_t*)ctx->root_of_rank.p, P,
+        ctx->exp_keys.p, ctx->key64, (const uint32_t*)ctx->lower_cell.p, (const uint32_t*)ctx->root_of_rank.p, P,
         (uint64_t*)tmp.p);
+    count_launch();
     if (keys)
         cudaMemcpyAsync(keys, tmp.p, 8 * (size_t)P, cudaMemcpyDeviceToHost, ctx->stream);
     if (ids)
-        cudaMemcpyAsync(ids, sids, 4 * (size_t)P, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaMemcpyAsync(ids, ctx->exp_ids.p, 4 * (size_t)P, cudaMemcpyDeviceToHost, ctx->stream);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     cudaFree(tmp.p);
     if (e != cudaSuccess)

@@ -164,13 +164,29 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= F.G)
         return;
-    const double* A = F.acc + BWD_NACC * g;
     double a[BWD_NACC];
     bool any = false;
-    for (int i = 0; i < BWD_NACC; i++)
+    if (F.partials)
     {
-        a[i] = A[i];
-        any = any || a[i] != 0.0;
+        // the Gaussian's (leaf, Gaussian) pairs are emission indices [e0, e1)
+        const uint64_t c0 = F.lcol_off[g], c1 = g + 1 < F.G ? F.lcol_off[g + 1] : F.NLC;
+        const uint64_t e0 = c0 < F.NLC ? F.lc_off[c0] : F.Q, e1 = c1 < F.NLC ? F.lc_off[c1] : F.Q;
+        for (int i = 0; i < BWD_NACC; i++)
+            a[i] = 0.0;
+        for (uint64_t e = e0; e < e1; e++)
+            for (int i = 0; i < BWD_NACC; i++)
+                a[i] += (double)F.partials[e * BWD_NACC + i];
+        for (int i = 0; i < BWD_NACC; i++)
+            any = any || a[i] != 0.0;
+    }
+    else
+    {
+        const double* A = F.acc + BWD_NACC * g;
+        for (int i = 0; i < BWD_NACC; i++)
+        {
+            a[i] = A[i];
+            any = any || a[i] != 0.0;
+        }
     }
     float dmu[3] = { 0.f, 0.f, 0.f }, dq[4] = { 0.f, 0.f, 0.f, 0.f }, ds[3] = { 0.f, 0.f, 0.f }, dop = 0.f,
           dc[3] = { 0.f, 0.f, 0.f };

@@ -53,6 +53,15 @@ __device__ __forceinline__ uint32_t root_n_of(int32_t x, int32_t y, int32_t z)
     return ((((uint32_t)x & 0x1FFFFu) >> 12) << 10) | ((((uint32_t)y & 0x1FFFFu) >> 12) << 5) |
            (((uint32_t)z & 0x1FFFFu) >> 12);
 }
+// origin (voxel coordinates) of root tile root_n (its low 15 bits)
+__device__ __forceinline__ void root_tile_origin(uint32_t rn, int32_t o[3])
+{
+    int32_t x = (int32_t)((rn >> 10) & 31), y = (int32_t)((rn >> 5) & 31), z = (int32_t)(rn & 31);
+    o[0] = (x >= 16 ? x - 32 : x) * 4096;
+    o[1] = (y >= 16 ? y - 32 : y) * 4096;
+    o[2] = (z >= 16 ? z - 32 : z) * 4096;
+}
+
 // root tile index across clouds: cloud << 15 | root_n.  Ranks of touched root
 // tiles and lower cells are taken in this order, so the cloud is the most
 // significant part of every compact key.

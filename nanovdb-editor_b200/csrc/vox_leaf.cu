@@ -1,0 +1,817 @@
+// vox_leaf.cu - leaf-granular voxelization: (leaf, Gaussian) pairs, one CTA
+// per candidate leaf.
+//
+// The reference tests every (voxel, Gaussian) fragment of a Gaussian's bbox in
+// 8M-fragment windows and inserts passing voxels into its tree with atomics
+// (raster/Raster.cpp:420-558, gaussian_frag_alloc.slang, grid_build_*.slang,
+// gaussian_frag_color.slang).  Here the unit of sorting is the leaf (8^3
+// voxels, the node2 leaf of PNanoVDBExt.h:72-81):
+//   k_leaf_cols / k_leaf_emit   per Gaussian, the leaf cells of its bbox whose
+//       box may reach its 0.01-opacity ellipsoid (a conservative test in
+//       double), written as (leaf key, emission index) in Gaussian-major
+//       order; a stable sort by leaf key keeps each leaf's Gaussians in
+//       ascending id;
+//   k_leaf_heads / k_leaf_compact   runs of equal leaf keys -> candidate leaves;
+//   k_leaf_pass   one CTA per candidate leaf, one thread per voxel (two per
+//       thread): the CTA walks the leaf's Gaussians in ascending id and every
+//       thread runs the reference test (gaussian_frag_alloc.slang:84-162) on
+//       its voxels, keeps the RGBA8 maximum (gaussian_frag_color.slang:239-246)
+//       and sums the float channels in (voxel key, Gaussian id) order; the
+//       leaf's value mask comes from ballots;
+//   k_leaf_popc / k_voxel_keys   active voxels as sorted compact keys, which
+//       the run / node-table / node2-writer stage turns into the tree;
+//   k_values      staged values to their value index.
+// The adjoint (k_leaf_backward) and the sorted pair list (k_leaf_export)
+// replay the same walk.
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "vox_device.cuh"
+#include "vox_internal.h"
+#include "vox_raster.h"
+
+namespace vox
+{
+
+constexpr int LP_THREADS = 256; // two voxels per thread: leaf_n = t and t + 256
+constexpr int LP_CHUNK = 32;    // Gaussian records staged in shared memory per round
+
+__device__ __forceinline__ int64_t upper_bound_u64_l(const uint64_t* a, int64_t lo, int64_t hi, uint64_t v)
+{
+    while (lo < hi)
+    {
+        int64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------ emission ----
+__global__ void k_leaf_cols(const GaussRec* recs, int64_t G, uint64_t* lcols)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G)
+        return;
+    const GaussRec R = recs[g];
+    if (!R.q4.w)
+    {
+        lcols[g] = 0;
+        return;
+    }
+    const int32_t lx0 = R.q4.x >> 3, lx1 = (R.q4.x + R.q5.x - 1) >> 3;
+    const int32_t ly0 = R.q4.y >> 3, ly1 = (R.q4.y + R.q5.y - 1) >> 3;
+    lcols[g] = (uint64_t)(lx1 - lx0 + 1) * (uint64_t)(ly1 - ly0 + 1);
+}
+
+// May a voxel of the leaf at origin o pass the reference test?  The local AABB
+// of the leaf box (monotone-corner identity, in double) contains every voxel's
+// local AABB; the float test's rounding is bounded by delta = 1e-5 (1 + B), B
+// bounding the magnitudes it sums (as for the column bound of the emit test).
+__device__ __forceinline__ bool leaf_may_hit(const GaussRec& R, const RInv& M, float vsf, int32_t ox, int32_t oy,
+                                             int32_t oz)
+{
+    const double vs = vsf;
+    const int32_t o[3] = { ox, oy, oz };
+    const double mu[3] = { R.q0.x, R.q0.y, R.q0.z };
+    const double inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
+    double lo[3], hi[3], E[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const double w0 = (double)o[a] * vs, w1 = (double)(o[a] + 8) * vs;
+        lo[a] = w0 - mu[a];
+        hi[a] = w1 - mu[a];
+        E[a] = fmax(fabs(w0), fabs(w1)) + fabs(mu[a]) + vs;
+    }
+    double sum = 0.0, B = 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+    {
+        const double sc = (double)R.q0.w * inv_s[r];
+        double mn = 0.0, mx = 0.0, mag = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+        {
+            const double m = (double)M.m[r][a];
+            const double p0 = lo[a] * m, p1 = hi[a] * m;
+            mn += fmin(p0, p1);
+            mx += fmax(p0, p1);
+            mag += fabs(m) * E[a];
+        }
+        mn *= sc;
+        mx *= sc;
+        const double d = mn > 0.0 ? mn : (mx < 0.0 ? -mx : 0.0);
+        sum += d * d;
+        B = fmax(B, mag * sc);
+    }
+    const double bound = 1.0 + 1e-5 * (1.0 + B);
+    return sum < bound * bound;
+}
+
+__device__ __forceinline__ uint32_t leaf_key_of(const GaussRec& R, int32_t x, int32_t y, int32_t z,
+                                                const uint64_t* root_bits, const uint64_t* root_prefix,
+                                                const uint64_t* lower_bits, const uint64_t* lower_prefix)
+{
+    const uint64_t rr = bit_rank(root_bits, root_prefix, root_index(rec_cloud(R), x, y, z));
+    const uint64_t cell = rr * 32768ull + upper_n_of(x, y, z);
+    const uint64_t lr = bit_rank(lower_bits, lower_prefix, cell);
+    return (uint32_t)((lr << 12) | lower_n_of(x, y, z));
+}
+
+// one thread per leaf column (lx, ly) of a Gaussian's bbox, looping over lz
+template <bool WRITE>
+__global__ void __launch_bounds__(256) k_leaf_emit(LeafEmitParams P, RankTables T)
+{
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < P.NLC; t += (uint64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t g = upper_bound_u64_l(P.lcol_off, 0, P.G, t) - 1;
+        const GaussRec R = P.recs[g];
+        const RInv M = rinv_of(R);
+        const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+        const int32_t lx0 = R.q4.x >> 3, ly0 = R.q4.y >> 3, ly1 = (R.q4.y + R.q5.y - 1) >> 3;
+        const int32_t lz0 = R.q4.z >> 3, lz1 = (R.q4.z + R.q5.z - 1) >> 3;
+        const uint32_t Ly = (uint32_t)(ly1 - ly0 + 1);
+        const uint32_t local = (uint32_t)(t - P.lcol_off[g]);
+        const int32_t ox = (lx0 + (int32_t)(local / Ly)) * 8, oy = (ly0 + (int32_t)(local % Ly)) * 8;
+        uint64_t e = WRITE ? P.lc_off[t] : 0;
+        uint64_t n = 0;
+        for (int32_t lz = lz0; lz <= lz1; lz++)
+        {
+            const int32_t oz = lz * 8;
+            const bool hit = leaf_may_hit(R, M, vsf, ox, oy, oz);
+            if (hit || P.check)
+            {
+                if (WRITE)
+                {
+                    P.keys[e] = leaf_key_of(R, ox, oy, oz, T.root_bits, T.root_prefix, T.lower_bits, T.lower_prefix);
+                    P.vals[e] = (uint32_t)e;
+                    P.emit_gid[e] = (uint32_t)g;
+                    if (P.check)
+                        P.emit_flag[e] = hit ? 0 : 1;
+                    e++;
+                }
+                n++;
+            }
+        }
+        if (!WRITE)
+            P.lc_count[t] = n;
+    }
+}
+
+__global__ void k_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < Q)
+        flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1ull : 0ull;
+}
+
+__global__ void k_leaf_compact(const uint32_t* keys, int64_t Q, const uint64_t* flags, const uint64_t* pos,
+                               uint32_t* cand_key, uint32_t* cand_start)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Q)
+        return;
+    if (flags[i])
+    {
+        cand_key[pos[i]] = keys[i];
+        cand_start[pos[i]] = (uint32_t)i;
+    }
+    if (i == Q - 1)
+        cand_start[pos[i] + flags[i]] = (uint32_t)Q;
+}
+
+// ------------------------------------------------------------ leaf walk ----
+struct LeafSmem
+{
+    GaussRec rec[LP_CHUNK];
+    uint32_t gid[LP_CHUNK];
+    uint32_t eidx[LP_CHUNK];
+    uint8_t flag[LP_CHUNK];
+    uint64_t mask[8];
+    float red[LP_THREADS / 32][BWD_NACC];
+    uint32_t pairs;
+    uint32_t cand;
+};
+
+__device__ __forceinline__ void cand_origin(const LeafPassParams& P, uint32_t key, int32_t o[3])
+{
+    const uint32_t lr = key >> 12, ln = key & 4095u;
+    const uint32_t cell = P.lower_cell[lr];
+    const uint32_t un = cell & 32767u;
+    root_tile_origin(P.root_of_rank[cell >> 15] & 32767u, o);
+    o[0] += (int32_t)((un >> 10) & 31) * 128 + (int32_t)((ln >> 8) & 15) * 8;
+    o[1] += (int32_t)((un >> 5) & 31) * 128 + (int32_t)((ln >> 4) & 15) * 8;
+    o[2] += (int32_t)(un & 31) * 128 + (int32_t)(ln & 15) * 8;
+}
+
+__device__ __forceinline__ bool in_bbox(const GaussRec& R, int32_t x, int32_t y, int32_t z)
+{
+    return (uint32_t)(x - R.q4.x) < (uint32_t)R.q5.x && (uint32_t)(y - R.q4.y) < (uint32_t)R.q5.y &&
+           (uint32_t)(z - R.q4.z) < (uint32_t)R.q5.z;
+}
+
+// stage Gaussians [q0, q0 + cnt) of the sorted pair list
+__device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S, uint32_t q0, uint32_t cnt)
+{
+    const int t = threadIdx.x;
+    if (t < (int)cnt * 8)
+    {
+        const uint32_t j = (uint32_t)t >> 3, w = (uint32_t)t & 7u;
+        const uint32_t e = P.vals[q0 + j];
+        const uint32_t g = P.emit_gid[e];
+        reinterpret_cast<float4*>(&S.rec[j])[w] = reinterpret_cast<const float4*>(&P.recs[g])[w];
+        if (w == 0)
+        {
+            S.gid[j] = g;
+            S.eidx[j] = e;
+            S.flag[j] = P.emit_flag ? P.emit_flag[e] : 0;
+        }
+    }
+}
+
+// ------------------------------------------------------ forward leaf walk
+// Per chunk of LQ_CHUNK Gaussians (ascending id) staged in shared memory:
+//   bound  the k-range of each of the leaf's 64 voxel columns per Gaussian
+//          (column_interval, conservative), spread over the CTA;
+//   test   every thread runs the reference test on its two voxels inside the
+//          bounds and keeps a pass bit per Gaussian;
+//   queue  a block scan lays the passing (Gaussian, voxel) pairs out voxel by
+//          voxel, each voxel's pairs in ascending id;
+//   alpha  the RGBA8 byte and the float-channel alpha of every queued pair,
+//          one pair per thread (dense, whatever the pass pattern);
+//   sum    each thread folds its voxels' queued results in order.
+constexpr int LQ_CHUNK = 16;
+
+struct LeafQSmem
+{
+    GaussRec rec[LQ_CHUNK];
+    uint32_t gid[LQ_CHUNK];
+    uint8_t flag[LQ_CHUNK];
+    int8_t klo[LQ_CHUNK][64], khi[LQ_CHUNK][64];   // tested z range per (Gaussian, column), leaf-relative
+    int8_t bklo[LQ_CHUNK][64], bkhi[LQ_CHUNK][64]; // the bound itself (check mode)
+    uint16_t queue[LQ_CHUNK * 512];
+    float res_a[LQ_CHUNK * 512];
+    uint32_t res_rgba[LQ_CHUNK * 512];
+    uint64_t s_warp[33];
+    uint64_t mask[8];
+    uint32_t pairs, cand;
+};
+
+template <bool CHECK>
+__global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint32_t* counter)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    LeafQSmem& S = *reinterpret_cast<LeafQSmem*>(smem_raw);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int colA = (t >> 6) * 8 + ((t >> 3) & 7), colB = colA + 32, zr = t & 7;
+    while (true)
+    {
+        if (t == 0)
+        {
+            S.cand = atomicAdd(counter, 1u);
+            S.pairs = 0;
+        }
+        if (t < 8)
+            S.mask[t] = 0;
+        __syncthreads();
+        const int64_t c = S.cand;
+        if (c >= P.NCL)
+            break;
+        int32_t o[3];
+        cand_origin(P, P.cand_key[c], o);
+        const int32_t xa = o[0] + (t >> 6), y = o[1] + ((t >> 3) & 7), z = o[2] + zr, xb = xa + 4;
+        uint32_t rgba[2] = { 0u, 0u }, pc[2] = { 0u, 0u };
+        float ds[2] = { 0.f, 0.f }, cr[2] = { 0.f, 0.f }, cgr[2] = { 0.f, 0.f }, cb[2] = { 0.f, 0.f };
+        const uint32_t p0 = P.cand_start[c], p1 = P.cand_start[c + 1];
+        for (uint32_t q0 = p0; q0 < p1; q0 += LQ_CHUNK)
+        {
+            const uint32_t cnt = min((uint32_t)LQ_CHUNK, p1 - q0);
+            if (t < (int)cnt * 8)
+            {
+                const uint32_t j = (uint32_t)t >> 3, w = (uint32_t)t & 7u;
+                const uint32_t e = P.vals[q0 + j];
+                const uint32_t g = P.emit_gid[e];
+                reinterpret_cast<float4*>(&S.rec[j])[w] = reinterpret_cast<const float4*>(&P.recs[g])[w];
+                if (w == 0)
+                {
+                    S.gid[j] = g;
+                    S.flag[j] = P.emit_flag ? P.emit_flag[e] : 0;
+                }
+            }
+            __syncthreads();
+            // ---- bound: one (Gaussian, column) per thread
+            for (uint32_t idx = (uint32_t)t; idx < cnt * 64; idx += LP_THREADS)
+            {
+                const uint32_t j = idx >> 6, col = idx & 63u;
+                const GaussRec& R = S.rec[j];
+                const int32_t x = o[0] + (int32_t)(col >> 3), yy = o[1] + (int32_t)(col & 7u);
+                int lo = 1, hi = 0, blo = 1, bhi = 0;
+                if ((uint32_t)(x - R.q4.x) < (uint32_t)R.q5.x && (uint32_t)(yy - R.q4.y) < (uint32_t)R.q5.y)
+                {
+                    const RInv M = rinv_of(R);
+                    int32_t k0, k1;
+                    column_interval(R, M, rec_vs(R, P.voxel_size, P.cloud_vs), x, yy, k0, k1);
+                    blo = max(k0, o[2]) - o[2];
+                    bhi = min(k1, o[2] + 7) - o[2];
+                    if (CHECK)
+                    {
+                        lo = max(R.q4.z, o[2]) - o[2];
+                        hi = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
+                    }
+                    else
+                    {
+                        lo = blo;
+                        hi = bhi;
+                    }
+                }
+                S.klo[j][col] = (int8_t)max(min(lo, 8), -1);
+                S.khi[j][col] = (int8_t)max(min(hi, 8), -1);
+                if (CHECK)
+                {
+                    S.bklo[j][col] = (int8_t)max(min(blo, 8), -1);
+                    S.bkhi[j][col] = (int8_t)max(min(bhi, 8), -1);
+                }
+            }
+            __syncthreads();
+            // ---- test
+            uint32_t pa = 0, pb = 0;
+            for (uint32_t j = 0; j < cnt; j++)
+            {
+                const bool la = S.klo[j][colA] <= zr && zr <= S.khi[j][colA];
+                const bool lb = S.klo[j][colB] <= zr && zr <= S.khi[j][colB];
+                if (!(la || lb))
+                    continue;
+                const GaussRec& R = S.rec[j];
+                const RInv M = rinv_of(R);
+                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+                if (la && aabb_hits_unit_sphere(voxel_local_aabb(R, M, vsf, xa, y, z)))
+                {
+                    pa |= 1u << j;
+                    if (CHECK && (S.flag[j] || zr < S.bklo[j][colA] || zr > S.bkhi[j][colA]))
+                        atomicOr(P.err, ERR_BOUNDS); // a bound would have dropped a passing voxel
+                }
+                if (lb && aabb_hits_unit_sphere(voxel_local_aabb(R, M, vsf, xb, y, z)))
+                {
+                    pb |= 1u << j;
+                    if (CHECK && (S.flag[j] || zr < S.bklo[j][colB] || zr > S.bkhi[j][colB]))
+                        atomicOr(P.err, ERR_BOUNDS);
+                }
+            }
+            // ---- queue: voxel A's pairs, then voxel B's, each in ascending Gaussian id
+            uint64_t total;
+            const uint32_t base = (uint32_t)block_excl_scan_u64((uint64_t)(__popc(pa) + __popc(pb)), S.s_warp, total);
+            {
+                uint32_t e = base;
+                for (uint32_t m = pa; m; m &= m - 1)
+                    S.queue[e++] = (uint16_t)(((__ffs(m) - 1) << 9) | t);
+                for (uint32_t m = pb; m; m &= m - 1)
+                    S.queue[e++] = (uint16_t)(((__ffs(m) - 1) << 9) | (t + 256));
+            }
+            __syncthreads();
+            // ---- alpha, one queued pair per thread
+            for (uint32_t e = (uint32_t)t; e < (uint32_t)total; e += LP_THREADS)
+            {
+                const uint32_t q = S.queue[e];
+                const uint32_t j = q >> 9, n = q & 511u;
+                const GaussRec& R = S.rec[j];
+                const RInv M = rinv_of(R);
+                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+                const int32_t x = o[0] + (int32_t)(n >> 6), yy = o[1] + (int32_t)((n >> 3) & 7), zz = o[2] + (int32_t)(n & 7);
+                float cx0, cx1, cy0, cy1, cz0, cz1;
+                axis_corners(vsf, R.q0.x, x, cx0, cx1);
+                axis_corners(vsf, R.q0.y, yy, cy0, cy1);
+                axis_corners(vsf, R.q0.z, zz, cz0, cz1);
+                const float a8 = pair_alpha(R, aabb_from_corners(R, M, cx0, cx1, cy0, cy1, cz0, cz1));
+                float a;
+                if (P.smooth)
+                {
+                    SmoothTerms st;
+                    a = smooth_kernel(R, M, vsf, x, yy, zz, st);
+                }
+                else
+                {
+                    // float channels: corner offsets rounded once from double
+                    float sx0, sx1, sy0, sy1, sz0, sz1;
+                    axis_corners_stable(vsf, R.q0.x, x, sx0, sx1);
+                    axis_corners_stable(vsf, R.q0.y, yy, sy0, sy1);
+                    axis_corners_stable(vsf, R.q0.z, zz, sz0, sz1);
+                    const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
+                    a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
+                }
+                S.res_a[e] = a;
+                S.res_rgba[e] = pack_rgba8(R, a8);
+            }
+            __syncthreads();
+            // ---- sum in order
+            {
+                uint32_t e = base;
+                for (uint32_t m = pa; m; m &= m - 1, e++)
+                {
+                    const GaussRec& R = S.rec[__ffs(m) - 1];
+                    const float a = S.res_a[e];
+                    const uint32_t px = S.res_rgba[e];
+                    rgba[0] = px > rgba[0] ? px : rgba[0];
+                    ds[0] = VOX_FADD(ds[0], a);
+                    cr[0] = VOX_FADD(cr[0], VOX_FMUL(a, R.q7.x));
+                    cgr[0] = VOX_FADD(cgr[0], VOX_FMUL(a, R.q7.y));
+                    cb[0] = VOX_FADD(cb[0], VOX_FMUL(a, R.q7.z));
+                    pc[0]++;
+                }
+                for (uint32_t m = pb; m; m &= m - 1, e++)
+                {
+                    const GaussRec& R = S.rec[__ffs(m) - 1];
+                    const float a = S.res_a[e];
+                    const uint32_t px = S.res_rgba[e];
+                    rgba[1] = px > rgba[1] ? px : rgba[1];
+                    ds[1] = VOX_FADD(ds[1], a);
+                    cr[1] = VOX_FADD(cr[1], VOX_FMUL(a, R.q7.x));
+                    cgr[1] = VOX_FADD(cgr[1], VOX_FMUL(a, R.q7.y));
+                    cb[1] = VOX_FADD(cb[1], VOX_FMUL(a, R.q7.z));
+                    pc[1]++;
+                }
+            }
+            __syncthreads();
+        }
+        // value mask from ballots: voxel A of warp w is bit 32 (w & 1) + lane of word w >> 1
+        const uint32_t ba = __ballot_sync(0xffffffffu, pc[0] > 0), bb = __ballot_sync(0xffffffffu, pc[1] > 0);
+        uint32_t wp = pc[0] + pc[1];
+#pragma unroll
+        for (int off = 16; off; off >>= 1)
+            wp += __shfl_xor_sync(0xffffffffu, wp, off);
+        if (lane == 0)
+        {
+            atomicOr((unsigned long long*)&S.mask[warp >> 1], (unsigned long long)ba << (32 * (warp & 1)));
+            atomicOr((unsigned long long*)&S.mask[4 + (warp >> 1)], (unsigned long long)bb << (32 * (warp & 1)));
+            atomicAdd(&S.pairs, wp);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            if (!pc[h])
+                continue;
+            const uint64_t slot = (uint64_t)c * 512u + (uint32_t)(t + 256 * h);
+            P.s_rgba[slot] = rgba[h];
+            P.s_dens[slot] = ds[h];
+            float col[3] = { cr[h], cgr[h], cb[h] };
+            if (!P.smooth)
+                for (int k = 0; k < 3; k++)
+                    col[k] = ds[h] > 0.f ? VOX_FDIV(col[k], ds[h]) : 0.f;
+            P.s_col[3 * slot + 0] = col[0];
+            P.s_col[3 * slot + 1] = col[1];
+            P.s_col[3 * slot + 2] = col[2];
+            P.s_pairs[slot] = pc[h];
+        }
+        __syncthreads();
+        if (t < 8)
+            P.cand_mask[8 * (uint64_t)c + t] = S.mask[t];
+        if (t == 0 && S.pairs)
+            atomicAdd((unsigned long long*)P.total_pairs, (unsigned long long)S.pairs);
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ uint32_t mask_rank(const uint64_t* m, uint32_t n)
+{
+    uint32_t r = 0;
+    for (uint32_t w = 0; w < (n >> 6); w++)
+        r += __popcll(m[w]);
+    return r + __popcll(m[n >> 6] & ((1ull << (n & 63)) - 1ull));
+}
+
+// adjoint: per candidate leaf, per Gaussian, the sum of its pairs' terms over
+// the leaf's voxels (block reduction), stored by emission index
+__global__ void __launch_bounds__(LP_THREADS) k_leaf_backward(LeafPassParams P, uint32_t* counter)
+{
+    __shared__ LeafSmem S;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    while (true)
+    {
+        if (t == 0)
+            S.cand = atomicAdd(counter, 1u);
+        if (t < 8)
+            S.mask[t] = 0;
+        __syncthreads();
+        const int64_t c = S.cand;
+        if (c >= P.NCL)
+            break;
+        if (t < 8)
+            S.mask[t] = P.cand_mask[8 * (uint64_t)c + t];
+        int32_t o[3];
+        cand_origin(P, P.cand_key[c], o);
+        __syncthreads();
+        const int32_t xa = o[0] + (t >> 6), y = o[1] + ((t >> 3) & 7), z = o[2] + (t & 7), xb = xa + 4;
+        // upstream gradients of this thread's voxels (value-concatenated arrays)
+        float gd[2] = { 0.f, 0.f }, gc[2][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
+        bool act[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t n = (uint32_t)(t + 256 * h);
+            act[h] = (S.mask[n >> 6] >> (n & 63)) & 1ull;
+            if (act[h])
+            {
+                const uint64_t vi = P.cand_vbase[c] + mask_rank(S.mask, n);
+                if (P.grad_density)
+                    gd[h] = P.grad_density[vi];
+                if (P.grad_color)
+                    for (int k = 0; k < 3; k++)
+                        gc[h][k] = P.grad_color[3 * vi + k];
+            }
+        }
+        const uint32_t p0 = P.cand_start[c], p1 = P.cand_start[c + 1];
+        for (uint32_t q0 = p0; q0 < p1; q0 += LP_CHUNK)
+        {
+            const uint32_t cnt = min((uint32_t)LP_CHUNK, p1 - q0);
+            stage_chunk(P, S, q0, cnt);
+            __syncthreads();
+            for (uint32_t j = 0; j < cnt; j++)
+            {
+                const GaussRec& R = S.rec[j];
+                float acc[BWD_NACC];
+#pragma unroll
+                for (int i = 0; i < BWD_NACC; i++)
+                    acc[i] = 0.f;
+                const RInv M = rinv_of(R);
+                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const int32_t x = h ? xb : xa;
+                    if (!act[h] || !in_bbox(R, x, y, z))
+                        continue;
+                    if (!aabb_hits_unit_sphere(voxel_local_aabb(R, M, vsf, x, y, z)))
+                        continue;
+                    SmoothTerms st;
+                    const float Kw = smooth_kernel(R, M, vsf, x, y, z, st);
+                    if (!(st.e > SMOOTH_TAU))
+                        continue;
+                    const float GK = gd[h] + gc[h][0] * R.q7.x + gc[h][1] * R.q7.y + gc[h][2] * R.q7.z;
+                    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
+                    acc[0] += GK * st.E;
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        const float dz = -GK * st.e * st.z[r];
+                        const float du = dz * inv_s[r];
+                        acc[1 + r] += du;
+                        acc[4 + r] += dz * st.z[r];
+#pragma unroll
+                        for (int a = 0; a < 3; a++)
+                            acc[7 + 3 * r + a] += du * st.d[a];
+                    }
+                    acc[16] += Kw * gc[h][0];
+                    acc[17] += Kw * gc[h][1];
+                    acc[18] += Kw * gc[h][2];
+                }
+#pragma unroll
+                for (int i = 0; i < BWD_NACC; i++)
+                {
+                    float v = acc[i];
+#pragma unroll
+                    for (int off = 16; off; off >>= 1)
+                        v += __shfl_xor_sync(0xffffffffu, v, off);
+                    if (lane == 0)
+                        S.red[warp][i] = v;
+                }
+                __syncthreads();
+                if (t < BWD_NACC)
+                {
+                    float v = 0.f;
+                    for (int w = 0; w < LP_THREADS / 32; w++)
+                        v += S.red[w][t];
+                    P.partials[(uint64_t)S.eidx[j] * BWD_NACC + t] = v;
+                }
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// the sorted (voxel key, Gaussian id) pair list: per voxel, its Gaussians in
+// ascending id, at the voxel's pair offset
+__global__ void __launch_bounds__(LP_THREADS) k_leaf_export(LeafPassParams P, uint32_t* counter)
+{
+    __shared__ LeafSmem S;
+    const int t = threadIdx.x;
+    while (true)
+    {
+        if (t == 0)
+            S.cand = atomicAdd(counter, 1u);
+        __syncthreads();
+        const int64_t c = S.cand;
+        if (c >= P.NCL)
+            break;
+        if (t < 8)
+            S.mask[t] = P.cand_mask[8 * (uint64_t)c + t];
+        const uint32_t key = P.cand_key[c];
+        int32_t o[3];
+        cand_origin(P, key, o);
+        __syncthreads();
+        const int32_t xa = o[0] + (t >> 6), y = o[1] + ((t >> 3) & 7), z = o[2] + (t & 7), xb = xa + 4;
+        uint64_t dst[2] = { 0, 0 };
+        bool act[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const uint32_t n = (uint32_t)(t + 256 * h);
+            act[h] = (S.mask[n >> 6] >> (n & 63)) & 1ull;
+            if (act[h])
+                dst[h] = P.pair_off[P.cand_voff[c] + mask_rank(S.mask, n)];
+        }
+        const uint32_t p0 = P.cand_start[c], p1 = P.cand_start[c + 1];
+        for (uint32_t q0 = p0; q0 < p1; q0 += LP_CHUNK)
+        {
+            const uint32_t cnt = min((uint32_t)LP_CHUNK, p1 - q0);
+            stage_chunk(P, S, q0, cnt);
+            __syncthreads();
+            for (uint32_t j = 0; j < cnt; j++)
+            {
+                const GaussRec& R = S.rec[j];
+                const RInv M = rinv_of(R);
+                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const int32_t x = h ? xb : xa;
+                    if (!act[h] || !in_bbox(R, x, y, z))
+                        continue;
+                    if (!aabb_hits_unit_sphere(voxel_local_aabb(R, M, vsf, x, y, z)))
+                        continue;
+                    const uint64_t k = ((uint64_t)key << 9) | (uint32_t)(t + 256 * h);
+                    if (P.key64)
+                        ((uint64_t*)P.out_keys)[dst[h]] = k;
+                    else
+                        ((uint32_t*)P.out_keys)[dst[h]] = (uint32_t)k;
+                    P.out_ids[dst[h]] = S.gid[j];
+                    dst[h]++;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void k_leaf_popc(const uint64_t* cand_mask, int64_t NCL, uint64_t* counts)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= NCL)
+        return;
+    uint64_t n = 0;
+    for (int w = 0; w < 8; w++)
+        n += (uint64_t)__popcll(cand_mask[8 * c + w]);
+    counts[c] = n;
+}
+
+// one thread per (candidate leaf, mask word)
+template <class K>
+__global__ void k_voxel_keys(const uint64_t* cand_mask, const uint32_t* cand_key, const uint64_t* cand_voff,
+                             int64_t NCL, K* vkeys, uint32_t* vslot)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= NCL * 8)
+        return;
+    const int64_t c = t >> 3;
+    const int w = (int)(t & 7);
+    uint64_t base = cand_voff[c];
+    for (int q = 0; q < w; q++)
+        base += (uint64_t)__popcll(cand_mask[8 * c + q]);
+    uint64_t m = cand_mask[8 * c + w];
+    const uint64_t lk = (uint64_t)cand_key[c] << 9;
+    while (m)
+    {
+        const uint32_t n = (uint32_t)(64 * w + __ffsll((long long)m) - 1);
+        m &= m - 1;
+        vkeys[base] = (K)(lk | n);
+        vslot[base] = (uint32_t)(c * 512 + n);
+        base++;
+    }
+}
+
+// staged values -> value index of every active voxel; leaf masks
+__global__ void k_values(ValueParams A, NodeParams N)
+{
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= A.V)
+        return;
+    const uint32_t slot = A.vslot[v];
+    const uint32_t l = A.vox_leaf[v];
+    const uint32_t n = A.vox_n[v];
+    const uint64_t vi = N.leaf_vidx[l] + (uint64_t)(v - N.leaf_vstart[l]);
+    const uint32_t b = N.C.leaf_cloud[l];
+    ((uint32_t*)(A.out + N.C.rgba_off[b]))[vi] = A.s_rgba[slot];
+    ((float*)(A.out + N.C.dens_off[b]))[vi] = A.s_dens[slot];
+    float* col = (float*)(A.out + N.C.col_off[b]);
+    col[3 * vi + 0] = A.s_col[3 * (uint64_t)slot + 0];
+    col[3 * vi + 1] = A.s_col[3 * (uint64_t)slot + 1];
+    col[3 * vi + 2] = A.s_col[3 * (uint64_t)slot + 2];
+    A.vpairs[v] = A.s_pairs[slot];
+    if ((uint64_t)v == N.leaf_vstart[l])
+        A.cand_vbase[slot >> 9] = N.C.value_base[b] + N.leaf_vidx[l];
+    atomicOr((unsigned long long*)&N.leaf_mask[8 * (uint64_t)l + (n >> 6)], 1ull << (n & 63));
+}
+
+// ---------------------------------------------------------------- launch ----
+void launch_leaf_cols(const GaussRec* recs, int64_t G, uint64_t* lcols, cudaStream_t s)
+{
+    if (G <= 0)
+        return;
+    { k_leaf_cols<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(recs, G, lcols); count_launch(); }
+}
+
+void launch_leaf_emit(const LeafEmitParams& P, const RankTables& T, bool write, cudaStream_t s)
+{
+    if (P.NLC == 0)
+        return;
+    uint64_t blocks = (P.NLC + 255) / 256;
+    if (blocks > 148ull * 64)
+        blocks = 148ull * 64;
+    if (write)
+        { k_leaf_emit<true><<<(unsigned)blocks, 256, 0, s>>>(P, T); count_launch(); }
+    else
+        { k_leaf_emit<false><<<(unsigned)blocks, 256, 0, s>>>(P, T); count_launch(); }
+}
+
+void launch_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags, cudaStream_t s)
+{
+    if (Q <= 0)
+        return;
+    { k_leaf_heads<<<(unsigned)((Q + 255) / 256), 256, 0, s>>>(keys, Q, flags); count_launch(); }
+}
+
+void launch_leaf_compact(const uint32_t* keys, int64_t Q, const uint64_t* flags, const uint64_t* pos,
+                         uint32_t* cand_key, uint32_t* cand_start, cudaStream_t s)
+{
+    if (Q <= 0)
+        return;
+    { k_leaf_compact<<<(unsigned)((Q + 255) / 256), 256, 0, s>>>(keys, Q, flags, pos, cand_key, cand_start); count_launch(); }
+}
+
+static unsigned walk_grid(int64_t NCL, int num_sms)
+{
+    int64_t g = (int64_t)num_sms * 8;
+    return (unsigned)(g < NCL ? g : (NCL > 0 ? NCL : 1));
+}
+
+void launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s)
+{
+    if (P.NCL <= 0)
+        return;
+    cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+    const size_t smem = sizeof(LeafQSmem);
+    auto kern = P.emit_flag ? k_leaf_pass<true> : k_leaf_pass<false>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LP_THREADS, smem);
+    int64_t grid = (int64_t)num_sms * (per_sm > 0 ? per_sm : 1);
+    if (grid > P.NCL)
+        grid = P.NCL;
+    { kern<<<(unsigned)grid, LP_THREADS, smem, s>>>(P, counter); count_launch(); }
+}
+
+void launch_leaf_backward(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s)
+{
+    if (P.NCL <= 0)
+        return;
+    cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+    { k_leaf_backward<<<walk_grid(P.NCL, num_sms), LP_THREADS, 0, s>>>(P, counter); count_launch(); }
+}
+
+void launch_leaf_export(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s)
+{
+    if (P.NCL <= 0)
+        return;
+    cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+    { k_leaf_export<<<walk_grid(P.NCL, num_sms), LP_THREADS, 0, s>>>(P, counter); count_launch(); }
+}
+
+void launch_leaf_popc(const uint64_t* cand_mask, int64_t NCL, uint64_t* counts, cudaStream_t s)
+{
+    if (NCL <= 0)
+        return;
+    { k_leaf_popc<<<(unsigned)((NCL + 255) / 256), 256, 0, s>>>(cand_mask, NCL, counts); count_launch(); }
+}
+
+void launch_voxel_keys(const uint64_t* cand_mask, const uint32_t* cand_key, const uint64_t* cand_voff, int64_t NCL,
+                       void* vkeys, int key64, uint32_t* vslot, cudaStream_t s)
+{
+    if (NCL <= 0)
+        return;
+    const unsigned blocks = (unsigned)((NCL * 8 + 255) / 256);
+    if (key64)
+        { k_voxel_keys<uint64_t><<<blocks, 256, 0, s>>>(cand_mask, cand_key, cand_voff, NCL, (uint64_t*)vkeys, vslot); count_launch(); }
+    else
+        { k_voxel_keys<uint32_t><<<blocks, 256, 0, s>>>(cand_mask, cand_key, cand_voff, NCL, (uint32_t*)vkeys, vslot); count_launch(); }
+}
+
+void launch_values(const ValueParams& A, const NodeParams& N, cudaStream_t s)
+{
+    if (A.V <= 0)
+        return;
+    { k_values<<<(unsigned)((A.V + 255) / 256), 256, 0, s>>>(A, N); count_launch(); }
+}
+
+} // namespace vox

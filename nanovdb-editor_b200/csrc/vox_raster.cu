@@ -239,13 +239,6 @@ __global__ void __launch_bounds__(RUN_BLOCK) k_runs(RunParams Rp, const K* __res
 }
 
 // ------------------------------------------------------------- node tables ----
-__device__ __forceinline__ void root_tile_origin(uint32_t rn, int32_t o[3])
-{
-    int32_t x = (int32_t)((rn >> 10) & 31), y = (int32_t)((rn >> 5) & 31), z = (int32_t)(rn & 31);
-    o[0] = (x >= 16 ? x - 32 : x) * 4096;
-    o[1] = (y >= 16 ? y - 32 : y) * 4096;
-    o[2] = (z >= 16 ? z - 32 : z) * 4096;
-}
 
 // per lower node: origin, parent upper; per upper: root_n, lower range
 __global__ void k_lower_info(NodeParams N)
@@ -466,8 +459,10 @@ __global__ void k_write_headers(NodeParams N, uint8_t* out)
     if (vc > 2)
         for (int a = 0; a < 6; a++)
             h.bbox[a] = C.bbox[6 * b + a];
-    const uint64_t p0 = C.vstart[b] < (uint64_t)C.V ? N.vox_start[C.vstart[b]] : (uint64_t)C.P;
-    const uint64_t p1 = C.vstart[b + 1] < (uint64_t)C.V ? N.vox_start[C.vstart[b + 1]] : (uint64_t)C.P;
+    const uint64_t* poff = C.pair_off ? C.pair_off : (const uint64_t*)nullptr;
+    const uint64_t p0 = C.vstart[b] < (uint64_t)C.V ? (poff ? poff[C.vstart[b]] : N.vox_start[C.vstart[b]]) : (uint64_t)C.P;
+    const uint64_t p1 =
+        C.vstart[b + 1] < (uint64_t)C.V ? (poff ? poff[C.vstart[b + 1]] : N.vox_start[C.vstart[b + 1]]) : (uint64_t)C.P;
     h.pair_count = p1 - p0;
     const int64_t g0 = C.cloud_start ? C.cloud_start[b] : 0, g1 = C.cloud_start ? C.cloud_start[b + 1] : C.G;
     const uint64_t f0 = g0 < C.G ? C.frag_off[g0] : *C.F_total, f1 = g1 < C.G ? C.frag_off[g1] : *C.F_total;

@@ -70,6 +70,7 @@ struct CloudParams
     const int64_t* cloud_start;  // [B + 1] Gaussian ranges (device) or null for one cloud
     const uint64_t* frag_off;    // exclusive scan of footprints (candidates per cloud)
     const uint64_t* F_total;
+    const uint64_t* pair_off;    // [V] pairs before each voxel (exclusive scan)
     int64_t G, P, V;
     uint32_t node_order;
 };
@@ -143,6 +144,10 @@ struct BwdParams
 struct BwdFinalParams
 {
     const double* acc;
+    const float* partials;   // per-leaf partials by emission index (null: acc holds the sums)
+    const uint64_t* lcol_off; // [G] first leaf column of each Gaussian
+    const uint64_t* lc_off;   // [NLC] first emission index of each leaf column
+    uint64_t NLC, Q;
     int64_t G;
     const float *means, *quats, *scales, *opacities, *colors; // the forward's inputs
     int raw;
@@ -151,6 +156,89 @@ struct BwdFinalParams
     const GaussRec* recs;
     float *d_means, *d_quats, *d_scales, *d_opacities, *d_colors; // any may be null
 };
+
+// ---------------------------------------------------------------- leaves --
+// (leaf cell, Gaussian) pairs: every Gaussian emits the leaf cells (8^3
+// voxels) its ellipsoid may touch, in Gaussian-major order; sorted stably by
+// leaf key they give, per candidate leaf, its Gaussians in ascending id.
+struct LeafEmitParams
+{
+    const GaussRec* recs;
+    int64_t G;
+    const uint64_t* lcol_off; // [G] exclusive scan of per-Gaussian leaf columns (Lx * Ly)
+    uint64_t NLC;             // leaf columns
+    uint64_t* lc_count;       // count pass: pairs per leaf column
+    const uint64_t* lc_off;   // write pass: exclusive scan of lc_count
+    uint32_t* keys;           // leaf key: lower rank << 12 | lower_n
+    uint32_t* vals;           // emission index (the sort's value)
+    uint32_t* emit_gid;       // Gaussian of each emission index
+    uint8_t* emit_flag;       // check mode: 1 = the leaf test culls this pair
+    float voxel_size;
+    const float* cloud_vs;
+    int check;                // emit every bbox leaf, flag the ones the test culls
+};
+
+struct LeafPassParams
+{
+    const GaussRec* recs;
+    const uint32_t* vals;      // sorted leaf pairs' emission indices
+    const uint32_t* emit_gid;
+    const uint8_t* emit_flag;  // check mode or null
+    const uint32_t* cand_key;  // [NCL] candidate leaf keys
+    const uint32_t* cand_start;// [NCL + 1] first sorted pair of each candidate
+    int64_t NCL;
+    const uint32_t* lower_cell;
+    const uint32_t* root_of_rank;
+    float voxel_size;
+    const float* cloud_vs;
+    int smooth;
+    uint64_t* cand_mask;       // [NCL][8]
+    uint32_t* s_rgba;          // staging [NCL * 512]
+    float* s_dens;
+    float* s_col;              // [NCL * 512][3]
+    uint32_t* s_pairs;
+    uint64_t* total_pairs;
+    int* err;
+    // adjoint
+    const uint64_t* cand_vbase; // [NCL] value index of each candidate's first voxel
+    const float* grad_density;
+    const float* grad_color;
+    float* partials;            // [emission index][BWD_NACC]
+    // pair export
+    const uint64_t* cand_voff;  // [NCL] first voxel (run order) of each candidate
+    const uint64_t* pair_off;   // [V] first pair of each voxel
+    void* out_keys;             // compact voxel keys
+    uint32_t* out_ids;
+    int key64;
+};
+
+void launch_leaf_cols(const GaussRec* recs, int64_t G, uint64_t* lcols, cudaStream_t s);
+void launch_leaf_emit(const LeafEmitParams& P, const RankTables& T, bool write, cudaStream_t s);
+void launch_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags, cudaStream_t s);
+void launch_leaf_compact(const uint32_t* keys, int64_t Q, const uint64_t* flags, const uint64_t* pos,
+                         uint32_t* cand_key, uint32_t* cand_start, cudaStream_t s);
+void launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
+void launch_leaf_backward(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
+void launch_leaf_export(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
+void launch_leaf_popc(const uint64_t* cand_mask, int64_t NCL, uint64_t* counts, cudaStream_t s);
+void launch_voxel_keys(const uint64_t* cand_mask, const uint32_t* cand_key, const uint64_t* cand_voff, int64_t NCL,
+                       void* vkeys, int key64, uint32_t* vslot, cudaStream_t s);
+
+struct ValueParams
+{
+    int64_t V;
+    const uint32_t* vslot;     // [V] staging slot (candidate * 512 + leaf_n)
+    const uint32_t* s_rgba;
+    const float* s_dens;
+    const float* s_col;
+    const uint32_t* s_pairs;
+    uint64_t* vpairs;          // [V] pairs per voxel
+    uint64_t* cand_vbase;      // [NCL]
+    const uint32_t* vox_leaf;
+    const uint16_t* vox_n;
+    uint8_t* out;
+};
+void launch_values(const ValueParams& A, const NodeParams& N, cudaStream_t s);
 
 void launch_bwd_pairs(const BwdParams& B, int key64, cudaStream_t s);
 void launch_bwd_finalize(const BwdFinalParams& F, cudaStream_t s);
