@@ -243,7 +243,7 @@ __device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S
 //   alpha  the RGBA8 byte and the float-channel alpha of every queued pair,
 //          one pair per thread (dense, whatever the pass pattern);
 //   sum    each thread folds its voxels' queued results in order.
-constexpr int LQ_CHUNK = 16;
+constexpr int LQ_CHUNK = 8;
 
 struct LeafQSmem
 {
