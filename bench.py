@@ -463,7 +463,7 @@ def main():
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind},
             "stages_ms": stage_ms,
-            "counts": {k: st[k] for k in ("candidates", "pairs", "voxels", "uppers", "lowers", "leaves", "key_bits", "sort_passes", "sort_shape")},
+            "counts": {k: st[k] for k in ("candidates", "pairs", "voxels", "uppers", "lowers", "leaves", "key_bits", "sort_passes", "sort_shape", "leaf_pairs", "candidate_leaves")},
             "pairs_per_s": world * P / (ms * 1e-3),
             "voxels_per_s": world * st["voxels"] / (ms * 1e-3),
             "clocks": clk,

@@ -300,6 +300,8 @@ typedef struct vox_stats_t
     int64_t kernel_launches; /* kernels this library launched in the call */
     float ms_backward;       /* last vox_backward */
     int32_t sort_shape;      /* onesweep tile shape the sort used (tuned) */
+    int64_t leaf_pairs;      /* (leaf, Gaussian) pairs sorted */
+    int64_t candidate_leaves; /* leaves walked (some end up empty) */
 } vox_stats_t;
 
 /* One context per caller thread; it owns a CUDA stream on `device` and a

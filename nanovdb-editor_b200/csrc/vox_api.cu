@@ -455,6 +455,8 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     if (rc)
         return rc;
     const int64_t NCL = (int64_t)ctx->hscal[SC_NCL];
+    ctx->stats.leaf_pairs = (int64_t)Q;
+    ctx->stats.candidate_leaves = NCL;
     if ((uint64_t)NCL * 512ull >= 0xFFFFFFF0ull)
     {
         set_error(ctx, "voxelize: %lld candidate leaves exceed the 2^23 the staging indices hold", (long long)NCL);

@@ -234,15 +234,14 @@ __device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S
 
 // ------------------------------------------------------ forward leaf walk
 // Per chunk of LQ_CHUNK Gaussians (ascending id) staged in shared memory:
-//   bound  the k-range of each of the leaf's 64 voxel columns per Gaussian
-//          (column_interval, conservative), spread over the CTA;
-//   test   every thread runs the reference test on its two voxels inside the
-//          bounds and keeps a pass bit per Gaussian;
-//   queue  a block scan lays the passing (Gaussian, voxel) pairs out voxel by
-//          voxel, each voxel's pairs in ascending id;
+//   box    the part of each Gaussian's bbox inside the leaf;
+//   test   the boxes' voxels laid out densely, one candidate per thread, the
+//          reference test on each; passing (Gaussian, voxel) pairs go to a
+//          shared queue (any order);
 //   alpha  the RGBA8 byte and the float-channel alpha of every queued pair,
-//          one pair per thread (dense, whatever the pass pattern);
-//   sum    each thread folds its voxels' queued results in order.
+//          one pair per thread, into a per-(Gaussian, voxel) table;
+//   sum    each thread folds its two voxels' table entries in ascending
+//          Gaussian id, so every float sum has the order of a serial loop.
 constexpr int LQ_CHUNK = 8;
 
 struct LeafQSmem
@@ -250,14 +249,20 @@ struct LeafQSmem
     GaussRec rec[LQ_CHUNK];
     uint32_t gid[LQ_CHUNK];
     uint8_t flag[LQ_CHUNK];
-    int8_t klo[LQ_CHUNK][64], khi[LQ_CHUNK][64];   // tested z range per (Gaussian, column), leaf-relative
-    int8_t bklo[LQ_CHUNK][64], bkhi[LQ_CHUNK][64]; // the bound itself (check mode)
+    int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK]; // box origin, leaf-relative
+    uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK];               // box extents in y and z
+    uint32_t bdiv_y[LQ_CHUNK], bdiv_z[LQ_CHUNK];         // 65536 / extent, rounded up (exact division below 512)
+    uint32_t bvol[LQ_CHUNK];
+    // the x / y share of the reference test per (Gaussian, leaf column):
+    // rounded sums of the per-axis minimum / maximum corner products
+    float sxy_lo[3][LQ_CHUNK * 64], sxy_hi[3][LQ_CHUNK * 64];
+    float mz[LQ_CHUNK][3], inv_s[LQ_CHUNK][3], inv_ls[LQ_CHUNK], posz[LQ_CHUNK], vs[LQ_CHUNK];
     uint16_t queue[LQ_CHUNK * 512];
-    float res_a[LQ_CHUNK * 512];
-    uint32_t res_rgba[LQ_CHUNK * 512];
-    uint64_t s_warp[33];
+    float res_a[LQ_CHUNK][512];
+    uint32_t res_rgba[LQ_CHUNK][512];
+    uint32_t pbits[512];
     uint64_t mask[8];
-    uint32_t pairs, cand;
+    uint32_t qn, pairs, cand;
 };
 
 template <bool CHECK>
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LeafQSmem& S = *reinterpret_cast<LeafQSmem*>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int colA = (t >> 6) * 8 + ((t >> 3) & 7), colB = colA + 32, zr = t & 7;
+    const uint32_t lt = (1u << lane) - 1u;
     while (true)
     {
         if (t == 0)
@@ -282,7 +287,6 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
             break;
         int32_t o[3];
         cand_origin(P, P.cand_key[c], o);
-        const int32_t xa = o[0] + (t >> 6), y = o[1] + ((t >> 3) & 7), z = o[2] + zr, xb = xa + 4;
         uint32_t rgba[2] = { 0u, 0u }, pc[2] = { 0u, 0u };
         float ds[2] = { 0.f, 0.f }, cr[2] = { 0.f, 0.f }, cgr[2] = { 0.f, 0.f }, cb[2] = { 0.f, 0.f };
         const uint32_t p0 = P.cand_start[c], p1 = P.cand_start[c + 1];
@@ -301,78 +305,126 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
                     S.flag[j] = P.emit_flag ? P.emit_flag[e] : 0;
                 }
             }
+            S.pbits[t] = 0;
+            S.pbits[t + 256] = 0;
+            if (t == 0)
+                S.qn = 0;
             __syncthreads();
-            // ---- bound: one (Gaussian, column) per thread
+            // ---- box
+            if (t < (int)cnt)
+            {
+                const GaussRec& R = S.rec[t];
+                const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
+                const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
+                const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
+                const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
+                const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
+                S.bx0[t] = x0;
+                S.by0[t] = y0;
+                S.bz0[t] = z0;
+                S.bny[t] = ny;
+                S.bnz[t] = nz;
+                S.bdiv_y[t] = (65536u + ny - 1u) / ny;
+                S.bdiv_z[t] = (65536u + nz - 1u) / nz;
+                S.bvol[t] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny * nz;
+                const RInv M = rinv_of(R);
+                S.mz[t][0] = M.m[0][2];
+                S.mz[t][1] = M.m[1][2];
+                S.mz[t][2] = M.m[2][2];
+                S.inv_s[t][0] = R.q3.y;
+                S.inv_s[t][1] = R.q3.z;
+                S.inv_s[t][2] = R.q3.w;
+                S.inv_ls[t] = R.q0.w;
+                S.posz[t] = R.q0.z;
+                S.vs[t] = rec_vs(R, P.voxel_size, P.cloud_vs);
+            }
+            // ---- column shares (every column of the leaf, bbox or not: cheap)
             for (uint32_t idx = (uint32_t)t; idx < cnt * 64; idx += LP_THREADS)
             {
                 const uint32_t j = idx >> 6, col = idx & 63u;
                 const GaussRec& R = S.rec[j];
-                const int32_t x = o[0] + (int32_t)(col >> 3), yy = o[1] + (int32_t)(col & 7u);
-                int lo = 1, hi = 0, blo = 1, bhi = 0;
-                if ((uint32_t)(x - R.q4.x) < (uint32_t)R.q5.x && (uint32_t)(yy - R.q4.y) < (uint32_t)R.q5.y)
+                const RInv M = rinv_of(R);
+                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+                float cx0, cx1, cy0, cy1;
+                axis_corners(vsf, R.q0.x, o[0] + (int32_t)(col >> 3), cx0, cx1);
+                axis_corners(vsf, R.q0.y, o[1] + (int32_t)(col & 7u), cy0, cy1);
+#pragma unroll
+                for (int r = 0; r < 3; r++)
                 {
-                    const RInv M = rinv_of(R);
-                    int32_t k0, k1;
-                    column_interval(R, M, rec_vs(R, P.voxel_size, P.cloud_vs), x, yy, k0, k1);
-                    blo = max(k0, o[2]) - o[2];
-                    bhi = min(k1, o[2] + 7) - o[2];
-                    if (CHECK)
-                    {
-                        lo = max(R.q4.z, o[2]) - o[2];
-                        hi = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
-                    }
-                    else
-                    {
-                        lo = blo;
-                        hi = bhi;
-                    }
-                }
-                S.klo[j][col] = (int8_t)max(min(lo, 8), -1);
-                S.khi[j][col] = (int8_t)max(min(hi, 8), -1);
-                if (CHECK)
-                {
-                    S.bklo[j][col] = (int8_t)max(min(blo, 8), -1);
-                    S.bkhi[j][col] = (int8_t)max(min(bhi, 8), -1);
+                    float xn, xx, yn, yx;
+                    minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
+                    minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
+                    S.sxy_lo[r][idx] = VOX_FADD(xn, yn);
+                    S.sxy_hi[r][idx] = VOX_FADD(xx, yx);
                 }
             }
             __syncthreads();
-            // ---- test
-            uint32_t pa = 0, pb = 0;
-            for (uint32_t j = 0; j < cnt; j++)
+            uint32_t start[LQ_CHUNK + 1];
+            start[0] = 0;
+#pragma unroll
+            for (int j = 0; j < LQ_CHUNK; j++)
+                start[j + 1] = start[j] + (j < (int)cnt ? S.bvol[j] : 0u);
+            const uint32_t T = start[LQ_CHUNK];
+            // ---- test, one candidate per thread
+            for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
             {
-                const bool la = S.klo[j][colA] <= zr && zr <= S.khi[j][colA];
-                const bool lb = S.klo[j][colB] <= zr && zr <= S.khi[j][colB];
-                if (!(la || lb))
-                    continue;
-                const GaussRec& R = S.rec[j];
-                const RInv M = rinv_of(R);
-                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
-                if (la && aabb_hits_unit_sphere(voxel_local_aabb(R, M, vsf, xa, y, z)))
+                const uint32_t e = b0 + (uint32_t)t;
+                bool pass = false;
+                uint32_t entry = 0;
+                if (e < T)
                 {
-                    pa |= 1u << j;
-                    if (CHECK && (S.flag[j] || zr < S.bklo[j][colA] || zr > S.bkhi[j][colA]))
-                        atomicOr(P.err, ERR_BOUNDS); // a bound would have dropped a passing voxel
+                    int j = 0;
+#pragma unroll
+                    for (int q = 1; q < LQ_CHUNK; q++)
+                        j += e >= start[q] ? 1 : 0;
+                    const uint32_t local = e - start[j];
+                    const uint32_t rest = (local * S.bdiv_z[j]) >> 16;
+                    const uint32_t dz = local - rest * S.bnz[j];
+                    const uint32_t dx = (rest * S.bdiv_y[j]) >> 16;
+                    const uint32_t dy = rest - dx * S.bny[j];
+                    const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz = S.bz0[j] + (int32_t)dz;
+                    // the reference test with the staged x / y shares (bit-identical to
+                    // voxel_local_aabb + aabb_hits_unit_sphere)
+                    const uint32_t ci = (uint32_t)j * 64u + (uint32_t)(rx * 8 + ry);
+                    const float vsf = S.vs[j], pz = S.posz[j], il = S.inv_ls[j];
+                    const float v0 = (float)(o[2] + rz);
+                    const float v1 = VOX_FADD(v0, 1.f);
+                    const float c0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz);
+                    const float c1 = VOX_FSUB(VOX_FMUL(v1, vsf), pz);
+                    float d2 = 1.f;
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        float zn, zx;
+                        minmax_prod(c0, c1, S.mz[j][r], zn, zx);
+                        const float lo = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_lo[r][ci], zn), il), S.inv_s[j][r]);
+                        const float hi = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_hi[r][ci], zx), il), S.inv_s[j][r]);
+                        if (0.f < lo)
+                            d2 = VOX_FSUB(d2, VOX_FMUL(lo, lo));
+                        else if (0.f > hi)
+                            d2 = VOX_FSUB(d2, VOX_FMUL(hi, hi));
+                    }
+                    pass = d2 > 0.f;
+                    entry = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz);
+                    if (CHECK && pass && S.flag[j])
+                        atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
                 }
-                if (lb && aabb_hits_unit_sphere(voxel_local_aabb(R, M, vsf, xb, y, z)))
+                const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+                if (bal)
                 {
-                    pb |= 1u << j;
-                    if (CHECK && (S.flag[j] || zr < S.bklo[j][colB] || zr > S.bkhi[j][colB]))
-                        atomicOr(P.err, ERR_BOUNDS);
+                    const int leader = __ffs(bal) - 1;
+                    uint32_t qb = 0;
+                    if (lane == leader)
+                        qb = atomicAdd(&S.qn, (uint32_t)__popc(bal));
+                    qb = __shfl_sync(0xffffffffu, qb, leader);
+                    if (pass)
+                        S.queue[qb + __popc(bal & lt)] = (uint16_t)entry;
                 }
-            }
-            // ---- queue: voxel A's pairs, then voxel B's, each in ascending Gaussian id
-            uint64_t total;
-            const uint32_t base = (uint32_t)block_excl_scan_u64((uint64_t)(__popc(pa) + __popc(pb)), S.s_warp, total);
-            {
-                uint32_t e = base;
-                for (uint32_t m = pa; m; m &= m - 1)
-                    S.queue[e++] = (uint16_t)(((__ffs(m) - 1) << 9) | t);
-                for (uint32_t m = pb; m; m &= m - 1)
-                    S.queue[e++] = (uint16_t)(((__ffs(m) - 1) << 9) | (t + 256));
             }
             __syncthreads();
             // ---- alpha, one queued pair per thread
-            for (uint32_t e = (uint32_t)t; e < (uint32_t)total; e += LP_THREADS)
+            const uint32_t qn = S.qn;
+            for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
             {
                 const uint32_t q = S.queue[e];
                 const uint32_t j = q >> 9, n = q & 511u;
@@ -401,41 +453,33 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
                     const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
                     a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
                 }
-                S.res_a[e] = a;
-                S.res_rgba[e] = pack_rgba8(R, a8);
+                S.res_a[j][n] = a;
+                S.res_rgba[j][n] = pack_rgba8(R, a8);
+                atomicOr(&S.pbits[n], 1u << j);
             }
             __syncthreads();
-            // ---- sum in order
+            // ---- sum in ascending Gaussian id
+#pragma unroll
+            for (int h = 0; h < 2; h++)
             {
-                uint32_t e = base;
-                for (uint32_t m = pa; m; m &= m - 1, e++)
+                const uint32_t n = (uint32_t)(t + 256 * h);
+                for (uint32_t m = S.pbits[n]; m; m &= m - 1)
                 {
-                    const GaussRec& R = S.rec[__ffs(m) - 1];
-                    const float a = S.res_a[e];
-                    const uint32_t px = S.res_rgba[e];
-                    rgba[0] = px > rgba[0] ? px : rgba[0];
-                    ds[0] = VOX_FADD(ds[0], a);
-                    cr[0] = VOX_FADD(cr[0], VOX_FMUL(a, R.q7.x));
-                    cgr[0] = VOX_FADD(cgr[0], VOX_FMUL(a, R.q7.y));
-                    cb[0] = VOX_FADD(cb[0], VOX_FMUL(a, R.q7.z));
-                    pc[0]++;
-                }
-                for (uint32_t m = pb; m; m &= m - 1, e++)
-                {
-                    const GaussRec& R = S.rec[__ffs(m) - 1];
-                    const float a = S.res_a[e];
-                    const uint32_t px = S.res_rgba[e];
-                    rgba[1] = px > rgba[1] ? px : rgba[1];
-                    ds[1] = VOX_FADD(ds[1], a);
-                    cr[1] = VOX_FADD(cr[1], VOX_FMUL(a, R.q7.x));
-                    cgr[1] = VOX_FADD(cgr[1], VOX_FMUL(a, R.q7.y));
-                    cb[1] = VOX_FADD(cb[1], VOX_FMUL(a, R.q7.z));
-                    pc[1]++;
+                    const int j = __ffs(m) - 1;
+                    const float a = S.res_a[j][n];
+                    const uint32_t px = S.res_rgba[j][n];
+                    const GaussRec& R = S.rec[j];
+                    rgba[h] = px > rgba[h] ? px : rgba[h];
+                    ds[h] = VOX_FADD(ds[h], a);
+                    cr[h] = VOX_FADD(cr[h], VOX_FMUL(a, R.q7.x));
+                    cgr[h] = VOX_FADD(cgr[h], VOX_FMUL(a, R.q7.y));
+                    cb[h] = VOX_FADD(cb[h], VOX_FMUL(a, R.q7.z));
+                    pc[h]++;
                 }
             }
             __syncthreads();
         }
-        // value mask from ballots: voxel A of warp w is bit 32 (w & 1) + lane of word w >> 1
+        // value mask from ballots: voxel A (leaf_n = t) of warp w is bit 32 (w & 1) + lane of word w >> 1
         const uint32_t ba = __ballot_sync(0xffffffffu, pc[0] > 0), bb = __ballot_sync(0xffffffffu, pc[1] > 0);
         uint32_t wp = pc[0] + pc[1];
 #pragma unroll

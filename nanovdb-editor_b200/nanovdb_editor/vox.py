@@ -66,6 +66,8 @@ class vox_stats_t(Structure):
         ("kernel_launches", c_int64),
         ("ms_backward", c_float),
         ("sort_shape", c_int32),
+        ("leaf_pairs", c_int64),
+        ("candidate_leaves", c_int64),
     ]
 
     def as_dict(self) -> dict:
