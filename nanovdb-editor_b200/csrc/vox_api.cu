@@ -50,14 +50,13 @@ struct vox_context_t
     std::string last_error;
     std::vector<DevBuf*> bufs;
     // device buffers
-    DevBuf recs, footprints, frag_off, columns, col_off, root_bits, root_prefix, root_of_rank, lower_bits, lower_prefix, lower_cell;
-    DevBuf scan_status, emit_status, run_status;
+    DevBuf recs, footprints, frag_off, root_bits, root_prefix, root_of_rank, lower_bits, lower_prefix, lower_cell;
+    DevBuf scan_status, run_status;
     DevBuf keys, ids, keys_alt, ids_alt, sort_ws;
     DevBuf vox_start, leaf_vstart, lower_lstart, lower_rank;
     DevBuf lower_origin, lower_upper_n, upper_head, upper_scan, lower_parent, upper_root_n, upper_lostart;
     DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
     DevBuf vox_leaf, vox_n, rank_to_lower;
-    DevBuf bwd_acc;                                 // differentiable calls
     // leaf-granular pipeline
     DevBuf lcols, lcol_off, lc_count, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask;
     DevBuf s_rgba, s_dens, s_col, s_pairs, cand_cnt, cand_voff, vkeys, vslot, vpairs, pair_off, cand_vbase;
@@ -69,10 +68,9 @@ struct vox_context_t
     DevBuf hier_keys;
     DevBuf prim_keys_alt, prim_vals_alt; // ping-pong buffers of vox_radix_sort_key64
     uint64_t* hscal = nullptr; // pinned mirror
-    Epochs scan_epochs, emit_epochs, run_epochs, sort_epochs;
-    uint64_t pair_cap = 0;
+    Epochs scan_epochs, run_epochs, sort_epochs;
     int check_sort = 0; // VOX_CHECK_SORT=1: validate key order after every sort
-    int check_emit = 0; // VOX_CHECK_EMIT=1: test the candidates the column bound skips
+    int check_emit = 0; // VOX_CHECK_EMIT=1: also walk the leaves the leaf test culls; a pass there is an error
     int key64 = 0;
     int sorted_in_alt = 0;
     vox_stats_t stats{};
@@ -107,7 +105,6 @@ enum
     SC_LO,
     SC_U,
     SC_ERR, // int in the low half
-    SC_NC,  // emission columns
     SC_GRID_BYTES,
     SC_NLC,  // leaf columns
     SC_Q,    // (leaf, Gaussian) pairs
@@ -269,8 +266,6 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     if (!ensure(ctx, ctx->recs, sizeof(GaussRec) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->footprints, sizeof(uint64_t) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->frag_off, sizeof(uint64_t) * (size_t)(G + 1)) ||
-        !ensure(ctx, ctx->columns, sizeof(uint64_t) * (size_t)(G + 1)) ||
-        !ensure(ctx, ctx->col_off, sizeof(uint64_t) * (size_t)(G + 1)) ||
         !ensure(ctx, ctx->root_bits, sizeof(uint64_t) * 512 * B) || !ensure(ctx, ctx->root_prefix, sizeof(uint64_t) * 512 * B) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(G > 512 * B ? G : 512 * B) * 2))
         return VOX_ERR_MEMORY;
@@ -288,8 +283,6 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     GaussRec* recs = (GaussRec*)ctx->recs.p;
     uint64_t* footprints = (uint64_t*)ctx->footprints.p;
     uint64_t* frag_off = (uint64_t*)ctx->frag_off.p;
-    uint64_t* columns = (uint64_t*)ctx->columns.p;
-    uint64_t* col_off = (uint64_t*)ctx->col_off.p;
     uint64_t* root_bits = (uint64_t*)ctx->root_bits.p;
     uint64_t* root_prefix = (uint64_t*)ctx->root_prefix.p;
     cudaMemsetAsync(root_bits, 0, sizeof(uint64_t) * 512 * B, s);
@@ -306,12 +299,10 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     P.cloud_start = d_cloud_start;
     P.cloud_vs = d_cloud_vs;
     P.clouds = B;
-    launch_prep(P, recs, footprints, columns, root_bits, d_err, s);
+    launch_prep(P, recs, footprints, root_bits, d_err, s);
     uint64_t* scan_status = (uint64_t*)ctx->scan_status.p;
     size_t scan_words = ctx->scan_status.cap / sizeof(uint64_t);
     scan_exclusive_u64(footprints, frag_off, G, 0, sc + SC_F, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
-                       d_counter, d_err, ctx->num_sms, s);
-    scan_exclusive_u64(columns, col_off, G, 0, sc + SC_NC, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
                        d_counter, d_err, ctx->num_sms, s);
     scan_exclusive_u64(root_bits, root_prefix, 512 * B, 1, sc + SC_NROOT, scan_status,
                        ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
@@ -323,7 +314,6 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     if (!ensure(ctx, ctx->root_of_rank, sizeof(uint32_t) * (NR + 1)))
         return VOX_ERR_MEMORY;
     launch_invert_bits(root_bits, root_prefix, 512 * B, (uint32_t*)ctx->root_of_rank.p, s);
-    const uint64_t NC = ctx->hscal[SC_NC];
     ctx->stats.candidates = (int64_t)F;
 
     // ------------------------------------------------------- lower ranks
@@ -585,7 +575,6 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     N.upper_count = sc + SC_U;
     N.leaf_lower = (uint32_t*)ctx->leaf_lower.p;
     N.leaf_lower_n = (uint32_t*)ctx->leaf_lower_n.p;
-    N.leaf_slot = nullptr;
     N.leaf_mask = (uint64_t*)ctx->leaf_mask.p;
     N.leaf_origin = (int32_t*)ctx->leaf_origin.p;
     uint64_t* ord = (uint64_t*)ctx->order.p;
@@ -866,15 +855,20 @@ void vox_context_destroy(vox_context_t* ctx)
         return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf* all[] = { &ctx->recs, &ctx->footprints, &ctx->frag_off, &ctx->columns, &ctx->col_off, &ctx->root_bits, &ctx->root_prefix,
+    DevBuf* all[] = { &ctx->recs, &ctx->footprints, &ctx->frag_off, &ctx->root_bits, &ctx->root_prefix,
                       &ctx->root_of_rank, &ctx->lower_bits, &ctx->lower_prefix, &ctx->lower_cell, &ctx->scan_status,
-                      &ctx->emit_status, &ctx->run_status, &ctx->keys, &ctx->ids, &ctx->keys_alt, &ctx->ids_alt,
+                      &ctx->run_status, &ctx->keys, &ctx->ids, &ctx->keys_alt, &ctx->ids_alt,
                       &ctx->sort_ws, &ctx->vox_start, &ctx->leaf_vstart, &ctx->lower_lstart, &ctx->lower_rank,
                       &ctx->lower_origin, &ctx->lower_upper_n, &ctx->upper_head, &ctx->upper_scan,
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
-                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt };
+                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->cloud_start,
+                      &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_off,
+                      &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
+                      &ctx->cand_mask, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
+                      &ctx->cand_voff, &ctx->vkeys, &ctx->vslot, &ctx->vpairs, &ctx->pair_off, &ctx->cand_vbase,
+                      &ctx->partials, &ctx->exp_keys, &ctx->exp_ids };
     for (DevBuf* b : all)
         if (b->p)
             cudaFree(b->p);

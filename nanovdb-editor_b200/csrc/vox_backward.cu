@@ -16,12 +16,11 @@
 // chained through the rotation of gaussian_prim.slang:83-90, the quaternion
 // normalisation, exp, the sigmoid and SH0 of raster/RasterUtils.cpp:59-117.
 //
-// k_bwd_pairs walks the pair list in emission order, which is sorted by
-// Gaussian id, so the pairs of one Gaussian are contiguous: each warp owns a
-// contiguous range, keeps the 19 per-Gaussian sums in registers, and reduces
-// them across the warp once per Gaussian segment.  A segment that lies wholly
-// inside one warp's range is stored; one cut by a range boundary is added with
-// FP64 atomics.  Nothing is stored per pair.
+// k_leaf_backward (vox_leaf.cu) replays the forward leaf walk: per candidate
+// leaf and Gaussian, the terms above summed over the leaf's voxels (a block
+// reduction) are stored by the pair's emission index; k_bwd_finalize sums a
+// Gaussian's partials (its emission indices are contiguous) in FP64 and
+// chains them.  No atomics, nothing stored per voxel pair.
 #include <cstdio>
 #include <cuda_runtime.h>
 
@@ -32,132 +31,6 @@
 namespace vox
 {
 
-constexpr int BWD_BLOCK = 256;
-constexpr int BWD_RANGE = 1024; // pairs per warp
-constexpr unsigned FULL = 0xffffffffu;
-
-template <class K>
-__device__ __forceinline__ void pair_adjoint(const BwdParams& B, uint64_t key, uint32_t gid, float (&c)[BWD_NACC])
-{
-    const uint32_t lr = (uint32_t)(key >> 21), ln = (uint32_t)(key >> 9) & 4095u, vn = (uint32_t)key & 511u;
-    const uint32_t lo = B.rank_to_lower[lr];
-    const uint32_t l = B.leaf_slot[(uint64_t)lo * 4096u + ln];
-    const uint64_t* m = B.leaf_mask + 8ull * l;
-    uint64_t below = 0;
-    for (uint32_t w = 0; w < (vn >> 6); w++)
-        below += (uint64_t)__popcll(m[w]);
-    below += (uint64_t)__popcll(m[vn >> 6] & ((1ull << (vn & 63)) - 1ull));
-    // value index in the value-concatenated upstream arrays (clouds back to back)
-    const uint64_t vi = B.value_base[B.leaf_cloud[l]] + B.leaf_vidx[l] + below;
-    const int32_t x = B.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8 + (int32_t)(vn >> 6);
-    const int32_t y = B.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8 + (int32_t)((vn >> 3) & 7);
-    const int32_t z = B.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8 + (int32_t)(vn & 7);
-    const GaussRec R = B.recs[gid];
-    const RInv M = rinv_of(R);
-    SmoothTerms t;
-    const float Kw = smooth_kernel(R, M, rec_vs(R, B.voxel_size, B.cloud_vs), x, y, z, t);
-    if (!(t.e > SMOOTH_TAU))
-        return;
-    const float gd = B.grad_density ? B.grad_density[vi] : 0.f;
-    float gc[3] = { 0.f, 0.f, 0.f };
-    if (B.grad_color)
-    {
-        gc[0] = B.grad_color[3 * vi + 0];
-        gc[1] = B.grad_color[3 * vi + 1];
-        gc[2] = B.grad_color[3 * vi + 2];
-    }
-    const float GK = gd + gc[0] * R.q7.x + gc[1] * R.q7.y + gc[2] * R.q7.z;
-    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
-    c[0] = GK * t.E;
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-    {
-        const float dz = -GK * t.e * t.z[r];
-        const float du = dz * inv_s[r];
-        c[1 + r] = du;
-        c[4 + r] = dz * t.z[r];
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-            c[7 + 3 * r + a] = du * t.d[a];
-    }
-    c[16] = Kw * gc[0];
-    c[17] = Kw * gc[1];
-    c[18] = Kw * gc[2];
-}
-
-__device__ __forceinline__ void bwd_flush(double* dst, float (&a)[BWD_NACC], bool exclusive, int lane)
-{
-#pragma unroll
-    for (int i = 0; i < BWD_NACC; i++)
-    {
-        float v = a[i];
-#pragma unroll
-        for (int o = 16; o; o >>= 1)
-            v += __shfl_xor_sync(FULL, v, o);
-        a[i] = 0.f;
-        if (lane == 0)
-        {
-            if (exclusive)
-                dst[i] = (double)v;
-            else
-                atomicAdd(&dst[i], (double)v);
-        }
-    }
-}
-
-template <class K>
-__global__ void __launch_bounds__(BWD_BLOCK) k_bwd_pairs(BwdParams B)
-{
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * BWD_BLOCK + threadIdx.x) >> 5;
-    const int64_t r0 = warp * BWD_RANGE;
-    if (r0 >= B.P)
-        return; // uniform per warp
-    const int64_t r1 = min(B.P, r0 + (int64_t)BWD_RANGE);
-    const K* keys = (const K*)B.keys;
-    float acc[BWD_NACC];
-#pragma unroll
-    for (int i = 0; i < BWD_NACC; i++)
-        acc[i] = 0.f;
-    uint32_t cur = B.ids[r0];
-    bool head = r0 == 0 || B.ids[r0 - 1] != cur;
-    for (int64_t base = r0; base < r1; base += 32)
-    {
-        const int64_t p = base + lane;
-        const bool valid = p < r1;
-        const uint32_t gid = valid ? B.ids[p] : 0xFFFFFFFFu;
-        float c[BWD_NACC];
-#pragma unroll
-        for (int i = 0; i < BWD_NACC; i++)
-            c[i] = 0.f;
-        if (valid && gid < (uint64_t)B.G)
-            pair_adjoint<K>(B, (uint64_t)keys[p], gid, c);
-        // one pass per Gaussian present in this chunk (at most 32)
-        bool pend = valid;
-        while (true)
-        {
-            if (pend && gid == cur)
-            {
-#pragma unroll
-                for (int i = 0; i < BWD_NACC; i++)
-                    acc[i] += c[i];
-                pend = false;
-            }
-            const unsigned later = __ballot_sync(FULL, pend);
-            if (!later)
-                break;
-            // the segment of `cur` ends inside this range
-            if (cur < (uint64_t)B.G)
-                bwd_flush(B.acc + (uint64_t)cur * BWD_NACC, acc, head, lane);
-            cur = __shfl_sync(FULL, gid, __ffs(later) - 1);
-            head = true;
-        }
-    }
-    const bool tail = r1 == B.P || B.ids[r1] != cur;
-    if (cur < (uint64_t)B.G)
-        bwd_flush(B.acc + (uint64_t)cur * BWD_NACC, acc, head && tail, lane);
-}
-
 // per Gaussian: chain the FP64 sums to the caller's parameters
 __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
 {
@@ -166,7 +39,6 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
         return;
     double a[BWD_NACC];
     bool any = false;
-    if (F.partials)
     {
         // the Gaussian's (leaf, Gaussian) pairs are emission indices [e0, e1)
         const uint64_t c0 = F.lcol_off[g], c1 = g + 1 < F.G ? F.lcol_off[g + 1] : F.NLC;
@@ -178,15 +50,6 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
                 a[i] += (double)F.partials[e * BWD_NACC + i];
         for (int i = 0; i < BWD_NACC; i++)
             any = any || a[i] != 0.0;
-    }
-    else
-    {
-        const double* A = F.acc + BWD_NACC * g;
-        for (int i = 0; i < BWD_NACC; i++)
-        {
-            a[i] = A[i];
-            any = any || a[i] != 0.0;
-        }
     }
     float dmu[3] = { 0.f, 0.f, 0.f }, dq[4] = { 0.f, 0.f, 0.f, 0.f }, ds[3] = { 0.f, 0.f, 0.f }, dop = 0.f,
           dc[3] = { 0.f, 0.f, 0.f };
@@ -277,18 +140,6 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
     if (F.d_colors)
         for (int k = 0; k < 3; k++)
             F.d_colors[3 * g + k] = dc[k];
-}
-
-void launch_bwd_pairs(const BwdParams& B, int key64, cudaStream_t s)
-{
-    if (B.P <= 0)
-        return;
-    const int64_t warps = (B.P + BWD_RANGE - 1) / BWD_RANGE;
-    const int64_t blocks = (warps + (BWD_BLOCK / 32) - 1) / (BWD_BLOCK / 32);
-    if (key64)
-        { k_bwd_pairs<uint64_t><<<(unsigned)blocks, BWD_BLOCK, 0, s>>>(B); count_launch(); }
-    else
-        { k_bwd_pairs<uint32_t><<<(unsigned)blocks, BWD_BLOCK, 0, s>>>(B); count_launch(); }
 }
 
 void launch_bwd_finalize(const BwdFinalParams& F, cudaStream_t s)

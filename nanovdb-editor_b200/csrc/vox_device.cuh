@@ -340,73 +340,6 @@ __device__ __forceinline__ Aabb voxel_local_aabb(const GaussRec& R, const RInv& 
     return b;
 }
 
-// Conservative k-range of one voxel column (x = i, y = j fixed) of a Gaussian.
-// The local AABB of voxel k is centred at l(k) = M (c_k - mu) with half
-// extents h_r = vs/2 sum_a |M_ra| (M_ra = rinv[r][a] / (ls s_r)), so it can
-// meet the unit ball only if |l(k)| < 1 + |h|.  l(k) is affine in k, which
-// gives a quadratic in k.  The bound is widened by delta = 1e-5 (1 + B), B
-// bounding the magnitudes the float test sums, which covers the test's own
-// rounding (a worst-case error bound is below 1.1e-6 B), and by one voxel on
-// each side.  Candidates outside [klo, khi] therefore fail the reference test.
-// Returns klo > khi for an empty column.  All arithmetic in double.
-__device__ __forceinline__ void column_interval(const GaussRec& R, const RInv& Mr, float vs, int32_t i, int32_t j,
-                                                int32_t& klo, int32_t& khi)
-{
-    const double vsd = vs;
-    const double mu[3] = { R.q0.x, R.q0.y, R.q0.z };
-    const double sc[3] = { (double)R.q0.w * (double)R.q3.y, (double)R.q0.w * (double)R.q3.z,
-                           (double)R.q0.w * (double)R.q3.w };
-    const int32_t kmin = R.q4.z, kmax = R.q4.z + R.q5.z - 1;
-    const double ax = ((double)i + 0.5) * vsd - mu[0];
-    const double ay = ((double)j + 0.5) * vsd - mu[1];
-    const double ex = fabs((double)i * vsd) + fabs(mu[0]) + vsd;
-    const double ey = fabs((double)j * vsd) + fabs(mu[1]) + vsd;
-    const double ez = fmax(fabs((double)kmin * vsd), fabs((double)(kmax + 1) * vsd)) + fabs(mu[2]) + vsd;
-    double a = 0.0, b = 0.0, c = 0.0, h2 = 0.0, B = 0.0;
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-    {
-        const double m0 = (double)Mr.m[r][0] * sc[r], m1 = (double)Mr.m[r][1] * sc[r], m2 = (double)Mr.m[r][2] * sc[r];
-        const double A = m0 * ax + m1 * ay;
-        const double h = 0.5 * vsd * (fabs(m0) + fabs(m1) + fabs(m2));
-        a += m2 * m2;
-        b += A * m2;
-        c += A * A;
-        h2 += h * h;
-        B = fmax(B, fabs(m0) * ex + fabs(m1) * ey + fabs(m2) * ez);
-    }
-    const double bound = 1.0 + sqrt(h2) + 1e-5 * (1.0 + B);
-    c -= bound * bound;
-    if (a < 1e-300)
-    {
-        // l independent of k
-        klo = c < 0.0 ? kmin : 1;
-        khi = c < 0.0 ? kmax : 0;
-        return;
-    }
-    const double disc = b * b - a * c;
-    if (disc < 0.0)
-    {
-        klo = 1;
-        khi = 0;
-        return;
-    }
-    const double sq = sqrt(disc);
-    // zc = (k + 1/2) vs - mu_z in [(-b - sq) / a, (-b + sq) / a]
-    double k1 = ((-b - sq) / a + mu[2]) / vsd - 0.5;
-    double k2 = ((-b + sq) / a + mu[2]) / vsd - 0.5;
-    k1 = fmax(floor(k1) - 1.0, (double)kmin);
-    k2 = fmin(ceil(k2) + 1.0, (double)kmax);
-    if (!(k1 <= k2))
-    {
-        klo = 1;
-        khi = 0;
-        return;
-    }
-    klo = (int32_t)k1;
-    khi = (int32_t)k2;
-}
-
 // dist2 test of gaussian_frag_alloc.slang:132-162
 __device__ __forceinline__ bool aabb_hits_unit_sphere(const Aabb& b)
 {

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -68,6 +69,60 @@ static float cull_from_params(pnanovdb_compute_array_t** shader_params_arrays)
 }
 
 // ------------------------------------------------------------------ arrays
+// Grids returned to the caller live in page-locked host memory so the
+// device-to-host copy runs at link speed.  Page-locking is slow, so blocks
+// come back to a small pool when the caller destroys the array and the next
+// result of a similar size reuses them.
+namespace
+{
+std::mutex g_pin_mutex;
+std::unordered_map<void*, size_t> g_pinned;           // live page-locked blocks -> capacity
+std::vector<std::pair<void*, size_t>> g_pin_free;     // pooled blocks
+constexpr size_t PIN_POOL_MAX = 4;                    // blocks kept for reuse
+
+void* pinned_alloc(size_t bytes)
+{
+    std::lock_guard<std::mutex> lock(g_pin_mutex);
+    size_t best = (size_t)-1;
+    for (size_t i = 0; i < g_pin_free.size(); i++)
+        if (g_pin_free[i].second >= bytes && g_pin_free[i].second <= 2 * bytes + 4096 &&
+            (best == (size_t)-1 || g_pin_free[i].second < g_pin_free[best].second))
+            best = i;
+    if (best != (size_t)-1)
+    {
+        auto blk = g_pin_free[best];
+        g_pin_free.erase(g_pin_free.begin() + (long)best);
+        g_pinned[blk.first] = blk.second;
+        return blk.first;
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocPortable) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return nullptr;
+    }
+    g_pinned[p] = bytes ? bytes : 1;
+    return p;
+}
+
+// returns true when p was a pooled page-locked block
+bool pinned_release(void* p)
+{
+    std::lock_guard<std::mutex> lock(g_pin_mutex);
+    auto it = g_pinned.find(p);
+    if (it == g_pinned.end())
+        return false;
+    g_pin_free.emplace_back(it->first, it->second);
+    g_pinned.erase(it);
+    if (g_pin_free.size() > PIN_POOL_MAX)
+    {
+        cudaFreeHost(g_pin_free.front().first);
+        g_pin_free.erase(g_pin_free.begin());
+    }
+    return true;
+}
+} // namespace
+
 static pnanovdb_compute_array_t* PNANOVDB_ABI array_create(size_t element_size, pnanovdb_uint64_t element_count,
                                                            const void* data)
 {
@@ -93,8 +148,26 @@ static void PNANOVDB_ABI array_destroy(pnanovdb_compute_array_t* a)
 {
     if (!a)
         return;
-    free(a->data);
+    if (!pinned_release(a->data))
+        free(a->data);
     free(a);
+}
+
+// an array whose contents the caller fills at once (page-locked, not cleared)
+static pnanovdb_compute_array_t* array_create_pinned(size_t element_size, pnanovdb_uint64_t element_count)
+{
+    pnanovdb_compute_array_t* a = (pnanovdb_compute_array_t*)calloc(1, sizeof(pnanovdb_compute_array_t));
+    if (!a)
+        return nullptr;
+    a->data = pinned_alloc(element_size * element_count);
+    if (!a->data)
+    {
+        free(a);
+        return nullptr;
+    }
+    a->element_size = element_size;
+    a->element_count = element_count;
+    return a;
 }
 static void* PNANOVDB_ABI array_map(pnanovdb_compute_array_t* a)
 {
@@ -364,7 +437,7 @@ static pnanovdb_compute_array_t* run_host(int device, const vox_gaussians_t* g, 
     uint64_t bytes = 0;
     if (vox_voxelize_host(v, g, voxel_size, cull, flags, nullptr, 0, &bytes) != VOX_OK)
         return nullptr;
-    pnanovdb_compute_array_t* a = array_create(4, (bytes + 3) / 4, nullptr);
+    pnanovdb_compute_array_t* a = array_create_pinned(4, (bytes + 3) / 4);
     if (!a)
         return nullptr;
     if (vox_copy_grid(v, a->data, bytes) != VOX_OK)

@@ -69,7 +69,8 @@ __global__ void k_leaf_cols(const GaussRec* recs, int64_t G, uint64_t* lcols)
 // May a voxel of the leaf at origin o pass the reference test?  The local AABB
 // of the leaf box (monotone-corner identity, in double) contains every voxel's
 // local AABB; the float test's rounding is bounded by delta = 1e-5 (1 + B), B
-// bounding the magnitudes it sums (as for the column bound of the emit test).
+// bounding the magnitudes it sums (a worst-case error bound of the float test
+// is below 1.1e-6 B).
 __device__ __forceinline__ bool leaf_may_hit(const GaussRec& R, const RInv& M, float vsf, int32_t ox, int32_t oy,
                                              int32_t oz)
 {

@@ -1,19 +1,19 @@
-// vox_raster.cu - emit -> (sort) -> build -> accumulate kernels of the
-// Gaussian -> node2 voxelization.
+// vox_raster.cu - per-Gaussian records, rank tables, run detection and the
+// node2 tree of the Gaussian -> node2 voxelization.
 //
 // Reference path (raster/Raster.cpp:420-558): two passes of fragment windows,
 // each re-running gaussian_prim / fanout / gaussian_frag_{alloc,color} and an
-// incremental 4-level tree build with atomics.  Here instead:
+// incremental 4-level tree build with atomics.  Here:
 //   k_prep        one record per Gaussian (bbox, inverse rotation, alpha
 //                 constants), footprint, touched root tiles
 //   k_mark_lower  touched lower-node cells (128^3 voxels) per Gaussian bbox
-//   k_emit        load-balanced fragment test over all candidate fragments,
-//                 passing pairs compacted in (Gaussian, fragment) order with a
-//                 decoupled look-back, written as (compact voxel key, id)
-//   [sort]        onesweep radix sort by key (stable: ids stay ascending)
-//   k_runs        unique-key runs -> voxels, leaves, lower nodes
-//   k_leaf_masks / k_node_* / k_write_*  node2 tables written exactly
-//   k_accumulate  per voxel, pairs in (key, id) order: RGBA8 max + float sums
+//   [vox_leaf.cu] (leaf, Gaussian) pairs, sort, one CTA per candidate leaf:
+//                 value masks, RGBA8, float sums; active voxel keys
+//   k_runs        unique-key runs of the sorted voxel keys -> voxels, leaves,
+//                 lower nodes
+//   k_lower_info / k_upper_info / k_leaf_info / k_cloud_*   node tables and
+//                 per-cloud layout
+//   k_write_*     node2 nodes, per-cloud headers, written exactly
 #include <cstdio>
 #include <cuda_runtime.h>
 
@@ -26,7 +26,7 @@ namespace vox
 {
 
 // ------------------------------------------------------------------ prep ----
-__global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint64_t* footprints, uint64_t* columns,
+__global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint64_t* footprints,
                                               unsigned long long* root_bits, int* err)
 {
     int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -72,7 +72,6 @@ __global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint
     }
     recs[g] = R;
     footprints[g] = fp;
-    columns[g] = fp ? (uint64_t)R.q5.x * (uint64_t)R.q5.y : 0ull;
     if (fp)
     {
         // root tiles (4096^3 voxels) spanned by the bbox
@@ -487,8 +486,6 @@ __global__ void __launch_bounds__(256) k_leaf_info(NodeParams N, const K* __rest
     const uint32_t ln = (uint32_t)((uint64_t)key0 >> 9) & 4095u;
     const uint32_t lo = N.leaf_lower[l];
     N.leaf_lower_n[l] = ln;
-    if (N.leaf_slot)
-        N.leaf_slot[(uint64_t)lo * 4096u + ln] = (uint32_t)l;
     N.leaf_origin[3 * l + 0] = N.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8;
     N.leaf_origin[3 * l + 1] = N.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8;
     N.leaf_origin[3 * l + 2] = N.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8;
@@ -731,137 +728,13 @@ __global__ void __launch_bounds__(256) k_write_leaf(NodeParams N, uint8_t* node2
     ((uint64_t*)(node2 + N.leaf_addr[l]))[w] = val;
 }
 
-// ------------------------------------------------------------- accumulate ----
-// A CTA owns 256 consecutive voxels (one per thread) and walks their pairs,
-// which are contiguous in the sorted array, in chunks: every thread computes
-// the alpha of one pair at a time (balanced across lanes) into shared memory,
-// then each voxel's thread sums its own pairs sequentially in (key, id)
-// order, so the float sums have the same fixed order as a serial loop.  The
-// voxel's bit is set in its leaf mask on the way.
-constexpr int ACC_BLOCK = 256;
-constexpr int ACC_CHUNK = 2048;
-
-struct AccSmem
-{
-    float a[ACC_CHUNK];
-    float ar[ACC_CHUNK], ag[ACC_CHUNK], ab[ACC_CHUNK];
-    uint32_t rgba[ACC_CHUNK];
-    uint32_t vstart[ACC_BLOCK + 1];
-};
-
-template <class K>
-__global__ void __launch_bounds__(ACC_BLOCK) k_accumulate(AccumParams A, NodeParams N, const uint32_t* __restrict__ ids)
-{
-    __shared__ AccSmem S;
-    const int64_t v0 = (int64_t)blockIdx.x * ACC_BLOCK;
-    const int64_t V = A.V;
-    if (v0 >= V)
-        return;
-    const int64_t nv = min((int64_t)ACC_BLOCK, V - v0);
-    for (int t = threadIdx.x; t <= nv; t += ACC_BLOCK)
-        S.vstart[t] = N.vox_start[v0 + t];
-    __syncthreads();
-    const uint32_t pa = S.vstart[0], pb = S.vstart[nv];
-    const K* keys = (const K*)A.keys;
-    const int t = threadIdx.x;
-    const bool mine = t < nv;
-    const uint32_t my0 = mine ? S.vstart[t] : 0u, my1 = mine ? S.vstart[t + 1] : 0u;
-    uint32_t rgba = 0;
-    float dsum = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-    for (uint32_t pc = pa; pc < pb; pc += ACC_CHUNK)
-    {
-        const uint32_t len = min((uint32_t)ACC_CHUNK, pb - pc);
-        for (uint32_t e = threadIdx.x; e < len; e += ACC_BLOCK)
-        {
-            const uint32_t p = pc + e;
-            const uint64_t key = (uint64_t)keys[p];
-            const uint32_t lo = A.rank_to_lower[key >> 21];
-            const uint32_t ln = (uint32_t)(key >> 9) & 4095u, vn = (uint32_t)key & 511u;
-            const int32_t x = N.lower_origin[3 * lo + 0] + (int32_t)((ln >> 8) & 15) * 8 + (int32_t)(vn >> 6);
-            const int32_t y = N.lower_origin[3 * lo + 1] + (int32_t)((ln >> 4) & 15) * 8 + (int32_t)((vn >> 3) & 7);
-            const int32_t z = N.lower_origin[3 * lo + 2] + (int32_t)(ln & 15) * 8 + (int32_t)(vn & 7);
-            const GaussRec R = A.recs[ids[p]];
-            const RInv M = rinv_of(R);
-            const float vs = rec_vs(R, A.voxel_size, A.cloud_vs);
-            float cx0, cx1, cy0, cy1, cz0, cz1;
-            axis_corners(vs, R.q0.x, x, cx0, cx1);
-            axis_corners(vs, R.q0.y, y, cy0, cy1);
-            axis_corners(vs, R.q0.z, z, cz0, cz1);
-            const float a8 = pair_alpha(R, aabb_from_corners(R, M, cx0, cx1, cy0, cy1, cz0, cz1));
-            float a;
-            if (A.smooth)
-            {
-                SmoothTerms st;
-                a = smooth_kernel(R, M, vs, x, y, z, st);
-            }
-            else
-            {
-                // float channels: corner offsets rounded once from double
-                float sx0, sx1, sy0, sy1, sz0, sz1;
-                axis_corners_stable(vs, R.q0.x, x, sx0, sx1);
-                axis_corners_stable(vs, R.q0.y, y, sy0, sy1);
-                axis_corners_stable(vs, R.q0.z, z, sz0, sz1);
-                const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
-                a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
-            }
-            S.a[e] = a;
-            S.ar[e] = VOX_FMUL(a, R.q7.x);
-            S.ag[e] = VOX_FMUL(a, R.q7.y);
-            S.ab[e] = VOX_FMUL(a, R.q7.z);
-            S.rgba[e] = pack_rgba8(R, a8);
-        }
-        __syncthreads();
-        if (mine)
-        {
-            const uint32_t q0 = max(my0, pc), q1 = min(my1, pc + len);
-            for (uint32_t p = q0; p < q1; p++)
-            {
-                const uint32_t e = p - pc;
-                rgba = S.rgba[e] > rgba ? S.rgba[e] : rgba;
-                dsum = VOX_FADD(dsum, S.a[e]);
-                c0 = VOX_FADD(c0, S.ar[e]);
-                c1 = VOX_FADD(c1, S.ag[e]);
-                c2 = VOX_FADD(c2, S.ab[e]);
-            }
-        }
-        __syncthreads();
-    }
-    if (mine)
-    {
-        const int64_t v = v0 + t;
-        const uint32_t l = A.vox_leaf[v];
-        const uint32_t n = A.vox_n[v];
-        const uint64_t vi = N.leaf_vidx[l] + (uint64_t)(v - N.leaf_vstart[l]);
-        const uint32_t b = N.C.leaf_cloud[l];
-        uint32_t* rgba8 = (uint32_t*)(A.out + N.C.rgba_off[b]);
-        float* density = (float*)(A.out + N.C.dens_off[b]);
-        float* color = (float*)(A.out + N.C.col_off[b]);
-        rgba8[vi] = rgba;
-        density[vi] = dsum;
-        if (A.smooth)
-        {
-            // premultiplied colour (linear in the per-pair weights)
-            color[3 * vi + 0] = c0;
-            color[3 * vi + 1] = c1;
-            color[3 * vi + 2] = c2;
-        }
-        else
-        {
-            color[3 * vi + 0] = dsum > 0.f ? VOX_FDIV(c0, dsum) : 0.f;
-            color[3 * vi + 1] = dsum > 0.f ? VOX_FDIV(c1, dsum) : 0.f;
-            color[3 * vi + 2] = dsum > 0.f ? VOX_FDIV(c2, dsum) : 0.f;
-        }
-        atomicOr((unsigned long long*)&N.leaf_mask[8 * (uint64_t)l + (n >> 6)], 1ull << (n & 63));
-    }
-}
-
 // =================================================================== launch
-void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* columns, uint64_t* root_bits,
-                 int* err, cudaStream_t s)
+void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* root_bits, int* err,
+                 cudaStream_t s)
 {
     if (P.count <= 0)
         return;
-    { k_prep<<<(unsigned)((P.count + 255) / 256), 256, 0, s>>>(P, recs, footprints, columns, (unsigned long long*)root_bits, err); count_launch(); }
+    { k_prep<<<(unsigned)((P.count + 255) / 256), 256, 0, s>>>(P, recs, footprints, (unsigned long long*)root_bits, err); count_launch(); }
 }
 
 void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits, const uint64_t* root_prefix,
@@ -959,15 +832,4 @@ void launch_write_headers(const NodeParams& N, uint8_t* out, cudaStream_t s)
 {
     { k_write_headers<<<(unsigned)((N.C.B + 127) / 128), 128, 0, s>>>(N, out); count_launch(); }
 }
-void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s)
-{
-    if (A.V <= 0)
-        return;
-    unsigned blocks = (unsigned)((A.V + ACC_BLOCK - 1) / ACC_BLOCK);
-    if (key64)
-        { k_accumulate<uint64_t><<<blocks, ACC_BLOCK, 0, s>>>(A, N, ids); count_launch(); }
-    else
-        { k_accumulate<uint32_t><<<blocks, ACC_BLOCK, 0, s>>>(A, N, ids); count_launch(); }
-}
-
 } // namespace vox

@@ -17,23 +17,6 @@ struct RankTables
     const uint64_t* lower_prefix;
 };
 
-struct EmitParams
-{
-    const GaussRec* recs;
-    const uint64_t* col_off; // exclusive scan of per-Gaussian column counts (bbox range x * range y)
-    int64_t G;
-    uint64_t NC;             // total columns
-    float voxel_size;
-    const float* cloud_vs; // per-cloud voxel sizes (batched calls) or null
-    uint64_t cap;
-    uint64_t* status;
-    uint32_t epoch;
-    uint32_t* counter;
-    uint64_t* total;
-    int* err;
-    int check; // also test the candidates the column bound skips (validation)
-};
-
 struct RunParams
 {
     int64_t P;
@@ -96,7 +79,6 @@ struct NodeParams
     uint64_t* upper_count;
     uint32_t* leaf_lower;
     uint32_t* leaf_lower_n;
-    uint32_t* leaf_slot; // optional [lower runs * 4096]: (lower run, lower_n) -> leaf index
     uint64_t* leaf_mask;
     int32_t* leaf_origin;
     uint64_t *upper_idx, *upper_addr, *upper_vidx;
@@ -104,47 +86,12 @@ struct NodeParams
     uint64_t *leaf_idx, *leaf_addr, *leaf_vidx;
 };
 
-struct AccumParams
-{
-    const GaussRec* recs;
-    const void* keys;
-    float voxel_size;
-    int64_t V;
-    const uint32_t* rank_to_lower; // lower rank -> lower node index
-    const uint32_t* vox_leaf;
-    const uint16_t* vox_n;
-    uint8_t* out;          // grid buffer: channels at the per-cloud offsets of NodeParams::C
-    const float* cloud_vs; // per-cloud voxel sizes or null
-    int smooth; // differentiable channels (smooth_kernel, premultiplied colour)
-};
-
 // per-Gaussian adjoint sums: [0] dL/d op, [1..3] U, [4..6] W, [7..15] Q[r][a], [16..18] dL/d rgb
 constexpr int BWD_NACC = 19;
 
-struct BwdParams
-{
-    const GaussRec* recs;
-    const void* keys;    // compact keys in emission order (sorted by Gaussian id)
-    const uint32_t* ids; // Gaussian ids in emission order
-    int64_t P, G;
-    const uint32_t* rank_to_lower;
-    const uint32_t* leaf_slot;
-    const uint64_t* leaf_vidx;
-    const uint64_t* leaf_mask;
-    const int32_t* lower_origin;
-    const float* grad_density; // [value_count] or null
-    const float* grad_color;   // [value_count][3] or null
-    const uint32_t* leaf_cloud;
-    const uint64_t* value_base; // values of cloud b start at value_base[b] in the grad arrays
-    float voxel_size;
-    const float* cloud_vs;
-    double* acc;               // [G][BWD_NACC], zeroed
-};
-
 struct BwdFinalParams
 {
-    const double* acc;
-    const float* partials;   // per-leaf partials by emission index (null: acc holds the sums)
+    const float* partials;    // per-(leaf, Gaussian) partial sums by emission index
     const uint64_t* lcol_off; // [G] first leaf column of each Gaussian
     const uint64_t* lc_off;   // [NLC] first emission index of each leaf column
     uint64_t NLC, Q;
@@ -240,19 +187,13 @@ struct ValueParams
 };
 void launch_values(const ValueParams& A, const NodeParams& N, cudaStream_t s);
 
-void launch_bwd_pairs(const BwdParams& B, int key64, cudaStream_t s);
 void launch_bwd_finalize(const BwdFinalParams& F, cudaStream_t s);
 
-void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* columns, uint64_t* root_bits,
-                 int* err, cudaStream_t s);
+void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* root_bits, int* err,
+                 cudaStream_t s);
 void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits, const uint64_t* root_prefix,
                        uint64_t* lower_bits, cudaStream_t s);
 void launch_invert_bits(const uint64_t* bits, const uint64_t* prefix, int64_t words, uint32_t* out, cudaStream_t s);
-void launch_emit_u32(const EmitParams& E, const RankTables& T, uint32_t* out_k, uint32_t* out_i, int num_sms,
-                     cudaStream_t s);
-void launch_emit_u64(const EmitParams& E, const RankTables& T, uint64_t* out_k, uint32_t* out_i, int num_sms,
-                     cudaStream_t s);
-int64_t emit_tile_count(uint64_t NC);
 void launch_runs(const RunParams& Rp, const void* keys, int key64, cudaStream_t s);
 int64_t runs_tile_count(int64_t P);
 void launch_lower_info(const NodeParams& N, cudaStream_t s);
@@ -263,6 +204,5 @@ void launch_cloud_layout(const NodeParams& N, cudaStream_t s);
 void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s);
 void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* out, cudaStream_t s);
 void launch_write_headers(const NodeParams& N, uint8_t* out, cudaStream_t s);
-void launch_accumulate(const AccumParams& A, const NodeParams& N, const uint32_t* ids, int key64, cudaStream_t s);
 
 } // namespace vox

@@ -121,9 +121,9 @@ def test_needles_and_discs(vox_ctx, oracle_mod):
     _check(vox_ctx, oracle_mod, cloud, 0.01)
 
 
-def test_column_bound_never_skips_a_passing_voxel(oracle_mod):
-    """VOX_CHECK_EMIT=1 also tests every candidate the per-column bound skips
-    and fails the call if one of them passes the reference test."""
+def test_leaf_bound_never_skips_a_passing_voxel(oracle_mod):
+    """VOX_CHECK_EMIT=1 also walks every bbox leaf the conservative leaf test
+    culls and fails the call if one of its voxels passes the reference test."""
     import os
 
     from nanovdb_editor.vox import VoxContext
