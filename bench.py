@@ -409,30 +409,36 @@ def main():
     # ---- roofline of the dominant stage
     st = stats[-1]
     P = st["pairs"]
+    Q = st["leaf_pairs"]
+    NCL = st["candidate_leaves"]
+    V = st["voxels"]
     passes = st["sort_passes"]
-    kb = 8 if st["key_bits"] > 32 else 4
     A = 56
-    # algorithmic bytes per stage (definitions in DESIGN.md)
+    # algorithmic bytes per stage: what each stage must read and write once
     stage_bytes = {
-        "emit": G * 128 + P * (kb + 4),  # read Gaussian records, write (key, id)
-        "sort": P * (kb + (kb + 4) * 2 * passes),  # histogram read + per pass read/write (key, id)
-        "accumulate": P * (kb + 4) + G * 128 + st["voxels"] * 20,
-        "prep": G * (A + 128 + 8),
+        "prep": G * (A + 128 + 8),  # raw attributes in, record + footprint out
+        "leaf_pairs": 2 * G * 128 + 12 * Q,  # records read by the count and write passes, (key, index, id) out
+        "sort": Q * (4 + 16 * passes),  # histogram read + per pass read/write (key, value)
+        "leaf_walk": 8 * Q + 128 * Q + 72 * NCL + 24 * V,  # pair lists, record gathers, masks, staged values
+        "tree_values": 60 * V,  # voxel keys, runs, node tables, values
     }
     stage_ms = {
-        "emit": float(np.mean([s["ms_emit"] for s in stats])),
-        "sort": float(np.mean([s["ms_sort"] for s in stats])),
-        "accumulate": float(np.mean([s["ms_accumulate"] for s in stats])),
         "prep": float(np.mean([s["ms_prep"] for s in stats])),
-        "build": float(np.mean([s["ms_build"] for s in stats])),
+        "leaf_pairs": float(np.mean([s["ms_emit"] for s in stats])),
+        "sort": float(np.mean([s["ms_sort"] for s in stats])),
+        "leaf_walk": float(np.mean([s["ms_accumulate"] for s in stats])),
+        "tree_values": float(np.mean([s["ms_build"] for s in stats])),
     }
-    dom = max(("emit", "sort", "accumulate"), key=lambda k: stage_ms[k])
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
     peak, peak_kind = load_peaks()
     achieved = stage_bytes[dom] / (stage_ms[dom] * 1e-3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dom)
+        # DRAM bytes ncu measured per launch of the dominant kernel, scaled to this workload
+        t = json.load(open(tp)).get(dom)
+        if t and t.get("voxels"):
+            traffic = t["bytes"] * V / t["voxels"]
 
     forms = {}
     if not args.no_forms:
@@ -461,7 +467,7 @@ def main():
             "config": dict(WORKLOAD, gaussians=G, parallelism=f"replicas{world}" if world > 1 else "single", l2="256 MB flush between steps; pair working set >> L2", inputs="raw (log-scale, logit, SH0)"),
             "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind, "note": "the leaf walk is FP32/FP64 instruction-issue bound, not HBM bound"},
             "stages_ms": stage_ms,
             "counts": {k: st[k] for k in ("candidates", "pairs", "voxels", "uppers", "lowers", "leaves", "key_bits", "sort_passes", "sort_shape", "leaf_pairs", "candidate_leaves")},
             "pairs_per_s": world * P / (ms * 1e-3),
