@@ -8,6 +8,7 @@
 // CUDA stream with three small read-backs (candidate count, pair count, node
 // counts) that size the buffers; buffers persist in the context and only
 // grow, so repeated calls allocate nothing.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -61,6 +62,9 @@ struct vox_context_t
     DevBuf lcols, lcol_off, lc_count, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask;
     DevBuf s_rgba, s_dens, s_col, s_pairs, cand_cnt, cand_voff, vkeys, vslot, vpairs, pair_off, cand_vbase;
     DevBuf partials, exp_keys, exp_ids;
+    // reference node order
+    DevBuf nwin, win_before, cand_wkey, wkey_u, wkey_lo, wkey_leaf, wcnt, wbase, okeys, okeys_alt, ovals, ovals_alt;
+    DevBuf rank_u, rank_lo, rank_leaf, leaf_popc, leaf_voff;
     DevBuf cloud_start, cloud_vs, clouds;           // batched calls: inputs, per-cloud layout
     DevBuf order; // 9 node order arrays
     DevBuf grid;
@@ -110,6 +114,7 @@ enum
     SC_Q,    // (leaf, Gaussian) pairs
     SC_NCL,  // candidate leaves
     SC_NVOX, // active voxels from the leaf masks
+    SC_NWIN, // reference fragment windows (window order)
     SC_BBOX, // 3 words (6 int32)
     SC_COUNT = SC_BBOX + 3,
     SC_SCRATCH = 24
@@ -213,6 +218,88 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b)
 // ---------------------------------------------------------------------------
 // the pipeline
 // ---------------------------------------------------------------------------
+// node_idx / addresses / value indices in the reference's window order
+// (vox_order.cu): per level a sort by (creation window, parent rank, n)
+static int window_order(vox_context_t* ctx, NodeParams& N, int64_t U, int64_t Lo, int64_t L, int64_t nw,
+                        cudaStream_t s)
+{
+    const int64_t mx = std::max<int64_t>(std::max<int64_t>(U, Lo), std::max<int64_t>(L, 1));
+    const int64_t W = nw > 0 ? nw : 1;
+    if (!ensure(ctx, ctx->wkey_u, 8 * (size_t)(U + 1)) || !ensure(ctx, ctx->wkey_lo, 8 * (size_t)(Lo + 1)) ||
+        !ensure(ctx, ctx->wkey_leaf, 8 * (size_t)(L + 1)) || !ensure(ctx, ctx->wcnt, 8 * 3 * (size_t)W) ||
+        !ensure(ctx, ctx->wbase, 8 * 4 * (size_t)(W + 1)) || !ensure(ctx, ctx->okeys, 8 * (size_t)mx) ||
+        !ensure(ctx, ctx->okeys_alt, 8 * (size_t)mx) || !ensure(ctx, ctx->ovals, 4 * (size_t)mx) ||
+        !ensure(ctx, ctx->ovals_alt, 4 * (size_t)mx) || !ensure(ctx, ctx->rank_u, 4 * (size_t)(U + 1)) ||
+        !ensure(ctx, ctx->rank_lo, 4 * (size_t)(Lo + 1)) || !ensure(ctx, ctx->rank_leaf, 4 * (size_t)(L + 1)) ||
+        !ensure(ctx, ctx->leaf_popc, 8 * (size_t)(L + 1)) || !ensure(ctx, ctx->leaf_voff, 8 * (size_t)(L + 1)) ||
+        !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(mx, 8)) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(L + 1) * 2))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    int* d_err = (int*)(sc + SC_ERR);
+    uint32_t* d_counter = (uint32_t*)(sc + SC_SCRATCH);
+    uint64_t* wk_u = (uint64_t*)ctx->wkey_u.p;
+    uint64_t* wk_lo = (uint64_t*)ctx->wkey_lo.p;
+    uint64_t* wk_leaf = (uint64_t*)ctx->wkey_leaf.p;
+    uint64_t* cnt = (uint64_t*)ctx->wcnt.p; // [3][W]
+    uint64_t* base = (uint64_t*)ctx->wbase.p; // [4][W + 1]
+    cudaMemsetAsync(cnt, 0, 8 * 3 * (size_t)W, s);
+    launch_leaf_wkey(L, N.leaf_vstart, (const uint32_t*)ctx->vslot.p, (const uint64_t*)ctx->cand_wkey.p, wk_leaf, s);
+    launch_run_min(Lo, N.lower_lstart, wk_leaf, wk_lo, s);
+    launch_run_min(U, N.upper_lostart, wk_lo, wk_u, s);
+    const int key_bits = 40 + bits_for((uint64_t)W + 1);
+    struct Level
+    {
+        int64_t n;
+        const uint64_t* wkey;
+        const uint32_t* parent;
+        const uint32_t* parent_rank;
+        const uint32_t* nval;
+        uint32_t nmask;
+        uint32_t* rank;
+    } lv[3] = { { U, wk_u, nullptr, nullptr, N.upper_root_n, 32767u, (uint32_t*)ctx->rank_u.p },
+                { Lo, wk_lo, N.lower_parent, (const uint32_t*)ctx->rank_u.p, N.lower_upper_n, 32767u,
+                  (uint32_t*)ctx->rank_lo.p },
+                { L, wk_leaf, N.leaf_lower, (const uint32_t*)ctx->rank_lo.p, N.leaf_lower_n, 4095u,
+                  (uint32_t*)ctx->rank_leaf.p } };
+    for (int l = 0; l < 3; l++)
+    {
+        if (lv[l].n <= 0)
+            continue;
+        launch_level_keys(lv[l].n, lv[l].wkey, lv[l].parent, lv[l].parent_rank, lv[l].nval, lv[l].nmask,
+                          (uint64_t*)ctx->okeys.p, (uint32_t*)ctx->ovals.p, cnt + (size_t)l * W, s);
+        const int in_alt = sort_pairs_u64((uint64_t*)ctx->okeys.p, (uint32_t*)ctx->ovals.p, (uint64_t*)ctx->okeys_alt.p,
+                                          (uint32_t*)ctx->ovals_alt.p, lv[l].n, key_bits, ctx->sort_ws.p,
+                                          &ctx->sort_epochs, d_err, ctx->num_sms, s, ctx->tuning);
+        const uint32_t* sv = (const uint32_t*)(in_alt ? ctx->ovals_alt.p : ctx->ovals.p);
+        launch_level_rank(lv[l].n, sv, lv[l].rank, s);
+        if (l == 2)
+            launch_leaf_popc_sorted(L, sv, N.leaf_vstart, (uint64_t*)ctx->leaf_popc.p, s);
+    }
+    uint64_t* scan_status = (uint64_t*)ctx->scan_status.p;
+    const size_t scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    scan_exclusive_u64((const uint64_t*)ctx->leaf_popc.p, (uint64_t*)ctx->leaf_voff.p, L, 0, sc + SC_SCRATCH + 4,
+                       scan_status, ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    launch_window_bases(W, cnt, cnt + W, cnt + 2 * (size_t)W, base, base + (W + 1), base + 2 * (W + 1),
+                        base + 3 * (W + 1), s);
+    WindowOrderParams P;
+    P.U = (uint64_t)U;
+    P.rank_u = lv[0].rank;
+    P.rank_lo = lv[1].rank;
+    P.rank_leaf = lv[2].rank;
+    P.wkey_u = wk_u;
+    P.wkey_lo = wk_lo;
+    P.wkey_leaf = wk_leaf;
+    P.base_u = base;
+    P.base_lo = base + (W + 1);
+    P.base_leaf = base + 2 * (W + 1);
+    P.base_all = base + 3 * (W + 1);
+    P.leaf_voff = (const uint64_t*)ctx->leaf_voff.p;
+    P.V = (uint64_t)N.C.V;
+    launch_window_place(P, N, s);
+    return check_cuda(ctx, "window order");
+}
+
 // B clouds: Gaussians [h_start[b], h_start[b + 1]) with voxel size h_vs[b]
 // (h_start / h_vs null: one cloud with voxel_size)
 static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float voxel_size, float cull_scale,
@@ -239,9 +326,10 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         set_error(ctx, "vox_voxelize: missing attribute array");
         return VOX_ERR_ARGS;
     }
-    if (flags & VOX_FLAG_WINDOW_ORDER)
+    const bool window = (flags & VOX_FLAG_WINDOW_ORDER) != 0;
+    if (window && B > 1)
     {
-        set_error(ctx, "vox_voxelize: reference window node order is not available in this build");
+        set_error(ctx, "vox_voxelize_batch: the reference window node order is for one cloud per call");
         return VOX_ERR_ARGS;
     }
     ctx->diff_ready = false;
@@ -464,8 +552,25 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         return VOX_ERR_MEMORY;
     scan_status = (uint64_t*)ctx->scan_status.p;
     scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    uint64_t* win_before = nullptr;
+    if (window)
+    {
+        // windows of the reference's 256K-Gaussian batches (raster/Raster.cpp:443-444)
+        const int64_t nbatch = (G + REF_PRIM_BATCH - 1) / REF_PRIM_BATCH;
+        if (!ensure(ctx, ctx->nwin, 8 * (size_t)(nbatch + 1)) || !ensure(ctx, ctx->win_before, 8 * (size_t)(nbatch + 1)) ||
+            !ensure(ctx, ctx->cand_wkey, 8 * (size_t)(NCL + 1)))
+            return VOX_ERR_MEMORY;
+        win_before = (uint64_t*)ctx->win_before.p;
+        launch_batch_windows(frag_off, sc + SC_F, G, nbatch, (uint64_t*)ctx->nwin.p, s);
+        scan_exclusive_u64((const uint64_t*)ctx->nwin.p, win_before, nbatch, 0, sc + SC_NWIN, scan_status,
+                           ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
+    }
     LeafPassParams LP;
     memset(&LP, 0, sizeof(LP));
+    LP.window = window ? 1 : 0;
+    LP.frag_off = frag_off;
+    LP.win_before = win_before;
+    LP.cand_wkey = window ? (uint64_t*)ctx->cand_wkey.p : nullptr;
     LP.recs = recs;
     LP.vals = lvals;
     LP.emit_gid = (const uint32_t*)ctx->emit_gid.p;
@@ -628,7 +733,14 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         return rc;
     const uint64_t U = Lo > 0 ? ctx->hscal[SC_U] : 0;
     const uint64_t grid_bytes = ctx->hscal[SC_GRID_BYTES];
-    launch_canonical_order(N, U, s);
+    if (window)
+    {
+        rc = window_order(ctx, N, (int64_t)U, Lo, L, (int64_t)ctx->hscal[SC_NWIN], s);
+        if (rc)
+            return rc;
+    }
+    else
+        launch_canonical_order(N, U, s);
 
     // --------------------------------------------------------- grid buffer
     // every cloud's grid: header, node2 region, bbox, RGBA8, density, colour
@@ -868,7 +980,10 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
                       &ctx->cand_voff, &ctx->vkeys, &ctx->vslot, &ctx->vpairs, &ctx->pair_off, &ctx->cand_vbase,
-                      &ctx->partials, &ctx->exp_keys, &ctx->exp_ids };
+                      &ctx->partials, &ctx->exp_keys, &ctx->exp_ids, &ctx->nwin, &ctx->win_before,
+                      &ctx->cand_wkey, &ctx->wkey_u, &ctx->wkey_lo, &ctx->wkey_leaf, &ctx->wcnt, &ctx->wbase,
+                      &ctx->okeys, &ctx->okeys_alt, &ctx->ovals, &ctx->ovals_alt, &ctx->rank_u, &ctx->rank_lo,
+                      &ctx->rank_leaf, &ctx->leaf_popc, &ctx->leaf_voff };
     for (DevBuf* b : all)
         if (b->p)
             cudaFree(b->p);

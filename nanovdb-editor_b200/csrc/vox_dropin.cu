@@ -68,6 +68,10 @@ static float cull_from_params(pnanovdb_compute_array_t** shader_params_arrays)
     return cull;
 }
 
+// The reference's table entries return the reference's node order: node_idx,
+// node2 addresses and value indices of its window-by-window build.
+constexpr uint32_t DROPIN_ORDER = VOX_FLAG_WINDOW_ORDER;
+
 // ------------------------------------------------------------------ arrays
 // Grids returned to the caller live in page-locked host memory so the
 // device-to-host copy runs at link speed.  Page-locking is slow, so blocks
@@ -412,7 +416,7 @@ static void PNANOVDB_ABI r_raster_gaussian_3d(const pnanovdb_compute_t*, pnanovd
     g.colors = d->dev + 11 * n;
     void* grid = nullptr;
     uint64_t bytes = 0;
-    if (vox_voxelize(ctx->vox, &g, voxel_size, d->cull_scale, d->raw ? VOX_FLAG_RAW_INPUTS : 0u, &grid, &bytes) !=
+    if (vox_voxelize(ctx->vox, &g, voxel_size, d->cull_scale, (d->raw ? VOX_FLAG_RAW_INPUTS : 0u) | DROPIN_ORDER, &grid, &bytes) !=
         VOX_OK)
         return;
     uint64_t cap = word_count * 4ull;
@@ -477,7 +481,7 @@ static pnanovdb_compute_array_t* PNANOVDB_ABI r_raster_to_nanovdb(
     g.scales = d->scales.data();
     g.opacities = d->opacities.data();
     g.colors = d->colors.data();
-    pnanovdb_compute_array_t* a = run_host(queue_device(queue), &g, voxel_size, d->cull_scale, 0u, profiler_report,
+    pnanovdb_compute_array_t* a = run_host(queue_device(queue), &g, voxel_size, d->cull_scale, DROPIN_ORDER, profiler_report,
                                            userdata);
     r_destroy_gaussian_data(nullptr, nullptr, d);
     return a;
@@ -515,7 +519,7 @@ static pnanovdb_bool_t PNANOVDB_ABI r_from_arrays(pnanovdb_raster_t*, const pnan
     g.scales = (const float*)s->data;
     g.opacities = (const float*)o->data;
     g.colors = (const float*)c->data;
-    *out = run_host(queue_device(queue), &g, voxel_size, 0.05f, VOX_FLAG_RAW_INPUTS, nullptr, nullptr);
+    *out = run_host(queue_device(queue), &g, voxel_size, 0.05f, VOX_FLAG_RAW_INPUTS | DROPIN_ORDER, nullptr, nullptr);
     return *out ? PNANOVDB_TRUE : PNANOVDB_FALSE;
 }
 

@@ -263,6 +263,8 @@ struct LeafQSmem
     uint32_t res_rgba[LQ_CHUNK][512];
     uint32_t pbits[512];
     uint64_t mask[8];
+    uint64_t wf0[LQ_CHUNK], wbase[LQ_CHUNK]; // reference windows: fragment offset in its batch, windows before
+    uint64_t wmin;
     uint32_t qn, pairs, cand;
 };
 
@@ -279,6 +281,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
         {
             S.cand = atomicAdd(counter, 1u);
             S.pairs = 0;
+            S.wmin = ~0ull;
         }
         if (t < 8)
             S.mask[t] = 0;
@@ -304,6 +307,12 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
                 {
                     S.gid[j] = g;
                     S.flag[j] = P.emit_flag ? P.emit_flag[e] : 0;
+                    if (P.window)
+                    {
+                        const int64_t batch = (int64_t)g / REF_PRIM_BATCH;
+                        S.wf0[j] = P.frag_off[g] - P.frag_off[batch * REF_PRIM_BATCH];
+                        S.wbase[j] = P.win_before[batch];
+                    }
                 }
             }
             S.pbits[t] = 0;
@@ -457,6 +466,15 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
                 S.res_a[j][n] = a;
                 S.res_rgba[j][n] = pack_rgba8(R, a8);
                 atomicOr(&S.pbits[n], 1u << j);
+                if (P.window)
+                {
+                    // the reference's window of this fragment: x-major index in the bbox
+                    // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
+                    const uint64_t r = (uint64_t)(x - R.q4.x) * (uint64_t)R.q5.y * (uint64_t)R.q5.z +
+                                       (uint64_t)(yy - R.q4.y) * (uint64_t)R.q5.z + (uint64_t)(zz - R.q4.z);
+                    atomicMin((unsigned long long*)&S.wmin,
+                              (unsigned long long)(S.wbase[j] + (S.wf0[j] + r) / REF_WINDOW));
+                }
             }
             __syncthreads();
             // ---- sum in ascending Gaussian id
@@ -514,6 +532,8 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
             P.cand_mask[8 * (uint64_t)c + t] = S.mask[t];
         if (t == 0 && S.pairs)
             atomicAdd((unsigned long long*)P.total_pairs, (unsigned long long)S.pairs);
+        if (t == 0 && P.window)
+            P.cand_wkey[c] = S.wmin;
         __syncthreads();
     }
 }

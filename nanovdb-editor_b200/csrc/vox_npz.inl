@@ -265,6 +265,6 @@ static pnanovdb_bool_t PNANOVDB_ABI r_raster_file(pnanovdb_raster_t* raster, con
     g.scales = (const float*)ca[3]->data;
     g.colors = (const float*)ca[4]->data;
     *nanovdb_arr = run_host(queue_device(queue), &g, voxel_size, cull_from_params(shader_params_arrays),
-                            VOX_FLAG_RAW_INPUTS, profiler_report, userdata);
+                            VOX_FLAG_RAW_INPUTS | DROPIN_ORDER, profiler_report, userdata);
     return *nanovdb_arr ? PNANOVDB_TRUE : PNANOVDB_FALSE;
 }

@@ -151,6 +151,11 @@ struct LeafPassParams
     const float* grad_density;
     const float* grad_color;
     float* partials;            // [emission index][BWD_NACC]
+    // reference node order: creation window of each candidate leaf
+    int window;
+    const uint64_t* frag_off;   // exclusive scan of footprints
+    const uint64_t* win_before; // windows of the earlier 256K-Gaussian batches
+    uint64_t* cand_wkey;        // [NCL]
     // pair export
     const uint64_t* cand_voff;  // [NCL] first voxel (run order) of each candidate
     const uint64_t* pair_off;   // [V] first pair of each voxel
@@ -186,6 +191,34 @@ struct ValueParams
     uint8_t* out;
 };
 void launch_values(const ValueParams& A, const NodeParams& N, cudaStream_t s);
+
+// the reference's fragment batches and windows (raster/Raster.cpp:443-444)
+constexpr int64_t REF_PRIM_BATCH = 262144; // Gaussians per batch (2^18)
+constexpr uint64_t REF_WINDOW = 8388608;   // fragments per window
+
+struct WindowOrderParams
+{
+    uint64_t U;
+    const uint32_t *rank_u, *rank_lo, *rank_leaf;   // position in each level's (window, parent, n) order
+    const uint64_t *wkey_u, *wkey_lo, *wkey_leaf;   // creation window
+    const uint64_t *base_u, *base_lo, *base_leaf, *base_all; // [windows + 1] nodes in earlier windows
+    const uint64_t* leaf_voff; // voxels of the leaves before, in node_idx order
+    uint64_t V;                // active voxels
+};
+void launch_batch_windows(const uint64_t* frag_off, const uint64_t* F_total, int64_t G, int64_t nbatch,
+                          uint64_t* nwin, cudaStream_t s);
+void launch_leaf_wkey(int64_t L, const uint32_t* leaf_vstart, const uint32_t* vslot, const uint64_t* cand_wkey,
+                      uint64_t* leaf_wkey, cudaStream_t s);
+void launch_run_min(int64_t n, const uint32_t* start, const uint64_t* child, uint64_t* out, cudaStream_t s);
+void launch_level_keys(int64_t n, const uint64_t* wkey, const uint32_t* parent, const uint32_t* parent_rank,
+                       const uint32_t* nval, uint32_t nmask, uint64_t* keys, uint32_t* vals, uint64_t* wcount,
+                       cudaStream_t s);
+void launch_level_rank(int64_t n, const uint32_t* sorted_vals, uint32_t* rank, cudaStream_t s);
+void launch_leaf_popc_sorted(int64_t L, const uint32_t* sorted_vals, const uint32_t* leaf_vstart, uint64_t* out,
+                             cudaStream_t s);
+void launch_window_bases(int64_t nw, const uint64_t* cu, const uint64_t* clo, const uint64_t* cleaf, uint64_t* base_u,
+                         uint64_t* base_lo, uint64_t* base_leaf, uint64_t* base_all, cudaStream_t s);
+void launch_window_place(const WindowOrderParams& W, const NodeParams& N, cudaStream_t s);
 
 void launch_bwd_finalize(const BwdFinalParams& F, cudaStream_t s);
 

@@ -150,3 +150,35 @@ def test_leaf_bound_never_skips_a_passing_voxel(oracle_mod):
             assert g.counts["pairs"] > 0
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("make,vs", [
+    (lambda: W.plain_cloud(100_000, 0), 0.01),      # the 100k workload: 12 fragment windows
+    (lambda: W.plain_cloud(270_000, 21), 0.02),     # two 256K-Gaussian batches
+    (lambda: W.pytest_cloud(), 1.0 / 8.0),          # one window
+])
+def test_reference_window_order(vox_ctx, oracle_mod, make, vs):
+    """VOX_FLAG_WINDOW_ORDER: node_idx, node2 addresses and value indices follow
+    the reference's 256K-Gaussian x 8M-fragment window build, byte for byte
+    against the oracle's window-by-window restatement."""
+    from nanovdb_editor.vox import FLAG_WINDOW_ORDER
+
+    cloud = make()
+    g = vox_ctx.voxelize_host(cloud["means"], cloud["quats"], cloud["scales"], cloud["opacities"], cloud["colors"], vs,
+                              0.05, flags=FLAG_WINDOW_ORDER)
+    ref = oracle_mod.OracleResult(cloud, vs, 0.05, window_mode=1)
+    assert ref.counts["error"] == 0
+    assert int(g.header["node_order"]) == 1
+    n2 = ref.node2()
+    if not np.array_equal(g.node2, n2):
+        bad = np.nonzero(g.node2.view(np.uint64) != n2.view(np.uint64))[0] if g.node2.shape == n2.shape else []
+        pytest.fail(f"node2 differs (windows {ref.counts['windows']}): {len(bad)} words, first {bad[:8]}")
+    v = ref.values()
+    np.testing.assert_array_equal(g.rgba8, v["rgba8"])
+    np.testing.assert_array_equal(g.density, v["density"])
+    np.testing.assert_array_equal(g.color, v["color"])
+    k_ref, i_ref = ref.pairs()
+    k_got, i_got = vox_ctx.pairs()
+    np.testing.assert_array_equal(k_got, k_ref)
+    np.testing.assert_array_equal(i_got, i_ref)
+    ref.close()
