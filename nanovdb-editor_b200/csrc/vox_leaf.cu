@@ -268,8 +268,8 @@ struct LeafQSmem
     uint32_t qn, pairs, cand;
 };
 
-template <bool CHECK>
-__global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint32_t* counter)
+template <bool CHECK, bool WINDOW>
+__global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, uint32_t* counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LeafQSmem& S = *reinterpret_cast<LeafQSmem*>(smem_raw);
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
                 {
                     S.gid[j] = g;
                     S.flag[j] = P.emit_flag ? P.emit_flag[e] : 0;
-                    if (P.window)
+                    if (WINDOW)
                     {
                         const int64_t batch = (int64_t)g / REF_PRIM_BATCH;
                         S.wf0[j] = P.frag_off[g] - P.frag_off[batch * REF_PRIM_BATCH];
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
                 S.res_a[j][n] = a;
                 S.res_rgba[j][n] = pack_rgba8(R, a8);
                 atomicOr(&S.pbits[n], 1u << j);
-                if (P.window)
+                if (WINDOW)
                 {
                     // the reference's window of this fragment: x-major index in the bbox
                     // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_pass(LeafPassParams P, uint
             P.cand_mask[8 * (uint64_t)c + t] = S.mask[t];
         if (t == 0 && S.pairs)
             atomicAdd((unsigned long long*)P.total_pairs, (unsigned long long)S.pairs);
-        if (t == 0 && P.window)
+        if (WINDOW && t == 0)
             P.cand_wkey[c] = S.wmin;
         __syncthreads();
     }
@@ -547,17 +547,33 @@ __device__ __forceinline__ uint32_t mask_rank(const uint64_t* m, uint32_t n)
 }
 
 // adjoint: per candidate leaf, per Gaussian, the sum of its pairs' terms over
-// the leaf's voxels (block reduction), stored by emission index
+// the leaf's voxels, stored by the leaf pair's emission index.  Same chunked,
+// dense candidate layout as the forward walk; the terms of a round are reduced
+// per Gaussian across each warp (its lanes hold consecutive candidates, so a
+// Gaussian's lanes are contiguous) into per-warp shared slots, which are summed
+// in warp order at the end of the chunk: deterministic, no atomics.
+struct LeafBSmem
+{
+    GaussRec rec[LQ_CHUNK];
+    uint32_t eidx[LQ_CHUNK];
+    int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK];
+    uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK], bdiv_y[LQ_CHUNK], bdiv_z[LQ_CHUNK], bvol[LQ_CHUNK];
+    float sxy_lo[3][LQ_CHUNK * 64], sxy_hi[3][LQ_CHUNK * 64];
+    float mz[LQ_CHUNK][3], inv_s[LQ_CHUNK][3], inv_ls[LQ_CHUNK], posz[LQ_CHUNK], vs[LQ_CHUNK];
+    float part[LP_THREADS / 32][LQ_CHUNK][BWD_NACC];
+    uint64_t mask[8];
+    uint32_t cand;
+};
+
 __global__ void __launch_bounds__(LP_THREADS) k_leaf_backward(LeafPassParams P, uint32_t* counter)
 {
-    __shared__ LeafSmem S;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    LeafBSmem& S = *reinterpret_cast<LeafBSmem*>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     while (true)
     {
         if (t == 0)
             S.cand = atomicAdd(counter, 1u);
-        if (t < 8)
-            S.mask[t] = 0;
         __syncthreads();
         const int64_t c = S.cand;
         if (c >= P.NCL)
@@ -566,93 +582,178 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_backward(LeafPassParams P, 
             S.mask[t] = P.cand_mask[8 * (uint64_t)c + t];
         int32_t o[3];
         cand_origin(P, P.cand_key[c], o);
-        __syncthreads();
-        const int32_t xa = o[0] + (t >> 6), y = o[1] + ((t >> 3) & 7), z = o[2] + (t & 7), xb = xa + 4;
-        // upstream gradients of this thread's voxels (value-concatenated arrays)
-        float gd[2] = { 0.f, 0.f }, gc[2][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
-        bool act[2];
-#pragma unroll
-        for (int h = 0; h < 2; h++)
-        {
-            const uint32_t n = (uint32_t)(t + 256 * h);
-            act[h] = (S.mask[n >> 6] >> (n & 63)) & 1ull;
-            if (act[h])
-            {
-                const uint64_t vi = P.cand_vbase[c] + mask_rank(S.mask, n);
-                if (P.grad_density)
-                    gd[h] = P.grad_density[vi];
-                if (P.grad_color)
-                    for (int k = 0; k < 3; k++)
-                        gc[h][k] = P.grad_color[3 * vi + k];
-            }
-        }
+        const uint64_t vbase = P.cand_vbase[c];
         const uint32_t p0 = P.cand_start[c], p1 = P.cand_start[c + 1];
-        for (uint32_t q0 = p0; q0 < p1; q0 += LP_CHUNK)
+        for (uint32_t q0 = p0; q0 < p1; q0 += LQ_CHUNK)
         {
-            const uint32_t cnt = min((uint32_t)LP_CHUNK, p1 - q0);
-            stage_chunk(P, S, q0, cnt);
-            __syncthreads();
-            for (uint32_t j = 0; j < cnt; j++)
+            const uint32_t cnt = min((uint32_t)LQ_CHUNK, p1 - q0);
+            if (t < (int)cnt * 8)
             {
+                const uint32_t j = (uint32_t)t >> 3, w = (uint32_t)t & 7u;
+                const uint32_t e = P.vals[q0 + j];
+                const uint32_t g = P.emit_gid[e];
+                reinterpret_cast<float4*>(&S.rec[j])[w] = reinterpret_cast<const float4*>(&P.recs[g])[w];
+                if (w == 0)
+                    S.eidx[j] = e;
+            }
+            for (int i = t; i < (LP_THREADS / 32) * LQ_CHUNK * BWD_NACC; i += LP_THREADS)
+                (&S.part[0][0][0])[i] = 0.f;
+            __syncthreads();
+            if (t < (int)cnt)
+            {
+                const GaussRec& R = S.rec[t];
+                const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
+                const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
+                const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
+                const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
+                const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
+                S.bx0[t] = x0;
+                S.by0[t] = y0;
+                S.bz0[t] = z0;
+                S.bny[t] = ny;
+                S.bnz[t] = nz;
+                S.bdiv_y[t] = (65536u + ny - 1u) / ny;
+                S.bdiv_z[t] = (65536u + nz - 1u) / nz;
+                S.bvol[t] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny * nz;
+                const RInv M = rinv_of(R);
+                S.mz[t][0] = M.m[0][2];
+                S.mz[t][1] = M.m[1][2];
+                S.mz[t][2] = M.m[2][2];
+                S.inv_s[t][0] = R.q3.y;
+                S.inv_s[t][1] = R.q3.z;
+                S.inv_s[t][2] = R.q3.w;
+                S.inv_ls[t] = R.q0.w;
+                S.posz[t] = R.q0.z;
+                S.vs[t] = rec_vs(R, P.voxel_size, P.cloud_vs);
+            }
+            for (uint32_t idx = (uint32_t)t; idx < cnt * 64; idx += LP_THREADS)
+            {
+                const uint32_t j = idx >> 6, col = idx & 63u;
                 const GaussRec& R = S.rec[j];
-                float acc[BWD_NACC];
-#pragma unroll
-                for (int i = 0; i < BWD_NACC; i++)
-                    acc[i] = 0.f;
                 const RInv M = rinv_of(R);
                 const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+                float cx0, cx1, cy0, cy1;
+                axis_corners(vsf, R.q0.x, o[0] + (int32_t)(col >> 3), cx0, cx1);
+                axis_corners(vsf, R.q0.y, o[1] + (int32_t)(col & 7u), cy0, cy1);
 #pragma unroll
-                for (int h = 0; h < 2; h++)
+                for (int r = 0; r < 3; r++)
                 {
-                    const int32_t x = h ? xb : xa;
-                    if (!act[h] || !in_bbox(R, x, y, z))
-                        continue;
-                    if (!aabb_hits_unit_sphere(voxel_local_aabb(R, M, vsf, x, y, z)))
-                        continue;
-                    SmoothTerms st;
-                    const float Kw = smooth_kernel(R, M, vsf, x, y, z, st);
-                    if (!(st.e > SMOOTH_TAU))
-                        continue;
-                    const float GK = gd[h] + gc[h][0] * R.q7.x + gc[h][1] * R.q7.y + gc[h][2] * R.q7.z;
-                    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
-                    acc[0] += GK * st.E;
+                    float xn, xx, yn, yx;
+                    minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
+                    minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
+                    S.sxy_lo[r][idx] = VOX_FADD(xn, yn);
+                    S.sxy_hi[r][idx] = VOX_FADD(xx, yx);
+                }
+            }
+            __syncthreads();
+            uint32_t start[LQ_CHUNK + 1];
+            start[0] = 0;
+#pragma unroll
+            for (int j = 0; j < LQ_CHUNK; j++)
+                start[j + 1] = start[j] + (j < (int)cnt ? S.bvol[j] : 0u);
+            const uint32_t T = start[LQ_CHUNK];
+            for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
+            {
+                const uint32_t e = b0 + (uint32_t)t;
+                int j = LQ_CHUNK; // past every Gaussian for lanes without a candidate
+                float cc[BWD_NACC];
+#pragma unroll
+                for (int i = 0; i < BWD_NACC; i++)
+                    cc[i] = 0.f;
+                if (e < T)
+                {
+                    j = 0;
+#pragma unroll
+                    for (int q = 1; q < LQ_CHUNK; q++)
+                        j += e >= start[q] ? 1 : 0;
+                    const uint32_t local = e - start[j];
+                    const uint32_t rest = (local * S.bdiv_z[j]) >> 16;
+                    const uint32_t dz = local - rest * S.bnz[j];
+                    const uint32_t dx = (rest * S.bdiv_y[j]) >> 16;
+                    const uint32_t dy = rest - dx * S.bny[j];
+                    const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz = S.bz0[j] + (int32_t)dz;
+                    const uint32_t ci = (uint32_t)j * 64u + (uint32_t)(rx * 8 + ry);
+                    const float vsf = S.vs[j], pz = S.posz[j], il = S.inv_ls[j];
+                    const float v0 = (float)(o[2] + rz);
+                    const float v1 = VOX_FADD(v0, 1.f);
+                    const float c0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz);
+                    const float c1 = VOX_FSUB(VOX_FMUL(v1, vsf), pz);
+                    float d2 = 1.f;
 #pragma unroll
                     for (int r = 0; r < 3; r++)
                     {
-                        const float dz = -GK * st.e * st.z[r];
-                        const float du = dz * inv_s[r];
-                        acc[1 + r] += du;
-                        acc[4 + r] += dz * st.z[r];
-#pragma unroll
-                        for (int a = 0; a < 3; a++)
-                            acc[7 + 3 * r + a] += du * st.d[a];
+                        float zn, zx;
+                        minmax_prod(c0, c1, S.mz[j][r], zn, zx);
+                        const float lo = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_lo[r][ci], zn), il), S.inv_s[j][r]);
+                        const float hi = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_hi[r][ci], zx), il), S.inv_s[j][r]);
+                        if (0.f < lo)
+                            d2 = VOX_FSUB(d2, VOX_FMUL(lo, lo));
+                        else if (0.f > hi)
+                            d2 = VOX_FSUB(d2, VOX_FMUL(hi, hi));
                     }
-                    acc[16] += Kw * gc[h][0];
-                    acc[17] += Kw * gc[h][1];
-                    acc[18] += Kw * gc[h][2];
-                }
+                    if (d2 > 0.f)
+                    {
+                        const GaussRec& R = S.rec[j];
+                        const RInv M = rinv_of(R);
+                        SmoothTerms st;
+                        const float Kw = smooth_kernel(R, M, vsf, o[0] + rx, o[1] + ry, o[2] + rz, st);
+                        if (st.e > SMOOTH_TAU)
+                        {
+                            const uint32_t n = (uint32_t)((rx << 6) | (ry << 3) | rz);
+                            const uint64_t vi = vbase + mask_rank(S.mask, n);
+                            const float gd = P.grad_density ? P.grad_density[vi] : 0.f;
+                            float gc[3] = { 0.f, 0.f, 0.f };
+                            if (P.grad_color)
+                                for (int k = 0; k < 3; k++)
+                                    gc[k] = P.grad_color[3 * vi + k];
+                            const float GK = gd + gc[0] * R.q7.x + gc[1] * R.q7.y + gc[2] * R.q7.z;
+                            cc[0] = GK * st.E;
 #pragma unroll
-                for (int i = 0; i < BWD_NACC; i++)
-                {
-                    float v = acc[i];
+                            for (int r = 0; r < 3; r++)
+                            {
+                                const float dzr = -GK * st.e * st.z[r];
+                                const float du = dzr * S.inv_s[j][r];
+                                cc[1 + r] = du;
+                                cc[4 + r] = dzr * st.z[r];
 #pragma unroll
-                    for (int off = 16; off; off >>= 1)
-                        v += __shfl_xor_sync(0xffffffffu, v, off);
-                    if (lane == 0)
-                        S.red[warp][i] = v;
+                                for (int a = 0; a < 3; a++)
+                                    cc[7 + 3 * r + a] = du * st.d[a];
+                            }
+                            cc[16] = Kw * gc[0];
+                            cc[17] = Kw * gc[1];
+                            cc[18] = Kw * gc[2];
+                        }
+                    }
                 }
-                __syncthreads();
-                if (t < BWD_NACC)
+                // per Gaussian present in this warp (lanes of one Gaussian are contiguous)
+                const int jlo = __shfl_sync(0xffffffffu, j, 0);
+                const int jhi = min(__shfl_sync(0xffffffffu, j, 31), (int)cnt - 1);
+                for (int jx = jlo; jx <= jhi; jx++)
                 {
-                    float v = 0.f;
-                    for (int w = 0; w < LP_THREADS / 32; w++)
-                        v += S.red[w][t];
-                    P.partials[(uint64_t)S.eidx[j] * BWD_NACC + t] = v;
+                    const bool mine = j == jx;
+#pragma unroll
+                    for (int i = 0; i < BWD_NACC; i++)
+                    {
+                        float v = mine ? cc[i] : 0.f;
+#pragma unroll
+                        for (int off = 16; off; off >>= 1)
+                            v += __shfl_xor_sync(0xffffffffu, v, off);
+                        if (lane == 0)
+                            S.part[warp][jx][i] += v;
+                    }
                 }
-                __syncthreads();
             }
+            __syncthreads();
+            if (t < (int)cnt * BWD_NACC)
+            {
+                const int j = t / BWD_NACC, i = t % BWD_NACC;
+                float v = 0.f;
+                for (int w = 0; w < LP_THREADS / 32; w++)
+                    v += S.part[w][j][i];
+                P.partials[(uint64_t)S.eidx[j] * BWD_NACC + i] = v;
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
@@ -827,7 +928,8 @@ void launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, c
         return;
     cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     const size_t smem = sizeof(LeafQSmem);
-    auto kern = P.emit_flag ? k_leaf_pass<true> : k_leaf_pass<false>;
+    auto kern = P.emit_flag ? (P.window ? k_leaf_pass<true, true> : k_leaf_pass<true, false>)
+                            : (P.window ? k_leaf_pass<false, true> : k_leaf_pass<false, false>);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LP_THREADS, smem);
@@ -842,7 +944,14 @@ void launch_leaf_backward(const LeafPassParams& P, uint32_t* counter, int num_sm
     if (P.NCL <= 0)
         return;
     cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-    { k_leaf_backward<<<walk_grid(P.NCL, num_sms), LP_THREADS, 0, s>>>(P, counter); count_launch(); }
+    const size_t smem = sizeof(LeafBSmem);
+    cudaFuncSetAttribute(k_leaf_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf_backward, LP_THREADS, smem);
+    int64_t grid = (int64_t)num_sms * (per_sm > 0 ? per_sm : 1);
+    if (grid > P.NCL)
+        grid = P.NCL;
+    { k_leaf_backward<<<(unsigned)grid, LP_THREADS, smem, s>>>(P, counter); count_launch(); }
 }
 
 void launch_leaf_export(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s)
