@@ -360,23 +360,24 @@ __device__ __forceinline__ bool aabb_hits_unit_sphere(const Aabb& b)
 // lattice p = w * hi + (1 - w) * lo.  |p|^2 = fl(fl(x^2 + y^2) + z^2) is
 // monotone in each per-axis square and exp (vox_expf_cr) is monotone, so the
 // maximum is the lattice point with the per-axis smallest square.
+// Lattice weights w_s = fl(fl(1/3) * s), 1 - w_s rounded (s = 1, 2); s = 0 and
+// s = 3 (w = 1 exactly) give p = lo and p = hi.
+constexpr float LAT_W1 = 0x1.555556p-2f, LAT_OW1 = 0x1.555554p-1f;
+constexpr float LAT_W2 = 0x1.555556p-1f, LAT_OW2 = 0x1.555554p-2f;
 __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
 {
-    const float third = VOX_FDIV(1.f, 3.f);
     float m[3];
 #pragma unroll
     for (int a = 0; a < 3; a++)
     {
-        float best = 0.f;
-#pragma unroll
-        for (int s = 0; s < 4; s++)
-        {
-            float w = VOX_FMUL(third, (float)s);
-            float ow = VOX_FSUB(1.f, w);
-            float p = VOX_FADD(VOX_FMUL(w, b.hi[a]), VOX_FMUL(ow, b.lo[a]));
-            float sq = VOX_FMUL(p, p);
-            best = (s == 0 || sq < best) ? sq : best;
-        }
+        const float p1 = VOX_FADD(VOX_FMUL(LAT_W1, b.hi[a]), VOX_FMUL(LAT_OW1, b.lo[a]));
+        const float p2 = VOX_FADD(VOX_FMUL(LAT_W2, b.hi[a]), VOX_FMUL(LAT_OW2, b.lo[a]));
+        const float s0 = VOX_FMUL(b.lo[a], b.lo[a]), s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2),
+                    s3 = VOX_FMUL(b.hi[a], b.hi[a]);
+        float best = s0;
+        best = s1 < best ? s1 : best;
+        best = s2 < best ? s2 : best;
+        best = s3 < best ? s3 : best;
         m[a] = best;
     }
     float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);

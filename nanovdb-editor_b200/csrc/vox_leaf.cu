@@ -236,9 +236,11 @@ __device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S
 // ------------------------------------------------------ forward leaf walk
 // Per chunk of LQ_CHUNK Gaussians (ascending id) staged in shared memory:
 //   box    the part of each Gaussian's bbox inside the leaf;
-//   test   the boxes' voxels laid out densely, one candidate per thread, the
-//          reference test on each; passing (Gaussian, voxel) pairs go to a
-//          shared queue (any order);
+//   test   the boxes' columns laid out densely, one (Gaussian, column) per
+//          thread: the x / y share of the reference test once per column, then
+//          the column's z run in order, each z's corner products shared with
+//          the next; passing (Gaussian, voxel) pairs go to a shared queue (any
+//          order);
 //   alpha  the RGBA8 byte and the float-channel alpha of every queued pair,
 //          one pair per thread, into a per-(Gaussian, voxel) table;
 //   sum    each thread folds its two voxels' table entries in ascending
@@ -252,12 +254,9 @@ struct LeafQSmem
     uint8_t flag[LQ_CHUNK];
     int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK]; // box origin, leaf-relative
     uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK];               // box extents in y and z
-    uint32_t bdiv_y[LQ_CHUNK], bdiv_z[LQ_CHUNK];         // 65536 / extent, rounded up (exact division below 512)
-    uint32_t bvol[LQ_CHUNK];
-    // the x / y share of the reference test per (Gaussian, leaf column):
-    // rounded sums of the per-axis minimum / maximum corner products
-    float sxy_lo[3][LQ_CHUNK * 64], sxy_hi[3][LQ_CHUNK * 64];
-    float mz[LQ_CHUNK][3], inv_s[LQ_CHUNK][3], inv_ls[LQ_CHUNK], posz[LQ_CHUNK], vs[LQ_CHUNK];
+    uint32_t bdiv_y[LQ_CHUNK];                           // 65536 / ny, rounded up (exact division below 64)
+    uint32_t bcol[LQ_CHUNK];                             // box columns, nx * ny (0: empty box)
+    float vs[LQ_CHUNK];
     uint16_t queue[LQ_CHUNK * 512];
     float res_a[LQ_CHUNK][512];
     uint32_t res_rgba[LQ_CHUNK][512];
@@ -274,7 +273,6 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LeafQSmem& S = *reinterpret_cast<LeafQSmem*>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
     while (true)
     {
         if (t == 0)
@@ -335,101 +333,100 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
                 S.bny[t] = ny;
                 S.bnz[t] = nz;
                 S.bdiv_y[t] = (65536u + ny - 1u) / ny;
-                S.bdiv_z[t] = (65536u + nz - 1u) / nz;
-                S.bvol[t] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny * nz;
-                const RInv M = rinv_of(R);
-                S.mz[t][0] = M.m[0][2];
-                S.mz[t][1] = M.m[1][2];
-                S.mz[t][2] = M.m[2][2];
-                S.inv_s[t][0] = R.q3.y;
-                S.inv_s[t][1] = R.q3.z;
-                S.inv_s[t][2] = R.q3.w;
-                S.inv_ls[t] = R.q0.w;
-                S.posz[t] = R.q0.z;
+                S.bcol[t] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
                 S.vs[t] = rec_vs(R, P.voxel_size, P.cloud_vs);
-            }
-            // ---- column shares (every column of the leaf, bbox or not: cheap)
-            for (uint32_t idx = (uint32_t)t; idx < cnt * 64; idx += LP_THREADS)
-            {
-                const uint32_t j = idx >> 6, col = idx & 63u;
-                const GaussRec& R = S.rec[j];
-                const RInv M = rinv_of(R);
-                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
-                float cx0, cx1, cy0, cy1;
-                axis_corners(vsf, R.q0.x, o[0] + (int32_t)(col >> 3), cx0, cx1);
-                axis_corners(vsf, R.q0.y, o[1] + (int32_t)(col & 7u), cy0, cy1);
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-                {
-                    float xn, xx, yn, yx;
-                    minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
-                    minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
-                    S.sxy_lo[r][idx] = VOX_FADD(xn, yn);
-                    S.sxy_hi[r][idx] = VOX_FADD(xx, yx);
-                }
             }
             __syncthreads();
             uint32_t start[LQ_CHUNK + 1];
             start[0] = 0;
 #pragma unroll
             for (int j = 0; j < LQ_CHUNK; j++)
-                start[j + 1] = start[j] + (j < (int)cnt ? S.bvol[j] : 0u);
+                start[j + 1] = start[j] + (j < (int)cnt ? S.bcol[j] : 0u);
             const uint32_t T = start[LQ_CHUNK];
-            // ---- test, one candidate per thread
+            // ---- test, one box column per thread.  Bit-identical to
+            // voxel_local_aabb + aabb_hits_unit_sphere per voxel: the z corner
+            // c1 of voxel z is c0 of voxel z + 1 (integer-valued floats), and
+            // "lo > 0: subtract lo^2, else hi < 0: subtract hi^2" selects the
+            // pre-scale sum with the same sign (inv_ls, inv_s > 0; an underflow
+            // to zero subtracts zero).
             for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
             {
                 const uint32_t e = b0 + (uint32_t)t;
-                bool pass = false;
-                uint32_t entry = 0;
+                uint32_t zmask = 0, ebase = 0;
                 if (e < T)
                 {
                     int j = 0;
+                    uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
 #pragma unroll
                     for (int q = 1; q < LQ_CHUNK; q++)
-                        j += e >= start[q] ? 1 : 0;
-                    const uint32_t local = e - start[j];
-                    const uint32_t rest = (local * S.bdiv_z[j]) >> 16;
-                    const uint32_t dz = local - rest * S.bnz[j];
-                    const uint32_t dx = (rest * S.bdiv_y[j]) >> 16;
-                    const uint32_t dy = rest - dx * S.bny[j];
-                    const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz = S.bz0[j] + (int32_t)dz;
-                    // the reference test with the staged x / y shares (bit-identical to
-                    // voxel_local_aabb + aabb_hits_unit_sphere)
-                    const uint32_t ci = (uint32_t)j * 64u + (uint32_t)(rx * 8 + ry);
-                    const float vsf = S.vs[j], pz = S.posz[j], il = S.inv_ls[j];
-                    const float v0 = (float)(o[2] + rz);
-                    const float v1 = VOX_FADD(v0, 1.f);
-                    const float c0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz);
-                    const float c1 = VOX_FSUB(VOX_FMUL(v1, vsf), pz);
-                    float d2 = 1.f;
+                    {
+                        const bool ge = e >= start[q];
+                        j += ge ? 1 : 0;
+                        sj = ge ? start[q] : sj;
+                    }
+                    const uint32_t local = e - sj;
+                    const uint32_t dx = (local * S.bdiv_y[j]) >> 16;
+                    const uint32_t dy = local - dx * S.bny[j];
+                    const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz0 = S.bz0[j];
+                    const GaussRec& R = S.rec[j];
+                    const RInv M = rinv_of(R);
+                    const float vsf = S.vs[j], il = R.q0.w, pz = R.q0.z;
+                    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+                    float cx0, cx1, cy0, cy1;
+                    axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
+                    axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
+                    float slo[3], shi[3], pa[3];
+                    float v = (float)(o[2] + rz0);
+                    float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
 #pragma unroll
                     for (int r = 0; r < 3; r++)
                     {
-                        float zn, zx;
-                        minmax_prod(c0, c1, S.mz[j][r], zn, zx);
-                        const float lo = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_lo[r][ci], zn), il), S.inv_s[j][r]);
-                        const float hi = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_hi[r][ci], zx), il), S.inv_s[j][r]);
-                        if (0.f < lo)
-                            d2 = VOX_FSUB(d2, VOX_FMUL(lo, lo));
-                        else if (0.f > hi)
-                            d2 = VOX_FSUB(d2, VOX_FMUL(hi, hi));
+                        float xn, xx, yn, yx;
+                        minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
+                        minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
+                        slo[r] = VOX_FADD(xn, yn);
+                        shi[r] = VOX_FADD(xx, yx);
+                        pa[r] = VOX_FMUL(cz, M.m[r][2]);
                     }
-                    pass = d2 > 0.f;
-                    entry = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz);
-                    if (CHECK && pass && S.flag[j])
+                    const uint32_t nz = S.bnz[j];
+                    for (uint32_t k = 0; k < nz; k++)
+                    {
+                        v = VOX_FADD(v, 1.f);
+                        cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                        float d2 = 1.f;
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+                        {
+                            const float pb = VOX_FMUL(cz, M.m[r][2]);
+                            const float zn = pa[r] < pb ? pa[r] : pb, zx = pa[r] < pb ? pb : pa[r];
+                            pa[r] = pb;
+                            const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
+                            const float x = 0.f < xl ? xl : (0.f > xh ? xh : 0.f);
+                            const float sv = VOX_FMUL(VOX_FMUL(x, il), is[r]);
+                            d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
+                        }
+                        zmask |= (d2 > 0.f ? 1u : 0u) << k;
+                    }
+                    ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
+                    if (CHECK && zmask && S.flag[j])
                         atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
                 }
-                const uint32_t bal = __ballot_sync(0xffffffffu, pass);
-                if (bal)
+                // queue slots: warp inclusive scan of the pass counts, one shared atomic per warp
+                const uint32_t np = (uint32_t)__popc(zmask);
+                uint32_t incl = np;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1)
                 {
-                    const int leader = __ffs(bal) - 1;
-                    uint32_t qb = 0;
-                    if (lane == leader)
-                        qb = atomicAdd(&S.qn, (uint32_t)__popc(bal));
-                    qb = __shfl_sync(0xffffffffu, qb, leader);
-                    if (pass)
-                        S.queue[qb + __popc(bal & lt)] = (uint16_t)entry;
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+                    if (lane >= off)
+                        incl += y;
                 }
+                uint32_t qb = 0;
+                if (lane == 31 && incl)
+                    qb = atomicAdd(&S.qn, incl);
+                qb = __shfl_sync(0xffffffffu, qb, 31) + incl - np;
+                for (uint32_t m = zmask; m; m &= m - 1)
+                    S.queue[qb++] = (uint16_t)(ebase + (uint32_t)(__ffs(m) - 1));
             }
             __syncthreads();
             // ---- alpha, one queued pair per thread
@@ -440,7 +437,7 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
                 const uint32_t j = q >> 9, n = q & 511u;
                 const GaussRec& R = S.rec[j];
                 const RInv M = rinv_of(R);
-                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
+                const float vsf = S.vs[j];
                 const int32_t x = o[0] + (int32_t)(n >> 6), yy = o[1] + (int32_t)((n >> 3) & 7), zz = o[2] + (int32_t)(n & 7);
                 float cx0, cx1, cy0, cy1, cz0, cz1;
                 axis_corners(vsf, R.q0.x, x, cx0, cx1);
@@ -663,10 +660,15 @@ __global__ void __launch_bounds__(LP_THREADS) k_leaf_backward(LeafPassParams P, 
                 if (e < T)
                 {
                     j = 0;
+                    uint32_t sj = 0;
 #pragma unroll
                     for (int q = 1; q < LQ_CHUNK; q++)
-                        j += e >= start[q] ? 1 : 0;
-                    const uint32_t local = e - start[j];
+                    {
+                        const bool ge = e >= start[q];
+                        j += ge ? 1 : 0;
+                        sj = ge ? start[q] : sj;
+                    }
+                    const uint32_t local = e - sj;
                     const uint32_t rest = (local * S.bdiv_z[j]) >> 16;
                     const uint32_t dz = local - rest * S.bnz[j];
                     const uint32_t dx = (rest * S.bdiv_y[j]) >> 16;
