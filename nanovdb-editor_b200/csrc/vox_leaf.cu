@@ -169,12 +169,15 @@ __global__ void k_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags)
         flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1ull : 0ull;
 }
 
-__global__ void k_leaf_compact(const uint32_t* keys, int64_t Q, const uint64_t* flags, const uint64_t* pos,
-                               uint32_t* cand_key, uint32_t* cand_start)
+// candidate leaves from the run heads; each sorted pair's Gaussian id
+__global__ void k_leaf_compact(const uint32_t* keys, const uint32_t* vals, const uint32_t* emit_gid, int64_t Q,
+                               const uint64_t* flags, const uint64_t* pos, uint32_t* cand_key, uint32_t* cand_start,
+                               uint32_t* pair_gid)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Q)
         return;
+    pair_gid[i] = emit_gid[vals[i]];
     if (flags[i])
     {
         cand_key[pos[i]] = keys[i];
@@ -246,11 +249,11 @@ __device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S
 //   sum    each thread folds its two voxels' table entries in ascending
 //          Gaussian id, so every float sum has the order of a serial loop.
 constexpr int LQ_CHUNK = 8;
+constexpr int LQ_STAGE_T0 = LP_THREADS - 32; // lanes 0..LQ_CHUNK-1 of the last warp stage the next chunk
 
 struct LeafQSmem
 {
-    GaussRec rec[LQ_CHUNK];
-    uint32_t gid[LQ_CHUNK];
+    GaussRec rec[2][LQ_CHUNK]; // double-buffered records: the next chunk's land while this one is walked
     uint8_t flag[LQ_CHUNK];
     int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK]; // box origin, leaf-relative
     uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK];               // box extents in y and z
@@ -264,274 +267,367 @@ struct LeafQSmem
     uint64_t mask[8];
     uint64_t wf0[LQ_CHUNK], wbase[LQ_CHUNK]; // reference windows: fragment offset in its batch, windows before
     uint64_t wmin;
-    uint32_t qn, pairs, cand;
+    int32_t nxt_o[3];                        // the next chunk: leaf origin and sorted pair range
+    uint32_t nxt_q0, nxt_p1;
+    uint32_t qn, pairs, cand, cand_next;
 };
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// the record of sorted leaf pair q into shared memory (asynchronous); returns its Gaussian id
+__device__ __forceinline__ uint32_t leaf_stage_issue(const LeafPassParams& P, GaussRec* dst, uint32_t q)
+{
+    const uint32_t g = P.pair_gid[q];
+    const float4* src = reinterpret_cast<const float4*>(&P.recs[g]);
+#pragma unroll
+    for (int w = 0; w < 8; w++)
+        cp_async16(reinterpret_cast<float4*>(dst) + w, src + w);
+    return g;
+}
+
+// once the record landed: the part of the Gaussian's bbox inside the leaf at o
+template <bool CHECK, bool WINDOW>
+__device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafQSmem& S, const GaussRec& R, int j,
+                                               uint32_t q, uint32_t g, const int32_t o[3])
+{
+    const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
+    const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
+    const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
+    const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
+    const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
+    S.bx0[j] = x0;
+    S.by0[j] = y0;
+    S.bz0[j] = z0;
+    S.bny[j] = ny;
+    S.bnz[j] = nz;
+    S.bdiv_y[j] = (65536u + ny - 1u) / ny;
+    S.bcol[j] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
+    S.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
+    S.flag[j] = CHECK ? P.emit_flag[P.vals[q]] : 0;
+    if (WINDOW)
+    {
+        const int64_t batch = (int64_t)g / REF_PRIM_BATCH;
+        S.wf0[j] = P.frag_off[g] - P.frag_off[batch * REF_PRIM_BATCH];
+        S.wbase[j] = P.win_before[batch];
+    }
+}
+
+// Chunks are software-pipelined: while chunk k is tested, the last warp's
+// first lanes copy chunk k + 1's records (cp.async, the other buffer); they
+// wait for their own copies and place chunk k + 1's boxes during chunk k's sum.
+// The next candidate leaf is claimed one leaf ahead, so a leaf's first chunk
+// is staged like any other.  Three barriers per chunk.
 template <bool CHECK, bool WINDOW>
 __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, uint32_t* counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LeafQSmem& S = *reinterpret_cast<LeafQSmem*>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int js = t - LQ_STAGE_T0; // staging slot (0 .. LQ_CHUNK - 1 on the stagers)
+    const bool stager = js >= 0 && js < LQ_CHUNK;
+    if (t == 0)
+    {
+        S.cand = atomicAdd(counter, 1u);
+        S.cand_next = atomicAdd(counter, 1u);
+        S.pairs = 0;
+        S.wmin = ~0ull;
+        S.qn = 0;
+    }
+    if (t < 8)
+        S.mask[t] = 0;
+    S.pbits[t] = 0;
+    S.pbits[t + 256] = 0;
+    __syncthreads();
+    int64_t c = S.cand;
+    if (c >= P.NCL)
+        return;
+    int64_t cn = S.cand_next;
+    int32_t o[3];
+    cand_origin(P, P.cand_key[c], o);
+    uint32_t q0 = P.cand_start[c], p1 = P.cand_start[c + 1];
+    int buf = 0;
+    if (stager && js < (int)min((uint32_t)LQ_CHUNK, p1 - q0))
+    {
+        const uint32_t g = leaf_stage_issue(P, &S.rec[0][js], q0 + (uint32_t)js);
+        cp_async_wait_all();
+        leaf_stage_box<CHECK, WINDOW>(P, S, S.rec[0][js], js, q0 + (uint32_t)js, g, o);
+    }
+    __syncthreads();
+    uint32_t rgba[2] = { 0u, 0u }, pc[2] = { 0u, 0u };
+    float ds[2] = { 0.f, 0.f }, cr[2] = { 0.f, 0.f }, cgr[2] = { 0.f, 0.f }, cb[2] = { 0.f, 0.f };
     while (true)
     {
-        if (t == 0)
+        const uint32_t cnt = min((uint32_t)LQ_CHUNK, p1 - q0);
+        const bool leaf_end = q0 + LQ_CHUNK >= p1;
+        const int64_t nc = leaf_end ? cn : c;
+        const bool has_next = nc < P.NCL;
+        // ---- stagers: the next chunk's pair range, its record copies
+        uint32_t nq0 = 0, np1 = 0, ncnt = 0, ng = 0;
+        if (stager && has_next)
         {
-            S.cand = atomicAdd(counter, 1u);
-            S.pairs = 0;
-            S.wmin = ~0ull;
+            nq0 = leaf_end ? P.cand_start[nc] : q0 + LQ_CHUNK;
+            np1 = leaf_end ? P.cand_start[nc + 1] : p1;
+            ncnt = min((uint32_t)LQ_CHUNK, np1 - nq0);
+            if (js < (int)ncnt)
+                ng = leaf_stage_issue(P, &S.rec[buf ^ 1][js], nq0 + (uint32_t)js);
         }
-        if (t < 8)
-            S.mask[t] = 0;
-        __syncthreads();
-        const int64_t c = S.cand;
-        if (c >= P.NCL)
-            break;
-        int32_t o[3];
-        cand_origin(P, P.cand_key[c], o);
-        uint32_t rgba[2] = { 0u, 0u }, pc[2] = { 0u, 0u };
-        float ds[2] = { 0.f, 0.f }, cr[2] = { 0.f, 0.f }, cgr[2] = { 0.f, 0.f }, cb[2] = { 0.f, 0.f };
-        const uint32_t p0 = P.cand_start[c], p1 = P.cand_start[c + 1];
-        for (uint32_t q0 = p0; q0 < p1; q0 += LQ_CHUNK)
+        const GaussRec* rec = S.rec[buf];
+        uint32_t start[LQ_CHUNK + 1];
+        start[0] = 0;
+#pragma unroll
+        for (int j = 0; j < LQ_CHUNK; j++)
+            start[j + 1] = start[j] + (j < (int)cnt ? S.bcol[j] : 0u);
+        const uint32_t T = start[LQ_CHUNK];
+        // ---- test, one box column per thread.  Bit-identical to
+        // voxel_local_aabb + aabb_hits_unit_sphere per voxel: the z corner c1
+        // of voxel z is c0 of voxel z + 1 (integer-valued floats), and "lo > 0:
+        // subtract lo^2, else hi < 0: subtract hi^2" selects the pre-scale sum
+        // with the same sign (inv_ls, inv_s > 0; an underflow to zero
+        // subtracts zero).
+        for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
         {
-            const uint32_t cnt = min((uint32_t)LQ_CHUNK, p1 - q0);
-            if (t < (int)cnt * 8)
+            const uint32_t e = b0 + (uint32_t)t;
+            uint32_t zmask = 0, ebase = 0;
+            if (e < T)
             {
-                const uint32_t j = (uint32_t)t >> 3, w = (uint32_t)t & 7u;
-                const uint32_t e = P.vals[q0 + j];
-                const uint32_t g = P.emit_gid[e];
-                reinterpret_cast<float4*>(&S.rec[j])[w] = reinterpret_cast<const float4*>(&P.recs[g])[w];
-                if (w == 0)
+                int j = 0;
+                uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
+#pragma unroll
+                for (int q = 1; q < LQ_CHUNK; q++)
                 {
-                    S.gid[j] = g;
-                    S.flag[j] = P.emit_flag ? P.emit_flag[e] : 0;
-                    if (WINDOW)
-                    {
-                        const int64_t batch = (int64_t)g / REF_PRIM_BATCH;
-                        S.wf0[j] = P.frag_off[g] - P.frag_off[batch * REF_PRIM_BATCH];
-                        S.wbase[j] = P.win_before[batch];
-                    }
+                    const bool ge = e >= start[q];
+                    j += ge ? 1 : 0;
+                    sj = ge ? start[q] : sj;
                 }
-            }
-            S.pbits[t] = 0;
-            S.pbits[t + 256] = 0;
-            if (t == 0)
-                S.qn = 0;
-            __syncthreads();
-            // ---- box
-            if (t < (int)cnt)
-            {
-                const GaussRec& R = S.rec[t];
-                const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
-                const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
-                const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
-                const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
-                const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
-                S.bx0[t] = x0;
-                S.by0[t] = y0;
-                S.bz0[t] = z0;
-                S.bny[t] = ny;
-                S.bnz[t] = nz;
-                S.bdiv_y[t] = (65536u + ny - 1u) / ny;
-                S.bcol[t] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
-                S.vs[t] = rec_vs(R, P.voxel_size, P.cloud_vs);
-            }
-            __syncthreads();
-            uint32_t start[LQ_CHUNK + 1];
-            start[0] = 0;
+                const uint32_t local = e - sj;
+                const uint32_t dx = (local * S.bdiv_y[j]) >> 16;
+                const uint32_t dy = local - dx * S.bny[j];
+                const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz0 = S.bz0[j];
+                const GaussRec& R = rec[j];
+                const RInv M = rinv_of(R);
+                const float vsf = S.vs[j], il = R.q0.w, pz = R.q0.z;
+                const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+                float cx0, cx1, cy0, cy1;
+                axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
+                axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
+                float slo[3], shi[3], pa[3];
+                float v = (float)(o[2] + rz0);
+                float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
 #pragma unroll
-            for (int j = 0; j < LQ_CHUNK; j++)
-                start[j + 1] = start[j] + (j < (int)cnt ? S.bcol[j] : 0u);
-            const uint32_t T = start[LQ_CHUNK];
-            // ---- test, one box column per thread.  Bit-identical to
-            // voxel_local_aabb + aabb_hits_unit_sphere per voxel: the z corner
-            // c1 of voxel z is c0 of voxel z + 1 (integer-valued floats), and
-            // "lo > 0: subtract lo^2, else hi < 0: subtract hi^2" selects the
-            // pre-scale sum with the same sign (inv_ls, inv_s > 0; an underflow
-            // to zero subtracts zero).
-            for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
-            {
-                const uint32_t e = b0 + (uint32_t)t;
-                uint32_t zmask = 0, ebase = 0;
-                if (e < T)
+                for (int r = 0; r < 3; r++)
                 {
-                    int j = 0;
-                    uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
-#pragma unroll
-                    for (int q = 1; q < LQ_CHUNK; q++)
-                    {
-                        const bool ge = e >= start[q];
-                        j += ge ? 1 : 0;
-                        sj = ge ? start[q] : sj;
-                    }
-                    const uint32_t local = e - sj;
-                    const uint32_t dx = (local * S.bdiv_y[j]) >> 16;
-                    const uint32_t dy = local - dx * S.bny[j];
-                    const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz0 = S.bz0[j];
-                    const GaussRec& R = S.rec[j];
-                    const RInv M = rinv_of(R);
-                    const float vsf = S.vs[j], il = R.q0.w, pz = R.q0.z;
-                    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
-                    float cx0, cx1, cy0, cy1;
-                    axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
-                    axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
-                    float slo[3], shi[3], pa[3];
-                    float v = (float)(o[2] + rz0);
-                    float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                    float xn, xx, yn, yx;
+                    minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
+                    minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
+                    slo[r] = VOX_FADD(xn, yn);
+                    shi[r] = VOX_FADD(xx, yx);
+                    pa[r] = VOX_FMUL(cz, M.m[r][2]);
+                }
+                const uint32_t nz = S.bnz[j];
+                for (uint32_t k = 0; k < nz; k++)
+                {
+                    v = VOX_FADD(v, 1.f);
+                    cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                    float d2 = 1.f;
 #pragma unroll
                     for (int r = 0; r < 3; r++)
                     {
-                        float xn, xx, yn, yx;
-                        minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
-                        minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
-                        slo[r] = VOX_FADD(xn, yn);
-                        shi[r] = VOX_FADD(xx, yx);
-                        pa[r] = VOX_FMUL(cz, M.m[r][2]);
+                        const float pb = VOX_FMUL(cz, M.m[r][2]);
+                        const float zn = pa[r] < pb ? pa[r] : pb, zx = pa[r] < pb ? pb : pa[r];
+                        pa[r] = pb;
+                        const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
+                        const float x = 0.f < xl ? xl : (0.f > xh ? xh : 0.f);
+                        const float sv = VOX_FMUL(VOX_FMUL(x, il), is[r]);
+                        d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
                     }
-                    const uint32_t nz = S.bnz[j];
-                    for (uint32_t k = 0; k < nz; k++)
-                    {
-                        v = VOX_FADD(v, 1.f);
-                        cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-                        float d2 = 1.f;
-#pragma unroll
-                        for (int r = 0; r < 3; r++)
-                        {
-                            const float pb = VOX_FMUL(cz, M.m[r][2]);
-                            const float zn = pa[r] < pb ? pa[r] : pb, zx = pa[r] < pb ? pb : pa[r];
-                            pa[r] = pb;
-                            const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
-                            const float x = 0.f < xl ? xl : (0.f > xh ? xh : 0.f);
-                            const float sv = VOX_FMUL(VOX_FMUL(x, il), is[r]);
-                            d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
-                        }
-                        zmask |= (d2 > 0.f ? 1u : 0u) << k;
-                    }
-                    ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
-                    if (CHECK && zmask && S.flag[j])
-                        atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
+                    zmask |= (d2 > 0.f ? 1u : 0u) << k;
                 }
-                // queue slots: warp inclusive scan of the pass counts, one shared atomic per warp
-                const uint32_t np = (uint32_t)__popc(zmask);
-                uint32_t incl = np;
-#pragma unroll
-                for (int off = 1; off < 32; off <<= 1)
-                {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
-                    if (lane >= off)
-                        incl += y;
-                }
-                uint32_t qb = 0;
-                if (lane == 31 && incl)
-                    qb = atomicAdd(&S.qn, incl);
-                qb = __shfl_sync(0xffffffffu, qb, 31) + incl - np;
-                for (uint32_t m = zmask; m; m &= m - 1)
-                    S.queue[qb++] = (uint16_t)(ebase + (uint32_t)(__ffs(m) - 1));
+                ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
+                if (CHECK && zmask && S.flag[j])
+                    atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
             }
-            __syncthreads();
-            // ---- alpha, one queued pair per thread
-            const uint32_t qn = S.qn;
-            for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
+            // queue slots: warp inclusive scan of the pass counts, one shared atomic per warp
+            const uint32_t np = (uint32_t)__popc(zmask);
+            uint32_t incl = np;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1)
             {
-                const uint32_t q = S.queue[e];
-                const uint32_t j = q >> 9, n = q & 511u;
-                const GaussRec& R = S.rec[j];
-                const RInv M = rinv_of(R);
-                const float vsf = S.vs[j];
-                const int32_t x = o[0] + (int32_t)(n >> 6), yy = o[1] + (int32_t)((n >> 3) & 7), zz = o[2] + (int32_t)(n & 7);
-                float cx0, cx1, cy0, cy1, cz0, cz1;
-                axis_corners(vsf, R.q0.x, x, cx0, cx1);
-                axis_corners(vsf, R.q0.y, yy, cy0, cy1);
-                axis_corners(vsf, R.q0.z, zz, cz0, cz1);
-                const float a8 = pair_alpha(R, aabb_from_corners(R, M, cx0, cx1, cy0, cy1, cz0, cz1));
-                float a;
-                if (P.smooth)
-                {
-                    SmoothTerms st;
-                    a = smooth_kernel(R, M, vsf, x, yy, zz, st);
-                }
-                else
-                {
-                    // float channels: corner offsets rounded once from double
-                    float sx0, sx1, sy0, sy1, sz0, sz1;
-                    axis_corners_stable(vsf, R.q0.x, x, sx0, sx1);
-                    axis_corners_stable(vsf, R.q0.y, yy, sy0, sy1);
-                    axis_corners_stable(vsf, R.q0.z, zz, sz0, sz1);
-                    const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
-                    a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
-                }
-                S.res_a[j][n] = a;
-                S.res_rgba[j][n] = pack_rgba8(R, a8);
-                atomicOr(&S.pbits[n], 1u << j);
-                if (WINDOW)
-                {
-                    // the reference's window of this fragment: x-major index in the bbox
-                    // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
-                    const uint64_t r = (uint64_t)(x - R.q4.x) * (uint64_t)R.q5.y * (uint64_t)R.q5.z +
-                                       (uint64_t)(yy - R.q4.y) * (uint64_t)R.q5.z + (uint64_t)(zz - R.q4.z);
-                    atomicMin((unsigned long long*)&S.wmin,
-                              (unsigned long long)(S.wbase[j] + (S.wf0[j] + r) / REF_WINDOW));
-                }
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off)
+                    incl += y;
             }
-            __syncthreads();
-            // ---- sum in ascending Gaussian id
-#pragma unroll
-            for (int h = 0; h < 2; h++)
-            {
-                const uint32_t n = (uint32_t)(t + 256 * h);
-                for (uint32_t m = S.pbits[n]; m; m &= m - 1)
-                {
-                    const int j = __ffs(m) - 1;
-                    const float a = S.res_a[j][n];
-                    const uint32_t px = S.res_rgba[j][n];
-                    const GaussRec& R = S.rec[j];
-                    rgba[h] = px > rgba[h] ? px : rgba[h];
-                    ds[h] = VOX_FADD(ds[h], a);
-                    cr[h] = VOX_FADD(cr[h], VOX_FMUL(a, R.q7.x));
-                    cgr[h] = VOX_FADD(cgr[h], VOX_FMUL(a, R.q7.y));
-                    cb[h] = VOX_FADD(cb[h], VOX_FMUL(a, R.q7.z));
-                    pc[h]++;
-                }
-            }
-            __syncthreads();
+            uint32_t qb = 0;
+            if (lane == 31 && incl)
+                qb = atomicAdd(&S.qn, incl);
+            qb = __shfl_sync(0xffffffffu, qb, 31) + incl - np;
+            for (uint32_t m = zmask; m; m &= m - 1)
+                S.queue[qb++] = (uint16_t)(ebase + (uint32_t)(__ffs(m) - 1));
         }
-        // value mask from ballots: voxel A (leaf_n = t) of warp w is bit 32 (w & 1) + lane of word w >> 1
-        const uint32_t ba = __ballot_sync(0xffffffffu, pc[0] > 0), bb = __ballot_sync(0xffffffffu, pc[1] > 0);
-        uint32_t wp = pc[0] + pc[1];
-#pragma unroll
-        for (int off = 16; off; off >>= 1)
-            wp += __shfl_xor_sync(0xffffffffu, wp, off);
-        if (lane == 0)
+        __syncthreads();
+        // ---- alpha, one queued pair per thread
+        const uint32_t qn = S.qn;
+        for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
         {
-            atomicOr((unsigned long long*)&S.mask[warp >> 1], (unsigned long long)ba << (32 * (warp & 1)));
-            atomicOr((unsigned long long*)&S.mask[4 + (warp >> 1)], (unsigned long long)bb << (32 * (warp & 1)));
-            atomicAdd(&S.pairs, wp);
+            const uint32_t q = S.queue[e];
+            const uint32_t j = q >> 9, n = q & 511u;
+            const GaussRec& R = rec[j];
+            const RInv M = rinv_of(R);
+            const float vsf = S.vs[j];
+            const int32_t x = o[0] + (int32_t)(n >> 6), yy = o[1] + (int32_t)((n >> 3) & 7), zz = o[2] + (int32_t)(n & 7);
+            float cx0, cx1, cy0, cy1, cz0, cz1;
+            axis_corners(vsf, R.q0.x, x, cx0, cx1);
+            axis_corners(vsf, R.q0.y, yy, cy0, cy1);
+            axis_corners(vsf, R.q0.z, zz, cz0, cz1);
+            const float a8 = pair_alpha(R, aabb_from_corners(R, M, cx0, cx1, cy0, cy1, cz0, cz1));
+            float a;
+            if (P.smooth)
+            {
+                SmoothTerms st;
+                a = smooth_kernel(R, M, vsf, x, yy, zz, st);
+            }
+            else
+            {
+                // float channels: corner offsets rounded once from double
+                float sx0, sx1, sy0, sy1, sz0, sz1;
+                axis_corners_stable(vsf, R.q0.x, x, sx0, sx1);
+                axis_corners_stable(vsf, R.q0.y, yy, sy0, sy1);
+                axis_corners_stable(vsf, R.q0.z, zz, sz0, sz1);
+                const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
+                a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
+            }
+            S.res_a[j][n] = a;
+            S.res_rgba[j][n] = pack_rgba8(R, a8);
+            atomicOr(&S.pbits[n], 1u << j);
+            if (WINDOW)
+            {
+                // the reference's window of this fragment: x-major index in the bbox
+                // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
+                const uint64_t r = (uint64_t)(x - R.q4.x) * (uint64_t)R.q5.y * (uint64_t)R.q5.z +
+                                   (uint64_t)(yy - R.q4.y) * (uint64_t)R.q5.z + (uint64_t)(zz - R.q4.z);
+                atomicMin((unsigned long long*)&S.wmin, (unsigned long long)(S.wbase[j] + (S.wf0[j] + r) / REF_WINDOW));
+            }
         }
+        __syncthreads();
+        // ---- sum in ascending Gaussian id; each thread clears its voxels' bits
 #pragma unroll
         for (int h = 0; h < 2; h++)
         {
-            if (!pc[h])
-                continue;
-            const uint64_t slot = (uint64_t)c * 512u + (uint32_t)(t + 256 * h);
-            P.s_rgba[slot] = rgba[h];
-            P.s_dens[slot] = ds[h];
-            float col[3] = { cr[h], cgr[h], cb[h] };
-            if (!P.smooth)
-                for (int k = 0; k < 3; k++)
-                    col[k] = ds[h] > 0.f ? VOX_FDIV(col[k], ds[h]) : 0.f;
-            P.s_col[3 * slot + 0] = col[0];
-            P.s_col[3 * slot + 1] = col[1];
-            P.s_col[3 * slot + 2] = col[2];
-            P.s_pairs[slot] = pc[h];
+            const uint32_t n = (uint32_t)(t + 256 * h);
+            const uint32_t bits = S.pbits[n];
+            for (uint32_t m = bits; m; m &= m - 1)
+            {
+                const int j = __ffs(m) - 1;
+                const float a = S.res_a[j][n];
+                const uint32_t px = S.res_rgba[j][n];
+                const GaussRec& R = rec[j];
+                rgba[h] = px > rgba[h] ? px : rgba[h];
+                ds[h] = VOX_FADD(ds[h], a);
+                cr[h] = VOX_FADD(cr[h], VOX_FMUL(a, R.q7.x));
+                cgr[h] = VOX_FADD(cgr[h], VOX_FMUL(a, R.q7.y));
+                cb[h] = VOX_FADD(cb[h], VOX_FMUL(a, R.q7.z));
+                pc[h]++;
+            }
+            if (bits)
+                S.pbits[n] = 0;
+        }
+        if (t == 0)
+            S.qn = 0;
+        if (leaf_end)
+        {
+            // value mask from ballots: voxel A (leaf_n = t) of warp w is bit 32 (w & 1) + lane of word w >> 1
+            const uint32_t ba = __ballot_sync(0xffffffffu, pc[0] > 0), bb = __ballot_sync(0xffffffffu, pc[1] > 0);
+            uint32_t wp = pc[0] + pc[1];
+#pragma unroll
+            for (int off = 16; off; off >>= 1)
+                wp += __shfl_xor_sync(0xffffffffu, wp, off);
+            if (lane == 0)
+            {
+                atomicOr((unsigned long long*)&S.mask[warp >> 1], (unsigned long long)ba << (32 * (warp & 1)));
+                atomicOr((unsigned long long*)&S.mask[4 + (warp >> 1)], (unsigned long long)bb << (32 * (warp & 1)));
+                atomicAdd(&S.pairs, wp);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+            {
+                if (pc[h])
+                {
+                    const uint64_t slot = (uint64_t)c * 512u + (uint32_t)(t + 256 * h);
+                    P.s_rgba[slot] = rgba[h];
+                    P.s_dens[slot] = ds[h];
+                    float col[3] = { cr[h], cgr[h], cb[h] };
+                    if (!P.smooth)
+                        for (int k = 0; k < 3; k++)
+                            col[k] = ds[h] > 0.f ? VOX_FDIV(col[k], ds[h]) : 0.f;
+                    P.s_col[3 * slot + 0] = col[0];
+                    P.s_col[3 * slot + 1] = col[1];
+                    P.s_col[3 * slot + 2] = col[2];
+                    P.s_pairs[slot] = pc[h];
+                }
+                rgba[h] = 0u;
+                pc[h] = 0u;
+                ds[h] = cr[h] = cgr[h] = cb[h] = 0.f;
+            }
+        }
+        // ---- stagers: the next chunk's boxes (their own copies have landed)
+        if (stager && has_next)
+        {
+            int32_t no[3] = { o[0], o[1], o[2] };
+            if (leaf_end)
+                cand_origin(P, P.cand_key[nc], no);
+            if (js < (int)ncnt)
+            {
+                cp_async_wait_all();
+                leaf_stage_box<CHECK, WINDOW>(P, S, S.rec[buf ^ 1][js], js, nq0 + (uint32_t)js, ng, no);
+            }
+            if (js == 0)
+            {
+                S.nxt_o[0] = no[0];
+                S.nxt_o[1] = no[1];
+                S.nxt_o[2] = no[2];
+                S.nxt_q0 = nq0;
+                S.nxt_p1 = np1;
+                if (leaf_end)
+                    S.cand_next = atomicAdd(counter, 1u);
+            }
         }
         __syncthreads();
-        if (t < 8)
-            P.cand_mask[8 * (uint64_t)c + t] = S.mask[t];
-        if (t == 0 && S.pairs)
-            atomicAdd((unsigned long long*)P.total_pairs, (unsigned long long)S.pairs);
-        if (WINDOW && t == 0)
-            P.cand_wkey[c] = S.wmin;
-        __syncthreads();
+        if (leaf_end)
+        {
+            if (t < 8)
+            {
+                P.cand_mask[8 * (uint64_t)c + t] = S.mask[t];
+                S.mask[t] = 0;
+            }
+            if (t == 0)
+            {
+                if (S.pairs)
+                    atomicAdd((unsigned long long*)P.total_pairs, (unsigned long long)S.pairs);
+                S.pairs = 0;
+                if (WINDOW)
+                    P.cand_wkey[c] = S.wmin;
+                S.wmin = ~0ull;
+            }
+        }
+        if (!has_next)
+            break;
+        if (leaf_end)
+            cn = S.cand_next;
+        c = nc;
+        q0 = S.nxt_q0;
+        p1 = S.nxt_p1;
+        o[0] = S.nxt_o[0];
+        o[1] = S.nxt_o[1];
+        o[2] = S.nxt_o[2];
+        buf ^= 1;
     }
 }
 
@@ -910,12 +1006,13 @@ void launch_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags, cudaStr
     { k_leaf_heads<<<(unsigned)((Q + 255) / 256), 256, 0, s>>>(keys, Q, flags); count_launch(); }
 }
 
-void launch_leaf_compact(const uint32_t* keys, int64_t Q, const uint64_t* flags, const uint64_t* pos,
-                         uint32_t* cand_key, uint32_t* cand_start, cudaStream_t s)
+void launch_leaf_compact(const uint32_t* keys, const uint32_t* vals, const uint32_t* emit_gid, int64_t Q,
+                         const uint64_t* flags, const uint64_t* pos, uint32_t* cand_key, uint32_t* cand_start,
+                         uint32_t* pair_gid, cudaStream_t s)
 {
     if (Q <= 0)
         return;
-    { k_leaf_compact<<<(unsigned)((Q + 255) / 256), 256, 0, s>>>(keys, Q, flags, pos, cand_key, cand_start); count_launch(); }
+    { k_leaf_compact<<<(unsigned)((Q + 255) / 256), 256, 0, s>>>(keys, vals, emit_gid, Q, flags, pos, cand_key, cand_start, pair_gid); count_launch(); }
 }
 
 static unsigned walk_grid(int64_t NCL, int num_sms)
