@@ -286,36 +286,6 @@ __device__ __forceinline__ void minmax_prod(float c0, float c1, float r, float& 
     mx = p0 < p1 ? p1 : p0;
 }
 
-// Corner offsets for the float density / colour channels: v * vs - mu in
-// double, rounded once, so far from the origin the offsets keep the
-// precision the reference's fl(fl(v * vs) - mu) loses.  (The RGBA8 channel and
-// the fragment test keep the reference's float formula.)
-__device__ __forceinline__ void axis_corners_stable(float vs, float pos, int32_t i, float& c0, float& c1)
-{
-    c0 = (float)VOX_DSUB(VOX_DMUL((double)i, (double)vs), (double)pos);
-    c1 = (float)VOX_DSUB(VOX_DMUL((double)i + 1.0, (double)vs), (double)pos);
-}
-
-__device__ __forceinline__ Aabb aabb_from_corners(const GaussRec& R, const RInv& M, float cx0, float cx1, float cy0,
-                                                  float cy1, float cz0, float cz1)
-{
-    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
-    Aabb b;
-#pragma unroll
-    for (int row = 0; row < 3; row++)
-    {
-        float xn, xx, yn, yx, zn, zx;
-        minmax_prod(cx0, cx1, M.m[row][0], xn, xx);
-        minmax_prod(cy0, cy1, M.m[row][1], yn, yx);
-        minmax_prod(cz0, cz1, M.m[row][2], zn, zx);
-        float lo = VOX_FADD(VOX_FADD(xn, yn), zn);
-        float hi = VOX_FADD(VOX_FADD(xx, yx), zx);
-        b.lo[row] = VOX_FMUL(VOX_FMUL(lo, R.q0.w), inv_s[row]);
-        b.hi[row] = VOX_FMUL(VOX_FMUL(hi, R.q0.w), inv_s[row]);
-    }
-    return b;
-}
-
 __device__ __forceinline__ Aabb voxel_local_aabb(const GaussRec& R, const RInv& M, float vs, int32_t i, int32_t j,
                                                  int32_t k)
 {
@@ -382,6 +352,34 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
     }
     float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
     float a = VOX_FMUL(R.q6.x, vox_expf_cr(-VOX_FMUL(R.q6.y, d)));
+    a = a > 0.f ? a : 0.f;
+    a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), R.q6.z));
+    if (R.q7.w != 0.f)
+        a = 0.f;
+    return a;
+}
+
+// Alpha of the float density / colour channels from the stable local AABB
+// (corner offsets fma(v, vs, -mu), sign-picked corners summed with fma): the
+// lattice points lo + w (hi - lo), float exp / pow.  The oracle's
+// frag_alpha_f evaluates the same operations in the same order.
+__device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
+{
+    float m[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const float dd = VOX_FSUB(b.hi[a], b.lo[a]);
+        const float p1 = VOX_FFMA(dd, 0x1.555556p-2f, b.lo[a]), p2 = VOX_FFMA(dd, 0x1.555556p-1f, b.lo[a]);
+        float best = VOX_FMUL(b.lo[a], b.lo[a]);
+        const float s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2), s3 = VOX_FMUL(b.hi[a], b.hi[a]);
+        best = s1 < best ? s1 : best;
+        best = s2 < best ? s2 : best;
+        best = s3 < best ? s3 : best;
+        m[a] = best;
+    }
+    const float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
+    float a = VOX_FMUL(R.q6.x, vox_expf(-VOX_FMUL(R.q6.y, d)));
     a = a > 0.f ? a : 0.f;
     a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), R.q6.z));
     if (R.q7.w != 0.f)

@@ -260,6 +260,11 @@ struct LeafQSmem
     uint32_t bdiv_y[LQ_CHUNK];                           // 65536 / ny, rounded up (exact division below 64)
     uint32_t bcol[LQ_CHUNK];                             // box columns, nx * ny (0: empty box)
     float vs[LQ_CHUNK];
+    // x / y shares of every column with a passing voxel, per row: the
+    // reference test's (sums of the per-axis min / max corner products) and the
+    // float channels' stable form (fma over the sign-picked corners)
+    float cr_lo[3][LQ_CHUNK * 64], cr_hi[3][LQ_CHUNK * 64];
+    float cf_lo[3][LQ_CHUNK * 64], cf_hi[3][LQ_CHUNK * 64];
     uint16_t queue[LQ_CHUNK * 512];
     float res_a[LQ_CHUNK][512];
     uint32_t res_rgba[LQ_CHUNK][512];
@@ -451,6 +456,24 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
                     }
                     zmask |= (d2 > 0.f ? 1u : 0u) << k;
                 }
+                if (zmask)
+                {
+                    const uint32_t ci = (uint32_t)j * 64u + (uint32_t)(rx * 8 + ry);
+                    const float vx = (float)(o[0] + rx), vy = (float)(o[1] + ry);
+                    const float sx0 = VOX_FFMA(vx, vsf, -R.q0.x), sx1 = VOX_FFMA(VOX_FADD(vx, 1.f), vsf, -R.q0.x);
+                    const float sy0 = VOX_FFMA(vy, vsf, -R.q0.y), sy1 = VOX_FFMA(VOX_FADD(vy, 1.f), vsf, -R.q0.y);
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        const float mx = M.m[r][0], my = M.m[r][1];
+                        const float clx = mx >= 0.f ? sx0 : sx1, chx = mx >= 0.f ? sx1 : sx0;
+                        const float cly = my >= 0.f ? sy0 : sy1, chy = my >= 0.f ? sy1 : sy0;
+                        S.cr_lo[r][ci] = slo[r];
+                        S.cr_hi[r][ci] = shi[r];
+                        S.cf_lo[r][ci] = VOX_FFMA(clx, mx, VOX_FMUL(cly, my));
+                        S.cf_hi[r][ci] = VOX_FFMA(chx, mx, VOX_FMUL(chy, my));
+                    }
+                }
                 ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
                 if (CHECK && zmask && S.flag[j])
                     atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
@@ -478,31 +501,46 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
         for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
         {
             const uint32_t q = S.queue[e];
-            const uint32_t j = q >> 9, n = q & 511u;
+            const uint32_t j = q >> 9, n = q & 511u, ci = (j << 6) | (n >> 3);
             const GaussRec& R = rec[j];
-            const RInv M = rinv_of(R);
-            const float vsf = S.vs[j];
+            const float vsf = S.vs[j], il = R.q0.w, pz = R.q0.z;
+            const float mz[3] = { R.q1.z, R.q2.y, R.q3.x }; // rinv[r][2]
+            const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
             const int32_t x = o[0] + (int32_t)(n >> 6), yy = o[1] + (int32_t)((n >> 3) & 7), zz = o[2] + (int32_t)(n & 7);
-            float cx0, cx1, cy0, cy1, cz0, cz1;
-            axis_corners(vsf, R.q0.x, x, cx0, cx1);
-            axis_corners(vsf, R.q0.y, yy, cy0, cy1);
-            axis_corners(vsf, R.q0.z, zz, cz0, cz1);
-            const float a8 = pair_alpha(R, aabb_from_corners(R, M, cx0, cx1, cy0, cy1, cz0, cz1));
+            const float v0 = (float)zz, v1 = VOX_FADD(v0, 1.f);
+            // RGBA8: the reference's local AABB from the column's staged x / y shares
+            // (bit-identical to voxel_local_aabb)
+            const float cz0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz), cz1 = VOX_FSUB(VOX_FMUL(v1, vsf), pz);
+            Aabb b;
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+            {
+                float zn, zx;
+                minmax_prod(cz0, cz1, mz[r], zn, zx);
+                b.lo[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(S.cr_lo[r][ci], zn), il), is[r]);
+                b.hi[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(S.cr_hi[r][ci], zx), il), is[r]);
+            }
+            const float a8 = pair_alpha(R, b);
             float a;
             if (P.smooth)
             {
                 SmoothTerms st;
-                a = smooth_kernel(R, M, vsf, x, yy, zz, st);
+                a = smooth_kernel(R, rinv_of(R), vsf, x, yy, zz, st);
             }
             else
             {
-                // float channels: corner offsets rounded once from double
-                float sx0, sx1, sy0, sy1, sz0, sz1;
-                axis_corners_stable(vsf, R.q0.x, x, sx0, sx1);
-                axis_corners_stable(vsf, R.q0.y, yy, sy0, sy1);
-                axis_corners_stable(vsf, R.q0.z, zz, sz0, sz1);
-                const bool same = sx0 == cx0 && sx1 == cx1 && sy0 == cy0 && sy1 == cy1 && sz0 == cz0 && sz1 == cz1;
-                a = same ? a8 : pair_alpha(R, aabb_from_corners(R, M, sx0, sx1, sy0, sy1, sz0, sz1));
+                // float channels: the stable form (corner offsets rounded once)
+                const float sz0 = VOX_FFMA(v0, vsf, -pz), sz1 = VOX_FFMA(v1, vsf, -pz);
+                Aabb f;
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                {
+                    const float k = VOX_FMUL(il, is[r]);
+                    const float cl = mz[r] >= 0.f ? sz0 : sz1, ch = mz[r] >= 0.f ? sz1 : sz0;
+                    f.lo[r] = VOX_FMUL(VOX_FFMA(cl, mz[r], S.cf_lo[r][ci]), k);
+                    f.hi[r] = VOX_FMUL(VOX_FFMA(ch, mz[r], S.cf_hi[r][ci]), k);
+                }
+                a = pair_alpha_f(R, f);
             }
             S.res_a[j][n] = a;
             S.res_rgba[j][n] = pack_rgba8(R, a8);

@@ -207,16 +207,7 @@ static void prim_setup(prim_t* P, const float* mean, const float* quat_wxyz, con
 }
 
 /* gaussian_frag_alloc.slang:84-162: returns 1 when dist2 > 0 */
-/* stable = 1: corner offsets v * vs - mu computed in double and rounded once
- * (used for the float density / colour channels only, not the reference test) */
-static int frag_test_ex(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float* vmin,
-                        float* vmax, int stable);
 static int frag_test(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float* vmin, float* vmax)
-{
-    return frag_test_ex(P, rinv, vs, ijk, vmin, vmax, 0);
-}
-static int frag_test_ex(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float* vmin,
-                        float* vmax, int stable)
 {
     float inv_ls = VOX_FDIV(1.f, P->ls);
     float inv_s[3] = { VOX_FDIV(1.f, P->s[0]), VOX_FDIV(1.f, P->s[1]), VOX_FDIV(1.f, P->s[2]) };
@@ -231,8 +222,7 @@ static int frag_test_ex(const prim_t* P, const float rinv[3][3], float vs, const
             vp[2] = VOX_FADD(vp[2], 1.f);
         float lp[3];
         for (int a = 0; a < 3; a++)
-            lp[a] = stable ? (float)((double)vp[a] * (double)vs - (double)P->pos[a])
-                           : VOX_FSUB(VOX_FMUL(vp[a], vs), P->pos[a]);
+            lp[a] = VOX_FSUB(VOX_FMUL(vp[a], vs), P->pos[a]);
         float l[3] = { dot3(lp, rinv[0]), dot3(lp, rinv[1]), dot3(lp, rinv[2]) };
         for (int a = 0; a < 3; a++)
         {
@@ -289,6 +279,63 @@ static uint32_t frag_rgba(const prim_t* P, float vs, float cull_scale, const flo
         out |= ((uint32_t)VOX_FMUL(255.f, v)) << (8 * c);
     }
     return out;
+}
+
+/* Float density / colour channels (this build's F-mode output; the reference
+ * has only RGBA8).  The alpha of gaussian_frag_color.slang:184-217 - local
+ * AABB of the voxel, maximum over the 4x4x4 lattice, opacity transform, cull -
+ * in a numerically stable float form:
+ *   corner offsets fma(v, vs, -mu), rounded once (fl(fl(v vs) - mu) loses
+ *     the low bits of mu far from the origin);
+ *   per row r the lower / upper corner of each axis picked by the sign of
+ *     rinv[r][a] (the products' minimum / maximum), summed with fma:
+ *     lo_r = fl(fma(cz, m_z, fma(cx, m_x, fl(cy m_y))) * fl(inv_ls inv_s_r));
+ *   lattice points lo + w (hi - lo), w = 0, 1/3, 2/3, 1; the maximum of the
+ *     decreasing exp is at the per-axis smallest square;
+ *   float exp / pow (vox_expf, vox_powf).
+ * The device evaluates the same operations in the same order. */
+static float frag_alpha_f(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float cull_scale)
+{
+    const float inv_ls = VOX_FDIV(1.f, P->ls);
+    float c0[3], c1[3];
+    for (int a = 0; a < 3; a++)
+    {
+        const float v = (float)ijk[a];
+        c0[a] = VOX_FFMA(v, vs, -P->pos[a]);
+        c1[a] = VOX_FFMA(VOX_FADD(v, 1.f), vs, -P->pos[a]);
+    }
+    float m[3];
+    for (int r = 0; r < 3; r++)
+    {
+        const float* w = rinv[r];
+        float cl[3], ch[3];
+        for (int a = 0; a < 3; a++)
+        {
+            cl[a] = w[a] >= 0.f ? c0[a] : c1[a];
+            ch[a] = w[a] >= 0.f ? c1[a] : c0[a];
+        }
+        const float k = VOX_FMUL(inv_ls, VOX_FDIV(1.f, P->s[r]));
+        const float lo = VOX_FMUL(VOX_FFMA(cl[2], w[2], VOX_FFMA(cl[0], w[0], VOX_FMUL(cl[1], w[1]))), k);
+        const float hi = VOX_FMUL(VOX_FFMA(ch[2], w[2], VOX_FFMA(ch[0], w[0], VOX_FMUL(ch[1], w[1]))), k);
+        const float dd = VOX_FSUB(hi, lo);
+        const float p1 = VOX_FFMA(dd, 0x1.555556p-2f, lo), p2 = VOX_FFMA(dd, 0x1.555556p-1f, lo);
+        float best = VOX_FMUL(lo, lo);
+        const float s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2), s3 = VOX_FMUL(hi, hi);
+        best = s1 < best ? s1 : best;
+        best = s2 < best ? s2 : best;
+        best = s3 < best ? s3 : best;
+        m[r] = best;
+    }
+    const float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
+    float a = VOX_FMUL(P->op, vox_expf(-VOX_FMUL(P->ls, d)));
+    a = a > 0.f ? a : 0.f;
+    const float scale1d = VOX_FSQRT(dot3(P->s, P->s));
+    const float vrs = VOX_FDIV(VOX_FMUL(0.1f, scale1d), vs);
+    a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), VOX_FDIV(1.f, vrs)));
+    const float cull = cull_scale > 0.f ? cull_scale : 0.05f;
+    if (scale1d > cull)
+        a = 0.f;
+    return a;
 }
 
 /* FP64 restatement of the same alpha (lattice of 64 samples, cull), computed
@@ -808,9 +855,7 @@ static void* values_worker(void* arg)
                 }
                 continue;
             }
-            /* float channels: the same alpha from corner offsets rounded once from double */
-            frag_test_ex(P, rinv, S->vs, ijk, vmin, vmax, 1);
-            frag_rgba(P, S->vs, S->cull, vmin, vmax, &a);
+            a = frag_alpha_f(P, rinv, S->vs, ijk, S->cull);
             dsum = VOX_FADD(dsum, a);
             for (int ch = 0; ch < 3; ch++)
                 csum[ch] = VOX_FADD(csum[ch], VOX_FMUL(a, P->rgb[ch]));
