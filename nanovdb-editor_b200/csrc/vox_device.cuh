@@ -359,6 +359,42 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
     return a;
 }
 
+// Stable local AABB of voxel (i, j, k) for the float channels: corner offsets
+// fma(v, vs, -mu) rounded once; per row the lower / upper corner of each axis
+// picked by the sign of the matrix entry (the products' minimum / maximum),
+// lo = fl(fma(cz, m_z, fma(cx, m_x, fl(cy m_y))) * fl(inv_ls * inv_s)).
+__device__ __forceinline__ Aabb stable_local_aabb(const GaussRec& R, const RInv& M, float vs, int32_t i, int32_t j,
+                                                  int32_t k)
+{
+    const int32_t v[3] = { i, j, k };
+    const float mu[3] = { R.q0.x, R.q0.y, R.q0.z };
+    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
+    float c0[3], c1[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const float vf = (float)v[a];
+        c0[a] = VOX_FFMA(vf, vs, -mu[a]);
+        c1[a] = VOX_FFMA(VOX_FADD(vf, 1.f), vs, -mu[a]);
+    }
+    Aabb b;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+    {
+        float cl[3], ch[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+        {
+            cl[a] = M.m[r][a] >= 0.f ? c0[a] : c1[a];
+            ch[a] = M.m[r][a] >= 0.f ? c1[a] : c0[a];
+        }
+        const float k = VOX_FMUL(R.q0.w, inv_s[r]);
+        b.lo[r] = VOX_FMUL(VOX_FFMA(cl[2], M.m[r][2], VOX_FFMA(cl[0], M.m[r][0], VOX_FMUL(cl[1], M.m[r][1]))), k);
+        b.hi[r] = VOX_FMUL(VOX_FFMA(ch[2], M.m[r][2], VOX_FFMA(ch[0], M.m[r][0], VOX_FMUL(ch[1], M.m[r][1]))), k);
+    }
+    return b;
+}
+
 // Alpha of the float density / colour channels from the stable local AABB
 // (corner offsets fma(v, vs, -mu), sign-picked corners summed with fma): the
 // lattice points lo + w (hi - lo), float exp / pow.  The oracle's
@@ -416,6 +452,32 @@ __device__ __forceinline__ float smooth_kernel(const GaussRec& R, const RInv& M,
     t.E = vox_expf_cr(VOX_FMUL(-0.5f, q));
     t.e = VOX_FMUL(R.q6.x, t.E);
     return t.e > SMOOTH_TAU ? VOX_FSUB(t.e, SMOOTH_TAU) : 0.f;
+}
+
+// Float channels accumulate as exact 64-bit fixed-point sums (2^-32 units):
+// every term is rounded once to the grid, so the sum is the same integer in any
+// order (shared-memory atomics are deterministic); the total is rounded once to
+// float.  Terms are clamped to +-2^30.
+constexpr float FX_SCALE = 4294967296.f;          // 2^32
+constexpr float FX_INV = 2.3283064365386963e-10f; // 2^-32
+constexpr float FX_CLAMP = 1073741824.f;          // 2^30
+__device__ __forceinline__ unsigned long long fx_of(float x)
+{
+    x = x < FX_CLAMP ? x : FX_CLAMP;
+    x = x > -FX_CLAMP ? x : -FX_CLAMP;
+    return (unsigned long long)__float2ll_rn(VOX_FMUL(x, FX_SCALE));
+}
+__device__ __forceinline__ float fx_to_float(unsigned long long s)
+{
+    return VOX_FMUL(__ll2float_rn((long long)s), FX_INV);
+}
+
+// one RGBA8 channel byte of gaussian_frag_color.slang:239-246: clamp to [0, 1], 255 v truncated
+__device__ __forceinline__ uint32_t rgba8_byte(float v)
+{
+    v = v < 1.f ? v : 1.f;
+    v = 0.f > v ? 0.f : v;
+    return (uint32_t)VOX_FMUL(255.f, v);
 }
 
 __device__ __forceinline__ uint32_t pack_rgba8(const GaussRec& R, float a)

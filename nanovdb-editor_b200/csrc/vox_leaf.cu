@@ -237,44 +237,59 @@ __device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S
 }
 
 // ------------------------------------------------------ forward leaf walk
-// Per chunk of LQ_CHUNK Gaussians (ascending id) staged in shared memory:
-//   box    the part of each Gaussian's bbox inside the leaf;
-//   test   the boxes' columns laid out densely, one (Gaussian, column) per
-//          thread: the x / y share of the reference test once per column, then
-//          the column's z run in order, each z's corner products shared with
-//          the next; passing (Gaussian, voxel) pairs go to a shared queue (any
-//          order);
-//   alpha  the RGBA8 byte and the float-channel alpha of every queued pair,
-//          one pair per thread, into a per-(Gaussian, voxel) table;
-//   sum    each thread folds its two voxels' table entries in ascending
-//          Gaussian id, so every float sum has the order of a serial loop.
+// A CTA walks a stream of candidate leaves in chunks of LQ_CHUNK Gaussians
+// (a leaf's Gaussians in ascending id).  Per chunk:
+//   test   the part of each Gaussian's bbox inside the leaf, one (Gaussian,
+//          column) per thread: the column's x / y share once, then its z run,
+//          each z's corner products shared with the next; passing (Gaussian,
+//          voxel) pairs go to a shared queue;
+//   alpha  one queued pair per thread: the reference's RGBA8 alpha and the
+//          float channels' stable alpha, accumulated per voxel with shared
+//          atomics - RGBA8 maximum, pair count, 64-bit fixed-point density /
+//          colour sums (exact, so independent of order);
+//   flush  once a leaf's last alpha is done: its staged values, value mask
+//          and pair count.
+// One barrier per chunk: phase i runs the flush of the leaf that ended with
+// chunk i - 2, the alpha of chunk i - 1, the test of chunk i, and the staging
+// of chunk i + 1 (lanes of the last warp copy its records with cp.async and
+// place its boxes).  Chunk data is triple-buffered, queues double-buffered,
+// the per-voxel accumulators double-buffered by leaf parity.
 constexpr int LQ_CHUNK = 8;
 constexpr int LQ_STAGE_T0 = LP_THREADS - 32; // lanes 0..LQ_CHUNK-1 of the last warp stage the next chunk
 
-struct LeafQSmem
+struct LeafChunk
 {
-    GaussRec rec[2][LQ_CHUNK]; // double-buffered records: the next chunk's land while this one is walked
-    uint8_t flag[LQ_CHUNK];
+    GaussRec rec[LQ_CHUNK];                              // first member: 16-byte aligned for cp.async
     int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK]; // box origin, leaf-relative
     uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK];               // box extents in y and z
     uint32_t bdiv_y[LQ_CHUNK];                           // 65536 / ny, rounded up (exact division below 64)
     uint32_t bcol[LQ_CHUNK];                             // box columns, nx * ny (0: empty box)
+    uint32_t rgb24[LQ_CHUNK];                            // the colour bytes of the packed RGBA8 value
     float vs[LQ_CHUNK];
-    // x / y shares of every column with a passing voxel, per row: the
-    // reference test's (sums of the per-axis min / max corner products) and the
-    // float channels' stable form (fma over the sign-picked corners)
-    float cr_lo[3][LQ_CHUNK * 64], cr_hi[3][LQ_CHUNK * 64];
-    float cf_lo[3][LQ_CHUNK * 64], cf_hi[3][LQ_CHUNK * 64];
-    uint16_t queue[LQ_CHUNK * 512];
-    float res_a[LQ_CHUNK][512];
-    uint32_t res_rgba[LQ_CHUNK][512];
-    uint32_t pbits[512];
-    uint64_t mask[8];
+    uint8_t flag[LQ_CHUNK];
     uint64_t wf0[LQ_CHUNK], wbase[LQ_CHUNK]; // reference windows: fragment offset in its batch, windows before
-    uint64_t wmin;
-    int32_t nxt_o[3];                        // the next chunk: leaf origin and sorted pair range
-    uint32_t nxt_q0, nxt_p1;
-    uint32_t qn, pairs, cand, cand_next;
+};
+
+struct LeafAcc
+{
+    unsigned long long dens[512];   // fixed-point sums
+    unsigned long long col[3][512];
+    uint32_t cnt[512];              // passing pairs
+    uint32_t rgba[512];             // packed RGBA8 maximum
+    unsigned long long wmin;        // creation window (reference node order)
+};
+
+struct LeafQSmem
+{
+    LeafChunk ch[3];
+    LeafAcc acc[2];
+    uint16_t queue[2][LQ_CHUNK * 512];
+    uint32_t qn[3];
+    int32_t nxt_o[2][3]; // the next chunk (by phase parity): leaf origin and sorted pair range
+    uint32_t nxt_q0[2], nxt_p1[2];
+    uint32_t cand_next[2];
+    uint32_t cand;
+    unsigned long long pairs;
 };
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src)
@@ -301,36 +316,33 @@ __device__ __forceinline__ uint32_t leaf_stage_issue(const LeafPassParams& P, Ga
 
 // once the record landed: the part of the Gaussian's bbox inside the leaf at o
 template <bool CHECK, bool WINDOW>
-__device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafQSmem& S, const GaussRec& R, int j,
-                                               uint32_t q, uint32_t g, const int32_t o[3])
+__device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChunk& C, int j, uint32_t q, uint32_t g,
+                                               const int32_t o[3])
 {
+    const GaussRec& R = C.rec[j];
     const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
     const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
     const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
     const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
     const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
-    S.bx0[j] = x0;
-    S.by0[j] = y0;
-    S.bz0[j] = z0;
-    S.bny[j] = ny;
-    S.bnz[j] = nz;
-    S.bdiv_y[j] = (65536u + ny - 1u) / ny;
-    S.bcol[j] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
-    S.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
-    S.flag[j] = CHECK ? P.emit_flag[P.vals[q]] : 0;
+    C.bx0[j] = x0;
+    C.by0[j] = y0;
+    C.bz0[j] = z0;
+    C.bny[j] = ny;
+    C.bnz[j] = nz;
+    C.bdiv_y[j] = (65536u + ny - 1u) / ny;
+    C.bcol[j] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
+    C.rgb24[j] = rgba8_byte(R.q7.x) | (rgba8_byte(R.q7.y) << 8) | (rgba8_byte(R.q7.z) << 16);
+    C.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
+    C.flag[j] = CHECK ? P.emit_flag[P.vals[q]] : 0;
     if (WINDOW)
     {
         const int64_t batch = (int64_t)g / REF_PRIM_BATCH;
-        S.wf0[j] = P.frag_off[g] - P.frag_off[batch * REF_PRIM_BATCH];
-        S.wbase[j] = P.win_before[batch];
+        C.wf0[j] = P.frag_off[g] - P.frag_off[batch * REF_PRIM_BATCH];
+        C.wbase[j] = P.win_before[batch];
     }
 }
 
-// Chunks are software-pipelined: while chunk k is tested, the last warp's
-// first lanes copy chunk k + 1's records (cp.async, the other buffer); they
-// wait for their own copies and place chunk k + 1's boxes during chunk k's sum.
-// The next candidate leaf is claimed one leaf ahead, so a leaf's first chunk
-// is staged like any other.  Three barriers per chunk.
 template <bool CHECK, bool WINDOW>
 __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, uint32_t* counter)
 {
@@ -342,331 +354,310 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
     if (t == 0)
     {
         S.cand = atomicAdd(counter, 1u);
-        S.cand_next = atomicAdd(counter, 1u);
+        S.cand_next[0] = atomicAdd(counter, 1u);
         S.pairs = 0;
-        S.wmin = ~0ull;
-        S.qn = 0;
+        S.qn[0] = S.qn[1] = S.qn[2] = 0;
+        S.acc[0].wmin = S.acc[1].wmin = ~0ull;
     }
-    if (t < 8)
-        S.mask[t] = 0;
-    S.pbits[t] = 0;
-    S.pbits[t + 256] = 0;
-    __syncthreads();
-    int64_t c = S.cand;
-    if (c >= P.NCL)
-        return;
-    int64_t cn = S.cand_next;
-    int32_t o[3];
-    cand_origin(P, P.cand_key[c], o);
-    uint32_t q0 = P.cand_start[c], p1 = P.cand_start[c + 1];
-    int buf = 0;
-    if (stager && js < (int)min((uint32_t)LQ_CHUNK, p1 - q0))
-    {
-        const uint32_t g = leaf_stage_issue(P, &S.rec[0][js], q0 + (uint32_t)js);
-        cp_async_wait_all();
-        leaf_stage_box<CHECK, WINDOW>(P, S, S.rec[0][js], js, q0 + (uint32_t)js, g, o);
-    }
-    __syncthreads();
-    uint32_t rgba[2] = { 0u, 0u }, pc[2] = { 0u, 0u };
-    float ds[2] = { 0.f, 0.f }, cr[2] = { 0.f, 0.f }, cgr[2] = { 0.f, 0.f }, cb[2] = { 0.f, 0.f };
-    while (true)
-    {
-        const uint32_t cnt = min((uint32_t)LQ_CHUNK, p1 - q0);
-        const bool leaf_end = q0 + LQ_CHUNK >= p1;
-        const int64_t nc = leaf_end ? cn : c;
-        const bool has_next = nc < P.NCL;
-        // ---- stagers: the next chunk's pair range, its record copies
-        uint32_t nq0 = 0, np1 = 0, ncnt = 0, ng = 0;
-        if (stager && has_next)
-        {
-            nq0 = leaf_end ? P.cand_start[nc] : q0 + LQ_CHUNK;
-            np1 = leaf_end ? P.cand_start[nc + 1] : p1;
-            ncnt = min((uint32_t)LQ_CHUNK, np1 - nq0);
-            if (js < (int)ncnt)
-                ng = leaf_stage_issue(P, &S.rec[buf ^ 1][js], nq0 + (uint32_t)js);
-        }
-        const GaussRec* rec = S.rec[buf];
-        uint32_t start[LQ_CHUNK + 1];
-        start[0] = 0;
 #pragma unroll
-        for (int j = 0; j < LQ_CHUNK; j++)
-            start[j + 1] = start[j] + (j < (int)cnt ? S.bcol[j] : 0u);
-        const uint32_t T = start[LQ_CHUNK];
-        // ---- test, one box column per thread.  Bit-identical to
-        // voxel_local_aabb + aabb_hits_unit_sphere per voxel: the z corner c1
-        // of voxel z is c0 of voxel z + 1 (integer-valued floats), and "lo > 0:
-        // subtract lo^2, else hi < 0: subtract hi^2" selects the pre-scale sum
-        // with the same sign (inv_ls, inv_s > 0; an underflow to zero
-        // subtracts zero).
-        for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
-        {
-            const uint32_t e = b0 + (uint32_t)t;
-            uint32_t zmask = 0, ebase = 0;
-            if (e < T)
-            {
-                int j = 0;
-                uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
-#pragma unroll
-                for (int q = 1; q < LQ_CHUNK; q++)
-                {
-                    const bool ge = e >= start[q];
-                    j += ge ? 1 : 0;
-                    sj = ge ? start[q] : sj;
-                }
-                const uint32_t local = e - sj;
-                const uint32_t dx = (local * S.bdiv_y[j]) >> 16;
-                const uint32_t dy = local - dx * S.bny[j];
-                const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz0 = S.bz0[j];
-                const GaussRec& R = rec[j];
-                const RInv M = rinv_of(R);
-                const float vsf = S.vs[j], il = R.q0.w, pz = R.q0.z;
-                const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
-                float cx0, cx1, cy0, cy1;
-                axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
-                axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
-                float slo[3], shi[3], pa[3];
-                float v = (float)(o[2] + rz0);
-                float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-                {
-                    float xn, xx, yn, yx;
-                    minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
-                    minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
-                    slo[r] = VOX_FADD(xn, yn);
-                    shi[r] = VOX_FADD(xx, yx);
-                    pa[r] = VOX_FMUL(cz, M.m[r][2]);
-                }
-                const uint32_t nz = S.bnz[j];
-                for (uint32_t k = 0; k < nz; k++)
-                {
-                    v = VOX_FADD(v, 1.f);
-                    cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-                    float d2 = 1.f;
-#pragma unroll
-                    for (int r = 0; r < 3; r++)
-                    {
-                        const float pb = VOX_FMUL(cz, M.m[r][2]);
-                        const float zn = pa[r] < pb ? pa[r] : pb, zx = pa[r] < pb ? pb : pa[r];
-                        pa[r] = pb;
-                        const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
-                        const float x = 0.f < xl ? xl : (0.f > xh ? xh : 0.f);
-                        const float sv = VOX_FMUL(VOX_FMUL(x, il), is[r]);
-                        d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
-                    }
-                    zmask |= (d2 > 0.f ? 1u : 0u) << k;
-                }
-                if (zmask)
-                {
-                    const uint32_t ci = (uint32_t)j * 64u + (uint32_t)(rx * 8 + ry);
-                    const float vx = (float)(o[0] + rx), vy = (float)(o[1] + ry);
-                    const float sx0 = VOX_FFMA(vx, vsf, -R.q0.x), sx1 = VOX_FFMA(VOX_FADD(vx, 1.f), vsf, -R.q0.x);
-                    const float sy0 = VOX_FFMA(vy, vsf, -R.q0.y), sy1 = VOX_FFMA(VOX_FADD(vy, 1.f), vsf, -R.q0.y);
-#pragma unroll
-                    for (int r = 0; r < 3; r++)
-                    {
-                        const float mx = M.m[r][0], my = M.m[r][1];
-                        const float clx = mx >= 0.f ? sx0 : sx1, chx = mx >= 0.f ? sx1 : sx0;
-                        const float cly = my >= 0.f ? sy0 : sy1, chy = my >= 0.f ? sy1 : sy0;
-                        S.cr_lo[r][ci] = slo[r];
-                        S.cr_hi[r][ci] = shi[r];
-                        S.cf_lo[r][ci] = VOX_FFMA(clx, mx, VOX_FMUL(cly, my));
-                        S.cf_hi[r][ci] = VOX_FFMA(chx, mx, VOX_FMUL(chy, my));
-                    }
-                }
-                ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
-                if (CHECK && zmask && S.flag[j])
-                    atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
-            }
-            // queue slots: warp inclusive scan of the pass counts, one shared atomic per warp
-            const uint32_t np = (uint32_t)__popc(zmask);
-            uint32_t incl = np;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1)
-            {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
-                if (lane >= off)
-                    incl += y;
-            }
-            uint32_t qb = 0;
-            if (lane == 31 && incl)
-                qb = atomicAdd(&S.qn, incl);
-            qb = __shfl_sync(0xffffffffu, qb, 31) + incl - np;
-            for (uint32_t m = zmask; m; m &= m - 1)
-                S.queue[qb++] = (uint16_t)(ebase + (uint32_t)(__ffs(m) - 1));
-        }
-        __syncthreads();
-        // ---- alpha, one queued pair per thread
-        const uint32_t qn = S.qn;
-        for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
-        {
-            const uint32_t q = S.queue[e];
-            const uint32_t j = q >> 9, n = q & 511u, ci = (j << 6) | (n >> 3);
-            const GaussRec& R = rec[j];
-            const float vsf = S.vs[j], il = R.q0.w, pz = R.q0.z;
-            const float mz[3] = { R.q1.z, R.q2.y, R.q3.x }; // rinv[r][2]
-            const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
-            const int32_t x = o[0] + (int32_t)(n >> 6), yy = o[1] + (int32_t)((n >> 3) & 7), zz = o[2] + (int32_t)(n & 7);
-            const float v0 = (float)zz, v1 = VOX_FADD(v0, 1.f);
-            // RGBA8: the reference's local AABB from the column's staged x / y shares
-            // (bit-identical to voxel_local_aabb)
-            const float cz0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz), cz1 = VOX_FSUB(VOX_FMUL(v1, vsf), pz);
-            Aabb b;
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-            {
-                float zn, zx;
-                minmax_prod(cz0, cz1, mz[r], zn, zx);
-                b.lo[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(S.cr_lo[r][ci], zn), il), is[r]);
-                b.hi[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(S.cr_hi[r][ci], zx), il), is[r]);
-            }
-            const float a8 = pair_alpha(R, b);
-            float a;
-            if (P.smooth)
-            {
-                SmoothTerms st;
-                a = smooth_kernel(R, rinv_of(R), vsf, x, yy, zz, st);
-            }
-            else
-            {
-                // float channels: the stable form (corner offsets rounded once)
-                const float sz0 = VOX_FFMA(v0, vsf, -pz), sz1 = VOX_FFMA(v1, vsf, -pz);
-                Aabb f;
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-                {
-                    const float k = VOX_FMUL(il, is[r]);
-                    const float cl = mz[r] >= 0.f ? sz0 : sz1, ch = mz[r] >= 0.f ? sz1 : sz0;
-                    f.lo[r] = VOX_FMUL(VOX_FFMA(cl, mz[r], S.cf_lo[r][ci]), k);
-                    f.hi[r] = VOX_FMUL(VOX_FFMA(ch, mz[r], S.cf_hi[r][ci]), k);
-                }
-                a = pair_alpha_f(R, f);
-            }
-            S.res_a[j][n] = a;
-            S.res_rgba[j][n] = pack_rgba8(R, a8);
-            atomicOr(&S.pbits[n], 1u << j);
-            if (WINDOW)
-            {
-                // the reference's window of this fragment: x-major index in the bbox
-                // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
-                const uint64_t r = (uint64_t)(x - R.q4.x) * (uint64_t)R.q5.y * (uint64_t)R.q5.z +
-                                   (uint64_t)(yy - R.q4.y) * (uint64_t)R.q5.z + (uint64_t)(zz - R.q4.z);
-                atomicMin((unsigned long long*)&S.wmin, (unsigned long long)(S.wbase[j] + (S.wf0[j] + r) / REF_WINDOW));
-            }
-        }
-        __syncthreads();
-        // ---- sum in ascending Gaussian id; each thread clears its voxels' bits
+    for (int b = 0; b < 2; b++)
 #pragma unroll
         for (int h = 0; h < 2; h++)
         {
-            const uint32_t n = (uint32_t)(t + 256 * h);
-            const uint32_t bits = S.pbits[n];
-            for (uint32_t m = bits; m; m &= m - 1)
-            {
-                const int j = __ffs(m) - 1;
-                const float a = S.res_a[j][n];
-                const uint32_t px = S.res_rgba[j][n];
-                const GaussRec& R = rec[j];
-                rgba[h] = px > rgba[h] ? px : rgba[h];
-                ds[h] = VOX_FADD(ds[h], a);
-                cr[h] = VOX_FADD(cr[h], VOX_FMUL(a, R.q7.x));
-                cgr[h] = VOX_FADD(cgr[h], VOX_FMUL(a, R.q7.y));
-                cb[h] = VOX_FADD(cb[h], VOX_FMUL(a, R.q7.z));
-                pc[h]++;
-            }
-            if (bits)
-                S.pbits[n] = 0;
+            const int n = t + 256 * h;
+            S.acc[b].dens[n] = 0;
+            S.acc[b].col[0][n] = S.acc[b].col[1][n] = S.acc[b].col[2][n] = 0;
+            S.acc[b].cnt[n] = 0;
+            S.acc[b].rgba[n] = 0;
         }
-        if (t == 0)
-            S.qn = 0;
-        if (leaf_end)
+    __syncthreads();
+    // the chunk being tested (t*), the chunk whose alpha runs (a*), the leaf being flushed (f*)
+    int64_t tc = S.cand;
+    if (tc >= P.NCL)
+        return;
+    int64_t cn = S.cand_next[0];
+    int32_t to[3];
+    cand_origin(P, P.cand_key[tc], to);
+    uint32_t tq0 = P.cand_start[tc], tp1 = P.cand_start[tc + 1];
+    if (stager && js < (int)min((uint32_t)LQ_CHUNK, tp1 - tq0))
+    {
+        const uint32_t g = leaf_stage_issue(P, &S.ch[0].rec[js], tq0 + (uint32_t)js);
+        cp_async_wait_all();
+        leaf_stage_box<CHECK, WINDOW>(P, S.ch[0], js, tq0 + (uint32_t)js, g, to);
+    }
+    __syncthreads();
+    bool t_valid = true, a_valid = false, f_valid = false, a_leaf_end = false;
+    int tpar = 0, apar = 0, fpar = 0;
+    int64_t ac = 0, fc = 0;
+    int32_t ao[3] = { 0, 0, 0 };
+    uint32_t i = 0; // phase
+    while (t_valid || a_valid || f_valid)
+    {
+        const int tb = (int)(i % 3u), ab = (int)((i + 2u) % 3u), nb = (int)((i + 1u) % 3u);
+        const bool t_leaf_end = t_valid && tq0 + LQ_CHUNK >= tp1;
+        const int64_t nc = t_leaf_end ? cn : tc;
+        const bool n_valid = t_valid && nc < P.NCL;
+        // ---- stagers: the next chunk's pair range, its record copies
+        uint32_t nq0 = 0, np1 = 0, ncnt = 0, ng = 0;
+        if (stager && n_valid)
         {
-            // value mask from ballots: voxel A (leaf_n = t) of warp w is bit 32 (w & 1) + lane of word w >> 1
-            const uint32_t ba = __ballot_sync(0xffffffffu, pc[0] > 0), bb = __ballot_sync(0xffffffffu, pc[1] > 0);
-            uint32_t wp = pc[0] + pc[1];
+            nq0 = t_leaf_end ? P.cand_start[nc] : tq0 + LQ_CHUNK;
+            np1 = t_leaf_end ? P.cand_start[nc + 1] : tp1;
+            ncnt = min((uint32_t)LQ_CHUNK, np1 - nq0);
+            if (js < (int)ncnt)
+                ng = leaf_stage_issue(P, &S.ch[nb].rec[js], nq0 + (uint32_t)js);
+        }
+        // ---- flush of the leaf whose last alpha ran in the previous phase
+        if (f_valid)
+        {
+            LeafAcc& A = S.acc[fpar];
+            uint32_t cnt[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+            {
+                const uint32_t n = (uint32_t)(t + 256 * h);
+                cnt[h] = A.cnt[n];
+                if (cnt[h])
+                {
+                    const uint64_t slot = (uint64_t)fc * 512u + n;
+                    const float ds = fx_to_float(A.dens[n]);
+                    float col[3];
+#pragma unroll
+                    for (int k = 0; k < 3; k++)
+                    {
+                        col[k] = fx_to_float(A.col[k][n]);
+                        if (!P.smooth)
+                            col[k] = ds > 0.f ? VOX_FDIV(col[k], ds) : 0.f;
+                    }
+                    P.s_rgba[slot] = A.rgba[n];
+                    P.s_dens[slot] = ds;
+                    P.s_col[3 * slot + 0] = col[0];
+                    P.s_col[3 * slot + 1] = col[1];
+                    P.s_col[3 * slot + 2] = col[2];
+                    P.s_pairs[slot] = cnt[h];
+                    A.dens[n] = 0;
+                    A.col[0][n] = A.col[1][n] = A.col[2][n] = 0;
+                    A.cnt[n] = 0;
+                    A.rgba[n] = 0;
+                }
+            }
+            // value mask: voxel t of warp w is bit lane of 32-bit word w (w + 8 for voxel t + 256)
+            const uint32_t ba = __ballot_sync(0xffffffffu, cnt[0] > 0), bb = __ballot_sync(0xffffffffu, cnt[1] > 0);
+            unsigned long long wp = cnt[0] + cnt[1];
 #pragma unroll
             for (int off = 16; off; off >>= 1)
                 wp += __shfl_xor_sync(0xffffffffu, wp, off);
             if (lane == 0)
             {
-                atomicOr((unsigned long long*)&S.mask[warp >> 1], (unsigned long long)ba << (32 * (warp & 1)));
-                atomicOr((unsigned long long*)&S.mask[4 + (warp >> 1)], (unsigned long long)bb << (32 * (warp & 1)));
-                atomicAdd(&S.pairs, wp);
+                uint32_t* m32 = reinterpret_cast<uint32_t*>(P.cand_mask + 8 * (uint64_t)fc);
+                m32[warp] = ba;
+                m32[8 + warp] = bb;
+                if (wp)
+                    atomicAdd(&S.pairs, wp);
             }
-#pragma unroll
-            for (int h = 0; h < 2; h++)
+            if (WINDOW && t == 0)
             {
-                if (pc[h])
-                {
-                    const uint64_t slot = (uint64_t)c * 512u + (uint32_t)(t + 256 * h);
-                    P.s_rgba[slot] = rgba[h];
-                    P.s_dens[slot] = ds[h];
-                    float col[3] = { cr[h], cgr[h], cb[h] };
-                    if (!P.smooth)
-                        for (int k = 0; k < 3; k++)
-                            col[k] = ds[h] > 0.f ? VOX_FDIV(col[k], ds[h]) : 0.f;
-                    P.s_col[3 * slot + 0] = col[0];
-                    P.s_col[3 * slot + 1] = col[1];
-                    P.s_col[3 * slot + 2] = col[2];
-                    P.s_pairs[slot] = pc[h];
-                }
-                rgba[h] = 0u;
-                pc[h] = 0u;
-                ds[h] = cr[h] = cgr[h] = cb[h] = 0.f;
+                P.cand_wkey[fc] = A.wmin;
+                A.wmin = ~0ull;
             }
         }
-        // ---- stagers: the next chunk's boxes (their own copies have landed)
-        if (stager && has_next)
+        // ---- alpha of the previous chunk, one queued pair per thread
+        if (a_valid)
         {
-            int32_t no[3] = { o[0], o[1], o[2] };
-            if (leaf_end)
+            const LeafChunk& C = S.ch[ab];
+            LeafAcc& A = S.acc[apar];
+            const uint16_t* queue = S.queue[(i + 1u) & 1u];
+            const uint32_t qn = S.qn[ab];
+            for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
+            {
+                const uint32_t q = queue[e];
+                const uint32_t j = q >> 9, n = q & 511u;
+                const GaussRec& R = C.rec[j];
+                const RInv M = rinv_of(R);
+                const float vsf = C.vs[j];
+                const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7), zz = ao[2] + (int32_t)(n & 7);
+                const float a8 = pair_alpha(R, voxel_local_aabb(R, M, vsf, x, yy, zz));
+                float a;
+                if (P.smooth)
+                {
+                    SmoothTerms st;
+                    a = smooth_kernel(R, M, vsf, x, yy, zz, st);
+                }
+                else
+                {
+                    a = pair_alpha_f(R, stable_local_aabb(R, M, vsf, x, yy, zz));
+                }
+                atomicAdd(&A.cnt[n], 1u);
+                atomicMax(&A.rgba[n], (rgba8_byte(a8) << 24) | C.rgb24[j]);
+                atomicAdd(&A.dens[n], fx_of(a));
+                atomicAdd(&A.col[0][n], fx_of(VOX_FMUL(a, R.q7.x)));
+                atomicAdd(&A.col[1][n], fx_of(VOX_FMUL(a, R.q7.y)));
+                atomicAdd(&A.col[2][n], fx_of(VOX_FMUL(a, R.q7.z)));
+                if (WINDOW)
+                {
+                    // the reference's window of this fragment: x-major index in the bbox
+                    // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
+                    const uint64_t r = (uint64_t)(x - R.q4.x) * (uint64_t)R.q5.y * (uint64_t)R.q5.z +
+                                       (uint64_t)(yy - R.q4.y) * (uint64_t)R.q5.z + (uint64_t)(zz - R.q4.z);
+                    atomicMin(&A.wmin, (unsigned long long)(C.wbase[j] + (C.wf0[j] + r) / REF_WINDOW));
+                }
+            }
+        }
+        // ---- test of this chunk, one box column per thread.  Bit-identical to
+        // voxel_local_aabb + aabb_hits_unit_sphere per voxel: the z corner c1
+        // of voxel z is c0 of voxel z + 1 (integer-valued floats), and "lo > 0:
+        // subtract lo^2, else hi < 0: subtract hi^2" selects the pre-scale sum
+        // with the same sign (inv_ls, inv_s > 0; an underflow to zero
+        // subtracts zero).
+        if (t_valid)
+        {
+            const LeafChunk& C = S.ch[tb];
+            uint16_t* queue = S.queue[i & 1u];
+            const uint32_t cnt = min((uint32_t)LQ_CHUNK, tp1 - tq0);
+            uint32_t start[LQ_CHUNK + 1];
+            start[0] = 0;
+#pragma unroll
+            for (int j = 0; j < LQ_CHUNK; j++)
+                start[j + 1] = start[j] + (j < (int)cnt ? C.bcol[j] : 0u);
+            const uint32_t T = start[LQ_CHUNK];
+            for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
+            {
+                const uint32_t e = b0 + (uint32_t)t;
+                uint32_t zmask = 0, ebase = 0;
+                if (e < T)
+                {
+                    int j = 0;
+                    uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
+#pragma unroll
+                    for (int q = 1; q < LQ_CHUNK; q++)
+                    {
+                        const bool ge = e >= start[q];
+                        j += ge ? 1 : 0;
+                        sj = ge ? start[q] : sj;
+                    }
+                    const uint32_t local = e - sj;
+                    const uint32_t dx = (local * C.bdiv_y[j]) >> 16;
+                    const uint32_t dy = local - dx * C.bny[j];
+                    const int32_t rx = C.bx0[j] + (int32_t)dx, ry = C.by0[j] + (int32_t)dy, rz0 = C.bz0[j];
+                    const GaussRec& R = C.rec[j];
+                    const RInv M = rinv_of(R);
+                    const float vsf = C.vs[j], il = R.q0.w, pz = R.q0.z;
+                    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+                    float cx0, cx1, cy0, cy1;
+                    axis_corners(vsf, R.q0.x, to[0] + rx, cx0, cx1);
+                    axis_corners(vsf, R.q0.y, to[1] + ry, cy0, cy1);
+                    float slo[3], shi[3], pa[3];
+                    float v = (float)(to[2] + rz0);
+                    float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        float xn, xx, yn, yx;
+                        minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
+                        minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
+                        slo[r] = VOX_FADD(xn, yn);
+                        shi[r] = VOX_FADD(xx, yx);
+                        pa[r] = VOX_FMUL(cz, M.m[r][2]);
+                    }
+                    const uint32_t nz = C.bnz[j];
+                    for (uint32_t k = 0; k < nz; k++)
+                    {
+                        v = VOX_FADD(v, 1.f);
+                        cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                        float d2 = 1.f;
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+                        {
+                            const float pb = VOX_FMUL(cz, M.m[r][2]);
+                            const float zn = pa[r] < pb ? pa[r] : pb, zx = pa[r] < pb ? pb : pa[r];
+                            pa[r] = pb;
+                            const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
+                            const float xs = 0.f < xl ? xl : (0.f > xh ? xh : 0.f);
+                            const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
+                            d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
+                        }
+                        zmask |= (d2 > 0.f ? 1u : 0u) << k;
+                    }
+                    ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
+                    if (CHECK && zmask && C.flag[j])
+                        atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
+                }
+                // queue slots: warp inclusive scan of the pass counts, one shared atomic per warp
+                const uint32_t np = (uint32_t)__popc(zmask);
+                uint32_t incl = np;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1)
+                {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+                    if (lane >= off)
+                        incl += y;
+                }
+                uint32_t qb = 0;
+                if (lane == 31 && incl)
+                    qb = atomicAdd(&S.qn[tb], incl);
+                qb = __shfl_sync(0xffffffffu, qb, 31) + incl - np;
+                for (uint32_t m = zmask; m; m &= m - 1)
+                    queue[qb++] = (uint16_t)(ebase + (uint32_t)(__ffs(m) - 1));
+            }
+        }
+        // the counter the test of phase i + 1 fills: last read by the alpha of phase i - 1
+        if (t == 0)
+            S.qn[nb] = 0;
+        // ---- stagers: the next chunk's boxes (their own copies have landed)
+        if (stager && n_valid)
+        {
+            int32_t no[3] = { to[0], to[1], to[2] };
+            if (t_leaf_end)
                 cand_origin(P, P.cand_key[nc], no);
             if (js < (int)ncnt)
             {
                 cp_async_wait_all();
-                leaf_stage_box<CHECK, WINDOW>(P, S, S.rec[buf ^ 1][js], js, nq0 + (uint32_t)js, ng, no);
+                leaf_stage_box<CHECK, WINDOW>(P, S.ch[nb], js, nq0 + (uint32_t)js, ng, no);
             }
             if (js == 0)
             {
-                S.nxt_o[0] = no[0];
-                S.nxt_o[1] = no[1];
-                S.nxt_o[2] = no[2];
-                S.nxt_q0 = nq0;
-                S.nxt_p1 = np1;
-                if (leaf_end)
-                    S.cand_next = atomicAdd(counter, 1u);
+                const int pp = (int)(i & 1u);
+                S.nxt_o[pp][0] = no[0];
+                S.nxt_o[pp][1] = no[1];
+                S.nxt_o[pp][2] = no[2];
+                S.nxt_q0[pp] = nq0;
+                S.nxt_p1[pp] = np1;
+                if (t_leaf_end)
+                    S.cand_next[pp] = atomicAdd(counter, 1u);
             }
         }
         __syncthreads();
-        if (leaf_end)
+        // ---- advance: flush <- alpha (at a leaf end), alpha <- test, test <- next
+        f_valid = a_valid && a_leaf_end;
+        fc = ac;
+        fpar = apar;
+        a_valid = t_valid;
+        a_leaf_end = t_leaf_end;
+        ac = tc;
+        apar = tpar;
+        ao[0] = to[0];
+        ao[1] = to[1];
+        ao[2] = to[2];
+        if (n_valid)
         {
-            if (t < 8)
+            const int pp = (int)(i & 1u);
+            if (t_leaf_end)
             {
-                P.cand_mask[8 * (uint64_t)c + t] = S.mask[t];
-                S.mask[t] = 0;
+                cn = S.cand_next[pp];
+                tpar ^= 1;
             }
-            if (t == 0)
-            {
-                if (S.pairs)
-                    atomicAdd((unsigned long long*)P.total_pairs, (unsigned long long)S.pairs);
-                S.pairs = 0;
-                if (WINDOW)
-                    P.cand_wkey[c] = S.wmin;
-                S.wmin = ~0ull;
-            }
+            tc = nc;
+            tq0 = S.nxt_q0[pp];
+            tp1 = S.nxt_p1[pp];
+            to[0] = S.nxt_o[pp][0];
+            to[1] = S.nxt_o[pp][1];
+            to[2] = S.nxt_o[pp][2];
         }
-        if (!has_next)
-            break;
-        if (leaf_end)
-            cn = S.cand_next;
-        c = nc;
-        q0 = S.nxt_q0;
-        p1 = S.nxt_p1;
-        o[0] = S.nxt_o[0];
-        o[1] = S.nxt_o[1];
-        o[2] = S.nxt_o[2];
-        buf ^= 1;
+        t_valid = n_valid;
+        i++;
     }
+    if (t == 0 && S.pairs)
+        atomicAdd((unsigned long long*)P.total_pairs, S.pairs);
 }
 
 __device__ __forceinline__ uint32_t mask_rank(const uint64_t* m, uint32_t n)

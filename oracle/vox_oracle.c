@@ -281,6 +281,24 @@ static uint32_t frag_rgba(const prim_t* P, float vs, float cull_scale, const flo
     return out;
 }
 
+/* The float channels sum as exact 64-bit fixed-point integers in units of
+ * 2^-32: each term rounded once to the grid (round to nearest even, clamped to
+ * +-2^30), the total rounded once to float.  The integer sum does not depend
+ * on the order of the terms; the device adds them with shared-memory atomics. */
+#define FX_SCALE 4294967296.f          /* 2^32 */
+#define FX_INV 2.3283064365386963e-10f /* 2^-32 */
+#define FX_CLAMP 1073741824.f          /* 2^30 */
+static int64_t fx_of(float x)
+{
+    x = x < FX_CLAMP ? x : FX_CLAMP;
+    x = x > -FX_CLAMP ? x : -FX_CLAMP;
+    return (int64_t)llrintf(VOX_FMUL(x, FX_SCALE));
+}
+static float fx_to_float(int64_t s)
+{
+    return VOX_FMUL((float)s, FX_INV);
+}
+
 /* Float density / colour channels (this build's F-mode output; the reference
  * has only RGBA8).  The alpha of gaussian_frag_color.slang:184-217 - local
  * AABB of the voxel, maximum over the 4x4x4 lattice, opacity transform, cull -
@@ -827,7 +845,7 @@ static void* values_worker(void* arg)
         uint64_t vi = S->vox_vidx[v];
         const int32_t* ijk = &S->vox_ijk[3 * v];
         uint32_t rgba = 0;
-        float dsum = 0.f, csum[3] = { 0.f, 0.f, 0.f };
+        int64_t dfx = 0, cfx[3] = { 0, 0, 0 };
         double dsum64 = 0.0, csum64[3] = { 0.0, 0.0, 0.0 };
         for (int64_t p = J->vstart[v]; p < J->vstart[v + 1]; p++)
         {
@@ -841,9 +859,9 @@ static void* values_worker(void* arg)
             if (S->smooth)
             {
                 float k = smooth_k_f32(P, rinv, S->vs, ijk);
-                dsum = VOX_FADD(dsum, k);
+                dfx += fx_of(k);
                 for (int ch = 0; ch < 3; ch++)
-                    csum[ch] = VOX_FADD(csum[ch], VOX_FMUL(k, P->rgb[ch]));
+                    cfx[ch] += fx_of(VOX_FMUL(k, P->rgb[ch]));
                 if (!S->skip_f64)
                 {
                     g64_t g;
@@ -856,14 +874,16 @@ static void* values_worker(void* arg)
                 continue;
             }
             a = frag_alpha_f(P, rinv, S->vs, ijk, S->cull);
-            dsum = VOX_FADD(dsum, a);
+            dfx += fx_of(a);
             for (int ch = 0; ch < 3; ch++)
-                csum[ch] = VOX_FADD(csum[ch], VOX_FMUL(a, P->rgb[ch]));
+                cfx[ch] += fx_of(VOX_FMUL(a, P->rgb[ch]));
             double a64 = S->skip_f64 ? 0.0 : frag_alpha64(P, (double)S->vs, (double)S->cull, ijk);
             dsum64 += a64;
             for (int ch = 0; ch < 3; ch++)
                 csum64[ch] += a64 * (double)P->rgb[ch];
         }
+        const float dsum = fx_to_float(dfx);
+        const float csum[3] = { fx_to_float(cfx[0]), fx_to_float(cfx[1]), fx_to_float(cfx[2]) };
         S->rgba[vi] = rgba;
         S->dens[vi] = dsum;
         S->dens64[vi] = dsum64;
