@@ -14,8 +14,14 @@ value   Gaussians/s with inputs resident in HBM (vox_voxelize on device
 e2e     same metric through the reference-facing C ABI with host buffers
         (pnanovdb_raster_t.raster_to_nanovdb_from_arrays: pinned host inputs
         in, host grid out, copies inside the timed call).
-roofline  achieved HBM GB/s of the dominant kernel stage from its algorithmic
-        bytes and its CUDA-event duration, against MEASURED_PEAKS.json.
+roofline  achieved HBM GB/s of the dominant kernel (the leaf walk) from the
+        algorithmic bytes of the (voxel, Gaussian)-pair work it performs - emit
+        12 B/pair (8 B key + 4 B id), sort 24 B/pair per 8-bit pass over the
+        voxel keys, accumulate 12 B/pair, values 20 B/voxel - and its
+        CUDA-event duration, against MEASURED_PEAKS.json; beside it the same
+        figure for the whole step (plus 2 x 56 B attribute reads per Gaussian
+        and the topology bytes), the kernel's own byte count, and the DRAM
+        traffic ncu measured for it.
 cpu_baseline  the CPU oracle (C restatement of the reference path; the
         reference's Vulkan path is unavailable on this box) on a bounded
         sample of the same workload on all host cores.
@@ -431,7 +437,16 @@ def main():
     }
     dom = max(stage_ms, key=lambda k: stage_ms[k])
     peak, peak_kind = load_peaks()
-    achieved = stage_bytes[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    # algorithmic bytes of the pair work: emit (8 B key + 4 B id), one 8-bit
+    # onesweep pass per 8 varying key bits (read + write key and id), one read
+    # of the sorted pairs to accumulate, density + colour + RGBA8 per voxel
+    sort_passes_pairs = (st["key_bits"] + 7) // 8
+    pair_bytes = 12 * P + 24 * P * sort_passes_pairs + 12 * P + 20 * V
+    topo_bytes = 80 * st["leaves"] + 1100 * st["lowers"] + 8300 * st["uppers"]
+    step_bytes = 2 * G * A + pair_bytes + topo_bytes
+    achieved = pair_bytes / (stage_ms["leaf_walk"] * 1e-3) / 1e9
+    step_achieved = step_bytes / (ms * 1e-3) / 1e9
+    own_achieved = stage_bytes[dom] / (stage_ms[dom] * 1e-3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -467,7 +482,21 @@ def main():
             "config": dict(WORKLOAD, gaussians=G, parallelism=f"replicas{world}" if world > 1 else "single", l2="256 MB flush between steps; pair working set >> L2", inputs="raw (log-scale, logit, SH0)"),
             "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind, "note": "the leaf walk is FP32/FP64 instruction-issue bound, not HBM bound"},
+            "roofline": {
+                "bound": "hbm",
+                "kernel": "leaf_walk",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": traffic,
+                "peak_source": peak_kind,
+                "algorithmic_bytes": pair_bytes,
+                "basis": f"pair work the leaf walk performs: 12 B/pair emit + 24 B/pair x {sort_passes_pairs} sort passes ({st['key_bits']}-bit voxel keys) + 12 B/pair accumulate + 20 B/voxel values",
+                "step": {"achieved": step_achieved, "frac": step_achieved / peak, "bytes": step_bytes},
+                "own_bytes": {"bytes": stage_bytes[dom], "achieved": own_achieved, "frac": own_achieved / peak,
+                              "note": "the leaf walk's own reads and writes: it never materialises the pairs, so DRAM stays far below peak; it is FP32/FP64 instruction-issue bound"},
+            },
             "stages_ms": stage_ms,
             "counts": {k: st[k] for k in ("candidates", "pairs", "voxels", "uppers", "lowers", "leaves", "key_bits", "sort_passes", "sort_shape", "leaf_pairs", "candidate_leaves")},
             "pairs_per_s": world * P / (ms * 1e-3),
