@@ -60,7 +60,7 @@ struct vox_context_t
     DevBuf vox_leaf, vox_n, rank_to_lower;
     // leaf-granular pipeline
     DevBuf lcols, lcol_off, lc_count, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask, pair_gid;
-    DevBuf s_rgba, s_dens, s_col, s_pairs, cand_cnt, cand_voff, vkeys, vslot, vpairs, pair_off, cand_vbase;
+    DevBuf s_rgba, s_dens, s_col, s_pairs, cand_cnt, cand_voff, vkeys, vslot, vpairs, pair_off, cand_vbase, cloud_pairs;
     DevBuf partials, exp_keys, exp_ids;
     // reference node order
     DevBuf nwin, win_before, cand_wkey, wkey_u, wkey_lo, wkey_leaf, wcnt, wbase, okeys, okeys_alt, ovals, ovals_alt;
@@ -749,13 +749,16 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     if (!ensure(ctx, ctx->grid, grid_bytes))
         return VOX_ERR_MEMORY;
     uint8_t* grid = (uint8_t*)ctx->grid.p;
-    cudaMemsetAsync(grid, 0, grid_bytes, s);
-    cudaMemsetAsync(N.leaf_mask, 0, 64 * (size_t)L, s);
-    if (!ensure(ctx, ctx->vpairs, 8 * (size_t)(V + 1)) || !ensure(ctx, ctx->pair_off, 8 * (size_t)(V + 1)) ||
-        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(V + 1) * 2))
-        return VOX_ERR_MEMORY;
-    scan_status = (uint64_t*)ctx->scan_status.p;
-    scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    launch_zero_gaps(N, grid, grid_bytes, s);
+    launch_leaf_masks(N, LP.cand_mask, (const uint32_t*)ctx->vslot.p, s);
+    uint64_t* cloud_pairs = nullptr;
+    if (B > 1)
+    {
+        if (!ensure(ctx, ctx->cloud_pairs, 8 * (size_t)(B + 1)))
+            return VOX_ERR_MEMORY;
+        cloud_pairs = (uint64_t*)ctx->cloud_pairs.p;
+        cudaMemsetAsync(cloud_pairs, 0, 8 * (size_t)B, s);
+    }
     ValueParams VA;
     VA.V = V;
     VA.vslot = (const uint32_t*)ctx->vslot.p;
@@ -763,15 +766,13 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     VA.s_dens = LP.s_dens;
     VA.s_col = LP.s_col;
     VA.s_pairs = LP.s_pairs;
-    VA.vpairs = (uint64_t*)ctx->vpairs.p;
+    VA.cloud_pairs = cloud_pairs;
     VA.cand_vbase = (uint64_t*)ctx->cand_vbase.p;
     VA.vox_leaf = (const uint32_t*)ctx->vox_leaf.p;
     VA.vox_n = (const uint16_t*)ctx->vox_n.p;
     VA.out = grid;
     launch_values(VA, N, s);
-    scan_exclusive_u64(VA.vpairs, (uint64_t*)ctx->pair_off.p, V, 0, sc + SC_SCRATCH + 3, scan_status,
-                       ctx->scan_epochs.next(scan_status, scan_words, s), d_counter, d_err, ctx->num_sms, s);
-    N.C.pair_off = (const uint64_t*)ctx->pair_off.p;
+    N.C.cloud_pairs = cloud_pairs;
     N.C.P = P_pairs;
     cudaEventRecord(ctx->timers.ev[5], s);
     launch_leaf_bbox(N, s);
@@ -812,7 +813,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     ctx->last_voxel_size = voxel_size;
     ctx->last_cloud_vs = d_cloud_vs;
     ctx->last_N = N;
-    LP.pair_off = N.C.pair_off;
+    LP.pair_off = nullptr; // built on demand by vox_copy_pairs
     ctx->last_LP = LP;
     ctx->last_NLC = NLC;
     ctx->last_Q = Q;
@@ -981,7 +982,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_off,
                       &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
-                      &ctx->cand_voff, &ctx->vkeys, &ctx->vslot, &ctx->vpairs, &ctx->pair_off, &ctx->cand_vbase,
+                      &ctx->cand_voff, &ctx->vkeys, &ctx->vslot, &ctx->vpairs, &ctx->pair_off, &ctx->cand_vbase, &ctx->cloud_pairs,
                       &ctx->partials, &ctx->exp_keys, &ctx->exp_ids, &ctx->nwin, &ctx->win_before,
                       &ctx->cand_wkey, &ctx->wkey_u, &ctx->wkey_lo, &ctx->wkey_leaf, &ctx->wcnt, &ctx->wbase,
                       &ctx->okeys, &ctx->okeys_alt, &ctx->ovals, &ctx->ovals_alt, &ctx->rank_u, &ctx->rank_lo,
@@ -1150,8 +1151,22 @@ int vox_copy_pairs(vox_context_t* ctx, uint64_t* keys, uint32_t* ids, int64_t ca
     const size_t kb = ctx->key64 ? 8 : 4;
     if (!ensure(ctx, ctx->exp_keys, kb * (size_t)P) || !ensure(ctx, ctx->exp_ids, 4 * (size_t)P))
         return VOX_ERR_MEMORY;
+    // pairs before each voxel: the staged per-voxel counts in run order, scanned
+    const int64_t V = ctx->last_V;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    if (!ensure(ctx, ctx->vpairs, 8 * (size_t)(V + 1)) || !ensure(ctx, ctx->pair_off, 8 * (size_t)(V + 1)) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(V + 1) * 2))
+        return VOX_ERR_MEMORY;
+    uint64_t* scan_status = (uint64_t*)ctx->scan_status.p;
+    const size_t scan_words = ctx->scan_status.cap / sizeof(uint64_t);
+    launch_voxel_pairs(V, (const uint32_t*)ctx->vslot.p, (const uint32_t*)ctx->s_pairs.p, (uint64_t*)ctx->vpairs.p,
+                       ctx->stream);
+    scan_exclusive_u64((const uint64_t*)ctx->vpairs.p, (uint64_t*)ctx->pair_off.p, V, 0, sc + SC_SCRATCH + 3,
+                       scan_status, ctx->scan_epochs.next(scan_status, scan_words, ctx->stream),
+                       (uint32_t*)(sc + SC_SCRATCH), (int*)(sc + SC_ERR), ctx->num_sms, ctx->stream);
     // replay the leaf walk, writing every passing pair at its voxel's pair offset
     LeafPassParams LP = ctx->last_LP;
+    LP.pair_off = (const uint64_t*)ctx->pair_off.p;
     LP.out_keys = ctx->exp_keys.p;
     LP.out_ids = (uint32_t*)ctx->exp_ids.p;
     launch_leaf_export(LP, (uint32_t*)((uint64_t*)ctx->scal.p + SC_SCRATCH), ctx->num_sms, ctx->stream);

@@ -959,28 +959,32 @@ __global__ void k_leaf_popc(const uint64_t* cand_mask, int64_t NCL, uint64_t* co
     counts[c] = n;
 }
 
-// one thread per (candidate leaf, mask word)
+// one warp per candidate leaf, 32 voxels per round: each active voxel's rank is
+// the popcount of the mask bits below it, so the writes are contiguous
 template <class K>
 __global__ void k_voxel_keys(const uint64_t* cand_mask, const uint32_t* cand_key, const uint64_t* cand_voff,
                              int64_t NCL, K* vkeys, uint32_t* vslot)
 {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= NCL * 8)
+    const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= NCL)
         return;
-    const int64_t c = t >> 3;
-    const int w = (int)(t & 7);
+    const uint32_t* m32 = reinterpret_cast<const uint32_t*>(cand_mask + 8 * c);
+    const uint32_t mine = m32[lane & 15];
     uint64_t base = cand_voff[c];
-    for (int q = 0; q < w; q++)
-        base += (uint64_t)__popcll(cand_mask[8 * c + q]);
-    uint64_t m = cand_mask[8 * c + w];
     const uint64_t lk = (uint64_t)cand_key[c] << 9;
-    while (m)
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int r = 0; r < 16; r++)
     {
-        const uint32_t n = (uint32_t)(64 * w + __ffsll((long long)m) - 1);
-        m &= m - 1;
-        vkeys[base] = (K)(lk | n);
-        vslot[base] = (uint32_t)(c * 512 + n);
-        base++;
+        const uint32_t bits = __shfl_sync(0xffffffffu, mine, r);
+        if ((bits >> lane) & 1u)
+        {
+            const uint64_t at = base + (uint64_t)__popc(bits & lt);
+            const uint32_t n = (uint32_t)(32 * r + lane);
+            vkeys[at] = (K)(lk | n);
+            vslot[at] = (uint32_t)(c * 512 + n);
+        }
+        base += (uint64_t)__popc(bits);
     }
 }
 
@@ -1001,10 +1005,42 @@ __global__ void k_values(ValueParams A, NodeParams N)
     col[3 * vi + 0] = A.s_col[3 * (uint64_t)slot + 0];
     col[3 * vi + 1] = A.s_col[3 * (uint64_t)slot + 1];
     col[3 * vi + 2] = A.s_col[3 * (uint64_t)slot + 2];
-    A.vpairs[v] = A.s_pairs[slot];
     if ((uint64_t)v == N.leaf_vstart[l])
         A.cand_vbase[slot >> 9] = N.C.value_base[b] + N.leaf_vidx[l];
-    atomicOr((unsigned long long*)&N.leaf_mask[8 * (uint64_t)l + (n >> 6)], 1ull << (n & 63));
+    (void)n;
+    if (A.cloud_pairs)
+    {
+        // pairs per cloud: a warp whose voxels share a cloud adds once
+        uint64_t pc = A.s_pairs[slot];
+        const uint32_t peers = __match_any_sync(__activemask(), b);
+        for (int off = 16; off; off >>= 1)
+        {
+            const uint64_t o = __shfl_down_sync(__activemask(), pc, off);
+            pc += ((threadIdx.x & 31) + off < 32 && ((peers >> ((threadIdx.x & 31) + off)) & 1u)) ? o : 0ull;
+        }
+        if ((threadIdx.x & 31) == __ffs(peers) - 1)
+            atomicAdd((unsigned long long*)&A.cloud_pairs[b], (unsigned long long)pc);
+    }
+}
+
+// every leaf's value mask is its candidate leaf's mask
+__global__ void k_leaf_masks(int64_t L, const uint32_t* leaf_vstart, const uint32_t* vslot, const uint64_t* cand_mask,
+                             uint64_t* leaf_mask)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L * 8)
+        return;
+    const int64_t l = t >> 3;
+    const uint32_t c = vslot[leaf_vstart[l]] >> 9;
+    leaf_mask[t] = cand_mask[8 * (uint64_t)c + (t & 7)];
+}
+
+// pairs per voxel (run order) from the staged counts
+__global__ void k_voxel_pairs(int64_t V, const uint32_t* vslot, const uint32_t* s_pairs, uint64_t* vpairs)
+{
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < V)
+        vpairs[v] = s_pairs[vslot[v]];
 }
 
 // ---------------------------------------------------------------- launch ----
@@ -1102,7 +1138,7 @@ void launch_voxel_keys(const uint64_t* cand_mask, const uint32_t* cand_key, cons
 {
     if (NCL <= 0)
         return;
-    const unsigned blocks = (unsigned)((NCL * 8 + 255) / 256);
+    const unsigned blocks = (unsigned)((NCL * 32 + 255) / 256);
     if (key64)
         { k_voxel_keys<uint64_t><<<blocks, 256, 0, s>>>(cand_mask, cand_key, cand_voff, NCL, (uint64_t*)vkeys, vslot); count_launch(); }
     else
@@ -1114,6 +1150,20 @@ void launch_values(const ValueParams& A, const NodeParams& N, cudaStream_t s)
     if (A.V <= 0)
         return;
     { k_values<<<(unsigned)((A.V + 255) / 256), 256, 0, s>>>(A, N); count_launch(); }
+}
+
+void launch_leaf_masks(const NodeParams& N, const uint64_t* cand_mask, const uint32_t* vslot, cudaStream_t s)
+{
+    if (N.L <= 0)
+        return;
+    { k_leaf_masks<<<(unsigned)((N.L * 8 + 255) / 256), 256, 0, s>>>(N.L, N.leaf_vstart, vslot, cand_mask, N.leaf_mask); count_launch(); }
+}
+
+void launch_voxel_pairs(int64_t V, const uint32_t* vslot, const uint32_t* s_pairs, uint64_t* vpairs, cudaStream_t s)
+{
+    if (V <= 0)
+        return;
+    { k_voxel_pairs<<<(unsigned)((V + 255) / 256), 256, 0, s>>>(V, vslot, s_pairs, vpairs); count_launch(); }
 }
 
 } // namespace vox

@@ -458,11 +458,7 @@ __global__ void k_write_headers(NodeParams N, uint8_t* out)
     if (vc > 2)
         for (int a = 0; a < 6; a++)
             h.bbox[a] = C.bbox[6 * b + a];
-    const uint64_t* poff = C.pair_off ? C.pair_off : (const uint64_t*)nullptr;
-    const uint64_t p0 = C.vstart[b] < (uint64_t)C.V ? (poff ? poff[C.vstart[b]] : N.vox_start[C.vstart[b]]) : (uint64_t)C.P;
-    const uint64_t p1 =
-        C.vstart[b + 1] < (uint64_t)C.V ? (poff ? poff[C.vstart[b + 1]] : N.vox_start[C.vstart[b + 1]]) : (uint64_t)C.P;
-    h.pair_count = p1 - p0;
+    h.pair_count = C.cloud_pairs ? C.cloud_pairs[b] : (uint64_t)C.P;
     const int64_t g0 = C.cloud_start ? C.cloud_start[b] : 0, g1 = C.cloud_start ? C.cloud_start[b + 1] : C.G;
     const uint64_t f0 = g0 < C.G ? C.frag_off[g0] : *C.F_total, f1 = g1 < C.G ? C.frag_off[g1] : *C.F_total;
     h.candidate_count = f1 - f0;
@@ -828,6 +824,48 @@ void launch_cloud_layout(const NodeParams& N, cudaStream_t s)
         { k_cloud_starts<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(N); count_launch(); }
     { k_cloud_layout<<<1, 1024, 0, s>>>(N); count_launch(); }
 }
+// Zero every byte of each cloud's grid that the node / value writers leave
+// alone: header, node2 region, bbox, the two background values of each value
+// array and the alignment gaps (the values 2 .. vc - 1 are all written).
+__device__ __forceinline__ void zero_range(uint8_t* out, uint64_t a, uint64_t b, uint64_t i, uint64_t n)
+{
+    // a, b multiples of 4
+    const uint64_t a16 = (a + 15) & ~15ull, b16 = b & ~15ull;
+    if (a16 >= b16)
+    {
+        for (uint64_t o = a + 4 * i; o < b; o += 4 * n)
+            *reinterpret_cast<uint32_t*>(out + o) = 0u;
+        return;
+    }
+    for (uint64_t o = a + 4 * i; o < a16; o += 4 * n)
+        *reinterpret_cast<uint32_t*>(out + o) = 0u;
+    for (uint64_t o = a16 + 16 * i; o < b16; o += 16 * n)
+        *reinterpret_cast<uint4*>(out + o) = make_uint4(0u, 0u, 0u, 0u);
+    for (uint64_t o = b16 + 4 * i; o < b; o += 4 * n)
+        *reinterpret_cast<uint32_t*>(out + o) = 0u;
+}
+
+__global__ void k_zero_gaps(NodeParams N, uint8_t* out)
+{
+    const CloudParams& C = N.C;
+    const int64_t b = blockIdx.y;
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, n = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t vc = 2 + (C.vstart[b + 1] - C.vstart[b]);
+    zero_range(out, C.grid_off[b], C.rgba_off[b] + 8, i, n);
+    zero_range(out, C.rgba_off[b] + 4 * vc, C.dens_off[b] + 8, i, n);
+    zero_range(out, C.dens_off[b] + 4 * vc, C.col_off[b] + 24, i, n);
+    zero_range(out, C.col_off[b] + 12 * vc, C.grid_off[b + 1], i, n);
+}
+
+void launch_zero_gaps(const NodeParams& N, uint8_t* out, uint64_t grid_bytes, cudaStream_t s)
+{
+    if (N.C.B <= 0)
+        return;
+    uint64_t bx = grid_bytes / (uint64_t)N.C.B / (1ull << 19);
+    bx = bx < 1 ? 1 : (bx > 1024 ? 1024 : bx);
+    { k_zero_gaps<<<dim3((unsigned)bx, (unsigned)N.C.B), 256, 0, s>>>(N, out); count_launch(); }
+}
+
 void launch_write_headers(const NodeParams& N, uint8_t* out, cudaStream_t s)
 {
     { k_write_headers<<<(unsigned)((N.C.B + 127) / 128), 128, 0, s>>>(N, out); count_launch(); }

@@ -53,7 +53,7 @@ struct CloudParams
     const int64_t* cloud_start;  // [B + 1] Gaussian ranges (device) or null for one cloud
     const uint64_t* frag_off;    // exclusive scan of footprints (candidates per cloud)
     const uint64_t* F_total;
-    const uint64_t* pair_off;    // [V] pairs before each voxel (exclusive scan)
+    const uint64_t* cloud_pairs; // [B] passing pairs per cloud (null: one cloud, P)
     int64_t G, P, V;
     uint32_t node_order;
 };
@@ -186,13 +186,16 @@ struct ValueParams
     const float* s_dens;
     const float* s_col;
     const uint32_t* s_pairs;
-    uint64_t* vpairs;          // [V] pairs per voxel
+    uint64_t* cloud_pairs;     // [B] passing pairs per cloud, summed here (null: one cloud)
     uint64_t* cand_vbase;      // [NCL]
     const uint32_t* vox_leaf;
     const uint16_t* vox_n;
     uint8_t* out;
 };
 void launch_values(const ValueParams& A, const NodeParams& N, cudaStream_t s);
+void launch_leaf_masks(const NodeParams& N, const uint64_t* cand_mask, const uint32_t* vslot, cudaStream_t s);
+void launch_voxel_pairs(int64_t V, const uint32_t* vslot, const uint32_t* s_pairs, uint64_t* vpairs, cudaStream_t s);
+void launch_zero_gaps(const NodeParams& N, uint8_t* out, uint64_t grid_bytes, cudaStream_t s);
 
 // the reference's fragment batches and windows (raster/Raster.cpp:443-444)
 constexpr int64_t REF_PRIM_BATCH = 262144; // Gaussians per batch (2^18)
