@@ -228,8 +228,10 @@ PNANOVDB_API pnanovdb_compute_t* pnanovdb_get_compute(void);
  * grid_build_blindmetadata.slang appends follow: the bbox (two int32x3,
  * inclusive voxel coordinates) and per-value arrays indexed by value index
  * (two background slots first): RGBA8 as the reference computes it, float
- * density = sum of per-pair alpha in (voxel key, Gaussian id) order, and
- * Vec3f colour = alpha-weighted mean RGB. */
+ * density = sum of per-pair alpha (an exact 64-bit fixed-point sum of the
+ * terms rounded to 2^-32, rounded once to float, so independent of order),
+ * and Vec3f colour = alpha-weighted mean RGB.  density_offset = color_offset
+ * = 0 marks a grid copied without the float channels. */
 #define VOX_GRID_MAGIC 0x32454E58564F5642ull /* "BVOXNE2" */
 #define VOX_GRID_HEADER_BYTES 256u
 
@@ -343,6 +345,14 @@ PNANOVDB_API int vox_voxelize_batch(vox_context_t* ctx, const vox_gaussians_t* g
 /* Copies the grid of the last vox_voxelize / vox_voxelize_host call to host
  * or device memory (`capacity` bytes). */
 PNANOVDB_API int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity);
+
+/* The part of the last single-cloud grid that the reference's raster entries
+ * return (raster/Raster.cpp:636-668: node2 tree and RGBA8 values): header,
+ * node2 region, bbox and RGBA8 array, copied to host or device memory; the
+ * copied header has grid_bytes = *bytes and density_offset = color_offset = 0
+ * (the float channels stay in the context's grid, vox_copy_grid).  With
+ * out = NULL only *bytes is set.  The drop-in raster entries return this. */
+PNANOVDB_API int vox_copy_grid_rgba8(vox_context_t* ctx, void* out, uint64_t capacity, uint64_t* bytes);
 
 /* Sorted (voxel, Gaussian) pairs of the last vox_voxelize call: hierarchical
  * 64-bit keys (root_n << 36 | upper_n << 21 | lower_n << 9 | leaf_n) and

@@ -1111,6 +1111,37 @@ int vox_copy_grid(vox_context_t* ctx, void* out, uint64_t capacity)
     return VOX_OK;
 }
 
+int vox_copy_grid_rgba8(vox_context_t* ctx, void* out, uint64_t capacity, uint64_t* bytes)
+{
+    if (!ctx || !bytes)
+        return VOX_ERR_ARGS;
+    if (ctx->last_V < 0 || ctx->h_grid_off.size() != 2)
+    {
+        set_error(ctx, "vox_copy_grid_rgba8: no single-cloud grid");
+        return VOX_ERR_ARGS;
+    }
+    cudaSetDevice(ctx->device);
+    vox_grid_header_t h;
+    cudaMemcpyAsync(&h, ctx->grid.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return check_cuda(ctx, "vox_copy_grid_rgba8");
+    const uint64_t n = h.rgba8_offset + 4 * h.value_count;
+    *bytes = n;
+    if (!out)
+        return VOX_OK;
+    if (capacity < n)
+        return VOX_ERR_SIZE;
+    h.grid_bytes = n;
+    h.density_offset = 0;
+    h.color_offset = 0;
+    cudaMemcpyAsync(out, &h, sizeof(h), cudaMemcpyDefault, ctx->stream);
+    cudaMemcpyAsync((uint8_t*)out + sizeof(h), (const uint8_t*)ctx->grid.p + sizeof(h), n - sizeof(h), cudaMemcpyDefault,
+                    ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return check_cuda(ctx, "vox_copy_grid_rgba8");
+    return VOX_OK;
+}
+
 int vox_voxel_coords(vox_context_t* ctx, int32_t* d_ijk, int64_t capacity)
 {
     if (!ctx || (!d_ijk && capacity > 0))

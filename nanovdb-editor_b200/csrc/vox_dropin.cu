@@ -441,10 +441,13 @@ static pnanovdb_compute_array_t* run_host(int device, const vox_gaussians_t* g, 
     uint64_t bytes = 0;
     if (vox_voxelize_host(v, g, voxel_size, cull, flags, nullptr, 0, &bytes) != VOX_OK)
         return nullptr;
+    // what the reference returns: node2 tree and RGBA8 values
+    if (vox_copy_grid_rgba8(v, nullptr, 0, &bytes) != VOX_OK)
+        return nullptr;
     pnanovdb_compute_array_t* a = array_create_pinned(4, (bytes + 3) / 4);
     if (!a)
         return nullptr;
-    if (vox_copy_grid(v, a->data, bytes) != VOX_OK)
+    if (vox_copy_grid_rgba8(v, a->data, 4 * a->element_count, &bytes) != VOX_OK)
     {
         array_destroy(a);
         return nullptr;

@@ -76,12 +76,16 @@ class NodeGrid:
         return self._slice(self.header["rgba8_offset"], self.value_count, np.uint32)
 
     @property
-    def density(self) -> np.ndarray:
-        return self._slice(self.header["density_offset"], self.value_count, np.float32)
+    def density(self) -> np.ndarray | None:
+        """Float density per value index; None for a grid copied without the float channels."""
+        off = self.header["density_offset"]
+        return self._slice(off, self.value_count, np.float32) if off else None
 
     @property
-    def color(self) -> np.ndarray:
-        return self._slice(self.header["color_offset"], 3 * self.value_count, np.float32).reshape(-1, 3)
+    def color(self) -> np.ndarray | None:
+        """Vec3f colour per value index; None for a grid copied without the float channels."""
+        off = self.header["color_offset"]
+        return self._slice(off, 3 * self.value_count, np.float32).reshape(-1, 3) if off else None
 
     @property
     def bbox(self) -> np.ndarray:
