@@ -282,7 +282,7 @@ struct LeafAcc
 struct LeafQSmem
 {
     LeafChunk ch[3];
-    LeafAcc acc[2];
+    LeafAcc acc[1];
     uint16_t queue[2][LQ_CHUNK * 512];
     uint32_t qn[3];
     int32_t nxt_o[2][3]; // the next chunk (by phase parity): leaf origin and sorted pair range
@@ -344,7 +344,7 @@ __device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChun
 }
 
 template <bool CHECK, bool WINDOW>
-__global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, uint32_t* counter)
+__global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, uint32_t* counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LeafQSmem& S = *reinterpret_cast<LeafQSmem*>(smem_raw);
@@ -357,10 +357,10 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
         S.cand_next[0] = atomicAdd(counter, 1u);
         S.pairs = 0;
         S.qn[0] = S.qn[1] = S.qn[2] = 0;
-        S.acc[0].wmin = S.acc[1].wmin = ~0ull;
+        S.acc[0].wmin = ~0ull;
     }
 #pragma unroll
-    for (int b = 0; b < 2; b++)
+    for (int b = 0; b < 1; b++)
 #pragma unroll
         for (int h = 0; h < 2; h++)
         {
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
         // ---- flush of the leaf whose last alpha ran in the previous phase
         if (f_valid)
         {
-            LeafAcc& A = S.acc[fpar];
+            LeafAcc& A = S.acc[0];
             uint32_t cnt[2];
 #pragma unroll
             for (int h = 0; h < 2; h++)
@@ -460,12 +460,13 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_pass(LeafPassParams P, u
                 P.cand_wkey[fc] = A.wmin;
                 A.wmin = ~0ull;
             }
+            __syncthreads(); // the next leaf's alpha reuses the accumulators
         }
         // ---- alpha of the previous chunk, one queued pair per thread
         if (a_valid)
         {
             const LeafChunk& C = S.ch[ab];
-            LeafAcc& A = S.acc[apar];
+            LeafAcc& A = S.acc[0];
             const uint16_t* queue = S.queue[(i + 1u) & 1u];
             const uint32_t qn = S.qn[ab];
             for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
