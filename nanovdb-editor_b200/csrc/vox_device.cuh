@@ -279,11 +279,14 @@ __device__ __forceinline__ void axis_corners(float vs, float pos, int32_t i, flo
     c1 = VOX_FSUB(VOX_FMUL(v1, vs), pos);
 }
 
+// The minimum / maximum of the two corner products.  fminf / fmaxf differ from
+// the compare-and-select form only in the sign of a zero on a tie, and every
+// consumer squares these bounds or compares them with zero.
 __device__ __forceinline__ void minmax_prod(float c0, float c1, float r, float& mn, float& mx)
 {
-    float p0 = VOX_FMUL(c0, r), p1 = VOX_FMUL(c1, r);
-    mn = p0 < p1 ? p0 : p1;
-    mx = p0 < p1 ? p1 : p0;
+    const float p0 = VOX_FMUL(c0, r), p1 = VOX_FMUL(c1, r);
+    mn = fminf(p0, p1);
+    mx = fmaxf(p0, p1);
 }
 
 __device__ __forceinline__ Aabb voxel_local_aabb(const GaussRec& R, const RInv& M, float vs, int32_t i, int32_t j,
@@ -344,11 +347,7 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
         const float p2 = VOX_FADD(VOX_FMUL(LAT_W2, b.hi[a]), VOX_FMUL(LAT_OW2, b.lo[a]));
         const float s0 = VOX_FMUL(b.lo[a], b.lo[a]), s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2),
                     s3 = VOX_FMUL(b.hi[a], b.hi[a]);
-        float best = s0;
-        best = s1 < best ? s1 : best;
-        best = s2 < best ? s2 : best;
-        best = s3 < best ? s3 : best;
-        m[a] = best;
+        m[a] = fminf(fminf(s0, s1), fminf(s2, s3)); // squares: no NaN, no signed zero
     }
     float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
     float a = VOX_FMUL(R.q6.x, vox_expf_cr(-VOX_FMUL(R.q6.y, d)));
@@ -407,12 +406,9 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
     {
         const float dd = VOX_FSUB(b.hi[a], b.lo[a]);
         const float p1 = VOX_FFMA(dd, 0x1.555556p-2f, b.lo[a]), p2 = VOX_FFMA(dd, 0x1.555556p-1f, b.lo[a]);
-        float best = VOX_FMUL(b.lo[a], b.lo[a]);
-        const float s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2), s3 = VOX_FMUL(b.hi[a], b.hi[a]);
-        best = s1 < best ? s1 : best;
-        best = s2 < best ? s2 : best;
-        best = s3 < best ? s3 : best;
-        m[a] = best;
+        const float s0 = VOX_FMUL(b.lo[a], b.lo[a]), s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2),
+                    s3 = VOX_FMUL(b.hi[a], b.hi[a]);
+        m[a] = fminf(fminf(s0, s1), fminf(s2, s3)); // squares: no NaN, no signed zero
     }
     const float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
     float a = VOX_FMUL(R.q6.x, vox_expf(-VOX_FMUL(R.q6.y, d)));
@@ -465,6 +461,11 @@ __device__ __forceinline__ unsigned long long fx_of(float x)
 {
     x = x < FX_CLAMP ? x : FX_CLAMP;
     x = x > -FX_CLAMP ? x : -FX_CLAMP;
+    return (unsigned long long)__float2ll_rn(VOX_FMUL(x, FX_SCALE));
+}
+// the same for a term known to lie in [0, 1] (an alpha or a smooth kernel value)
+__device__ __forceinline__ unsigned long long fx_of_unit(float x)
+{
     return (unsigned long long)__float2ll_rn(VOX_FMUL(x, FX_SCALE));
 }
 __device__ __forceinline__ float fx_to_float(unsigned long long s)

@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                 }
                 atomicAdd(&A.cnt[n], 1u);
                 atomicMax(&A.rgba[n], (rgba8_byte(a8) << 24) | C.rgb24[j]);
-                atomicAdd(&A.dens[n], fx_of(a));
+                atomicAdd(&A.dens[n], fx_of_unit(a));
                 atomicAdd(&A.col[0][n], fx_of(VOX_FMUL(a, R.q7.x)));
                 atomicAdd(&A.col[1][n], fx_of(VOX_FMUL(a, R.q7.y)));
                 atomicAdd(&A.col[2][n], fx_of(VOX_FMUL(a, R.q7.z)));
@@ -560,7 +560,15 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                         shi[r] = VOX_FADD(xx, yx);
                         pa[r] = VOX_FMUL(cz, M.m[r][2]);
                     }
+                    // the corner offsets grow with z, so per row the smaller product is the
+                    // lower corner's when the matrix entry is >= 0 (fl(c m) is monotone in c;
+                    // a tie differs at most in the sign of a zero, which the test squares)
+                    bool up[3];
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                        up[r] = M.m[r][2] >= 0.f;
                     const uint32_t nz = C.bnz[j];
+#pragma unroll 2
                     for (uint32_t k = 0; k < nz; k++)
                     {
                         v = VOX_FADD(v, 1.f);
@@ -570,10 +578,11 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                         for (int r = 0; r < 3; r++)
                         {
                             const float pb = VOX_FMUL(cz, M.m[r][2]);
-                            const float zn = pa[r] < pb ? pa[r] : pb, zx = pa[r] < pb ? pb : pa[r];
+                            const float zn = up[r] ? pa[r] : pb, zx = up[r] ? pb : pa[r];
                             pa[r] = pb;
                             const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
-                            const float xs = 0.f < xl ? xl : (0.f > xh ? xh : 0.f);
+                            // xl <= xh: the bound of the row's interval nearest to zero, or zero
+                            const float xs = VOX_FADD(fmaxf(xl, 0.f), fminf(xh, 0.f));
                             const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
                             d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
                         }
