@@ -329,6 +329,7 @@ def main():
 
     from ctypes import POINTER, byref, c_float, c_uint32, pointer
 
+    from nanovdb_editor import replicas as R
     from nanovdb_editor import workloads as W
     from nanovdb_editor.compute import Compute, pnanovdb_ComputeArray
     from nanovdb_editor.raster import Raster
@@ -370,12 +371,8 @@ def main():
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    ms = sum(times) / len(times)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * G / (ms * 1e-3)
+    ms = R.max_over_ranks(sum(times) / len(times), dist, device="cuda")
+    value = R.job_rate(world * G, ms)
 
     # ---- e2e through the reference-facing C ABI with host buffers
     e2e = None
@@ -404,12 +401,8 @@ def main():
             e2e_times.append(time.perf_counter() - t0)
             d2h = int(out.element_size * out.element_count)
             comp.destroy_array(out)
-        e2e_s = sum(e2e_times) / len(e2e_times)
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e_value = world * G / e2e_s
+        e2e_s = R.max_over_ranks(sum(e2e_times) / len(e2e_times), dist, device="cuda")
+        e2e_value = R.job_rate(world * G, e2e_s * 1e3)
         e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3}
 
     # ---- roofline of the dominant stage
