@@ -292,6 +292,148 @@ struct LeafQSmem
     unsigned long long pairs;
 };
 
+// The reference test on the boxes of a chunk, one box column per thread, its
+// passing (Gaussian, voxel) pairs appended to queue (entry j << 9 | leaf_n).
+// Bit-identical to voxel_local_aabb + aabb_hits_unit_sphere per voxel: the z
+// corner c1 of voxel z is c0 of voxel z + 1 (integer-valued floats), and "lo >
+// 0: subtract lo^2, else hi < 0: subtract hi^2" selects the pre-scale bound
+// with the same sign (inv_ls, inv_s > 0; an underflow to zero subtracts zero).
+// Every thread of the CTA calls it (warp-synchronous queue slots).  PER_WARP:
+// warp w appends to its own region queue[w * 512, ...) at warp-local
+// positions and stores its count in qcount[w] - a deterministic order (a warp
+// tests at most 2 x 32 columns of 8 voxels).  Otherwise one shared queue, a
+// shared atomic per warp and round.
+template <bool CHECK, bool PER_WARP = false, class Chunk>
+__device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const Chunk& C, uint32_t cnt,
+                                                const int32_t o[3], uint16_t* queue, uint32_t* qcount, int t, int lane)
+{
+    uint32_t wbase = 0; // PER_WARP: entries this warp has written
+    if (PER_WARP)
+        queue += (t >> 5) * (LQ_CHUNK * 64);
+    uint32_t start[LQ_CHUNK + 1];
+    start[0] = 0;
+#pragma unroll
+    for (int j = 0; j < LQ_CHUNK; j++)
+        start[j + 1] = start[j] + (j < (int)cnt ? C.bcol[j] : 0u);
+    const uint32_t T = start[LQ_CHUNK];
+    for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
+    {
+        const uint32_t e = b0 + (uint32_t)t;
+        uint32_t zmask = 0, ebase = 0;
+        if (e < T)
+        {
+            int j = 0;
+            uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
+#pragma unroll
+            for (int q = 1; q < LQ_CHUNK; q++)
+            {
+                const bool ge = e >= start[q];
+                j += ge ? 1 : 0;
+                sj = ge ? start[q] : sj;
+            }
+            const uint32_t local = e - sj;
+            const uint32_t dx = (local * C.bdiv_y[j]) >> 16;
+            const uint32_t dy = local - dx * C.bny[j];
+            const int32_t rx = C.bx0[j] + (int32_t)dx, ry = C.by0[j] + (int32_t)dy, rz0 = C.bz0[j];
+            const GaussRec& R = C.rec[j];
+            const RInv M = rinv_of(R);
+            const float vsf = C.vs[j], il = R.q0.w, pz = R.q0.z;
+            const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+            float cx0, cx1, cy0, cy1;
+            axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
+            axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
+            float slo[3], shi[3], pa[3];
+            float v = (float)(o[2] + rz0);
+            float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+            {
+                float xn, xx, yn, yx;
+                minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
+                minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
+                slo[r] = VOX_FADD(xn, yn);
+                shi[r] = VOX_FADD(xx, yx);
+                pa[r] = VOX_FMUL(cz, M.m[r][2]);
+            }
+            // the corner offsets grow with z, so per row the smaller product is the
+            // lower corner's when the matrix entry is >= 0 (fl(c m) is monotone in c;
+            // a tie differs at most in the sign of a zero, which the test squares)
+            bool up[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                up[r] = M.m[r][2] >= 0.f;
+            const uint32_t nz = C.bnz[j];
+#pragma unroll 2
+            for (uint32_t k = 0; k < nz; k++)
+            {
+                v = VOX_FADD(v, 1.f);
+                cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                float d2 = 1.f;
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                {
+                    const float pb = VOX_FMUL(cz, M.m[r][2]);
+                    const float zn = up[r] ? pa[r] : pb, zx = up[r] ? pb : pa[r];
+                    pa[r] = pb;
+                    const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
+                    // xl <= xh: the bound of the row's interval nearest to zero, or zero
+                    const float xs = VOX_FADD(fmaxf(xl, 0.f), fminf(xh, 0.f));
+                    const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
+                    d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
+                }
+                zmask |= (d2 > 0.f ? 1u : 0u) << k;
+            }
+            ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
+            if (CHECK && zmask && C.flag[j])
+                atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
+        }
+        // queue slots: warp inclusive scan of the pass counts, one shared atomic per warp
+        const uint32_t np = (uint32_t)__popc(zmask);
+        uint32_t incl = np;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off)
+                incl += y;
+        }
+        uint32_t qb = 0;
+        if (PER_WARP)
+        {
+            qb = wbase + incl - np;
+            wbase += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        else
+        {
+            if (lane == 31 && incl)
+                qb = atomicAdd(qcount, incl);
+            qb = __shfl_sync(0xffffffffu, qb, 31) + incl - np;
+        }
+        for (uint32_t m = zmask; m; m &= m - 1)
+            queue[qb++] = (uint16_t)(ebase + (uint32_t)(__ffs(m) - 1));
+    }
+    if (PER_WARP && lane == 0)
+        qcount[t >> 5] = wbase;
+}
+
+// the part of a Gaussian's bbox inside the leaf at o
+template <class Chunk>
+__device__ __forceinline__ void leaf_box_fields(Chunk& C, int j, const GaussRec& R, const int32_t o[3])
+{
+    const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
+    const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
+    const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
+    const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
+    const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
+    C.bx0[j] = x0;
+    C.by0[j] = y0;
+    C.bz0[j] = z0;
+    C.bny[j] = ny;
+    C.bnz[j] = nz;
+    C.bdiv_y[j] = (65536u + ny - 1u) / ny;
+    C.bcol[j] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
+}
+
 __device__ __forceinline__ void cp_async16(void* dst, const void* src)
 {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
@@ -320,18 +462,7 @@ __device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChun
                                                const int32_t o[3])
 {
     const GaussRec& R = C.rec[j];
-    const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
-    const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
-    const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
-    const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
-    const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
-    C.bx0[j] = x0;
-    C.by0[j] = y0;
-    C.bz0[j] = z0;
-    C.bny[j] = ny;
-    C.bnz[j] = nz;
-    C.bdiv_y[j] = (65536u + ny - 1u) / ny;
-    C.bcol[j] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
+    leaf_box_fields(C, j, R, o);
     C.rgb24[j] = rgba8_byte(R.q7.x) | (rgba8_byte(R.q7.y) << 8) | (rgba8_byte(R.q7.z) << 16);
     C.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
     C.flag[j] = CHECK ? P.emit_flag[P.vals[q]] : 0;
@@ -504,112 +635,10 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                 }
             }
         }
-        // ---- test of this chunk, one box column per thread.  Bit-identical to
-        // voxel_local_aabb + aabb_hits_unit_sphere per voxel: the z corner c1
-        // of voxel z is c0 of voxel z + 1 (integer-valued floats), and "lo > 0:
-        // subtract lo^2, else hi < 0: subtract hi^2" selects the pre-scale sum
-        // with the same sign (inv_ls, inv_s > 0; an underflow to zero
-        // subtracts zero).
+        // ---- test of this chunk
         if (t_valid)
-        {
-            const LeafChunk& C = S.ch[tb];
-            uint16_t* queue = S.queue[i & 1u];
-            const uint32_t cnt = min((uint32_t)LQ_CHUNK, tp1 - tq0);
-            uint32_t start[LQ_CHUNK + 1];
-            start[0] = 0;
-#pragma unroll
-            for (int j = 0; j < LQ_CHUNK; j++)
-                start[j + 1] = start[j] + (j < (int)cnt ? C.bcol[j] : 0u);
-            const uint32_t T = start[LQ_CHUNK];
-            for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
-            {
-                const uint32_t e = b0 + (uint32_t)t;
-                uint32_t zmask = 0, ebase = 0;
-                if (e < T)
-                {
-                    int j = 0;
-                    uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
-#pragma unroll
-                    for (int q = 1; q < LQ_CHUNK; q++)
-                    {
-                        const bool ge = e >= start[q];
-                        j += ge ? 1 : 0;
-                        sj = ge ? start[q] : sj;
-                    }
-                    const uint32_t local = e - sj;
-                    const uint32_t dx = (local * C.bdiv_y[j]) >> 16;
-                    const uint32_t dy = local - dx * C.bny[j];
-                    const int32_t rx = C.bx0[j] + (int32_t)dx, ry = C.by0[j] + (int32_t)dy, rz0 = C.bz0[j];
-                    const GaussRec& R = C.rec[j];
-                    const RInv M = rinv_of(R);
-                    const float vsf = C.vs[j], il = R.q0.w, pz = R.q0.z;
-                    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
-                    float cx0, cx1, cy0, cy1;
-                    axis_corners(vsf, R.q0.x, to[0] + rx, cx0, cx1);
-                    axis_corners(vsf, R.q0.y, to[1] + ry, cy0, cy1);
-                    float slo[3], shi[3], pa[3];
-                    float v = (float)(to[2] + rz0);
-                    float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-#pragma unroll
-                    for (int r = 0; r < 3; r++)
-                    {
-                        float xn, xx, yn, yx;
-                        minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
-                        minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
-                        slo[r] = VOX_FADD(xn, yn);
-                        shi[r] = VOX_FADD(xx, yx);
-                        pa[r] = VOX_FMUL(cz, M.m[r][2]);
-                    }
-                    // the corner offsets grow with z, so per row the smaller product is the
-                    // lower corner's when the matrix entry is >= 0 (fl(c m) is monotone in c;
-                    // a tie differs at most in the sign of a zero, which the test squares)
-                    bool up[3];
-#pragma unroll
-                    for (int r = 0; r < 3; r++)
-                        up[r] = M.m[r][2] >= 0.f;
-                    const uint32_t nz = C.bnz[j];
-#pragma unroll 2
-                    for (uint32_t k = 0; k < nz; k++)
-                    {
-                        v = VOX_FADD(v, 1.f);
-                        cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-                        float d2 = 1.f;
-#pragma unroll
-                        for (int r = 0; r < 3; r++)
-                        {
-                            const float pb = VOX_FMUL(cz, M.m[r][2]);
-                            const float zn = up[r] ? pa[r] : pb, zx = up[r] ? pb : pa[r];
-                            pa[r] = pb;
-                            const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
-                            // xl <= xh: the bound of the row's interval nearest to zero, or zero
-                            const float xs = VOX_FADD(fmaxf(xl, 0.f), fminf(xh, 0.f));
-                            const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
-                            d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
-                        }
-                        zmask |= (d2 > 0.f ? 1u : 0u) << k;
-                    }
-                    ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
-                    if (CHECK && zmask && C.flag[j])
-                        atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
-                }
-                // queue slots: warp inclusive scan of the pass counts, one shared atomic per warp
-                const uint32_t np = (uint32_t)__popc(zmask);
-                uint32_t incl = np;
-#pragma unroll
-                for (int off = 1; off < 32; off <<= 1)
-                {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
-                    if (lane >= off)
-                        incl += y;
-                }
-                uint32_t qb = 0;
-                if (lane == 31 && incl)
-                    qb = atomicAdd(&S.qn[tb], incl);
-                qb = __shfl_sync(0xffffffffu, qb, 31) + incl - np;
-                for (uint32_t m = zmask; m; m &= m - 1)
-                    queue[qb++] = (uint16_t)(ebase + (uint32_t)(__ffs(m) - 1));
-            }
-        }
+            leaf_test_chunk<CHECK>(P, S.ch[tb], min((uint32_t)LQ_CHUNK, tp1 - tq0), to, S.queue[i & 1u], &S.qn[tb], t,
+                                   lane);
         // the counter the test of phase i + 1 fills: last read by the alpha of phase i - 1
         if (t == 0)
             S.qn[nb] = 0;
@@ -678,219 +707,269 @@ __device__ __forceinline__ uint32_t mask_rank(const uint64_t* m, uint32_t n)
     return r + __popcll(m[n >> 6] & ((1ull << (n & 63)) - 1ull));
 }
 
-// adjoint: per candidate leaf, per Gaussian, the sum of its pairs' terms over
-// the leaf's voxels, stored by the leaf pair's emission index.  Same chunked,
-// dense candidate layout as the forward walk; the terms of a round are reduced
-// per Gaussian across each warp (its lanes hold consecutive candidates, so a
-// Gaussian's lanes are contiguous) into per-warp shared slots, which are summed
-// in warp order at the end of the chunk: deterministic, no atomics.
+// adjoint: per (leaf, Gaussian) pair, the sum of its voxel pairs' terms,
+// stored by the leaf pair's emission index.  The forward walk's pipeline: phase
+// p flushes the sums of chunk p - 2, runs the adjoint terms of chunk p - 1's
+// queued pairs, tests chunk p's columns (the same test) and stages chunk p + 1.
+// The queue has one region per warp at warp-local positions, so its order is
+// fixed; a pair's terms are summed per Gaussian across each warp (shuffles)
+// into that warp's slots, and the flush adds the warps' slots in warp order:
+// deterministic, no atomics.
+struct LeafBChunk
+{
+    GaussRec rec[LQ_CHUNK]; // first member: 16-byte aligned for cp.async
+    int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK];
+    uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK], bdiv_y[LQ_CHUNK], bcol[LQ_CHUNK];
+    float vs[LQ_CHUNK];
+    uint8_t flag[LQ_CHUNK];
+    uint32_t eidx[LQ_CHUNK]; // emission index of each leaf pair
+    uint64_t mask[8];        // the leaf's value mask
+    uint64_t vbase;          // value index of the leaf's first voxel
+};
+
+struct LeafGradSum
+{
+    float part[LP_THREADS / 32][LQ_CHUNK][BWD_NACC]; // per warp: a fixed set of rounds, summed in order
+    uint32_t eidx[LQ_CHUNK];
+    uint32_t cnt;
+};
+
 struct LeafBSmem
 {
-    GaussRec rec[LQ_CHUNK];
-    uint32_t eidx[LQ_CHUNK];
-    int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK];
-    uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK], bdiv_y[LQ_CHUNK], bdiv_z[LQ_CHUNK], bvol[LQ_CHUNK];
-    float sxy_lo[3][LQ_CHUNK * 64], sxy_hi[3][LQ_CHUNK * 64];
-    float mz[LQ_CHUNK][3], inv_s[LQ_CHUNK][3], inv_ls[LQ_CHUNK], posz[LQ_CHUNK], vs[LQ_CHUNK];
-    float part[LP_THREADS / 32][LQ_CHUNK][BWD_NACC];
-    uint64_t mask[8];
+    LeafBChunk ch[3];
+    LeafGradSum gs[2];
+    uint16_t queue[2][LQ_CHUNK * 512]; // per warp regions of LQ_CHUNK * 64 entries
+    uint32_t wqn[2][LP_THREADS / 32];   // entries per warp region
+    int32_t nxt_o[2][3];
+    uint32_t nxt_q0[2], nxt_p1[2];
+    uint32_t cand_next[2];
     uint32_t cand;
 };
 
-__global__ void __launch_bounds__(LP_THREADS) k_leaf_backward(LeafPassParams P, uint32_t* counter)
+// stager js of the chunk at sorted pair q0 of candidate c (origin o): the leaf's
+// mask word js, and for js < cnt its record's box once the copy has landed
+__device__ __forceinline__ void leaf_bstage(const LeafPassParams& P, LeafBChunk& C, int js, uint32_t cnt, uint32_t q0,
+                                            int64_t c, const int32_t o[3])
+{
+    C.mask[js] = P.cand_mask[8 * (uint64_t)c + js];
+    if (js == 0)
+        C.vbase = P.cand_vbase[c];
+    if (js < (int)cnt)
+    {
+        cp_async_wait_all();
+        leaf_box_fields(C, js, C.rec[js], o);
+        C.vs[js] = rec_vs(C.rec[js], P.voxel_size, P.cloud_vs);
+        C.flag[js] = 0;
+        C.eidx[js] = P.vals[q0 + (uint32_t)js];
+    }
+}
+
+__global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_backward(LeafPassParams P, uint32_t* counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LeafBSmem& S = *reinterpret_cast<LeafBSmem*>(smem_raw);
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    while (true)
+    const int t = threadIdx.x, lane = t & 31;
+    const int js = t - LQ_STAGE_T0;
+    const bool stager = js >= 0 && js < LQ_CHUNK;
+    if (t == 0)
     {
-        if (t == 0)
-            S.cand = atomicAdd(counter, 1u);
-        __syncthreads();
-        const int64_t c = S.cand;
-        if (c >= P.NCL)
-            break;
-        if (t < 8)
-            S.mask[t] = P.cand_mask[8 * (uint64_t)c + t];
-        int32_t o[3];
-        cand_origin(P, P.cand_key[c], o);
-        const uint64_t vbase = P.cand_vbase[c];
-        const uint32_t p0 = P.cand_start[c], p1 = P.cand_start[c + 1];
-        for (uint32_t q0 = p0; q0 < p1; q0 += LQ_CHUNK)
+        S.cand = atomicAdd(counter, 1u);
+        S.cand_next[0] = atomicAdd(counter, 1u);
+    }
+    for (int i = t; i < (LP_THREADS / 32) * LQ_CHUNK * BWD_NACC; i += LP_THREADS)
+    {
+        (&S.gs[0].part[0][0][0])[i] = 0.f;
+        (&S.gs[1].part[0][0][0])[i] = 0.f;
+    }
+    __syncthreads();
+    int64_t tc = S.cand;
+    if (tc >= P.NCL)
+        return;
+    int64_t cn = S.cand_next[0];
+    int32_t to[3];
+    cand_origin(P, P.cand_key[tc], to);
+    uint32_t tq0 = P.cand_start[tc], tp1 = P.cand_start[tc + 1];
+    if (stager)
+    {
+        const uint32_t cnt = min((uint32_t)LQ_CHUNK, tp1 - tq0);
+        if (js < (int)cnt)
+            leaf_stage_issue(P, &S.ch[0].rec[js], tq0 + (uint32_t)js);
+        leaf_bstage(P, S.ch[0], js, cnt, tq0, tc, to);
+    }
+    __syncthreads();
+    bool t_valid = true, a_valid = false, f_valid = false;
+    uint32_t acnt = 0;
+    int32_t ao[3] = { 0, 0, 0 };
+    uint32_t p = 0;
+    while (t_valid || a_valid || f_valid)
+    {
+        const int tb = (int)(p % 3u), ab = (int)((p + 2u) % 3u), nb = (int)((p + 1u) % 3u);
+        const bool t_end = t_valid && tq0 + LQ_CHUNK >= tp1;
+        const int64_t nc = t_end ? cn : tc;
+        const bool n_valid = t_valid && nc < P.NCL;
+        uint32_t nq0 = 0, np1 = 0, ncnt = 0;
+        if (stager && n_valid)
         {
-            const uint32_t cnt = min((uint32_t)LQ_CHUNK, p1 - q0);
-            if (t < (int)cnt * 8)
+            nq0 = t_end ? P.cand_start[nc] : tq0 + LQ_CHUNK;
+            np1 = t_end ? P.cand_start[nc + 1] : tp1;
+            ncnt = min((uint32_t)LQ_CHUNK, np1 - nq0);
+            if (js < (int)ncnt)
+                leaf_stage_issue(P, &S.ch[nb].rec[js], nq0 + (uint32_t)js);
+        }
+        // ---- flush: chunk p - 2's sums to its leaf pairs' partials
+        if (f_valid)
+        {
+            LeafGradSum& Gs = S.gs[p & 1u];
+            const uint32_t n = Gs.cnt * BWD_NACC;
+            for (uint32_t i = (uint32_t)t; i < n; i += LP_THREADS)
             {
-                const uint32_t j = (uint32_t)t >> 3, w = (uint32_t)t & 7u;
-                const uint32_t e = P.vals[q0 + j];
-                const uint32_t g = P.emit_gid[e];
-                reinterpret_cast<float4*>(&S.rec[j])[w] = reinterpret_cast<const float4*>(&P.recs[g])[w];
-                if (w == 0)
-                    S.eidx[j] = e;
-            }
-            for (int i = t; i < (LP_THREADS / 32) * LQ_CHUNK * BWD_NACC; i += LP_THREADS)
-                (&S.part[0][0][0])[i] = 0.f;
-            __syncthreads();
-            if (t < (int)cnt)
-            {
-                const GaussRec& R = S.rec[t];
-                const int32_t x0 = max(R.q4.x, o[0]) - o[0], x1 = min(R.q4.x + R.q5.x - 1, o[0] + 7) - o[0];
-                const int32_t y0 = max(R.q4.y, o[1]) - o[1], y1 = min(R.q4.y + R.q5.y - 1, o[1] + 7) - o[1];
-                const int32_t z0 = max(R.q4.z, o[2]) - o[2], z1 = min(R.q4.z + R.q5.z - 1, o[2] + 7) - o[2];
-                const bool empty = x1 < x0 || y1 < y0 || z1 < z0;
-                const uint32_t ny = empty ? 1u : (uint32_t)(y1 - y0 + 1), nz = empty ? 1u : (uint32_t)(z1 - z0 + 1);
-                S.bx0[t] = x0;
-                S.by0[t] = y0;
-                S.bz0[t] = z0;
-                S.bny[t] = ny;
-                S.bnz[t] = nz;
-                S.bdiv_y[t] = (65536u + ny - 1u) / ny;
-                S.bdiv_z[t] = (65536u + nz - 1u) / nz;
-                S.bvol[t] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny * nz;
-                const RInv M = rinv_of(R);
-                S.mz[t][0] = M.m[0][2];
-                S.mz[t][1] = M.m[1][2];
-                S.mz[t][2] = M.m[2][2];
-                S.inv_s[t][0] = R.q3.y;
-                S.inv_s[t][1] = R.q3.z;
-                S.inv_s[t][2] = R.q3.w;
-                S.inv_ls[t] = R.q0.w;
-                S.posz[t] = R.q0.z;
-                S.vs[t] = rec_vs(R, P.voxel_size, P.cloud_vs);
-            }
-            for (uint32_t idx = (uint32_t)t; idx < cnt * 64; idx += LP_THREADS)
-            {
-                const uint32_t j = idx >> 6, col = idx & 63u;
-                const GaussRec& R = S.rec[j];
-                const RInv M = rinv_of(R);
-                const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
-                float cx0, cx1, cy0, cy1;
-                axis_corners(vsf, R.q0.x, o[0] + (int32_t)(col >> 3), cx0, cx1);
-                axis_corners(vsf, R.q0.y, o[1] + (int32_t)(col & 7u), cy0, cy1);
-#pragma unroll
-                for (int r = 0; r < 3; r++)
+                const uint32_t j = i / BWD_NACC, k = i - j * BWD_NACC;
+                float v = 0.f;
+                for (int w = 0; w < LP_THREADS / 32; w++)
                 {
-                    float xn, xx, yn, yx;
-                    minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
-                    minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
-                    S.sxy_lo[r][idx] = VOX_FADD(xn, yn);
-                    S.sxy_hi[r][idx] = VOX_FADD(xx, yx);
+                    v += Gs.part[w][j][k];
+                    Gs.part[w][j][k] = 0.f;
                 }
+                P.partials[(uint64_t)Gs.eidx[j] * BWD_NACC + k] = v;
             }
-            __syncthreads();
-            uint32_t start[LQ_CHUNK + 1];
-            start[0] = 0;
+        }
+        // ---- adjoint terms of chunk p - 1's queued pairs
+        if (a_valid)
+        {
+            const LeafBChunk& C = S.ch[ab];
+            LeafGradSum& Gs = S.gs[(p + 1u) & 1u];
+            if (t < LQ_CHUNK)
+                Gs.eidx[t] = C.eidx[t];
+            if (t == 0)
+                Gs.cnt = acnt;
+            const uint16_t* queue = S.queue[(p + 1u) & 1u];
+            const uint32_t* wqn = S.wqn[(p + 1u) & 1u];
+            uint32_t wstart[LP_THREADS / 32 + 1];
+            wstart[0] = 0;
 #pragma unroll
-            for (int j = 0; j < LQ_CHUNK; j++)
-                start[j + 1] = start[j] + (j < (int)cnt ? S.bvol[j] : 0u);
-            const uint32_t T = start[LQ_CHUNK];
-            for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
+            for (int w = 0; w < LP_THREADS / 32; w++)
+                wstart[w + 1] = wstart[w] + wqn[w];
+            const uint32_t qn = wstart[LP_THREADS / 32];
+            const int warp = t >> 5;
+            for (uint32_t b0 = 0; b0 < qn; b0 += LP_THREADS)
             {
                 const uint32_t e = b0 + (uint32_t)t;
-                int j = LQ_CHUNK; // past every Gaussian for lanes without a candidate
+                int j = -1;
                 float cc[BWD_NACC];
 #pragma unroll
-                for (int i = 0; i < BWD_NACC; i++)
-                    cc[i] = 0.f;
-                if (e < T)
+                for (int k = 0; k < BWD_NACC; k++)
+                    cc[k] = 0.f;
+                if (e < qn)
                 {
-                    j = 0;
-                    uint32_t sj = 0;
+                    // entry e of the concatenated warp regions
+                    uint32_t wr = 0, ws = 0;
 #pragma unroll
-                    for (int q = 1; q < LQ_CHUNK; q++)
+                    for (int w = 1; w < LP_THREADS / 32; w++)
                     {
-                        const bool ge = e >= start[q];
-                        j += ge ? 1 : 0;
-                        sj = ge ? start[q] : sj;
+                        const bool ge = e >= wstart[w];
+                        wr = ge ? (uint32_t)w : wr;
+                        ws = ge ? wstart[w] : ws;
                     }
-                    const uint32_t local = e - sj;
-                    const uint32_t rest = (local * S.bdiv_z[j]) >> 16;
-                    const uint32_t dz = local - rest * S.bnz[j];
-                    const uint32_t dx = (rest * S.bdiv_y[j]) >> 16;
-                    const uint32_t dy = rest - dx * S.bny[j];
-                    const int32_t rx = S.bx0[j] + (int32_t)dx, ry = S.by0[j] + (int32_t)dy, rz = S.bz0[j] + (int32_t)dz;
-                    const uint32_t ci = (uint32_t)j * 64u + (uint32_t)(rx * 8 + ry);
-                    const float vsf = S.vs[j], pz = S.posz[j], il = S.inv_ls[j];
-                    const float v0 = (float)(o[2] + rz);
-                    const float v1 = VOX_FADD(v0, 1.f);
-                    const float c0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz);
-                    const float c1 = VOX_FSUB(VOX_FMUL(v1, vsf), pz);
-                    float d2 = 1.f;
+                    const uint32_t q = queue[wr * (LQ_CHUNK * 64) + (e - ws)];
+                    j = (int)(q >> 9);
+                    const uint32_t n = q & 511u;
+                    const GaussRec& R = C.rec[j];
+                    const RInv M = rinv_of(R);
+                    const float vsf = C.vs[j];
+                    const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7), zz = ao[2] + (int32_t)(n & 7);
+                    SmoothTerms st;
+                    const float Kw = smooth_kernel(R, M, vsf, x, yy, zz, st);
+                    if (st.e > SMOOTH_TAU)
+                    {
+                        const uint64_t vi = C.vbase + mask_rank(C.mask, n);
+                        const float gd = P.grad_density ? P.grad_density[vi] : 0.f;
+                        float gc[3] = { 0.f, 0.f, 0.f };
+                        if (P.grad_color)
+                            for (int k = 0; k < 3; k++)
+                                gc[k] = P.grad_color[3 * vi + k];
+                        const float GK = gd + gc[0] * R.q7.x + gc[1] * R.q7.y + gc[2] * R.q7.z;
+                        cc[0] = GK * st.E;
 #pragma unroll
-                    for (int r = 0; r < 3; r++)
-                    {
-                        float zn, zx;
-                        minmax_prod(c0, c1, S.mz[j][r], zn, zx);
-                        const float lo = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_lo[r][ci], zn), il), S.inv_s[j][r]);
-                        const float hi = VOX_FMUL(VOX_FMUL(VOX_FADD(S.sxy_hi[r][ci], zx), il), S.inv_s[j][r]);
-                        if (0.f < lo)
-                            d2 = VOX_FSUB(d2, VOX_FMUL(lo, lo));
-                        else if (0.f > hi)
-                            d2 = VOX_FSUB(d2, VOX_FMUL(hi, hi));
-                    }
-                    if (d2 > 0.f)
-                    {
-                        const GaussRec& R = S.rec[j];
-                        const RInv M = rinv_of(R);
-                        SmoothTerms st;
-                        const float Kw = smooth_kernel(R, M, vsf, o[0] + rx, o[1] + ry, o[2] + rz, st);
-                        if (st.e > SMOOTH_TAU)
+                        for (int r = 0; r < 3; r++)
                         {
-                            const uint32_t n = (uint32_t)((rx << 6) | (ry << 3) | rz);
-                            const uint64_t vi = vbase + mask_rank(S.mask, n);
-                            const float gd = P.grad_density ? P.grad_density[vi] : 0.f;
-                            float gc[3] = { 0.f, 0.f, 0.f };
-                            if (P.grad_color)
-                                for (int k = 0; k < 3; k++)
-                                    gc[k] = P.grad_color[3 * vi + k];
-                            const float GK = gd + gc[0] * R.q7.x + gc[1] * R.q7.y + gc[2] * R.q7.z;
-                            cc[0] = GK * st.E;
+                            const float dzr = -GK * st.e * st.z[r];
+                            const float du = dzr * (r == 0 ? R.q3.y : (r == 1 ? R.q3.z : R.q3.w));
+                            cc[1 + r] = du;
+                            cc[4 + r] = dzr * st.z[r];
 #pragma unroll
-                            for (int r = 0; r < 3; r++)
-                            {
-                                const float dzr = -GK * st.e * st.z[r];
-                                const float du = dzr * S.inv_s[j][r];
-                                cc[1 + r] = du;
-                                cc[4 + r] = dzr * st.z[r];
-#pragma unroll
-                                for (int a = 0; a < 3; a++)
-                                    cc[7 + 3 * r + a] = du * st.d[a];
-                            }
-                            cc[16] = Kw * gc[0];
-                            cc[17] = Kw * gc[1];
-                            cc[18] = Kw * gc[2];
+                            for (int a = 0; a < 3; a++)
+                                cc[7 + 3 * r + a] = du * st.d[a];
                         }
+                        cc[16] = Kw * gc[0];
+                        cc[17] = Kw * gc[1];
+                        cc[18] = Kw * gc[2];
                     }
                 }
-                // per Gaussian present in this warp (lanes of one Gaussian are contiguous)
-                const int jlo = __shfl_sync(0xffffffffu, j, 0);
-                const int jhi = min(__shfl_sync(0xffffffffu, j, 31), (int)cnt - 1);
-                for (int jx = jlo; jx <= jhi; jx++)
+                // per Gaussian present in this warp: its terms summed across the warp
+                // (fixed shuffle tree) into this warp's slots
+                uint32_t todo = __ballot_sync(0xffffffffu, j >= 0);
+                while (todo)
                 {
+                    const int jx = __shfl_sync(0xffffffffu, j, __ffs(todo) - 1);
                     const bool mine = j == jx;
 #pragma unroll
-                    for (int i = 0; i < BWD_NACC; i++)
+                    for (int k = 0; k < BWD_NACC; k++)
                     {
-                        float v = mine ? cc[i] : 0.f;
+                        float v = mine ? cc[k] : 0.f;
 #pragma unroll
                         for (int off = 16; off; off >>= 1)
                             v += __shfl_xor_sync(0xffffffffu, v, off);
                         if (lane == 0)
-                            S.part[warp][jx][i] += v;
+                            Gs.part[warp][jx][k] += v;
                     }
+                    todo &= ~__ballot_sync(0xffffffffu, mine);
                 }
             }
-            __syncthreads();
-            if (t < (int)cnt * BWD_NACC)
-            {
-                const int j = t / BWD_NACC, i = t % BWD_NACC;
-                float v = 0.f;
-                for (int w = 0; w < LP_THREADS / 32; w++)
-                    v += S.part[w][j][i];
-                P.partials[(uint64_t)S.eidx[j] * BWD_NACC + i] = v;
-            }
-            __syncthreads();
         }
+        // ---- test of chunk p
+        if (t_valid)
+            leaf_test_chunk<false, true>(P, S.ch[tb], min((uint32_t)LQ_CHUNK, tp1 - tq0), to, S.queue[p & 1u],
+                                         S.wqn[p & 1u], t, lane);
+        // ---- stagers: chunk p + 1's mask words and boxes
+        if (stager && n_valid)
+        {
+            int32_t no[3] = { to[0], to[1], to[2] };
+            if (t_end)
+                cand_origin(P, P.cand_key[nc], no);
+            leaf_bstage(P, S.ch[nb], js, ncnt, nq0, nc, no);
+            if (js == 0)
+            {
+                const int pp = (int)(p & 1u);
+                S.nxt_o[pp][0] = no[0];
+                S.nxt_o[pp][1] = no[1];
+                S.nxt_o[pp][2] = no[2];
+                S.nxt_q0[pp] = nq0;
+                S.nxt_p1[pp] = np1;
+                if (t_end)
+                    S.cand_next[pp] = atomicAdd(counter, 1u);
+            }
+        }
+        __syncthreads();
+        f_valid = a_valid;
+        a_valid = t_valid;
+        acnt = t_valid ? min((uint32_t)LQ_CHUNK, tp1 - tq0) : 0u;
+        ao[0] = to[0];
+        ao[1] = to[1];
+        ao[2] = to[2];
+        if (n_valid)
+        {
+            const int pp = (int)(p & 1u);
+            if (t_end)
+                cn = S.cand_next[pp];
+            tc = nc;
+            tq0 = S.nxt_q0[pp];
+            tp1 = S.nxt_p1[pp];
+            to[0] = S.nxt_o[pp][0];
+            to[1] = S.nxt_o[pp][1];
+            to[2] = S.nxt_o[pp][2];
+        }
+        t_valid = n_valid;
+        p++;
     }
 }
 
