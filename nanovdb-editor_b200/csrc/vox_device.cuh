@@ -333,6 +333,56 @@ __device__ __forceinline__ bool aabb_hits_unit_sphere(const Aabb& b)
 // lattice p = w * hi + (1 - w) * lo.  |p|^2 = fl(fl(x^2 + y^2) + z^2) is
 // monotone in each per-axis square and exp (vox_expf_cr) is monotone, so the
 // maximum is the lattice point with the per-axis smallest square.
+// vox_powf(b, e) for 0 <= b <= 1 and finite e > 0, the operations vox_logf /
+// vox_expf perform in that domain (the same results): log of a normal b < 1
+// (b = 1 - a with a < 1 is at least 2^-24), exp of a non-positive argument.
+__device__ __forceinline__ float vox_powf_unit(float b, float e)
+{
+    if (b == 0.0f)
+        return 0.0f;
+    if (b == 1.0f)
+        return 1.0f;
+    // vox_logf(b)
+    const uint32_t bits = vox_f2u(b);
+    int ex = (int)((bits >> 23) & 0xff) - 127;
+    float m = vox_u2f((bits & 0x007fffffu) | 0x3f800000u);
+    if (m > VOX_SQRT2_F)
+    {
+        m = VOX_FMUL(m, 0.5f);
+        ex += 1;
+    }
+    const float t = VOX_FDIV(VOX_FSUB(m, 1.0f), VOX_FADD(m, 1.0f));
+    const float t2 = VOX_FMUL(t, t);
+    float p = 1.0f / 11.0f;
+    p = VOX_FFMA(p, t2, 1.0f / 9.0f);
+    p = VOX_FFMA(p, t2, 1.0f / 7.0f);
+    p = VOX_FFMA(p, t2, 1.0f / 5.0f);
+    p = VOX_FFMA(p, t2, 1.0f / 3.0f);
+    p = VOX_FFMA(p, t2, 1.0f);
+    const float logm = VOX_FMUL(VOX_FMUL(2.0f, t), p);
+    const float ef = (float)ex;
+    const float lg = VOX_FADD(VOX_FMUL(ef, VOX_LN2_HI_F), VOX_FADD(VOX_FMUL(ef, VOX_LN2_LO_F), logm));
+    // vox_expf(e * lg), argument <= 0
+    const float x = VOX_FMUL(e, lg);
+    if (x < -87.3f)
+        return 0.0f;
+    const float kf = VOX_FLOORF(VOX_FADD(VOX_FMUL(x, VOX_INV_LN2_F), 0.5f));
+    const float r = VOX_FSUB(VOX_FSUB(x, VOX_FMUL(kf, VOX_LN2_HI_F)), VOX_FMUL(kf, VOX_LN2_LO_F));
+    float q = 1.0f / 40320.0f;
+    q = VOX_FFMA(q, r, 1.0f / 5040.0f);
+    q = VOX_FFMA(q, r, 1.0f / 720.0f);
+    q = VOX_FFMA(q, r, 1.0f / 120.0f);
+    q = VOX_FFMA(q, r, 1.0f / 24.0f);
+    q = VOX_FFMA(q, r, 1.0f / 6.0f);
+    q = VOX_FFMA(q, r, 0.5f);
+    q = VOX_FFMA(q, r, 1.0f);
+    q = VOX_FFMA(q, r, 1.0f);
+    const int k = (int)kf;
+    const int k1 = k / 2, k2 = k - k1;
+    const float s1 = vox_u2f((uint32_t)(k1 + 127) << 23), s2 = vox_u2f((uint32_t)(k2 + 127) << 23);
+    return VOX_FMUL(VOX_FMUL(q, s1), s2);
+}
+
 // Lattice weights w_s = fl(fl(1/3) * s), 1 - w_s rounded (s = 1, 2); s = 0 and
 // s = 3 (w = 1 exactly) give p = lo and p = hi.
 constexpr float LAT_W1 = 0x1.555556p-2f, LAT_OW1 = 0x1.555554p-1f;
@@ -352,7 +402,7 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
     float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
     float a = VOX_FMUL(R.q6.x, vox_expf_cr(-VOX_FMUL(R.q6.y, d)));
     a = a > 0.f ? a : 0.f;
-    a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), R.q6.z));
+    a = VOX_FSUB(1.f, vox_powf_unit(VOX_FSUB(1.f, a), R.q6.z));
     if (R.q7.w != 0.f)
         a = 0.f;
     return a;
@@ -413,7 +463,7 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
     const float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
     float a = VOX_FMUL(R.q6.x, vox_expf(-VOX_FMUL(R.q6.y, d)));
     a = a > 0.f ? a : 0.f;
-    a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), R.q6.z));
+    a = VOX_FSUB(1.f, vox_powf_unit(VOX_FSUB(1.f, a), R.q6.z));
     if (R.q7.w != 0.f)
         a = 0.f;
     return a;

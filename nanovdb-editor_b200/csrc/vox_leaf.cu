@@ -257,9 +257,17 @@ __device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S
 constexpr int LQ_CHUNK = 8;
 constexpr int LQ_STAGE_T0 = LP_THREADS - 32; // lanes 0..LQ_CHUNK-1 of the last warp stage the next chunk
 
+// A record slot padded to 144 B: the same field of a chunk's 8 records falls in
+// 8 different shared-memory banks (a 128 B stride puts them all in one).
+struct RecSlot
+{
+    GaussRec r;
+    float4 pad;
+};
+
 struct LeafChunk
 {
-    GaussRec rec[LQ_CHUNK];                              // first member: 16-byte aligned for cp.async
+    RecSlot rec[LQ_CHUNK];                               // first member: 16-byte aligned for cp.async
     int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK]; // box origin, leaf-relative
     uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK];               // box extents in y and z
     uint32_t bdiv_y[LQ_CHUNK];                           // 65536 / ny, rounded up (exact division below 64)
@@ -335,7 +343,7 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
             const uint32_t dx = (local * C.bdiv_y[j]) >> 16;
             const uint32_t dy = local - dx * C.bny[j];
             const int32_t rx = C.bx0[j] + (int32_t)dx, ry = C.by0[j] + (int32_t)dy, rz0 = C.bz0[j];
-            const GaussRec& R = C.rec[j];
+            const GaussRec& R = C.rec[j].r;
             const RInv M = rinv_of(R);
             const float vsf = C.vs[j], il = R.q0.w, pz = R.q0.z;
             const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
@@ -461,7 +469,7 @@ template <bool CHECK, bool WINDOW>
 __device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChunk& C, int j, uint32_t q, uint32_t g,
                                                const int32_t o[3])
 {
-    const GaussRec& R = C.rec[j];
+    const GaussRec& R = C.rec[j].r;
     leaf_box_fields(C, j, R, o);
     C.rgb24[j] = rgba8_byte(R.q7.x) | (rgba8_byte(R.q7.y) << 8) | (rgba8_byte(R.q7.z) << 16);
     C.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
@@ -512,7 +520,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
     uint32_t tq0 = P.cand_start[tc], tp1 = P.cand_start[tc + 1];
     if (stager && js < (int)min((uint32_t)LQ_CHUNK, tp1 - tq0))
     {
-        const uint32_t g = leaf_stage_issue(P, &S.ch[0].rec[js], tq0 + (uint32_t)js);
+        const uint32_t g = leaf_stage_issue(P, &S.ch[0].rec[js].r, tq0 + (uint32_t)js);
         cp_async_wait_all();
         leaf_stage_box<CHECK, WINDOW>(P, S.ch[0], js, tq0 + (uint32_t)js, g, to);
     }
@@ -536,7 +544,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
             np1 = t_leaf_end ? P.cand_start[nc + 1] : tp1;
             ncnt = min((uint32_t)LQ_CHUNK, np1 - nq0);
             if (js < (int)ncnt)
-                ng = leaf_stage_issue(P, &S.ch[nb].rec[js], nq0 + (uint32_t)js);
+                ng = leaf_stage_issue(P, &S.ch[nb].rec[js].r, nq0 + (uint32_t)js);
         }
         // ---- flush of the leaf whose last alpha ran in the previous phase
         if (f_valid)
@@ -604,7 +612,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
             {
                 const uint32_t q = queue[e];
                 const uint32_t j = q >> 9, n = q & 511u;
-                const GaussRec& R = C.rec[j];
+                const GaussRec& R = C.rec[j].r;
                 const RInv M = rinv_of(R);
                 const float vsf = C.vs[j];
                 const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7), zz = ao[2] + (int32_t)(n & 7);
@@ -717,7 +725,7 @@ __device__ __forceinline__ uint32_t mask_rank(const uint64_t* m, uint32_t n)
 // deterministic, no atomics.
 struct LeafBChunk
 {
-    GaussRec rec[LQ_CHUNK]; // first member: 16-byte aligned for cp.async
+    RecSlot rec[LQ_CHUNK]; // first member: 16-byte aligned for cp.async
     int32_t bx0[LQ_CHUNK], by0[LQ_CHUNK], bz0[LQ_CHUNK];
     uint32_t bny[LQ_CHUNK], bnz[LQ_CHUNK], bdiv_y[LQ_CHUNK], bcol[LQ_CHUNK];
     float vs[LQ_CHUNK];
@@ -757,8 +765,8 @@ __device__ __forceinline__ void leaf_bstage(const LeafPassParams& P, LeafBChunk&
     if (js < (int)cnt)
     {
         cp_async_wait_all();
-        leaf_box_fields(C, js, C.rec[js], o);
-        C.vs[js] = rec_vs(C.rec[js], P.voxel_size, P.cloud_vs);
+        leaf_box_fields(C, js, C.rec[js].r, o);
+        C.vs[js] = rec_vs(C.rec[js].r, P.voxel_size, P.cloud_vs);
         C.flag[js] = 0;
         C.eidx[js] = P.vals[q0 + (uint32_t)js];
     }
@@ -793,7 +801,7 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_backward(LeafPassParams 
     {
         const uint32_t cnt = min((uint32_t)LQ_CHUNK, tp1 - tq0);
         if (js < (int)cnt)
-            leaf_stage_issue(P, &S.ch[0].rec[js], tq0 + (uint32_t)js);
+            leaf_stage_issue(P, &S.ch[0].rec[js].r, tq0 + (uint32_t)js);
         leaf_bstage(P, S.ch[0], js, cnt, tq0, tc, to);
     }
     __syncthreads();
@@ -814,7 +822,7 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_backward(LeafPassParams 
             np1 = t_end ? P.cand_start[nc + 1] : tp1;
             ncnt = min((uint32_t)LQ_CHUNK, np1 - nq0);
             if (js < (int)ncnt)
-                leaf_stage_issue(P, &S.ch[nb].rec[js], nq0 + (uint32_t)js);
+                leaf_stage_issue(P, &S.ch[nb].rec[js].r, nq0 + (uint32_t)js);
         }
         // ---- flush: chunk p - 2's sums to its leaf pairs' partials
         if (f_valid)
@@ -873,7 +881,7 @@ __global__ void __launch_bounds__(LP_THREADS, 3) k_leaf_backward(LeafPassParams 
                     const uint32_t q = queue[wr * (LQ_CHUNK * 64) + (e - ws)];
                     j = (int)(q >> 9);
                     const uint32_t n = q & 511u;
-                    const GaussRec& R = C.rec[j];
+                    const GaussRec& R = C.rec[j].r;
                     const RInv M = rinv_of(R);
                     const float vsf = C.vs[j];
                     const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7), zz = ao[2] + (int32_t)(n & 7);
