@@ -139,10 +139,16 @@ __global__ void __launch_bounds__(256) k_leaf_emit(LeafEmitParams P, RankTables 
         const int32_t ox = (lx0 + (int32_t)(local / Ly)) * 8, oy = (ly0 + (int32_t)(local % Ly)) * 8;
         uint64_t e = WRITE ? P.lc_off[t] : 0;
         uint64_t n = 0;
+        // the write pass reuses the count pass's test results (first 32 leaves)
+        const uint32_t known = WRITE ? P.lc_mask[t] : 0u;
+        uint32_t mask = 0;
         for (int32_t lz = lz0; lz <= lz1; lz++)
         {
             const int32_t oz = lz * 8;
-            const bool hit = leaf_may_hit(R, M, vsf, ox, oy, oz);
+            const int32_t i = lz - lz0;
+            const bool hit = (WRITE && i < 32) ? ((known >> i) & 1u) != 0u : leaf_may_hit(R, M, vsf, ox, oy, oz);
+            if (!WRITE && hit && i < 32)
+                mask |= 1u << i;
             if (hit || P.check)
             {
                 if (WRITE)
@@ -158,7 +164,10 @@ __global__ void __launch_bounds__(256) k_leaf_emit(LeafEmitParams P, RankTables 
             }
         }
         if (!WRITE)
+        {
             P.lc_count[t] = n;
+            P.lc_mask[t] = mask;
+        }
     }
 }
 

@@ -115,6 +115,8 @@ struct LeafEmitParams
     const uint64_t* lcol_off; // [G] exclusive scan of per-Gaussian leaf columns (Lx * Ly)
     uint64_t NLC;             // leaf columns
     uint64_t* lc_count;       // count pass: pairs per leaf column
+    uint32_t* lc_mask;        // count pass writes, write pass reads: leaf-test results of a
+                              // column's first 32 leaves (bit lz - lz0)
     const uint64_t* lc_off;   // write pass: exclusive scan of lc_count
     uint32_t* keys;           // leaf key: lower rank << 12 | lower_n
     uint32_t* vals;           // emission index (the sort's value)

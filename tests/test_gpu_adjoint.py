@@ -1,8 +1,8 @@
 """GPU parity of the differentiable path.
 
 Forward: the differentiable channels of the CUDA path are bit-identical to
-the oracle's float restatement (same per-pair arithmetic, same (key, id)
-summation order) and within 1e-5 of the channel maximum against FP64.
+the oracle's float restatement (same per-pair arithmetic, exact fixed-point
+sums) and within 1e-5 of the channel maximum against FP64.
 Backward: the CUDA adjoint (vox_backward) is within 1e-5 of each parameter
 family's maximum against the oracle's FP64 adjoint, which
 tests/test_oracle_adjoint.py pins with FP64 central differences.
