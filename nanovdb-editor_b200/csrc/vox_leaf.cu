@@ -263,7 +263,7 @@ __device__ __forceinline__ void stage_chunk(const LeafPassParams& P, LeafSmem& S
 // of chunk i + 1 (lanes of the last warp copy its records with cp.async and
 // place its boxes).  Chunk data is triple-buffered, queues double-buffered,
 // the per-voxel accumulators double-buffered by leaf parity.
-constexpr int LQ_CHUNK = 8;
+constexpr int LQ_CHUNK = 12;
 constexpr int LQ_STAGE_T0 = LP_THREADS - 32; // lanes 0..LQ_CHUNK-1 of the last warp stage the next chunk
 
 // A record slot padded to 144 B: the same field of a chunk's 8 records falls in
@@ -768,7 +768,8 @@ struct LeafBSmem
 __device__ __forceinline__ void leaf_bstage(const LeafPassParams& P, LeafBChunk& C, int js, uint32_t cnt, uint32_t q0,
                                             int64_t c, const int32_t o[3])
 {
-    C.mask[js] = P.cand_mask[8 * (uint64_t)c + js];
+    if (js < 8)
+        C.mask[js] = P.cand_mask[8 * (uint64_t)c + js];
     if (js == 0)
         C.vbase = P.cand_vbase[c];
     if (js < (int)cnt)
