@@ -59,7 +59,7 @@ struct vox_context_t
     DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
     DevBuf vox_leaf, vox_n, rank_to_lower;
     // leaf-granular pipeline
-    DevBuf lcols, lcol_off, lc_count, lc_mask, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask, pair_gid;
+    DevBuf cand_org, lcols, lcol_off, lc_count, lc_mask, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask, pair_gid;
     DevBuf s_rgba, s_dens, s_col, s_pairs, cand_cnt, cand_voff, vkeys, vslot, vpairs, pair_off, cand_vbase, cloud_pairs;
     DevBuf partials, exp_keys, exp_ids;
     // reference node order
@@ -488,6 +488,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         (ctx->check_emit && !ensure(ctx, ctx->emit_flag, (size_t)(Q + 1))) ||
         !ensure(ctx, ctx->sort_ws, sort_workspace_bytes((int64_t)Q, 4)) || !ensure(ctx, ctx->lflags, 8 * (size_t)(Q + 1)) ||
         !ensure(ctx, ctx->lpos, 8 * (size_t)(Q + 1)) || !ensure(ctx, ctx->cand_key, 4 * (size_t)(Q + 1)) ||
+        !ensure(ctx, ctx->cand_org, 16 * (size_t)(Q + 1)) ||
         !ensure(ctx, ctx->cand_start, 4 * (size_t)(Q + 2)) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words((int64_t)Q + 1) * 2))
         return VOX_ERR_MEMORY;
@@ -531,7 +532,9 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     if (Q == 0)
         cudaMemsetAsync(ctx->cand_start.p, 0, 4, s);
     launch_leaf_compact(lkeys, lvals, (const uint32_t*)ctx->emit_gid.p, (int64_t)Q, lflags, lpos,
-                        (uint32_t*)ctx->cand_key.p, (uint32_t*)ctx->cand_start.p, (uint32_t*)ctx->pair_gid.p, s);
+                        (const uint32_t*)ctx->lower_cell.p, (const uint32_t*)ctx->root_of_rank.p,
+                        (uint32_t*)ctx->cand_key.p, (int4*)ctx->cand_org.p, (uint32_t*)ctx->cand_start.p,
+                        (uint32_t*)ctx->pair_gid.p, s);
     rc = sync_scalars(ctx, "candidate leaves");
     if (rc)
         return rc;
@@ -580,6 +583,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     LP.pair_gid = (const uint32_t*)ctx->pair_gid.p;
     LP.emit_flag = ctx->check_emit ? (const uint8_t*)ctx->emit_flag.p : nullptr;
     LP.cand_key = (const uint32_t*)ctx->cand_key.p;
+    LP.cand_org = (const int4*)ctx->cand_org.p;
     LP.cand_start = (const uint32_t*)ctx->cand_start.p;
     LP.NCL = NCL;
     LP.lower_cell = (const uint32_t*)ctx->lower_cell.p;
@@ -982,7 +986,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
                       &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->cloud_start,
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_mask, &ctx->lc_off,
-                      &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
+                      &ctx->cand_org, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
                       &ctx->cand_voff, &ctx->vkeys, &ctx->vslot, &ctx->vpairs, &ctx->pair_off, &ctx->cand_vbase, &ctx->cloud_pairs,
                       &ctx->partials, &ctx->exp_keys, &ctx->exp_ids, &ctx->nwin, &ctx->win_before,

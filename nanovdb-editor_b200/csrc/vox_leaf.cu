@@ -178,10 +178,24 @@ __global__ void k_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags)
         flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1ull : 0ull;
 }
 
-// candidate leaves from the run heads; each sorted pair's Gaussian id
+// origin of the leaf with compact key lower_rank << 12 | lower_n
+__device__ __forceinline__ void leaf_origin_of_key(uint32_t key, const uint32_t* lower_cell,
+                                                   const uint32_t* root_of_rank, int32_t o[3])
+{
+    const uint32_t lr = key >> 12, ln = key & 4095u;
+    const uint32_t cell = lower_cell[lr];
+    const uint32_t un = cell & 32767u;
+    root_tile_origin(root_of_rank[cell >> 15] & 32767u, o);
+    o[0] += (int32_t)((un >> 10) & 31) * 128 + (int32_t)((ln >> 8) & 15) * 8;
+    o[1] += (int32_t)((un >> 5) & 31) * 128 + (int32_t)((ln >> 4) & 15) * 8;
+    o[2] += (int32_t)(un & 31) * 128 + (int32_t)(ln & 15) * 8;
+}
+
+// candidate leaves (key, origin, first pair) from the run heads; each sorted pair's Gaussian id
 __global__ void k_leaf_compact(const uint32_t* keys, const uint32_t* vals, const uint32_t* emit_gid, int64_t Q,
-                               const uint64_t* flags, const uint64_t* pos, uint32_t* cand_key, uint32_t* cand_start,
-                               uint32_t* pair_gid)
+                               const uint64_t* flags, const uint64_t* pos, const uint32_t* lower_cell,
+                               const uint32_t* root_of_rank, uint32_t* cand_key, int4* cand_org,
+                               uint32_t* cand_start, uint32_t* pair_gid)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Q)
@@ -189,6 +203,9 @@ __global__ void k_leaf_compact(const uint32_t* keys, const uint32_t* vals, const
     pair_gid[i] = emit_gid[vals[i]];
     if (flags[i])
     {
+        int32_t o[3];
+        leaf_origin_of_key(keys[i], lower_cell, root_of_rank, o);
+        cand_org[pos[i]] = make_int4(o[0], o[1], o[2], 0);
         cand_key[pos[i]] = keys[i];
         cand_start[pos[i]] = (uint32_t)i;
     }
@@ -211,13 +228,7 @@ struct LeafSmem
 
 __device__ __forceinline__ void cand_origin(const LeafPassParams& P, uint32_t key, int32_t o[3])
 {
-    const uint32_t lr = key >> 12, ln = key & 4095u;
-    const uint32_t cell = P.lower_cell[lr];
-    const uint32_t un = cell & 32767u;
-    root_tile_origin(P.root_of_rank[cell >> 15] & 32767u, o);
-    o[0] += (int32_t)((un >> 10) & 31) * 128 + (int32_t)((ln >> 8) & 15) * 8;
-    o[1] += (int32_t)((un >> 5) & 31) * 128 + (int32_t)((ln >> 4) & 15) * 8;
-    o[2] += (int32_t)(un & 31) * 128 + (int32_t)(ln & 15) * 8;
+    leaf_origin_of_key(key, P.lower_cell, P.root_of_rank, o);
 }
 
 __device__ __forceinline__ bool in_bbox(const GaussRec& R, int32_t x, int32_t y, int32_t z)
@@ -525,7 +536,18 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
         return;
     int64_t cn = S.cand_next[0];
     int32_t to[3];
-    cand_origin(P, P.cand_key[tc], to);
+    {
+        const int4 o4 = P.cand_org[tc];
+        to[0] = o4.x;
+        to[1] = o4.y;
+        to[2] = o4.z;
+    }
+    // stagers: the next leaf's origin and pair range, loaded as soon as the leaf
+    // is known and used at the current leaf's end; lane 0 claims the leaf after
+    // it just as early, so no leaf end waits on global memory
+    int4 pre_org = make_int4(0, 0, 0, 0);
+    uint32_t pre_q0 = 0, pre_p1 = 0, cn2 = 0;
+    bool cn_fresh = true;
     uint32_t tq0 = P.cand_start[tc], tp1 = P.cand_start[tc + 1];
     if (stager && js < (int)min((uint32_t)LQ_CHUNK, tp1 - tq0))
     {
@@ -545,12 +567,24 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
         const bool t_leaf_end = t_valid && tq0 + LQ_CHUNK >= tp1;
         const int64_t nc = t_leaf_end ? cn : tc;
         const bool n_valid = t_valid && nc < P.NCL;
+        if (stager && cn_fresh)
+        {
+            if (cn < P.NCL)
+            {
+                pre_org = P.cand_org[cn];
+                pre_q0 = P.cand_start[cn];
+                pre_p1 = P.cand_start[cn + 1];
+                if (js == 0)
+                    cn2 = atomicAdd(counter, 1u);
+            }
+        }
+        cn_fresh = false;
         // ---- stagers: the next chunk's pair range, its record copies
         uint32_t nq0 = 0, np1 = 0, ncnt = 0, ng = 0;
         if (stager && n_valid)
         {
-            nq0 = t_leaf_end ? P.cand_start[nc] : tq0 + LQ_CHUNK;
-            np1 = t_leaf_end ? P.cand_start[nc + 1] : tp1;
+            nq0 = t_leaf_end ? pre_q0 : tq0 + LQ_CHUNK;
+            np1 = t_leaf_end ? pre_p1 : tp1;
             ncnt = min((uint32_t)LQ_CHUNK, np1 - nq0);
             if (js < (int)ncnt)
                 ng = leaf_stage_issue(P, &S.ch[nb].rec[js].r, nq0 + (uint32_t)js);
@@ -664,7 +698,11 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
         {
             int32_t no[3] = { to[0], to[1], to[2] };
             if (t_leaf_end)
-                cand_origin(P, P.cand_key[nc], no);
+            {
+                no[0] = pre_org.x;
+                no[1] = pre_org.y;
+                no[2] = pre_org.z;
+            }
             if (js < (int)ncnt)
             {
                 cp_async_wait_all();
@@ -679,7 +717,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                 S.nxt_q0[pp] = nq0;
                 S.nxt_p1[pp] = np1;
                 if (t_leaf_end)
-                    S.cand_next[pp] = atomicAdd(counter, 1u);
+                    S.cand_next[pp] = cn2;
             }
         }
         __syncthreads();
@@ -700,6 +738,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
             if (t_leaf_end)
             {
                 cn = S.cand_next[pp];
+                cn_fresh = true;
                 tpar ^= 1;
             }
             tc = nc;
@@ -1179,12 +1218,13 @@ void launch_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags, cudaStr
 }
 
 void launch_leaf_compact(const uint32_t* keys, const uint32_t* vals, const uint32_t* emit_gid, int64_t Q,
-                         const uint64_t* flags, const uint64_t* pos, uint32_t* cand_key, uint32_t* cand_start,
+                         const uint64_t* flags, const uint64_t* pos, const uint32_t* lower_cell,
+                         const uint32_t* root_of_rank, uint32_t* cand_key, int4* cand_org, uint32_t* cand_start,
                          uint32_t* pair_gid, cudaStream_t s)
 {
     if (Q <= 0)
         return;
-    { k_leaf_compact<<<(unsigned)((Q + 255) / 256), 256, 0, s>>>(keys, vals, emit_gid, Q, flags, pos, cand_key, cand_start, pair_gid); count_launch(); }
+    { k_leaf_compact<<<(unsigned)((Q + 255) / 256), 256, 0, s>>>(keys, vals, emit_gid, Q, flags, pos, lower_cell, root_of_rank, cand_key, cand_org, cand_start, pair_gid); count_launch(); }
 }
 
 static unsigned walk_grid(int64_t NCL, int num_sms)

@@ -135,6 +135,7 @@ struct LeafPassParams
     const uint32_t* pair_gid;  // sorted leaf pairs' Gaussian ids
     const uint8_t* emit_flag;  // check mode or null
     const uint32_t* cand_key;  // [NCL] candidate leaf keys
+    const int4* cand_org;      // [NCL] candidate leaf origins (x, y, z, 0)
     const uint32_t* cand_start;// [NCL + 1] first sorted pair of each candidate
     int64_t NCL;
     const uint32_t* lower_cell;
@@ -171,7 +172,8 @@ void launch_leaf_cols(const GaussRec* recs, int64_t G, uint64_t* lcols, cudaStre
 void launch_leaf_emit(const LeafEmitParams& P, const RankTables& T, bool write, cudaStream_t s);
 void launch_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags, cudaStream_t s);
 void launch_leaf_compact(const uint32_t* keys, const uint32_t* vals, const uint32_t* emit_gid, int64_t Q,
-                         const uint64_t* flags, const uint64_t* pos, uint32_t* cand_key, uint32_t* cand_start,
+                         const uint64_t* flags, const uint64_t* pos, const uint32_t* lower_cell,
+                         const uint32_t* root_of_rank, uint32_t* cand_key, int4* cand_org, uint32_t* cand_start,
                          uint32_t* pair_gid, cudaStream_t s);
 void launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
 void launch_leaf_backward(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
