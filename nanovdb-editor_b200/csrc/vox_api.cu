@@ -59,7 +59,7 @@ struct vox_context_t
     DevBuf leaf_lower, leaf_lower_n, leaf_mask, leaf_origin;
     DevBuf vox_leaf, vox_n, rank_to_lower;
     // leaf-granular pipeline
-    DevBuf cand_org, lcols, lcol_off, lc_count, lc_mask, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask, pair_gid;
+    DevBuf cand_org, tile_g0, lcols, lcol_off, lc_count, lc_mask, lc_off, emit_gid, emit_flag, lflags, lpos, cand_key, cand_start, cand_mask, pair_gid;
     DevBuf s_rgba, s_dens, s_col, s_pairs, cand_cnt, cand_voff, vkeys, vslot, vpairs, pair_off, cand_vbase, cloud_pairs;
     DevBuf partials, exp_keys, exp_ids;
     // reference node order
@@ -453,7 +453,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
         return rc;
     const uint64_t NLC = ctx->hscal[SC_NLC];
     if (!ensure(ctx, ctx->lc_count, 8 * (size_t)(NLC + 1)) || !ensure(ctx, ctx->lc_off, 8 * (size_t)(NLC + 1)) ||
-        !ensure(ctx, ctx->lc_mask, 4 * (size_t)(NLC + 1)) ||
+        !ensure(ctx, ctx->lc_mask, 4 * (size_t)(NLC + 1)) || !ensure(ctx, ctx->tile_g0, 8 * (size_t)(NLC / 256 + 2)) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words((int64_t)NLC + 1) * 2))
         return VOX_ERR_MEMORY;
     scan_status = (uint64_t*)ctx->scan_status.p;
@@ -466,6 +466,8 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     LE.NLC = NLC;
     LE.lc_count = (uint64_t*)ctx->lc_count.p;
     LE.lc_mask = (uint32_t*)ctx->lc_mask.p;
+    LE.tile_g0 = (const int64_t*)ctx->tile_g0.p;
+    launch_tile_gauss(lcol_off, G, NLC, (int64_t*)ctx->tile_g0.p, s);
     LE.voxel_size = voxel_size;
     LE.cloud_vs = d_cloud_vs;
     LE.check = ctx->check_emit;
@@ -986,7 +988,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
                       &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->cloud_start,
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_mask, &ctx->lc_off,
-                      &ctx->cand_org, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
+                      &ctx->cand_org, &ctx->tile_g0, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
                       &ctx->cand_voff, &ctx->vkeys, &ctx->vslot, &ctx->vpairs, &ctx->pair_off, &ctx->cand_vbase, &ctx->cloud_pairs,
                       &ctx->partials, &ctx->exp_keys, &ctx->exp_ids, &ctx->nwin, &ctx->win_before,

@@ -123,12 +123,49 @@ __device__ __forceinline__ uint32_t leaf_key_of(const GaussRec& R, int32_t x, in
 }
 
 // one thread per leaf column (lx, ly) of a Gaussian's bbox, looping over lz
+// the Gaussian of each 256-column tile's first column
+__global__ void k_tile_gauss(const uint64_t* lcol_off, int64_t G, uint64_t NLC, int64_t* tile_g0)
+{
+    const uint64_t tile = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile * 256 < NLC)
+        tile_g0[tile] = upper_bound_u64_l(lcol_off, 0, G, tile * 256) - 1;
+}
+
+// Blocks walk 256-column tiles; a tile's Gaussians [g0, g1] (g1 = the next
+// tile's first) have their column offsets copied to shared memory, where each
+// thread finds its column's Gaussian.
 template <bool WRITE>
 __global__ void __launch_bounds__(256) k_leaf_emit(LeafEmitParams P, RankTables T)
 {
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < P.NLC; t += (uint64_t)gridDim.x * blockDim.x)
+    __shared__ uint64_t s_off[257];
+    const uint64_t ntiles = (P.NLC + 255) / 256;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        const int64_t g = upper_bound_u64_l(P.lcol_off, 0, P.G, t) - 1;
+        const int64_t g0 = P.tile_g0[tile];
+        const int64_t g1 = tile + 1 < ntiles ? P.tile_g0[tile + 1] : P.G - 1;
+        const int64_t n = g1 - g0 + 1;
+        if (n <= 256 && (int64_t)threadIdx.x < n)
+            s_off[threadIdx.x] = P.lcol_off[g0 + threadIdx.x];
+        __syncthreads();
+        const uint64_t t = tile * 256 + threadIdx.x;
+        if (t < P.NLC)
+        {
+        int64_t g;
+        if (n <= 256)
+        {
+            int64_t lo = 0, hi = n; // upper bound of t in s_off[0, n)
+            while (lo < hi)
+            {
+                const int64_t mid = (lo + hi) >> 1;
+                if (s_off[mid] <= t)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            g = g0 + lo - 1;
+        }
+        else
+            g = upper_bound_u64_l(P.lcol_off, g0, g1 + 1, t) - 1;
         const GaussRec R = P.recs[g];
         const RInv M = rinv_of(R);
         const float vsf = rec_vs(R, P.voxel_size, P.cloud_vs);
@@ -138,7 +175,7 @@ __global__ void __launch_bounds__(256) k_leaf_emit(LeafEmitParams P, RankTables 
         const uint32_t local = (uint32_t)(t - P.lcol_off[g]);
         const int32_t ox = (lx0 + (int32_t)(local / Ly)) * 8, oy = (ly0 + (int32_t)(local % Ly)) * 8;
         uint64_t e = WRITE ? P.lc_off[t] : 0;
-        uint64_t n = 0;
+        uint64_t npairs = 0;
         // the write pass reuses the count pass's test results (first 32 leaves)
         const uint32_t known = WRITE ? P.lc_mask[t] : 0u;
         uint32_t mask = 0;
@@ -160,14 +197,16 @@ __global__ void __launch_bounds__(256) k_leaf_emit(LeafEmitParams P, RankTables 
                         P.emit_flag[e] = hit ? 0 : 1;
                     e++;
                 }
-                n++;
+                npairs++;
             }
         }
         if (!WRITE)
         {
-            P.lc_count[t] = n;
+            P.lc_count[t] = npairs;
             P.lc_mask[t] = mask;
         }
+        }
+        __syncthreads();
     }
 }
 
@@ -1195,6 +1234,14 @@ void launch_leaf_cols(const GaussRec* recs, int64_t G, uint64_t* lcols, cudaStre
     if (G <= 0)
         return;
     { k_leaf_cols<<<(unsigned)((G + 255) / 256), 256, 0, s>>>(recs, G, lcols); count_launch(); }
+}
+
+void launch_tile_gauss(const uint64_t* lcol_off, int64_t G, uint64_t NLC, int64_t* tile_g0, cudaStream_t s)
+{
+    if (NLC == 0)
+        return;
+    const uint64_t ntiles = (NLC + 255) / 256;
+    { k_tile_gauss<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(lcol_off, G, NLC, tile_g0); count_launch(); }
 }
 
 void launch_leaf_emit(const LeafEmitParams& P, const RankTables& T, bool write, cudaStream_t s)

@@ -114,6 +114,7 @@ struct LeafEmitParams
     int64_t G;
     const uint64_t* lcol_off; // [G] exclusive scan of per-Gaussian leaf columns (Lx * Ly)
     uint64_t NLC;             // leaf columns
+    const int64_t* tile_g0;   // [NLC / 256 + 1] Gaussian of each 256-column tile's first column
     uint64_t* lc_count;       // count pass: pairs per leaf column
     uint32_t* lc_mask;        // count pass writes, write pass reads: leaf-test results of a
                               // column's first 32 leaves (bit lz - lz0)
@@ -170,6 +171,7 @@ struct LeafPassParams
 
 void launch_leaf_cols(const GaussRec* recs, int64_t G, uint64_t* lcols, cudaStream_t s);
 void launch_leaf_emit(const LeafEmitParams& P, const RankTables& T, bool write, cudaStream_t s);
+void launch_tile_gauss(const uint64_t* lcol_off, int64_t G, uint64_t NLC, int64_t* tile_g0, cudaStream_t s);
 void launch_leaf_heads(const uint32_t* keys, int64_t Q, uint64_t* flags, cudaStream_t s);
 void launch_leaf_compact(const uint32_t* keys, const uint32_t* vals, const uint32_t* emit_gid, int64_t Q,
                          const uint64_t* flags, const uint64_t* pos, const uint32_t* lower_cell,
