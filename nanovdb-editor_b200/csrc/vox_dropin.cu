@@ -3,6 +3,7 @@
 // headless pnanovdb_get_compute() whose array functions follow
 // nanovdb_editor/putil/Compute.h:838-843.  Every raster entry is a thin
 // wrapper over vox_voxelize / vox_voxelize_host.
+#include <cctype>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>

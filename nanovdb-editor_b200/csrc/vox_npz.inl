@@ -3,11 +3,17 @@
 //
 // raster_file reads the Gaussian arrays the reference looks up by name
 // (means, opacities, quaternions, scales, sh_0, sh_n; RasterUtils.cpp:322-325)
-// from an .npz archive.  Only the layout numpy.savez writes is accepted:
-// stored (uncompressed) zip entries, ZIP64 sizes allowed, each entry a
-// little-endian float32 C-order .npy array.  Other formats (ply, e57, ingp,
-// compressed npz) belong to the reference's fileformat module and are
-// reported as unsupported.
+// from an .npz archive or a .ply file, the two formats the reference's
+// fileformat module loads for it (fileformat/FileFormat.cpp:51, :766-790).
+// .npz: the layout numpy.savez writes - stored (uncompressed) zip entries,
+// ZIP64 sizes allowed, each entry a little-endian float32 C-order .npy array.
+// .ply: the binary Gaussian-splat layout FileFormat.cpp:205-580 reads - vertex
+// properties as 4-byte floats (little or big endian), x/y/z -> means,
+// opacity, rot_0..3 -> quaternions, scale_0..2 -> scales, f_dc_0..2 -> sh_0,
+// 45 f_rest_* -> sh_n, red/green/blue -> colors.  Unlike the reference, header
+// lines may end in CRLF, and a vertex property that is not a 4-byte float is
+// rejected rather than misread.  Other formats (e57, ingp, compressed npz)
+// are reported as unsupported.
 
 namespace
 {
@@ -161,6 +167,137 @@ static bool read_npz(const char* path, std::vector<NpzArray>& arrays, std::strin
     return true;
 }
 
+// one header line without its line ending (LF or CRLF)
+static std::string ply_line(const std::string& raw)
+{
+    std::string l = raw;
+    while (!l.empty() && (l.back() == '\n' || l.back() == '\r'))
+        l.pop_back();
+    return l;
+}
+
+static bool read_ply(const char* path, std::vector<NpzArray>& arrays, std::string& why)
+{
+    FILE* f = fopen(path, "rb");
+    if (!f)
+    {
+        why = "cannot open file";
+        return false;
+    }
+    std::vector<std::string> props; // vertex property names, in file order
+    uint64_t vertex_count = 0;
+    bool in_vertex = false, big_endian = false, binary = false, header_done = false, bad_prop = false;
+    char buf[512];
+    while (fgets(buf, sizeof(buf), f))
+    {
+        const std::string line = ply_line(buf);
+        if (line == "end_header")
+        {
+            header_done = true;
+            break;
+        }
+        if (line.rfind("format ", 0) == 0)
+        {
+            binary = line.find("binary_little_endian") != std::string::npos ||
+                     line.find("binary_big_endian") != std::string::npos;
+            big_endian = line.find("binary_big_endian") != std::string::npos;
+        }
+        else if (line.rfind("element ", 0) == 0)
+        {
+            in_vertex = line.rfind("element vertex ", 0) == 0;
+            if (in_vertex)
+                vertex_count = (uint64_t)strtoull(line.c_str() + 15, nullptr, 10);
+        }
+        else if (line.rfind("property ", 0) == 0 && in_vertex)
+        {
+            const size_t sp = line.find(' ', 9);
+            const std::string type = line.substr(9, sp == std::string::npos ? std::string::npos : sp - 9);
+            if (type != "float" && type != "float32")
+                bad_prop = true;
+            props.push_back(sp == std::string::npos ? std::string() : line.substr(sp + 1));
+        }
+    }
+    if (!header_done || !binary)
+    {
+        fclose(f);
+        why = header_done ? "only binary ply files are supported" : "no ply header";
+        return false;
+    }
+    if (bad_prop)
+    {
+        fclose(f);
+        why = "every vertex property must be a 4-byte float";
+        return false;
+    }
+    auto col = [&](const char* name) -> int {
+        for (size_t i = 0; i < props.size(); i++)
+            if (props[i] == name)
+                return (int)i;
+        return -1;
+    };
+    const int x = col("x"), y = col("y"), z = col("z"), op = col("opacity");
+    const int r[4] = { col("rot_0"), col("rot_1"), col("rot_2"), col("rot_3") };
+    const int sc[3] = { col("scale_0"), col("scale_1"), col("scale_2") };
+    const int dc[3] = { col("f_dc_0"), col("f_dc_1"), col("f_dc_2") };
+    const int rest0 = col("f_rest_0");
+    const int rgb[3] = { col("red"), col("green"), col("blue") };
+    const size_t nprop = props.size();
+    std::vector<float> rows(nprop * (size_t)vertex_count);
+    const size_t got = nprop ? fread(rows.data(), sizeof(float) * nprop, (size_t)vertex_count, f) : 0;
+    fclose(f);
+    if (got != (size_t)vertex_count)
+    {
+        why = "truncated ply vertex data";
+        return false;
+    }
+    if (big_endian)
+        for (float& v : rows)
+        {
+            uint32_t u;
+            memcpy(&u, &v, 4);
+            u = (u >> 24) | ((u >> 8) & 0xFF00u) | ((u << 8) & 0xFF0000u) | (u << 24);
+            memcpy(&v, &u, 4);
+        }
+    auto gather = [&](const char* name, const int* cols, int ncol) {
+        for (int c = 0; c < ncol; c++)
+            if (cols[c] < 0)
+                return;
+        NpzArray a;
+        a.name = name;
+        a.data.resize((size_t)vertex_count * ncol);
+        for (uint64_t v = 0; v < vertex_count; v++)
+            for (int c = 0; c < ncol; c++)
+                a.data[(size_t)v * ncol + c] = rows[(size_t)v * nprop + cols[c]];
+        arrays.push_back(std::move(a));
+    };
+    const int xyz[3] = { x, y, z };
+    gather("means", xyz, 3);
+    gather("opacities", &op, 1);
+    gather("quaternions", r, 4);
+    gather("scales", sc, 3);
+    gather("sh_0", dc, 3);
+    gather("colors", rgb, 3);
+    if (rest0 >= 0 && rest0 + 45 <= (int)nprop)
+    {
+        int rest[45];
+        for (int i = 0; i < 45; i++)
+            rest[i] = rest0 + i;
+        gather("sh_n", rest, 45);
+    }
+    return true;
+}
+
+static bool has_suffix(const char* s, const char* suffix)
+{
+    const size_t n = strlen(s), m = strlen(suffix);
+    if (n < m)
+        return false;
+    for (size_t i = 0; i < m; i++)
+        if (tolower((unsigned char)s[n - m + i]) != suffix[i])
+            return false;
+    return true;
+}
+
 } // namespace
 
 static pnanovdb_bool_t PNANOVDB_ABI r_create_from_arrays(pnanovdb_raster_t* raster, const pnanovdb_compute_t*,
@@ -214,7 +351,14 @@ static pnanovdb_bool_t PNANOVDB_ABI r_raster_file(pnanovdb_raster_t* raster, con
         return PNANOVDB_FALSE;
     std::vector<NpzArray> arrays;
     std::string why;
-    if (!read_npz(filename, arrays, why))
+    bool loaded = false;
+    if (has_suffix(filename, ".ply"))
+        loaded = read_ply(filename, arrays, why);
+    else if (has_suffix(filename, ".npz"))
+        loaded = read_npz(filename, arrays, why);
+    else
+        why = "file format not supported (.npz and .ply are)";
+    if (!loaded)
     {
         std::string msg = std::string("raster_file: failed to load Gaussian data from '") + filename + "': " + why;
         log_err(msg.c_str());

@@ -78,6 +78,56 @@ def test_raster_file(raster, oracle_mod, tmp_path):
     _against_oracle(g, oracle_mod.preprocess(raw), 0.01, oracle_mod)
 
 
+def _write_ply(path, raw, big_endian=False, extra=()):
+    """A binary Gaussian-splat .ply as 3DGS tools write it: per vertex x y z,
+    normals, f_dc_0..2, f_rest_0..44, opacity, scale_0..2, rot_0..3 (float32)."""
+    means, logits, quats, log_scales, sh0, shn = raw
+    n = means.shape[0]
+    names = ["x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2"]
+    names += [f"f_rest_{i}" for i in range(45)] + ["opacity", "scale_0", "scale_1", "scale_2"]
+    names += ["rot_0", "rot_1", "rot_2", "rot_3"] + list(extra)
+    rest = shn.reshape(n, 45) if shn.size == 45 * n else np.zeros((n, 45), np.float32)
+    cols = [means, np.zeros((n, 3), np.float32), sh0.reshape(n, 3), rest, logits.reshape(n, 1),
+            log_scales.reshape(n, 3), quats.reshape(n, 4)] + [np.zeros((n, 1), np.float32)] * len(extra)
+    rows = np.concatenate(cols, axis=1).astype(">f4" if big_endian else "<f4")
+    fmt = "binary_big_endian" if big_endian else "binary_little_endian"
+    head = f"ply\nformat {fmt} 1.0\nelement vertex {n}\n" + "".join(f"property float {c}\n" for c in names)
+    head += "end_header\n"
+    with open(path, "wb") as f:
+        f.write(head.encode())
+        f.write(rows.tobytes())
+
+
+@pytest.mark.parametrize("big_endian", [False, True])
+def test_raster_file_ply(raster, oracle_mod, tmp_path, big_endian):
+    # fileformat/FileFormat.cpp:205-580: the splat .ply layout raster_file also loads
+    compute, r = raster
+    raw = W.plain_cloud(20_000, 46).raw_arrays()
+    path = tmp_path / "splats.ply"
+    _write_ply(path, raw, big_endian)
+    g = _grid(compute, r.raster_file(str(path), 0.01))
+    _against_oracle(g, oracle_mod.preprocess(raw), 0.01, oracle_mod)
+
+
+def test_raster_file_rejects_unsupported(raster, tmp_path):
+    compute, r = raster
+    raw = W.plain_cloud(100, 47).raw_arrays()
+    ascii_ply = tmp_path / "a.ply"
+    ascii_ply.write_text("ply\nformat ascii 1.0\nelement vertex 1\nproperty float x\nend_header\n0\n")
+    with pytest.raises(RuntimeError):
+        r.raster_file(str(ascii_ply), 0.01)
+    other = tmp_path / "a.xyz"
+    other.write_bytes(b"0 0 0\n")
+    with pytest.raises(RuntimeError):
+        r.raster_file(str(other), 0.01)
+    no_scales = tmp_path / "b.ply"
+    _write_ply(no_scales, raw)
+    data = no_scales.read_bytes().replace(b"property float scale_0", b"property float sxale_0")
+    no_scales.write_bytes(data)
+    with pytest.raises(RuntimeError):
+        r.raster_file(str(no_scales), 0.01)
+
+
 def test_raster_file_missing_array(raster, tmp_path):
     compute, r = raster
     raw = W.plain_cloud(100, 44).raw_arrays()
