@@ -829,6 +829,11 @@ struct LeafGradSum
     uint32_t cnt;
 };
 
+// a warp tests at most ceil(LQ_CHUNK * 64 / LP_THREADS) rounds of 32 columns of
+// up to 8 voxels; its queue region (LQ_CHUNK * 64 entries) must hold them all
+static_assert(((LQ_CHUNK * 64 + LP_THREADS - 1) / LP_THREADS) * 32 * 8 <= LQ_CHUNK * 64,
+              "per-warp queue regions too small for this chunk size");
+
 struct LeafBSmem
 {
     LeafBChunk ch[3];
