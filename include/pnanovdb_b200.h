@@ -399,6 +399,48 @@ PNANOVDB_API int vox_global_scan_u64(vox_context_t* ctx, const uint64_t* d_in, u
 PNANOVDB_API int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n,
                                       uint32_t key_bit_count);
 
+/* ------------------------------------------------ VoxelBVH ingestion -- */
+
+/* replaces ijkl_from_gaussians (raster/VoxelBVH.cpp:1225-1435; the device
+ * half of ijkl_from_gaussians_file, :1437-1575, after its host activation):
+ * for `count` activated Gaussians on the device (means [count][3], opacities
+ * [count], quaternions [count][4] as w x y z, scales [count][3]; the
+ * reference's sh0 / shn buffers play no part in this step):
+ *   d_world_bbox [6]      the box of every Gaussian's transformed
+ *                         sqrt(2 ln(max(op, 0.01) / 0.01))-sigma cube
+ *                         (min xyz, max xyz);
+ *   d_ijkl [8 count]      per Gaussian the cells of the finest level
+ *                         (0..11, cells of edge 2^level in a grid of
+ *                         `resolution` voxels over the box's longest side)
+ *                         at which at most 8 cells overlap its ellipsoid, as
+ *                         i << 48 | j << 32 | k << 16 | level, unused slots
+ *                         ~0; sorted (stable) with
+ *   d_prim_id [8 count]   the Gaussian index of each key (~0 for unused);
+ *   d_range [16 count]    [2 r] = first, [2 r + 1] = one past the last sorted
+ *                         position of the r-th distinct key, zeros after the
+ *                         last range;
+ *   *range_count (host, may be NULL) the number of ranges.
+ * `transform` (host, 16 floats or NULL for the identity) is the reference's
+ * transform_floats: the rows x y z w of a pnanovdb_camera_mat_t applied to row
+ * vectors, p' = [p 1] M; its inverse is taken in double precision
+ * (vox_voxelbvh_transform_inverse) and rounded to float.  count <= 2^29 - 1
+ * (8 count positions index in 32 bits), 1 <= resolution <= 65536, d_ijkl and
+ * d_prim_id 16-byte aligned.  A Gaussian whose box is not finite or maps
+ * outside [-65536, 65536] voxels (a zero-size world box) returns
+ * VOX_ERR_RANGE; the outputs are then undefined.  Ordered on the context's stream; returns after completion. */
+PNANOVDB_API int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, const float* d_opacities,
+                                                  const float* d_quats, const float* d_scales, int64_t count,
+                                                  uint32_t resolution, const float* transform, uint64_t* d_ijkl,
+                                                  uint32_t* d_prim_id, uint32_t* d_range, float* d_world_bbox,
+                                                  int64_t* range_count);
+
+/* The inverse vox_voxelbvh_ijkl_from_gaussians applies for `m` (16 floats,
+ * host): Gauss-Jordan elimination with partial pivoting in double precision,
+ * rounded to float.  The reference inverts in float by cofactor expansion
+ * (nanovdb_editor/putil/Camera.h:316), so the two may differ in the last
+ * bits.  VOX_ERR_ARGS for a singular or non-finite matrix. */
+PNANOVDB_API int vox_voxelbvh_transform_inverse(const float* m, float* inv);
+
 /* Scan that allocates nothing.  No counterpart in the reference.
  *
  * Same result as vox_global_scan_u64, for callers that cannot let a library

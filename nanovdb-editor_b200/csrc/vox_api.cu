@@ -9,6 +9,7 @@
 // counts) that size the buffers; buffers persist in the context and only
 // grow, so repeated calls allocate nothing.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -71,6 +72,7 @@ struct vox_context_t
     DevBuf scal; // device scalars
     DevBuf hier_keys;
     DevBuf prim_keys_alt, prim_vals_alt; // ping-pong buffers of vox_radix_sort_key64
+    DevBuf vb_work; // VoxelBVH ingestion: world-box keys, range tile counts
     uint64_t* hscal = nullptr; // pinned mirror
     Epochs scan_epochs, run_epochs, sort_epochs;
     int check_sort = 0; // VOX_CHECK_SORT=1: validate key order after every sort
@@ -986,7 +988,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
-                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->cloud_start,
+                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->cloud_start,
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_mask, &ctx->lc_off,
                       &ctx->cand_org, &ctx->tile_g0, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
@@ -1276,6 +1278,142 @@ int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals,
         cudaMemcpyAsync(d_vals, ctx->prim_vals_alt.p, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
     }
     return sync_scalars(ctx, "vox_radix_sort_key64");
+}
+
+int vox_voxelbvh_transform_inverse(const float* m, float* inv)
+{
+    if (!m || !inv)
+        return VOX_ERR_ARGS;
+    double a[4][8];
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++)
+        {
+            if (!std::isfinite(m[4 * r + c]))
+                return VOX_ERR_ARGS;
+            a[r][c] = (double)m[4 * r + c];
+            a[r][4 + c] = r == c ? 1.0 : 0.0;
+        }
+    double scale = 0.0;
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++)
+            scale = std::fmax(scale, std::fabs(a[r][c]));
+    if (scale == 0.0)
+        return VOX_ERR_ARGS;
+    for (int col = 0; col < 4; col++)
+    {
+        int piv = col;
+        for (int r = col + 1; r < 4; r++)
+            if (std::fabs(a[r][col]) > std::fabs(a[piv][col]))
+                piv = r;
+        if (std::fabs(a[piv][col]) <= 1e-12 * scale)
+            return VOX_ERR_ARGS;
+        if (piv != col)
+            for (int c = 0; c < 8; c++)
+                std::swap(a[piv][c], a[col][c]);
+        const double d = a[col][col];
+        for (int c = 0; c < 8; c++)
+            a[col][c] /= d;
+        for (int r = 0; r < 4; r++)
+        {
+            if (r == col)
+                continue;
+            const double f = a[r][col];
+            if (f != 0.0)
+                for (int c = 0; c < 8; c++)
+                    a[r][c] -= f * a[col][c];
+        }
+    }
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++)
+            inv[4 * r + c] = (float)a[r][4 + c];
+    return VOX_OK;
+}
+
+int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, const float* d_opacities,
+                                     const float* d_quats, const float* d_scales, int64_t count, uint32_t resolution,
+                                     const float* transform, uint64_t* d_ijkl, uint32_t* d_prim_id, uint32_t* d_range,
+                                     float* d_world_bbox, int64_t* range_count)
+{
+    if (!ctx || count < 0 || count > (1ll << 29) - 1 || resolution < 1u || resolution > 65536u || !d_world_bbox)
+        return VOX_ERR_ARGS;
+    if (count > 0 && (!d_means || !d_opacities || !d_quats || !d_scales || !d_ijkl || !d_prim_id || !d_range ||
+                      ((uintptr_t)d_ijkl & 15u) || ((uintptr_t)d_prim_id & 15u)))
+        return VOX_ERR_ARGS;
+    VoxelBvhParams P{};
+    P.means = d_means;
+    P.opac = d_opacities;
+    P.quats = d_quats;
+    P.scales = d_scales;
+    P.n = count;
+    P.resolution = resolution;
+    if (transform)
+    {
+        if (vox_voxelbvh_transform_inverse(transform, P.ti) != VOX_OK)
+        {
+            set_error(ctx, "vox_voxelbvh_ijkl_from_gaussians: transform is singular or not finite");
+            return VOX_ERR_ARGS;
+        }
+        for (int i = 0; i < 16; i++)
+            P.t[i] = transform[i];
+        P.has_xform = 1;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int64_t N = 8 * count;
+    const int64_t tiles = vb_range_tiles(N);
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) ||
+        !ensure(ctx, ctx->vb_work, 256 + sizeof(uint64_t) * (size_t)(2 * tiles + 2)) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(tiles > 512 ? tiles : 512) * 2))
+        return VOX_ERR_MEMORY;
+    if (N > 1 && (!ensure(ctx, ctx->prim_keys_alt, 8 * (size_t)N) || !ensure(ctx, ctx->prim_vals_alt, 4 * (size_t)N) ||
+                  !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(N, 8))))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    int* err = (int*)(sc + SC_ERR);
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    P.box_keys = (uint32_t*)ctx->vb_work.p;
+    P.world_bbox = d_world_bbox;
+    P.keys = d_ijkl;
+    P.ids = d_prim_id;
+    P.err = err;
+    uint64_t* tile_cnt = (uint64_t*)((char*)ctx->vb_work.p + 256);
+    uint64_t* tile_off = tile_cnt + tiles;
+    uint64_t* d_total = tile_off + tiles;
+    launch_vb_init(P.box_keys, s);
+    launch_vb_box(P, ctx->num_sms, s);
+    launch_vb_ijkl(P, s);
+    if (N > 1)
+    {
+        // stable sort by the whole key (radix_sort_key64 with 64 key bits, VoxelBVH.cpp:1374-1378)
+        const int in_alt = sort_pairs_u64(d_ijkl, d_prim_id, (uint64_t*)ctx->prim_keys_alt.p,
+                                          (uint32_t*)ctx->prim_vals_alt.p, N, 64, ctx->sort_ws.p, &ctx->sort_epochs,
+                                          err, ctx->num_sms, s, ctx->tuning);
+        if (in_alt)
+        {
+            cudaMemcpyAsync(d_ijkl, ctx->prim_keys_alt.p, 8 * (size_t)N, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(d_prim_id, ctx->prim_vals_alt.p, 4 * (size_t)N, cudaMemcpyDeviceToDevice, s);
+        }
+    }
+    if (N > 0)
+    {
+        launch_vb_range_count(d_ijkl, N, tile_cnt, s);
+        uint64_t* status = (uint64_t*)ctx->scan_status.p;
+        scan_exclusive_u64(tile_cnt, tile_off, tiles, 0, d_total, status,
+                           ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s),
+                           (uint32_t*)(sc + SC_SCRATCH), err, ctx->num_sms, s);
+        launch_vb_range_scatter(d_ijkl, N, tile_off, d_total, d_range, s);
+        cudaMemcpyAsync(sc + SC_F, d_total, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+    }
+    int rc = check_cuda(ctx, "vox_voxelbvh_ijkl_from_gaussians");
+    if (rc != VOX_OK)
+        return rc;
+    rc = sync_scalars(ctx, "vox_voxelbvh_ijkl_from_gaussians");
+    if (rc == VOX_ERR_RANGE)
+        set_error(ctx, "vox_voxelbvh_ijkl_from_gaussians: a Gaussian's box is not finite or maps outside "
+                       "[-65536, 65536] voxels (a zero-size world box)");
+    if (rc == VOX_OK && range_count)
+        *range_count = (int64_t)ctx->hscal[SC_F];
+    return rc;
 }
 
 } // extern "C"

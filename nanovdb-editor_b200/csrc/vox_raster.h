@@ -249,4 +249,30 @@ void launch_canonical_order(const NodeParams& N, uint64_t U, cudaStream_t s);
 void launch_write_nodes(const NodeParams& N, uint64_t U, uint8_t* out, cudaStream_t s);
 void launch_write_headers(const NodeParams& N, uint8_t* out, cudaStream_t s);
 
+// VoxelBVH Gaussian ingestion (raster/VoxelBVH.cpp:1225-1435)
+struct VoxelBvhParams
+{
+    const float* means;  // [n][3]
+    const float* opac;   // [n]
+    const float* quats;  // [n][4] w x y z
+    const float* scales; // [n][3]
+    int64_t n;
+    uint32_t resolution;
+    int has_xform;       // 0: identity transform
+    float t[16];         // p' = [p 1] t (rows of the caller's matrix)
+    float ti[16];        // inverse of t
+    uint32_t* box_keys;  // [6] order-preserving keys of the world box (min xyz, max xyz)
+    float* world_bbox;   // [6] output
+    uint64_t* keys;      // [8 n], 16-byte aligned
+    uint32_t* ids;       // [8 n], 16-byte aligned
+    int* err;
+};
+void launch_vb_init(uint32_t* box_keys, cudaStream_t s);
+void launch_vb_box(const VoxelBvhParams& P, int num_sms, cudaStream_t s);
+void launch_vb_ijkl(const VoxelBvhParams& P, cudaStream_t s);
+int64_t vb_range_tiles(int64_t N);
+void launch_vb_range_count(const uint64_t* keys, int64_t N, uint64_t* counts, cudaStream_t s);
+void launch_vb_range_scatter(const uint64_t* keys, int64_t N, const uint64_t* offs, const uint64_t* total,
+                             uint32_t* range, cudaStream_t s);
+
 } // namespace vox

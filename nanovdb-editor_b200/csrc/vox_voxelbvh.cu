@@ -1,0 +1,510 @@
+// vox_voxelbvh.cu - VoxelBVH Gaussian ingestion: per Gaussian, the finest
+// power-of-two cell level at which at most 8 cells overlap its 0.01-opacity
+// ellipsoid, those cells as 64-bit keys i << 48 | j << 32 | k << 16 | level,
+// and after the key sort the [start, end) range of every distinct key
+// (raster/VoxelBVH.cpp:1225-1435, ijkl_from_gaussians).
+//
+// Kernels, all on the caller's stream:
+//   k_vb_init           world-box accumulator = (+inf, -inf)
+//   k_vb_box            per-Gaussian transformed 8-corner box, warp-reduced,
+//                       one atomicMin / atomicMax per warp on order-preserving
+//                       integer keys (deterministic; -0 orders below +0)
+//                       (voxelbvh_gaussians_bbox_reduce1/2.slang)
+//   k_vb_ijkl           one thread per Gaussian: level search from 11 down,
+//                       stops once more than 8 cells overlap, writes 8 keys and
+//                       8 ids as 16-byte vector stores
+//                       (voxelbvh_gaussians_to_ijkl.slang:25-250)
+//   (sort)              stable onesweep LSD sort of the 64-bit keys
+//   k_vb_range_count    starts per 2048-key tile
+//   (scan)              exclusive scan of the tile counts
+//   k_vb_range_scatter  headers [2r] = start, [2r + 1] = end; every header
+//                       slot at or past the range count is zeroed
+//                       (voxelbvh_find_range_starts.slang,
+//                       voxelbvh_scatter_range_headers.slang)
+//
+// Float arithmetic: every operation is one IEEE round-to-nearest intrinsic in
+// the order the shaders write it (no contraction), so the keys are the same
+// bits as the C restatement's.  Values the shaders recompute per corner
+// (the per-axis voxel-to-world coordinates, the products of a corner's
+// coordinates with the rotation) are computed once and reused: the same
+// operations on the same operands.
+#include <cuda_runtime.h>
+
+#include "vox_device.cuh"
+#include "vox_internal.h"
+#include "vox_raster.h"
+
+namespace vox
+{
+
+namespace
+{
+
+constexpr int VB_THREADS = 256;
+constexpr int VB_TILE = 2048; // keys per range tile (8 per thread)
+constexpr float VB_CELL_LIMIT = 65536.f;
+
+__device__ __forceinline__ uint32_t vb_fkey(float f)
+{
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ float vb_funkey(uint32_t k)
+{
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+struct VbGauss
+{
+    float mu[3];
+    float R[3][3]; // forward rotation rows; the inverse is the transpose
+    float e[3];    // scale * local_scale
+    float inv[3];  // 1 / (local_scale * scale)
+};
+
+__device__ __forceinline__ void vb_load(const VoxelBvhParams& P, int64_t g, VbGauss& G)
+{
+    for (int a = 0; a < 3; a++)
+        G.mu[a] = P.means[3 * g + a];
+    const float w = P.quats[4 * g + 0], x = P.quats[4 * g + 1], y = P.quats[4 * g + 2], z = P.quats[4 * g + 3];
+    float s[3];
+    for (int a = 0; a < 3; a++)
+        s[a] = P.scales[3 * g + a];
+    const float op = P.opac[g];
+    const float o = 0.01f > op ? 0.01f : op;
+    const float ls = __fsqrt_rn(__fmul_rn(2.f, vox_logf(__fdiv_rn(o, 0.01f))));
+    G.R[0][0] = __fsub_rn(1.f, __fmul_rn(2.f, __fadd_rn(__fmul_rn(y, y), __fmul_rn(z, z))));
+    G.R[0][1] = __fmul_rn(2.f, __fsub_rn(__fmul_rn(x, y), __fmul_rn(z, w)));
+    G.R[0][2] = __fmul_rn(2.f, __fadd_rn(__fmul_rn(x, z), __fmul_rn(y, w)));
+    G.R[1][0] = __fmul_rn(2.f, __fadd_rn(__fmul_rn(x, y), __fmul_rn(z, w)));
+    G.R[1][1] = __fsub_rn(1.f, __fmul_rn(2.f, __fadd_rn(__fmul_rn(x, x), __fmul_rn(z, z))));
+    G.R[1][2] = __fmul_rn(2.f, __fsub_rn(__fmul_rn(y, z), __fmul_rn(x, w)));
+    G.R[2][0] = __fmul_rn(2.f, __fsub_rn(__fmul_rn(x, z), __fmul_rn(y, w)));
+    G.R[2][1] = __fmul_rn(2.f, __fadd_rn(__fmul_rn(y, z), __fmul_rn(x, w)));
+    G.R[2][2] = __fsub_rn(1.f, __fmul_rn(2.f, __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y))));
+    for (int a = 0; a < 3; a++)
+    {
+        G.e[a] = __fmul_rn(s[a], ls);
+        G.inv[a] = __fdiv_rn(1.f, __fmul_rn(ls, s[a]));
+    }
+}
+
+// p' = [p 1] T (row vector), sums left to right
+__device__ __forceinline__ float vb_xf(const float* T, float p0, float p1, float p2, int c)
+{
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(p0, T[c]), __fmul_rn(p1, T[4 + c])), __fmul_rn(p2, T[8 + c])),
+                     T[12 + c]);
+}
+
+__device__ __forceinline__ bool vb_finite(float x)
+{
+    return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u;
+}
+
+// transformed 8-corner box of the local_scale cube; minima / maxima as keys.
+// Returns false when a corner is not finite (the keys then cover the finite
+// corners only): the caller reports an error, since NaN has no place in the
+// order the keys encode.
+__device__ __forceinline__ bool vb_box_keys(const VoxelBvhParams& P, const VbGauss& G, uint32_t kmn[3], uint32_t kmx[3])
+{
+    bool finite = true;
+    float pr[3][3]; // pr[c][a] = e[a] * R[c][a]; the -e corner's product is its negation
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+            pr[c][a] = __fmul_rn(G.e[a], G.R[c][a]);
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        kmn[a] = 0xffffffffu;
+        kmx[a] = 0u;
+    }
+#pragma unroll
+    for (int v = 0; v < 8; v++)
+    {
+        float wp[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+        {
+            const float t0 = (v & 1) ? pr[c][0] : -pr[c][0];
+            const float t1 = (v & 2) ? pr[c][1] : -pr[c][1];
+            const float t2 = (v & 4) ? pr[c][2] : -pr[c][2];
+            wp[c] = __fadd_rn(__fadd_rn(__fadd_rn(t0, t1), t2), G.mu[c]);
+        }
+        float tp[3];
+        if (P.has_xform)
+        {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                tp[c] = vb_xf(P.t, wp[0], wp[1], wp[2], c);
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                tp[c] = wp[c];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+        {
+            if (!vb_finite(tp[a]))
+            {
+                finite = false;
+                continue;
+            }
+            const uint32_t k = vb_fkey(tp[a]);
+            kmn[a] = k < kmn[a] ? k : kmn[a];
+            kmx[a] = k > kmx[a] ? k : kmx[a];
+        }
+    }
+    return finite;
+}
+
+// voxel_ellipsoid_overlap of the cell at ijk, edge 2^level
+__device__ __forceinline__ bool vb_overlap(const VoxelBvhParams& P, const VbGauss& G, const float w2v[4], int i, int j,
+                                           int k, uint32_t level)
+{
+    const float step = (float)(1u << level);
+    const int ijk[3] = { i, j, k };
+    float lp[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const float v0 = (float)ijk[a];
+        lp[a][0] = __fdiv_rn(__fsub_rn(v0, w2v[a]), w2v[3]);
+        lp[a][1] = __fdiv_rn(__fsub_rn(__fadd_rn(v0, step), w2v[a]), w2v[3]);
+    }
+    float vmin[3] = { 0.f, 0.f, 0.f }, vmax[3] = { 0.f, 0.f, 0.f };
+    if (!P.has_xform)
+    {
+        // q[r][a][b] = (lp[a][b] - mu[a]) * Rinv[r][a], Rinv[r][a] = R[a][r]
+        float q[3][3][2];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+            {
+                const float d = __fsub_rn(lp[a][b], G.mu[a]);
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    q[r][a][b] = __fmul_rn(d, G.R[a][r]);
+            }
+#pragma unroll
+        for (int v = 0; v < 8; v++)
+        {
+            const int b0 = v & 1, b1 = (v >> 1) & 1, b2 = (v >> 2) & 1;
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+            {
+                float lr = __fadd_rn(__fadd_rn(q[r][0][b0], q[r][1][b1]), q[r][2][b2]);
+                lr = __fmul_rn(lr, G.inv[r]);
+                if (v == 0 || lr < vmin[r])
+                    vmin[r] = lr;
+                if (v == 0 || lr > vmax[r])
+                    vmax[r] = lr;
+            }
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int v = 0; v < 8; v++)
+        {
+            const float p0 = lp[0][v & 1], p1 = lp[1][(v >> 1) & 1], p2 = lp[2][(v >> 2) & 1];
+            float d[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                d[c] = __fsub_rn(vb_xf(P.ti, p0, p1, p2, c), G.mu[c]);
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+            {
+                float lr = __fadd_rn(__fadd_rn(__fmul_rn(d[0], G.R[0][r]), __fmul_rn(d[1], G.R[1][r])),
+                                     __fmul_rn(d[2], G.R[2][r]));
+                lr = __fmul_rn(lr, G.inv[r]);
+                if (v == 0 || lr < vmin[r])
+                    vmin[r] = lr;
+                if (v == 0 || lr > vmax[r])
+                    vmax[r] = lr;
+            }
+        }
+    }
+    float dist2 = 1.f;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        if (0.f < vmin[a])
+            dist2 = __fsub_rn(dist2, __fmul_rn(vmin[a], vmin[a]));
+        else if (0.f > vmax[a])
+            dist2 = __fsub_rn(dist2, __fmul_rn(vmax[a], vmax[a]));
+    }
+    return dist2 > 0.f;
+}
+
+__global__ void k_vb_init(uint32_t* box_keys)
+{
+    if (threadIdx.x < 3)
+        box_keys[threadIdx.x] = 0xff800000u; // key of +inf
+    else if (threadIdx.x < 6)
+        box_keys[threadIdx.x] = 0x007fffffu; // key of -inf
+}
+
+__global__ void __launch_bounds__(VB_THREADS) k_vb_box(VoxelBvhParams P)
+{
+    uint32_t mn[3] = { 0xff800000u, 0xff800000u, 0xff800000u }, mx[3] = { 0x007fffffu, 0x007fffffu, 0x007fffffu };
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < P.n; g += (int64_t)gridDim.x * blockDim.x)
+    {
+        VbGauss G;
+        vb_load(P, g, G);
+        uint32_t a0[3], a1[3];
+        if (!vb_box_keys(P, G, a0, a1))
+            atomicOr(P.err, ERR_RANGE);
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+        {
+            mn[a] = a0[a] < mn[a] ? a0[a] : mn[a];
+            mx[a] = a1[a] > mx[a] ? a1[a] : mx[a];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const uint32_t wmn = __reduce_min_sync(0xffffffffu, mn[a]);
+        const uint32_t wmx = __reduce_max_sync(0xffffffffu, mx[a]);
+        if ((threadIdx.x & 31) == 0)
+        {
+            atomicMin(&P.box_keys[a], wmn);
+            atomicMax(&P.box_keys[3 + a], wmx);
+        }
+    }
+}
+
+__device__ __forceinline__ bool vb_cell_ok(float v)
+{
+    return v >= -VB_CELL_LIMIT && v <= VB_CELL_LIMIT; // false for NaN
+}
+
+__global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
+{
+    // compute_world_to_voxel (voxelbvh_gaussians_to_ijkl.slang:111-118)
+    float wmin[3], wmax[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        wmin[a] = vb_funkey(P.box_keys[a]);
+        wmax[a] = vb_funkey(P.box_keys[3 + a]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 6)
+        P.world_bbox[threadIdx.x] = threadIdx.x < 3 ? wmin[threadIdx.x] : wmax[threadIdx.x - 3];
+    const float d0 = __fsub_rn(wmax[0], wmin[0]), d1 = __fsub_rn(wmax[1], wmin[1]), d2 = __fsub_rn(wmax[2], wmin[2]);
+    const float dyz = d1 > d2 ? d1 : d2;
+    const float dmax = d0 > dyz ? d0 : dyz;
+    const float sc = __fdiv_rn((float)(P.resolution - 1u), dmax);
+    const float w2v[4] = { __fadd_rn(__fmul_rn(-wmin[0], sc), 0.5f), __fadd_rn(__fmul_rn(-wmin[1], sc), 0.5f),
+                           __fadd_rn(__fmul_rn(-wmin[2], sc), 0.5f), sc };
+
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= P.n)
+        return;
+    VbGauss G;
+    vb_load(P, g, G);
+    uint32_t kmn[3], kmx[3];
+    bool ok = vb_box_keys(P, G, kmn, kmx);
+    int lo[3], hi[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const float fl = floorf(__fadd_rn(__fmul_rn(sc, vb_funkey(kmn[a])), w2v[a]));
+        const float fh = floorf(__fadd_rn(__fmul_rn(sc, vb_funkey(kmx[a])), w2v[a]));
+        ok = ok && vb_cell_ok(fl) && vb_cell_ok(fh);
+        lo[a] = (int)fl;
+        hi[a] = (int)fh;
+    }
+    uint64_t key[8] = { ~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull };
+    uint32_t nkeys = 0;
+    if (ok)
+    {
+        // level search (voxelbvh_gaussians_to_ijkl.slang:187-229); the count
+        // stops at 9 since only "more than 8" matters
+        uint32_t level = 11u, last_good = 11u;
+        while (true)
+        {
+            const int msk = ~((1 << level) - 1), st = 1 << level;
+            uint32_t count = 0;
+            for (int i = lo[0] & msk; i <= (hi[0] & msk) && count <= 8u; i += st)
+                for (int j = lo[1] & msk; j <= (hi[1] & msk) && count <= 8u; j += st)
+                    for (int k = lo[2] & msk; k <= (hi[2] & msk) && count <= 8u; k += st)
+                        count += vb_overlap(P, G, w2v, i, j, k, level) ? 1u : 0u;
+            if (count > 8u)
+            {
+                level = last_good;
+                break;
+            }
+            if (level == 0u)
+                break;
+            last_good = level;
+            level -= 1u;
+        }
+        // emission: the first 8 overlapping cells in i, j, k loop order
+        const int msk = ~((1 << level) - 1), st = 1 << level;
+        for (int i = lo[0] & msk; i <= (hi[0] & msk) && nkeys < 8u; i += st)
+            for (int j = lo[1] & msk; j <= (hi[1] & msk) && nkeys < 8u; j += st)
+                for (int k = lo[2] & msk; k <= (hi[2] & msk) && nkeys < 8u; k += st)
+                    if (vb_overlap(P, G, w2v, i, j, k, level))
+                    {
+                        const uint64_t kv = ((uint64_t)(int64_t)i << 48) | ((uint64_t)(int64_t)j << 32) |
+                                            ((uint64_t)(int64_t)k << 16) | (uint64_t)level;
+#pragma unroll
+                        for (int s = 0; s < 8; s++) // register-resident insert
+                            if ((uint32_t)s == nkeys)
+                                key[s] = kv;
+                        nkeys++;
+                    }
+    }
+    else
+        atomicOr(P.err, ERR_RANGE);
+    ulonglong2* kd = reinterpret_cast<ulonglong2*>(P.keys + 8 * g);
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+        kd[s] = make_ulonglong2(key[2 * s], key[2 * s + 1]);
+    const uint32_t id = (uint32_t)g;
+    uint4* idd = reinterpret_cast<uint4*>(P.ids + 8 * g);
+    idd[0] = make_uint4(nkeys > 0 ? id : ~0u, nkeys > 1 ? id : ~0u, nkeys > 2 ? id : ~0u, nkeys > 3 ? id : ~0u);
+    idd[1] = make_uint4(nkeys > 4 ? id : ~0u, nkeys > 5 ? id : ~0u, nkeys > 6 ? id : ~0u, nkeys > 7 ? id : ~0u);
+}
+
+// starts (key differs from its predecessor) of one 2048-key tile, per thread 8
+// consecutive keys
+__device__ __forceinline__ uint32_t vb_tile_flags(const uint64_t* keys, int64_t N, int64_t i0, uint32_t& first,
+                                                  uint32_t& last)
+{
+    first = 0;
+    last = 0;
+    if (i0 >= N)
+        return 0;
+    uint64_t prev = i0 > 0 ? keys[i0 - 1] : 0;
+    uint64_t cur = keys[i0];
+#pragma unroll
+    for (int s = 0; s < 8; s++)
+    {
+        const int64_t i = i0 + s;
+        if (i >= N)
+            break;
+        const uint64_t next = i + 1 < N ? keys[i + 1] : ~cur;
+        if (i == 0 || cur != prev)
+            first |= 1u << s;
+        if (cur != next)
+            last |= 1u << s;
+        prev = cur;
+        cur = next;
+    }
+    return (uint32_t)__popc(first);
+}
+
+__global__ void __launch_bounds__(VB_THREADS) k_vb_range_count(const uint64_t* keys, int64_t N, uint64_t* counts)
+{
+    __shared__ uint32_t s_w[VB_THREADS / 32];
+    const int64_t i0 = (int64_t)blockIdx.x * VB_TILE + 8 * threadIdx.x;
+    uint32_t f, l;
+    uint32_t c = vb_tile_flags(keys, N, i0, f, l);
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0)
+        s_w[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint64_t t = 0;
+        for (int w = 0; w < VB_THREADS / 32; w++)
+            t += s_w[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(VB_THREADS) k_vb_range_scatter(const uint64_t* keys, int64_t N,
+                                                                   const uint64_t* offs, const uint64_t* total,
+                                                                   uint32_t* range)
+{
+    __shared__ uint64_t s_warp[33];
+    const int64_t i0 = (int64_t)blockIdx.x * VB_TILE + 8 * threadIdx.x;
+    uint32_t first, last;
+    const uint32_t c = vb_tile_flags(keys, N, i0, first, last);
+    uint64_t tile_total;
+    // inclusive count of starts before this thread's first key, minus one
+    const int64_t base = (int64_t)offs[blockIdx.x] + (int64_t)block_excl_scan_u64(c, s_warp, tile_total) - 1;
+    const uint64_t R = *total;
+    int64_t r = base;
+#pragma unroll
+    for (int s = 0; s < 8; s++)
+    {
+        const int64_t i = i0 + s;
+        if (i >= N)
+            break;
+        if (first & (1u << s))
+        {
+            r++;
+            range[2 * r] = (uint32_t)i;
+        }
+        if (last & (1u << s))
+            range[2 * r + 1] = (uint32_t)(i + 1);
+        if ((uint64_t)i >= R)
+        {
+            range[2 * i] = 0u;
+            range[2 * i + 1] = 0u;
+        }
+    }
+}
+
+} // namespace
+
+void launch_vb_init(uint32_t* box_keys, cudaStream_t s)
+{
+    k_vb_init<<<1, 32, 0, s>>>(box_keys);
+    count_launch();
+}
+
+void launch_vb_box(const VoxelBvhParams& P, int num_sms, cudaStream_t s)
+{
+    if (P.n <= 0)
+        return;
+    int64_t grid = (P.n + VB_THREADS - 1) / VB_THREADS;
+    const int64_t cap = (int64_t)num_sms * 8;
+    if (grid > cap)
+        grid = cap;
+    k_vb_box<<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
+    count_launch();
+}
+
+void launch_vb_ijkl(const VoxelBvhParams& P, cudaStream_t s)
+{
+    // one block even for n = 0: it writes the world box
+    const int64_t grid = P.n > 0 ? (P.n + VB_THREADS - 1) / VB_THREADS : 1;
+    k_vb_ijkl<<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
+    count_launch();
+}
+
+int64_t vb_range_tiles(int64_t N)
+{
+    return (N + VB_TILE - 1) / VB_TILE;
+}
+
+void launch_vb_range_count(const uint64_t* keys, int64_t N, uint64_t* counts, cudaStream_t s)
+{
+    const int64_t tiles = vb_range_tiles(N);
+    if (tiles == 0)
+        return;
+    k_vb_range_count<<<(unsigned)tiles, VB_THREADS, 0, s>>>(keys, N, counts);
+    count_launch();
+}
+
+void launch_vb_range_scatter(const uint64_t* keys, int64_t N, const uint64_t* offs, const uint64_t* total,
+                             uint32_t* range, cudaStream_t s)
+{
+    const int64_t tiles = vb_range_tiles(N);
+    if (tiles == 0)
+        return;
+    k_vb_range_scatter<<<(unsigned)tiles, VB_THREADS, 0, s>>>(keys, N, offs, total, range);
+    count_launch();
+}
+
+} // namespace vox

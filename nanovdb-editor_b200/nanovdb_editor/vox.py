@@ -103,6 +103,10 @@ def _lib():
         lib.vox_backward.argtypes = [c_void_p, POINTER(vox_gaussians_t)] + [c_void_p] * 7
         lib.vox_radix_sort_key64.restype = c_int
         lib.vox_radix_sort_key64.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_uint32]
+        lib.vox_voxelbvh_ijkl_from_gaussians.restype = c_int
+        lib.vox_voxelbvh_ijkl_from_gaussians.argtypes = [c_void_p] + [c_void_p] * 4 + [c_int64, c_uint32] + [c_void_p] * 5 + [POINTER(c_int64)]
+        lib.vox_voxelbvh_transform_inverse.restype = c_int
+        lib.vox_voxelbvh_transform_inverse.argtypes = [c_void_p, c_void_p]
         lib._vox_bound = True
     return lib
 
@@ -251,6 +255,46 @@ class VoxContext:
         """Scan of CUDA uint64 tensors (the reference's global_scan_uint64 is inclusive)."""
         n = int(d_in.numel())
         self._check(self.lib.vox_global_scan_u64(self.handle, _ptr(d_in), _ptr(d_out), n, 1 if inclusive else 0, _ptr(d_total)), "vox_global_scan_u64")
+
+    def voxelbvh_ijkl_from_gaussians(self, means, opacities, quats, scales, resolution: int, transform=None):
+        """VoxelBVH Gaussian ingestion (the reference's ijkl_from_gaussians,
+        raster/VoxelBVH.cpp:1225-1435) of activated CUDA float32 tensors
+        (quaternions w x y z).  Returns a dict of CUDA tensors: ``ijkl``
+        (int64 holding the uint64 keys, 8 per Gaussian, sorted), ``prim_id``
+        (int32 holding uint32 ids), ``range`` (int32 holding uint32
+        [start, end) pairs, 16 per Gaussian), ``world_bbox`` (6 floats) and the
+        int ``range_count``.  ``transform``: 4x4 (row-vector convention,
+        p' = [p 1] M) or None."""
+        import torch
+
+        n = int(means.shape[0]) if means.dim() > 0 else 0
+        dev = means.device
+        ijkl = torch.empty(8 * n, dtype=torch.int64, device=dev)
+        prim_id = torch.empty(8 * n, dtype=torch.int32, device=dev)
+        rng = torch.empty(16 * n, dtype=torch.int32, device=dev)
+        box = torch.empty(6, dtype=torch.float32, device=dev)
+        T = None
+        if transform is not None:
+            T = np.ascontiguousarray(np.asarray(transform, dtype=np.float32).reshape(16))
+        count = c_int64(0)
+        args = [means.contiguous(), opacities.contiguous(), quats.contiguous(), scales.contiguous()]
+        for a in args:
+            if a.dtype != torch.float32 or a.device != dev:
+                raise ValueError("voxelbvh_ijkl_from_gaussians takes float32 tensors on one device")
+        # the library works on its own stream: let torch's finish producing the
+        # inputs and releasing the outputs' memory first
+        torch.cuda.current_stream(dev).synchronize()
+        self._check(self.lib.vox_voxelbvh_ijkl_from_gaussians(self.handle, *[_ptr(a) for a in args], n, int(resolution),
+                                                              _ptr(T), _ptr(ijkl), _ptr(prim_id), _ptr(rng), _ptr(box),
+                                                              byref(count)), "vox_voxelbvh_ijkl_from_gaussians")
+        return {"ijkl": ijkl, "prim_id": prim_id, "range": rng, "world_bbox": box, "range_count": int(count.value)}
+
+    def voxelbvh_transform_inverse(self, transform):
+        """The float32 inverse vox_voxelbvh_ijkl_from_gaussians applies for `transform` (4x4)."""
+        m = np.ascontiguousarray(np.asarray(transform, dtype=np.float32).reshape(16))
+        out = np.empty(16, np.float32)
+        self._check(self.lib.vox_voxelbvh_transform_inverse(m.ctypes.data, out.ctypes.data), "vox_voxelbvh_transform_inverse")
+        return out.reshape(4, 4)
 
     def radix_sort_key64(self, d_keys, d_vals, key_bits: int = 64) -> None:
         """Stable in-place sort of CUDA (uint64 key, uint32 value) tensors by key bits [0, key_bits)."""

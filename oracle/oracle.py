@@ -74,6 +74,8 @@ def lib():
         L.ov_smooth_grad64.argtypes = [c_void_p] + [c_void_p] * 5 + [c_int] + [c_void_p] * 7
         L.ov_smooth_loss64.restype = ctypes.c_double
         L.ov_smooth_loss64.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
+        L.ov_voxelbvh_ijkl.argtypes = [c_int64] + [c_void_p] * 4 + [ctypes.c_uint32] + [c_void_p] * 6
+        L.ov_voxelbvh_ijkl.restype = c_int64
         _LIB = L
     return _LIB
 
@@ -186,3 +188,23 @@ class OracleResult:
 
 def hier_key(i, j, k) -> int:
     return int(lib().ov_hier_key(int(i), int(j), int(k)))
+
+
+def voxelbvh_ijkl(cloud, resolution: int, transform=None, transform_inv=None):
+    """VoxelBVH Gaussian ingestion (raster/VoxelBVH.cpp:1225-1435) of an
+    activated cloud: sorted 64-bit cell keys, their Gaussian ids, the
+    [start, end) header of every distinct key (zeros past `ranges`) and the
+    world box.  transform / transform_inv: 4x4 float32 (row-vector
+    convention, p' = [p 1] T) or None for the identity."""
+    means, q, s, o = (_f32(cloud[k]) for k in ("means", "quats", "scales", "opacities"))
+    n = means.reshape(-1, 3).shape[0]
+    T = None if transform is None else _f32(transform).reshape(16)
+    Ti = None if transform_inv is None else _f32(transform_inv).reshape(16)
+    keys = np.empty(8 * n, np.uint64)
+    ids = np.empty(8 * n, np.uint32)
+    rng = np.empty(16 * n, np.uint32)
+    box = np.empty(6, np.float32)
+    r = lib().ov_voxelbvh_ijkl(n, means.ctypes.data, o.ctypes.data, q.ctypes.data, s.ctypes.data, int(resolution),
+                               None if T is None else T.ctypes.data, None if Ti is None else Ti.ctypes.data,
+                               keys.ctypes.data, ids.ctypes.data, rng.ctypes.data, box.ctypes.data)
+    return {"ijkl": keys, "prim_id": ids, "range": rng, "ranges": int(r), "world_bbox": box}

@@ -1,6 +1,6 @@
 #!/bin/sh
 # Builds oracle/_ref/libref_shaders.so: the reference's per-thread raster
-# shaders compiled as C++ straight from the reference checkout.  Test
+# and VoxelBVH-ingestion shaders compiled as C++ straight from the reference checkout.  Test
 # infrastructure only; the outputs are git-ignored and nothing in the product
 # links them.  The only source change is mechanical and made on the fly:
 # Slang attributes / system-value semantics are stripped and the `.xxx`
@@ -24,6 +24,14 @@ for s in gaussian_prim gaussian_frag_alloc gaussian_frag_color fanout_scatter_pr
         -e 's/ : SV_Group[A-Za-z]*//g' \
         -e 's/\([A-Za-z_][A-Za-z_0-9.]*\)\.xxx/float3(\1)/g' \
         "$REF/raster/shaders/$s.slang" > "$OUT/$s.inc"
+done
+# VoxelBVH Gaussian ingestion; `.xyz` reads of a float4 become `.xyz()`
+for s in voxelbvh_gaussians_to_ijkl; do
+    sed -e 's/\[shader("compute")\]//g' \
+        -e 's/\[numthreads([^]]*)\]//g' \
+        -e 's/ : SV_Group[A-Za-z]*//g' \
+        -e 's/\.xyz\b/.xyz()/g' \
+        "$REF/raster/shaders/voxelbvh/$s.slang" > "$OUT/$s.inc"
 done
 ${CXX:-g++} -O2 -fPIC -std=c++17 -ffp-contract=off -w -Wno-narrowing \
     -I"$HERE" -I"$HERE/../../include" -I"$OUT" \

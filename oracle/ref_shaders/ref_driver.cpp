@@ -10,6 +10,7 @@
  *   fanout_compute_fragment_idxs.slang  window fan-out, raster index per slot
  *   gaussian_frag_alloc.slang           fragment test -> ijk or 0x7FFFFFFF
  *   gaussian_frag_color.slang           alpha / RGBA8 of a passing fragment
+ *   voxelbvh/voxelbvh_gaussians_to_ijkl.slang  per-Gaussian level and cells
  */
 #include <math.h>
 #include <stdint.h>
@@ -44,6 +45,12 @@ namespace sh_color
 #include "slang_compat.h"
 #include "pnanovdb_capture.h"
 #include "gaussian_frag_color.inc"
+}
+
+namespace sh_vbijkl
+{
+#include "slang_compat.h"
+#include "voxelbvh_gaussians_to_ijkl.inc"
 }
 
 template <class C>
@@ -182,6 +189,45 @@ void ref_frag_color(uint32_t ijk_batch_size, uint32_t prim_begin, float vs, floa
         {
             uint3 gi = { g, 0, 0 }, ti = { t, 0, 0 };
             g_capture_slot = (uint64_t)g * VOX_REF_GROUP + t;
+            main(gi, ti);
+        }
+}
+
+/* voxelbvh_gaussians_to_ijkl over all Gaussians (raster/VoxelBVH.cpp:1355-1372)
+ * given the reduced world box bbox6 (min xyz, max xyz).  T / Tinv: 16 floats,
+ * the logical float4x4 the shader reads (rows of the caller's matrix; the
+ * host uploads its transpose and the shaders read constants column-major,
+ * compiler/SlangCompiler.cpp:298-299, nanovdb_editor/putil/Compiler.h:134),
+ * NULL = identity.  keys / ids hold 8 x 256 x ceil(n / 256) entries: the
+ * shader writes the unused-slot sentinel for every thread of the last group. */
+void ref_voxelbvh_to_ijkl(uint32_t n, uint32_t resolution, const float* means, const float* opac, const float* quats,
+                          const float* scales, const float* T, const float* Tinv, const float* bbox6, uint64_t* keys,
+                          uint32_t* ids)
+{
+    using namespace sh_vbijkl;
+    memset(&constants, 0, sizeof(constants));
+    constants.point_count = n;
+    constants.workgroup_count = (n + 255u) / 256u;
+    constants.voxel_count = 8u * n;
+    constants.voxel_workgroup_count = (constants.voxel_count + 255u) / 256u;
+    constants.resolution = resolution;
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++)
+        {
+            constants.transform.m[r][c] = T ? T[4 * r + c] : (r == c ? 1.f : 0.f);
+            constants.transform_inv.m[r][c] = Tinv ? Tinv[4 * r + c] : (r == c ? 1.f : 0.f);
+        }
+    means_in.p = (float*)means;
+    opacities_in.p = (float*)opac;
+    quats_in.p = (float*)quats;
+    scales_in.p = (float*)scales;
+    bbox_in.p = (float*)bbox6;
+    keys_out.p = keys;
+    bbox_ids_out.p = ids;
+    for (uint32_t g = 0; g < constants.workgroup_count; g++)
+        for (uint32_t t = 0; t < VOX_REF_GROUP; t++)
+        {
+            uint3 gi = { g, 0, 0 }, ti = { t, 0, 0 };
             main(gi, ti);
         }
 }

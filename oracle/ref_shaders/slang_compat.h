@@ -80,6 +80,7 @@ struct int3
     int x, y, z;
     int3() : x(0), y(0), z(0) {}
     int3(int a, int b, int c) : x(a), y(b), z(c) {}
+    explicit int3(const float3& v) : x((int)v.x), y((int)v.y), z((int)v.z) {}
     int3& operator+=(const int3& o)
     {
         x += o.x;
@@ -103,7 +104,33 @@ struct float4
             float r, g, b, a;
         };
     };
+    float4() : x(0.f), y(0.f), z(0.f), w(0.f) {}
+    float4(float a0, float a1, float a2, float a3) : x(a0), y(a1), z(a2), w(a3) {}
+    float4(const float3& v, float a3) : x(v.x), y(v.y), z(v.z), w(a3) {}
+    /* the `.xyz` swizzle, spelled `.xyz()` by build_ref.sh */
+    float3 xyz() const
+    {
+        return float3(x, y, z);
+    }
 };
+
+/* float4x4 as the shader indexes it, m[row][column].  mul(v, M) treats v as a
+ * row vector: result_j = ((v.x M[0][j] + v.y M[1][j]) + v.z M[2][j]) + v.w M[3][j]. */
+struct float4x4
+{
+    float m[4][4];
+};
+inline float4 mul(const float4& v, const float4x4& M)
+{
+    float r[4];
+    for (int j = 0; j < 4; j++)
+    {
+        float s = v.x * M.m[0][j] + v.y * M.m[1][j];
+        s = s + v.z * M.m[2][j];
+        r[j] = s + v.w * M.m[3][j];
+    }
+    return float4(r[0], r[1], r[2], r[3]);
+}
 
 inline float3 operator*(const float3& a, const float3& b)
 {
@@ -128,6 +155,30 @@ inline float3 operator+(const float3& a, const float3& b)
 inline float3 operator-(float s, const float3& b)
 {
     return float3(s - b.x, s - b.y, s - b.z);
+}
+inline float3 operator-(const float3& a, const float3& b)
+{
+    return float3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+inline float3 operator-(const float3& a)
+{
+    return float3(-a.x, -a.y, -a.z);
+}
+inline float3 operator+(const float3& a, float s)
+{
+    return float3(a.x + s, a.y + s, a.z + s);
+}
+inline float3 operator/(const float3& a, float s)
+{
+    return float3(a.x / s, a.y / s, a.z / s);
+}
+inline int3 operator&(const int3& a, int m)
+{
+    return int3(a.x & m, a.y & m, a.z & m);
+}
+inline float3 floor(const float3& a)
+{
+    return float3(floorf(a.x), floorf(a.y), floorf(a.z));
 }
 inline int3 operator+(const int3& a, int s)
 {

@@ -696,6 +696,285 @@ static void radix_sort_pairs(uint64_t* keys, uint32_t* ids, int64_t n, int key_b
 
 
 /* ------------------------------------------------------------------------ */
+/* VoxelBVH Gaussian ingestion (raster/VoxelBVH.cpp:1225-1435): per Gaussian  */
+/* the finest power-of-two cell level at which at most 8 cells overlap it,   */
+/* and those cells as 64-bit keys i << 48 | j << 32 | k << 16 | level; keys  */
+/* sorted stably, then the [start, end) range of every distinct key.  Inputs */
+/* are activated (normalised quaternions w,x,y,z, scales, opacities).  The   */
+/* float arithmetic follows the shaders literally, left to right:            */
+/* voxelbvh_gaussians_bbox_reduce1/2.slang, voxelbvh_gaussians_to_ijkl.slang */
+/* (:25-250), voxelbvh_find_range_starts.slang, voxelbvh_scatter_range_      */
+/* headers.slang.  T / Tinv: 16 floats, rows x y z w of the reference's      */
+/* pnanovdb_camera_mat_t, applied to row vectors (p' = [p 1] T, the shader's */
+/* mul(float4(p, 1), transform) with the transposed constant read back       */
+/* column-major, VoxelBVH.cpp:1285-1291); NULL = identity.  World-box        */
+/* minima and maxima order -0 below +0 (a total order, as a deterministic    */
+/* device reduction has it).  A non-finite box corner, or a box that maps    */
+/* beyond +-65536 voxels, is an error (-1), where the shaders' result is     */
+/* undefined.                                                                */
+/* ------------------------------------------------------------------------ */
+static void vb_xform(const float* T, const float p[3], float out[3])
+{
+    if (!T)
+    {
+        out[0] = p[0];
+        out[1] = p[1];
+        out[2] = p[2];
+        return;
+    }
+    for (int c = 0; c < 3; c++)
+        out[c] = VOX_FADD(VOX_FADD(VOX_FADD(VOX_FMUL(p[0], T[c]), VOX_FMUL(p[1], T[4 + c])), VOX_FMUL(p[2], T[8 + c])),
+                          T[12 + c]);
+}
+
+/* float -> uint32 whose unsigned order is the float order, -0 below +0 */
+static uint32_t vb_fkey(float f)
+{
+    const uint32_t u = vox_f2u(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+static float vb_fmin(float a, float b)
+{
+    return vb_fkey(a) < vb_fkey(b) ? a : b;
+}
+
+static float vb_fmax(float a, float b)
+{
+    return vb_fkey(a) > vb_fkey(b) ? a : b;
+}
+
+static float vb_local_scale(float opacity)
+{
+    const float o = 0.01f > opacity ? 0.01f : opacity; /* max(0.01, opacity) */
+    return VOX_FSQRT(VOX_FMUL(2.f, vox_logf(VOX_FDIV(o, 0.01f))));
+}
+
+/* the transformed 8-corner box of the 1-sigma * local_scale cube; returns 0
+ * when a corner is not finite (an error for the caller) */
+static int vb_gauss_aabb(const float* mean, const float* q_wxyz, const float* scale, float opacity, const float* T,
+                          float mn[3], float mx[3])
+{
+    const float x = q_wxyz[1], y = q_wxyz[2], z = q_wxyz[3], w = q_wxyz[0];
+    const float ls = vb_local_scale(opacity);
+    const float r0[3] = { VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, y), VOX_FMUL(z, z)))),
+                          VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, y), VOX_FMUL(z, w))),
+                          VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, z), VOX_FMUL(y, w))) };
+    const float r1[3] = { VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, y), VOX_FMUL(z, w))),
+                          VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(z, z)))),
+                          VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(y, z), VOX_FMUL(x, w))) };
+    const float r2[3] = { VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, z), VOX_FMUL(y, w))),
+                          VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, z), VOX_FMUL(x, w))),
+                          VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(y, y)))) };
+    const float* rr[3] = { r0, r1, r2 };
+    for (int a = 0; a < 3; a++)
+    {
+        mn[a] = vox_u2f(0x7f800000u);
+        mx[a] = -vox_u2f(0x7f800000u);
+    }
+    for (int v = 0; v < 8; v++)
+    {
+        float cp[3];
+        for (int a = 0; a < 3; a++)
+        {
+            const float e = VOX_FMUL(scale[a], ls);
+            cp[a] = ((v >> a) & 1) ? e : -e;
+        }
+        float wp[3];
+        for (int c = 0; c < 3; c++)
+            wp[c] = VOX_FADD(VOX_FADD(VOX_FADD(VOX_FMUL(cp[0], rr[c][0]), VOX_FMUL(cp[1], rr[c][1])),
+                                      VOX_FMUL(cp[2], rr[c][2])),
+                             mean[c]);
+        float tp[3];
+        vb_xform(T, wp, tp);
+        for (int a = 0; a < 3; a++)
+        {
+            if (!isfinite(tp[a]))
+                return 0;
+            mn[a] = vb_fmin(tp[a], mn[a]);
+            mx[a] = vb_fmax(tp[a], mx[a]);
+        }
+    }
+    return 1;
+}
+
+/* voxel_ellipsoid_overlap of voxelbvh_gaussians_to_ijkl.slang:25-109 */
+static int vb_overlap(const float* mean, const float* q_wxyz, const float* scale, float opacity, const float w2v[4],
+                      const int32_t ijk[3], uint32_t level, const float* Tinv)
+{
+    const float x = q_wxyz[1], y = q_wxyz[2], z = q_wxyz[3], w = q_wxyz[0];
+    const float ls = vb_local_scale(opacity);
+    const float i0[3] = { VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, y), VOX_FMUL(z, z)))),
+                          VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, y), VOX_FMUL(z, w))),
+                          VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, z), VOX_FMUL(y, w))) };
+    const float i1[3] = { VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(x, y), VOX_FMUL(z, w))),
+                          VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(z, z)))),
+                          VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(y, z), VOX_FMUL(x, w))) };
+    const float i2[3] = { VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, z), VOX_FMUL(y, w))),
+                          VOX_FMUL(2.f, VOX_FSUB(VOX_FMUL(y, z), VOX_FMUL(x, w))),
+                          VOX_FSUB(1.f, VOX_FMUL(2.f, VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(y, y)))) };
+    const float* ii[3] = { i0, i1, i2 };
+    const float step = (float)(1u << level);
+    float vmin[3] = { 0, 0, 0 }, vmax[3] = { 0, 0, 0 };
+    for (int v = 0; v < 8; v++)
+    {
+        float vp[3];
+        for (int a = 0; a < 3; a++)
+        {
+            vp[a] = (float)ijk[a];
+            if ((v >> a) & 1)
+                vp[a] = VOX_FADD(vp[a], step);
+        }
+        float lp[3];
+        for (int a = 0; a < 3; a++)
+            lp[a] = VOX_FDIV(VOX_FSUB(vp[a], w2v[a]), w2v[3]);
+        float tp[3];
+        vb_xform(Tinv, lp, tp);
+        for (int a = 0; a < 3; a++)
+            tp[a] = VOX_FSUB(tp[a], mean[a]);
+        float lr[3];
+        for (int r = 0; r < 3; r++)
+            lr[r] = VOX_FADD(VOX_FADD(VOX_FMUL(tp[0], ii[r][0]), VOX_FMUL(tp[1], ii[r][1])), VOX_FMUL(tp[2], ii[r][2]));
+        for (int a = 0; a < 3; a++)
+        {
+            lr[a] = VOX_FMUL(lr[a], VOX_FDIV(1.f, VOX_FMUL(ls, scale[a])));
+            if (v == 0 || lr[a] < vmin[a])
+                vmin[a] = lr[a];
+            if (v == 0 || lr[a] > vmax[a])
+                vmax[a] = lr[a];
+        }
+    }
+    float dist2 = 1.f;
+    for (int a = 0; a < 3; a++)
+    {
+        if (0.f < vmin[a])
+            dist2 = VOX_FSUB(dist2, VOX_FMUL(vmin[a], vmin[a]));
+        else if (0.f > vmax[a])
+            dist2 = VOX_FSUB(dist2, VOX_FMUL(vmax[a], vmax[a]));
+    }
+    return dist2 > 0.f;
+}
+
+int64_t ov_voxelbvh_ijkl(int64_t n, const float* means, const float* opacities, const float* quats_wxyz,
+                         const float* scales, uint32_t resolution, const float* T, const float* Tinv,
+                         uint64_t* ijkl, uint32_t* prim_id, uint32_t* range, float* world_bbox)
+{
+    /* world bbox (bbox_reduce1/2) */
+    float wmin[3], wmax[3];
+    for (int a = 0; a < 3; a++)
+    {
+        wmin[a] = vox_u2f(0x7f800000u);
+        wmax[a] = -vox_u2f(0x7f800000u);
+    }
+    for (int64_t g = 0; g < n; g++)
+    {
+        float mn[3], mx[3];
+        if (!vb_gauss_aabb(&means[3 * g], &quats_wxyz[4 * g], &scales[3 * g], opacities[g], T, mn, mx))
+            return -1;
+        for (int a = 0; a < 3; a++)
+        {
+            wmin[a] = vb_fmin(mn[a], wmin[a]);
+            wmax[a] = vb_fmax(mx[a], wmax[a]);
+        }
+    }
+    for (int a = 0; a < 3; a++)
+    {
+        world_bbox[a] = wmin[a];
+        world_bbox[3 + a] = wmax[a];
+    }
+    /* compute_world_to_voxel */
+    const float d[3] = { VOX_FSUB(wmax[0], wmin[0]), VOX_FSUB(wmax[1], wmin[1]), VOX_FSUB(wmax[2], wmin[2]) };
+    const float dyz = d[1] > d[2] ? d[1] : d[2];
+    const float dmax = d[0] > dyz ? d[0] : dyz;
+    const float sc = VOX_FDIV((float)(resolution - 1u), dmax);
+    const float w2v[4] = { VOX_FADD(VOX_FMUL(-wmin[0], sc), 0.5f), VOX_FADD(VOX_FMUL(-wmin[1], sc), 0.5f),
+                           VOX_FADD(VOX_FMUL(-wmin[2], sc), 0.5f), sc };
+    const int64_t nv = 8 * n;
+    for (int64_t g = 0; g < n; g++)
+    {
+        const float* mu = &means[3 * g];
+        const float* q = &quats_wxyz[4 * g];
+        const float* s = &scales[3 * g];
+        const float op = opacities[g];
+        float mn[3], mx[3];
+        if (!vb_gauss_aabb(mu, q, s, op, T, mn, mx))
+            return -1;
+        int32_t lo[3], hi[3];
+        for (int a = 0; a < 3; a++)
+        {
+            const float fl = floorf(VOX_FADD(VOX_FMUL(sc, mn[a]), w2v[a]));
+            const float fh = floorf(VOX_FADD(VOX_FMUL(sc, mx[a]), w2v[a]));
+            /* cells beyond +-65536 (non-finite input, zero-size world box):
+             * an error, as the device reports it, not an unbounded search */
+            if (!(fl >= -65536.f && fl <= 65536.f && fh >= -65536.f && fh <= 65536.f))
+                return -1;
+            lo[a] = (int32_t)fl;
+            hi[a] = (int32_t)fh;
+        }
+        uint32_t level = 11u, last_good = 11u;
+        while (level < 12u)
+        {
+            const int32_t msk = ~((1 << level) - 1), st = 1 << level;
+            uint32_t count = 0;
+            for (int32_t i = lo[0] & msk; i <= (hi[0] & msk); i += st)
+                for (int32_t j = lo[1] & msk; j <= (hi[1] & msk); j += st)
+                    for (int32_t k = lo[2] & msk; k <= (hi[2] & msk); k += st)
+                    {
+                        const int32_t c[3] = { i, j, k };
+                        count += (uint32_t)vb_overlap(mu, q, s, op, w2v, c, level, Tinv);
+                    }
+            if (count > 8u)
+            {
+                level = last_good;
+                break;
+            }
+            if (level == 0u)
+                break;
+            last_good = level;
+            level -= 1u;
+        }
+        uint32_t sub = 0;
+        {
+            const int32_t msk = ~((1 << level) - 1), st = 1 << level;
+            for (int32_t i = lo[0] & msk; i <= (hi[0] & msk); i += st)
+                for (int32_t j = lo[1] & msk; j <= (hi[1] & msk); j += st)
+                    for (int32_t k = lo[2] & msk; k <= (hi[2] & msk); k += st)
+                    {
+                        const int32_t c[3] = { i, j, k };
+                        if (sub < 8u && vb_overlap(mu, q, s, op, w2v, c, level, Tinv))
+                        {
+                            ijkl[8 * g + sub] = ((uint64_t)(int64_t)i << 48) | ((uint64_t)(int64_t)j << 32) |
+                                                ((uint64_t)(int64_t)k << 16) | (uint64_t)level;
+                            prim_id[8 * g + sub] = (uint32_t)g;
+                            sub++;
+                        }
+                    }
+        }
+        for (; sub < 8u; sub++)
+        {
+            ijkl[8 * g + sub] = ~0ull;
+            prim_id[8 * g + sub] = ~0u;
+        }
+    }
+    /* stable sort by the full 64-bit key */
+    radix_sort_pairs(ijkl, prim_id, nv, 64);
+    /* ranges: [start, end) of every distinct key, at the key's rank; the rest 0 */
+    memset(range, 0, sizeof(uint32_t) * 2 * (size_t)nv);
+    int64_t r = -1;
+    for (int64_t i = 0; i < nv; i++)
+    {
+        if (i == 0 || ijkl[i] != ijkl[i - 1])
+        {
+            r++;
+            range[2 * r] = (uint32_t)i;
+        }
+        if (i + 1 == nv || ijkl[i] != ijkl[i + 1])
+            range[2 * r + 1] = (uint32_t)(i + 1);
+    }
+    return r + 1;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Differentiable (smooth) channels.  The reference's alpha (max over a 4^3  */
 /* lattice, opacity transform, cull) is discontinuous at the pair-set        */
 /* boundary and piecewise in every parameter, so the differentiable channels */

@@ -99,6 +99,15 @@ int ov_smooth_grad64(void* h, const float* means, const float* quats_wxyz, const
  * opacity, colour[3], raw as above) to L, summed over its kernel's support */
 double ov_smooth_loss64(void* h, const double* theta, int raw, const double* grad_density, const double* grad_color);
 
+/* VoxelBVH Gaussian ingestion (raster/VoxelBVH.cpp:1225-1435), activated
+ * inputs; outputs sized 8 n (range: 2 x 8 n); returns the number of ranges,
+ * or -1 when a Gaussian's box maps outside [-65536, 65536] voxels.
+ * T / Tinv: 16 floats (rows of pnanovdb_camera_mat_t) for row vectors,
+ * p' = [p 1] T, or NULL for the identity. */
+int64_t ov_voxelbvh_ijkl(int64_t n, const float* means, const float* opacities, const float* quats_wxyz,
+                         const float* scales, uint32_t resolution, const float* T, const float* Tinv,
+                         uint64_t* ijkl, uint32_t* prim_id, uint32_t* range, float* world_bbox);
+
 #ifdef __cplusplus
 }
 #endif
