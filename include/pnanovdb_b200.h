@@ -304,6 +304,12 @@ typedef struct vox_stats_t
     int32_t sort_shape;      /* onesweep tile shape the sort used (tuned) */
     int64_t leaf_pairs;      /* (leaf, Gaussian) pairs sorted */
     int64_t candidate_leaves; /* leaves walked (some end up empty) */
+    /* last vox_voxelbvh_ijkl_from_gaussians */
+    float ms_vb_keys;     /* world box + level search + keys */
+    float ms_vb_sort;     /* key compression + radix sort */
+    float ms_vb_ranges;   /* range headers + 64-bit key write-back */
+    int32_t vb_sort_bits; /* key bits sorted (compressed key width, or 64) */
+    int64_t vb_launches;  /* kernels launched by that call */
 } vox_stats_t;
 
 /* One context per caller thread; it owns a CUDA stream on `device` and a
@@ -424,7 +430,8 @@ PNANOVDB_API int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint
  * transform_floats: the rows x y z w of a pnanovdb_camera_mat_t applied to row
  * vectors, p' = [p 1] M; its inverse is taken in double precision
  * (vox_voxelbvh_transform_inverse) and rounded to float.  count <= 2^29 - 1
- * (8 count positions index in 32 bits), 1 <= resolution <= 65536, d_ijkl and
+ * (8 count positions index in 32 bits), 1 <= resolution <= 4096 (the
+ * reference's PNANOVDB_VOXELBVH_MAX_RESOLUTION), d_ijkl and
  * d_prim_id 16-byte aligned.  A Gaussian whose box is not finite or maps
  * outside [-65536, 65536] voxels (a zero-size world box) returns
  * VOX_ERR_RANGE; the outputs are then undefined.  Ordered on the context's stream; returns after completion. */

@@ -73,6 +73,7 @@ struct vox_context_t
     DevBuf hier_keys;
     DevBuf prim_keys_alt, prim_vals_alt; // ping-pong buffers of vox_radix_sort_key64
     DevBuf vb_work; // VoxelBVH ingestion: world-box keys, range tile counts
+    DevBuf vb_keys; // VoxelBVH ingestion: compressed sort keys
     uint64_t* hscal = nullptr; // pinned mirror
     Epochs scan_epochs, run_epochs, sort_epochs;
     int check_sort = 0; // VOX_CHECK_SORT=1: validate key order after every sort
@@ -988,7 +989,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
-                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->cloud_start,
+                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->vb_keys, &ctx->cloud_start,
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_mask, &ctx->lc_off,
                       &ctx->cand_org, &ctx->tile_g0, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
@@ -1329,12 +1330,24 @@ int vox_voxelbvh_transform_inverse(const float* m, float* inv)
     return VOX_OK;
 }
 
+static int bit_length(int64_t v)
+{
+    int b = 0;
+    while (v > 0)
+    {
+        b++;
+        v >>= 1;
+    }
+    return b;
+}
+
 int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, const float* d_opacities,
                                      const float* d_quats, const float* d_scales, int64_t count, uint32_t resolution,
                                      const float* transform, uint64_t* d_ijkl, uint32_t* d_prim_id, uint32_t* d_range,
                                      float* d_world_bbox, int64_t* range_count)
 {
-    if (!ctx || count < 0 || count > (1ll << 29) - 1 || resolution < 1u || resolution > 65536u || !d_world_bbox)
+    // resolution 1..4096: validate_resolution (raster/VoxelBVH.cpp:30-33)
+    if (!ctx || count < 0 || count > (1ll << 29) - 1 || resolution < 1u || resolution > 4096u || !d_world_bbox)
         return VOX_ERR_ARGS;
     if (count > 0 && (!d_means || !d_opacities || !d_quats || !d_scales || !d_ijkl || !d_prim_id || !d_range ||
                       ((uintptr_t)d_ijkl & 15u) || ((uintptr_t)d_prim_id & 15u)))
@@ -1359,19 +1372,21 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
     }
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
+    const int64_t launches0 = launch_count();
     const int64_t N = 8 * count;
     const int64_t tiles = vb_range_tiles(N);
     if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) ||
         !ensure(ctx, ctx->vb_work, 256 + sizeof(uint64_t) * (size_t)(2 * tiles + 2)) ||
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(tiles > 512 ? tiles : 512) * 2))
         return VOX_ERR_MEMORY;
-    if (N > 1 && (!ensure(ctx, ctx->prim_keys_alt, 8 * (size_t)N) || !ensure(ctx, ctx->prim_vals_alt, 4 * (size_t)N) ||
-                  !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(N, 8))))
+    if (N > 1 && (!ensure(ctx, ctx->vb_keys, 8 * (size_t)N) || !ensure(ctx, ctx->prim_keys_alt, 8 * (size_t)N) ||
+                  !ensure(ctx, ctx->prim_vals_alt, 4 * (size_t)N) || !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(N, 8))))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
     int* err = (int*)(sc + SC_ERR);
     cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
     P.box_keys = (uint32_t*)ctx->vb_work.p;
+    P.cell_minmax = (int*)(sc + SC_BBOX);
     P.world_bbox = d_world_bbox;
     P.keys = d_ijkl;
     P.ids = d_prim_id;
@@ -1379,41 +1394,102 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
     uint64_t* tile_cnt = (uint64_t*)((char*)ctx->vb_work.p + 256);
     uint64_t* tile_off = tile_cnt + tiles;
     uint64_t* d_total = tile_off + tiles;
-    launch_vb_init(P.box_keys, s);
+    cudaEventRecord(ctx->timers.ev[0], s);
+    launch_vb_init(P.box_keys, P.cell_minmax, s);
     launch_vb_box(P, ctx->num_sms, s);
     launch_vb_ijkl(P, s);
-    if (N > 1)
+    cudaEventRecord(ctx->timers.ev[1], s);
+    int rc = check_cuda(ctx, "vox_voxelbvh_ijkl_from_gaussians");
+    if (rc == VOX_OK)
+        rc = sync_scalars(ctx, "vox_voxelbvh_ijkl_from_gaussians");
+    if (rc == VOX_ERR_RANGE)
+        set_error(ctx, "vox_voxelbvh_ijkl_from_gaussians: a Gaussian's box is not finite or maps outside "
+                       "[-65536, 65536] voxels (a zero-size world box)");
+    if (rc != VOX_OK)
+        return rc;
+
+    // Sort key: the emitted cells' coordinate range sizes a compressed key
+    // (4 level bits + the bits of i, j, k) in the same order as the 64-bit
+    // key, which the radix sort then covers in fewer passes; with a cell
+    // outside [0, 2^16) the 64-bit keys themselves are sorted (64 key bits,
+    // radix_sort_key64 of VoxelBVH.cpp:1374-1378).  Only unused slots: already
+    // in order.
+    const int* mm = (const int*)(ctx->hscal + SC_BBOX);
+    VbRangeParams R{};
+    R.range = d_range;
+    R.keys_out = d_ijkl;
+    R.ids_out = d_prim_id;
+    int key32 = 0, sort_bits = 0;
+    const void* sorted_keys = d_ijkl;
+    const bool any_cell = mm[3] >= mm[0];
+    const bool compress = any_cell && mm[0] >= 0 && mm[1] >= 0 && mm[2] >= 0 && mm[3] < 65536 && mm[4] < 65536 &&
+                          mm[5] < 65536;
+    cudaEventRecord(ctx->timers.ev[2], s);
+    if (N > 1 && any_cell)
     {
-        // stable sort by the whole key (radix_sort_key64 with 64 key bits, VoxelBVH.cpp:1374-1378)
-        const int in_alt = sort_pairs_u64(d_ijkl, d_prim_id, (uint64_t*)ctx->prim_keys_alt.p,
-                                          (uint32_t*)ctx->prim_vals_alt.p, N, 64, ctx->sort_ws.p, &ctx->sort_epochs,
-                                          err, ctx->num_sms, s, ctx->tuning);
-        if (in_alt)
+        uint64_t* alt_k = (uint64_t*)ctx->prim_keys_alt.p;
+        uint32_t* alt_v = (uint32_t*)ctx->prim_vals_alt.p;
+        int in_alt = 0;
+        if (compress)
         {
-            cudaMemcpyAsync(d_ijkl, ctx->prim_keys_alt.p, 8 * (size_t)N, cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(d_prim_id, ctx->prim_vals_alt.p, 4 * (size_t)N, cudaMemcpyDeviceToDevice, s);
+            for (int a = 0; a < 3; a++)
+                R.bits[a] = bit_length(mm[3 + a]);
+            sort_bits = 4 + R.bits[0] + R.bits[1] + R.bits[2];
+            key32 = sort_bits <= 32;
+            R.sentinel = sort_bits >= 64 ? ~0ull : (1ull << sort_bits) - 1;
+            R.expand = 1;
+            launch_vb_compress(d_ijkl, N, R, ctx->vb_keys.p, key32, ctx->num_sms, s);
+            if (key32)
+                in_alt = sort_pairs_u32((uint32_t*)ctx->vb_keys.p, d_prim_id, (uint32_t*)alt_k, alt_v, N, sort_bits,
+                                        ctx->sort_ws.p, &ctx->sort_epochs, err, ctx->num_sms, s, ctx->tuning);
+            else
+                in_alt = sort_pairs_u64((uint64_t*)ctx->vb_keys.p, d_prim_id, alt_k, alt_v, N, sort_bits,
+                                        ctx->sort_ws.p, &ctx->sort_epochs, err, ctx->num_sms, s, ctx->tuning);
+            sorted_keys = in_alt ? (const void*)alt_k : (const void*)ctx->vb_keys.p;
         }
+        else
+        {
+            sort_bits = 64;
+            in_alt = sort_pairs_u64(d_ijkl, d_prim_id, alt_k, alt_v, N, 64, ctx->sort_ws.p, &ctx->sort_epochs, err,
+                                    ctx->num_sms, s, ctx->tuning);
+            if (in_alt)
+                cudaMemcpyAsync(d_ijkl, alt_k, 8 * (size_t)N, cudaMemcpyDeviceToDevice, s);
+        }
+        if (in_alt)
+            R.ids_src = alt_v;
     }
+    cudaEventRecord(ctx->timers.ev[3], s);
     if (N > 0)
     {
-        launch_vb_range_count(d_ijkl, N, tile_cnt, s);
+        launch_vb_range_count(sorted_keys, key32, N, tile_cnt, s);
         uint64_t* status = (uint64_t*)ctx->scan_status.p;
         scan_exclusive_u64(tile_cnt, tile_off, tiles, 0, d_total, status,
                            ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s),
                            (uint32_t*)(sc + SC_SCRATCH), err, ctx->num_sms, s);
-        launch_vb_range_scatter(d_ijkl, N, tile_off, d_total, d_range, s);
+        launch_vb_range_scatter(sorted_keys, key32, N, tile_off, d_total, R, s);
         cudaMemcpyAsync(sc + SC_F, d_total, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
     }
-    int rc = check_cuda(ctx, "vox_voxelbvh_ijkl_from_gaussians");
+    cudaEventRecord(ctx->timers.ev[4], s);
+    rc = check_cuda(ctx, "vox_voxelbvh_ijkl_from_gaussians");
     if (rc != VOX_OK)
         return rc;
     rc = sync_scalars(ctx, "vox_voxelbvh_ijkl_from_gaussians");
-    if (rc == VOX_ERR_RANGE)
-        set_error(ctx, "vox_voxelbvh_ijkl_from_gaussians: a Gaussian's box is not finite or maps outside "
-                       "[-65536, 65536] voxels (a zero-size world box)");
-    if (rc == VOX_OK && range_count)
+    if (rc != VOX_OK)
+        return rc;
+    if (range_count)
         *range_count = (int64_t)ctx->hscal[SC_F];
-    return rc;
+    auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    };
+    vox_stats_t& st = ctx->stats;
+    st.ms_vb_keys = elapsed(ctx->timers.ev[0], ctx->timers.ev[1]);
+    st.ms_vb_sort = elapsed(ctx->timers.ev[2], ctx->timers.ev[3]);
+    st.ms_vb_ranges = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]);
+    st.vb_sort_bits = sort_bits;
+    st.vb_launches = launch_count() - launches0;
+    return VOX_OK;
 }
 
 } // extern "C"

@@ -262,17 +262,31 @@ struct VoxelBvhParams
     float t[16];         // p' = [p 1] t (rows of the caller's matrix)
     float ti[16];        // inverse of t
     uint32_t* box_keys;  // [6] order-preserving keys of the world box (min xyz, max xyz)
+    int* cell_minmax;    // [6] min i j k, max i j k over the emitted cells
     float* world_bbox;   // [6] output
     uint64_t* keys;      // [8 n], 16-byte aligned
     uint32_t* ids;       // [8 n], 16-byte aligned
     int* err;
 };
-void launch_vb_init(uint32_t* box_keys, cudaStream_t s);
+// sorted-key pass: compressed key layout, range headers, 64-bit key write-back
+struct VbRangeParams
+{
+    int bits[3];         // bits of i, j, k in a compressed key
+    uint64_t sentinel;   // compressed key of an unused slot
+    int expand;          // write keys_out from the compressed keys
+    uint32_t* range;     // [2 N] headers
+    uint64_t* keys_out;  // [N] 64-bit keys (expand)
+    const uint32_t* ids_src; // sorted ids to copy into ids_out, or null
+    uint32_t* ids_out;
+};
+void launch_vb_init(uint32_t* box_keys, int* cell_minmax, cudaStream_t s);
 void launch_vb_box(const VoxelBvhParams& P, int num_sms, cudaStream_t s);
 void launch_vb_ijkl(const VoxelBvhParams& P, cudaStream_t s);
 int64_t vb_range_tiles(int64_t N);
-void launch_vb_range_count(const uint64_t* keys, int64_t N, uint64_t* counts, cudaStream_t s);
-void launch_vb_range_scatter(const uint64_t* keys, int64_t N, const uint64_t* offs, const uint64_t* total,
-                             uint32_t* range, cudaStream_t s);
+void launch_vb_compress(const uint64_t* keys, int64_t N, const VbRangeParams& R, void* out, int key32, int num_sms,
+                        cudaStream_t s);
+void launch_vb_range_count(const void* keys, int key32, int64_t N, uint64_t* counts, cudaStream_t s);
+void launch_vb_range_scatter(const void* keys, int key32, int64_t N, const uint64_t* offs, const uint64_t* total,
+                             const VbRangeParams& R, cudaStream_t s);
 
 } // namespace vox

@@ -14,11 +14,17 @@
 //                       stops once more than 8 cells overlap, writes 8 keys and
 //                       8 ids as 16-byte vector stores
 //                       (voxelbvh_gaussians_to_ijkl.slang:25-250)
-//   (sort)              stable onesweep LSD sort of the 64-bit keys
+//   k_vb_compress       keys -> compressed keys of 4 + bits(i) + bits(j) +
+//                       bits(k) bits (32-bit when they fit), sized by the
+//                       emitted cells' range that k_vb_ijkl reduces: the same
+//                       order in fewer radix passes
+//   (sort)              stable onesweep LSD sort of the compressed keys (of
+//                       the 64-bit keys when a cell lies outside [0, 2^16))
 //   k_vb_range_count    starts per 2048-key tile
 //   (scan)              exclusive scan of the tile counts
 //   k_vb_range_scatter  headers [2r] = start, [2r + 1] = end; every header
-//                       slot at or past the range count is zeroed
+//                       slot at or past the range count is zeroed; writes
+//                       the sorted keys back as 64-bit keys
 //                       (voxelbvh_find_range_starts.slang,
 //                       voxelbvh_scatter_range_headers.slang)
 //
@@ -162,92 +168,132 @@ __device__ __forceinline__ bool vb_box_keys(const VoxelBvhParams& P, const VbGau
     return finite;
 }
 
-// voxel_ellipsoid_overlap of the cell at ijk, edge 2^level
-__device__ __forceinline__ bool vb_overlap(const VoxelBvhParams& P, const VbGauss& G, const float w2v[4], int i, int j,
-                                           int k, uint32_t level)
+// Voxel-to-world coordinate of one cell boundary on axis a:
+// (v - offset) / scale, v = the boundary's voxel coordinate.
+__device__ __forceinline__ float vb_lp(const float w2v[4], float v, int a)
 {
-    const float step = (float)(1u << level);
-    const int ijk[3] = { i, j, k };
-    float lp[3][2];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-    {
-        const float v0 = (float)ijk[a];
-        lp[a][0] = __fdiv_rn(__fsub_rn(v0, w2v[a]), w2v[3]);
-        lp[a][1] = __fdiv_rn(__fsub_rn(__fadd_rn(v0, step), w2v[a]), w2v[3]);
-    }
-    float vmin[3] = { 0.f, 0.f, 0.f }, vmax[3] = { 0.f, 0.f, 0.f };
-    if (!P.has_xform)
-    {
-        // q[r][a][b] = (lp[a][b] - mu[a]) * Rinv[r][a], Rinv[r][a] = R[a][r]
-        float q[3][3][2];
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-#pragma unroll
-            for (int b = 0; b < 2; b++)
-            {
-                const float d = __fsub_rn(lp[a][b], G.mu[a]);
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-                    q[r][a][b] = __fmul_rn(d, G.R[a][r]);
-            }
-#pragma unroll
-        for (int v = 0; v < 8; v++)
-        {
-            const int b0 = v & 1, b1 = (v >> 1) & 1, b2 = (v >> 2) & 1;
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-            {
-                float lr = __fadd_rn(__fadd_rn(q[r][0][b0], q[r][1][b1]), q[r][2][b2]);
-                lr = __fmul_rn(lr, G.inv[r]);
-                if (v == 0 || lr < vmin[r])
-                    vmin[r] = lr;
-                if (v == 0 || lr > vmax[r])
-                    vmax[r] = lr;
-            }
-        }
-    }
-    else
-    {
-#pragma unroll
-        for (int v = 0; v < 8; v++)
-        {
-            const float p0 = lp[0][v & 1], p1 = lp[1][(v >> 1) & 1], p2 = lp[2][(v >> 2) & 1];
-            float d[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-                d[c] = __fsub_rn(vb_xf(P.ti, p0, p1, p2, c), G.mu[c]);
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-            {
-                float lr = __fadd_rn(__fadd_rn(__fmul_rn(d[0], G.R[0][r]), __fmul_rn(d[1], G.R[1][r])),
-                                     __fmul_rn(d[2], G.R[2][r]));
-                lr = __fmul_rn(lr, G.inv[r]);
-                if (v == 0 || lr < vmin[r])
-                    vmin[r] = lr;
-                if (v == 0 || lr > vmax[r])
-                    vmax[r] = lr;
-            }
-        }
-    }
-    float dist2 = 1.f;
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-    {
-        if (0.f < vmin[a])
-            dist2 = __fsub_rn(dist2, __fmul_rn(vmin[a], vmin[a]));
-        else if (0.f > vmax[a])
-            dist2 = __fsub_rn(dist2, __fmul_rn(vmax[a], vmax[a]));
-    }
-    return dist2 > 0.f;
+    return __fdiv_rn(__fsub_rn(v, w2v[a]), w2v[3]);
 }
 
-__global__ void k_vb_init(uint32_t* box_keys)
+// voxel_ellipsoid_overlap (voxelbvh_gaussians_to_ijkl.slang:25-109) of the
+// cells of edge 2^level in the cell box [lo, hi], in the shader's i, j, k
+// loop order.  Counts overlapping cells and stops at `limit`; EMIT also
+// stores the keys of the first 8.  Per corner the arithmetic is the shader's;
+// what a corner shares with its neighbours is computed once: the boundary
+// coordinates of an axis (cell k's upper boundary is cell k + 1's lower one,
+// the same float: (float)(k + st) == (float)k + (float)st below 2^24), the
+// products with the inverse rotation, and the i-j part of each corner's sum.
+template <bool EMIT, bool XF>
+__device__ __forceinline__ uint32_t vb_scan_level(const VoxelBvhParams& P, const VbGauss& G, const float w2v[4],
+                                                  const int lo[3], const int hi[3], uint32_t level, uint32_t limit,
+                                                  uint64_t key[8])
+{
+    const int msk = ~((1 << level) - 1), st = 1 << level;
+    const float step = (float)(1u << level);
+    uint32_t count = 0;
+    for (int i = lo[0] & msk; i <= (hi[0] & msk); i += st)
+    {
+        const float pi[2] = { vb_lp(w2v, (float)i, 0), vb_lp(w2v, __fadd_rn((float)i, step), 0) };
+        for (int j = lo[1] & msk; j <= (hi[1] & msk); j += st)
+        {
+            const float pj[2] = { vb_lp(w2v, (float)j, 1), vb_lp(w2v, __fadd_rn((float)j, step), 1) };
+            // no transform: s01[r][b0][b1] = (pi - mu0) R[0][r] + (pj - mu1) R[1][r]
+            // transform:    s01[c][b0][b1] = pi T[c] + pj T[4 + c]
+            float s01[3][2][2];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int b0 = 0; b0 < 2; b0++)
+#pragma unroll
+                    for (int b1 = 0; b1 < 2; b1++)
+                    {
+                        if (XF)
+                            s01[r][b0][b1] = __fadd_rn(__fmul_rn(pi[b0], P.ti[r]), __fmul_rn(pj[b1], P.ti[4 + r]));
+                        else
+                            s01[r][b0][b1] = __fadd_rn(__fmul_rn(__fsub_rn(pi[b0], G.mu[0]), G.R[0][r]),
+                                                       __fmul_rn(__fsub_rn(pj[b1], G.mu[1]), G.R[1][r]));
+                    }
+            int k = lo[2] & msk;
+            float pk0 = vb_lp(w2v, (float)k, 2);
+            for (; k <= (hi[2] & msk); k += st)
+            {
+                const float pk1 = vb_lp(w2v, __fadd_rn((float)k, step), 2);
+                const float pk[2] = { pk0, pk1 };
+                pk0 = pk1;
+                float vmin[3] = { 0.f, 0.f, 0.f }, vmax[3] = { 0.f, 0.f, 0.f };
+#pragma unroll
+                for (int v = 0; v < 8; v++)
+                {
+                    const int b0 = v & 1, b1 = (v >> 1) & 1, b2 = (v >> 2) & 1;
+                    float lr[3];
+                    if (XF)
+                    {
+                        float d[3];
+#pragma unroll
+                        for (int c = 0; c < 3; c++)
+                            d[c] = __fsub_rn(
+                                __fadd_rn(__fadd_rn(s01[c][b0][b1], __fmul_rn(pk[b2], P.ti[8 + c])), P.ti[12 + c]),
+                                G.mu[c]);
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+                            lr[r] = __fadd_rn(__fadd_rn(__fmul_rn(d[0], G.R[0][r]), __fmul_rn(d[1], G.R[1][r])),
+                                              __fmul_rn(d[2], G.R[2][r]));
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+                            lr[r] = __fadd_rn(s01[r][b0][b1], __fmul_rn(__fsub_rn(pk[b2], G.mu[2]), G.R[2][r]));
+                    }
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        const float x = __fmul_rn(lr[r], G.inv[r]);
+                        if (v == 0 || x < vmin[r])
+                            vmin[r] = x;
+                        if (v == 0 || x > vmax[r])
+                            vmax[r] = x;
+                    }
+                }
+                float dist2 = 1.f;
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                {
+                    if (0.f < vmin[a])
+                        dist2 = __fsub_rn(dist2, __fmul_rn(vmin[a], vmin[a]));
+                    else if (0.f > vmax[a])
+                        dist2 = __fsub_rn(dist2, __fmul_rn(vmax[a], vmax[a]));
+                }
+                if (dist2 > 0.f)
+                {
+                    if (EMIT)
+                    {
+                        const uint64_t kv = ((uint64_t)(int64_t)i << 48) | ((uint64_t)(int64_t)j << 32) |
+                                            ((uint64_t)(int64_t)k << 16) | (uint64_t)level;
+#pragma unroll
+                        for (int s = 0; s < 8; s++) // register-resident insert
+                            if ((uint32_t)s == count)
+                                key[s] = kv;
+                    }
+                    if (++count >= limit)
+                        return count;
+                }
+            }
+        }
+    }
+    return count;
+}
+
+__global__ void k_vb_init(uint32_t* box_keys, int* cell_minmax)
 {
     if (threadIdx.x < 3)
         box_keys[threadIdx.x] = 0xff800000u; // key of +inf
     else if (threadIdx.x < 6)
         box_keys[threadIdx.x] = 0x007fffffu; // key of -inf
+    if (threadIdx.x < 3)
+        cell_minmax[threadIdx.x] = 0x7fffffff;
+    else if (threadIdx.x < 6)
+        cell_minmax[threadIdx.x] = (int)0x80000000;
 }
 
 __global__ void __launch_bounds__(VB_THREADS) k_vb_box(VoxelBvhParams P)
@@ -285,6 +331,7 @@ __device__ __forceinline__ bool vb_cell_ok(float v)
     return v >= -VB_CELL_LIMIT && v <= VB_CELL_LIMIT; // false for NaN
 }
 
+template <bool XF>
 __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
 {
     // compute_world_to_voxel (voxelbvh_gaussians_to_ijkl.slang:111-118)
@@ -325,18 +372,18 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
     uint32_t nkeys = 0;
     if (ok)
     {
-        // level search (voxelbvh_gaussians_to_ijkl.slang:187-229); the count
-        // stops at 9 since only "more than 8" matters
+        // level search (voxelbvh_gaussians_to_ijkl.slang:187-229): only
+        // "more than 8 overlap" matters, so a level whose box holds at most 8
+        // cells needs no test, and a count stops at 9
         uint32_t level = 11u, last_good = 11u;
         while (true)
         {
-            const int msk = ~((1 << level) - 1), st = 1 << level;
-            uint32_t count = 0;
-            for (int i = lo[0] & msk; i <= (hi[0] & msk) && count <= 8u; i += st)
-                for (int j = lo[1] & msk; j <= (hi[1] & msk) && count <= 8u; j += st)
-                    for (int k = lo[2] & msk; k <= (hi[2] & msk) && count <= 8u; k += st)
-                        count += vb_overlap(P, G, w2v, i, j, k, level) ? 1u : 0u;
-            if (count > 8u)
+            const int msk = ~((1 << level) - 1);
+            int64_t cells = 1;
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                cells *= (int64_t)(((hi[a] & msk) - (lo[a] & msk)) >> level) + 1;
+            if (cells > 8 && vb_scan_level<false, XF>(P, G, w2v, lo, hi, level, 9u, key) > 8u)
             {
                 level = last_good;
                 break;
@@ -347,23 +394,24 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
             level -= 1u;
         }
         // emission: the first 8 overlapping cells in i, j, k loop order
-        const int msk = ~((1 << level) - 1), st = 1 << level;
-        for (int i = lo[0] & msk; i <= (hi[0] & msk) && nkeys < 8u; i += st)
-            for (int j = lo[1] & msk; j <= (hi[1] & msk) && nkeys < 8u; j += st)
-                for (int k = lo[2] & msk; k <= (hi[2] & msk) && nkeys < 8u; k += st)
-                    if (vb_overlap(P, G, w2v, i, j, k, level))
-                    {
-                        const uint64_t kv = ((uint64_t)(int64_t)i << 48) | ((uint64_t)(int64_t)j << 32) |
-                                            ((uint64_t)(int64_t)k << 16) | (uint64_t)level;
-#pragma unroll
-                        for (int s = 0; s < 8; s++) // register-resident insert
-                            if ((uint32_t)s == nkeys)
-                                key[s] = kv;
-                        nkeys++;
-                    }
+        nkeys = vb_scan_level<true, XF>(P, G, w2v, lo, hi, level, 8u, key);
     }
     else
         atomicOr(P.err, ERR_RANGE);
+    // range of the emitted cell coordinates (sizes the compressed sort key)
+    int cmin[3] = { 0x7fffffff, 0x7fffffff, 0x7fffffff }, cmax[3] = { (int)0x80000000, (int)0x80000000, (int)0x80000000 };
+#pragma unroll
+    for (int s = 0; s < 8; s++)
+        if ((uint32_t)s < nkeys)
+        {
+            const int c[3] = { (int)(int16_t)(key[s] >> 48), (int)(int16_t)(key[s] >> 32), (int)(int16_t)(key[s] >> 16) };
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+            {
+                cmin[a] = min(cmin[a], c[a]);
+                cmax[a] = max(cmax[a], c[a]);
+            }
+        }
     ulonglong2* kd = reinterpret_cast<ulonglong2*>(P.keys + 8 * g);
 #pragma unroll
     for (int s = 0; s < 4; s++)
@@ -372,26 +420,40 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
     uint4* idd = reinterpret_cast<uint4*>(P.ids + 8 * g);
     idd[0] = make_uint4(nkeys > 0 ? id : ~0u, nkeys > 1 ? id : ~0u, nkeys > 2 ? id : ~0u, nkeys > 3 ? id : ~0u);
     idd[1] = make_uint4(nkeys > 4 ? id : ~0u, nkeys > 5 ? id : ~0u, nkeys > 6 ? id : ~0u, nkeys > 7 ? id : ~0u);
+    const uint32_t active = __activemask();
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const int wmn = __reduce_min_sync(active, cmin[a]), wmx = __reduce_max_sync(active, cmax[a]);
+        if ((threadIdx.x & 31) == __ffs(active) - 1)
+        {
+            if (wmn != 0x7fffffff)
+                atomicMin(&P.cell_minmax[a], wmn);
+            if (wmx != (int)0x80000000)
+                atomicMax(&P.cell_minmax[3 + a], wmx);
+        }
+    }
 }
 
 // starts (key differs from its predecessor) of one 2048-key tile, per thread 8
 // consecutive keys
-__device__ __forceinline__ uint32_t vb_tile_flags(const uint64_t* keys, int64_t N, int64_t i0, uint32_t& first,
+template <class K>
+__device__ __forceinline__ uint32_t vb_tile_flags(const K* keys, int64_t N, int64_t i0, uint32_t& first,
                                                   uint32_t& last)
 {
     first = 0;
     last = 0;
     if (i0 >= N)
         return 0;
-    uint64_t prev = i0 > 0 ? keys[i0 - 1] : 0;
-    uint64_t cur = keys[i0];
+    K prev = i0 > 0 ? keys[i0 - 1] : K(0);
+    K cur = keys[i0];
 #pragma unroll
     for (int s = 0; s < 8; s++)
     {
         const int64_t i = i0 + s;
         if (i >= N)
             break;
-        const uint64_t next = i + 1 < N ? keys[i + 1] : ~cur;
+        const K next = i + 1 < N ? keys[i + 1] : K(~cur);
         if (i == 0 || cur != prev)
             first |= 1u << s;
         if (cur != next)
@@ -402,7 +464,8 @@ __device__ __forceinline__ uint32_t vb_tile_flags(const uint64_t* keys, int64_t 
     return (uint32_t)__popc(first);
 }
 
-__global__ void __launch_bounds__(VB_THREADS) k_vb_range_count(const uint64_t* keys, int64_t N, uint64_t* counts)
+template <class K>
+__global__ void __launch_bounds__(VB_THREADS) k_vb_range_count(const K* keys, int64_t N, uint64_t* counts)
 {
     __shared__ uint32_t s_w[VB_THREADS / 32];
     const int64_t i0 = (int64_t)blockIdx.x * VB_TILE + 8 * threadIdx.x;
@@ -421,9 +484,26 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_range_count(const uint64_t* k
     }
 }
 
-__global__ void __launch_bounds__(VB_THREADS) k_vb_range_scatter(const uint64_t* keys, int64_t N,
-                                                                   const uint64_t* offs, const uint64_t* total,
-                                                                   uint32_t* range)
+// 64-bit key of a compressed key (VbRangeParams::bits)
+template <class K>
+__device__ __forceinline__ uint64_t vb_expand(K c, const VbRangeParams& R)
+{
+    if ((uint64_t)c == R.sentinel)
+        return ~0ull;
+    const uint64_t u = (uint64_t)c;
+    const uint64_t level = u & 15u;
+    const uint64_t k = (u >> 4) & ((1ull << R.bits[2]) - 1);
+    const uint64_t j = (u >> (4 + R.bits[2])) & ((1ull << R.bits[1]) - 1);
+    const uint64_t i = u >> (4 + R.bits[2] + R.bits[1]);
+    return (i << 48) | (j << 32) | (k << 16) | level;
+}
+
+// headers [2r] = start, [2r + 1] = end, zeros from the range count on; with
+// R.expand the sorted compressed keys are written out as 64-bit keys, and the
+// ids copied when the sort left them in its second buffer
+template <class K>
+__global__ void __launch_bounds__(VB_THREADS) k_vb_range_scatter(const K* keys, int64_t N, const uint64_t* offs,
+                                                                   const uint64_t* total, VbRangeParams R)
 {
     __shared__ uint64_t s_warp[33];
     const int64_t i0 = (int64_t)blockIdx.x * VB_TILE + 8 * threadIdx.x;
@@ -432,7 +512,7 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_range_scatter(const uint64_t*
     uint64_t tile_total;
     // inclusive count of starts before this thread's first key, minus one
     const int64_t base = (int64_t)offs[blockIdx.x] + (int64_t)block_excl_scan_u64(c, s_warp, tile_total) - 1;
-    const uint64_t R = *total;
+    const uint64_t nr = *total;
     int64_t r = base;
 #pragma unroll
     for (int s = 0; s < 8; s++)
@@ -443,23 +523,49 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_range_scatter(const uint64_t*
         if (first & (1u << s))
         {
             r++;
-            range[2 * r] = (uint32_t)i;
+            R.range[2 * r] = (uint32_t)i;
         }
         if (last & (1u << s))
-            range[2 * r + 1] = (uint32_t)(i + 1);
-        if ((uint64_t)i >= R)
+            R.range[2 * r + 1] = (uint32_t)(i + 1);
+        if ((uint64_t)i >= nr)
         {
-            range[2 * i] = 0u;
-            range[2 * i + 1] = 0u;
+            R.range[2 * i] = 0u;
+            R.range[2 * i + 1] = 0u;
         }
+        if (R.expand)
+            R.keys_out[i] = vb_expand(keys[i], R);
+        if (R.ids_src)
+            R.ids_out[i] = R.ids_src[i];
+    }
+}
+
+// 64-bit keys -> compressed keys: i, j, k in bits[0], bits[1], bits[2] bits
+// above a 4-bit level, the unused slot as all ones (above every cell key,
+// whose level is at most 11).  Order-preserving for cells in [0, 2^bits).
+template <class K>
+__global__ void __launch_bounds__(VB_THREADS) k_vb_compress(const uint64_t* keys, int64_t N, VbRangeParams R,
+                                                              K* out)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const uint64_t u = keys[t];
+        uint64_t c;
+        if (u == ~0ull)
+            c = R.sentinel;
+        else
+        {
+            const uint64_t i = (u >> 48) & 0xffffu, j = (u >> 32) & 0xffffu, k = (u >> 16) & 0xffffu, level = u & 15u;
+            c = (((i << R.bits[1] | j) << R.bits[2] | k) << 4) | level;
+        }
+        out[t] = (K)c;
     }
 }
 
 } // namespace
 
-void launch_vb_init(uint32_t* box_keys, cudaStream_t s)
+void launch_vb_init(uint32_t* box_keys, int* cell_minmax, cudaStream_t s)
 {
-    k_vb_init<<<1, 32, 0, s>>>(box_keys);
+    k_vb_init<<<1, 32, 0, s>>>(box_keys, cell_minmax);
     count_launch();
 }
 
@@ -479,7 +585,10 @@ void launch_vb_ijkl(const VoxelBvhParams& P, cudaStream_t s)
 {
     // one block even for n = 0: it writes the world box
     const int64_t grid = P.n > 0 ? (P.n + VB_THREADS - 1) / VB_THREADS : 1;
-    k_vb_ijkl<<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
+    if (P.has_xform)
+        k_vb_ijkl<true><<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
+    else
+        k_vb_ijkl<false><<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
     count_launch();
 }
 
@@ -488,22 +597,44 @@ int64_t vb_range_tiles(int64_t N)
     return (N + VB_TILE - 1) / VB_TILE;
 }
 
-void launch_vb_range_count(const uint64_t* keys, int64_t N, uint64_t* counts, cudaStream_t s)
+void launch_vb_compress(const uint64_t* keys, int64_t N, const VbRangeParams& R, void* out, int key32, int num_sms,
+                        cudaStream_t s)
 {
-    const int64_t tiles = vb_range_tiles(N);
-    if (tiles == 0)
+    if (N <= 0)
         return;
-    k_vb_range_count<<<(unsigned)tiles, VB_THREADS, 0, s>>>(keys, N, counts);
+    int64_t grid = (N + VB_THREADS - 1) / VB_THREADS;
+    const int64_t cap = (int64_t)num_sms * 16;
+    if (grid > cap)
+        grid = cap;
+    if (key32)
+        k_vb_compress<uint32_t><<<(unsigned)grid, VB_THREADS, 0, s>>>(keys, N, R, (uint32_t*)out);
+    else
+        k_vb_compress<uint64_t><<<(unsigned)grid, VB_THREADS, 0, s>>>(keys, N, R, (uint64_t*)out);
     count_launch();
 }
 
-void launch_vb_range_scatter(const uint64_t* keys, int64_t N, const uint64_t* offs, const uint64_t* total,
-                             uint32_t* range, cudaStream_t s)
+void launch_vb_range_count(const void* keys, int key32, int64_t N, uint64_t* counts, cudaStream_t s)
 {
     const int64_t tiles = vb_range_tiles(N);
     if (tiles == 0)
         return;
-    k_vb_range_scatter<<<(unsigned)tiles, VB_THREADS, 0, s>>>(keys, N, offs, total, range);
+    if (key32)
+        k_vb_range_count<uint32_t><<<(unsigned)tiles, VB_THREADS, 0, s>>>((const uint32_t*)keys, N, counts);
+    else
+        k_vb_range_count<uint64_t><<<(unsigned)tiles, VB_THREADS, 0, s>>>((const uint64_t*)keys, N, counts);
+    count_launch();
+}
+
+void launch_vb_range_scatter(const void* keys, int key32, int64_t N, const uint64_t* offs, const uint64_t* total,
+                             const VbRangeParams& R, cudaStream_t s)
+{
+    const int64_t tiles = vb_range_tiles(N);
+    if (tiles == 0)
+        return;
+    if (key32)
+        k_vb_range_scatter<uint32_t><<<(unsigned)tiles, VB_THREADS, 0, s>>>((const uint32_t*)keys, N, offs, total, R);
+    else
+        k_vb_range_scatter<uint64_t><<<(unsigned)tiles, VB_THREADS, 0, s>>>((const uint64_t*)keys, N, offs, total, R);
     count_launch();
 }
 

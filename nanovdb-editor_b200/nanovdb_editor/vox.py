@@ -68,6 +68,11 @@ class vox_stats_t(Structure):
         ("sort_shape", c_int32),
         ("leaf_pairs", c_int64),
         ("candidate_leaves", c_int64),
+        ("ms_vb_keys", c_float),
+        ("ms_vb_sort", c_float),
+        ("ms_vb_ranges", c_float),
+        ("vb_sort_bits", c_int32),
+        ("vb_launches", c_int64),
     ]
 
     def as_dict(self) -> dict:

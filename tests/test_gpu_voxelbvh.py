@@ -105,6 +105,25 @@ def test_ijkl_large_properties(vox_ctx, oracle_mod):
     assert np.bincount(got["prim_id"][real].astype(np.int64), minlength=cloud.n).max() <= 8
 
 
+def test_ijkl_far_cloud_without_cells(vox_ctx, oracle_mod):
+    # 3e8 from the origin the float cell lattice is coarser than the cloud:
+    # no Gaussian overlaps a cell, every slot is unused (one range), and the
+    # sort is skipped (unused slots are already in order)
+    cloud = W.plain_cloud(2000, 60)
+    cloud["means"][:, 0] += np.float32(3e8)
+    ref = oracle_mod.voxelbvh_ijkl(cloud, 4096)
+    assert ref["ranges"] == 1 and np.all(ref["ijkl"] == SENTINEL)
+    _compare(_run(vox_ctx, cloud, 4096), ref)
+
+
+@pytest.mark.parametrize("offset", [1e6, 1e7])
+def test_ijkl_far_cloud(vox_ctx, oracle_mod, offset):
+    # far from the origin the cell arithmetic rounds coarsely; still bit-exact
+    cloud = W.plain_cloud(2000, 60)
+    cloud["means"][:, 0] += np.float32(offset)
+    _compare(_run(vox_ctx, cloud, 4096), oracle_mod.voxelbvh_ijkl(cloud, 4096))
+
+
 def test_ijkl_signed_zero_world_min(vox_ctx, oracle_mod):
     # a faint Gaussian (opacity < 0.01: a point box) at x = -0 is the world
     # minimum in x: its corners are +0 and -0, and -0 orders first
@@ -145,7 +164,7 @@ def test_ijkl_argument_checks(vox_ctx):
     with pytest.raises(PipelineError):
         _run(vox_ctx, cloud, 0)
     with pytest.raises(PipelineError):
-        _run(vox_ctx, cloud, 65537)
+        _run(vox_ctx, cloud, 4097)
     sing = np.eye(4, dtype=np.float32)
     sing[1, 1] = 0.0
     with pytest.raises(PipelineError):
