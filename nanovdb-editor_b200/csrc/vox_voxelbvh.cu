@@ -49,6 +49,10 @@ namespace
 constexpr int VB_THREADS = 256;
 constexpr int VB_TILE = 2048; // keys per range tile (8 per thread)
 constexpr float VB_CELL_LIMIT = 65536.f;
+// a level whose cell box exceeds this is reported (VOX_ERR_RANGE) instead of
+// searched: it bounds the search, and no Gaussian whose box is its own
+// ellipsoid's reaches it (more than 8 of its cells overlap long before)
+constexpr int64_t VB_MAX_CELLS = 1ll << 24;
 
 __device__ __forceinline__ uint32_t vb_fkey(float f)
 {
@@ -376,6 +380,7 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
         // "more than 8 overlap" matters, so a level whose box holds at most 8
         // cells needs no test, and a count stops at 9
         uint32_t level = 11u, last_good = 11u;
+        bool bounded = true;
         while (true)
         {
             const int msk = ~((1 << level) - 1);
@@ -383,6 +388,11 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
 #pragma unroll
             for (int a = 0; a < 3; a++)
                 cells *= (int64_t)(((hi[a] & msk) - (lo[a] & msk)) >> level) + 1;
+            if (cells > VB_MAX_CELLS)
+            {
+                bounded = false;
+                break;
+            }
             if (cells > 8 && vb_scan_level<false, XF>(P, G, w2v, lo, hi, level, 9u, key) > 8u)
             {
                 level = last_good;
@@ -394,7 +404,10 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
             level -= 1u;
         }
         // emission: the first 8 overlapping cells in i, j, k loop order
-        nkeys = vb_scan_level<true, XF>(P, G, w2v, lo, hi, level, 8u, key);
+        if (bounded)
+            nkeys = vb_scan_level<true, XF>(P, G, w2v, lo, hi, level, 8u, key);
+        else
+            atomicOr(P.err, ERR_RANGE);
     }
     else
         atomicOr(P.err, ERR_RANGE);

@@ -915,6 +915,13 @@ int64_t ov_voxelbvh_ijkl(int64_t n, const float* means, const float* opacities, 
         while (level < 12u)
         {
             const int32_t msk = ~((1 << level) - 1), st = 1 << level;
+            /* a level of more than 2^24 cells: an error, not a search (the
+             * device bounds its search the same way) */
+            int64_t cells = 1;
+            for (int a = 0; a < 3; a++)
+                cells *= (int64_t)(((hi[a] & msk) - (lo[a] & msk)) >> level) + 1;
+            if (cells > (1ll << 24))
+                return -1;
             uint32_t count = 0;
             for (int32_t i = lo[0] & msk; i <= (hi[0] & msk); i += st)
                 for (int32_t j = lo[1] & msk; j <= (hi[1] & msk); j += st)
