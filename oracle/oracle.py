@@ -74,7 +74,7 @@ def lib():
         L.ov_smooth_grad64.argtypes = [c_void_p] + [c_void_p] * 5 + [c_int] + [c_void_p] * 7
         L.ov_smooth_loss64.restype = ctypes.c_double
         L.ov_smooth_loss64.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
-        L.ov_voxelbvh_ijkl.argtypes = [c_int64] + [c_void_p] * 4 + [ctypes.c_uint32] + [c_void_p] * 6
+        L.ov_voxelbvh_ijkl.argtypes = [c_int64] + [c_void_p] * 4 + [ctypes.c_uint32] + [c_void_p] * 6 + [c_int]
         L.ov_voxelbvh_ijkl.restype = c_int64
         _LIB = L
     return _LIB
@@ -190,7 +190,7 @@ def hier_key(i, j, k) -> int:
     return int(lib().ov_hier_key(int(i), int(j), int(k)))
 
 
-def voxelbvh_ijkl(cloud, resolution: int, transform=None, transform_inv=None):
+def voxelbvh_ijkl(cloud, resolution: int, transform=None, transform_inv=None, nthreads=None):
     """VoxelBVH Gaussian ingestion (raster/VoxelBVH.cpp:1225-1435) of an
     activated cloud: sorted 64-bit cell keys, their Gaussian ids, the
     [start, end) header of every distinct key (zeros past `ranges`) and the
@@ -206,5 +206,6 @@ def voxelbvh_ijkl(cloud, resolution: int, transform=None, transform_inv=None):
     box = np.empty(6, np.float32)
     r = lib().ov_voxelbvh_ijkl(n, means.ctypes.data, o.ctypes.data, q.ctypes.data, s.ctypes.data, int(resolution),
                                None if T is None else T.ctypes.data, None if Ti is None else Ti.ctypes.data,
-                               keys.ctypes.data, ids.ctypes.data, rng.ctypes.data, box.ctypes.data)
+                               keys.ctypes.data, ids.ctypes.data, rng.ctypes.data, box.ctypes.data,
+                               int(nthreads or max(1, min(16, os.cpu_count() or 1))))
     return {"ijkl": keys, "prim_id": ids, "range": rng, "ranges": int(r), "world_bbox": box}

@@ -855,27 +855,181 @@ static int vb_overlap(const float* mean, const float* q_wxyz, const float* scale
     return dist2 > 0.f;
 }
 
+/* keys of Gaussian g (voxelbvh_gaussians_to_ijkl.slang main); 0 = error */
+static int vb_gauss_keys(int64_t g, const float* means, const float* opacities, const float* quats_wxyz,
+                         const float* scales, const float* T, const float* Tinv, float sc, const float w2v[4],
+                         uint64_t* ijkl, uint32_t* prim_id)
+{
+    const float* mu = &means[3 * g];
+    const float* q = &quats_wxyz[4 * g];
+    const float* s = &scales[3 * g];
+    const float op = opacities[g];
+    float mn[3], mx[3];
+    if (!vb_gauss_aabb(mu, q, s, op, T, mn, mx))
+        return 0;
+    int32_t lo[3], hi[3];
+    for (int a = 0; a < 3; a++)
+    {
+        const float fl = floorf(VOX_FADD(VOX_FMUL(sc, mn[a]), w2v[a]));
+        const float fh = floorf(VOX_FADD(VOX_FMUL(sc, mx[a]), w2v[a]));
+        /* cells beyond +-65536 (non-finite input, zero-size world box):
+         * an error, as the device reports it, not an unbounded search */
+        if (!(fl >= -65536.f && fl <= 65536.f && fh >= -65536.f && fh <= 65536.f))
+            return 0;
+        lo[a] = (int32_t)fl;
+        hi[a] = (int32_t)fh;
+    }
+    uint32_t level = 11u, last_good = 11u;
+    while (level < 12u)
+    {
+        const int32_t msk = ~((1 << level) - 1), st = 1 << level;
+        /* a level of more than 2^24 cells: an error, not a search (the
+         * device bounds its search the same way) */
+        int64_t cells = 1;
+        for (int a = 0; a < 3; a++)
+            cells *= (int64_t)(((hi[a] & msk) - (lo[a] & msk)) >> level) + 1;
+        if (cells > (1ll << 24))
+            return 0;
+        uint32_t count = 0;
+        for (int32_t i = lo[0] & msk; i <= (hi[0] & msk); i += st)
+            for (int32_t j = lo[1] & msk; j <= (hi[1] & msk); j += st)
+                for (int32_t k = lo[2] & msk; k <= (hi[2] & msk); k += st)
+                {
+                    const int32_t c[3] = { i, j, k };
+                    count += (uint32_t)vb_overlap(mu, q, s, op, w2v, c, level, Tinv);
+                }
+        if (count > 8u)
+        {
+            level = last_good;
+            break;
+        }
+        if (level == 0u)
+            break;
+        last_good = level;
+        level -= 1u;
+    }
+    uint32_t sub = 0;
+    {
+        const int32_t msk = ~((1 << level) - 1), st = 1 << level;
+        for (int32_t i = lo[0] & msk; i <= (hi[0] & msk); i += st)
+            for (int32_t j = lo[1] & msk; j <= (hi[1] & msk); j += st)
+                for (int32_t k = lo[2] & msk; k <= (hi[2] & msk); k += st)
+                {
+                    const int32_t c[3] = { i, j, k };
+                    if (sub < 8u && vb_overlap(mu, q, s, op, w2v, c, level, Tinv))
+                    {
+                        ijkl[8 * g + sub] = ((uint64_t)(int64_t)i << 48) | ((uint64_t)(int64_t)j << 32) |
+                                            ((uint64_t)(int64_t)k << 16) | (uint64_t)level;
+                        prim_id[8 * g + sub] = (uint32_t)g;
+                        sub++;
+                    }
+                }
+    }
+    for (; sub < 8u; sub++)
+    {
+        ijkl[8 * g + sub] = ~0ull;
+        prim_id[8 * g + sub] = ~0u;
+    }
+
+    return 1;
+}
+
+typedef struct
+{
+    int64_t g0, g1;
+    const float *means, *opacities, *quats, *scales, *T, *Tinv;
+    float sc, w2v[4];
+    uint64_t* ijkl;
+    uint32_t* prim_id;
+    float mn[3], mx[3];
+    int err;
+} vbjob_t;
+
+static void* vb_box_worker(void* arg)
+{
+    vbjob_t* J = (vbjob_t*)arg;
+    for (int a = 0; a < 3; a++)
+    {
+        J->mn[a] = vox_u2f(0x7f800000u);
+        J->mx[a] = -vox_u2f(0x7f800000u);
+    }
+    for (int64_t g = J->g0; g < J->g1; g++)
+    {
+        float mn[3], mx[3];
+        if (!vb_gauss_aabb(&J->means[3 * g], &J->quats[4 * g], &J->scales[3 * g], J->opacities[g], J->T, mn, mx))
+        {
+            J->err = 1;
+            return NULL;
+        }
+        for (int a = 0; a < 3; a++)
+        {
+            J->mn[a] = vb_fmin(mn[a], J->mn[a]);
+            J->mx[a] = vb_fmax(mx[a], J->mx[a]);
+        }
+    }
+    return NULL;
+}
+
+static void* vb_keys_worker(void* arg)
+{
+    vbjob_t* J = (vbjob_t*)arg;
+    for (int64_t g = J->g0; g < J->g1 && !J->err; g++)
+        if (!vb_gauss_keys(g, J->means, J->opacities, J->quats, J->scales, J->T, J->Tinv, J->sc, J->w2v, J->ijkl,
+                           J->prim_id))
+            J->err = 1;
+    return NULL;
+}
+
 int64_t ov_voxelbvh_ijkl(int64_t n, const float* means, const float* opacities, const float* quats_wxyz,
                          const float* scales, uint32_t resolution, const float* T, const float* Tinv,
-                         uint64_t* ijkl, uint32_t* prim_id, uint32_t* range, float* world_bbox)
+                         uint64_t* ijkl, uint32_t* prim_id, uint32_t* range, float* world_bbox, int nthreads)
 {
-    /* world bbox (bbox_reduce1/2) */
+    if (nthreads < 1)
+        nthreads = 1;
+    if ((int64_t)nthreads > n)
+        nthreads = n > 0 ? (int)n : 1;
+    vbjob_t* jobs = (vbjob_t*)calloc((size_t)nthreads, sizeof(vbjob_t));
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)nthreads);
+    for (int t = 0; t < nthreads; t++)
+    {
+        vbjob_t* J = &jobs[t];
+        J->g0 = n * t / nthreads;
+        J->g1 = n * (t + 1) / nthreads;
+        J->means = means;
+        J->opacities = opacities;
+        J->quats = quats_wxyz;
+        J->scales = scales;
+        J->T = T;
+        J->Tinv = Tinv;
+        J->ijkl = ijkl;
+        J->prim_id = prim_id;
+    }
+    /* world bbox (bbox_reduce1/2): minima / maxima in a total order, so the
+     * split over threads does not change the result */
+    for (int t = 0; t < nthreads; t++)
+        pthread_create(&th[t], NULL, vb_box_worker, &jobs[t]);
+    int err = 0;
     float wmin[3], wmax[3];
     for (int a = 0; a < 3; a++)
     {
         wmin[a] = vox_u2f(0x7f800000u);
         wmax[a] = -vox_u2f(0x7f800000u);
     }
-    for (int64_t g = 0; g < n; g++)
+    for (int t = 0; t < nthreads; t++)
     {
-        float mn[3], mx[3];
-        if (!vb_gauss_aabb(&means[3 * g], &quats_wxyz[4 * g], &scales[3 * g], opacities[g], T, mn, mx))
-            return -1;
+        pthread_join(th[t], NULL);
+        err |= jobs[t].err;
         for (int a = 0; a < 3; a++)
         {
-            wmin[a] = vb_fmin(mn[a], wmin[a]);
-            wmax[a] = vb_fmax(mx[a], wmax[a]);
+            wmin[a] = vb_fmin(jobs[t].mn[a], wmin[a]);
+            wmax[a] = vb_fmax(jobs[t].mx[a], wmax[a]);
         }
+    }
+    if (err)
+    {
+        free(jobs);
+        free(th);
+        return -1;
     }
     for (int a = 0; a < 3; a++)
     {
@@ -889,80 +1043,23 @@ int64_t ov_voxelbvh_ijkl(int64_t n, const float* means, const float* opacities, 
     const float sc = VOX_FDIV((float)(resolution - 1u), dmax);
     const float w2v[4] = { VOX_FADD(VOX_FMUL(-wmin[0], sc), 0.5f), VOX_FADD(VOX_FMUL(-wmin[1], sc), 0.5f),
                            VOX_FADD(VOX_FMUL(-wmin[2], sc), 0.5f), sc };
-    const int64_t nv = 8 * n;
-    for (int64_t g = 0; g < n; g++)
+    for (int t = 0; t < nthreads; t++)
     {
-        const float* mu = &means[3 * g];
-        const float* q = &quats_wxyz[4 * g];
-        const float* s = &scales[3 * g];
-        const float op = opacities[g];
-        float mn[3], mx[3];
-        if (!vb_gauss_aabb(mu, q, s, op, T, mn, mx))
-            return -1;
-        int32_t lo[3], hi[3];
-        for (int a = 0; a < 3; a++)
-        {
-            const float fl = floorf(VOX_FADD(VOX_FMUL(sc, mn[a]), w2v[a]));
-            const float fh = floorf(VOX_FADD(VOX_FMUL(sc, mx[a]), w2v[a]));
-            /* cells beyond +-65536 (non-finite input, zero-size world box):
-             * an error, as the device reports it, not an unbounded search */
-            if (!(fl >= -65536.f && fl <= 65536.f && fh >= -65536.f && fh <= 65536.f))
-                return -1;
-            lo[a] = (int32_t)fl;
-            hi[a] = (int32_t)fh;
-        }
-        uint32_t level = 11u, last_good = 11u;
-        while (level < 12u)
-        {
-            const int32_t msk = ~((1 << level) - 1), st = 1 << level;
-            /* a level of more than 2^24 cells: an error, not a search (the
-             * device bounds its search the same way) */
-            int64_t cells = 1;
-            for (int a = 0; a < 3; a++)
-                cells *= (int64_t)(((hi[a] & msk) - (lo[a] & msk)) >> level) + 1;
-            if (cells > (1ll << 24))
-                return -1;
-            uint32_t count = 0;
-            for (int32_t i = lo[0] & msk; i <= (hi[0] & msk); i += st)
-                for (int32_t j = lo[1] & msk; j <= (hi[1] & msk); j += st)
-                    for (int32_t k = lo[2] & msk; k <= (hi[2] & msk); k += st)
-                    {
-                        const int32_t c[3] = { i, j, k };
-                        count += (uint32_t)vb_overlap(mu, q, s, op, w2v, c, level, Tinv);
-                    }
-            if (count > 8u)
-            {
-                level = last_good;
-                break;
-            }
-            if (level == 0u)
-                break;
-            last_good = level;
-            level -= 1u;
-        }
-        uint32_t sub = 0;
-        {
-            const int32_t msk = ~((1 << level) - 1), st = 1 << level;
-            for (int32_t i = lo[0] & msk; i <= (hi[0] & msk); i += st)
-                for (int32_t j = lo[1] & msk; j <= (hi[1] & msk); j += st)
-                    for (int32_t k = lo[2] & msk; k <= (hi[2] & msk); k += st)
-                    {
-                        const int32_t c[3] = { i, j, k };
-                        if (sub < 8u && vb_overlap(mu, q, s, op, w2v, c, level, Tinv))
-                        {
-                            ijkl[8 * g + sub] = ((uint64_t)(int64_t)i << 48) | ((uint64_t)(int64_t)j << 32) |
-                                                ((uint64_t)(int64_t)k << 16) | (uint64_t)level;
-                            prim_id[8 * g + sub] = (uint32_t)g;
-                            sub++;
-                        }
-                    }
-        }
-        for (; sub < 8u; sub++)
-        {
-            ijkl[8 * g + sub] = ~0ull;
-            prim_id[8 * g + sub] = ~0u;
-        }
+        jobs[t].sc = sc;
+        for (int a = 0; a < 4; a++)
+            jobs[t].w2v[a] = w2v[a];
+        pthread_create(&th[t], NULL, vb_keys_worker, &jobs[t]);
     }
+    for (int t = 0; t < nthreads; t++)
+    {
+        pthread_join(th[t], NULL);
+        err |= jobs[t].err;
+    }
+    free(jobs);
+    free(th);
+    if (err)
+        return -1;
+    const int64_t nv = 8 * n;
     /* stable sort by the full 64-bit key */
     radix_sort_pairs(ijkl, prim_id, nv, 64);
     /* ranges: [start, end) of every distinct key, at the key's rank; the rest 0 */

@@ -106,7 +106,7 @@ double ov_smooth_loss64(void* h, const double* theta, int raw, const double* gra
  * p' = [p 1] T, or NULL for the identity. */
 int64_t ov_voxelbvh_ijkl(int64_t n, const float* means, const float* opacities, const float* quats_wxyz,
                          const float* scales, uint32_t resolution, const float* T, const float* Tinv,
-                         uint64_t* ijkl, uint32_t* prim_id, uint32_t* range, float* world_bbox);
+                         uint64_t* ijkl, uint32_t* prim_id, uint32_t* range, float* world_bbox, int nthreads);
 
 #ifdef __cplusplus
 }

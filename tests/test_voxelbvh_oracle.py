@@ -138,6 +138,18 @@ def test_oracle_invariants(oracle_mod, res):
     assert np.all(m >= box[:3]) and np.all(m <= box[3:])
 
 
+def test_oracle_thread_count_independent(oracle_mod):
+    # the world box is a total-order min / max and every Gaussian owns its
+    # 8 slots, so splitting the Gaussians over threads changes nothing
+    cloud = W.cluster_cloud(5000, 42, clusters=8)
+    one = oracle_mod.voxelbvh_ijkl(cloud, 1024, nthreads=1)
+    for t in (2, 7):
+        many = oracle_mod.voxelbvh_ijkl(cloud, 1024, nthreads=t)
+        assert many["ranges"] == one["ranges"]
+        for k in ("ijkl", "prim_id", "range", "world_bbox"):
+            np.testing.assert_array_equal(many[k], one[k])
+
+
 def test_oracle_rejects_unbounded_cells(oracle_mod):
     cloud = W.plain_cloud(50, 43)
     cloud["means"][7, 1] = np.nan
