@@ -1422,8 +1422,10 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
     int key32 = 0, sort_bits = 0;
     const void* sorted_keys = d_ijkl;
     const bool any_cell = mm[3] >= mm[0];
+    // VOX_VB_SORT64=1 sorts the 64-bit keys even when they compress (testing)
+    const char* force64 = getenv("VOX_VB_SORT64");
     const bool compress = any_cell && mm[0] >= 0 && mm[1] >= 0 && mm[2] >= 0 && mm[3] < 65536 && mm[4] < 65536 &&
-                          mm[5] < 65536;
+                          mm[5] < 65536 && !(force64 && force64[0] == '1');
     cudaEventRecord(ctx->timers.ev[2], s);
     if (N > 1 && any_cell)
     {

@@ -105,6 +105,21 @@ def test_ijkl_large_properties(vox_ctx, oracle_mod):
     assert np.bincount(got["prim_id"][real].astype(np.int64), minlength=cloud.n).max() <= 8
 
 
+def test_ijkl_full_key_sort_path(vox_ctx, oracle_mod, monkeypatch):
+    # the 64-bit key sort (taken when a cell lies outside [0, 2^15)) gives
+    # the same result as the compressed-key sort
+    cloud = W.cluster_cloud(30_000, 25, clusters=8)
+    ref = oracle_mod.voxelbvh_ijkl(cloud, 4096)
+    monkeypatch.setenv("VOX_VB_SORT64", "1")
+    got = _run(vox_ctx, cloud, 4096)
+    assert vox_ctx.stats()["vb_sort_bits"] == 64
+    _compare(got, ref)
+    monkeypatch.delenv("VOX_VB_SORT64")
+    got = _run(vox_ctx, cloud, 4096)
+    assert vox_ctx.stats()["vb_sort_bits"] < 64
+    _compare(got, ref)
+
+
 def test_ijkl_far_cloud_without_cells(vox_ctx, oracle_mod):
     # 3e8 from the origin the float cell lattice is coarser than the cloud:
     # no Gaussian overlaps a cell, every slot is unused (one range), and the
