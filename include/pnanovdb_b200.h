@@ -398,10 +398,40 @@ PNANOVDB_API int vox_backward(vox_context_t* ctx, const vox_gaussians_t* gaussia
 PNANOVDB_API int vox_global_scan_u64(vox_context_t* ctx, const uint64_t* d_in, uint64_t* d_out, int64_t n,
                                      int inclusive, uint64_t* d_total);
 
+/* replaces pnanovdb_parallel_primitives_t::global_scan
+ * (nanovdb_editor/putil/ParallelPrimitives.h:33-39, raster/ParallelPrimitives.cpp:276-286):
+ * scan of n uint32 values, sums wrapping mod 2^32, inclusive when `inclusive`
+ * is non-zero (the reference's), else exclusive; *d_total (device, may be
+ * NULL) receives the sum mod 2^32.  The reference's dispatch_count repeats
+ * the same scan and has no counterpart. */
+PNANOVDB_API int vox_global_scan_u32(vox_context_t* ctx, const uint32_t* d_in, uint32_t* d_out, int64_t n,
+                                     int inclusive, uint32_t* d_total);
+
+/* replaces pnanovdb_parallel_primitives_t::global_scan_max
+ * (ParallelPrimitives.h:49-55, ParallelPrimitives.cpp:300-310): inclusive
+ * running maximum of n uint32 values. */
+PNANOVDB_API int vox_global_scan_max_u32(vox_context_t* ctx, const uint32_t* d_in, uint32_t* d_out, int64_t n);
+
+/* replaces pnanovdb_parallel_primitives_t::radix_sort
+ * (ParallelPrimitives.h:57-64, ParallelPrimitives.cpp:347-525): stable sort
+ * of n (32-bit key, 32-bit value) device pairs in place by key bits
+ * [0, key_bit_count); higher key bits take no part in the order. */
+PNANOVDB_API int vox_radix_sort_u32(vox_context_t* ctx, uint32_t* d_keys, uint32_t* d_vals, int64_t n,
+                                    uint32_t key_bit_count);
+
+/* replaces pnanovdb_parallel_primitives_t::radix_sort_dual_key
+ * (ParallelPrimitives.h:66-75, ParallelPrimitives.cpp:527-683), the tile sort
+ * of raster_gaussian_2d (raster/Raster2D.cpp:495-506): stable sort of n
+ * (low key, high key, value) uint32 triples in place by (high key bits
+ * [0, key_high_bit_count), low key bits [0, key_low_bit_count)). */
+PNANOVDB_API int vox_radix_sort_dual_key(vox_context_t* ctx, uint32_t* d_keys_low, uint32_t* d_keys_high,
+                                         uint32_t* d_vals, int64_t n, uint32_t key_low_bit_count,
+                                         uint32_t key_high_bit_count);
+
 /* replaces pnanovdb_parallel_primitives_t::radix_sort_key64
  * (nanovdb_editor/putil/ParallelPrimitives.h:77-84, raster/ParallelPrimitives.cpp:685-869):
  * stable sort of n (64-bit key, 32-bit value) device pairs in place by key
- * bits [0, key_bit_count). */
+ * bits [0, key_bit_count); higher key bits take no part in the order. */
 PNANOVDB_API int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n,
                                       uint32_t key_bit_count);
 

@@ -73,7 +73,8 @@ struct vox_context_t
     DevBuf hier_keys;
     DevBuf prim_keys_alt, prim_vals_alt; // ping-pong buffers of vox_radix_sort_key64
     DevBuf vb_work; // VoxelBVH ingestion: world-box keys, range tile counts
-    DevBuf vb_keys; // VoxelBVH ingestion: compressed sort keys
+    DevBuf vb_keys; // VoxelBVH ingestion: compressed sort keys (also the dual-key sort's keys)
+    DevBuf dual_idx; // dual-key sort: original indices
     uint64_t* hscal = nullptr; // pinned mirror
     Epochs scan_epochs, run_epochs, sort_epochs;
     int check_sort = 0; // VOX_CHECK_SORT=1: validate key order after every sort
@@ -989,7 +990,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
-                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->vb_keys, &ctx->cloud_start,
+                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->vb_keys, &ctx->dual_idx, &ctx->cloud_start,
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_mask, &ctx->lc_off,
                       &ctx->cand_org, &ctx->tile_g0, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
@@ -1253,6 +1254,107 @@ int vox_global_scan_u64(vox_context_t* ctx, const uint64_t* d_in, uint64_t* d_ou
                        ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s),
                        (uint32_t*)(sc + SC_SCRATCH), (int*)(sc + SC_ERR), ctx->num_sms, s);
     return sync_scalars(ctx, "vox_global_scan_u64");
+}
+
+int vox_global_scan_u32(vox_context_t* ctx, const uint32_t* d_in, uint32_t* d_out, int64_t n, int inclusive,
+                        uint32_t* d_total)
+{
+    if (!ctx || n < 0 || (n > 0 && (!d_in || !d_out)))
+        return VOX_ERR_ARGS;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(n > 512 ? n : 512) * 2))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    uint64_t* status = (uint64_t*)ctx->scan_status.p;
+    scan_u32(d_in, d_out, n, inclusive ? 1 : 0, 0, sc + SC_F, status,
+             ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s), (uint32_t*)(sc + SC_SCRATCH),
+             (int*)(sc + SC_ERR), s);
+    if (d_total)
+        cudaMemcpyAsync(d_total, sc + SC_F, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s); // low half: mod 2^32
+    return sync_scalars(ctx, "vox_global_scan_u32");
+}
+
+int vox_global_scan_max_u32(vox_context_t* ctx, const uint32_t* d_in, uint32_t* d_out, int64_t n)
+{
+    if (!ctx || n < 0 || (n > 0 && (!d_in || !d_out)))
+        return VOX_ERR_ARGS;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) ||
+        !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(n > 512 ? n : 512) * 2))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    uint64_t* status = (uint64_t*)ctx->scan_status.p;
+    scan_u32(d_in, d_out, n, 1, 1, sc + SC_F, status,
+             ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s), (uint32_t*)(sc + SC_SCRATCH),
+             (int*)(sc + SC_ERR), s);
+    return sync_scalars(ctx, "vox_global_scan_max_u32");
+}
+
+int vox_radix_sort_u32(vox_context_t* ctx, uint32_t* d_keys, uint32_t* d_vals, int64_t n, uint32_t key_bit_count)
+{
+    if (!ctx || n < 0 || (n > 0 && (!d_keys || !d_vals)) || key_bit_count > 32)
+        return VOX_ERR_ARGS;
+    if (n <= 1 || key_bit_count == 0)
+        return VOX_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) ||
+        !ensure(ctx, ctx->prim_keys_alt, 4 * (size_t)n) || !ensure(ctx, ctx->prim_vals_alt, 4 * (size_t)n) ||
+        !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(n, 4)))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    int in_alt = sort_pairs_u32(d_keys, d_vals, (uint32_t*)ctx->prim_keys_alt.p, (uint32_t*)ctx->prim_vals_alt.p, n,
+                                (int)key_bit_count, ctx->sort_ws.p, &ctx->sort_epochs, (int*)(sc + SC_ERR),
+                                ctx->num_sms, s, ctx->tuning);
+    if (in_alt)
+    {
+        cudaMemcpyAsync(d_keys, ctx->prim_keys_alt.p, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d_vals, ctx->prim_vals_alt.p, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    }
+    return sync_scalars(ctx, "vox_radix_sort_u32");
+}
+
+int vox_radix_sort_dual_key(vox_context_t* ctx, uint32_t* d_keys_low, uint32_t* d_keys_high, uint32_t* d_vals,
+                            int64_t n, uint32_t key_low_bit_count, uint32_t key_high_bit_count)
+{
+    if (!ctx || n < 0 || (n > 0 && (!d_keys_low || !d_keys_high || !d_vals)) || key_low_bit_count > 32 ||
+        key_high_bit_count > 32 || n > 0xffffffffll)
+        return VOX_ERR_ARGS;
+    const int bits = (int)(key_low_bit_count + key_high_bit_count);
+    if (n <= 1 || bits == 0)
+        return VOX_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4) || !ensure(ctx, ctx->vb_keys, 8 * (size_t)n) ||
+        !ensure(ctx, ctx->prim_keys_alt, 8 * (size_t)n) || !ensure(ctx, ctx->prim_vals_alt, 4 * (size_t)n) ||
+        !ensure(ctx, ctx->dual_idx, 4 * (size_t)n) || !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(n, 8)))
+        return VOX_ERR_MEMORY;
+    uint64_t* sc = (uint64_t*)ctx->scal.p;
+    int* err = (int*)(sc + SC_ERR);
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    // one stable sort by (high, low): the order of the reference's sort by
+    // the low key then, stably, by the high key (ParallelPrimitives.cpp:527-683)
+    uint64_t* key = (uint64_t*)ctx->vb_keys.p;
+    uint32_t* idx = (uint32_t*)ctx->dual_idx.p;
+    dual_combine(d_keys_low, d_keys_high, n, (int)key_low_bit_count, (int)key_high_bit_count, key, idx, ctx->num_sms, s);
+    const int in_alt = sort_pairs_u64(key, idx, (uint64_t*)ctx->prim_keys_alt.p, (uint32_t*)ctx->prim_vals_alt.p, n,
+                                      bits, ctx->sort_ws.p, &ctx->sort_epochs, err, ctx->num_sms, s, ctx->tuning);
+    const uint32_t* sidx = in_alt ? (const uint32_t*)ctx->prim_vals_alt.p : idx;
+    // copies of the inputs in buffers the sorted indices do not live in
+    uint32_t* low_c = (uint32_t*)ctx->vb_keys.p;
+    uint32_t* high_c = low_c + n;
+    uint32_t* val_c = (uint32_t*)ctx->prim_keys_alt.p;
+    cudaMemcpyAsync(low_c, d_keys_low, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(high_c, d_keys_high, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(val_c, d_vals, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    dual_gather(sidx, n, low_c, high_c, val_c, d_keys_low, d_keys_high, d_vals, err, ctx->num_sms, s);
+    return sync_scalars(ctx, "vox_radix_sort_dual_key");
 }
 
 int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, uint32_t key_bit_count)

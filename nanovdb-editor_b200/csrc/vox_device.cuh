@@ -567,8 +567,10 @@ __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p)
 // Publishes `aggregate` for `tile`, walks predecessors and returns the
 // exclusive prefix.  Every wait is bounded; on timeout *err is set and the
 // partial prefix is returned (the host treats the call as failed).
+// max_op: combine predecessors by maximum instead of sum (a running-max scan)
 __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_t tile, uint64_t aggregate,
-                                                       uint32_t epoch, int* err, size_t stride = 1)
+                                                       uint32_t epoch, int* err, size_t stride = 1,
+                                                       bool max_op = false)
 {
     const uint64_t tag = (uint64_t)epoch << 56;
     if (tile == 0)
@@ -587,18 +589,20 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_
         {
             if (++spins > LB_SPIN_LIMIT)
             {
-                atomicExch(err, 1);
+                atomicOr(err, 1); // ERR_LOOKBACK
                 break;
             }
             __nanosleep(32);
             continue;
         }
-        excl += s & LB_VALUE_MASK;
+        const uint64_t v = s & LB_VALUE_MASK;
+        excl = max_op ? (v > excl ? v : excl) : excl + v;
         if (s & LB_INCL)
             break;
         p--;
     }
-    st_release_u64(&status[tile * stride], tag | LB_INCL | ((excl + aggregate) & LB_VALUE_MASK));
+    const uint64_t incl = max_op ? (aggregate > excl ? aggregate : excl) : excl + aggregate;
+    st_release_u64(&status[tile * stride], tag | LB_INCL | (incl & LB_VALUE_MASK));
     return excl;
 }
 

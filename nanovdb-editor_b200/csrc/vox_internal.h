@@ -66,6 +66,17 @@ size_t scan_status_words(int64_t n);
 void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, uint64_t* total, uint64_t* status,
                         uint32_t epoch, uint32_t* counter, int* err, int num_sms, cudaStream_t s);
 
+// u32 scan (sum mod 2^32, or running maximum with max_op), inclusive or
+// exclusive; *total (u64) receives the sum / maximum
+void scan_u32(const uint32_t* in, uint32_t* out, int64_t n, int inclusive, int max_op, uint64_t* total,
+              uint64_t* status, uint32_t epoch, uint32_t* counter, int* err, cudaStream_t s);
+// dual-key sort helpers: key = (high & mask) << low_bits | (low & mask), idx = i;
+// then low / high / val gathered through the sorted idx from copies
+void dual_combine(const uint32_t* low, const uint32_t* high, int64_t n, int low_bits, int high_bits, uint64_t* key,
+                  uint32_t* idx, int num_sms, cudaStream_t s);
+void dual_gather(const uint32_t* sidx, int64_t n, const uint32_t* low_c, const uint32_t* high_c, const uint32_t* val_c,
+                 uint32_t* low, uint32_t* high, uint32_t* val, int* err, int num_sms, cudaStream_t s);
+
 // ---------------------------------------------------------------- sort ----
 struct SortTuning
 {
@@ -80,7 +91,8 @@ struct SortTuning
     }
 };
 size_t sort_workspace_bytes(int64_t n, int key_bytes);
-// Stable LSD sort of (key, value) pairs by key bits [0, key_bits).  Uses
+// Stable LSD sort of (key, value) pairs by key bits [0, key_bits) (higher
+// bits take no part in the order).  Uses
 // keys_alt / vals_alt as ping-pong buffers; returns 0 if the result is in
 // keys / vals and 1 if it is in keys_alt / vals_alt.
 int sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, int64_t n, int key_bits,

@@ -94,6 +94,171 @@ void scan_exclusive_u64(const uint64_t* in, uint64_t* out, int64_t n, int mode, 
     { k_scan_excl<<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(in, out, n, mode, total, status, epoch, counter, err); count_launch(); }
 }
 
+// u32 scans: the reference's global_scan (sum, wrapping mod 2^32) and
+// global_scan_max (running maximum), inclusive or exclusive; sums are carried
+// in 64 bits (the look-back keeps them mod 2^55, a multiple of 2^32)
+template <bool MAX>
+__device__ __forceinline__ uint64_t scan_op(uint64_t a, uint64_t b)
+{
+    return MAX ? (a > b ? a : b) : a + b;
+}
+
+template <bool MAX>
+__device__ __forceinline__ uint64_t block_excl_scan_op(uint64_t v, uint64_t* s_warp, uint64_t& total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    uint64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o)
+            incl = scan_op<MAX>(incl, t);
+    }
+    if (lane == 31)
+        s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0)
+    {
+        const uint64_t w = lane < nwarps ? s_warp[lane] : 0;
+        uint64_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const uint64_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o)
+                wi = scan_op<MAX>(wi, t);
+        }
+        const uint64_t prev = __shfl_up_sync(0xffffffffu, wi, 1);
+        if (lane < nwarps)
+            s_warp[lane] = lane == 0 ? 0 : prev; // exclusive over warps
+        if (lane == nwarps - 1)
+            s_warp[32] = wi;
+    }
+    __syncthreads();
+    total = s_warp[32];
+    // exclusive within the warp: the inclusive value of the lane before
+    const uint64_t before = __shfl_up_sync(0xffffffffu, incl, 1);
+    const uint64_t r = scan_op<MAX>(s_warp[warp], lane == 0 ? 0 : before);
+    __syncthreads();
+    return r;
+}
+
+template <bool MAX>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, int inclusive,
+                                                           uint64_t* total, uint64_t* status, uint32_t epoch,
+                                                           uint32_t* counter, int* err)
+{
+    __shared__ uint64_t s_warp[33];
+    __shared__ uint64_t s_excl;
+    __shared__ uint32_t s_tile;
+    if (threadIdx.x == 0)
+        s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    const int64_t base = (int64_t)tile * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    uint64_t agg = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+    {
+        const int64_t idx = base + i;
+        v[i] = idx < n ? in[idx] : 0u;
+        agg = scan_op<MAX>(agg, (uint64_t)v[i]);
+    }
+    uint64_t block_total;
+    const uint64_t texcl = block_excl_scan_op<MAX>(agg, s_warp, block_total);
+    if (threadIdx.x == 0)
+        s_excl = lookback_exclusive(status, tile, block_total, epoch, err, 1, MAX);
+    __syncthreads();
+    uint64_t run = scan_op<MAX>(s_excl, texcl);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+    {
+        const int64_t idx = base + i;
+        if (idx < n)
+        {
+            const uint64_t next = scan_op<MAX>(run, (uint64_t)v[i]);
+            out[idx] = (uint32_t)(inclusive ? next : run);
+            run = next;
+            if (idx == n - 1)
+                *total = run;
+        }
+    }
+}
+
+void scan_u32(const uint32_t* in, uint32_t* out, int64_t n, int inclusive, int max_op, uint64_t* total,
+              uint64_t* status, uint32_t epoch, uint32_t* counter, int* err, cudaStream_t s)
+{
+    if (n <= 0)
+    {
+        cudaMemsetAsync(total, 0, sizeof(uint64_t), s);
+        return;
+    }
+    cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+    const int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (max_op)
+        k_scan_u32<true><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(in, out, n, inclusive, total, status, epoch, counter, err);
+    else
+        k_scan_u32<false><<<(unsigned)tiles, SCAN_BLOCK, 0, s>>>(in, out, n, inclusive, total, status, epoch, counter, err);
+    count_launch();
+}
+
+// dual-key sort helpers: (high, low) -> one 64-bit key + original index, and
+// the gather of the three arrays by the sorted indices
+__global__ void k_dual_combine(const uint32_t* low, const uint32_t* high, int64_t n, int low_bits, int high_bits,
+                               uint64_t* key, uint32_t* idx)
+{
+    const uint64_t ml = low_bits >= 32 ? 0xffffffffull : ((1ull << low_bits) - 1);
+    const uint64_t mh = high_bits >= 32 ? 0xffffffffull : ((1ull << high_bits) - 1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+        key[i] = (((uint64_t)high[i] & mh) << low_bits) | ((uint64_t)low[i] & ml);
+        idx[i] = (uint32_t)i;
+    }
+}
+
+__global__ void k_dual_gather(const uint32_t* sidx, int64_t n, const uint32_t* low_c, const uint32_t* high_c,
+                              const uint32_t* val_c, uint32_t* low, uint32_t* high, uint32_t* val, int* err)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+        const uint32_t j = sidx[i];
+        if ((int64_t)j >= n)
+        {
+            atomicOr(err, ERR_BOUNDS);
+            continue;
+        }
+        low[i] = low_c[j];
+        high[i] = high_c[j];
+        val[i] = val_c[j];
+    }
+}
+
+void dual_combine(const uint32_t* low, const uint32_t* high, int64_t n, int low_bits, int high_bits, uint64_t* key,
+                  uint32_t* idx, int num_sms, cudaStream_t s)
+{
+    if (n <= 0)
+        return;
+    int64_t grid = (n + 255) / 256;
+    if (grid > (int64_t)num_sms * 16)
+        grid = (int64_t)num_sms * 16;
+    k_dual_combine<<<(unsigned)grid, 256, 0, s>>>(low, high, n, low_bits, high_bits, key, idx);
+    count_launch();
+}
+
+void dual_gather(const uint32_t* sidx, int64_t n, const uint32_t* low_c, const uint32_t* high_c, const uint32_t* val_c,
+                 uint32_t* low, uint32_t* high, uint32_t* val, int* err, int num_sms, cudaStream_t s)
+{
+    if (n <= 0)
+        return;
+    int64_t grid = (n + 255) / 256;
+    if (grid > (int64_t)num_sms * 16)
+        grid = (int64_t)num_sms * 16;
+    k_dual_gather<<<(unsigned)grid, 256, 0, s>>>(sidx, n, low_c, high_c, val_c, low, high, val, err);
+    count_launch();
+}
+
 // ===================================================================== sort
 // Tile: block threads x items keys (SORT_SHAPES).  One up-front pass computes the
 // digit histograms of every pass (global counts are permutation-invariant);
@@ -159,12 +324,19 @@ __device__ __forceinline__ uint32_t digit_of(K k, int shift, uint32_t mask)
 
 // up-front histogram of every pass's digit (per-CTA shared counters, then
 // one global atomic per bin); counts fit 32 bits for n < 2^32
+// digit width of pass p: `bits`, the last pass only the key bits left, so
+// bits at and above key_bits never take part in the order
+__host__ __device__ __forceinline__ int pass_bits(int p, int bits, int key_bits)
+{
+    const int left = key_bits - p * bits;
+    return left < bits ? left : bits;
+}
+
 template <class K>
-__global__ void __launch_bounds__(512) k_sort_hist(const K* keys, int64_t n, int passes, int bits,
+__global__ void __launch_bounds__(512) k_sort_hist(const K* keys, int64_t n, int passes, int bits, int key_bits,
                                                             uint32_t* hist)
 {
     __shared__ uint32_t s_h[SORT_MAX_PASSES * 256];
-    const uint32_t mask = (1u << bits) - 1u;
     for (int i = threadIdx.x; i < SORT_MAX_PASSES * 256; i += blockDim.x)
         s_h[i] = 0;
     __syncthreads();
@@ -172,7 +344,7 @@ __global__ void __launch_bounds__(512) k_sort_hist(const K* keys, int64_t n, int
     {
         K k = keys[idx];
         for (int p = 0; p < passes; p++)
-            atomicAdd(&s_h[p * 256 + digit_of(k, p * bits, mask)], 1u);
+            atomicAdd(&s_h[p * 256 + digit_of(k, p * bits, (1u << pass_bits(p, bits, key_bits)) - 1u)], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
@@ -377,7 +549,7 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     int64_t need = (n + 511) / 512;
     if (hist_grid > need)
         hist_grid = need;
-    { k_sort_hist<K><<<(unsigned)hist_grid, 512, 0, s>>>(keys, n, passes, bits, w.hist); count_launch(); }
+    { k_sort_hist<K><<<(unsigned)hist_grid, 512, 0, s>>>(keys, n, passes, bits, key_bits, w.hist); count_launch(); }
     { k_sort_bases<<<1, 256, 0, s>>>(w.hist, w.base, passes); count_launch(); }
     const size_t words = sort_status_words(n);
     const int kw = sizeof(K) == 8 ? 1 : 0, sc = size_class(n);
@@ -395,8 +567,8 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
             uint32_t epoch = epochs->next(w.status, words, s);
             cudaMemsetAsync(w.counters + SORT_MAX_PASSES, 0, sizeof(uint32_t), s);
             cudaEventRecord(e0, s);
-            onesweep_pass<K>(t, keys, vals, keys_alt, vals_alt, n, 0, bits, w.base, w.status, epoch,
-                             w.counters + SORT_MAX_PASSES, err, s);
+            onesweep_pass<K>(t, keys, vals, keys_alt, vals_alt, n, 0, pass_bits(0, bits, key_bits), w.base, w.status,
+                             epoch, w.counters + SORT_MAX_PASSES, err, s);
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             float ms = 0.f;
@@ -418,8 +590,8 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     for (int p = 0; p < passes; p++)
     {
         uint32_t epoch = epochs->next(w.status, words, s);
-        onesweep_pass<K>(shape, src_k, src_v, dst_k, dst_v, n, p * bits, bits, w.base + p * 256, w.status, epoch,
-                         w.counters + p, err, s);
+        onesweep_pass<K>(shape, src_k, src_v, dst_k, dst_v, n, p * bits, pass_bits(p, bits, key_bits),
+                         w.base + p * 256, w.status, epoch, w.counters + p, err, s);
         K* tk = src_k;
         src_k = dst_k;
         dst_k = tk;

@@ -108,6 +108,14 @@ def _lib():
         lib.vox_backward.argtypes = [c_void_p, POINTER(vox_gaussians_t)] + [c_void_p] * 7
         lib.vox_radix_sort_key64.restype = c_int
         lib.vox_radix_sort_key64.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_uint32]
+        lib.vox_global_scan_u32.restype = c_int
+        lib.vox_global_scan_u32.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]
+        lib.vox_global_scan_max_u32.restype = c_int
+        lib.vox_global_scan_max_u32.argtypes = [c_void_p, c_void_p, c_void_p, c_int64]
+        lib.vox_radix_sort_u32.restype = c_int
+        lib.vox_radix_sort_u32.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_uint32]
+        lib.vox_radix_sort_dual_key.restype = c_int
+        lib.vox_radix_sort_dual_key.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_uint32, c_uint32]
         lib.vox_voxelbvh_ijkl_from_gaussians.restype = c_int
         lib.vox_voxelbvh_ijkl_from_gaussians.argtypes = [c_void_p] + [c_void_p] * 4 + [c_int64, c_uint32] + [c_void_p] * 5 + [POINTER(c_int64)]
         lib.vox_voxelbvh_transform_inverse.restype = c_int
@@ -300,6 +308,26 @@ class VoxContext:
         out = np.empty(16, np.float32)
         self._check(self.lib.vox_voxelbvh_transform_inverse(m.ctypes.data, out.ctypes.data), "vox_voxelbvh_transform_inverse")
         return out.reshape(4, 4)
+
+    def global_scan_u32(self, d_in, d_out, d_total=None, inclusive: bool = True) -> None:
+        """Scan of CUDA uint32 tensors (int32 storage), sums mod 2^32 (the reference's global_scan)."""
+        n = int(d_in.numel())
+        self._check(self.lib.vox_global_scan_u32(self.handle, _ptr(d_in), _ptr(d_out), n, 1 if inclusive else 0, _ptr(d_total)), "vox_global_scan_u32")
+
+    def global_scan_max_u32(self, d_in, d_out) -> None:
+        """Inclusive running maximum of CUDA uint32 tensors (the reference's global_scan_max)."""
+        n = int(d_in.numel())
+        self._check(self.lib.vox_global_scan_max_u32(self.handle, _ptr(d_in), _ptr(d_out), n), "vox_global_scan_max_u32")
+
+    def radix_sort_u32(self, d_keys, d_vals, key_bits: int = 32) -> None:
+        """Stable in-place sort of CUDA (uint32 key, uint32 value) tensors by key bits [0, key_bits)."""
+        n = int(d_keys.numel())
+        self._check(self.lib.vox_radix_sort_u32(self.handle, _ptr(d_keys), _ptr(d_vals), n, int(key_bits)), "vox_radix_sort_u32")
+
+    def radix_sort_dual_key(self, d_low, d_high, d_vals, low_bits: int = 32, high_bits: int = 32) -> None:
+        """Stable in-place sort of CUDA uint32 (low key, high key, value) tensors by (high, low)."""
+        n = int(d_low.numel())
+        self._check(self.lib.vox_radix_sort_dual_key(self.handle, _ptr(d_low), _ptr(d_high), _ptr(d_vals), n, int(low_bits), int(high_bits)), "vox_radix_sort_dual_key")
 
     def radix_sort_key64(self, d_keys, d_vals, key_bits: int = 64) -> None:
         """Stable in-place sort of CUDA (uint64 key, uint32 value) tensors by key bits [0, key_bits)."""

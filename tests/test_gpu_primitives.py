@@ -66,3 +66,85 @@ def test_sort_partial_key_bits_is_stable(vox_ctx):
     gk = dk.cpu().numpy().view(np.uint64)
     order = np.argsort(keys & np.uint64(255), kind="stable")
     np.testing.assert_array_equal(gk, keys[order])
+
+
+def _dev(a, dtype):
+    import torch
+
+    t = torch.from_numpy(np.ascontiguousarray(a).view(dtype).copy()).cuda()
+    torch.cuda.synchronize()
+    return t
+
+
+@pytest.mark.parametrize("n", [0, 1, 2047, 2049, 700_001])
+@pytest.mark.parametrize("inclusive", [True, False])
+def test_scan_u32_wraps_like_reference(vox_ctx, n, inclusive):
+    # the reference's global_scan: uint32 sums that wrap mod 2^32
+    import torch
+
+    rng = np.random.default_rng(n + 7 * inclusive)
+    x = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    d_in, d_out = _dev(x, np.int32), torch.empty(n, dtype=torch.int32, device="cuda")
+    d_tot = torch.zeros(1, dtype=torch.int32, device="cuda")
+    vox_ctx.global_scan_u32(d_in, d_out, d_tot, inclusive)
+    ref = np.cumsum(x.astype(np.uint64)) & np.uint64(0xFFFFFFFF)
+    if not inclusive and n:
+        ref = np.concatenate([[0], ref[:-1]])
+    np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint32), ref.astype(np.uint32))
+    assert int(d_tot.cpu().numpy().view(np.uint32)[0]) == int(x.astype(np.uint64).sum()) % (1 << 32)
+
+
+@pytest.mark.parametrize("n", [1, 2048, 2049, 1_000_003])
+def test_scan_max_u32(vox_ctx, n):
+    # the reference's global_scan_max: inclusive running maximum
+    import torch
+
+    rng = np.random.default_rng(n)
+    x = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    x[::3] = rng.integers(0, 1000, len(x[::3])).astype(np.uint32)
+    d_in, d_out = _dev(x, np.int32), torch.empty(n, dtype=torch.int32, device="cuda")
+    vox_ctx.global_scan_max_u32(d_in, d_out)
+    np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint32), np.maximum.accumulate(x))
+
+
+@pytest.mark.parametrize("n,bits", [(2, 32), (9_000, 20), (3_000_001, 32), (500_000, 13)])
+def test_radix_sort_u32_partial_bits(vox_ctx, n, bits):
+    # only key bits [0, bits) order the pairs; the others ride along
+    rng = np.random.default_rng(n + bits)
+    keys = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    dk, dv = _dev(keys, np.int32), _dev(vals, np.int32)
+    vox_ctx.radix_sort_u32(dk, dv, bits)
+    order = np.argsort(keys & np.uint32((1 << bits) - 1 if bits < 32 else 0xFFFFFFFF), kind="stable")
+    np.testing.assert_array_equal(dk.cpu().numpy().view(np.uint32), keys[order])
+    np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[order])
+
+
+@pytest.mark.parametrize("n,bits", [(100_000, 20), (70_000, 41)])
+def test_radix_sort_key64_ignores_bits_above_count(vox_ctx, n, bits):
+    rng = np.random.default_rng(bits)
+    keys = rng.integers(0, np.iinfo(np.uint64).max, n, dtype=np.uint64, endpoint=True)
+    vals = np.arange(n, dtype=np.uint32)
+    dk, dv = _dev(keys, np.int64), _dev(vals, np.int32)
+    vox_ctx.radix_sort_key64(dk, dv, bits)
+    order = np.argsort(keys & np.uint64((1 << bits) - 1), kind="stable")
+    np.testing.assert_array_equal(dk.cpu().numpy().view(np.uint64), keys[order])
+    np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[order])
+
+
+@pytest.mark.parametrize("n,low_bits,high_bits", [(2, 32, 1), (50_000, 32, 10), (400_001, 16, 7), (9_999, 32, 0)])
+def test_radix_sort_dual_key(vox_ctx, n, low_bits, high_bits):
+    # the tile sort of raster_gaussian_2d: (tile id, depth) with the tile id in
+    # the high key (raster/Raster2D.cpp:495-506)
+    rng = np.random.default_rng(n + low_bits)
+    low = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    high = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    vals = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    dl, dh, dv = _dev(low, np.int32), _dev(high, np.int32), _dev(vals, np.int32)
+    vox_ctx.radix_sort_dual_key(dl, dh, dv, low_bits, high_bits)
+    ml = np.uint32((1 << low_bits) - 1 if low_bits < 32 else 0xFFFFFFFF)
+    mh = np.uint32((1 << high_bits) - 1 if high_bits < 32 else 0xFFFFFFFF)
+    order = np.lexsort((np.arange(n), low & ml, high & mh))  # last key primary; index keeps it stable
+    np.testing.assert_array_equal(dl.cpu().numpy().view(np.uint32), low[order])
+    np.testing.assert_array_equal(dh.cpu().numpy().view(np.uint32), high[order])
+    np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[order])
