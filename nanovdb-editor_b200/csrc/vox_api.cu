@@ -75,6 +75,7 @@ struct vox_context_t
     DevBuf vb_work; // VoxelBVH ingestion: world-box keys, range tile counts
     DevBuf vb_keys; // VoxelBVH ingestion: compressed sort keys (also the dual-key sort's keys)
     DevBuf dual_idx; // dual-key sort: original indices
+    DevBuf vb_rec;   // VoxelBVH ingestion: per-Gaussian search records
     uint64_t* hscal = nullptr; // pinned mirror
     Epochs scan_epochs, run_epochs, sort_epochs;
     int check_sort = 0; // VOX_CHECK_SORT=1: validate key order after every sort
@@ -990,7 +991,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
-                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->vb_keys, &ctx->dual_idx, &ctx->cloud_start,
+                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->vb_keys, &ctx->dual_idx, &ctx->vb_rec, &ctx->cloud_start,
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_mask, &ctx->lc_off,
                       &ctx->cand_org, &ctx->tile_g0, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
@@ -1499,7 +1500,17 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
     cudaEventRecord(ctx->timers.ev[0], s);
     launch_vb_init(P.box_keys, P.cell_minmax, s);
     launch_vb_box(P, ctx->num_sms, s);
-    launch_vb_ijkl(P, s);
+    // VOX_VB_SEARCH=thread: the thread-per-Gaussian search (comparison)
+    const char* search = getenv("VOX_VB_SEARCH");
+    if (search && search[0] == 't')
+        launch_vb_ijkl(P, s);
+    else
+    {
+        if (!ensure(ctx, ctx->vb_rec, sizeof(float) * 24 * (size_t)(count > 0 ? count : 1)))
+            return VOX_ERR_MEMORY;
+        P.rec = (float*)ctx->vb_rec.p;
+        launch_vb_search(P, ctx->num_sms, s);
+    }
     cudaEventRecord(ctx->timers.ev[1], s);
     int rc = check_cuda(ctx, "vox_voxelbvh_ijkl_from_gaussians");
     if (rc == VOX_OK)

@@ -266,6 +266,7 @@ struct VoxelBvhParams
     float* world_bbox;   // [6] output
     uint64_t* keys;      // [8 n], 16-byte aligned
     uint32_t* ids;       // [8 n], 16-byte aligned
+    float* rec;          // [n][24] per-Gaussian search records (lane-balanced search)
     int* err;
 };
 // sorted-key pass: compressed key layout, range headers, 64-bit key write-back
@@ -282,6 +283,7 @@ struct VbRangeParams
 void launch_vb_init(uint32_t* box_keys, int* cell_minmax, cudaStream_t s);
 void launch_vb_box(const VoxelBvhParams& P, int num_sms, cudaStream_t s);
 void launch_vb_ijkl(const VoxelBvhParams& P, cudaStream_t s);
+void launch_vb_search(const VoxelBvhParams& P, int num_sms, cudaStream_t s);
 int64_t vb_range_tiles(int64_t N);
 void launch_vb_compress(const uint64_t* keys, int64_t N, const VbRangeParams& R, void* out, int key32, int num_sms,
                         cudaStream_t s);

@@ -448,6 +448,375 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_ijkl(VoxelBvhParams P)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Lane-balanced search: k_vb_setup writes one 96-byte record per Gaussian
+// (mean, rotation, 1 / (local_scale * scale), cell box, status) with a thread
+// per Gaussian; k_vb_search then runs a persistent loop in which every lane
+// tests ONE cell per iteration and, when its Gaussian is done, takes the next
+// one (static stride).  Lanes stay busy whatever the per-Gaussian trip counts,
+// which differ by orders of magnitude between neighbouring Gaussians.  Same
+// tests, same order, same keys as k_vb_ijkl.
+constexpr int VB_REC = 24; // floats per record: mu 3, R 9, inv 3, lo 3, hi 3, status 1, pad 2
+
+__global__ void __launch_bounds__(VB_THREADS) k_vb_setup(VoxelBvhParams P)
+{
+    float wmin[3], wmax[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        wmin[a] = vb_funkey(P.box_keys[a]);
+        wmax[a] = vb_funkey(P.box_keys[3 + a]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 6)
+        P.world_bbox[threadIdx.x] = threadIdx.x < 3 ? wmin[threadIdx.x] : wmax[threadIdx.x - 3];
+    const float d0 = __fsub_rn(wmax[0], wmin[0]), d1 = __fsub_rn(wmax[1], wmin[1]), d2 = __fsub_rn(wmax[2], wmin[2]);
+    const float dyz = d1 > d2 ? d1 : d2;
+    const float dmax = d0 > dyz ? d0 : dyz;
+    const float sc = __fdiv_rn((float)(P.resolution - 1u), dmax);
+    const float w2v[3] = { __fadd_rn(__fmul_rn(-wmin[0], sc), 0.5f), __fadd_rn(__fmul_rn(-wmin[1], sc), 0.5f),
+                           __fadd_rn(__fmul_rn(-wmin[2], sc), 0.5f) };
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= P.n)
+        return;
+    VbGauss G;
+    vb_load(P, g, G);
+    uint32_t kmn[3], kmx[3];
+    bool ok = vb_box_keys(P, G, kmn, kmx);
+    float r[VB_REC];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const float fl = floorf(__fadd_rn(__fmul_rn(sc, vb_funkey(kmn[a])), w2v[a]));
+        const float fh = floorf(__fadd_rn(__fmul_rn(sc, vb_funkey(kmx[a])), w2v[a]));
+        ok = ok && vb_cell_ok(fl) && vb_cell_ok(fh);
+        r[15 + a] = __int_as_float(vb_cell_ok(fl) ? (int)fl : 0);
+        r[18 + a] = __int_as_float(vb_cell_ok(fh) ? (int)fh : 0);
+        r[a] = G.mu[a];
+        r[12 + a] = G.inv[a];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            r[3 + 3 * a + c] = G.R[a][c];
+    }
+    r[21] = ok ? 1.f : 0.f;
+    r[22] = 0.f;
+    r[23] = 0.f;
+    if (!ok)
+        atomicOr(P.err, ERR_RANGE);
+    float4* dst = reinterpret_cast<float4*>(P.rec + (size_t)VB_REC * g);
+#pragma unroll
+    for (int q = 0; q < VB_REC / 4; q++)
+        dst[q] = make_float4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+}
+
+// voxel_ellipsoid_overlap of one cell (corner arithmetic as in vb_scan_level,
+// without the reuse across neighbouring cells)
+template <bool XF>
+__device__ __forceinline__ bool vb_overlap_cell(const VoxelBvhParams& P, const float* rec, const float w2v[4], int i,
+                                                int j, int k, uint32_t level)
+{
+    const float* mu = rec;
+    const float* R = rec + 3; // R[3 * a + r] = G.R[a][r]
+    const float* inv = rec + 12;
+    const float step = (float)(1u << level);
+    const int ijk[3] = { i, j, k };
+    float lp[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const float v0 = (float)ijk[a];
+        lp[a][0] = vb_lp(w2v, v0, a);
+        lp[a][1] = vb_lp(w2v, __fadd_rn(v0, step), a);
+    }
+    float q[3][3][2];
+    if (!XF)
+    {
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+            {
+                const float d = __fsub_rn(lp[a][b], mu[a]);
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    q[r][a][b] = __fmul_rn(d, R[3 * a + r]);
+            }
+    }
+    float vmin[3] = { 0.f, 0.f, 0.f }, vmax[3] = { 0.f, 0.f, 0.f };
+#pragma unroll
+    for (int v = 0; v < 8; v++)
+    {
+        const int b0 = v & 1, b1 = (v >> 1) & 1, b2 = (v >> 2) & 1;
+        float lr[3];
+        if (XF)
+        {
+            float d[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                d[c] = __fsub_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(lp[0][b0], P.ti[c]),
+                                                               __fmul_rn(lp[1][b1], P.ti[4 + c])),
+                                                     __fmul_rn(lp[2][b2], P.ti[8 + c])),
+                                           P.ti[12 + c]),
+                                 mu[c]);
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                lr[r] = __fadd_rn(__fadd_rn(__fmul_rn(d[0], R[r]), __fmul_rn(d[1], R[3 + r])), __fmul_rn(d[2], R[6 + r]));
+        }
+        else
+        {
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                lr[r] = __fadd_rn(__fadd_rn(q[r][0][b0], q[r][1][b1]), q[r][2][b2]);
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+        {
+            const float x = __fmul_rn(lr[r], inv[r]);
+            if (v == 0 || x < vmin[r])
+                vmin[r] = x;
+            if (v == 0 || x > vmax[r])
+                vmax[r] = x;
+        }
+    }
+    float dist2 = 1.f;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        if (0.f < vmin[a])
+            dist2 = __fsub_rn(dist2, __fmul_rn(vmin[a], vmin[a]));
+        else if (0.f > vmax[a])
+            dist2 = __fsub_rn(dist2, __fmul_rn(vmax[a], vmax[a]));
+    }
+    return dist2 > 0.f;
+}
+
+struct VbCursor
+{
+    int i, j, k, i1, j0, j1, k0, k1, st;
+};
+
+__device__ __forceinline__ int64_t vb_level_cells(const int lo[3], const int hi[3], uint32_t level)
+{
+    const int msk = ~((1 << level) - 1);
+    int64_t cells = 1;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+        cells *= (int64_t)(((hi[a] & msk) - (lo[a] & msk)) >> level) + 1;
+    return cells;
+}
+
+__device__ __forceinline__ void vb_cursor_start(VbCursor& C, const int lo[3], const int hi[3], uint32_t level)
+{
+    const int msk = ~((1 << level) - 1);
+    C.st = 1 << level;
+    C.i = lo[0] & msk;
+    C.i1 = hi[0] & msk;
+    C.j0 = C.j = lo[1] & msk;
+    C.j1 = hi[1] & msk;
+    C.k0 = C.k = lo[2] & msk;
+    C.k1 = hi[2] & msk;
+}
+
+// Position the search at the first level from `level` down that needs a
+// test (more than 8 cells: count with limit 9), or at an untested level 0
+// (emit).  Levels of at most 8 cells are chosen-so-far without a test.
+// Returns false when a level exceeds VB_MAX_CELLS.
+__device__ __forceinline__ bool vb_descend(const int lo[3], const int hi[3], uint32_t& level, uint32_t& last_good,
+                                           bool& have, bool& emit, VbCursor& C, uint32_t& count, uint64_t cur[8])
+{
+    while (true)
+    {
+        const int64_t cells = vb_level_cells(lo, hi, level);
+        if (cells > VB_MAX_CELLS)
+            return false;
+        if (cells > 8 || level == 0u)
+        {
+            emit = cells <= 8;
+            if (emit)
+                have = false;
+            vb_cursor_start(C, lo, hi, level);
+            count = 0;
+#pragma unroll
+            for (int s = 0; s < 8; s++)
+                cur[s] = ~0ull;
+            return true;
+        }
+        have = false;
+        last_good = level;
+        level -= 1u;
+    }
+}
+
+template <bool XF>
+__global__ void __launch_bounds__(VB_THREADS) k_vb_search(VoxelBvhParams P)
+{
+    float wmin[3], wmax[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        wmin[a] = vb_funkey(P.box_keys[a]);
+        wmax[a] = vb_funkey(P.box_keys[3 + a]);
+    }
+    const float d0 = __fsub_rn(wmax[0], wmin[0]), d1 = __fsub_rn(wmax[1], wmin[1]), d2 = __fsub_rn(wmax[2], wmin[2]);
+    const float dyz = d1 > d2 ? d1 : d2;
+    const float dmax = d0 > dyz ? d0 : dyz;
+    const float sc = __fdiv_rn((float)(P.resolution - 1u), dmax);
+    const float w2v[4] = { __fadd_rn(__fmul_rn(-wmin[0], sc), 0.5f), __fadd_rn(__fmul_rn(-wmin[1], sc), 0.5f),
+                           __fadd_rn(__fmul_rn(-wmin[2], sc), 0.5f), sc };
+
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x - stride;
+    float rec[VB_REC];
+    int lo[3] = { 0, 0, 0 }, hi[3] = { 0, 0, 0 };
+    uint32_t level = 0, last_good = 0, count = 0, nkeys = 0;
+    bool busy = false, have = false, emit = false;
+    VbCursor C{};
+    uint64_t cur[8];
+    int cmin[3] = { 0x7fffffff, 0x7fffffff, 0x7fffffff }, cmax[3] = { (int)0x80000000, (int)0x80000000, (int)0x80000000 };
+    while (true)
+    {
+        int finish = 0; // 1: done with cells, 2: done without (unused slots)
+        if (!busy)
+        {
+            // ---- the lane's next Gaussian
+            g += stride;
+            if (g >= P.n)
+                break;
+            const float4* src = reinterpret_cast<const float4*>(P.rec + (size_t)VB_REC * g);
+#pragma unroll
+            for (int q = 0; q < VB_REC / 4; q++)
+            {
+                const float4 v = src[q];
+                rec[4 * q] = v.x;
+                rec[4 * q + 1] = v.y;
+                rec[4 * q + 2] = v.z;
+                rec[4 * q + 3] = v.w;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+            {
+                lo[a] = __float_as_int(rec[15 + a]);
+                hi[a] = __float_as_int(rec[18 + a]);
+            }
+            level = 11u;
+            last_good = 11u;
+            have = false;
+            nkeys = 0;
+            if (rec[21] == 0.f || !vb_descend(lo, hi, level, last_good, have, emit, C, count, cur))
+                finish = 2;
+            else
+                busy = true;
+        }
+        else
+        {
+            // ---- one cell of the current level
+            if (vb_overlap_cell<XF>(P, rec, w2v, C.i, C.j, C.k, level))
+            {
+                const uint64_t kv = ((uint64_t)(int64_t)C.i << 48) | ((uint64_t)(int64_t)C.j << 32) |
+                                    ((uint64_t)(int64_t)C.k << 16) | (uint64_t)level;
+#pragma unroll
+                for (int s = 0; s < 8; s++) // register-resident insert
+                    if ((uint32_t)s == count)
+                        cur[s] = kv;
+                count++;
+            }
+            C.k += C.st;
+            if (C.k > C.k1)
+            {
+                C.k = C.k0;
+                C.j += C.st;
+                if (C.j > C.j1)
+                {
+                    C.j = C.j0;
+                    C.i += C.st;
+                }
+            }
+            if (C.i > C.i1 || (emit ? count >= 8u : count > 8u))
+            {
+                // level done; it is the chosen one so far unless it
+                // overflows below level 11 (level 11 stays with its first 8)
+                if (emit || count <= 8u || level == last_good)
+                {
+                    ulonglong2* kd = reinterpret_cast<ulonglong2*>(P.keys + 8 * g);
+#pragma unroll
+                    for (int s = 0; s < 4; s++)
+                        kd[s] = make_ulonglong2(cur[2 * s], cur[2 * s + 1]);
+                    nkeys = count < 8u ? count : 8u;
+                    have = true;
+                }
+                if (emit)
+                    finish = 1;
+                else if (count > 8u)
+                {
+                    level = last_good;
+                    if (have)
+                        finish = 1;
+                    else
+                    {
+                        // the chosen level was decided untested: emit it
+                        emit = true;
+                        vb_cursor_start(C, lo, hi, level);
+                        count = 0;
+#pragma unroll
+                        for (int s = 0; s < 8; s++)
+                            cur[s] = ~0ull;
+                    }
+                }
+                else if (level == 0u)
+                    finish = 1;
+                else
+                {
+                    last_good = level;
+                    level -= 1u;
+                    if (!vb_descend(lo, hi, level, last_good, have, emit, C, count, cur))
+                        finish = 2;
+                }
+            }
+        }
+        if (finish != 0)
+        {
+            if (finish == 2)
+            {
+                // not finite / out of range / unbounded: unused slots, error
+                if (rec[21] != 0.f)
+                    atomicOr(P.err, ERR_RANGE);
+                ulonglong2* kd = reinterpret_cast<ulonglong2*>(P.keys + 8 * g);
+#pragma unroll
+                for (int s = 0; s < 4; s++)
+                    kd[s] = make_ulonglong2(~0ull, ~0ull);
+                nkeys = 0;
+            }
+            else if (nkeys > 0)
+            {
+                const int msk = ~((1 << level) - 1);
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                {
+                    cmin[a] = min(cmin[a], lo[a] & msk);
+                    cmax[a] = max(cmax[a], hi[a] & msk);
+                }
+            }
+            const uint32_t id = (uint32_t)g;
+            uint4* idd = reinterpret_cast<uint4*>(P.ids + 8 * g);
+            idd[0] = make_uint4(nkeys > 0 ? id : ~0u, nkeys > 1 ? id : ~0u, nkeys > 2 ? id : ~0u, nkeys > 3 ? id : ~0u);
+            idd[1] = make_uint4(nkeys > 4 ? id : ~0u, nkeys > 5 ? id : ~0u, nkeys > 6 ? id : ~0u, nkeys > 7 ? id : ~0u);
+            busy = false;
+        }
+    }
+    // every lane gets here (the loop only breaks)
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+    {
+        const int wmn = __reduce_min_sync(0xffffffffu, cmin[a]), wmx = __reduce_max_sync(0xffffffffu, cmax[a]);
+        if ((threadIdx.x & 31) == 0)
+        {
+            if (wmn != 0x7fffffff)
+                atomicMin(&P.cell_minmax[a], wmn);
+            if (wmx != (int)0x80000000)
+                atomicMax(&P.cell_minmax[3 + a], wmx);
+        }
+    }
+}
+
 // starts (key differs from its predecessor) of one 2048-key tile, per thread 8
 // consecutive keys
 template <class K>
@@ -591,6 +960,28 @@ void launch_vb_box(const VoxelBvhParams& P, int num_sms, cudaStream_t s)
     if (grid > cap)
         grid = cap;
     k_vb_box<<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
+    count_launch();
+}
+
+void launch_vb_search(const VoxelBvhParams& P, int num_sms, cudaStream_t s)
+{
+    const int64_t grid1 = P.n > 0 ? (P.n + VB_THREADS - 1) / VB_THREADS : 1;
+    k_vb_setup<<<(unsigned)grid1, VB_THREADS, 0, s>>>(P);
+    count_launch();
+    if (P.n <= 0)
+        return;
+    int per_sm = 0;
+    if (P.has_xform)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vb_search<true>, VB_THREADS, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vb_search<false>, VB_THREADS, 0);
+    int64_t grid = (int64_t)num_sms * (per_sm > 0 ? per_sm : 1);
+    if (grid > grid1)
+        grid = grid1;
+    if (P.has_xform)
+        k_vb_search<true><<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
+    else
+        k_vb_search<false><<<(unsigned)grid, VB_THREADS, 0, s>>>(P);
     count_launch();
 }
 
