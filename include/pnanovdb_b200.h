@@ -471,6 +471,24 @@ PNANOVDB_API int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const floa
                                                   uint32_t* d_prim_id, uint32_t* d_range, float* d_world_bbox,
                                                   int64_t* range_count);
 
+/* replaces ijkl_from_gaussians_file (raster/VoxelBVH.cpp:1437-1575): loads
+ * `filename` (.npz or binary Gaussian-splat .ply; arrays means, opacities,
+ * quaternions, scales, and sh_0 / sh_n when present), activates them on the
+ * host as the reference does (normalised quaternions, exp scales, sigmoid
+ * opacities), runs vox_voxelbvh_ijkl_from_gaussians and returns page-locked
+ * host arrays: *ijkl_out (8-byte elements, 8 per Gaussian), *prim_id_out
+ * (4-byte, 8 per Gaussian), *range_out (8-byte [start, end) pairs, 8 per
+ * Gaussian), *world_bbox_out (6 floats), and in gaussian_arrays_out (up to
+ * gaussian_array_count of the 6, may be NULL) the activated arrays.  Release
+ * each with pnanovdb_get_compute()->destroy_array. */
+PNANOVDB_API int vox_voxelbvh_ijkl_from_gaussians_file(vox_context_t* ctx, const char* filename, uint32_t resolution,
+                                                       const float* transform, pnanovdb_compute_array_t** ijkl_out,
+                                                       pnanovdb_compute_array_t** prim_id_out,
+                                                       pnanovdb_compute_array_t** range_out,
+                                                       pnanovdb_compute_array_t** world_bbox_out,
+                                                       pnanovdb_compute_array_t** gaussian_arrays_out,
+                                                       uint32_t gaussian_array_count);
+
 /* The inverse vox_voxelbvh_ijkl_from_gaussians applies for `m` (16 floats,
  * host): Gauss-Jordan elimination with partial pivoting in double precision,
  * rounded to float.  The reference inverts in float by cofactor expansion

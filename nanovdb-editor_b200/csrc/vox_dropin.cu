@@ -550,7 +550,147 @@ static pnanovdb_bool_t PNANOVDB_ABI r_create_from_desc(pnanovdb_raster_t*, const
 
 #include "vox_npz.inl"
 
+#include "vox_detmath.h"
+
+namespace
+{
+
+// the reference's host activation of file arrays in ijkl_from_gaussians_file
+// (raster/VoxelBVH.cpp:1474-1503): quaternions (w x y z) scaled by
+// 1 / sqrt(x^2 + y^2 + z^2 + w^2), scales exp, opacities 1 / (1 + exp(-x)),
+// one IEEE operation at a time; exp is vox_expf_cr (correctly rounded but
+// for ties), the same exp the raster path's preprocessing uses
+void vb_activate_host(int64_t n, float* quats, float* scales, float* opac)
+{
+    for (int64_t p = 0; p < n; p++)
+    {
+        const float x = quats[4 * p + 1], y = quats[4 * p + 2], z = quats[4 * p + 3], w = quats[4 * p + 0];
+        const float ss = VOX_FADD(VOX_FADD(VOX_FADD(VOX_FMUL(x, x), VOX_FMUL(y, y)), VOX_FMUL(z, z)), VOX_FMUL(w, w));
+        const float inv = VOX_FDIV(1.f, VOX_FSQRT(ss));
+        quats[4 * p + 1] = VOX_FMUL(x, inv);
+        quats[4 * p + 2] = VOX_FMUL(y, inv);
+        quats[4 * p + 3] = VOX_FMUL(z, inv);
+        quats[4 * p + 0] = VOX_FMUL(w, inv);
+        for (int a = 0; a < 3; a++)
+            scales[3 * p + a] = vox_expf_cr(scales[3 * p + a]);
+        opac[p] = VOX_FDIV(1.f, VOX_FADD(1.f, vox_expf_cr(-opac[p])));
+    }
+}
+
+} // namespace
+
 extern "C" {
+
+int vox_voxelbvh_ijkl_from_gaussians_file(vox_context_t* ctx, const char* filename, uint32_t resolution,
+                                          const float* transform, pnanovdb_compute_array_t** ijkl_out,
+                                          pnanovdb_compute_array_t** prim_id_out, pnanovdb_compute_array_t** range_out,
+                                          pnanovdb_compute_array_t** world_bbox_out,
+                                          pnanovdb_compute_array_t** gaussian_arrays_out,
+                                          uint32_t gaussian_array_count)
+{
+    if (!ctx || !filename || !ijkl_out || !prim_id_out || !range_out || !world_bbox_out)
+        return VOX_ERR_ARGS;
+    *ijkl_out = *prim_id_out = *range_out = *world_bbox_out = nullptr;
+    std::vector<NpzArray> arrays;
+    std::string why;
+    bool loaded = false;
+    if (has_suffix(filename, ".ply"))
+        loaded = read_ply(filename, arrays, why);
+    else if (has_suffix(filename, ".npz"))
+        loaded = read_npz(filename, arrays, why);
+    else
+        why = "file format not supported (.npz and .ply are)";
+    if (!loaded)
+    {
+        log_err((std::string("ijkl_from_gaussians_file: failed to load '") + filename + "': " + why).c_str());
+        return VOX_ERR_ARGS;
+    }
+    // means, opacities, quaternions, scales, sh_0, sh_n (the reference's names and order)
+    const char* names[6] = { "means", "opacities", "quaternions", "scales", "sh_0", "sh_n" };
+    std::vector<float>* a[6] = {};
+    for (int i = 0; i < 6; i++)
+        for (auto& x : arrays)
+            if (x.name == names[i])
+                a[i] = &x.data;
+    for (int i = 0; i < 4; i++)
+        if (!a[i])
+        {
+            log_err((std::string("ijkl_from_gaussians_file: '") + filename + "' has no array '" + names[i] + "'").c_str());
+            return VOX_ERR_ARGS;
+        }
+    const int64_t n = (int64_t)a[1]->size(); // gaussian_count = opacities (VoxelBVH.cpp:1458)
+    if ((int64_t)a[0]->size() < 3 * n || (int64_t)a[2]->size() < 4 * n || (int64_t)a[3]->size() < 3 * n)
+    {
+        log_err("ijkl_from_gaussians_file: attribute counts do not match the opacities");
+        return VOX_ERR_ARGS;
+    }
+    vb_activate_host(n, a[2]->data(), a[3]->data(), a[1]->data());
+
+    // device copies on the context's stream, outputs back to page-locked arrays
+    cudaStream_t s = (cudaStream_t)vox_context_stream(ctx);
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t b_means = 12 * (size_t)n, b_op = 4 * (size_t)n, b_q = 16 * (size_t)n, b_s = 12 * (size_t)n;
+    const size_t b_k = 64 * (size_t)n, b_id = 32 * (size_t)n, b_r = 64 * (size_t)n, b_box = 24;
+    const size_t total = al(b_means) + al(b_op) + al(b_q) + al(b_s) + al(b_k) + al(b_id) + al(b_r) + al(b_box);
+    char* base = nullptr;
+    if (cudaMalloc(&base, total) != cudaSuccess)
+    {
+        cudaGetLastError();
+        log_err("ijkl_from_gaussians_file: out of device memory");
+        return VOX_ERR_MEMORY;
+    }
+    char* p = base;
+    float* d_means = (float*)p;
+    p += al(b_means);
+    float* d_op = (float*)p;
+    p += al(b_op);
+    float* d_q = (float*)p;
+    p += al(b_q);
+    float* d_s = (float*)p;
+    p += al(b_s);
+    uint64_t* d_k = (uint64_t*)p;
+    p += al(b_k);
+    uint32_t* d_id = (uint32_t*)p;
+    p += al(b_id);
+    uint32_t* d_r = (uint32_t*)p;
+    p += al(b_r);
+    float* d_box = (float*)p;
+    cudaMemcpyAsync(d_means, a[0]->data(), b_means, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_op, a[1]->data(), b_op, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_q, a[2]->data(), b_q, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_s, a[3]->data(), b_s, cudaMemcpyHostToDevice, s);
+    int rc = vox_voxelbvh_ijkl_from_gaussians(ctx, d_means, d_op, d_q, d_s, n, resolution, transform, d_k, d_id, d_r,
+                                              d_box, nullptr);
+    pnanovdb_compute_array_t* out[4] = { array_create_pinned(8, 8 * (uint64_t)n), array_create_pinned(4, 8 * (uint64_t)n),
+                                         array_create_pinned(8, 8 * (uint64_t)n), array_create_pinned(4, 6) };
+    if (rc == VOX_OK && !(out[0] && out[1] && out[2] && out[3]))
+        rc = VOX_ERR_MEMORY;
+    if (rc == VOX_OK)
+    {
+        cudaMemcpyAsync(out[0]->data, d_k, b_k, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(out[1]->data, d_id, b_id, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(out[2]->data, d_r, b_r, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(out[3]->data, d_box, b_box, cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess)
+            rc = VOX_ERR_CUDA;
+    }
+    cudaFree(base);
+    if (rc != VOX_OK)
+    {
+        for (auto* x : out)
+            array_destroy(x);
+        return rc;
+    }
+    *ijkl_out = out[0];
+    *prim_id_out = out[1];
+    *range_out = out[2];
+    *world_bbox_out = out[3];
+    // the activated arrays, as the reference hands them back
+    if (gaussian_arrays_out)
+        for (uint32_t i = 0; i < gaussian_array_count && i < 6; i++)
+            gaussian_arrays_out[i] = a[i] ? array_create(4, a[i]->size(), a[i]->data()) : array_create(4, 0, nullptr);
+    return VOX_OK;
+}
 
 pnanovdb_compute_t* pnanovdb_get_compute(void)
 {

@@ -118,6 +118,8 @@ def _lib():
         lib.vox_radix_sort_dual_key.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_uint32, c_uint32]
         lib.vox_voxelbvh_ijkl_from_gaussians.restype = c_int
         lib.vox_voxelbvh_ijkl_from_gaussians.argtypes = [c_void_p] + [c_void_p] * 4 + [c_int64, c_uint32] + [c_void_p] * 5 + [POINTER(c_int64)]
+        lib.vox_voxelbvh_ijkl_from_gaussians_file.restype = c_int
+        lib.vox_voxelbvh_ijkl_from_gaussians_file.argtypes = [c_void_p, ctypes.c_char_p, c_uint32, c_void_p] + [c_void_p] * 5 + [c_uint32]
         lib.vox_voxelbvh_transform_inverse.restype = c_int
         lib.vox_voxelbvh_transform_inverse.argtypes = [c_void_p, c_void_p]
         lib._vox_bound = True
@@ -301,6 +303,38 @@ class VoxContext:
                                                               _ptr(T), _ptr(ijkl), _ptr(prim_id), _ptr(rng), _ptr(box),
                                                               byref(count)), "vox_voxelbvh_ijkl_from_gaussians")
         return {"ijkl": ijkl, "prim_id": prim_id, "range": rng, "world_bbox": box, "range_count": int(count.value)}
+
+    def voxelbvh_ijkl_from_file(self, filename: str, resolution: int, transform=None) -> dict:
+        """VoxelBVH ingestion of a Gaussian file (the reference's
+        ijkl_from_gaussians_file, raster/VoxelBVH.cpp:1437-1575): .npz or .ply
+        with raw attributes, activated on the host.  Returns numpy arrays
+        ``ijkl`` (uint64), ``prim_id`` (uint32), ``range`` (uint32 pairs),
+        ``world_bbox`` and the activated ``means``, ``opacities``,
+        ``quaternions``, ``scales``."""
+        from .compute import Compute, pnanovdb_ComputeArray
+
+        T = None
+        if transform is not None:
+            T = np.ascontiguousarray(np.asarray(transform, dtype=np.float32).reshape(16))
+        outs = [POINTER(pnanovdb_ComputeArray)() for _ in range(4)]
+        garr = (POINTER(pnanovdb_ComputeArray) * 6)()
+        self._check(self.lib.vox_voxelbvh_ijkl_from_gaussians_file(
+            self.handle, str(filename).encode(), int(resolution), _ptr(T), *[ctypes.addressof(o) for o in outs],
+            ctypes.addressof(garr), 6), "vox_voxelbvh_ijkl_from_gaussians_file")
+        comp = Compute()
+
+        def take(ptr, dtype):
+            a = ptr.contents
+            nbytes = int(a.element_size * a.element_count)
+            out = np.frombuffer((ctypes.c_byte * nbytes).from_address(a.data), dtype=dtype).copy() if nbytes else np.zeros(0, dtype)
+            comp.destroy_array(a)
+            return out
+
+        res = {"ijkl": take(outs[0], np.uint64), "prim_id": take(outs[1], np.uint32),
+               "range": take(outs[2], np.uint32), "world_bbox": take(outs[3], np.float32)}
+        for name, ptr in zip(("means", "opacities", "quaternions", "scales", "sh_0", "sh_n"), garr):
+            res[name] = take(ptr, np.float32)
+        return res
 
     def voxelbvh_transform_inverse(self, transform):
         """The float32 inverse vox_voxelbvh_ijkl_from_gaussians applies for `transform` (4x4)."""

@@ -184,3 +184,27 @@ def test_ijkl_argument_checks(vox_ctx):
     sing[1, 1] = 0.0
     with pytest.raises(PipelineError):
         _run(vox_ctx, cloud, 256, sing)
+
+
+@pytest.mark.parametrize("fmt", ["npz", "ply"])
+def test_ijkl_from_file(vox_ctx, oracle_mod, tmp_path, fmt):
+    # ijkl_from_gaussians_file: raw attributes in a file, activated on the
+    # host (the raster path's preprocessing restated by the oracle)
+    from test_gpu_dropin import _write_ply
+
+    raw = W.cluster_cloud(5000, 47, clusters=4).raw_arrays()
+    path = tmp_path / f"splats.{fmt}"
+    if fmt == "npz":
+        np.savez(path, means=raw[0], opacities=raw[1], quaternions=raw[2], scales=raw[3], sh_0=raw[4], sh_n=raw[5])
+    else:
+        _write_ply(path, raw)
+    got = vox_ctx.voxelbvh_ijkl_from_file(str(path), 512)
+    act = oracle_mod.preprocess(raw)
+    np.testing.assert_array_equal(got["quaternions"].reshape(-1, 4).view(np.uint32), act["quats"].view(np.uint32))
+    np.testing.assert_array_equal(got["scales"].reshape(-1, 3).view(np.uint32), act["scales"].view(np.uint32))
+    np.testing.assert_array_equal(got["opacities"].view(np.uint32), act["opacities"].view(np.uint32))
+    ref = oracle_mod.voxelbvh_ijkl(act, 512)
+    np.testing.assert_array_equal(got["world_bbox"].view(np.uint32), ref["world_bbox"].view(np.uint32))
+    np.testing.assert_array_equal(got["ijkl"], ref["ijkl"])
+    np.testing.assert_array_equal(got["prim_id"], ref["prim_id"])
+    np.testing.assert_array_equal(got["range"], ref["range"])
