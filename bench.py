@@ -272,6 +272,44 @@ VOXELBVH = {"workload": "voxelbvh_ijkl_2M_clusters64_res512", "gaussians": 2_000
 VOXELBVH_METRIC = "Gaussians/s ingested into VoxelBVH keys (ijkl_from_gaussians)"
 
 
+def measure_voxelbvh_form(ctx, torch, rank, steps, warmup, flush):
+    """VoxelBVH Gaussian ingestion on the main cloud's distribution (2M
+    Gaussians, 64 clusters, resolution 512), activated inputs resident in HBM,
+    CUDA events on the library's stream; `python bench.py --workload
+    voxelbvh` prints the full line for it (e2e, roofline, CPU baseline)."""
+    from nanovdb_editor import workloads as W
+
+    cloud = W.cluster_cloud(VOXELBVH["gaussians"], 1 + rank, clusters=VOXELBVH["clusters"])
+    dev = [torch.from_numpy(np.ascontiguousarray(cloud[k], dtype=np.float32)).cuda()
+           for k in ("means", "opacities", "quats", "scales")]
+    res = VOXELBVH["resolution"]
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(warmup):
+        out = ctx.voxelbvh_ijkl_from_gaussians(*dev, res)
+    times, stats = [], []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0.record(ext)
+        out = ctx.voxelbvh_ijkl_from_gaussians(*dev, res)
+        ev1.record(ext)
+        ev1.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+        stats.append(ctx.stats())
+    ms = float(np.mean(times))
+    return {
+        "workload": VOXELBVH["workload"],
+        "gaussians": VOXELBVH["gaussians"],
+        "ms_per_call": ms,
+        "gaussians_per_s": VOXELBVH["gaussians"] / (ms * 1e-3),
+        "stages_ms": {k: float(np.mean([x[f"ms_vb_{k}"] for x in stats])) for k in ("keys", "sort", "ranges")},
+        "ranges": int(out["range_count"]),
+        "sort_bits": int(stats[-1]["vb_sort_bits"]),
+        "parity": "keys, ids, range headers and world box bit-exact to the oracle (tests/test_gpu_voxelbvh.py)",
+    }
+
+
 def voxelbvh_cpu(target_s=10.0):
     """The oracle's VoxelBVH ingestion on a bounded sample, all host cores
     (per-Gaussian work split over threads; the key sort is serial)."""
@@ -636,6 +674,10 @@ def main():
     if not args.no_forms:
         forms["fwd_bwd"] = measure_fwd_bwd(ctx, torch, rank, args.steps, args.warmup, flush)
         forms["batched"] = measure_batched(ctx, torch, rank, args.steps, args.warmup, flush)
+        try:
+            forms["voxelbvh"] = measure_voxelbvh_form(ctx, torch, rank, args.steps, args.warmup, flush)
+        except Exception as e:  # a secondary row: never lose the main line to it
+            forms["voxelbvh"] = {"error": f"{type(e).__name__}: {e}"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
