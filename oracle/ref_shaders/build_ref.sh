@@ -26,7 +26,7 @@ for s in gaussian_prim gaussian_frag_alloc gaussian_frag_color fanout_scatter_pr
         "$REF/raster/shaders/$s.slang" > "$OUT/$s.inc"
 done
 # VoxelBVH Gaussian ingestion; `.xyz` reads of a float4 become `.xyz()`
-for s in voxelbvh_gaussians_to_ijkl; do
+for s in voxelbvh_gaussians_to_ijkl voxelbvh_find_range_starts voxelbvh_scatter_range_headers; do
     sed -e 's/\[shader("compute")\]//g' \
         -e 's/\[numthreads([^]]*)\]//g' \
         -e 's/ : SV_Group[A-Za-z]*//g' \

@@ -11,6 +11,8 @@
  *   gaussian_frag_alloc.slang           fragment test -> ijk or 0x7FFFFFFF
  *   gaussian_frag_color.slang           alpha / RGBA8 of a passing fragment
  *   voxelbvh/voxelbvh_gaussians_to_ijkl.slang  per-Gaussian level and cells
+ *   voxelbvh/voxelbvh_find_range_starts.slang, voxelbvh_scatter_range_headers.slang
+ *                                       range headers of the sorted keys
  */
 #include <math.h>
 #include <stdint.h>
@@ -51,6 +53,17 @@ namespace sh_vbijkl
 {
 #include "slang_compat.h"
 #include "voxelbvh_gaussians_to_ijkl.inc"
+}
+
+namespace sh_vbstarts
+{
+#include "slang_compat.h"
+#include "voxelbvh_find_range_starts.inc"
+}
+namespace sh_vbscatter
+{
+#include "slang_compat.h"
+#include "voxelbvh_scatter_range_headers.inc"
 }
 
 template <class C>
@@ -230,6 +243,51 @@ void ref_voxelbvh_to_ijkl(uint32_t n, uint32_t resolution, const float* means, c
             uint3 gi = { g, 0, 0 }, ti = { t, 0, 0 };
             main(gi, ti);
         }
+}
+
+/* range headers of n sorted keys (raster/VoxelBVH.cpp:1380-1431): range
+ * starts, the inclusive uint32 global_scan of them, the header scatter.
+ * headers: 2 n words; starts / scan: n words of scratch each. */
+void ref_voxelbvh_ranges(uint32_t n, const uint64_t* keys, uint32_t* starts, uint32_t* scan, uint32_t* headers)
+{
+    const uint32_t groups = (n + VOX_REF_GROUP - 1) / VOX_REF_GROUP;
+    {
+        using namespace sh_vbstarts;
+        memset(&constants, 0, sizeof(constants));
+        constants.voxel_count = n;
+        constants.voxel_workgroup_count = groups;
+        keys_in.p = (uint64_t*)keys;
+        range_starts_out.p = starts;
+        range_headers_out.p = headers;
+        for (uint32_t g = 0; g < groups; g++)
+            for (uint32_t t = 0; t < VOX_REF_GROUP; t++)
+            {
+                uint3 gi = { g, 0, 0 }, ti = { t, 0, 0 };
+                main(gi, ti);
+            }
+    }
+    uint32_t run = 0; /* global_scan: inclusive, uint32 */
+    for (uint32_t i = 0; i < n; i++)
+    {
+        run += starts[i];
+        scan[i] = run;
+    }
+    {
+        using namespace sh_vbscatter;
+        memset(&constants, 0, sizeof(constants));
+        constants.voxel_count = n;
+        constants.voxel_workgroup_count = groups;
+        keys_in.p = (uint64_t*)keys;
+        range_starts_in.p = starts;
+        range_scan_in.p = scan;
+        range_headers_out.p = headers;
+        for (uint32_t g = 0; g < groups; g++)
+            for (uint32_t t = 0; t < VOX_REF_GROUP; t++)
+            {
+                uint3 gi = { g, 0, 0 }, ti = { t, 0, 0 };
+                main(gi, ti);
+            }
+    }
 }
 
 } /* extern "C" */

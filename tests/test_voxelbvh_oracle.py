@@ -6,9 +6,11 @@
    same keys and Gaussian ids once both are sorted stably by key, for plain,
    clustered, anisotropic, faint and the 32-Gaussian pytest clouds, three
    resolutions, with and without a transform.
-2. The invariants the reference's range headers state
-   (voxelbvh_find_range_starts.slang, voxelbvh_scatter_range_headers.slang):
-   ranges partition the sorted keys, one range per distinct key, zeros after.
+2. The range headers against the reference's own
+   voxelbvh_find_range_starts.slang and voxelbvh_scatter_range_headers.slang
+   (compiled the same way) on the oracle's sorted keys, and the invariants
+   they state: ranges partition the sorted keys, one range per distinct key,
+   zeros after.
 3. The library's host-side transform inverse (no GPU needed).
 """
 
@@ -34,6 +36,8 @@ def ref():
     if not hasattr(L, "ref_voxelbvh_to_ijkl"):
         pytest.skip("oracle/_ref predates the VoxelBVH shader; rerun oracle/ref_shaders/build_ref.sh")
     L.ref_voxelbvh_to_ijkl.argtypes = [ctypes.c_uint32, ctypes.c_uint32] + [ctypes.c_void_p] * 9
+    if hasattr(L, "ref_voxelbvh_ranges"):
+        L.ref_voxelbvh_ranges.argtypes = [ctypes.c_uint32] + [ctypes.c_void_p] * 4
     return L
 
 
@@ -109,6 +113,24 @@ def test_oracle_matches_reference_shader(ref, oracle_mod, name, res, xform):
     k, i = ref_keys(ref, cloud, res, T, Ti, out["world_bbox"])
     np.testing.assert_array_equal(out["ijkl"], k)
     np.testing.assert_array_equal(out["prim_id"], i)
+
+
+@pytest.mark.parametrize("name", ["plain", "clusters", "faint"])
+@pytest.mark.parametrize("res", [64, 4096])
+def test_oracle_ranges_match_reference_shaders(ref, oracle_mod, name, res):
+    # voxelbvh_find_range_starts + the inclusive global_scan +
+    # voxelbvh_scatter_range_headers, compiled from the reference, on the
+    # oracle's sorted keys
+    if not hasattr(ref, "ref_voxelbvh_ranges"):
+        pytest.skip("oracle/_ref predates the range shaders; rerun oracle/ref_shaders/build_ref.sh")
+    out = oracle_mod.voxelbvh_ijkl(clouds()[name], res)
+    keys = np.ascontiguousarray(out["ijkl"])
+    N = keys.size
+    starts, scan = np.zeros(N, np.uint32), np.zeros(N, np.uint32)
+    headers = np.full(2 * N, 0xDEADBEEF, np.uint32)
+    ref.ref_voxelbvh_ranges(N, keys.ctypes.data, starts.ctypes.data, scan.ctypes.data, headers.ctypes.data)
+    np.testing.assert_array_equal(headers, out["range"])
+    assert int(scan[-1]) == out["ranges"]
 
 
 @pytest.mark.parametrize("res", [16, 1024])
