@@ -10,16 +10,22 @@
 //                       one atomicMin / atomicMax per warp on order-preserving
 //                       integer keys (deterministic; -0 orders below +0)
 //                       (voxelbvh_gaussians_bbox_reduce1/2.slang)
-//   k_vb_ijkl           one thread per Gaussian: level search from 11 down,
-//                       stops once more than 8 cells overlap, writes 8 keys and
-//                       8 ids as 16-byte vector stores
+//   k_vb_setup          a 96-byte search record per Gaussian (mean,
+//                       rotation, 1 / (local_scale scale), cell box, status)
+//   k_vb_search         the level search from 11 down, stopping once more
+//                       than 8 cells overlap, lane-balanced: a persistent loop
+//                       in which every lane tests one cell per iteration and
+//                       takes its next Gaussian when its search ends; 8 keys
+//                       and 8 ids per Gaussian in 16-byte stores
 //                       (voxelbvh_gaussians_to_ijkl.slang:25-250)
+//   k_vb_ijkl           the same search, one thread per Gaussian with the
+//                       per-axis reuse below (VOX_VB_SEARCH=thread)
 //   k_vb_compress       keys -> compressed keys of 4 + bits(i) + bits(j) +
 //                       bits(k) bits (32-bit when they fit), sized by the
-//                       emitted cells' range that k_vb_ijkl reduces: the same
+//                       emitted cells' range the search reduces: the same
 //                       order in fewer radix passes
 //   (sort)              stable onesweep LSD sort of the compressed keys (of
-//                       the 64-bit keys when a cell lies outside [0, 2^16))
+//                       the 64-bit keys when a cell lies outside [0, 2^15))
 //   k_vb_range_count    starts per 2048-key tile
 //   (scan)              exclusive scan of the tile counts
 //   k_vb_range_scatter  headers [2r] = start, [2r + 1] = end; every header
@@ -32,8 +38,9 @@
 // the order the shaders write it (no contraction), so the keys are the same
 // bits as the C restatement's.  Values the shaders recompute per corner
 // (the per-axis voxel-to-world coordinates, the products of a corner's
-// coordinates with the rotation) are computed once and reused: the same
-// operations on the same operands.
+// coordinates with the rotation) are computed once per cell (and, in
+// k_vb_ijkl, once per row of cells) and reused: the same operations on the
+// same operands.
 #include <cuda_runtime.h>
 
 #include "vox_device.cuh"
