@@ -129,6 +129,9 @@ def main():
     L = load_ref()
     for name, (cloud, vs) in raster_cases().items():
         np.savez_compressed(os.path.join(HERE, f"raster_{name}.npz"), **raster_fixture(L, cloud, vs))
+    # a tighter cull radius (gaussian_frag_color.slang:205, the shader parameter)
+    cloud, vs = raster_cases()["clusters"]
+    np.savez_compressed(os.path.join(HERE, "raster_clusters_cull0.01.npz"), **raster_fixture(L, cloud, vs, cull=0.01))
     for name, (cloud, res) in voxelbvh_cases().items():
         np.savez_compressed(os.path.join(HERE, f"voxelbvh_{name}.npz"), **voxelbvh_fixture(L, cloud, res))
     for f in sorted(os.listdir(HERE)):
