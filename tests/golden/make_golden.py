@@ -106,14 +106,19 @@ def voxelbvh_cases():
     }
 
 
-def voxelbvh_fixture(L, cloud, res):
+def voxelbvh_fixture(L, cloud, res, T=None):
     n = cloud.n
     m, q, s, o = (_f(cloud[k]) for k in ("means", "quats", "scales", "opacities"))
-    box = O.voxelbvh_ijkl(cloud, res)["world_bbox"]  # a min / max over the Gaussians' boxes
+    Ti = None if T is None else np.linalg.inv(T.astype(np.float64)).astype(np.float32)
+    box = O.voxelbvh_ijkl(cloud, res, T, Ti)["world_bbox"]  # a min / max over the Gaussians' boxes
     pad = 8 * 256 * ((n + 255) // 256)
     k = np.zeros(pad, np.uint64)
     i = np.zeros(pad, np.uint32)
-    L.ref_voxelbvh_to_ijkl(n, res, m.ctypes.data, o.ctypes.data, q.ctypes.data, s.ctypes.data, None, None, _f(box).ctypes.data, k.ctypes.data, i.ctypes.data)
+    Tp = None if T is None else _f(T).reshape(16)
+    Tip = None if Ti is None else _f(Ti).reshape(16)
+    L.ref_voxelbvh_to_ijkl(n, res, m.ctypes.data, o.ctypes.data, q.ctypes.data, s.ctypes.data,
+                           None if Tp is None else Tp.ctypes.data, None if Tip is None else Tip.ctypes.data,
+                           _f(box).ctypes.data, k.ctypes.data, i.ctypes.data)
     k, i = k[: 8 * n], i[: 8 * n]
     order = np.argsort(k, kind="stable")
     k, i = np.ascontiguousarray(k[order]), np.ascontiguousarray(i[order])
@@ -121,8 +126,9 @@ def voxelbvh_fixture(L, cloud, res):
     starts, scan = np.zeros(N, np.uint32), np.zeros(N, np.uint32)
     headers = np.zeros(2 * N, np.uint32)
     L.ref_voxelbvh_ranges(N, k.ctypes.data, starts.ctypes.data, scan.ctypes.data, headers.ctypes.data)
+    extra = {} if T is None else {"transform": _f(T), "transform_inv": _f(Ti)}
     return dict(means=m, quats=q, scales=s, opacities=o, resolution=np.uint32(res), world_bbox=_f(box),
-                ijkl=k, prim_id=i, range=headers, ranges=np.int64(scan[-1] if N else 0))
+                ijkl=k, prim_id=i, range=headers, ranges=np.int64(scan[-1] if N else 0), **extra)
 
 
 def main():
@@ -134,6 +140,15 @@ def main():
     np.savez_compressed(os.path.join(HERE, "raster_clusters_cull0.01.npz"), **raster_fixture(L, cloud, vs, cull=0.01))
     for name, (cloud, res) in voxelbvh_cases().items():
         np.savez_compressed(os.path.join(HERE, f"voxelbvh_{name}.npz"), **voxelbvh_fixture(L, cloud, res))
+    # a transform (rows of the reference's pnanovdb_camera_mat_t, row vectors):
+    # rotation about z, uniform scale 1.5, translation
+    ang = 0.7
+    T = np.eye(4)
+    T[:3, :3] = np.array([[np.cos(ang), np.sin(ang), 0], [-np.sin(ang), np.cos(ang), 0], [0, 0, 1]]) * 1.5
+    T[3, :3] = [0.3, -2.0, 5.0]
+    cloud, res = voxelbvh_cases()["clusters_res512"]
+    np.savez_compressed(os.path.join(HERE, "voxelbvh_clusters_res512_transform.npz"),
+                        **voxelbvh_fixture(L, cloud, res, T.astype(np.float32)))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -68,7 +68,9 @@ def test_oracle_matches_golden_raster(oracle_mod, path):
 @pytest.mark.parametrize("path", _files("voxelbvh_"), ids=os.path.basename)
 def test_oracle_matches_golden_voxelbvh(oracle_mod, path):
     z = np.load(path)
-    out = oracle_mod.voxelbvh_ijkl(_cloud(z), int(z["resolution"]), nthreads=2)
+    T = np.array(z["transform"]) if "transform" in z else None
+    Ti = np.array(z["transform_inv"]) if "transform_inv" in z else None
+    out = oracle_mod.voxelbvh_ijkl(_cloud(z), int(z["resolution"]), T, Ti, nthreads=2)
     np.testing.assert_array_equal(out["world_bbox"].view(np.uint32), z["world_bbox"].view(np.uint32))
     np.testing.assert_array_equal(out["ijkl"], z["ijkl"])
     np.testing.assert_array_equal(out["prim_id"], z["prim_id"])
