@@ -217,6 +217,27 @@ PNANOVDB_API pnanovdb_raster_t* pnanovdb_get_raster(void);
 /* replaces the compute table the reference builds in compute/Compute.cpp */
 PNANOVDB_API pnanovdb_compute_t* pnanovdb_get_compute(void);
 
+/* ------------------------------------------------------- file formats -- */
+/* Layout of pnanovdb_fileformat_t (nanovdb_editor/putil/FileFormat.h:19-36,
+ * without the optional e57 entry).  load_file fills out_arrays[i] with the
+ * float32 array named array_names[i] ("means", "opacities", "quaternions",
+ * "scales", "sh_0", "sh_n", "colors"; NULL when the file has none), each freed
+ * with the compute table's destroy_array, and returns FALSE when the file
+ * cannot be read or lacks one of the arrays (fileformat/FileFormat.cpp:87-205,
+ * :754-800).  Formats: .npz (stored or deflated entries; an "sh" array of
+ * shape (G, K, 3) stands for sh_0 / sh_n) and binary .ply. */
+typedef struct pnanovdb_fileformat_t
+{
+    void* interface_pnanovdb_reflect_data_type;
+    pnanovdb_bool_t(PNANOVDB_ABI* can_load_file)(const char* filename);
+    pnanovdb_bool_t(PNANOVDB_ABI* load_file)(const char* filename, pnanovdb_uint32_t array_count,
+                                             const char** array_names, pnanovdb_compute_array_t** out_arrays);
+    void* module;
+} pnanovdb_fileformat_t;
+
+/* replaces fileformat/FileFormat.cpp:803-811 (libpnanovdbfileformat) */
+PNANOVDB_API pnanovdb_fileformat_t* pnanovdb_get_fileformat(void);
+
 /* ------------------------------------------------------ grid container -- */
 /* The grid buffer this library produces.  The reference returns a NanoVDB
  * grid whose GridData/TreeData headers come from PNanoVDB.h, which the

@@ -57,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [nvcc(), *NVCC_FLAGS, "-shared", f"-I{INCLUDE}", f"-I{CSRC}", *sources(), "-o", LIB]
+    cmd = [nvcc(), *NVCC_FLAGS, "-shared", f"-I{INCLUDE}", f"-I{CSRC}", *sources(), "-lz", "-o", LIB]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

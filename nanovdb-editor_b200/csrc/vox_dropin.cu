@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -17,19 +18,28 @@
 #include "pnanovdb_b200.h"
 
 // ------------------------------------------------------------- queue / device
-struct pnanovdb_compute_device_t
-{
-    int index;
-    pnanovdb_compute_queue_t* queue;
-};
+// A queue is a CUDA device plus its own voxelization context (one stream and
+// its buffers), created on the queue's first raster call.  The reference's
+// callers are editor worker threads, each with its own queue
+// (editor/PipelineRuntime.cpp:416-427), so calls on different queues run
+// concurrently; the per-queue mutex only serialises callers that share a queue.
 struct pnanovdb_compute_queue_t
 {
-    int device;
+    int device = 0;
+    std::mutex mu;
+    vox_context_t* vox = nullptr;
+};
+struct pnanovdb_compute_device_t
+{
+    int index = 0;
+    pnanovdb_compute_queue_t* queue = nullptr;         // get_device_queue
+    pnanovdb_compute_queue_t* compute_queue = nullptr; // get_compute_queue
 };
 
 struct pnanovdb_raster_context_t
 {
     vox_context_t* vox;
+    std::mutex mu;
 };
 
 struct pnanovdb_raster_gaussian_data_t
@@ -50,6 +60,50 @@ static int queue_device(pnanovdb_compute_queue_t* q)
 static void log_err(const char* msg)
 {
     fprintf(stderr, "[pnanovdb_b200] %s\n", msg);
+}
+
+// Table entries run their bodies through this: no C++ exception (an allocation
+// failure, say) crosses the C ABI; it is logged and the entry's failure value
+// returned, as the reference's entries report errors (log + FALSE / NULL).
+template <class R, class F>
+static R no_throw(const char* entry, R fail, F&& body)
+{
+    try
+    {
+        return body();
+    }
+    catch (const std::bad_alloc&)
+    {
+        fprintf(stderr, "[pnanovdb_b200] %s: out of host memory\n", entry);
+    }
+    catch (const std::exception& e)
+    {
+        fprintf(stderr, "[pnanovdb_b200] %s: %s\n", entry, e.what());
+    }
+    catch (...)
+    {
+        fprintf(stderr, "[pnanovdb_b200] %s: unexpected error\n", entry);
+    }
+    return fail;
+}
+
+// callers that pass no queue share one default queue per device
+constexpr int MAX_DEVICES = 64;
+static pnanovdb_compute_queue_t g_default_queue[MAX_DEVICES];
+
+static pnanovdb_compute_queue_t* resolve_queue(pnanovdb_compute_queue_t* q)
+{
+    if (q)
+        return q;
+    return &g_default_queue[0];
+}
+
+// the queue's context; the caller holds q->mu
+static vox_context_t* queue_context(pnanovdb_compute_queue_t* q)
+{
+    if (!q->vox)
+        q->vox = vox_context_create(q->device);
+    return q->vox;
 }
 
 // cull scale from gaussian_frag_color's parameter block (gaussian_frag_color.slang:205-213)
@@ -234,24 +288,57 @@ static pnanovdb_bool_t PNANOVDB_ABI dev_enumerate(void*, pnanovdb_uint32_t index
     }
     return (int)index < n ? PNANOVDB_TRUE : PNANOVDB_FALSE;
 }
-static pnanovdb_compute_device_t* PNANOVDB_ABI dev_create(void*, const void*)
+static pnanovdb_compute_queue_t* new_queue(int device)
 {
-    pnanovdb_compute_device_t* d = new pnanovdb_compute_device_t();
-    d->index = 0;
-    d->queue = new pnanovdb_compute_queue_t();
-    d->queue->device = 0;
-    return d;
+    pnanovdb_compute_queue_t* q = new pnanovdb_compute_queue_t();
+    q->device = device;
+    return q;
+}
+static void delete_queue(pnanovdb_compute_queue_t* q)
+{
+    if (!q)
+        return;
+    if (q->vox)
+        vox_context_destroy(q->vox);
+    delete q;
+}
+// desc: pnanovdb_compute_device_desc_t (nanovdb_editor/putil/Compute.h:503-508),
+// whose first field is the device index
+static pnanovdb_compute_device_t* PNANOVDB_ABI dev_create(void*, const void* desc)
+{
+    return no_throw<pnanovdb_compute_device_t*>("create_device", nullptr, [&]() -> pnanovdb_compute_device_t* {
+        uint32_t index = 0;
+        if (desc)
+            memcpy(&index, desc, sizeof(index));
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || (int)index >= n)
+        {
+            cudaGetLastError();
+            log_err("create_device: no such CUDA device");
+            return nullptr;
+        }
+        pnanovdb_compute_device_t* d = new pnanovdb_compute_device_t();
+        d->index = (int)index;
+        d->queue = new_queue((int)index);
+        d->compute_queue = new_queue((int)index);
+        return d;
+    });
 }
 static void PNANOVDB_ABI dev_destroy(void*, pnanovdb_compute_device_t* d)
 {
     if (!d)
         return;
-    delete d->queue;
+    delete_queue(d->queue);
+    delete_queue(d->compute_queue);
     delete d;
 }
 static pnanovdb_compute_queue_t* PNANOVDB_ABI dev_queue(const pnanovdb_compute_device_t* d)
 {
     return d ? d->queue : nullptr;
+}
+static pnanovdb_compute_queue_t* PNANOVDB_ABI dev_compute_queue(const pnanovdb_compute_device_t* d)
+{
+    return d ? d->compute_queue : nullptr;
 }
 static int PNANOVDB_ABI dev_flush(pnanovdb_compute_queue_t*, pnanovdb_uint64_t* flushed, void*, void*)
 {
@@ -261,6 +348,15 @@ static int PNANOVDB_ABI dev_flush(pnanovdb_compute_queue_t*, pnanovdb_uint64_t* 
 }
 static void PNANOVDB_ABI dev_wait_idle(pnanovdb_compute_queue_t* q)
 {
+    if (q)
+    {
+        std::lock_guard<std::mutex> lock(q->mu);
+        if (q->vox)
+        {
+            cudaStreamSynchronize((cudaStream_t)vox_context_stream(q->vox));
+            return;
+        }
+    }
     cudaSetDevice(queue_device(q));
     cudaDeviceSynchronize();
 }
@@ -270,28 +366,17 @@ static pnanovdb_uint32_t PNANOVDB_ABI dev_index(const pnanovdb_compute_device_t*
 }
 
 // ------------------------------------------------------------------- raster
-// one cached vox context per device for the one-shot entry points
-static std::mutex g_oneshot_mutex;
-static vox_context_t* g_oneshot[64] = {};
-
-static vox_context_t* oneshot_context(int device)
-{
-    if (device < 0 || device >= 64)
-        device = 0;
-    if (!g_oneshot[device])
-        g_oneshot[device] = vox_context_create(device);
-    return g_oneshot[device];
-}
-
 static pnanovdb_raster_context_t* PNANOVDB_ABI r_create_context(const pnanovdb_compute_t*,
                                                                   pnanovdb_compute_queue_t* queue)
 {
-    vox_context_t* v = vox_context_create(queue_device(queue));
-    if (!v)
-        return nullptr;
-    pnanovdb_raster_context_t* c = new pnanovdb_raster_context_t();
-    c->vox = v;
-    return c;
+    return no_throw<pnanovdb_raster_context_t*>("create_context", nullptr, [&]() -> pnanovdb_raster_context_t* {
+        vox_context_t* v = vox_context_create(queue_device(queue));
+        if (!v)
+            return nullptr;
+        pnanovdb_raster_context_t* c = new pnanovdb_raster_context_t();
+        c->vox = v;
+        return c;
+    });
 }
 static void PNANOVDB_ABI r_destroy_context(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
                                            pnanovdb_raster_context_t* c)
@@ -310,6 +395,8 @@ static bool copy_floats(std::vector<float>& dst, pnanovdb_compute_array_t* a, in
     return true;
 }
 
+// raster/RasterContext.cpp:92-229: copies the caller's arrays (activated
+// attributes; colours from `colors`, else from sh_0 as c0 * sh_0 + 0.5)
 static pnanovdb_raster_gaussian_data_t* PNANOVDB_ABI r_create_gaussian_data(
     const pnanovdb_compute_t*, pnanovdb_compute_queue_t* queue, pnanovdb_raster_context_t*,
     pnanovdb_compute_array_t* means, pnanovdb_compute_array_t* quaternions, pnanovdb_compute_array_t* scales,
@@ -317,45 +404,49 @@ static pnanovdb_raster_gaussian_data_t* PNANOVDB_ABI r_create_gaussian_data(
     pnanovdb_compute_array_t* opacities, pnanovdb_compute_array_t** shader_params_arrays,
     pnanovdb_raster_shader_params_t*)
 {
-    if (!means || means->element_size != 4)
-    {
-        log_err("create_gaussian_data: means must be float32");
-        return nullptr;
-    }
-    pnanovdb_raster_gaussian_data_t* d = new pnanovdb_raster_gaussian_data_t();
-    d->n = (int64_t)(means->element_count / 3);
-    d->device = queue_device(queue);
-    bool ok = copy_floats(d->means, means, 3 * d->n) && copy_floats(d->quats, quaternions, 4 * d->n) &&
-              copy_floats(d->scales, scales, 3 * d->n) && copy_floats(d->opacities, opacities, d->n);
-    if (ok && colors)
-        ok = copy_floats(d->colors, colors, 3 * d->n);
-    else if (ok && sh_0)
-    {
-        ok = copy_floats(d->colors, sh_0, 3 * d->n);
-        for (auto& c : d->colors)
-            c = 0.28209479177387814f * c + 0.5f;
-    }
-    if (!ok)
-    {
-        log_err("create_gaussian_data: attribute arrays must be float32 with 3/4/3/3/1 values per Gaussian");
-        delete d;
-        return nullptr;
-    }
-    d->cull_scale = cull_from_params(shader_params_arrays);
-    return d;
+    return no_throw<pnanovdb_raster_gaussian_data_t*>("create_gaussian_data", nullptr, [&]() -> pnanovdb_raster_gaussian_data_t* {
+        if (!means || means->element_size != 4)
+        {
+            log_err("create_gaussian_data: means must be float32");
+            return nullptr;
+        }
+        std::unique_ptr<pnanovdb_raster_gaussian_data_t> d(new pnanovdb_raster_gaussian_data_t());
+        d->n = (int64_t)(means->element_count / 3);
+        d->device = queue_device(queue);
+        bool ok = copy_floats(d->means, means, 3 * d->n) && copy_floats(d->quats, quaternions, 4 * d->n) &&
+                  copy_floats(d->scales, scales, 3 * d->n) && copy_floats(d->opacities, opacities, d->n);
+        if (ok && colors)
+            ok = copy_floats(d->colors, colors, 3 * d->n);
+        else if (ok && sh_0)
+        {
+            ok = copy_floats(d->colors, sh_0, 3 * d->n);
+            for (auto& c : d->colors)
+                c = 0.28209479177387814f * c + 0.5f;
+        }
+        else
+            ok = false;
+        if (!ok)
+        {
+            log_err("create_gaussian_data: attribute arrays must be float32 with 3/4/3/3/1 values per Gaussian");
+            return nullptr;
+        }
+        d->cull_scale = cull_from_params(shader_params_arrays);
+        return d.release();
+    });
 }
 
+// the device copy of the attributes, one allocation: means, quats, scales, opacities, colours
 static void PNANOVDB_ABI r_upload_gaussian_data(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
-                                                pnanovdb_raster_context_t* ctx, pnanovdb_raster_gaussian_data_t* d)
+                                                pnanovdb_raster_context_t*, pnanovdb_raster_gaussian_data_t* d)
 {
     if (!d)
         return;
-    (void)ctx;
     cudaSetDevice(d->device);
     if (d->dev)
         cudaFree(d->dev);
     d->dev = nullptr;
-    size_t floats = (size_t)d->n * 14;
+    const int64_t n = d->n;
+    const size_t floats = (size_t)n * 14;
     if (cudaMalloc(&d->dev, floats * 4 + 4) != cudaSuccess)
     {
         cudaGetLastError();
@@ -363,12 +454,18 @@ static void PNANOVDB_ABI r_upload_gaussian_data(const pnanovdb_compute_t*, pnano
         d->dev = nullptr;
         return;
     }
-    int64_t n = d->n;
-    cudaMemcpy(d->dev, d->means.data(), 12 * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(d->dev + 3 * n, d->quats.data(), 16 * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(d->dev + 7 * n, d->scales.data(), 12 * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(d->dev + 10 * n, d->opacities.data(), 4 * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(d->dev + 11 * n, d->colors.data(), 12 * n, cudaMemcpyHostToDevice);
+    bool ok = cudaMemcpy(d->dev, d->means.data(), 12 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(d->dev + 3 * n, d->quats.data(), 16 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(d->dev + 7 * n, d->scales.data(), 12 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(d->dev + 10 * n, d->opacities.data(), 4 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(d->dev + 11 * n, d->colors.data(), 12 * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok)
+    {
+        cudaGetLastError();
+        log_err("upload_gaussian_data: host to device copy failed");
+        cudaFree(d->dev);
+        d->dev = nullptr;
+    }
 }
 
 static void PNANOVDB_ABI r_destroy_gaussian_data(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
@@ -392,7 +489,10 @@ static void PNANOVDB_ABI r_raster_gaussian_2d(const pnanovdb_compute_t*, pnanovd
     log_err("raster_gaussian_2d: the screen-space splatting path is not provided by this library");
 }
 
-// raster/Raster.cpp:420-558: device Gaussians -> grid in the caller's device buffer
+// raster/Raster.cpp:420-558: uploaded Gaussians -> the reference's output, the
+// node2 tree and its RGBA8 values (vox_copy_grid_rgba8), written to the
+// caller's device buffer of word_count 32-bit words.  A void entry: failures
+// are logged, as the reference's are.
 static void PNANOVDB_ABI r_raster_gaussian_3d(const pnanovdb_compute_t*, pnanovdb_compute_queue_t*,
                                               pnanovdb_raster_context_t* ctx, float voxel_size,
                                               pnanovdb_raster_gaussian_data_t* d, pnanovdb_compute_buffer_t* out,
@@ -403,12 +503,13 @@ static void PNANOVDB_ABI r_raster_gaussian_3d(const pnanovdb_compute_t*, pnanovd
         log_err("raster_gaussian_3d: missing context, data or output buffer");
         return;
     }
+    std::lock_guard<std::mutex> lock(ctx->mu);
     if (!d->dev)
         r_upload_gaussian_data(nullptr, nullptr, ctx, d);
     if (!d->dev)
         return;
     vox_gaussians_t g;
-    int64_t n = d->n;
+    const int64_t n = d->n;
     g.count = n;
     g.means = d->dev;
     g.quats = d->dev + 3 * n;
@@ -417,39 +518,52 @@ static void PNANOVDB_ABI r_raster_gaussian_3d(const pnanovdb_compute_t*, pnanovd
     g.colors = d->dev + 11 * n;
     void* grid = nullptr;
     uint64_t bytes = 0;
-    if (vox_voxelize(ctx->vox, &g, voxel_size, d->cull_scale, (d->raw ? VOX_FLAG_RAW_INPUTS : 0u) | DROPIN_ORDER, &grid, &bytes) !=
-        VOX_OK)
+    if (vox_voxelize(ctx->vox, &g, voxel_size, d->cull_scale, (d->raw ? VOX_FLAG_RAW_INPUTS : 0u) | DROPIN_ORDER,
+                     &grid, &bytes) != VOX_OK)
+    {
+        log_err((std::string("raster_gaussian_3d: ") + vox_last_error(ctx->vox)).c_str());
         return;
+    }
     uint64_t cap = word_count * 4ull;
     if (out->size_bytes && out->size_bytes < cap)
         cap = out->size_bytes;
-    if (bytes > cap)
-    {
-        log_err("raster_gaussian_3d: output buffer too small for the grid");
-        return;
-    }
-    cudaMemcpyAsync(out->device_ptr, grid, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)vox_context_stream(ctx->vox));
-    cudaStreamSynchronize((cudaStream_t)vox_context_stream(ctx->vox));
+    const int rc = vox_copy_grid_rgba8(ctx->vox, out->device_ptr, cap, &bytes);
+    if (rc == VOX_ERR_SIZE)
+        log_err("raster_gaussian_3d: output buffer too small for the node2 grid and its RGBA8 values");
+    else if (rc != VOX_OK)
+        log_err((std::string("raster_gaussian_3d: ") + vox_last_error(ctx->vox)).c_str());
 }
 
-static pnanovdb_compute_array_t* run_host(int device, const vox_gaussians_t* g, float voxel_size, float cull,
-                                          uint32_t flags, pnanovdb_profiler_report_t report, void* userdata)
+// voxelizes host arrays on the queue's context; the result is what the
+// reference's host entries return: the node2 tree and its RGBA8 values
+static pnanovdb_compute_array_t* run_host(pnanovdb_compute_queue_t* queue, const vox_gaussians_t* g, float voxel_size,
+                                          float cull, uint32_t flags, pnanovdb_profiler_report_t report, void* userdata,
+                                          const char* entry)
 {
-    std::lock_guard<std::mutex> lock(g_oneshot_mutex);
-    vox_context_t* v = oneshot_context(device);
+    pnanovdb_compute_queue_t* q = resolve_queue(queue);
+    std::lock_guard<std::mutex> lock(q->mu);
+    vox_context_t* v = queue_context(q);
     if (!v)
+    {
+        fprintf(stderr, "[pnanovdb_b200] %s: cannot create a CUDA context on device %d\n", entry, q->device);
         return nullptr;
+    }
     uint64_t bytes = 0;
-    if (vox_voxelize_host(v, g, voxel_size, cull, flags, nullptr, 0, &bytes) != VOX_OK)
+    if (vox_voxelize_host(v, g, voxel_size, cull, flags, nullptr, 0, &bytes) != VOX_OK ||
+        vox_copy_grid_rgba8(v, nullptr, 0, &bytes) != VOX_OK)
+    {
+        fprintf(stderr, "[pnanovdb_b200] %s: %s\n", entry, vox_last_error(v));
         return nullptr;
-    // what the reference returns: node2 tree and RGBA8 values
-    if (vox_copy_grid_rgba8(v, nullptr, 0, &bytes) != VOX_OK)
-        return nullptr;
+    }
     pnanovdb_compute_array_t* a = array_create_pinned(4, (bytes + 3) / 4);
     if (!a)
+    {
+        fprintf(stderr, "[pnanovdb_b200] %s: out of page-locked host memory\n", entry);
         return nullptr;
+    }
     if (vox_copy_grid_rgba8(v, a->data, 4 * a->element_count, &bytes) != VOX_OK)
     {
+        fprintf(stderr, "[pnanovdb_b200] %s: %s\n", entry, vox_last_error(v));
         array_destroy(a);
         return nullptr;
     }
@@ -473,24 +587,27 @@ static pnanovdb_compute_array_t* PNANOVDB_ABI r_raster_to_nanovdb(
     pnanovdb_compute_array_t* sh_0, pnanovdb_compute_array_t* sh_n, pnanovdb_compute_array_t* opacities,
     pnanovdb_compute_array_t** shader_params_arrays, pnanovdb_profiler_report_t profiler_report, void* userdata)
 {
-    pnanovdb_raster_gaussian_data_t* d = r_create_gaussian_data(nullptr, queue, nullptr, means, quaternions, scales,
-                                                                colors, sh_0, sh_n, opacities, shader_params_arrays,
-                                                                nullptr);
-    if (!d)
-        return nullptr;
-    vox_gaussians_t g;
-    g.count = d->n;
-    g.means = d->means.data();
-    g.quats = d->quats.data();
-    g.scales = d->scales.data();
-    g.opacities = d->opacities.data();
-    g.colors = d->colors.data();
-    pnanovdb_compute_array_t* a = run_host(queue_device(queue), &g, voxel_size, d->cull_scale, DROPIN_ORDER, profiler_report,
-                                           userdata);
-    r_destroy_gaussian_data(nullptr, nullptr, d);
-    return a;
+    return no_throw<pnanovdb_compute_array_t*>("raster_to_nanovdb", nullptr, [&]() -> pnanovdb_compute_array_t* {
+        pnanovdb_raster_gaussian_data_t* d = r_create_gaussian_data(nullptr, queue, nullptr, means, quaternions, scales,
+                                                                    colors, sh_0, sh_n, opacities, shader_params_arrays,
+                                                                    nullptr);
+        if (!d)
+            return nullptr;
+        std::unique_ptr<pnanovdb_raster_gaussian_data_t, void (*)(pnanovdb_raster_gaussian_data_t*)> hold(
+            d, [](pnanovdb_raster_gaussian_data_t* x) { r_destroy_gaussian_data(nullptr, nullptr, x); });
+        vox_gaussians_t g;
+        g.count = d->n;
+        g.means = d->means.data();
+        g.quats = d->quats.data();
+        g.scales = d->scales.data();
+        g.opacities = d->opacities.data();
+        g.colors = d->colors.data();
+        return run_host(queue, &g, voxel_size, d->cull_scale, DROPIN_ORDER, profiler_report, userdata,
+                        "raster_to_nanovdb");
+    });
 }
 
+// raster/RasterUtils.cpp:400-415
 static pnanovdb_bool_t PNANOVDB_ABI r_from_arrays(pnanovdb_raster_t*, const pnanovdb_compute_t*,
                                                   pnanovdb_compute_queue_t* queue, float voxel_size,
                                                   pnanovdb_compute_array_t** arrays, pnanovdb_uint32_t count,
@@ -499,32 +616,35 @@ static pnanovdb_bool_t PNANOVDB_ABI r_from_arrays(pnanovdb_raster_t*, const pnan
     if (!out || !arrays || count < 5u)
         return PNANOVDB_FALSE;
     *out = nullptr;
-    pnanovdb_compute_array_t *m = arrays[0], *o = arrays[1], *q = arrays[2], *s = arrays[3], *c = arrays[4];
-    if (!m || !o || !q || !s || !c || m->element_size != 4 || o->element_size != 4 || q->element_size != 4 ||
-        s->element_size != 4 || c->element_size != 4)
-    {
-        log_err("raster_to_nanovdb_from_arrays: arrays must be float32 [means, opacities, quaternions, scales, sh_0]");
-        return PNANOVDB_FALSE;
-    }
-    int64_t n = (int64_t)(m->element_count / 3);
-    if ((int64_t)o->element_count < n || (int64_t)q->element_count < 4 * n || (int64_t)s->element_count < 3 * n ||
-        (int64_t)c->element_count < 3 * n)
-    {
-        log_err("raster_to_nanovdb_from_arrays: attribute counts do not match means");
-        return PNANOVDB_FALSE;
-    }
-    // raw inputs: the reference preprocesses them on the host in place
-    // (RasterUtils.cpp:59-117); here the same arithmetic runs inside the prep
-    // kernel and the caller's arrays are left untouched.
-    vox_gaussians_t g;
-    g.count = n;
-    g.means = (const float*)m->data;
-    g.quats = (const float*)q->data;
-    g.scales = (const float*)s->data;
-    g.opacities = (const float*)o->data;
-    g.colors = (const float*)c->data;
-    *out = run_host(queue_device(queue), &g, voxel_size, 0.05f, VOX_FLAG_RAW_INPUTS | DROPIN_ORDER, nullptr, nullptr);
-    return *out ? PNANOVDB_TRUE : PNANOVDB_FALSE;
+    return no_throw<pnanovdb_bool_t>("raster_to_nanovdb_from_arrays", PNANOVDB_FALSE, [&]() -> pnanovdb_bool_t {
+        pnanovdb_compute_array_t *m = arrays[0], *o = arrays[1], *q = arrays[2], *s = arrays[3], *c = arrays[4];
+        if (!m || !o || !q || !s || !c || m->element_size != 4 || o->element_size != 4 || q->element_size != 4 ||
+            s->element_size != 4 || c->element_size != 4)
+        {
+            log_err("raster_to_nanovdb_from_arrays: arrays must be float32 [means, opacities, quaternions, scales, sh_0]");
+            return PNANOVDB_FALSE;
+        }
+        const int64_t n = (int64_t)(m->element_count / 3);
+        if ((int64_t)o->element_count < n || (int64_t)q->element_count < 4 * n || (int64_t)s->element_count < 3 * n ||
+            (int64_t)c->element_count < 3 * n)
+        {
+            log_err("raster_to_nanovdb_from_arrays: attribute counts do not match means");
+            return PNANOVDB_FALSE;
+        }
+        // raw inputs: the reference preprocesses them on the host in place
+        // (RasterUtils.cpp:59-117); here the same arithmetic runs inside the prep
+        // kernel and the caller's arrays are left untouched.
+        vox_gaussians_t g;
+        g.count = n;
+        g.means = (const float*)m->data;
+        g.quats = (const float*)q->data;
+        g.scales = (const float*)s->data;
+        g.opacities = (const float*)o->data;
+        g.colors = (const float*)c->data;
+        *out = run_host(queue, &g, voxel_size, 0.05f, VOX_FLAG_RAW_INPUTS | DROPIN_ORDER, nullptr, nullptr,
+                        "raster_to_nanovdb_from_arrays");
+        return *out ? PNANOVDB_TRUE : PNANOVDB_FALSE;
+    });
 }
 
 static pnanovdb_bool_t PNANOVDB_ABI r_create_from_arrays(pnanovdb_raster_t*, const pnanovdb_compute_t*,
@@ -579,35 +699,24 @@ void vb_activate_host(int64_t n, float* quats, float* scales, float* opac)
 
 } // namespace
 
-extern "C" {
-
-int vox_voxelbvh_ijkl_from_gaussians_file(vox_context_t* ctx, const char* filename, uint32_t resolution,
-                                          const float* transform, pnanovdb_compute_array_t** ijkl_out,
-                                          pnanovdb_compute_array_t** prim_id_out, pnanovdb_compute_array_t** range_out,
-                                          pnanovdb_compute_array_t** world_bbox_out,
-                                          pnanovdb_compute_array_t** gaussian_arrays_out,
-                                          uint32_t gaussian_array_count)
+static int vb_file_body(vox_context_t* ctx, const char* filename, uint32_t resolution, const float* transform,
+                        pnanovdb_compute_array_t** ijkl_out, pnanovdb_compute_array_t** prim_id_out,
+                        pnanovdb_compute_array_t** range_out, pnanovdb_compute_array_t** world_bbox_out,
+                        pnanovdb_compute_array_t** gaussian_arrays_out, uint32_t gaussian_array_count)
 {
     if (!ctx || !filename || !ijkl_out || !prim_id_out || !range_out || !world_bbox_out)
         return VOX_ERR_ARGS;
     *ijkl_out = *prim_id_out = *range_out = *world_bbox_out = nullptr;
     std::vector<NpzArray> arrays;
     std::string why;
-    bool loaded = false;
-    if (has_suffix(filename, ".ply"))
-        loaded = read_ply(filename, arrays, why);
-    else if (has_suffix(filename, ".npz"))
-        loaded = read_npz(filename, arrays, why);
-    else
-        why = "file format not supported (.npz and .ply are)";
-    if (!loaded)
+    if (!read_gaussian_file(filename, arrays, why, true))
     {
         log_err((std::string("ijkl_from_gaussians_file: failed to load '") + filename + "': " + why).c_str());
         return VOX_ERR_ARGS;
     }
     // means, opacities, quaternions, scales, sh_0, sh_n (the reference's names and order)
     const char* names[6] = { "means", "opacities", "quaternions", "scales", "sh_0", "sh_n" };
-    std::vector<float>* a[6] = {};
+    FloatBuf* a[6] = {};
     for (int i = 0; i < 6; i++)
         for (auto& x : arrays)
             if (x.name == names[i])
@@ -692,6 +801,21 @@ int vox_voxelbvh_ijkl_from_gaussians_file(vox_context_t* ctx, const char* filena
     return VOX_OK;
 }
 
+extern "C" {
+
+int vox_voxelbvh_ijkl_from_gaussians_file(vox_context_t* ctx, const char* filename, uint32_t resolution,
+                                          const float* transform, pnanovdb_compute_array_t** ijkl_out,
+                                          pnanovdb_compute_array_t** prim_id_out, pnanovdb_compute_array_t** range_out,
+                                          pnanovdb_compute_array_t** world_bbox_out,
+                                          pnanovdb_compute_array_t** gaussian_arrays_out,
+                                          uint32_t gaussian_array_count)
+{
+    return no_throw<int>("ijkl_from_gaussians_file", VOX_ERR_MEMORY, [&]() {
+        return vb_file_body(ctx, filename, resolution, transform, ijkl_out, prim_id_out, range_out, world_bbox_out,
+                            gaussian_arrays_out, gaussian_array_count);
+    });
+}
+
 pnanovdb_compute_t* pnanovdb_get_compute(void)
 {
     static pnanovdb_compute_t t;
@@ -705,7 +829,7 @@ pnanovdb_compute_t* pnanovdb_get_compute(void)
         t.device_interface.create_device = dev_create;
         t.device_interface.destroy_device = dev_destroy;
         t.device_interface.get_device_queue = dev_queue;
-        t.device_interface.get_compute_queue = dev_queue;
+        t.device_interface.get_compute_queue = dev_compute_queue;
         t.device_interface.flush = dev_flush;
         t.device_interface.wait_idle = dev_wait_idle;
         t.device_interface.get_device_index = dev_index;
@@ -718,6 +842,12 @@ pnanovdb_compute_t* pnanovdb_get_compute(void)
         t.duplicate_array = array_duplicate;
         init = true;
     }
+    return &t;
+}
+
+pnanovdb_fileformat_t* pnanovdb_get_fileformat(void)
+{
+    static pnanovdb_fileformat_t t = { nullptr, ff_can_load_file, ff_load_file, nullptr };
     return &t;
 }
 
