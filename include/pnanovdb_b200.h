@@ -340,6 +340,18 @@ PNANOVDB_API void vox_context_destroy(vox_context_t* ctx);
 PNANOVDB_API void* vox_context_stream(vox_context_t* ctx);
 PNANOVDB_API const char* vox_last_error(vox_context_t* ctx);
 
+/* Bounded device waits.  The single-pass scans, the onesweep sort and the run
+ * detection wait on their predecessor tiles (decoupled look-back); every such
+ * wait gives up after a bounded number of polls, records the failure and lets
+ * the kernel finish, and the call returns VOX_ERR_TIMEOUT with the context
+ * still usable.  This sets that bound for later calls on ctx: max_polls polls
+ * per wait (VOX_WAIT_DEFAULT restores the default of 2^22 polls of >= 32 ns);
+ * withhold_publication != 0 also stops those calls' tiles from publishing, so
+ * every wait runs out - a test of the error path (no counterpart in the
+ * reference, whose Vulkan dispatches have no inter-workgroup waits). */
+#define VOX_WAIT_DEFAULT 0xffffffffu
+PNANOVDB_API int vox_context_set_wait_limit(vox_context_t* ctx, uint32_t max_polls, int withhold_publication);
+
 /* Voxelizes device-resident Gaussians (the path of raster_gaussian_3d,
  * raster/Raster.cpp:420-558).  On success *grid (device) points at the
  * context-owned grid buffer (valid until the next call) and *grid_bytes is
@@ -519,21 +531,24 @@ PNANOVDB_API int vox_voxelbvh_transform_inverse(const float* m, float* inv);
 
 /* Scan that allocates nothing.  No counterpart in the reference.
  *
- * Same result as vox_global_scan_u64, for callers that cannot let a library
- * allocate device memory: hosts whose device memory is owned by their own
- * allocator (a framework's caching pool holding the free memory, where an
- * extra cudaMalloc can fail or fragment it) and loops where the implicit
- * device synchronisation of cudaMalloc / cudaFree is not acceptable.  It
- * needs no vox_context_t and calls no cudaMalloc, cudaFree or other
- * allocating routine: its look-back scratch is a fixed 64 KiB device array
+ * Same result as vox_global_scan_u64 (exact mod 2^64), for callers that cannot
+ * let a library allocate device memory: hosts whose device memory is owned by
+ * their own allocator (a framework's caching pool holding the free memory,
+ * where an extra cudaMalloc can fail or fragment it) and loops where the
+ * implicit device synchronisation of cudaMalloc / cudaFree is not acceptable.
+ * It needs no vox_context_t and calls no cudaMalloc, cudaFree or other
+ * allocating routine: its look-back scratch is a fixed 256 KiB device array
  * inside the library (held by every GPU that loads the library until exit),
  * which limits n to VOX_NOALLOC_SCAN_MAX; larger n returns VOX_ERR_SIZE.
  *
- * The first call on each device looks up that array's device address, so
- * make it before any stream capture.  All calls share the one array: calls
- * whose work overlaps on the GPU (concurrent streams or threads) race and
- * must be serialised by the caller.  The call is ordered on `stream`
- * (cudaStream_t, may be 0) and returns after the scan has completed. */
+ * Each call looks up that array's address on the current device, so the
+ * first call on a device also loads the library's kernels there.  All calls
+ * share the one array and it keeps the last call's contents (each call clears
+ * what it uses first): calls whose work overlaps on the GPU (concurrent
+ * streams or threads) race and must be serialised by the caller.  The call is
+ * ordered on `stream` (cudaStream_t, may be 0) and synchronises it before
+ * returning (it reads the device error word back), so it cannot be recorded
+ * into a stream capture. */
 #define VOX_NOALLOC_SCAN_MAX (1ll << 24)
 PNANOVDB_API int vox_global_scan_u64_noalloc(const uint64_t* d_in, uint64_t* d_out, int64_t n, int inclusive,
                                              uint64_t* d_total, void* stream);

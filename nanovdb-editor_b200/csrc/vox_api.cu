@@ -49,6 +49,7 @@ struct vox_context_t
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
+    uint32_t wait_ctl = 0; // look-back wait control (0: default limit), see vox_context_set_wait_limit
     std::string last_error;
     std::vector<DevBuf*> bufs;
     // device buffers
@@ -135,6 +136,21 @@ static void set_error(vox_context_t* ctx, const char* fmt, ...)
     if (ctx)
         ctx->last_error = buf;
     fprintf(stderr, "[pnanovdb_b200] %s\n", buf);
+}
+
+// The look-back wait control (vox_context_set_wait_limit) lives in the upper
+// half of the device error word, which every call clears: re-arm it.
+static void arm_wait(vox_context_t* ctx, uint64_t* sc, cudaStream_t s)
+{
+    if (ctx->wait_ctl)
+        cudaMemcpyAsync((uint32_t*)(sc + SC_ERR) + 1, &ctx->wait_ctl, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+}
+
+// zeroes the per-call device scalars (counts, error word) and re-arms the wait control
+static void clear_scalars(vox_context_t* ctx, uint64_t* sc, cudaStream_t s)
+{
+    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    arm_wait(ctx, sc, s);
 }
 
 static bool ensure(vox_context_t* ctx, DevBuf& b, size_t bytes)
@@ -349,7 +365,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     if (!ensure(ctx, ctx->scal, sizeof(uint64_t) * SC_SCRATCH * 4))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     int* d_err = (int*)(sc + SC_ERR);
     uint32_t* d_counter = (uint32_t*)(sc + SC_SCRATCH);
     cudaEventRecord(ctx->timers.ev[0], s);
@@ -867,6 +883,7 @@ static int run_backward(vox_context_t* ctx, const vox_gaussians_t* gs, const flo
         return VOX_ERR_MEMORY;
     cudaEventRecord(ctx->timers.ev[0], s);
     cudaMemsetAsync((uint64_t*)ctx->scal.p + SC_ERR, 0, sizeof(uint64_t), s);
+    arm_wait(ctx, (uint64_t*)ctx->scal.p, s);
     float* partials = (float*)ctx->partials.p;
     if (grad_density || grad_color)
     {
@@ -1016,6 +1033,20 @@ void vox_context_destroy(vox_context_t* ctx)
 void* vox_context_stream(vox_context_t* ctx)
 {
     return ctx ? (void*)ctx->stream : nullptr;
+}
+
+int vox_context_set_wait_limit(vox_context_t* ctx, uint32_t max_polls, int withhold_publication)
+{
+    if (!ctx)
+        return VOX_ERR_ARGS;
+    if (max_polls == VOX_WAIT_DEFAULT && !withhold_publication)
+    {
+        ctx->wait_ctl = 0;
+        return VOX_OK;
+    }
+    const uint32_t lim = max_polls > 0x7ffffffeu ? 0x7ffffffeu : max_polls;
+    ctx->wait_ctl = (lim + 1u) | (withhold_publication ? 0x80000000u : 0u);
+    return VOX_OK;
 }
 
 const char* vox_last_error(vox_context_t* ctx)
@@ -1249,7 +1280,7 @@ int vox_global_scan_u64(vox_context_t* ctx, const uint64_t* d_in, uint64_t* d_ou
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(n > 512 ? n : 512) * 2))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     uint64_t* status = (uint64_t*)ctx->scan_status.p;
     scan_exclusive_u64(d_in, d_out, n, inclusive ? 2 : 0, d_total, status,
                        ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s),
@@ -1268,7 +1299,7 @@ int vox_global_scan_u32(vox_context_t* ctx, const uint32_t* d_in, uint32_t* d_ou
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(n > 512 ? n : 512) * 2))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     uint64_t* status = (uint64_t*)ctx->scan_status.p;
     scan_u32(d_in, d_out, n, inclusive ? 1 : 0, 0, sc + SC_F, status,
              ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s), (uint32_t*)(sc + SC_SCRATCH),
@@ -1288,7 +1319,7 @@ int vox_global_scan_max_u32(vox_context_t* ctx, const uint32_t* d_in, uint32_t* 
         !ensure(ctx, ctx->scan_status, sizeof(uint64_t) * scan_status_words(n > 512 ? n : 512) * 2))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     uint64_t* status = (uint64_t*)ctx->scan_status.p;
     scan_u32(d_in, d_out, n, 1, 1, sc + SC_F, status,
              ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s), (uint32_t*)(sc + SC_SCRATCH),
@@ -1309,7 +1340,7 @@ int vox_radix_sort_u32(vox_context_t* ctx, uint32_t* d_keys, uint32_t* d_vals, i
         !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(n, 4)))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     int in_alt = sort_pairs_u32(d_keys, d_vals, (uint32_t*)ctx->prim_keys_alt.p, (uint32_t*)ctx->prim_vals_alt.p, n,
                                 (int)key_bit_count, ctx->sort_ws.p, &ctx->sort_epochs, (int*)(sc + SC_ERR),
                                 ctx->num_sms, s, ctx->tuning);
@@ -1338,7 +1369,7 @@ int vox_radix_sort_dual_key(vox_context_t* ctx, uint32_t* d_keys_low, uint32_t* 
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
     int* err = (int*)(sc + SC_ERR);
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     // one stable sort by (high, low): the order of the reference's sort by
     // the low key then, stably, by the high key (ParallelPrimitives.cpp:527-683)
     uint64_t* key = (uint64_t*)ctx->vb_keys.p;
@@ -1371,7 +1402,7 @@ int vox_radix_sort_key64(vox_context_t* ctx, uint64_t* d_keys, uint32_t* d_vals,
         !ensure(ctx, ctx->sort_ws, sort_workspace_bytes(n, 8)))
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     SortTuning& t = ctx->tuning;
     int in_alt = sort_pairs_u64(d_keys, d_vals, (uint64_t*)ctx->prim_keys_alt.p, (uint32_t*)ctx->prim_vals_alt.p, n,
                                 (int)key_bit_count, ctx->sort_ws.p, &ctx->sort_epochs, (int*)(sc + SC_ERR),
@@ -1487,7 +1518,7 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
         return VOX_ERR_MEMORY;
     uint64_t* sc = (uint64_t*)ctx->scal.p;
     int* err = (int*)(sc + SC_ERR);
-    cudaMemsetAsync(sc, 0, sizeof(uint64_t) * SC_COUNT, s);
+    clear_scalars(ctx, sc, s);
     P.box_keys = (uint32_t*)ctx->vb_work.p;
     P.cell_minmax = (int*)(sc + SC_BBOX);
     P.world_bbox = d_world_bbox;

@@ -547,7 +547,10 @@ __device__ __forceinline__ uint32_t pack_rgba8(const GaussRec& R, float a)
 
 // ------------------------------------------------------------------------
 // decoupled look-back status words: [63:56] epoch, [55] inclusive flag,
-// [54:0] value.  Epoch 0 means "not yet written in this use".
+// [54:0] value.  Epoch 0 means "not yet written in this use".  Values are
+// kept mod 2^55: the sort's digit counts, the run counts and the u32 scans
+// (whose sums are wanted mod 2^32) stay far below that; the u64 scan, whose
+// prefixes may use all 64 bits, uses lookback_exclusive_wide.
 // ------------------------------------------------------------------------
 constexpr uint64_t LB_VALUE_MASK = (1ull << 55) - 1ull;
 constexpr uint64_t LB_INCL = 1ull << 55;
@@ -564,21 +567,44 @@ __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p)
     return v;
 }
 
+// Wait control of a look-back, from the 32-bit word after the device error
+// word (err[1]): 0 = the default limit of LB_SPIN_LIMIT polls; otherwise bits
+// 30:0 hold limit + 1 and bit 31 withholds this call's publications, so every
+// successor waits on a word nothing writes.  Set only through
+// vox_context_set_wait_limit, to make the bounded waits run out in tests.
+struct LbControl
+{
+    uint32_t limit;
+    bool withhold;
+};
+__device__ __forceinline__ LbControl lb_control(const int* err)
+{
+    const uint32_t c = ((const volatile uint32_t*)err)[1];
+    LbControl o;
+    o.withhold = (c >> 31) != 0u;
+    o.limit = (c & 0x7fffffffu) ? (c & 0x7fffffffu) - 1u : LB_SPIN_LIMIT;
+    return o;
+}
+
 // Publishes `aggregate` for `tile`, walks predecessors and returns the
 // exclusive prefix.  Every wait is bounded; on timeout *err is set and the
-// partial prefix is returned (the host treats the call as failed).
+// partial prefix (never larger than the true one) is returned, and the host
+// treats the call as failed.
 // max_op: combine predecessors by maximum instead of sum (a running-max scan)
 __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_t tile, uint64_t aggregate,
                                                        uint32_t epoch, int* err, size_t stride = 1,
                                                        bool max_op = false)
 {
+    const LbControl ctl = lb_control(err);
     const uint64_t tag = (uint64_t)epoch << 56;
     if (tile == 0)
     {
-        st_release_u64(&status[0], tag | LB_INCL | (aggregate & LB_VALUE_MASK));
+        if (!ctl.withhold)
+            st_release_u64(&status[0], tag | LB_INCL | (aggregate & LB_VALUE_MASK));
         return 0;
     }
-    st_release_u64(&status[tile * stride], tag | (aggregate & LB_VALUE_MASK));
+    if (!ctl.withhold)
+        st_release_u64(&status[tile * stride], tag | (aggregate & LB_VALUE_MASK));
     uint64_t excl = 0;
     int64_t p = (int64_t)tile - 1;
     uint32_t spins = 0;
@@ -587,7 +613,7 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_
         uint64_t s = ld_acquire_u64(&status[(uint64_t)p * stride]);
         if ((s >> 56) != epoch)
         {
-            if (++spins > LB_SPIN_LIMIT)
+            if (++spins > ctl.limit)
             {
                 atomicOr(err, 1); // ERR_LOOKBACK
                 break;
@@ -602,7 +628,60 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_
         p--;
     }
     const uint64_t incl = max_op ? (aggregate > excl ? aggregate : excl) : excl + aggregate;
-    st_release_u64(&status[tile * stride], tag | LB_INCL | (incl & LB_VALUE_MASK));
+    if (!ctl.withhold)
+        st_release_u64(&status[tile * stride], tag | LB_INCL | (incl & LB_VALUE_MASK));
+    return excl;
+}
+
+// The same walk for sums that may use all 64 bits (the prefix is exact mod
+// 2^64, as uint64 addition is).  Per tile four words: the aggregate's low and
+// high halves, then the inclusive prefix's, each word (epoch << 32) | half.
+// Every word is written once per use, so two halves that both carry the
+// current epoch belong to the same value: a reader can never combine halves
+// of different values.
+__device__ __forceinline__ uint64_t lookback_exclusive_wide(uint64_t* status, uint64_t tile, uint64_t aggregate,
+                                                            uint32_t epoch, int* err)
+{
+    const LbControl ctl = lb_control(err);
+    const uint64_t tag = (uint64_t)epoch << 32;
+    uint64_t* mine = status + 4 * tile;
+    if (tile > 0 && !ctl.withhold)
+    {
+        st_release_u64(mine + 0, tag | (aggregate & 0xffffffffull));
+        st_release_u64(mine + 1, tag | (aggregate >> 32));
+    }
+    uint64_t excl = 0;
+    int64_t p = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (p >= 0)
+    {
+        const uint64_t* w = status + 4 * (uint64_t)p;
+        const uint64_t il = ld_acquire_u64(w + 2), ih = ld_acquire_u64(w + 3);
+        if ((il >> 32) == epoch && (ih >> 32) == epoch)
+        {
+            excl += (ih << 32) | (il & 0xffffffffull);
+            break;
+        }
+        const uint64_t al = ld_acquire_u64(w + 0), ah = ld_acquire_u64(w + 1);
+        if ((al >> 32) == epoch && (ah >> 32) == epoch)
+        {
+            excl += (ah << 32) | (al & 0xffffffffull);
+            p--;
+            continue;
+        }
+        if (++spins > ctl.limit)
+        {
+            atomicOr(err, 1); // ERR_LOOKBACK
+            break;
+        }
+        __nanosleep(32);
+    }
+    const uint64_t incl = excl + aggregate;
+    if (!ctl.withhold)
+    {
+        st_release_u64(mine + 2, tag | (incl & 0xffffffffull));
+        st_release_u64(mine + 3, tag | (incl >> 32));
+    }
     return excl;
 }
 

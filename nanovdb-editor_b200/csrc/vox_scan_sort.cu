@@ -31,9 +31,11 @@ constexpr int SCAN_BLOCK = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
 
+// status words of a scan of n elements: four per tile for the u64 scan (its
+// full 64-bit look-back), one per tile for the u32 scans
 size_t scan_status_words(int64_t n)
 {
-    return (size_t)((n + SCAN_TILE - 1) / SCAN_TILE) + 1;
+    return 4 * ((size_t)((n + SCAN_TILE - 1) / SCAN_TILE) + 1);
 }
 
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_excl(const uint64_t* in, uint64_t* out, int64_t n, int mode,
@@ -63,7 +65,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_excl(const uint64_t* in, ui
     uint64_t block_total;
     uint64_t texcl = block_excl_scan_u64(sum, s_warp, block_total);
     if (threadIdx.x == 0)
-        s_excl = lookback_exclusive(status, tile, block_total, epoch, err);
+        s_excl = lookback_exclusive_wide(status, tile, block_total, epoch, err);
     __syncthreads();
     uint64_t run = s_excl + texcl;
 #pragma unroll

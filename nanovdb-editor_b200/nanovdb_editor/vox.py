@@ -122,6 +122,8 @@ def _lib():
         lib.vox_voxelbvh_ijkl_from_gaussians_file.argtypes = [c_void_p, ctypes.c_char_p, c_uint32, c_void_p] + [c_void_p] * 5 + [c_uint32]
         lib.vox_voxelbvh_transform_inverse.restype = c_int
         lib.vox_voxelbvh_transform_inverse.argtypes = [c_void_p, c_void_p]
+        lib.vox_context_set_wait_limit.restype = c_int
+        lib.vox_context_set_wait_limit.argtypes = [c_void_p, c_uint32, c_int]
         lib._vox_bound = True
     return lib
 
@@ -265,6 +267,13 @@ class VoxContext:
         st = vox_stats_t()
         self.lib.vox_get_stats(self.handle, byref(st))
         return st.as_dict()
+
+    def set_wait_limit(self, max_polls=None, withhold_publication: bool = False) -> None:
+        """Bound of the device look-back waits for later calls (None: the
+        default); withhold_publication makes every wait run out (a test of the
+        VOX_ERR_TIMEOUT path)."""
+        polls = 0xFFFFFFFF if max_polls is None else int(max_polls)
+        self._check(self.lib.vox_context_set_wait_limit(self.handle, polls, 1 if withhold_publication else 0), "set_wait_limit")
 
     def global_scan_u64(self, d_in, d_out, d_total, inclusive: bool = True) -> None:
         """Scan of CUDA uint64 tensors (the reference's global_scan_uint64 is inclusive)."""

@@ -29,6 +29,35 @@ def test_scan_matches_numpy(vox_ctx, n, inclusive):
     assert int(d_tot.cpu().numpy().view(np.uint64)[0]) == int(x.sum())
 
 
+def _scan_ref(x, inclusive):
+    ref = np.cumsum(x, dtype=np.uint64)  # numpy uint64 addition wraps mod 2^64
+    if not inclusive and x.size:
+        ref = np.concatenate([[np.uint64(0)], ref[:-1]]).astype(np.uint64)
+    return ref
+
+
+@pytest.mark.parametrize("n", [2049, 700_001])
+@pytest.mark.parametrize("top", [1 << 40, 1 << 50, 1 << 62])
+def test_scan_full_64_bit_prefixes(vox_ctx, n, top):
+    # running sums that pass 2^55 (top 2^40 and 2^50 over many tiles) and wrap
+    # mod 2^64 (top 2^62): the reference's global_scan_uint64
+    # (raster/ParallelPrimitives.cpp:151-310) is plain uint64 arithmetic
+    import torch
+
+    rng = np.random.default_rng(n ^ top)
+    x = rng.integers(0, top, n, dtype=np.uint64)
+    for inclusive in (True, False):
+        d_in = torch.from_numpy(x.view(np.int64)).cuda()
+        d_out = torch.empty_like(d_in)
+        d_tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        vox_ctx.global_scan_u64(d_in, d_out, d_tot, inclusive)
+        np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint64), _scan_ref(x, inclusive))
+        assert int(d_tot.cpu().numpy().view(np.uint64)[0]) == int(x.sum(dtype=np.uint64))
+    if top == 1 << 40:
+        assert int(np.cumsum(x, dtype=np.uint64)[-1]) > (1 << 55)
+
+
 @pytest.mark.parametrize("n,bits", [(2, 64), (8191, 17), (8193, 64), (12_993_895, 64), (3_000_000, 33)])
 def test_radix_sort_key64(vox_ctx, n, bits):
     # 12,993,895 random 64-bit keys: the size of the reference's self-test
