@@ -24,14 +24,20 @@ typedef uint32_t uint;
 struct uint2
 {
     uint x, y;
+    uint2() : x(0u), y(0u) {}
+    uint2(uint a, uint b) : x(a), y(b) {}
 };
 struct uint3
 {
     uint x, y, z;
+    uint3() : x(0u), y(0u), z(0u) {}
+    uint3(uint a, uint b, uint c) : x(a), y(b), z(c) {}
 };
 struct uint4
 {
     uint x, y, z, w;
+    uint4() : x(0u), y(0u), z(0u), w(0u) {}
+    uint4(uint a, uint b, uint c, uint d) : x(a), y(b), z(c), w(d) {}
 };
 struct bool3
 {

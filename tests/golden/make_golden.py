@@ -15,9 +15,23 @@ Fixtures:
   voxelbvh_<case>.npz  voxelbvh_gaussians_to_ijkl keys and ids (sorted
                        stably by key) and the range headers of
                        voxelbvh_find_range_starts / scatter_range_headers
+  topology_<case>.npz  the node2 region (root first, every node at its node2
+                       maximum size in the order the reference allocates it)
+                       that the reference's grid-build shaders produce for the
+                       cloud - grid_build_set_masks / count_new / scatter_new /
+                       finalize per tree level and fragment window, then
+                       grid_build_blindmetadata and grid_build_compute_bbox -
+                       as its SHA-256 (and the bytes themselves for the small
+                       clouds), with node counts, value count, window count and
+                       bbox.  The two large clouds (12 fragment windows; two
+                       prim batches) are stored as their generator, seed and
+                       the SHA-256 of their float32 inputs instead of the inputs.
+
+    python tests/golden/make_golden.py [--topology]   (--topology: only topology_*)
 """
 
 import ctypes
+import hashlib
 import os
 import sys
 
@@ -131,7 +145,70 @@ def voxelbvh_fixture(L, cloud, res, T=None):
                 ijkl=k, prim_id=i, range=headers, ranges=np.int64(scan[-1] if N else 0), **extra)
 
 
+def load_ref_topology():
+    L = load_ref()
+    L.ref_node2_build.restype = ctypes.c_int64
+    L.ref_node2_build.argtypes = [ctypes.c_int64] + [P] * 4 + [ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32, P, P]
+    L.ref_node2_copy.restype = ctypes.c_int64
+    L.ref_node2_copy.argtypes = [P, ctypes.c_int64]
+    return L
+
+
+# the reference's batch sizes (raster/Raster.cpp:443-444)
+PRIM_BATCH = 256 * 1024
+IJK_BATCH = 8 * 1024 * 1024
+
+
+def inputs_sha256(cloud) -> str:
+    h = hashlib.sha256()
+    for k in ("means", "quats", "scales", "opacities"):
+        h.update(_f(cloud[k]).tobytes())
+    return h.hexdigest()
+
+
+def topology_fixture(L, cloud, vs, keep_bytes):
+    m, q, s, o = (_f(cloud[k]) for k in ("means", "quats", "scales", "opacities"))
+    cnt = np.zeros(5, np.int64)
+    bb = np.zeros(6, np.int32)
+    nb = L.ref_node2_build(cloud.n, m.ctypes.data, q.ctypes.data, s.ctypes.data, o.ctypes.data, vs, PRIM_BATCH,
+                           IJK_BATCH, cnt.ctypes.data, bb.ctypes.data)
+    if nb <= 0:
+        raise SystemExit("reference grid build failed")
+    region = np.empty(nb, np.uint8)
+    L.ref_node2_copy(region.ctypes.data, nb)
+    out = dict(voxel_size=np.float32(vs), node2_sha256=np.array(hashlib.sha256(region.tobytes()).hexdigest()),
+               node2_bytes=np.int64(nb), upper=np.int64(cnt[0]), lower=np.int64(cnt[1]), leaf=np.int64(cnt[2]),
+               value_count=np.int64(cnt[3]), windows=np.int64(cnt[4]), bbox=bb)
+    if keep_bytes:
+        out["node2"] = region
+    return out
+
+
+def topology_cases():
+    """(cloud, voxel size, regeneration spec or None, keep the region bytes)"""
+    cases = {name: (c, vs, None, name in ("tiny", "pytest32", "plain", "aniso")) for name, (c, vs) in raster_cases().items()}
+    cases["windows_100k"] = (W.plain_cloud(100_000, 0), 0.01, ("plain_cloud", 100_000, 0), False)
+    cases["batches_300k"] = (W.plain_cloud(300_000, 0), 0.04, ("plain_cloud", 300_000, 0), False)
+    return cases
+
+
+def write_topology(L):
+    for name, (cloud, vs, spec, keep) in topology_cases().items():
+        z = topology_fixture(L, cloud, vs, keep)
+        if spec is None:
+            z.update(means=_f(cloud["means"]), quats=_f(cloud["quats"]), scales=_f(cloud["scales"]),
+                     opacities=_f(cloud["opacities"]))
+        else:
+            z.update(generator=np.array(spec[0]), count=np.int64(spec[1]), seed=np.int64(spec[2]),
+                     inputs_sha256=np.array(inputs_sha256(cloud)))
+        np.savez_compressed(os.path.join(HERE, f"topology_{name}.npz"), **z)
+        print("topology", name, int(z["windows"]), "windows", str(z["node2_sha256"])[:16])
+
+
 def main():
+    if "--topology" in sys.argv:
+        write_topology(load_ref_topology())
+        return
     L = load_ref()
     for name, (cloud, vs) in raster_cases().items():
         np.savez_compressed(os.path.join(HERE, f"raster_{name}.npz"), **raster_fixture(L, cloud, vs))
@@ -149,6 +226,7 @@ def main():
     cloud, res = voxelbvh_cases()["clusters_res512"]
     np.savez_compressed(os.path.join(HERE, "voxelbvh_clusters_res512_transform.npz"),
                         **voxelbvh_fixture(L, cloud, res, T.astype(np.float32)))
+    write_topology(load_ref_topology())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -2,6 +2,11 @@
 (tests/golden/make_golden.py: the reference's shader files compiled as C++),
 so the pin holds where the reference checkout is absent.
 
+topology_*.npz: the node2 region, node counts, value count and bbox the
+reference's grid-build shaders produce (grid_build_*.slang, run window by
+window as raster_gaussian_3d runs them), including a 12-window and a
+two-prim-batch cloud.
+
 raster_*.npz: per-Gaussian bbox and fragment count (gaussian_prim.slang),
 the sorted passing (voxel, Gaussian) pairs of one fragment window
 (fanout_*.slang, gaussian_frag_alloc.slang) and the per-voxel RGBA8 maximum
@@ -34,7 +39,7 @@ def _files(prefix):
 
 
 def test_fixtures_present():
-    assert len(_files("raster_")) >= 5 and len(_files("voxelbvh_")) >= 4
+    assert len(_files("raster_")) >= 5 and len(_files("voxelbvh_")) >= 4 and len(_files("topology_")) >= 7
 
 
 @pytest.mark.parametrize("path", _files("raster_"), ids=os.path.basename)
@@ -76,3 +81,48 @@ def test_oracle_matches_golden_voxelbvh(oracle_mod, path):
     np.testing.assert_array_equal(out["prim_id"], z["prim_id"])
     np.testing.assert_array_equal(out["range"], z["range"])
     assert out["ranges"] == int(z["ranges"])
+
+
+def topology_cloud(z):
+    """The fixture's cloud: its float32 inputs, or its generator re-run and
+    checked against the SHA-256 of the inputs it was made from."""
+    import hashlib
+
+    if "means" in z:
+        return _cloud(z)
+    gen = getattr(W, str(z["generator"]))
+    c = gen(int(z["count"]), int(z["seed"]))
+    h = hashlib.sha256()
+    for k in ("means", "quats", "scales", "opacities"):
+        h.update(np.ascontiguousarray(c[k], np.float32).tobytes())
+    assert h.hexdigest() == str(z["inputs_sha256"]), "the generator no longer reproduces the fixture's inputs"
+    return c
+
+
+def check_topology(z, region, counts, bbox):
+    """A node2 region, node counts and bbox against a topology fixture."""
+    import hashlib
+
+    assert counts == {k: int(z[k]) for k in ("upper", "lower", "leaf", "value_count")}
+    np.testing.assert_array_equal(np.asarray(bbox, np.int32), z["bbox"])
+    assert region.size == int(z["node2_bytes"])
+    if "node2" in z:
+        np.testing.assert_array_equal(region, z["node2"])
+    assert hashlib.sha256(region.tobytes()).hexdigest() == str(z["node2_sha256"])
+
+
+@pytest.mark.parametrize("path", _files("topology_"), ids=os.path.basename)
+def test_oracle_matches_golden_topology(oracle_mod, path):
+    """The oracle's window-by-window node2 build (window_mode 1) against the
+    region the reference's grid-build shaders wrote for the same cloud:
+    raster_gaussian_3d's prim batches of 256K and fragment windows of 8M
+    (raster/Raster.cpp:420-510), per window and tree level
+    grid_build_set_masks / count_new / scatter_new / finalize
+    (raster/GridBuild.cpp:361-506), then grid_build_blindmetadata and
+    grid_build_compute_bbox (GridBuild.cpp:508-650)."""
+    z = np.load(path)
+    cloud = topology_cloud(z)
+    res = oracle_mod.OracleResult(cloud, float(z["voxel_size"]), 0.05, window_mode=1)
+    assert res.counts["windows"] == int(z["windows"])
+    check_topology(z, res.node2(), {k: res.counts[k] for k in ("upper", "lower", "leaf", "value_count")}, res.bbox())
+    res.close()
