@@ -216,6 +216,14 @@ typedef struct pnanovdb_raster_t
 PNANOVDB_API pnanovdb_raster_t* pnanovdb_get_raster(void);
 /* replaces the compute table the reference builds in compute/Compute.cpp */
 PNANOVDB_API pnanovdb_compute_t* pnanovdb_get_compute(void);
+/* the device interface inside that table (vulkan/PublicDeviceVulkan.cpp:114,
+ * declared at nanovdb_editor/putil/Compute.h:705): a CUDA device and its
+ * queues, whatever `api` asks for (0 = Vulkan is the only value the
+ * reference defines) */
+PNANOVDB_API pnanovdb_compute_device_interface_t* pnanovdb_get_compute_device_interface(uint32_t api);
+/* the shader interface inside that table (compute/ComputeShader.cpp:173,
+ * Compute.h:758): no Slang shaders here, every entry is NULL */
+PNANOVDB_API pnanovdb_compute_shader_interface_t* pnanovdb_get_compute_shader_interface(void);
 
 /* ------------------------------------------------------- file formats -- */
 /* Layout of pnanovdb_fileformat_t (nanovdb_editor/putil/FileFormat.h:19-36,

@@ -845,6 +845,16 @@ pnanovdb_compute_t* pnanovdb_get_compute(void)
     return &t;
 }
 
+pnanovdb_compute_device_interface_t* pnanovdb_get_compute_device_interface(uint32_t)
+{
+    return &pnanovdb_get_compute()->device_interface;
+}
+
+pnanovdb_compute_shader_interface_t* pnanovdb_get_compute_shader_interface(void)
+{
+    return &pnanovdb_get_compute()->shader_interface;
+}
+
 pnanovdb_fileformat_t* pnanovdb_get_fileformat(void)
 {
     static pnanovdb_fileformat_t t = { nullptr, ff_can_load_file, ff_load_file, nullptr };
