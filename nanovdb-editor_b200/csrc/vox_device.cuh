@@ -383,11 +383,22 @@ __device__ __forceinline__ float vox_powf_unit(float b, float e)
     return VOX_FMUL(VOX_FMUL(q, s1), s2);
 }
 
+// one RGBA8 channel byte of gaussian_frag_color.slang:239-246: clamp to [0, 1], 255 v truncated
+__device__ __forceinline__ uint32_t rgba8_byte(float v)
+{
+    v = v < 1.f ? v : 1.f;
+    v = 0.f > v ? 0.f : v;
+    return (uint32_t)VOX_FMUL(255.f, v);
+}
+
 // Lattice weights w_s = fl(fl(1/3) * s), 1 - w_s rounded (s = 1, 2); s = 0 and
 // s = 3 (w = 1 exactly) give p = lo and p = hi.
 constexpr float LAT_W1 = 0x1.555556p-2f, LAT_OW1 = 0x1.555554p-1f;
 constexpr float LAT_W2 = 0x1.555556p-1f, LAT_OW2 = 0x1.555554p-2f;
-__device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
+
+// The smallest |p|^2 of the 4x4x4 lattice (gaussian_frag_color.slang:190-197),
+// the sum of the per-axis smallest squares
+__device__ __forceinline__ float lattice_min_d2(const Aabb& b)
 {
     float m[3];
 #pragma unroll
@@ -399,13 +410,74 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
                     s3 = VOX_FMUL(b.hi[a], b.hi[a]);
         m[a] = fminf(fminf(s0, s1), fminf(s2, s3)); // squares: no NaN, no signed zero
     }
-    float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
+    return VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
+}
+
+// alpha from the lattice minimum d (gaussian_frag_color.slang:197-213)
+__device__ __forceinline__ float alpha_of_d2(const GaussRec& R, float d)
+{
     float a = VOX_FMUL(R.q6.x, vox_expf_cr(-VOX_FMUL(R.q6.y, d)));
     a = a > 0.f ? a : 0.f;
     a = VOX_FSUB(1.f, vox_powf_unit(VOX_FSUB(1.f, a), R.q6.z));
     if (R.q7.w != 0.f)
         a = 0.f;
     return a;
+}
+
+__device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
+{
+    return alpha_of_d2(R, lattice_min_d2(b));
+}
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(float x)
+{
+    float y;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// The RGBA8 alpha byte of a passing pair, rgba8_byte(pair_alpha(R, b)), with
+// the exp and pow of the exact evaluation replaced, where that is safe, by
+// bounds from the hardware ex2 / lg2 approximations.  The lattice minimum d
+// and x = ls * d are the exact evaluation's.  Then
+//   a  = fl(op exp(-x))           lies in [a_lo, a_hi] = op e^-x (1 -+ 2^-16)
+//                                  (the approximation's error and the exact
+//                                  path's rounding are both below 2^-19),
+//   P  = (1 - a)^e, increasing in 1 - a, lies in [P(1 - a_hi), P(1 - a_lo)]
+//        widened by (|ln P| + e + 8) 2^-17 relative (both evaluations of the
+//        power err by well under that: the log's error is scaled by e),
+//   a' = fl(1 - P) and the byte trunc(255 clamp(a')) are monotone in P,
+// so the byte is known when both ends of the interval give the same byte;
+// otherwise (rarely: near a byte boundary) the exact evaluation decides.  A
+// Gaussian culled by scale gives 0; x > 20 gives a' < e op e^-20 < 1/255.
+__device__ __forceinline__ uint32_t pair_alpha_byte(const GaussRec& R, const Aabb& b)
+{
+    if (R.q7.w != 0.f)
+        return 0u;
+    const float d = lattice_min_d2(b);
+    const float x = VOX_FMUL(R.q6.y, d);
+    if (!(x <= 20.f))
+        return x > 20.f ? 0u : rgba8_byte(alpha_of_d2(R, d));
+    const float a = R.q6.x * ex2_approx(x * -1.44269504f);
+    const float a_hi = a * (1.f + 0x1p-16f), a_lo = a * (1.f - 0x1p-16f);
+    const float b_lo = 1.f - a_hi, b_hi = 1.f - a_lo;
+    if (b_lo > 0.f)
+    {
+        const float e = R.q6.z;
+        const float y_lo = e * lg2_approx(b_lo), y_hi = e * lg2_approx(b_hi); // log2 P at both ends, <= 0
+        const float mu = (fabsf(y_lo) * 0.6931472f + e + 8.f) * 0x1p-17f;
+        const float p_hi = ex2_approx(y_hi) * (1.f + mu), p_lo = ex2_approx(y_lo) * (1.f - mu);
+        const uint32_t byte_lo = rgba8_byte(1.f - p_hi), byte_hi = rgba8_byte(1.f - p_lo);
+        if (byte_lo == byte_hi)
+            return byte_lo;
+    }
+    return rgba8_byte(alpha_of_d2(R, d));
 }
 
 // Stable local AABB of voxel (i, j, k) for the float channels: corner offsets
@@ -523,13 +595,6 @@ __device__ __forceinline__ float fx_to_float(unsigned long long s)
     return VOX_FMUL(__ll2float_rn((long long)s), FX_INV);
 }
 
-// one RGBA8 channel byte of gaussian_frag_color.slang:239-246: clamp to [0, 1], 255 v truncated
-__device__ __forceinline__ uint32_t rgba8_byte(float v)
-{
-    v = v < 1.f ? v : 1.f;
-    v = 0.f > v ? 0.f : v;
-    return (uint32_t)VOX_FMUL(255.f, v);
-}
 
 __device__ __forceinline__ uint32_t pack_rgba8(const GaussRec& R, float a)
 {

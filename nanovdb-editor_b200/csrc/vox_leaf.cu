@@ -698,7 +698,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                 const RInv M = rinv_of(R);
                 const float vsf = C.vs[j];
                 const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7), zz = ao[2] + (int32_t)(n & 7);
-                const float a8 = pair_alpha(R, voxel_local_aabb(R, M, vsf, x, yy, zz));
+                const uint32_t a8 = pair_alpha_byte(R, voxel_local_aabb(R, M, vsf, x, yy, zz));
                 float a;
                 if (P.smooth)
                 {
@@ -710,7 +710,7 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                     a = pair_alpha_f(R, stable_local_aabb(R, M, vsf, x, yy, zz));
                 }
                 atomicAdd(&A.cnt[n], 1u);
-                atomicMax(&A.rgba[n], (rgba8_byte(a8) << 24) | C.rgb24[j]);
+                atomicMax(&A.rgba[n], (a8 << 24) | C.rgb24[j]);
                 atomicAdd(&A.dens[n], fx_of_unit(a));
                 atomicAdd(&A.col[0][n], fx_of(VOX_FMUL(a, R.q7.x)));
                 atomicAdd(&A.col[1][n], fx_of(VOX_FMUL(a, R.q7.y)));

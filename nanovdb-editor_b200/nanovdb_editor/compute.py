@@ -21,6 +21,7 @@ from ctypes import (
     c_uint32,
     c_uint64,
     c_void_p,
+    cast,
     pointer,
 )
 
@@ -105,7 +106,10 @@ class Compute:
         self._compute.contents.module = self._lib._handle
         di = self._compute.contents.device_interface
         self._manager = di.create_device_manager(0)
-        self._device = di.create_device(self._manager, None)
+        # pnanovdb_compute_device_desc_t (putil/Compute.h:503-508): device_index first
+        desc = (c_uint32 * 4)(int(device_index), 0, 0, 0)
+        # NULL without a CUDA device: the host-side array functions still work
+        self._device = di.create_device(self._manager, cast(desc, c_void_p).value)
         self._queue = di.get_compute_queue(self._device)
 
     def get_compute(self):

@@ -135,3 +135,115 @@ def test_raster_file_missing_array(raster, tmp_path):
     np.savez(path, means=raw[0], opacities=raw[1])
     with pytest.raises(RuntimeError):
         r.raster_file(str(path), 0.01)
+
+
+class _Buffer(__import__("ctypes").Structure):
+    """pnanovdb_compute_buffer_t: a device pointer and its size"""
+
+    _fields_ = [("device_ptr", __import__("ctypes").c_void_p), ("size_bytes", __import__("ctypes").c_uint64)]
+
+
+def _raster_3d(compute, r, ctx, data, vs, words):
+    """raster_gaussian_3d into a device buffer of `words` 32-bit words; the buffer's bytes on the host"""
+    import ctypes
+
+    import torch
+
+    dev = torch.zeros(words, dtype=torch.int32, device="cuda")
+    buf = _Buffer(dev.data_ptr(), 4 * words)
+    torch.cuda.synchronize()
+    t = r._raster.contents
+    t.raster_gaussian_3d(compute.get_compute(), compute.queue(), ctx, vs, data, ctypes.byref(buf), words, None)
+    torch.cuda.synchronize()
+    return dev.cpu().numpy().view(np.uint8)
+
+
+def test_gaussian_data_and_raster_gaussian_3d(raster, oracle_mod):
+    """create_context / create_gaussian_data / upload_gaussian_data /
+    raster_gaussian_3d / destroy_gaussian_data / destroy_context through the
+    table (raster/RasterContext.cpp:92-229, raster/Raster.cpp:420-558): the
+    device buffer receives the reference's output (node2 in the reference's
+    node order and RGBA8 values), equal to the oracle; a buffer too small for
+    it is left untouched."""
+    compute, r = raster
+    t = r._raster.contents
+    cloud = W.cluster_cloud(20_000, 48, clusters=3)
+    vs = 0.004
+    arrs = {k: compute.create_array(np.ascontiguousarray(cloud[k])) for k in ("means", "quats", "scales", "colors", "opacities")}
+    empty = compute.create_array(np.zeros(0, np.float32))
+    ctx = t.create_context(compute.get_compute(), compute.queue())
+    assert ctx
+    data = t.create_gaussian_data(compute.get_compute(), compute.queue(), ctx, arrs["means"], arrs["quats"], arrs["scales"],
+                                  arrs["colors"], empty, empty, arrs["opacities"], None, None)
+    assert data
+    t.upload_gaussian_data(compute.get_compute(), compute.queue(), ctx, data)
+    out = _raster_3d(compute, r, ctx, data, vs, 16 << 20)
+    g = NodeGrid(out)
+    _against_oracle(g, cloud, vs, oracle_mod)
+    need = int(g.header["grid_bytes"])
+    small = _raster_3d(compute, r, ctx, data, vs, (need - 4) // 4)
+    assert not small.any()  # too small: logged, nothing written
+    t.destroy_gaussian_data(compute.get_compute(), compute.queue(), data)
+    t.destroy_context(compute.get_compute(), compute.queue(), ctx)
+    for a in list(arrs.values()) + [empty]:
+        compute.destroy_array(a)
+
+
+def test_gaussian_data_from_arrays(raster, oracle_mod):
+    """create_gaussian_data_from_arrays (raw arrays, raster/RasterUtils.cpp:208-245)
+    with a new context, then raster_gaussian_3d: the reference's preprocessing
+    runs in the prep kernel and the result equals the oracle's."""
+    import ctypes
+
+    from nanovdb_editor.compute import pnanovdb_ComputeArray
+
+    compute, r = raster
+    t = r._raster.contents
+    raw = W.plain_cloud(15_000, 49).raw_arrays()
+    arrays = [compute.create_array(a) for a in raw]
+    Arr = ctypes.POINTER(pnanovdb_ComputeArray)
+    arr_c = (Arr * 6)(*[ctypes.pointer(a) for a in arrays])
+    data, ctx = ctypes.c_void_p(), ctypes.c_void_p()
+    ok = t.create_gaussian_data_from_arrays(ctypes.addressof(t), compute.get_compute(), compute.queue(), arr_c, 6,
+                                            ctypes.byref(data), None, ctypes.byref(ctx))
+    assert ok == 1 and data.value and ctx.value
+    g = NodeGrid(_raster_3d(compute, r, ctx.value, data.value, 0.01, 16 << 20))
+    _against_oracle(g, oracle_mod.preprocess(raw), 0.01, oracle_mod)
+    t.destroy_gaussian_data(compute.get_compute(), compute.queue(), data.value)
+    t.destroy_context(compute.get_compute(), compute.queue(), ctx.value)
+    for a in arrays:
+        compute.destroy_array(a)
+
+
+def test_queues_run_concurrently(vox_ctx):
+    """Worker threads with their own queues (editor/PipelineRuntime.cpp:416-427)
+    each get their own context: two threads voxelizing different clouds at once
+    return the same grids as one after the other."""
+    import threading
+
+    from nanovdb_editor import Compute, Raster
+
+    computes = [Compute(device_index=0) for _ in range(2)]
+    rasters = [Raster(c) for c in computes]
+    raws = [W.plain_cloud(40_000, 50 + i).raw_arrays() for i in range(2)]
+
+    def run(i, out):
+        c = computes[i]
+        arrays = [c.create_array(a) for a in raws[i]]
+        for _ in range(3):
+            g = _grid(c, rasters[i].raster_to_nanovdb_from_arrays(0.01, arrays))
+        out[i] = g.buf.copy()
+        for a in arrays:
+            c.destroy_array(a)
+
+    serial = [None, None]
+    for i in range(2):
+        run(i, serial)
+    both = [None, None]
+    th = [threading.Thread(target=run, args=(i, both)) for i in range(2)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    for i in range(2):
+        assert np.array_equal(both[i], serial[i])
