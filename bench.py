@@ -113,6 +113,12 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def run_config(G, world):
+    """The workload config both arms report (the CPU arm times a stated sample of it)."""
+    return dict(WORKLOAD, gaussians=G, parallelism=f"replicas{world}" if world > 1 else "single",
+                l2="256 MB flush between steps; pair working set >> L2", inputs="raw (log-scale, logit, SH0)")
+
+
 def cpu_baseline(steps=1, target_s=15.0):
     """Oracle (float outputs only) on a bounded sample of the workload, all host cores."""
     import oracle as oracle_py
@@ -124,19 +130,75 @@ def cpu_baseline(steps=1, target_s=15.0):
     n = 20_000
     rate = None
     sample = None
+    counts = {}
+    dt = 0.0
     for _ in range(4):
-        cloud = W.cluster_cloud(n, 1, clusters=max(1, int(64 * n / 2_000_000)) or 1)
+        # clusters of the 2M workload's size (31,250 Gaussians), so the sample has its density
+        clusters = max(1, round(n / 31_250))
+        cloud = W.cluster_cloud(n, 1, clusters=clusters)
         t0 = time.perf_counter()
         r = oracle_py.OracleResult(cloud, vs, 0.05, window_mode=1 | 2, nthreads=cores)
         dt = time.perf_counter() - t0
         ok = r.counts["error"] == 0
+        counts = dict(r.counts)
         r.close()
         rate = n / dt if ok else None
-        sample = f"{n} Gaussians of the 2M-cluster distribution (density-preserving subset: {max(1, int(64 * n / 2_000_000))} clusters), voxel 0.002, {dt:.1f}s"
+        sample = (f"a sample of the workload: {n} Gaussians in {clusters} cluster(s) of the 2M workload's "
+                  f"distribution and per-cluster density, voxel 0.002, {dt:.1f}s")
         if dt > target_s / 4 or n >= 400_000:
             break
         n = int(min(400_000, n * max(2.0, target_s / max(dt, 1e-3) / 2)))
-    return {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    return {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+            "pairs_per_s": counts.get("P", 0) / dt if dt else None, "voxels_per_s": counts.get("V", 0) / dt if dt else None}
+
+
+CFG0 = {"workload": "cfg0_plain_100k_vs0.01", "gaussians": 100_000, "voxel_size": 0.01}
+
+
+def cpu_cfg0():
+    """The reference's CPU-runnable configuration (100K Gaussians, uniform in
+    [-1, 1]^3, voxel 0.01) voxelized in full by the CPU restatement in the
+    reference's fragment windows, on all host cores."""
+    import oracle as oracle_py
+    from nanovdb_editor import workloads as W
+
+    oracle_py.build()
+    cores = os.cpu_count() or 1
+    cloud = W.plain_cloud(CFG0["gaussians"], 0)
+    t0 = time.perf_counter()
+    r = oracle_py.OracleResult(cloud, CFG0["voxel_size"], 0.05, window_mode=1 | 2, nthreads=cores)
+    dt = time.perf_counter() - t0
+    c = dict(r.counts)
+    r.close()
+    return dict(CFG0, cores=cores, seconds=dt, gaussians_per_s=CFG0["gaussians"] / dt, pairs_per_s=c["P"] / dt,
+                voxels_per_s=c["V"] / dt, windows=c["windows"])
+
+
+def gpu_cfg0(ctx, torch, steps, warmup, flush):
+    """The same configuration on the GPU through raster_to_nanovdb-style device
+    inputs (activated arrays, the reference's node order), CUDA events."""
+    from nanovdb_editor import workloads as W
+    from nanovdb_editor.vox import FLAG_WINDOW_ORDER
+
+    cloud = W.plain_cloud(CFG0["gaussians"], 0)
+    dev = [torch.from_numpy(np.ascontiguousarray(cloud[k])).cuda() for k in ("means", "quats", "scales", "opacities", "colors")]
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(warmup):
+        ctx.voxelize(*dev, CFG0["voxel_size"], 0.05, FLAG_WINDOW_ORDER)
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0.record(ext)
+        ctx.voxelize(*dev, CFG0["voxel_size"], 0.05, FLAG_WINDOW_ORDER)
+        e1.record(ext)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    st = ctx.stats()
+    ms = float(np.mean(ts))
+    return dict(CFG0, ms_per_step=ms, gaussians_per_s=CFG0["gaussians"] / (ms * 1e-3), pairs_per_s=st["pairs"] / (ms * 1e-3),
+                voxels_per_s=st["voxels"] / (ms * 1e-3), node_order="reference (window order)")
 
 
 FWD_BWD = {"workload": "fwd_bwd_500k_clusters64_vs0.004", "gaussians": 500_000, "clusters": 64, "voxel_size": 0.004}
@@ -493,6 +555,7 @@ def run_reference(args, rank, world):
         res.append(cpu_baseline())
     vals = [r["value"] for r in res if r["value"]]
     v = statistics.median(vals) if vals else None
+    cfg0 = cpu_cfg0()
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -506,8 +569,13 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": dict(WORKLOAD, note="CPU restatement of the reference path (the reference's Vulkan path cannot run here)"),
-        "cpu_baseline": {"kind": "port", "cores": res[-1]["cores"], "sample": res[-1]["sample"], "value": v, "unit": UNIT},
+        "config": run_config(args.gaussians, world),
+        "cpu_baseline": {"kind": "port", "cores": res[-1]["cores"], "sample": res[-1]["sample"], "value": v, "unit": UNIT,
+                         "implementation": "CPU restatement of the reference path (oracle/vox_oracle.c); the reference's "
+                                           "own path runs only on Vulkan, which this box cannot bring up",
+                         "pairs_per_s": statistics.median([r["pairs_per_s"] for r in res if r["pairs_per_s"]] or [0]),
+                         "voxels_per_s": statistics.median([r["voxels_per_s"] for r in res if r["voxels_per_s"]] or [0])},
+        "cfg0_full": cfg0,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -596,6 +664,26 @@ def main():
     ms = R.max_over_ranks(sum(times) / len(times), dist, device="cuda")
     value = R.job_rate(world * G, ms)
 
+    # the same step in the reference's node order (its window-by-window build), device-timed
+    from nanovdb_editor.vox import FLAG_WINDOW_ORDER
+
+    def step_window():
+        ctx.voxelize(dev[0], dev[2], dev[3], dev[1], dev[4], vs, 0.05, FLAG_RAW_INPUTS | FLAG_WINDOW_ORDER)
+
+    step_window()
+    wtimes = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        start.record(ext_stream)
+        step_window()
+        end.record(ext_stream)
+        end.synchronize()
+        wtimes.append(start.elapsed_time(end))
+    w_ms = R.max_over_ranks(sum(wtimes) / len(wtimes), dist, device="cuda")
+    window_order = {"ms_per_step": w_ms, "value": R.job_rate(world * G, w_ms), "unit": UNIT,
+                    "note": "the same step with VOX_FLAG_WINDOW_ORDER: node2 bytes in the reference's node order"}
+
     # ---- e2e through the reference-facing C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -679,9 +767,15 @@ def main():
         except Exception as e:  # a secondary row: never lose the main line to it
             forms["voxelbvh"] = {"error": f"{type(e).__name__}: {e}"}
 
+    cfg0 = None
+    if not args.no_forms:
+        cfg0 = {"gpu": gpu_cfg0(ctx, torch, args.steps, args.warmup, flush)}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu = cpu_baseline()
+        if cfg0 is not None:
+            cfg0["cpu"] = cpu_cfg0()
+            cfg0["gpu_over_cpu"] = cfg0["gpu"]["gaussians_per_s"] / cfg0["cpu"]["gaussians_per_s"]
 
     if rank == 0:
         clk = clocks.summary()
@@ -698,7 +792,9 @@ def main():
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": dict(WORKLOAD, gaussians=G, parallelism=f"replicas{world}" if world > 1 else "single", l2="256 MB flush between steps; pair working set >> L2", inputs="raw (log-scale, logit, SH0)"),
+            "config": run_config(G, world),
+            "window_order": window_order,
+            "cfg0_full": cfg0,
             "e2e": e2e,
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "roofline": {

@@ -54,7 +54,7 @@ def test_scan_full_64_bit_prefixes(vox_ctx, n, top):
         vox_ctx.global_scan_u64(d_in, d_out, d_tot, inclusive)
         np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint64), _scan_ref(x, inclusive))
         assert int(d_tot.cpu().numpy().view(np.uint64)[0]) == int(x.sum(dtype=np.uint64))
-    if top == 1 << 40:
+    if top == 1 << 40 and n > 100_000:
         assert int(np.cumsum(x, dtype=np.uint64)[-1]) > (1 << 55)
 
 
