@@ -330,6 +330,210 @@ def measure_batched(ctx, torch, rank, steps, warmup, flush):
     }
 
 
+def measure_batched_fwd_bwd(ctx, torch, rank, steps, warmup, flush):
+    """The 256-cloud batch (as measure_batched) differentiable: one batched
+    forward (VOX_FLAG_DIFFERENTIABLE) plus one batched adjoint with upstream
+    dL/dvoxel ~ N(0, 1), against the batched forward alone."""
+    from nanovdb_editor import workloads as W
+    from nanovdb_editor.vox import FLAG_DIFFERENTIABLE, FLAG_RAW_INPUTS
+
+    clouds, start, vs = W.batch_clouds(BATCHED["clouds"], 3 + rank, BATCHED["min_n"], BATCHED["max_n"])
+    raw = W.concat(clouds).raw_arrays()
+    dev = [torch.from_numpy(a).cuda() for a in raw[:5]]
+    ins = (dev[0], dev[2], dev[3], dev[1], dev[4])
+    out = {k: torch.empty_like(t) for k, t in zip(("means", "quats", "scales", "opacities", "colors"), ins)}
+    flags = FLAG_RAW_INPUTS | FLAG_DIFFERENTIABLE
+    _, _, voff = ctx.voxelize_batch(*ins, start, vs, 0.05, flags)
+    vc = int(voff[-1])
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    gd = torch.randn(vc, device="cuda", generator=gen)
+    gc = torch.randn((vc, 3), device="cuda", generator=gen)
+    torch.cuda.synchronize()
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        res = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0.record(ext)
+            fn()
+            e1.record(ext)
+            e1.synchronize()
+            res.append(e0.elapsed_time(e1))
+        return float(np.mean(res))
+
+    fwd_ms = timed(lambda: ctx.voxelize_batch(*ins, start, vs, 0.05, FLAG_RAW_INPUTS))
+
+    def fwd_bwd():
+        ctx.voxelize_batch(*ins, start, vs, 0.05, flags)
+        ctx.backward(*ins, gd, gc, out)
+
+    fb_ms = timed(fwd_bwd)
+    G = int(start[-1])
+    return {"workload": "batched_fwd_bwd_256_clouds_1k-200k_vs0.002-0.02", "clouds": len(clouds), "gaussians": G,
+            "batched_forward_ms": fwd_ms, "batched_fwd_bwd_ms": fb_ms, "fwd_bwd_over_forward": fb_ms / fwd_ms,
+            "fwd_bwd_gaussians_per_s": G / (fb_ms * 1e-3),
+            "parity": "batched adjoint = per-cloud adjoints (tests/test_gpu_batch.py); 1e-5 of each family's max vs FP64 "
+                      "(tests/test_gpu_adjoint.py)"}
+
+
+FIT = {"workload": "fit_500k_clusters64_vs0.004_200steps", "gaussians": 500_000, "clusters": 64, "voxel_size": 0.004,
+       "steps": 200}
+
+
+def measure_fit(ctx, torch, rank):
+    """L2 fit (200 Adam steps, FP32) of 500K Gaussians (cluster distribution,
+    voxel 0.004) to the grid of an independently seeded 500K set: forward,
+    loss over the union of both grids' voxels, adjoint and update per step,
+    CUDA events around each step."""
+    from nanovdb_editor import workloads as W
+    from nanovdb_editor.autograd import TargetGrid, l2_to_target, voxelize
+
+    G, vs = FIT["gaussians"], FIT["voxel_size"]
+    names = ("means", "quats", "scales", "opacities", "colors")
+
+    def dev_params(seed):
+        r = W.cluster_cloud(G, seed, clusters=FIT["clusters"]).raw_arrays()
+        return {k: torch.from_numpy(a).cuda() for k, a in zip(names, (r[0], r[2], r[3], r[1], r[4]))}
+
+    tgt = dev_params(201 + rank)
+    tdens, _, _ = voxelize(*[tgt[k] for k in names], vs, raw=True, context=ctx)
+    target = TargetGrid.from_last(ctx, tdens)
+    leaves = {k: t.clone().requires_grad_(True) for k, t in dev_params(202 + rank).items()}
+    lr = {"means": 2e-4, "quats": 1e-3, "scales": 2e-3, "opacities": 1e-2, "colors": 1e-2}
+    opt = torch.optim.Adam([{"params": [leaves[k]], "lr": lr[k]} for k in names])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times, losses = [], []
+    for _ in range(FIT["steps"]):
+        torch.cuda.synchronize()
+        e0.record()
+        opt.zero_grad()
+        density, _, _ = voxelize(*[leaves[k] for k in names], vs, raw=True, context=ctx)
+        loss = l2_to_target(density, ctx, target)
+        loss.backward()
+        opt.step()
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        losses.append(float(loss.detach()))
+    ms = float(np.median(times))
+    return {"workload": FIT["workload"], "gaussians": G, "steps": FIT["steps"], "ms_per_step": ms,
+            "total_s": float(np.sum(times)) * 1e-3, "gaussians_per_s": G / (ms * 1e-3),
+            "loss_first": losses[0], "loss_last": losses[-1], "loss_ratio": losses[-1] / losses[0],
+            "note": "step = differentiable forward + L2 loss + adjoint + torch Adam (FP32); gradients checked against "
+                    "FP64 finite differences and the FP64 adjoint in tests/test_oracle_adjoint.py, tests/test_gpu_adjoint.py"}
+
+
+FIT_BF16 = {"workload": "fit_bf16_64_clouds_50k-1M_vs0.002-0.01_100steps", "clouds": 64, "min_n": 50_000,
+            "max_n": 1_000_000, "vs_min": 0.002, "vs_max": 0.01, "steps": 100}
+
+
+class _DeviceBytes:
+    """A device pointer as a uint8 CUDA array (no copy)."""
+
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (int(nbytes),), "typestr": "|u1", "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def measure_fit_bf16(ctx, torch, rank, steps=None):
+    """Batched fitting loop: 64 clouds (log-uniform 50K-1M Gaussians, 1-16
+    clusters of the 2M workload's distribution, voxel sizes log-uniform in
+    [0.002, 0.01]) fitted to per-cloud target grids (independently seeded
+    clouds of the same sizes and voxel sizes).  Attributes stored in bfloat16
+    (VOX_FLAG_BF16_INPUTS), FP32 master copies and moments; per step one
+    batched differentiable forward, the L2 loss per cloud, one batched
+    adjoint (FP32 gradients) and the fused vox_adam_bf16 update.  At the end
+    the smallest cloud's density and gradients are compared with the FP64
+    oracle on the same (bfloat16) values."""
+    import oracle as oracle_py
+    from nanovdb_editor import workloads as W
+    from nanovdb_editor.autograd import BatchTargetGrid, batch_voxel_keys, l2_to_batch_target
+    from nanovdb_editor.grid import HEADER_DTYPE
+    from nanovdb_editor.vox import FLAG_BF16_INPUTS, FLAG_DIFFERENTIABLE, FLAG_RAW_INPUTS
+
+    F = FIT_BF16
+    steps = steps or F["steps"]
+    names = ("means", "quats", "scales", "opacities", "colors")
+    clouds, start, vs = W.batch_clouds(F["clouds"], 301 + rank, F["min_n"], F["max_n"], vs_min=F["vs_min"], vs_max=F["vs_max"])
+    targets = [W.cluster_cloud(c.n, 5000 + 97 * b + rank, clusters=1 + b % 16) for b, c in enumerate(clouds)]
+    G = int(start[-1])
+    flags = FLAG_RAW_INPUTS | FLAG_DIFFERENTIABLE | FLAG_BF16_INPUTS
+
+    def as_params(cl):
+        r = W.concat(cl).raw_arrays()
+        return {k: torch.from_numpy(a).cuda() for k, a in zip(names, (r[0], r[2], r[3], r[1], r[4]))}
+
+    def density_of(ptr, goff):
+        """the batch's density channel, value index order (clouds back to back)"""
+        buf = torch.as_tensor(_DeviceBytes(ptr, int(goff[-1])), device="cuda")
+        heads = np.frombuffer(torch.stack([buf[int(o): int(o) + 256] for o in goff[:-1]]).cpu().numpy().tobytes(),
+                              HEADER_DTYPE)
+        parts = [buf[int(o) + int(h["density_offset"]): int(o) + int(h["density_offset"]) + 4 * int(h["value_count"])]
+                 for o, h in zip(goff[:-1], heads)]
+        return torch.cat(parts).view(torch.float32)
+
+    tp = {k: v.to(torch.bfloat16).contiguous() for k, v in as_params(targets).items()}
+    torch.cuda.synchronize()
+    ptr, goff, voff = ctx.voxelize_batch(*[tp[k] for k in names], start, vs, 0.05, flags)
+    tkeys, tvalid = batch_voxel_keys(ctx, voff, "cuda")
+    target = BatchTargetGrid(tkeys, tvalid, density_of(ptr, goff).clone())
+    del tp
+    master = as_params(clouds)
+    bf = {k: v.to(torch.bfloat16).contiguous() for k, v in master.items()}
+    mom = {k: (torch.zeros_like(v), torch.zeros_like(v)) for k, v in master.items()}
+    grads = {k: torch.empty_like(v) for k, v in master.items()}
+    lr = {"means": 2e-4, "quats": 1e-3, "scales": 2e-3, "opacities": 1e-2, "colors": 1e-2}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    times, losses = [], []
+    pairs = voxels = 0
+    for t in range(1, steps + 1):
+        torch.cuda.synchronize()
+        e0.record(ext)
+        ptr, goff, voff = ctx.voxelize_batch(*[bf[k] for k in names], start, vs, 0.05, flags)
+        st = ctx.stats()
+        pairs, voxels = int(st["pairs"]), int(st["voxels"])
+        density = density_of(ptr, goff)
+        keys, valid = batch_voxel_keys(ctx, voff, "cuda")
+        loss, gd = l2_to_batch_target(density, keys, valid, target)
+        torch.cuda.synchronize()
+        ctx.backward(*[bf[k] for k in names], gd.contiguous(), None, grads)
+        for k in names:
+            ctx.adam_bf16(master[k], mom[k][0], mom[k][1], grads[k], bf[k], t, lr[k])
+        e1.record(ext)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        losses.append(loss)
+    # FP64 check on the smallest cloud: the last step's density and gradients
+    b = int(np.argmin([c.n for c in clouds]))
+    g0, g1 = int(start[b]), int(start[b + 1])
+    v0, v1 = int(voff[b]), int(voff[b + 1])
+    cur = {k: bf[k][g0:g1].to(torch.float32).cpu().numpy() for k in names}
+    act = oracle_py.preprocess([cur["means"], cur["opacities"], cur["quats"], cur["scales"], cur["colors"]])
+    ref = oracle_py.OracleResult(act, float(vs[b]), 0.05, window_mode=oracle_py.OV_MODE_SMOOTH)
+    vals = ref.values()
+    d64 = vals["density64"]
+    dens_err = float(np.abs(density[v0:v1].cpu().numpy().astype(np.float64) - d64).max()) / float(np.abs(d64).max())
+    an = ref.smooth_grad64(cur, True, gd[v0:v1].cpu().numpy().astype(np.float64), None)
+    grad_err = {}
+    for k in names:
+        got = grads[k][g0:g1].cpu().numpy().astype(np.float64).reshape(an[k].shape)
+        grad_err[k] = float(np.abs(got - an[k]).max()) / max(float(np.abs(an[k]).max()), 1e-30)
+    ref.close()
+    ms = float(np.median(times))
+    return {"workload": F["workload"], "clouds": len(clouds), "gaussians": G, "steps": steps, "pairs": pairs,
+            "voxels": voxels, "ms_per_step": ms, "total_s": float(np.sum(times)) * 1e-3,
+            "gaussians_per_s": G / (ms * 1e-3), "loss_first": losses[0], "loss_last": losses[-1],
+            "storage": "bfloat16 attributes, FP32 masters / moments / gradients / accumulation",
+            "fp64_check": {"cloud": b, "gaussians": g1 - g0, "density_rel_err": dens_err, "grad_rel_err": grad_err,
+                           "tolerance": 1e-5}}
+
+
 VOXELBVH = {"workload": "voxelbvh_ijkl_2M_clusters64_res512", "gaussians": 2_000_000, "clusters": 64, "resolution": 512}
 VOXELBVH_METRIC = "Gaussians/s ingested into VoxelBVH keys (ijkl_from_gaussians)"
 
@@ -762,6 +966,13 @@ def main():
     if not args.no_forms:
         forms["fwd_bwd"] = measure_fwd_bwd(ctx, torch, rank, args.steps, args.warmup, flush)
         forms["batched"] = measure_batched(ctx, torch, rank, args.steps, args.warmup, flush)
+        for name, fn in (("batched_fwd_bwd", lambda: measure_batched_fwd_bwd(ctx, torch, rank, args.steps, args.warmup, flush)),
+                         ("fit", lambda: measure_fit(ctx, torch, rank)),
+                         ("fit_bf16", lambda: measure_fit_bf16(ctx, torch, rank))):
+            try:
+                forms[name] = fn()
+            except Exception as e:  # a secondary row: never lose the main line to it
+                forms[name] = {"error": f"{type(e).__name__}: {e}"}
         try:
             forms["voxelbvh"] = measure_voxelbvh_form(ctx, torch, rank, args.steps, args.warmup, flush)
         except Exception as e:  # a secondary row: never lose the main line to it

@@ -300,6 +300,10 @@ typedef struct vox_context_t vox_context_t;
  * colour = sum K rgb (premultiplied); RGBA8 stays the reference's
  * (gaussian_frag_color.slang:182-246).  Keeps what vox_backward needs. */
 #define VOX_FLAG_DIFFERENTIABLE 4u
+/* every attribute array holds bfloat16 values (2 bytes each, same layouts);
+ * they are read exactly as float and all arithmetic stays FP32 / FP64 (the
+ * batched fitting loop's storage format; no counterpart in the reference) */
+#define VOX_FLAG_BF16_INPUTS 8u
 
 /* status codes */
 #define VOX_OK 0
@@ -536,6 +540,18 @@ PNANOVDB_API int vox_voxelbvh_ijkl_from_gaussians_file(vox_context_t* ctx, const
  * (nanovdb_editor/putil/Camera.h:316), so the two may differ in the last
  * bits.  VOX_ERR_ARGS for a singular or non-finite matrix. */
 PNANOVDB_API int vox_voxelbvh_transform_inverse(const float* m, float* inv);
+
+/* One Adam step (Kingma & Ba) on n parameters stored in bfloat16 for the
+ * voxelizer with FP32 master copies: with t the 1-based step,
+ *   m = b1 m + (1 - b1) g,  v = b2 v + (1 - b2) g^2,
+ *   master -= lr (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps),
+ *   out_bf16 = master rounded to nearest even,
+ * all in one pass over device arrays, ordered on `stream` (cudaStream_t, may
+ * be 0), asynchronous.  No counterpart in the reference (it has no training
+ * loop); it closes the forward / adjoint / update step of the BF16 fitting
+ * loop without a round trip through another library. */
+PNANOVDB_API int vox_adam_bf16(float* master, float* m, float* v, const float* grad, uint16_t* out_bf16, int64_t n,
+                               float lr, float beta1, float beta2, float eps, int64_t step, void* stream);
 
 /* Scan that allocates nothing.  No counterpart in the reference.
  *

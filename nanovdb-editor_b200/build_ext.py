@@ -19,7 +19,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB_DIR = os.path.join(HERE, "nanovdb_editor", "lib")
 LIB = os.path.join(LIB_DIR, "libpnanovdbcompute.so")
 
-SOURCES = ["vox_scan_sort.cu", "vox_raster.cu", "vox_leaf.cu", "vox_order.cu", "vox_backward.cu", "vox_api.cu", "vox_dropin.cu", "vox_noalloc.cu", "vox_voxelbvh.cu"]
+SOURCES = ["vox_scan_sort.cu", "vox_raster.cu", "vox_leaf.cu", "vox_order.cu", "vox_backward.cu", "vox_api.cu", "vox_dropin.cu", "vox_noalloc.cu", "vox_voxelbvh.cu", "vox_optim.cu"]
 NVCC_FLAGS = [
     "-gencode",
     "arch=compute_100a,code=sm_100a",

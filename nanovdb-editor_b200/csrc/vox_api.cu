@@ -403,6 +403,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     P.colors = gs->colors;
     P.count = G;
     P.raw = (flags & VOX_FLAG_RAW_INPUTS) ? 1 : 0;
+    P.bf16 = (flags & VOX_FLAG_BF16_INPUTS) ? 1 : 0;
     P.voxel_size = voxel_size;
     P.cull_scale = cull;
     P.cloud_start = d_cloud_start;
@@ -909,6 +910,7 @@ static int run_backward(vox_context_t* ctx, const vox_gaussians_t* gs, const flo
     F.opacities = gs->opacities;
     F.colors = gs->colors;
     F.raw = (ctx->last_flags & VOX_FLAG_RAW_INPUTS) ? 1 : 0;
+    F.bf16 = (ctx->last_flags & VOX_FLAG_BF16_INPUTS) ? 1 : 0;
     F.voxel_size = ctx->last_voxel_size;
     F.cloud_vs = ctx->last_cloud_vs;
     F.recs = (const GaussRec*)ctx->recs.p;
@@ -1103,24 +1105,27 @@ int vox_voxelize_host(vox_context_t* ctx, const vox_gaussians_t* gaussians, floa
     cudaSetDevice(ctx->device);
     const int64_t n = gaussians->count;
     DevBuf& in = ctx->hier_keys; // reused as the attribute upload area between calls
+    const size_t es = (flags & VOX_FLAG_BF16_INPUTS) ? 2 : 4; // bytes per attribute value
     const size_t per = 16 * sizeof(float);
     if (!ensure(ctx, in, per * (size_t)(n + 1)))
         return VOX_ERR_MEMORY;
     float* d = (float*)in.p;
     vox_gaussians_t dg;
     dg.count = n;
-    dg.means = d;
-    dg.quats = d + 3 * n;
-    dg.scales = d + 7 * n;
-    dg.opacities = d + 10 * n;
-    dg.colors = d + 11 * n;
+    // the arrays back to back, in their own element size
+    char* db = (char*)d;
+    dg.means = (const float*)db;
+    dg.quats = (const float*)(db + 3 * n * es);
+    dg.scales = (const float*)(db + 7 * n * es);
+    dg.opacities = (const float*)(db + 10 * n * es);
+    dg.colors = (const float*)(db + 11 * n * es);
     if (n > 0)
     {
-        cudaMemcpyAsync((void*)dg.means, gaussians->means, 12 * n, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.quats, gaussians->quats, 16 * n, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.scales, gaussians->scales, 12 * n, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.opacities, gaussians->opacities, 4 * n, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.colors, gaussians->colors, 12 * n, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.means, gaussians->means, 3 * n * es, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.quats, gaussians->quats, 4 * n * es, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.scales, gaussians->scales, 3 * n * es, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.opacities, gaussians->opacities, n * es, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((void*)dg.colors, gaussians->colors, 3 * n * es, cudaMemcpyHostToDevice, ctx->stream);
     }
     int rc = run_voxelize(ctx, &dg, voxel_size, cull_scale, flags);
     if (rc)

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
         const float vsf = rec_vs(F.recs[g], F.voxel_size, F.cloud_vs);
         const double vs = (double)vsf;
         // rotation of the quaternion as the forward used it (normalised for raw inputs)
-        double x = F.quats[4 * g + 1], y = F.quats[4 * g + 2], z = F.quats[4 * g + 3], w = F.quats[4 * g + 0];
+        double x = ld_attr(F.quats, 4 * g + 1, F.bf16), y = ld_attr(F.quats, 4 * g + 2, F.bf16), z = ld_attr(F.quats, 4 * g + 3, F.bf16), w = ld_attr(F.quats, 4 * g + 0, F.bf16);
         const double n = F.raw ? sqrt(x * x + y * y + z * z + w * w) : 1.0;
         x /= n;
         y /= n;
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
         const float min_scale = VOX_FMUL(0.125f, vsf);
         for (int r = 0; r < 3; r++)
         {
-            const float in = F.scales[3 * g + r];
+            const float in = ld_attr(F.scales, 3 * g + r, F.bf16);
             const float sf = F.raw ? vox_expf_cr(in) : in; // the forward's clamp decision
             const bool clamped = !(sf > min_scale);
             const double s_act = F.raw ? exp((double)in) : (double)in;
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) k_bwd_finalize(BwdFinalParams F)
         dq[3] = (float)dz;
         if (F.raw)
         {
-            const double op = 1.0 / (1.0 + exp(-(double)F.opacities[g]));
+            const double op = 1.0 / (1.0 + exp(-(double)ld_attr(F.opacities, g, F.bf16)));
             dop = (float)(a[0] * op * (1.0 - op));
             for (int c = 0; c < 3; c++)
                 dc[c] = (float)(0.28209479177387814 * a[16 + c]);

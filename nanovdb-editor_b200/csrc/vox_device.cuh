@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "vox_detmath.h"
@@ -114,6 +115,7 @@ struct PrepParams
     const float* colors;  // 3G RGB (SH0 when raw)
     int64_t count;
     int raw;              // 1: apply the host preprocessing of raster/RasterUtils.cpp:59-117
+    int bf16;             // 1: every attribute array holds bfloat16 values (read exactly as float)
     float voxel_size;     // every cloud's voxel size when cloud_vs is null
     float cull_scale;     // > 0
     // batched calls: Gaussians [cloud_start[b], cloud_start[b + 1]) form cloud b
@@ -124,6 +126,24 @@ struct PrepParams
 };
 
 
+
+// attribute i of an array of float, or of bfloat16 when bf16 (the upper 16 bits
+// of a float: the conversion is exact, so every later operation is FP32)
+__host__ __device__ __forceinline__ float ld_attr(const float* p, int64_t i, int bf16)
+{
+    if (bf16)
+    {
+        const uint32_t u = (uint32_t)reinterpret_cast<const uint16_t*>(p)[i] << 16;
+#if defined(__CUDA_ARCH__)
+        return __uint_as_float(u);
+#else
+        float f;
+        memcpy(&f, &u, 4);
+        return f;
+#endif
+    }
+    return p[i];
+}
 
 // dot with the reference's fixed evaluation order (a.x*b.x + a.y*b.y) + a.z*b.z
 __device__ __forceinline__ float dot3_rn(float ax, float ay, float az, float bx, float by, float bz)
@@ -141,11 +161,13 @@ __device__ __forceinline__ bool finite_f(float v)
 // Returns the bbox footprint (0 when the Gaussian emits nothing).
 __device__ __forceinline__ uint64_t make_record(const PrepParams& P, int64_t g, float vs, GaussRec& R, int32_t bmax[3])
 {
-    float pos[3] = { P.means[3 * g + 0], P.means[3 * g + 1], P.means[3 * g + 2] };
-    float qw = P.quats[4 * g + 0], qx = P.quats[4 * g + 1], qy = P.quats[4 * g + 2], qz = P.quats[4 * g + 3];
-    float s[3] = { P.scales[3 * g + 0], P.scales[3 * g + 1], P.scales[3 * g + 2] };
-    float op = P.opac[g];
-    float rgb[3] = { P.colors[3 * g + 0], P.colors[3 * g + 1], P.colors[3 * g + 2] };
+    const int h = P.bf16;
+    float pos[3] = { ld_attr(P.means, 3 * g + 0, h), ld_attr(P.means, 3 * g + 1, h), ld_attr(P.means, 3 * g + 2, h) };
+    float qw = ld_attr(P.quats, 4 * g + 0, h), qx = ld_attr(P.quats, 4 * g + 1, h), qy = ld_attr(P.quats, 4 * g + 2, h),
+          qz = ld_attr(P.quats, 4 * g + 3, h);
+    float s[3] = { ld_attr(P.scales, 3 * g + 0, h), ld_attr(P.scales, 3 * g + 1, h), ld_attr(P.scales, 3 * g + 2, h) };
+    float op = ld_attr(P.opac, g, h);
+    float rgb[3] = { ld_attr(P.colors, 3 * g + 0, h), ld_attr(P.colors, 3 * g + 1, h), ld_attr(P.colors, 3 * g + 2, h) };
     if (P.raw)
     {
         // raster/RasterUtils.cpp:59-117
@@ -429,57 +451,6 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
     return alpha_of_d2(R, lattice_min_d2(b));
 }
 
-__device__ __forceinline__ float ex2_approx(float x)
-{
-    float y;
-    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float lg2_approx(float x)
-{
-    float y;
-    asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// The RGBA8 alpha byte of a passing pair, rgba8_byte(pair_alpha(R, b)), with
-// the exp and pow of the exact evaluation replaced, where that is safe, by
-// bounds from the hardware ex2 / lg2 approximations.  The lattice minimum d
-// and x = ls * d are the exact evaluation's.  Then
-//   a  = fl(op exp(-x))           lies in [a_lo, a_hi] = op e^-x (1 -+ 2^-16)
-//                                  (the approximation's error and the exact
-//                                  path's rounding are both below 2^-19),
-//   P  = (1 - a)^e, increasing in 1 - a, lies in [P(1 - a_hi), P(1 - a_lo)]
-//        widened by (|ln P| + e + 8) 2^-17 relative (both evaluations of the
-//        power err by well under that: the log's error is scaled by e),
-//   a' = fl(1 - P) and the byte trunc(255 clamp(a')) are monotone in P,
-// so the byte is known when both ends of the interval give the same byte;
-// otherwise (rarely: near a byte boundary) the exact evaluation decides.  A
-// Gaussian culled by scale gives 0; x > 20 gives a' < e op e^-20 < 1/255.
-__device__ __forceinline__ uint32_t pair_alpha_byte(const GaussRec& R, const Aabb& b)
-{
-    if (R.q7.w != 0.f)
-        return 0u;
-    const float d = lattice_min_d2(b);
-    const float x = VOX_FMUL(R.q6.y, d);
-    if (!(x <= 20.f))
-        return x > 20.f ? 0u : rgba8_byte(alpha_of_d2(R, d));
-    const float a = R.q6.x * ex2_approx(x * -1.44269504f);
-    const float a_hi = a * (1.f + 0x1p-16f), a_lo = a * (1.f - 0x1p-16f);
-    const float b_lo = 1.f - a_hi, b_hi = 1.f - a_lo;
-    if (b_lo > 0.f)
-    {
-        const float e = R.q6.z;
-        const float y_lo = e * lg2_approx(b_lo), y_hi = e * lg2_approx(b_hi); // log2 P at both ends, <= 0
-        const float mu = (fabsf(y_lo) * 0.6931472f + e + 8.f) * 0x1p-17f;
-        const float p_hi = ex2_approx(y_hi) * (1.f + mu), p_lo = ex2_approx(y_lo) * (1.f - mu);
-        const uint32_t byte_lo = rgba8_byte(1.f - p_hi), byte_hi = rgba8_byte(1.f - p_lo);
-        if (byte_lo == byte_hi)
-            return byte_lo;
-    }
-    return rgba8_byte(alpha_of_d2(R, d));
-}
-
 // Stable local AABB of voxel (i, j, k) for the float channels: corner offsets
 // fma(v, vs, -mu) rounded once; per row the lower / upper corner of each axis
 // picked by the sign of the matrix entry (the products' minimum / maximum),
@@ -519,9 +490,19 @@ __device__ __forceinline__ Aabb stable_local_aabb(const GaussRec& R, const RInv&
 // Alpha of the float density / colour channels from the stable local AABB
 // (corner offsets fma(v, vs, -mu), sign-picked corners summed with fma): the
 // lattice points lo + w (hi - lo), float exp / pow.  The oracle's
-// frag_alpha_f evaluates the same operations in the same order.
-__device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
+// frag_alpha_f evaluates the same operations in the same order.  Also keeps
+// what alpha_byte_from_stable needs: the lattice minimum d, op exp(-ls d) and
+// the largest bound magnitude per axis.
+struct AlphaF
 {
+    float a1;   // the channel's alpha
+    float d;    // smallest lattice |p|^2
+    float a;    // op exp(-ls d), before the opacity transform
+    float B[3]; // max(|lo|, |hi|) per axis
+};
+__device__ __forceinline__ AlphaF pair_alpha_f_ex(const GaussRec& R, const Aabb& b)
+{
+    AlphaF f;
     float m[3];
 #pragma unroll
     for (int a = 0; a < 3; a++)
@@ -531,14 +512,84 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
         const float s0 = VOX_FMUL(b.lo[a], b.lo[a]), s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2),
                     s3 = VOX_FMUL(b.hi[a], b.hi[a]);
         m[a] = fminf(fminf(s0, s1), fminf(s2, s3)); // squares: no NaN, no signed zero
+        f.B[a] = fmaxf(fabsf(b.lo[a]), fabsf(b.hi[a]));
     }
-    const float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
-    float a = VOX_FMUL(R.q6.x, vox_expf(-VOX_FMUL(R.q6.y, d)));
+    f.d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
+    float a = VOX_FMUL(R.q6.x, vox_expf(-VOX_FMUL(R.q6.y, f.d)));
     a = a > 0.f ? a : 0.f;
+    f.a = a;
     a = VOX_FSUB(1.f, vox_powf_unit(VOX_FSUB(1.f, a), R.q6.z));
     if (R.q7.w != 0.f)
         a = 0.f;
-    return a;
+    f.a1 = a;
+    return f;
+}
+__device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
+{
+    return pair_alpha_f_ex(R, b).a1;
+}
+
+// The RGBA8 alpha byte of a passing pair, rgba8_byte(pair_alpha(R, b_ref))
+// with b_ref = voxel_local_aabb(...), decided where possible from the float
+// channel's alpha f (same formula, evaluated from the stable local AABB).
+// Both AABBs approximate the exact local AABB of the voxel; per row r their
+// bounds differ by at most
+//   D_r = 2^-21 il is_r sum_k |m_rk| A_k + 2^-20 B_r,
+// A_k = |mu_k| + 3 |centre offset_k| + 2 vs bounding the corner magnitudes:
+// the reference's fl(v vs) - mu rounds twice (2^-24 of |v vs| and of the
+// offset), its products, sums and scaling once each, the stable form's
+// likewise; the 2^-20 B_r term also covers the lattice points' rounding.
+// So the lattice minima d differ by at most md = sum_r (2 B'_r D_r + D_r^2 +
+// 2^-22 B'_r^2) + 2^-21 d (B' = B + D; squares and sums rounded), and the
+// alpha a' = 1 - (1 - op e^-ls d)^e, whose slope in d is at most
+// e ls a_hi (times 1 / (1 - a_hi) when e < 1) for a_hi >= op e^-ls (d - md),
+// by at most that slope times md, plus both evaluations' own error (a few ulp
+// of the exp and pow: 4e-6 (1 + e) bounds it).  When a' +- that margin falls
+// in one byte (rgba8_byte is monotone) the byte is the reference's; else the
+// reference's evaluation runs.  VOX_CHECK_EMIT=1 compares every decided byte
+// with the reference's evaluation.
+__device__ __forceinline__ uint32_t alpha_byte_from_stable(const GaussRec& R, const RInv& M, float vs, int32_t i,
+                                                           int32_t j, int32_t k, const AlphaF& f, bool& decided)
+{
+    decided = true;
+    if (R.q7.w != 0.f)
+        return 0u; // culled by scale: both alphas are 0
+    const int32_t v[3] = { i, j, k };
+    const float mu[3] = { R.q0.x, R.q0.y, R.q0.z };
+    float A[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+        A[a] = fabsf(mu[a]) + 3.f * fabsf(fmaf((float)v[a] + 0.5f, vs, -mu[a])) + 2.f * vs;
+    const float il = R.q0.w;
+    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+    float md = 0.f;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+    {
+        const float S = fabsf(M.m[r][0]) * A[0] + fabsf(M.m[r][1]) * A[1] + fabsf(M.m[r][2]) * A[2];
+        const float D = 0x1p-21f * il * is[r] * S + 0x1p-20f * f.B[r];
+        const float Bp = f.B[r] + D;
+        md += 2.f * Bp * D + D * D + 0x1p-22f * Bp * Bp;
+    }
+    md = md * (1.f + 0x1p-20f) + 0x1p-21f * f.d;
+    const float ls = R.q6.y, e = R.q6.z;
+    const float x = ls * md;
+    if (x < 0.25f)
+    {
+        const float a_hi = f.a * (1.f + 2.f * x) * (1.f + 1e-6f); // e^x <= 1 + 2x for x <= 1
+        if (a_hi < 1.f)
+        {
+            float slope = e * ls * a_hi;
+            if (e < 1.f)
+                slope = slope / (1.f - a_hi);
+            const float delta = 1.25f * slope * md + 4e-6f * (1.f + e) + 1e-6f;
+            const uint32_t lo = rgba8_byte(f.a1 - delta), hi = rgba8_byte(f.a1 + delta);
+            if (lo == hi)
+                return lo;
+        }
+    }
+    decided = false;
+    return rgba8_byte(pair_alpha(R, voxel_local_aabb(R, M, vs, i, j, k)));
 }
 
 // Differentiable channels (VOX_FLAG_DIFFERENTIABLE).  The reference alpha

@@ -698,16 +698,22 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                 const RInv M = rinv_of(R);
                 const float vsf = C.vs[j];
                 const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7), zz = ao[2] + (int32_t)(n & 7);
-                const uint32_t a8 = pair_alpha_byte(R, voxel_local_aabb(R, M, vsf, x, yy, zz));
                 float a;
+                uint32_t a8;
                 if (P.smooth)
                 {
                     SmoothTerms st;
                     a = smooth_kernel(R, M, vsf, x, yy, zz, st);
+                    a8 = rgba8_byte(pair_alpha(R, voxel_local_aabb(R, M, vsf, x, yy, zz)));
                 }
                 else
                 {
-                    a = pair_alpha_f(R, stable_local_aabb(R, M, vsf, x, yy, zz));
+                    const AlphaF af = pair_alpha_f_ex(R, stable_local_aabb(R, M, vsf, x, yy, zz));
+                    a = af.a1;
+                    bool decided;
+                    a8 = alpha_byte_from_stable(R, M, vsf, x, yy, zz, af, decided);
+                    if (CHECK && decided && a8 != rgba8_byte(pair_alpha(R, voxel_local_aabb(R, M, vsf, x, yy, zz))))
+                        atomicOr(P.err, ERR_BOUNDS); // the margin failed to cover the reference's byte
                 }
                 atomicAdd(&A.cnt[n], 1u);
                 atomicMax(&A.rgba[n], (a8 << 24) | C.rgb24[j]);

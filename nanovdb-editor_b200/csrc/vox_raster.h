@@ -98,6 +98,7 @@ struct BwdFinalParams
     int64_t G;
     const float *means, *quats, *scales, *opacities, *colors; // the forward's inputs
     int raw;
+    int bf16; // the inputs are bfloat16 arrays
     float voxel_size;
     const float* cloud_vs;
     const GaussRec* recs;

@@ -16,23 +16,25 @@ import torch
 
 from .exceptions import PipelineError
 from .grid import HEADER_DTYPE
-from .vox import FLAG_DIFFERENTIABLE, FLAG_RAW_INPUTS, VoxContext
+from .vox import FLAG_BF16_INPUTS, FLAG_DIFFERENTIABLE, FLAG_RAW_INPUTS, VoxContext
 
 _NAMES = ("means", "quats", "scales", "opacities", "colors")
 
 
-def _prep(t: torch.Tensor) -> torch.Tensor:
+def _prep(t: torch.Tensor, bf16: bool) -> torch.Tensor:
     if not t.is_cuda:
         raise PipelineError("voxelize: inputs must be CUDA tensors")
-    return t.detach().to(torch.float32).contiguous()
+    return t.detach().to(torch.bfloat16 if bf16 else torch.float32).contiguous()
 
 
 class VoxelizeFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means, quats, scales, opacities, colors, voxel_size, raw, vox):
-        ins = [_prep(t) for t in (means, quats, scales, opacities, colors)]
+        # bfloat16 attributes (all five) are read as such (VOX_FLAG_BF16_INPUTS); gradients are FP32
+        bf16 = all(t.dtype == torch.bfloat16 for t in (means, quats, scales, opacities, colors))
+        ins = [_prep(t, bf16) for t in (means, quats, scales, opacities, colors)]
         torch.cuda.current_stream(ins[0].device).synchronize()  # the library reads on its own stream
-        flags = FLAG_DIFFERENTIABLE | (FLAG_RAW_INPUTS if raw else 0)
+        flags = FLAG_DIFFERENTIABLE | (FLAG_RAW_INPUTS if raw else 0) | (FLAG_BF16_INPUTS if bf16 else 0)
         _, nbytes = vox.voxelize(*ins, float(voxel_size), 0.05, flags)
         grid = torch.empty(nbytes, dtype=torch.uint8, device=ins[0].device)
         vox.grid_device(grid)
@@ -56,7 +58,8 @@ class VoxelizeFunction(torch.autograd.Function):
         ins = ctx.saved_tensors
         gd = None if g_density is None else g_density.detach().to(torch.float32).contiguous()
         gc = None if g_color is None else g_color.detach().to(torch.float32).contiguous()
-        out = {k: torch.empty_like(t) for k, t, need in zip(_NAMES, ins, ctx.needs_input_grad[:5]) if need}
+        out = {k: torch.empty(t.shape, dtype=torch.float32, device=t.device)
+               for k, t, need in zip(_NAMES, ins, ctx.needs_input_grad[:5]) if need}
         torch.cuda.current_stream(ins[0].device).synchronize()
         vox.backward(*ins, gd, gc, out)
         return tuple(out.get(k) for k in _NAMES) + (None, None, None)
@@ -131,3 +134,49 @@ def l2_to_target(density: torch.Tensor, vox: VoxContext, target: TargetGrid) -> 
     d = density[2:]
     missing = target.total_sq - float((t.double() ** 2).sum())  # target voxels the grid lacks: constant
     return 0.5 * ((d - t) ** 2).sum() + 0.5 * missing
+
+
+def batch_voxel_keys(vox: VoxContext, value_offsets, device):
+    """int64 keys (cloud, i, j, k) of every value index of the context's last
+    batched grid (clouds back to back), and a mask that is False on each
+    cloud's two background slots."""
+    voff = torch.as_tensor(np.asarray(value_offsets, dtype=np.int64), device=device)
+    total = int(voff[-1])
+    ijk = torch.full((max(total, 1), 3), -(1 << 31), dtype=torch.int32, device=device)
+    if total:
+        vox.voxel_coords(ijk)
+    ijk = ijk[:total]
+    counts = voff[1:] - voff[:-1]
+    cloud = torch.repeat_interleave(torch.arange(counts.numel(), device=device), counts)
+    local = torch.arange(total, device=device) - voff[:-1][cloud]
+    valid = local >= 2
+    b = ijk.to(torch.int64) + (1 << 18)  # |coordinate| < 2^17 (the node2 root key range)
+    keys = (cloud << 57) | (b[:, 0] << 38) | (b[:, 1] << 19) | b[:, 2]
+    return keys, valid
+
+
+class BatchTargetGrid:
+    """Per-cloud target densities of a batched grid, looked up by (cloud, voxel)."""
+
+    def __init__(self, keys: torch.Tensor, valid: torch.Tensor, density: torch.Tensor):
+        k = keys[valid]
+        d = density[valid].detach()
+        order = torch.argsort(k)
+        self.keys = k[order].contiguous()
+        self.density = d[order].contiguous()
+        self.total_sq = float((self.density.double() ** 2).sum())
+
+    def lookup(self, keys: torch.Tensor):
+        if self.keys.numel() == 0:
+            return torch.zeros(keys.shape, dtype=torch.float32, device=keys.device)
+        pos = torch.searchsorted(self.keys, keys).clamp(max=self.keys.numel() - 1)
+        return torch.where(self.keys[pos] == keys, self.density[pos], torch.zeros((), device=keys.device))
+
+
+def l2_to_batch_target(density: torch.Tensor, keys: torch.Tensor, valid: torch.Tensor, target: BatchTargetGrid):
+    """0.5 * sum over every cloud's voxels (the union with its target's) of
+    (density - target)^2, and dL/d density (zero on background slots)."""
+    t = target.lookup(keys)
+    diff = torch.where(valid, density - t, torch.zeros((), device=density.device))
+    missing = target.total_sq - float((torch.where(valid, t, torch.zeros((), device=t.device)).double() ** 2).sum())
+    return 0.5 * float((diff.double() ** 2).sum()) + 0.5 * missing, diff

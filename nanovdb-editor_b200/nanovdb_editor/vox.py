@@ -20,6 +20,7 @@ from .utils import load_library
 FLAG_RAW_INPUTS = 1
 FLAG_WINDOW_ORDER = 2
 FLAG_DIFFERENTIABLE = 4
+FLAG_BF16_INPUTS = 8
 
 STATUS = {
     0: "ok",
@@ -124,6 +125,8 @@ def _lib():
         lib.vox_voxelbvh_transform_inverse.argtypes = [c_void_p, c_void_p]
         lib.vox_context_set_wait_limit.restype = c_int
         lib.vox_context_set_wait_limit.argtypes = [c_void_p, c_uint32, c_int]
+        lib.vox_adam_bf16.restype = c_int
+        lib.vox_adam_bf16.argtypes = [c_void_p] * 5 + [c_int64, c_float, c_float, c_float, c_float, c_int64, c_void_p]
         lib._vox_bound = True
     return lib
 
@@ -267,6 +270,20 @@ class VoxContext:
         st = vox_stats_t()
         self.lib.vox_get_stats(self.handle, byref(st))
         return st.as_dict()
+
+    def adam_bf16(self, master, m, v, grad, out_bf16, step: int, lr: float, beta1: float = 0.9, beta2: float = 0.999,
+                  eps: float = 1e-8) -> None:
+        """One fused Adam step on the context's stream: FP32 master / moments
+        (float32 CUDA tensors) updated from `grad`, the bfloat16 attribute
+        tensor `out_bf16` rewritten from the master copy."""
+        n = int(master.numel())
+        for t in (m, v, grad, out_bf16):
+            if int(t.numel()) != n:
+                raise PipelineError("adam_bf16: tensors of different sizes")
+        rc = self.lib.vox_adam_bf16(_ptr(master), _ptr(m), _ptr(v), _ptr(grad), _ptr(out_bf16), n, float(lr), float(beta1),
+                                    float(beta2), float(eps), int(step), self.stream)
+        if rc != 0:
+            raise PipelineError(f"vox_adam_bf16: {STATUS.get(rc, rc)}")
 
     def set_wait_limit(self, max_polls=None, withhold_publication: bool = False) -> None:
         """Bound of the device look-back waits for later calls (None: the
