@@ -503,6 +503,10 @@ def measure_fit_bf16(ctx, torch, rank, steps=None):
         loss, gd = l2_to_batch_target(density, keys, valid, target)
         torch.cuda.synchronize()
         ctx.backward(*[bf[k] for k in names], gd.contiguous(), None, grads)
+        if t == steps:  # the values this step's density and gradients belong to, before the update
+            b = int(np.argmin([c.n for c in clouds]))
+            g0, g1 = int(start[b]), int(start[b + 1])
+            cur = {k: bf[k][g0:g1].to(torch.float32).cpu().numpy() for k in names}
         for k in names:
             ctx.adam_bf16(master[k], mom[k][0], mom[k][1], grads[k], bf[k], t, lr[k])
         e1.record(ext)
@@ -510,10 +514,7 @@ def measure_fit_bf16(ctx, torch, rank, steps=None):
         times.append(e0.elapsed_time(e1))
         losses.append(loss)
     # FP64 check on the smallest cloud: the last step's density and gradients
-    b = int(np.argmin([c.n for c in clouds]))
-    g0, g1 = int(start[b]), int(start[b + 1])
     v0, v1 = int(voff[b]), int(voff[b + 1])
-    cur = {k: bf[k][g0:g1].to(torch.float32).cpu().numpy() for k in names}
     act = oracle_py.preprocess([cur["means"], cur["opacities"], cur["quats"], cur["scales"], cur["colors"]])
     ref = oracle_py.OracleResult(act, float(vs[b]), 0.05, window_mode=oracle_py.OV_MODE_SMOOTH)
     vals = ref.values()

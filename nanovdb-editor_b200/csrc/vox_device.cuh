@@ -529,17 +529,56 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
     return pair_alpha_f_ex(R, b).a1;
 }
 
+// unit in the last place of |x| (a float), 0 for 0
+__device__ __forceinline__ float ulp_of(float x)
+{
+    return __uint_as_float(__float_as_uint(fabsf(x)) & 0x7f800000u) * 0x1p-23f;
+}
+
+// How far the reference's local AABB of a voxel (voxel_local_aabb: corner
+// offsets fl(fl(v vs) - mu), products, sums, the two scalings) and the stable
+// one (stable_local_aabb: fma(v, vs, -mu), an fma chain, one scaling) can
+// differ, per row, for any voxel of the leaf at o, apart from a term
+// proportional to the bound itself.  Per axis k the two corner offsets differ
+// by at most E_k = ulp(max |v vs|) / 2 + ulp(max |c|) over the leaf's corner
+// coordinates v in [o, o + 8] (one rounding of v vs, one of the difference in
+// each evaluation); the products, sums and fma roundings of both add at most
+// 6 2^-24 sum_k |m_rk| |c_k| <= 2^-21 sum_k |m_rk| C_k; the row's distance is
+// then scaled by il is_r.  The scalings' and lattice points' roundings are
+// proportional to the bound magnitude B_r and are added per pair
+// (alpha_byte_from_stable).  Computed once per (leaf, Gaussian) pair.
+__device__ __forceinline__ void aabb_difference_bound(const GaussRec& R, float vs, const int32_t o[3], float& d0,
+                                                      float& d1, float& d2)
+{
+    const float mu[3] = { R.q0.x, R.q0.y, R.q0.z };
+    const RInv M = rinv_of(R);
+    float G[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+    {
+        const float w0 = (float)o[k] * vs, w1 = (float)(o[k] + 8) * vs;
+        const float W = fmaxf(fabsf(w0), fabsf(w1)) * (1.f + 0x1p-20f);
+        const float Cm = fmaxf(fabsf(w0 - mu[k]), fabsf(w1 - mu[k])) * (1.f + 0x1p-20f);
+        G[k] = 0.5f * ulp_of(W) + ulp_of(Cm) + 0x1p-21f * Cm;
+    }
+    const float il = R.q0.w;
+    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+    float d[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+        d[r] = (1.f + 0x1p-20f) * il * is[r] *
+               (fabsf(M.m[r][0]) * G[0] + fabsf(M.m[r][1]) * G[1] + fabsf(M.m[r][2]) * G[2]);
+    d0 = d[0];
+    d1 = d[1];
+    d2 = d[2];
+}
+
 // The RGBA8 alpha byte of a passing pair, rgba8_byte(pair_alpha(R, b_ref))
 // with b_ref = voxel_local_aabb(...), decided where possible from the float
 // channel's alpha f (same formula, evaluated from the stable local AABB).
-// Both AABBs approximate the exact local AABB of the voxel; per row r their
-// bounds differ by at most
-//   D_r = 2^-21 il is_r sum_k |m_rk| A_k + 2^-20 B_r,
-// A_k = |mu_k| + 3 |centre offset_k| + 2 vs bounding the corner magnitudes:
-// the reference's fl(v vs) - mu rounds twice (2^-24 of |v vs| and of the
-// offset), its products, sums and scaling once each, the stable form's
-// likewise; the 2^-20 B_r term also covers the lattice points' rounding.
-// So the lattice minima d differ by at most md = sum_r (2 B'_r D_r + D_r^2 +
+// Per row the two AABBs' bounds differ by at most D_r = dab_r + 2^-20 B_r
+// (aabb_difference_bound, plus the scalings' and lattice points' roundings),
+// so their lattice minima d differ by at most md = sum_r (2 B'_r D_r + D_r^2 +
 // 2^-22 B'_r^2) + 2^-21 d (B' = B + D; squares and sums rounded), and the
 // alpha a' = 1 - (1 - op e^-ls d)^e, whose slope in d is at most
 // e ls a_hi (times 1 / (1 - a_hi) when e < 1) for a_hi >= op e^-ls (d - md),
@@ -549,27 +588,19 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
 // reference's evaluation runs.  VOX_CHECK_EMIT=1 compares every decided byte
 // with the reference's evaluation.
 __device__ __forceinline__ uint32_t alpha_byte_from_stable(const GaussRec& R, const RInv& M, float vs, int32_t i,
-                                                           int32_t j, int32_t k, const AlphaF& f, bool& decided)
+                                                           int32_t j, int32_t k, const AlphaF& f, const float dab[3],
+                                                           bool& decided)
 {
     decided = true;
     if (R.q7.w != 0.f)
         return 0u; // culled by scale: both alphas are 0
-    const int32_t v[3] = { i, j, k };
-    const float mu[3] = { R.q0.x, R.q0.y, R.q0.z };
-    float A[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-        A[a] = fabsf(mu[a]) + 3.f * fabsf(fmaf((float)v[a] + 0.5f, vs, -mu[a])) + 2.f * vs;
-    const float il = R.q0.w;
-    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
     float md = 0.f;
 #pragma unroll
     for (int r = 0; r < 3; r++)
     {
-        const float S = fabsf(M.m[r][0]) * A[0] + fabsf(M.m[r][1]) * A[1] + fabsf(M.m[r][2]) * A[2];
-        const float D = 0x1p-21f * il * is[r] * S + 0x1p-20f * f.B[r];
+        const float D = dab[r] + 0x1p-20f * f.B[r];
         const float Bp = f.B[r] + D;
-        md += 2.f * Bp * D + D * D + 0x1p-22f * Bp * Bp;
+        md += (2.f * Bp + D) * D + 0x1p-22f * Bp * Bp;
     }
     md = md * (1.f + 0x1p-20f) + 0x1p-21f * f.d;
     const float ls = R.q6.y, e = R.q6.z;

@@ -333,6 +333,7 @@ struct LeafChunk
     uint32_t bcol[LQ_CHUNK];                             // box columns, nx * ny (0: empty box)
     uint32_t rgb24[LQ_CHUNK];                            // the colour bytes of the packed RGBA8 value
     float vs[LQ_CHUNK];
+    float dab[3][LQ_CHUNK]; // per row: how far the two local-AABB evaluations can differ in this leaf
     uint8_t flag[LQ_CHUNK];
     uint64_t wf0[LQ_CHUNK], wbase[LQ_CHUNK]; // reference windows: fragment offset in its batch, windows before
 };
@@ -532,6 +533,7 @@ __device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChun
     leaf_box_fields(C, j, R, o);
     C.rgb24[j] = rgba8_byte(R.q7.x) | (rgba8_byte(R.q7.y) << 8) | (rgba8_byte(R.q7.z) << 16);
     C.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
+    aabb_difference_bound(R, C.vs[j], o, C.dab[0][j], C.dab[1][j], C.dab[2][j]);
     C.flag[j] = CHECK ? P.emit_flag[P.vals[q]] : 0;
     if (WINDOW)
     {
@@ -711,7 +713,8 @@ __global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, u
                     const AlphaF af = pair_alpha_f_ex(R, stable_local_aabb(R, M, vsf, x, yy, zz));
                     a = af.a1;
                     bool decided;
-                    a8 = alpha_byte_from_stable(R, M, vsf, x, yy, zz, af, decided);
+                    const float dab[3] = { C.dab[0][j], C.dab[1][j], C.dab[2][j] };
+                    a8 = alpha_byte_from_stable(R, M, vsf, x, yy, zz, af, dab, decided);
                     if (CHECK && decided && a8 != rgba8_byte(pair_alpha(R, voxel_local_aabb(R, M, vsf, x, yy, zz))))
                         atomicOr(P.err, ERR_BOUNDS); // the margin failed to cover the reference's byte
                 }
