@@ -343,6 +343,9 @@ typedef struct vox_stats_t
     float ms_vb_ranges;   /* range headers + 64-bit key write-back */
     int32_t vb_sort_bits; /* key bits sorted (compressed key width, or 64) */
     int64_t vb_launches;  /* kernels launched by that call */
+    /* the online tuner's choices (variants give identical results) */
+    int32_t walk_ctas_per_sm; /* leaf walk: resident CTAs per SM it ran with */
+    int32_t vb_search;        /* VoxelBVH level search: 0 lane-balanced, 1 thread per Gaussian */
 } vox_stats_t;
 
 /* One context per caller thread; it owns a CUDA stream on `device` and a

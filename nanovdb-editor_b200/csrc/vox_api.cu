@@ -86,6 +86,9 @@ struct vox_context_t
     vox_stats_t stats{};
     Timers timers;
     SortTuning tuning;
+    OnlineChoice walk_choice{ 2 };     // leaf walk: 4 or 3 CTAs per SM
+    OnlineChoice vb_search_choice{ 2 }; // VoxelBVH level search: lane-balanced or thread per Gaussian
+    int walk_variant = 0, vb_variant = 0;
     // last result
     int64_t last_P = 0;
     uint64_t last_grid_bytes = 0;
@@ -625,7 +628,8 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     LP.cand_vbase = (const uint64_t*)ctx->cand_vbase.p;
     LP.cand_voff = (const uint64_t*)ctx->cand_voff.p;
     LP.key64 = key64;
-    launch_leaf_pass(LP, d_counter, ctx->num_sms, s);
+    ctx->walk_variant = ctx->walk_choice.pick((int64_t)Q);
+    ctx->stats.walk_ctas_per_sm = launch_leaf_pass(LP, d_counter, ctx->num_sms, s, ctx->walk_variant);
     cudaEventRecord(ctx->timers.ev[4], s);
     launch_leaf_popc(LP.cand_mask, NCL, (uint64_t*)ctx->cand_cnt.p, s);
     scan_exclusive_u64((const uint64_t*)ctx->cand_cnt.p, (uint64_t*)ctx->cand_voff.p, NCL, 0, sc + SC_NVOX, scan_status,
@@ -833,6 +837,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     st.ms_emit = elapsed(ctx->timers.ev[1], ctx->timers.ev[2]);       // (leaf, Gaussian) pairs
     st.ms_sort = elapsed(ctx->timers.ev[2], ctx->timers.ev[3]);       // sort + candidate leaves
     st.ms_accumulate = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]); // leaf walk: test, RGBA8, float sums
+    ctx->walk_choice.report((int64_t)Q, ctx->walk_variant, st.ms_accumulate);
     st.ms_build = elapsed(ctx->timers.ev[4], ctx->timers.ev[6]);      // topology, values, node2
     st.ms_total = elapsed(ctx->timers.ev[0], ctx->timers.ev[6]);
     st.kernel_launches = launch_count() - launches0;
@@ -1536,9 +1541,11 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
     cudaEventRecord(ctx->timers.ev[0], s);
     launch_vb_init(P.box_keys, P.cell_minmax, s);
     launch_vb_box(P, ctx->num_sms, s);
-    // VOX_VB_SEARCH=thread: the thread-per-Gaussian search (comparison)
+    // the level search variant: the tuner's choice, or VOX_VB_SEARCH=thread / lane
     const char* search = getenv("VOX_VB_SEARCH");
-    if (search && search[0] == 't')
+    ctx->vb_variant = search && search[0] == 't' ? 1 : search && search[0] == 'l' ? 0 : ctx->vb_search_choice.pick(count);
+    ctx->stats.vb_search = ctx->vb_variant;
+    if (ctx->vb_variant == 1)
         launch_vb_ijkl(P, s);
     else
     {
@@ -1636,6 +1643,8 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
     };
     vox_stats_t& st = ctx->stats;
     st.ms_vb_keys = elapsed(ctx->timers.ev[0], ctx->timers.ev[1]);
+    if (!search)
+        ctx->vb_search_choice.report(count, ctx->vb_variant, st.ms_vb_keys);
     st.ms_vb_sort = elapsed(ctx->timers.ev[2], ctx->timers.ev[3]);
     st.ms_vb_ranges = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]);
     st.vb_sort_bits = sort_bits;

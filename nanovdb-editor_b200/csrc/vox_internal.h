@@ -77,6 +77,49 @@ void dual_combine(const uint32_t* low, const uint32_t* high, int64_t n, int low_
 void dual_gather(const uint32_t* sidx, int64_t n, const uint32_t* low_c, const uint32_t* high_c, const uint32_t* val_c,
                  uint32_t* low, uint32_t* high, uint32_t* val, int* err, int num_sms, cudaStream_t s);
 
+// Online choice among launch variants that give identical results.  Per size
+// class (floor(log2) of the work), each call of a class that has untried
+// variants runs the next one and reports its time per unit of work; later
+// calls run the fastest.  No extra work is launched to tune.
+struct OnlineChoice
+{
+    static const int kClasses = 40, kMax = 4;
+    int variants = 1;
+    float cost[kClasses][kMax];
+    explicit OnlineChoice(int n = 1) : variants(n)
+    {
+        for (auto& r : cost)
+            for (float& c : r)
+                c = -1.f;
+    }
+    static int size_class(int64_t work)
+    {
+        int c = 0;
+        while (c < kClasses - 1 && (1ll << (c + 1)) <= work)
+            c++;
+        return c;
+    }
+    int pick(int64_t work) const
+    {
+        const int c = size_class(work);
+        int best = 0;
+        for (int v = 0; v < variants; v++)
+        {
+            if (cost[c][v] < 0.f)
+                return v;
+            if (cost[c][v] < cost[c][best])
+                best = v;
+        }
+        return best;
+    }
+    void report(int64_t work, int v, float ms)
+    {
+        const int c = size_class(work);
+        if (v >= 0 && v < variants && work > 0 && cost[c][v] < 0.f && ms > 0.f)
+            cost[c][v] = ms / (float)work;
+    }
+};
+
 // ---------------------------------------------------------------- sort ----
 struct SortTuning
 {

@@ -543,8 +543,8 @@ __device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChun
     }
 }
 
-template <bool CHECK, bool WINDOW>
-__global__ void __launch_bounds__(LP_THREADS, 4) k_leaf_pass(LeafPassParams P, uint32_t* counter)
+template <bool CHECK, bool WINDOW, int MINB = 4>
+__global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P, uint32_t* counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LeafQSmem& S = *reinterpret_cast<LeafQSmem*>(smem_raw);
@@ -1294,14 +1294,15 @@ static unsigned walk_grid(int64_t NCL, int num_sms)
     return (unsigned)(g < NCL ? g : (NCL > 0 ? NCL : 1));
 }
 
-void launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s)
+int launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s, int variant)
 {
     if (P.NCL <= 0)
-        return;
+        return 0;
     cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     const size_t smem = sizeof(LeafQSmem);
     auto kern = P.emit_flag ? (P.window ? k_leaf_pass<true, true> : k_leaf_pass<true, false>)
-                            : (P.window ? k_leaf_pass<false, true> : k_leaf_pass<false, false>);
+                : variant == 1 ? (P.window ? k_leaf_pass<false, true, 3> : k_leaf_pass<false, false, 3>)
+                               : (P.window ? k_leaf_pass<false, true> : k_leaf_pass<false, false>);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LP_THREADS, smem);
@@ -1309,6 +1310,7 @@ void launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, c
     if (grid > P.NCL)
         grid = P.NCL;
     { kern<<<(unsigned)grid, LP_THREADS, smem, s>>>(P, counter); count_launch(); }
+    return per_sm;
 }
 
 void launch_leaf_backward(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s)

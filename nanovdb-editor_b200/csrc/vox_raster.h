@@ -178,7 +178,9 @@ void launch_leaf_compact(const uint32_t* keys, const uint32_t* vals, const uint3
                          const uint64_t* flags, const uint64_t* pos, const uint32_t* lower_cell,
                          const uint32_t* root_of_rank, uint32_t* cand_key, int4* cand_org, uint32_t* cand_start,
                          uint32_t* pair_gid, cudaStream_t s);
-void launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
+// variant 0: 4 resident CTAs per SM (64 registers per thread), 1: 3 CTAs per SM;
+// returns the CTAs per SM it ran with
+int launch_leaf_pass(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s, int variant = 0);
 void launch_leaf_backward(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
 void launch_leaf_export(const LeafPassParams& P, uint32_t* counter, int num_sms, cudaStream_t s);
 void launch_leaf_popc(const uint64_t* cand_mask, int64_t NCL, uint64_t* counts, cudaStream_t s);

@@ -74,6 +74,8 @@ class vox_stats_t(Structure):
         ("ms_vb_ranges", c_float),
         ("vb_sort_bits", c_int32),
         ("vb_launches", c_int64),
+        ("walk_ctas_per_sm", c_int32),
+        ("vb_search", c_int32),
     ]
 
     def as_dict(self) -> dict:
