@@ -334,6 +334,8 @@ struct LeafChunk
     uint32_t rgb24[LQ_CHUNK];                            // the colour bytes of the packed RGBA8 value
     float vs[LQ_CHUNK];
     float dab[3][LQ_CHUNK]; // per row: how far the two local-AABB evaluations can differ in this leaf
+    float zst[3][LQ_CHUNK]; // per row: the scaled z step fl(vs m_r2 il is_r)
+    uint32_t cstart[16];    // first column of box j (boxes past the chunk's count: empty); [LQ_CHUNK]: all
     uint8_t flag[LQ_CHUNK];
     uint64_t wf0[LQ_CHUNK], wbase[LQ_CHUNK]; // reference windows: fragment offset in its batch, windows before
 };
@@ -371,7 +373,27 @@ struct LeafQSmem
 // positions and stores its count in qcount[w] - a deterministic order (a warp
 // tests at most 2 x 32 columns of 8 voxels).  Otherwise one shared queue, a
 // shared atomic per warp and round.
-template <bool CHECK, bool PER_WARP = false, class Chunk>
+//
+// APPROX (the chunk carries dab and zst): each voxel of the column is first
+// classified from bounds linear in k - the reference's scaled bounds of the
+// column's first voxel, sl / sh, plus k times the scaled z step st = fl(vs
+// m_r2 il is_r) - and only voxels near the sphere run the reference test.
+// Per row, the reference's bound of voxel k and the linear one both lie
+// within dab_r + 2^-21 |bound| of the exact-arithmetic bound (corner offsets,
+// products and sums as in aabb_difference_bound; the sum and two scalings
+// relative), the step's three roundings times k <= 8 and the fma's own
+// rounding add at most 2^-20 (|sl| + |sh| + 8 |st|) in all, so the selected
+// values (max(lo, min(hi, 0)), 1-Lipschitz in both bounds) differ by at most
+// delta_r = 2 dab_r + 2^-20 (|sl| + |sh| + 8 |st|), and the vectors of the
+// three by at most Delta = sum delta_r in norm.  The reference passes a
+// voxel when its fl-evaluated 1 - S > 0, surely if S < 1 - 2^-22 and surely
+// not if S > 1 + 2^-20 (six roundings of values below 2 S + 1); with D the
+// fma-summed squares of the linear values (relative error <= 2^-21) and
+// Delta <= 1/16, D < 1 - Mg implies the first and D > 1 + Mg the second for
+// Mg = 4 Delta + 2^-18.  Voxels with D in [1 - Mg, 1 + Mg] (or NaN), and every
+// voxel of a column with Delta > 1/16, take the reference test.  In CHECK
+// mode every voxel also takes it and a difference sets ERR_BOUNDS.
+template <bool CHECK, bool PER_WARP = false, bool APPROX = false, class Chunk>
 __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const Chunk& C, uint32_t cnt,
                                                 const int32_t o[3], uint16_t* queue, uint32_t* qcount, int t, int lane)
 {
@@ -379,25 +401,43 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
     if (PER_WARP)
         queue += (t >> 5) * (LQ_CHUNK * 64);
     uint32_t start[LQ_CHUNK + 1];
-    start[0] = 0;
+    uint32_t T;
+    if constexpr (APPROX)
+        T = C.cstart[LQ_CHUNK]; // the staged prefix (no registers held across the rounds)
+    else
+    {
+        start[0] = 0;
 #pragma unroll
-    for (int j = 0; j < LQ_CHUNK; j++)
-        start[j + 1] = start[j] + (j < (int)cnt ? C.bcol[j] : 0u);
-    const uint32_t T = start[LQ_CHUNK];
+        for (int j = 0; j < LQ_CHUNK; j++)
+            start[j + 1] = start[j] + (j < (int)cnt ? C.bcol[j] : 0u);
+        T = start[LQ_CHUNK];
+    }
     for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
     {
         const uint32_t e = b0 + (uint32_t)t;
         uint32_t zmask = 0, ebase = 0;
         if (e < T)
         {
+            // j: the last box whose first column is <= e (empty boxes skipped); sj its first column
             int j = 0;
-            uint32_t sj = 0; // start[j], without a dynamically indexed (local memory) array
-#pragma unroll
-            for (int q = 1; q < LQ_CHUNK; q++)
+            uint32_t sj = 0;
+            if constexpr (APPROX)
             {
-                const bool ge = e >= start[q];
-                j += ge ? 1 : 0;
-                sj = ge ? start[q] : sj;
+#pragma unroll
+                for (int s = 8; s; s >>= 1)
+                    if (j + s < LQ_CHUNK && C.cstart[j + s] <= e)
+                        j += s;
+                sj = C.cstart[j];
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 1; q < LQ_CHUNK; q++) // without a dynamically indexed (local memory) array
+                {
+                    const bool ge = e >= start[q];
+                    j += ge ? 1 : 0;
+                    sj = ge ? start[q] : sj;
+                }
             }
             const uint32_t local = e - sj;
             const uint32_t dx = (local * C.bdiv_y[j]) >> 16;
@@ -410,9 +450,7 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
             float cx0, cx1, cy0, cy1;
             axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
             axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
-            float slo[3], shi[3], pa[3];
-            float v = (float)(o[2] + rz0);
-            float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+            float slo[3], shi[3];
 #pragma unroll
             for (int r = 0; r < 3; r++)
             {
@@ -421,36 +459,101 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
                 minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
                 slo[r] = VOX_FADD(xn, yn);
                 shi[r] = VOX_FADD(xx, yx);
-                pa[r] = VOX_FMUL(cz, M.m[r][2]);
             }
-            // the corner offsets grow with z, so per row the smaller product is the
-            // lower corner's when the matrix entry is >= 0 (fl(c m) is monotone in c;
-            // a tie differs at most in the sign of a zero, which the test squares)
-            bool up[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-                up[r] = M.m[r][2] >= 0.f;
             const uint32_t nz = C.bnz[j];
+            // the reference test of the column's voxels, z run from k0 (mask bits from k0)
+            auto exact_run = [&](uint32_t k0, uint32_t k1) -> uint32_t {
+                uint32_t mk = 0;
+                float v = (float)(o[2] + rz0 + (int32_t)k0);
+                float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                float pa[3];
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    pa[r] = VOX_FMUL(cz, M.m[r][2]);
 #pragma unroll 2
-            for (uint32_t k = 0; k < nz; k++)
+                for (uint32_t k = k0; k < k1; k++)
+                {
+                    v = VOX_FADD(v, 1.f);
+                    cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                    float d2 = 1.f;
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        // the corner offsets grow with z: per row the smaller product is the
+                        // lower corner's when the matrix entry is >= 0 (fl(c m) is monotone
+                        // in c; a tie differs at most in the sign of a zero, which is squared)
+                        const float pb = VOX_FMUL(cz, M.m[r][2]);
+                        const bool up = M.m[r][2] >= 0.f;
+                        const float zn = up ? pa[r] : pb, zx = up ? pb : pa[r];
+                        pa[r] = pb;
+                        const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
+                        // xl <= xh: the bound of the row's interval nearest to zero, or zero
+                        const float xs = VOX_FADD(fmaxf(xl, 0.f), fminf(xh, 0.f));
+                        const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
+                        d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
+                    }
+                    mk |= (d2 > 0.f ? 1u : 0u) << k;
+                }
+                return mk;
+            };
+            if constexpr (APPROX)
             {
-                v = VOX_FADD(v, 1.f);
-                cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-                float d2 = 1.f;
+                // the reference's scaled bounds of voxel 0 of the run, the scaled z step
+                const float v0 = (float)(o[2] + rz0);
+                const float cz0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz);
+                const float cz1 = VOX_FSUB(VOX_FMUL(VOX_FADD(v0, 1.f), vsf), pz);
+                float sl[3], sh[3], st[3], Dl = 0.f;
 #pragma unroll
                 for (int r = 0; r < 3; r++)
                 {
-                    const float pb = VOX_FMUL(cz, M.m[r][2]);
-                    const float zn = up[r] ? pa[r] : pb, zx = up[r] ? pb : pa[r];
-                    pa[r] = pb;
-                    const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
-                    // xl <= xh: the bound of the row's interval nearest to zero, or zero
-                    const float xs = VOX_FADD(fmaxf(xl, 0.f), fminf(xh, 0.f));
-                    const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
-                    d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
+                    float zn, zx;
+                    minmax_prod(cz0, cz1, M.m[r][2], zn, zx);
+                    sl[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(slo[r], zn), il), is[r]);
+                    sh[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(shi[r], zx), il), is[r]);
+                    st[r] = C.zst[r][j];
+                    Dl += 2.f * C.dab[r][j] + 0x1p-20f * (fabsf(sl[r]) + fabsf(sh[r]) + 8.f * fabsf(st[r]));
                 }
-                zmask |= (d2 > 0.f ? 1u : 0u) << k;
+                Dl *= 1.f + 0x1p-20f;
+                uint32_t unc = (1u << nz) - 1u;
+                if (Dl <= 0.0625f) // false for NaN
+                {
+                    const float Mg = 4.f * Dl + 0x1p-18f;
+                    const float lo_t = 1.f - Mg, hi_t = 1.f + Mg;
+                    unc = 0;
+#pragma unroll 2
+                    for (uint32_t k = 0; k < nz; k++)
+                    {
+                        const float kf = (float)k;
+                        float D = 0.f;
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+                        {
+                            const float a = __fmaf_rn(kf, st[r], sl[r]), b = __fmaf_rn(kf, st[r], sh[r]);
+                            const float xs = fmaxf(a, fminf(b, 0.f));
+                            D = __fmaf_rn(xs, xs, D);
+                        }
+                        zmask |= (D < lo_t ? 1u : 0u) << k;
+                        unc |= (!(D < lo_t) && !(D > hi_t) ? 1u : 0u) << k;
+                    }
+                }
+                // the reference test of one voxel, from the record (nothing of the column kept live)
+                auto exact_voxel = [&](uint32_t k) -> uint32_t {
+                    const Aabb b = voxel_local_aabb(R, rinv_of(R), vsf, o[0] + rx, o[1] + ry, o[2] + rz0 + (int32_t)k);
+                    return aabb_hits_unit_sphere(b) ? 1u << k : 0u;
+                };
+                for (uint32_t m = unc; m; m &= m - 1u)
+                    zmask |= exact_voxel((uint32_t)(__ffs(m) - 1));
+                if (CHECK)
+                {
+                    uint32_t ex = 0;
+                    for (uint32_t k = 0; k < nz; k++)
+                        ex |= exact_voxel(k);
+                    if (ex != zmask)
+                        atomicOr(P.err, ERR_BOUNDS); // a linear classification differs from the reference test
+                }
             }
+            else
+                zmask = exact_run(0, nz);
             ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
             if (CHECK && zmask && C.flag[j])
                 atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
@@ -502,6 +605,23 @@ __device__ __forceinline__ void leaf_box_fields(Chunk& C, int j, const GaussRec&
     C.bcol[j] = empty ? 0u : (uint32_t)(x1 - x0 + 1) * ny;
 }
 
+// all stagers (lanes 0 .. LQ_CHUNK - 1 of the last warp), once the boxes of the
+// chunk's cnt Gaussians are placed: the chunk's column prefix
+__device__ __forceinline__ void leaf_stage_prefix(LeafChunk& C, int js, uint32_t cnt)
+{
+    uint32_t b = js < (int)cnt ? C.bcol[js] : 0u;
+#pragma unroll
+    for (int off = 1; off < LQ_CHUNK; off <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync((1u << LQ_CHUNK) - 1u, b, off);
+        if (js >= off)
+            b += y;
+    }
+    C.cstart[js + 1] = b;
+    if (js == 0)
+        C.cstart[0] = 0;
+}
+
 __device__ __forceinline__ void cp_async16(void* dst, const void* src)
 {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
@@ -534,6 +654,10 @@ __device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChun
     C.rgb24[j] = rgba8_byte(R.q7.x) | (rgba8_byte(R.q7.y) << 8) | (rgba8_byte(R.q7.z) << 16);
     C.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
     aabb_difference_bound(R, C.vs[j], o, C.dab[0][j], C.dab[1][j], C.dab[2][j]);
+    const RInv M = rinv_of(R);
+    C.zst[0][j] = VOX_FMUL(VOX_FMUL(VOX_FMUL(C.vs[j], M.m[0][2]), R.q0.w), R.q3.y);
+    C.zst[1][j] = VOX_FMUL(VOX_FMUL(VOX_FMUL(C.vs[j], M.m[1][2]), R.q0.w), R.q3.z);
+    C.zst[2][j] = VOX_FMUL(VOX_FMUL(VOX_FMUL(C.vs[j], M.m[2][2]), R.q0.w), R.q3.w);
     C.flag[j] = CHECK ? P.emit_flag[P.vals[q]] : 0;
     if (WINDOW)
     {
@@ -590,11 +714,16 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
     uint32_t pre_q0 = 0, pre_p1 = 0, cn2 = 0;
     bool cn_fresh = true;
     uint32_t tq0 = P.cand_start[tc], tp1 = P.cand_start[tc + 1];
-    if (stager && js < (int)min((uint32_t)LQ_CHUNK, tp1 - tq0))
+    if (stager)
     {
-        const uint32_t g = leaf_stage_issue(P, &S.ch[0].rec[js].r, tq0 + (uint32_t)js);
-        cp_async_wait_all();
-        leaf_stage_box<CHECK, WINDOW>(P, S.ch[0], js, tq0 + (uint32_t)js, g, to);
+        const uint32_t c0 = min((uint32_t)LQ_CHUNK, tp1 - tq0);
+        if (js < (int)c0)
+        {
+            const uint32_t g = leaf_stage_issue(P, &S.ch[0].rec[js].r, tq0 + (uint32_t)js);
+            cp_async_wait_all();
+            leaf_stage_box<CHECK, WINDOW>(P, S.ch[0], js, tq0 + (uint32_t)js, g, to);
+        }
+        leaf_stage_prefix(S.ch[0], js, c0);
     }
     __syncthreads();
     bool t_valid = true, a_valid = false, f_valid = false, a_leaf_end = false;
@@ -736,7 +865,7 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
         }
         // ---- test of this chunk
         if (t_valid)
-            leaf_test_chunk<CHECK>(P, S.ch[tb], min((uint32_t)LQ_CHUNK, tp1 - tq0), to, S.queue[i & 1u], &S.qn[tb], t,
+            leaf_test_chunk<CHECK, false, true>(P, S.ch[tb], min((uint32_t)LQ_CHUNK, tp1 - tq0), to, S.queue[i & 1u], &S.qn[tb], t,
                                    lane);
         // the counter the test of phase i + 1 fills: last read by the alpha of phase i - 1
         if (t == 0)
@@ -756,6 +885,7 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
                 cp_async_wait_all();
                 leaf_stage_box<CHECK, WINDOW>(P, S.ch[nb], js, nq0 + (uint32_t)js, ng, no);
             }
+            leaf_stage_prefix(S.ch[nb], js, ncnt);
             if (js == 0)
             {
                 const int pp = (int)(i & 1u);

@@ -429,11 +429,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_onesweep(const K* __restrict__ 
         uint32_t peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = __popc(peers & lt);
         uint32_t leader = __ffs(peers) - 1;
-        uint32_t prev = valid ? S.warp_hist[warp][d] : 0u;
-        __syncwarp();
+        // the group's leader reserves its slots; the others take its old count
+        uint32_t prev = 0u;
         if (valid && (uint32_t)lane == leader)
-            S.warp_hist[warp][d] = prev + __popc(peers);
-        __syncwarp();
+            prev = atomicAdd(&S.warp_hist[warp][d], (uint32_t)__popc(peers));
+        prev = __shfl_sync(0xffffffffu, prev, (int)leader);
         rank[i] = prev + before;
     }
     __syncthreads();

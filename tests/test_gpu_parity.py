@@ -145,6 +145,11 @@ def test_leaf_bound_never_skips_a_passing_voxel(oracle_mod):
         needles = W.plain_cloud(5000, 15)
         needles["scales"][:, 2] *= 20.0
         clouds.append((needles, 0.01))
+        # the 2M-Gaussian / 64-cluster cloud at vs 0.002 (about 1.6e9 pairs): the
+        # check also runs the reference test on every voxel the linear
+        # classification decided and on every pair's RGBA8 byte decided from the
+        # float channel's alpha
+        clouds.append((W.cluster_cloud(2_000_000, 1, clusters=64), 0.002))
         for cloud, vs in clouds:
             g = ctx.voxelize_host(cloud["means"], cloud["quats"], cloud["scales"], cloud["opacities"], cloud["colors"], vs)
             assert g.counts["pairs"] > 0
