@@ -451,47 +451,138 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
     return alpha_of_d2(R, lattice_min_d2(b));
 }
 
-// Stable local AABB of voxel (i, j, k) for the float channels: corner offsets
-// fma(v, vs, -mu) rounded once; per row the lower / upper corner of each axis
-// picked by the sign of the matrix entry (the products' minimum / maximum),
-// lo = fl(fma(cz, m_z, fma(cx, m_x, fl(cy m_y))) * fl(inv_ls * inv_s)).
-__device__ __forceinline__ Aabb stable_local_aabb(const GaussRec& R, const RInv& M, float vs, int32_t i, int32_t j,
-                                                  int32_t k)
+// Per (leaf, Gaussian) constants of the leaf walk, computed once when a chunk
+// is staged (leaf_pair_consts).
+//
+// The float channels' local AABB is anchored at one voxel of the leaf: c =
+// o + r0, r0_a = clamp(bmin_a + (range_a >> 1) - o_a, 0, 7) (the leaf voxel
+// nearest the centre voxel of the Gaussian's bbox, integer arithmetic).  With d0_a = fma(c_a, vs, -mu_a) (the anchor's
+// corner offset, rounded once, so the low bits of mu survive far from the
+// origin), k_r = fl(inv_ls inv_s_r) and the scaled voxel steps A_ra =
+// fl(fl(vs m_ra) k_r), row r of voxel o + (rx, ry, rz), t_a = r_a - r0_a, is
+//   base_r = fl(fl(fma(m_r2, d0_2, fma(m_r0, d0_0, fl(m_r1 d0_1)))) k_r)
+//   lo0_r  = fl(fl(fl(base_r + min(A_r0, 0)) + min(A_r1, 0)) + min(A_r2, 0))
+//   W_r    = fl(fl(|A_r0| + |A_r1|) + |A_r2|)
+//   lo_r   = fma(t_z, A_r2, fma(t_y, A_r1, fma(t_x, A_r0, lo0_r))),  hi_r = fl(lo_r + W_r)
+// (the lower corner of each axis is the one picked by the sign of the step).
+// Every rounding is relative to the local magnitudes E_a = |d0_a| + 8 vs
+// (|t| <= 7), and near the centre the anchor's offsets are about a voxel, so
+// the form is about as accurate as one rounding of each corner offset; a pair
+// costs three fma and one add per row.  The oracle's frag_alpha_f evaluates the same operations in
+// the same order.
+//
+// dab_r bounds how far the reference's local AABB (voxel_local_aabb) and this
+// one can differ in the leaf, apart from the per-pair 2^-20 B_r term added in
+// alpha_byte_bound: per axis the reference's corner offset fl(fl(v vs) -
+// mu) is within 0.5 ulp(W) + 0.5 ulp(Cm) of exact (W, Cm: the largest |v vs|
+// and |v vs - mu| over the leaf's corners), its products and two sums add at
+// most 3 2^-24 sum_a |m_ra| Cm_a <= 2^-21 sum_a |m_ra| Cm_a; this form's d0
+// rounding adds 0.5 ulp(E_a), its other roundings (the chain 3, k and base 2,
+// the steps' 3 times |t| <= 7 with 8 vs <= E, lo0 3, the per-voxel fma 3, W and
+// the hi sum about 1.3, in units of 2^-24 sum_a |m_ra| E_a) at most
+// 2^-20 sum_a |m_ra| E_a; all scaled by il is_r.  The linear z classification of the leaf test (leaf_test_chunk)
+// needs only the reference's z terms: dz_r = il is_r |m_r2| (0.5 ulp(W_z) +
+// 0.5 ulp(Cm_z) + 2^-21 Cm_z), and the leaf's largest scaled bound magnitude
+// Bl_r = il is_r sum_a |m_ra| Cm_a; from them its thresholds lo_t / hi_t.
+struct LeafPairConst
 {
-    const int32_t v[3] = { i, j, k };
+    float lo0[3], W[3]; // per row: the scaled lower bound of the anchor voxel, the scaled voxel width
+    float A[3][3];      // A[r][a]: the scaled step of one voxel along axis a
+    float dab[3];       // per row: the reference / float-channel AABB difference bound
+    float lo_t, hi_t;   // the linear z classification: certain pass below lo_t, certain fail above hi_t
+    uint32_t r0;        // the anchor voxel in the leaf: r0_x | r0_y << 8 | r0_z << 16
+};
+
+// the anchor of the float channels' AABB along one axis (leaf origin o)
+// (bbox minimum bmin, extent range = max + 1 - min)
+__host__ __device__ __forceinline__ int32_t anchor_of(int32_t bmin, int32_t range, int32_t o)
+{
+    const int32_t r = bmin + (range >> 1) - o;
+    return r < 0 ? 0 : r > 7 ? 7 : r;
+}
+
+// unit in the last place of |x| (a float), 0 for 0
+__device__ __forceinline__ float ulp_of(float x)
+{
+    return __uint_as_float(__float_as_uint(fabsf(x)) & 0x7f800000u) * 0x1p-23f;
+}
+
+__device__ __forceinline__ LeafPairConst leaf_pair_consts(const GaussRec& R, float vs, const int32_t o[3])
+{
+    LeafPairConst c;
     const float mu[3] = { R.q0.x, R.q0.y, R.q0.z };
-    const float inv_s[3] = { R.q3.y, R.q3.z, R.q3.w };
-    float c0[3], c1[3];
+    const float il = R.q0.w;
+    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+    const RInv M = rinv_of(R);
+    float d0[3], Gr[3], G[3], Cm[3];
+    c.r0 = 0;
 #pragma unroll
     for (int a = 0; a < 3; a++)
     {
-        const float vf = (float)v[a];
-        c0[a] = VOX_FFMA(vf, vs, -mu[a]);
-        c1[a] = VOX_FFMA(VOX_FADD(vf, 1.f), vs, -mu[a]);
+        const int32_t r0 = anchor_of((&R.q4.x)[a], (&R.q5.x)[a], o[a]);
+        c.r0 |= (uint32_t)r0 << (8 * a);
+        d0[a] = VOX_FFMA((float)(o[a] + r0), vs, -mu[a]);
+        const float w0 = (float)o[a] * vs, w1 = (float)(o[a] + 8) * vs;
+        const float W = fmaxf(fabsf(w0), fabsf(w1)) * (1.f + 0x1p-20f);
+        Cm[a] = fmaxf(fabsf(w0 - mu[a]), fabsf(w1 - mu[a])) * (1.f + 0x1p-20f);
+        Gr[a] = 0.5f * ulp_of(W) + 0.5f * ulp_of(Cm[a]) + 0x1p-21f * Cm[a];
+        const float E = (fabsf(d0[a]) + 8.f * vs) * (1.f + 0x1p-20f);
+        G[a] = Gr[a] + 0.5f * ulp_of(E) + 0x1p-20f * E;
     }
+    float Dl = 0.f;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+    {
+        const float k = VOX_FMUL(il, is[r]);
+        const float base =
+            VOX_FMUL(VOX_FFMA(M.m[r][2], d0[2], VOX_FFMA(M.m[r][0], d0[0], VOX_FMUL(M.m[r][1], d0[1]))), k);
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+            c.A[r][a] = VOX_FMUL(VOX_FMUL(vs, M.m[r][a]), k);
+        c.lo0[r] = VOX_FADD(VOX_FADD(VOX_FADD(base, fminf(c.A[r][0], 0.f)), fminf(c.A[r][1], 0.f)),
+                            fminf(c.A[r][2], 0.f));
+        c.W[r] = VOX_FADD(VOX_FADD(fabsf(c.A[r][0]), fabsf(c.A[r][1])), fabsf(c.A[r][2]));
+        const float s = (1.f + 0x1p-20f) * il * is[r];
+        const float m0 = fabsf(M.m[r][0]), m1 = fabsf(M.m[r][1]), m2 = fabsf(M.m[r][2]);
+        c.dab[r] = s * (m0 * G[0] + m1 * G[1] + m2 * G[2]);
+        const float dz = s * m2 * Gr[2];
+        const float Bl = s * (m0 * Cm[0] + m1 * Cm[1] + m2 * Cm[2]);
+        Dl += 2.f * dz + 0x1p-20f * (2.f * Bl + 8.f * fabsf(c.A[r][2]));
+    }
+    Dl *= 1.f + 0x1p-20f;
+    if (Dl <= 0.0625f) // false for NaN
+    {
+        c.lo_t = 1.f - (2.f * Dl + 0x1p-19f);
+        c.hi_t = 1.f + (2.f * Dl + Dl * Dl + 0x1p-18f);
+    }
+    else
+    {
+        c.lo_t = -1.f; // every voxel takes the reference test
+        c.hi_t = __int_as_float(0x7f800000);
+    }
+    return c;
+}
+
+// the float channels' local AABB of voxel o + (rx, ry, rz) from the leaf's constants (r0: the packed anchor)
+__device__ __forceinline__ Aabb stable_leaf_aabb(const float lo0[3], const float W[3], const float A[3][3], uint32_t r0,
+                                                 int32_t rx, int32_t ry, int32_t rz)
+{
+    const float fx = (float)(rx - (int32_t)(r0 & 255u)), fy = (float)(ry - (int32_t)((r0 >> 8) & 255u)),
+                fz = (float)(rz - (int32_t)(r0 >> 16));
     Aabb b;
 #pragma unroll
     for (int r = 0; r < 3; r++)
     {
-        float cl[3], ch[3];
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-        {
-            cl[a] = M.m[r][a] >= 0.f ? c0[a] : c1[a];
-            ch[a] = M.m[r][a] >= 0.f ? c1[a] : c0[a];
-        }
-        const float k = VOX_FMUL(R.q0.w, inv_s[r]);
-        b.lo[r] = VOX_FMUL(VOX_FFMA(cl[2], M.m[r][2], VOX_FFMA(cl[0], M.m[r][0], VOX_FMUL(cl[1], M.m[r][1]))), k);
-        b.hi[r] = VOX_FMUL(VOX_FFMA(ch[2], M.m[r][2], VOX_FFMA(ch[0], M.m[r][0], VOX_FMUL(ch[1], M.m[r][1]))), k);
+        b.lo[r] = VOX_FFMA(fz, A[r][2], VOX_FFMA(fy, A[r][1], VOX_FFMA(fx, A[r][0], lo0[r])));
+        b.hi[r] = VOX_FADD(b.lo[r], W[r]);
     }
     return b;
 }
 
-// Alpha of the float density / colour channels from the stable local AABB
-// (corner offsets fma(v, vs, -mu), sign-picked corners summed with fma): the
-// lattice points lo + w (hi - lo), float exp / pow.  The oracle's
+// Alpha of the float density / colour channels from their local AABB
+// (stable_leaf_aabb): the lattice points lo + w (hi - lo), float exp / pow.  The oracle's
 // frag_alpha_f evaluates the same operations in the same order.  Also keeps
-// what alpha_byte_from_stable needs: the lattice minimum d, op exp(-ls d) and
+// what alpha_byte_bound needs: the lattice minimum d, op exp(-ls d) and
 // the largest bound magnitude per axis.
 struct AlphaF
 {
@@ -529,67 +620,24 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
     return pair_alpha_f_ex(R, b).a1;
 }
 
-// unit in the last place of |x| (a float), 0 for 0
-__device__ __forceinline__ float ulp_of(float x)
-{
-    return __uint_as_float(__float_as_uint(fabsf(x)) & 0x7f800000u) * 0x1p-23f;
-}
-
-// How far the reference's local AABB of a voxel (voxel_local_aabb: corner
-// offsets fl(fl(v vs) - mu), products, sums, the two scalings) and the stable
-// one (stable_local_aabb: fma(v, vs, -mu), an fma chain, one scaling) can
-// differ, per row, for any voxel of the leaf at o, apart from a term
-// proportional to the bound itself.  Per axis k the two corner offsets differ
-// by at most E_k = ulp(max |v vs|) / 2 + ulp(max |c|) over the leaf's corner
-// coordinates v in [o, o + 8] (one rounding of v vs, one of the difference in
-// each evaluation); the products, sums and fma roundings of both add at most
-// 6 2^-24 sum_k |m_rk| |c_k| <= 2^-21 sum_k |m_rk| C_k; the row's distance is
-// then scaled by il is_r.  The scalings' and lattice points' roundings are
-// proportional to the bound magnitude B_r and are added per pair
-// (alpha_byte_from_stable).  Computed once per (leaf, Gaussian) pair.
-__device__ __forceinline__ void aabb_difference_bound(const GaussRec& R, float vs, const int32_t o[3], float& d0,
-                                                      float& d1, float& d2)
-{
-    const float mu[3] = { R.q0.x, R.q0.y, R.q0.z };
-    const RInv M = rinv_of(R);
-    float G[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-    {
-        const float w0 = (float)o[k] * vs, w1 = (float)(o[k] + 8) * vs;
-        const float W = fmaxf(fabsf(w0), fabsf(w1)) * (1.f + 0x1p-20f);
-        const float Cm = fmaxf(fabsf(w0 - mu[k]), fabsf(w1 - mu[k])) * (1.f + 0x1p-20f);
-        G[k] = 0.5f * ulp_of(W) + ulp_of(Cm) + 0x1p-21f * Cm;
-    }
-    const float il = R.q0.w;
-    const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
-    float d[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-        d[r] = (1.f + 0x1p-20f) * il * is[r] *
-               (fabsf(M.m[r][0]) * G[0] + fabsf(M.m[r][1]) * G[1] + fabsf(M.m[r][2]) * G[2]);
-    d0 = d[0];
-    d1 = d[1];
-    d2 = d[2];
-}
 
 // The RGBA8 alpha byte of a passing pair, rgba8_byte(pair_alpha(R, b_ref))
 // with b_ref = voxel_local_aabb(...), decided where possible from the float
-// channel's alpha f (same formula, evaluated from the stable local AABB).
+// channel's alpha f (same formula, evaluated from stable_leaf_aabb).
 // Per row the two AABBs' bounds differ by at most D_r = dab_r + 2^-20 B_r
-// (aabb_difference_bound, plus the scalings' and lattice points' roundings),
+// (leaf_pair_consts, plus the scalings' and lattice points' roundings),
 // so their lattice minima d differ by at most md = sum_r (2 B'_r D_r + D_r^2 +
 // 2^-22 B'_r^2) + 2^-21 d (B' = B + D; squares and sums rounded), and the
 // alpha a' = 1 - (1 - op e^-ls d)^e, whose slope in d is at most
 // e ls a_hi (times 1 / (1 - a_hi) when e < 1) for a_hi >= op e^-ls (d - md),
 // by at most that slope times md, plus both evaluations' own error (a few ulp
 // of the exp and pow: 4e-6 (1 + e) bounds it).  When a' +- that margin falls
-// in one byte (rgba8_byte is monotone) the byte is the reference's; else the
-// reference's evaluation runs.  VOX_CHECK_EMIT=1 compares every decided byte
-// with the reference's evaluation.
-__device__ __forceinline__ uint32_t alpha_byte_from_stable(const GaussRec& R, const RInv& M, float vs, int32_t i,
-                                                           int32_t j, int32_t k, const AlphaF& f, const float dab[3],
-                                                           bool& decided)
+// in one byte (rgba8_byte is monotone) the byte is the reference's and
+// decided is set; otherwise the caller runs the reference's evaluation
+// (ref_alpha_byte).  VOX_CHECK_EMIT=1 compares every decided byte with the
+// reference's evaluation.
+__device__ __forceinline__ uint32_t alpha_byte_bound(const GaussRec& R, const AlphaF& f, const float dab[3],
+                                                     bool& decided)
 {
     decided = true;
     if (R.q7.w != 0.f)
@@ -620,7 +668,13 @@ __device__ __forceinline__ uint32_t alpha_byte_from_stable(const GaussRec& R, co
         }
     }
     decided = false;
-    return rgba8_byte(pair_alpha(R, voxel_local_aabb(R, M, vs, i, j, k)));
+    return 0u;
+}
+
+// the reference's RGBA8 alpha byte of voxel (i, j, k) and the record's Gaussian
+__device__ __forceinline__ uint32_t ref_alpha_byte(const GaussRec& R, float vs, int32_t i, int32_t j, int32_t k)
+{
+    return rgba8_byte(pair_alpha(R, voxel_local_aabb(R, rinv_of(R), vs, i, j, k)));
 }
 
 // Differentiable channels (VOX_FLAG_DIFFERENTIABLE).  The reference alpha

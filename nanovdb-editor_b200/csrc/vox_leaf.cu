@@ -333,8 +333,12 @@ struct LeafChunk
     uint32_t bcol[LQ_CHUNK];                             // box columns, nx * ny (0: empty box)
     uint32_t rgb24[LQ_CHUNK];                            // the colour bytes of the packed RGBA8 value
     float vs[LQ_CHUNK];
-    float dab[3][LQ_CHUNK]; // per row: how far the two local-AABB evaluations can differ in this leaf
-    float zst[3][LQ_CHUNK]; // per row: the scaled z step fl(vs m_r2 il is_r)
+    // leaf_pair_consts of each (leaf, Gaussian), by row
+    float lo0[3][LQ_CHUNK], wid[3][LQ_CHUNK]; // the float channels' AABB of the leaf's voxel (0, 0, 0)
+    float stp[3][3][LQ_CHUNK];                 // [r][a]: the scaled voxel steps ([r][2]: the z step of the test)
+    float dab[3][LQ_CHUNK];                    // reference / float-channel AABB difference bound
+    float lo_t[LQ_CHUNK], hi_t[LQ_CHUNK];      // the linear z classification's thresholds
+    uint32_t anchor[LQ_CHUNK];                 // the float channels' anchor voxel (packed)
     uint32_t cstart[16];    // first column of box j (boxes past the chunk's count: empty); [LQ_CHUNK]: all
     uint8_t flag[LQ_CHUNK];
     uint64_t wf0[LQ_CHUNK], wbase[LQ_CHUNK]; // reference windows: fragment offset in its batch, windows before
@@ -354,6 +358,7 @@ struct LeafQSmem
     LeafChunk ch[3];
     LeafAcc acc[1];
     uint16_t queue[2][LQ_CHUNK * 512];
+    uint16_t defer[LP_THREADS / 32][64]; // per warp: queued pairs whose RGBA8 byte the bound left open
     uint32_t qn[3];
     int32_t nxt_o[2][3]; // the next chunk (by phase parity): leaf origin and sorted pair range
     uint32_t nxt_q0[2], nxt_p1[2];
@@ -374,25 +379,28 @@ struct LeafQSmem
 // tests at most 2 x 32 columns of 8 voxels).  Otherwise one shared queue, a
 // shared atomic per warp and round.
 //
-// APPROX (the chunk carries dab and zst): each voxel of the column is first
-// classified from bounds linear in k - the reference's scaled bounds of the
-// column's first voxel, sl / sh, plus k times the scaled z step st = fl(vs
-// m_r2 il is_r) - and only voxels near the sphere run the reference test.
-// Per row, the reference's bound of voxel k and the linear one both lie
-// within dab_r + 2^-21 |bound| of the exact-arithmetic bound (corner offsets,
-// products and sums as in aabb_difference_bound; the sum and two scalings
-// relative), the step's three roundings times k <= 8 and the fma's own
-// rounding add at most 2^-20 (|sl| + |sh| + 8 |st|) in all, so the selected
-// values (max(lo, min(hi, 0)), 1-Lipschitz in both bounds) differ by at most
-// delta_r = 2 dab_r + 2^-20 (|sl| + |sh| + 8 |st|), and the vectors of the
-// three by at most Delta = sum delta_r in norm.  The reference passes a
-// voxel when its fl-evaluated 1 - S > 0, surely if S < 1 - 2^-22 and surely
-// not if S > 1 + 2^-20 (six roundings of values below 2 S + 1); with D the
-// fma-summed squares of the linear values (relative error <= 2^-21) and
-// Delta <= 1/16, D < 1 - Mg implies the first and D > 1 + Mg the second for
-// Mg = 4 Delta + 2^-18.  Voxels with D in [1 - Mg, 1 + Mg] (or NaN), and every
-// voxel of a column with Delta > 1/16, take the reference test.  In CHECK
-// mode every voxel also takes it and a difference sets ERR_BOUNDS.
+// APPROX (a LeafChunk, carrying the leaf_pair_consts of each Gaussian): each
+// voxel of the column is first classified from bounds linear in k - the
+// reference's scaled bounds of the column's first voxel, sl / sh, plus k times
+// the scaled z step st = fl(fl(vs m_r2) fl(il is_r)) - and only voxels near the
+// sphere run the reference test.  Per row, the reference's bound of voxel k
+// differs from the exact-arithmetic one by at most dz_r + 2^-22 Bl_r (the z
+// corner offset, product and sum roundings; the x + y share is common to both;
+// the sum and two scalings relative), and so does sl; the step's three
+// roundings times k <= 8 and the fma's rounding add at most 2^-21 (Bl_r +
+// 8 |st_r|).  The selected values (max(lo, min(hi, 0)), 1-Lipschitz in both
+// bounds) therefore differ by at most delta_r = 2 dz_r + 2^-20 (2 Bl_r +
+// 8 |st_r|), and the vectors of the three by eta <= Delta = sum delta_r in
+// norm.  The reference passes a voxel when its fl-evaluated 1 - S > 0: surely
+// if S < 1 - 2^-22 (three subtractions and squares of values below 1) and
+// surely not if S > 1 + 2^-20.  With D the fma-summed squares of the linear
+// values (relative error <= 3 2^-24) and Delta <= 1/16, (sqrt(D) + eta)^2 <
+// 1 - 2^-22 holds when D < lo_t = 1 - (2 Delta + 2^-19), and (sqrt(D) - eta)^2
+// > 1 + 2^-20 when D > hi_t = 1 + (2 Delta + Delta^2 + 2^-18) (the slack
+// covers the roundings of the thresholds themselves).  Voxels with D in
+// [lo_t, hi_t] (or NaN), and every voxel of a (leaf, Gaussian) with Delta >
+// 1/16 (lo_t = -1, hi_t = inf), take the reference test.  In CHECK mode every
+// voxel also takes it and a difference sets ERR_BOUNDS.
 template <bool CHECK, bool PER_WARP = false, bool APPROX = false, class Chunk>
 __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const Chunk& C, uint32_t cnt,
                                                 const int32_t o[3], uint16_t* queue, uint32_t* qcount, int t, int lane)
@@ -502,7 +510,7 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
                 const float v0 = (float)(o[2] + rz0);
                 const float cz0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz);
                 const float cz1 = VOX_FSUB(VOX_FMUL(VOX_FADD(v0, 1.f), vsf), pz);
-                float sl[3], sh[3], st[3], Dl = 0.f;
+                float sl[3], sh[3], st[3];
 #pragma unroll
                 for (int r = 0; r < 3; r++)
                 {
@@ -510,20 +518,15 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
                     minmax_prod(cz0, cz1, M.m[r][2], zn, zx);
                     sl[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(slo[r], zn), il), is[r]);
                     sh[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(shi[r], zx), il), is[r]);
-                    st[r] = C.zst[r][j];
-                    Dl += 2.f * C.dab[r][j] + 0x1p-20f * (fabsf(sl[r]) + fabsf(sh[r]) + 8.f * fabsf(st[r]));
+                    st[r] = C.stp[r][2][j];
                 }
-                Dl *= 1.f + 0x1p-20f;
-                uint32_t unc = (1u << nz) - 1u;
-                if (Dl <= 0.0625f) // false for NaN
+                const float lo_t = C.lo_t[j], hi_t = C.hi_t[j];
+                uint32_t unc = 0;
                 {
-                    const float Mg = 4.f * Dl + 0x1p-18f;
-                    const float lo_t = 1.f - Mg, hi_t = 1.f + Mg;
-                    unc = 0;
+                    float kf = 0.f;
 #pragma unroll 2
-                    for (uint32_t k = 0; k < nz; k++)
+                    for (uint32_t k = 0; k < nz; k++, kf += 1.f)
                     {
-                        const float kf = (float)k;
                         float D = 0.f;
 #pragma unroll
                         for (int r = 0; r < 3; r++)
@@ -653,11 +656,20 @@ __device__ __forceinline__ void leaf_stage_box(const LeafPassParams& P, LeafChun
     leaf_box_fields(C, j, R, o);
     C.rgb24[j] = rgba8_byte(R.q7.x) | (rgba8_byte(R.q7.y) << 8) | (rgba8_byte(R.q7.z) << 16);
     C.vs[j] = rec_vs(R, P.voxel_size, P.cloud_vs);
-    aabb_difference_bound(R, C.vs[j], o, C.dab[0][j], C.dab[1][j], C.dab[2][j]);
-    const RInv M = rinv_of(R);
-    C.zst[0][j] = VOX_FMUL(VOX_FMUL(VOX_FMUL(C.vs[j], M.m[0][2]), R.q0.w), R.q3.y);
-    C.zst[1][j] = VOX_FMUL(VOX_FMUL(VOX_FMUL(C.vs[j], M.m[1][2]), R.q0.w), R.q3.z);
-    C.zst[2][j] = VOX_FMUL(VOX_FMUL(VOX_FMUL(C.vs[j], M.m[2][2]), R.q0.w), R.q3.w);
+    const LeafPairConst K = leaf_pair_consts(R, C.vs[j], o);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+    {
+        C.lo0[r][j] = K.lo0[r];
+        C.wid[r][j] = K.W[r];
+        C.dab[r][j] = K.dab[r];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+            C.stp[r][a][j] = K.A[r][a];
+    }
+    C.lo_t[j] = K.lo_t;
+    C.hi_t[j] = K.hi_t;
+    C.anchor[j] = K.r0;
     C.flag[j] = CHECK ? P.emit_flag[P.vals[q]] : 0;
     if (WINDOW)
     {
@@ -814,53 +826,109 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
             }
             __syncthreads(); // the next leaf's alpha reuses the accumulators
         }
-        // ---- alpha of the previous chunk, one queued pair per thread
+        // ---- alpha of the previous chunk, one queued pair per thread.  A pair
+        // whose RGBA8 byte the bound leaves open (a few percent) is deferred to
+        // its warp's list and the reference's byte is evaluated 32 pairs at a
+        // time, so the rare branch costs one converged pass per 32 pairs.
         if (a_valid)
         {
             const LeafChunk& C = S.ch[ab];
             LeafAcc& A = S.acc[0];
             const uint16_t* queue = S.queue[(i + 1u) & 1u];
             const uint32_t qn = S.qn[ab];
-            for (uint32_t e = (uint32_t)t; e < qn; e += LP_THREADS)
-            {
-                const uint32_t q = queue[e];
+            uint16_t* dq = S.defer[warp];
+            uint32_t dn = 0; // this warp's deferred pairs (warp-uniform)
+            auto ref_byte = [&](uint32_t q) {
                 const uint32_t j = q >> 9, n = q & 511u;
                 const GaussRec& R = C.rec[j].r;
-                const RInv M = rinv_of(R);
-                const float vsf = C.vs[j];
-                const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7), zz = ao[2] + (int32_t)(n & 7);
-                float a;
-                uint32_t a8;
-                if (P.smooth)
-                {
-                    SmoothTerms st;
-                    a = smooth_kernel(R, M, vsf, x, yy, zz, st);
-                    a8 = rgba8_byte(pair_alpha(R, voxel_local_aabb(R, M, vsf, x, yy, zz)));
-                }
-                else
-                {
-                    const AlphaF af = pair_alpha_f_ex(R, stable_local_aabb(R, M, vsf, x, yy, zz));
-                    a = af.a1;
-                    bool decided;
-                    const float dab[3] = { C.dab[0][j], C.dab[1][j], C.dab[2][j] };
-                    a8 = alpha_byte_from_stable(R, M, vsf, x, yy, zz, af, dab, decided);
-                    if (CHECK && decided && a8 != rgba8_byte(pair_alpha(R, voxel_local_aabb(R, M, vsf, x, yy, zz))))
-                        atomicOr(P.err, ERR_BOUNDS); // the margin failed to cover the reference's byte
-                }
-                atomicAdd(&A.cnt[n], 1u);
+                const uint32_t a8 = ref_alpha_byte(R, C.vs[j], ao[0] + (int32_t)(n >> 6),
+                                                   ao[1] + (int32_t)((n >> 3) & 7u), ao[2] + (int32_t)(n & 7u));
                 atomicMax(&A.rgba[n], (a8 << 24) | C.rgb24[j]);
-                atomicAdd(&A.dens[n], fx_of_unit(a));
-                atomicAdd(&A.col[0][n], fx_of(VOX_FMUL(a, R.q7.x)));
-                atomicAdd(&A.col[1][n], fx_of(VOX_FMUL(a, R.q7.y)));
-                atomicAdd(&A.col[2][n], fx_of(VOX_FMUL(a, R.q7.z)));
-                if (WINDOW)
+            };
+            for (uint32_t e0 = (uint32_t)(t & ~31); e0 < qn; e0 += LP_THREADS) // warp-uniform trip count
+            {
+                const uint32_t e = e0 + (uint32_t)lane;
+                bool defer = false;
+                uint32_t q = 0;
+                if (e < qn)
                 {
-                    // the reference's window of this fragment: x-major index in the bbox
-                    // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
-                    const uint64_t r = (uint64_t)(x - R.q4.x) * (uint64_t)R.q5.y * (uint64_t)R.q5.z +
-                                       (uint64_t)(yy - R.q4.y) * (uint64_t)R.q5.z + (uint64_t)(zz - R.q4.z);
-                    atomicMin(&A.wmin, (unsigned long long)(C.wbase[j] + (C.wf0[j] + r) / REF_WINDOW));
+                    q = queue[e];
+                    const uint32_t j = q >> 9, n = q & 511u;
+                    const GaussRec& R = C.rec[j].r;
+                    const float vsf = C.vs[j];
+                    const int32_t x = ao[0] + (int32_t)(n >> 6), yy = ao[1] + (int32_t)((n >> 3) & 7),
+                                  zz = ao[2] + (int32_t)(n & 7);
+                    float a;
+                    uint32_t a8;
+                    if (P.smooth)
+                    {
+                        SmoothTerms st;
+                        a = smooth_kernel(R, rinv_of(R), vsf, x, yy, zz, st);
+                        a8 = ref_alpha_byte(R, vsf, x, yy, zz);
+                    }
+                    else
+                    {
+                        float lo0[3], wid[3], stp[3][3];
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+                        {
+                            lo0[r] = C.lo0[r][j];
+                            wid[r] = C.wid[r][j];
+#pragma unroll
+                            for (int a = 0; a < 3; a++)
+                                stp[r][a] = C.stp[r][a][j];
+                        }
+                        const AlphaF af = pair_alpha_f_ex(R, stable_leaf_aabb(lo0, wid, stp, C.anchor[j], (int32_t)(n >> 6),
+                                                                              (int32_t)((n >> 3) & 7u), (int32_t)(n & 7u)));
+                        a = af.a1;
+                        bool decided;
+                        const float dab[3] = { C.dab[0][j], C.dab[1][j], C.dab[2][j] };
+                        a8 = alpha_byte_bound(R, af, dab, decided);
+                        defer = !decided;
+                        if (CHECK && decided && a8 != ref_alpha_byte(R, vsf, x, yy, zz))
+                            atomicOr(P.err, ERR_BOUNDS); // the margin failed to cover the reference's byte
+                    }
+                    atomicAdd(&A.cnt[n], 1u);
+                    if (!defer)
+                        atomicMax(&A.rgba[n], (a8 << 24) | C.rgb24[j]);
+                    atomicAdd(&A.dens[n], fx_of_unit(a));
+                    atomicAdd(&A.col[0][n], fx_of(VOX_FMUL(a, R.q7.x)));
+                    atomicAdd(&A.col[1][n], fx_of(VOX_FMUL(a, R.q7.y)));
+                    atomicAdd(&A.col[2][n], fx_of(VOX_FMUL(a, R.q7.z)));
+                    if (WINDOW)
+                    {
+                        // the reference's window of this fragment: x-major index in the bbox
+                        // (gaussian_frag_alloc.slang:55-58) after the Gaussian's batch offset
+                        const uint64_t r = (uint64_t)(x - R.q4.x) * (uint64_t)R.q5.y * (uint64_t)R.q5.z +
+                                           (uint64_t)(yy - R.q4.y) * (uint64_t)R.q5.z + (uint64_t)(zz - R.q4.z);
+                        atomicMin(&A.wmin, (unsigned long long)(C.wbase[j] + (C.wf0[j] + r) / REF_WINDOW));
+                    }
                 }
+                const uint32_t bal = __ballot_sync(0xffffffffu, defer);
+                if (bal)
+                {
+                    if (defer)
+                        dq[dn + (uint32_t)__popc(bal & ((1u << lane) - 1u))] = (uint16_t)q;
+                    dn += (uint32_t)__popc(bal);
+                    if (dn >= 32u) // dn <= 63: a batch of 32, the rest moved to the front
+                    {
+                        __syncwarp();
+                        ref_byte(dq[lane]);
+                        const uint32_t rest = dn - 32u;
+                        const uint16_t mv = (uint32_t)lane < rest ? dq[32 + lane] : (uint16_t)0;
+                        __syncwarp();
+                        if ((uint32_t)lane < rest)
+                            dq[lane] = mv;
+                        __syncwarp();
+                        dn = rest;
+                    }
+                }
+            }
+            if (dn)
+            {
+                __syncwarp();
+                if ((uint32_t)lane < dn)
+                    ref_byte(dq[lane]);
             }
         }
         // ---- test of this chunk

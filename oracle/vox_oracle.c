@@ -302,39 +302,49 @@ static float fx_to_float(int64_t s)
 /* Float density / colour channels (this build's F-mode output; the reference
  * has only RGBA8).  The alpha of gaussian_frag_color.slang:184-217 - local
  * AABB of the voxel, maximum over the 4x4x4 lattice, opacity transform, cull -
- * in a numerically stable float form:
- *   corner offsets fma(v, vs, -mu), rounded once (fl(fl(v vs) - mu) loses
- *     the low bits of mu far from the origin);
- *   per row r the lower / upper corner of each axis picked by the sign of
- *     rinv[r][a] (the products' minimum / maximum), summed with fma:
- *     lo_r = fl(fma(cz, m_z, fma(cx, m_x, fl(cy m_y))) * fl(inv_ls inv_s_r));
+ * in a numerically stable float form, leaf-relative:
+ *   the anchor c = o + r0, o the origin of the voxel's 8^3 leaf, r0_a =
+ *     clamp(bmin_a + ((bmax_a + 1 - bmin_a) >> 1) - o_a, 0, 7) (the leaf voxel
+ *     nearest the bbox's centre voxel); d0_a = fma(c_a, vs, -mu_a), the anchor corner's offset rounded
+ *     once (fl(fl(v vs) - mu) loses the low bits of mu far from the origin);
+ *     k_r = fl(inv_ls inv_s_r);
+ *   per row r the scaled voxel steps A_ra = fl(fl(vs m_ra) k_r), the leaf
+ *     origin's row base_r = fl(fl(fma(m_r2, d0_2, fma(m_r0, d0_0, fl(m_r1 d0_1)))) k_r),
+ *     lo0_r = base_r + min(A_r0, 0) + min(A_r1, 0) + min(A_r2, 0) and
+ *     W_r = |A_r0| + |A_r1| + |A_r2| (sums left to right, rounded);
+ *   for the voxel at r = (rx, ry, rz) in its leaf, t = r - r0: lo_r =
+ *     fma(t_z, A_r2, fma(t_y, A_r1, fma(t_x, A_r0, lo0_r))), hi_r = fl(lo_r + W_r);
  *   lattice points lo + w (hi - lo), w = 0, 1/3, 2/3, 1; the maximum of the
  *     decreasing exp is at the per-axis smallest square;
  *   float exp / pow (vox_expf, vox_powf).
- * The device evaluates the same operations in the same order. */
+ * The device evaluates the same operations in the same order (leaf_pair_consts,
+ * stable_leaf_aabb); the signs of zero sums may differ, which the squares hide. */
 static float frag_alpha_f(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float cull_scale)
 {
     const float inv_ls = VOX_FDIV(1.f, P->ls);
-    float c0[3], c1[3];
+    float d0[3], rel[3];
     for (int a = 0; a < 3; a++)
     {
-        const float v = (float)ijk[a];
-        c0[a] = VOX_FFMA(v, vs, -P->pos[a]);
-        c1[a] = VOX_FFMA(VOX_FADD(v, 1.f), vs, -P->pos[a]);
+        const int32_t o = ijk[a] - (ijk[a] & 7);
+        const int32_t rc = P->bmin[a] + ((P->bmax[a] + 1 - P->bmin[a]) >> 1) - o;
+        const int32_t r0 = rc < 0 ? 0 : rc > 7 ? 7 : rc;
+        d0[a] = VOX_FFMA((float)(o + r0), vs, -P->pos[a]);
+        rel[a] = (float)((ijk[a] & 7) - r0);
     }
     float m[3];
     for (int r = 0; r < 3; r++)
     {
         const float* w = rinv[r];
-        float cl[3], ch[3];
-        for (int a = 0; a < 3; a++)
-        {
-            cl[a] = w[a] >= 0.f ? c0[a] : c1[a];
-            ch[a] = w[a] >= 0.f ? c1[a] : c0[a];
-        }
         const float k = VOX_FMUL(inv_ls, VOX_FDIV(1.f, P->s[r]));
-        const float lo = VOX_FMUL(VOX_FFMA(cl[2], w[2], VOX_FFMA(cl[0], w[0], VOX_FMUL(cl[1], w[1]))), k);
-        const float hi = VOX_FMUL(VOX_FFMA(ch[2], w[2], VOX_FFMA(ch[0], w[0], VOX_FMUL(ch[1], w[1]))), k);
+        const float base = VOX_FMUL(VOX_FFMA(w[2], d0[2], VOX_FFMA(w[0], d0[0], VOX_FMUL(w[1], d0[1]))), k);
+        float A[3];
+        for (int a = 0; a < 3; a++)
+            A[a] = VOX_FMUL(VOX_FMUL(vs, w[a]), k);
+        const float lo0 = VOX_FADD(VOX_FADD(VOX_FADD(base, A[0] < 0.f ? A[0] : 0.f), A[1] < 0.f ? A[1] : 0.f),
+                                   A[2] < 0.f ? A[2] : 0.f);
+        const float W = VOX_FADD(VOX_FADD(fabsf(A[0]), fabsf(A[1])), fabsf(A[2]));
+        const float lo = VOX_FFMA(rel[2], A[2], VOX_FFMA(rel[1], A[1], VOX_FFMA(rel[0], A[0], lo0)));
+        const float hi = VOX_FADD(lo, W);
         const float dd = VOX_FSUB(hi, lo);
         const float p1 = VOX_FFMA(dd, 0x1.555556p-2f, lo), p2 = VOX_FFMA(dd, 0x1.555556p-1f, lo);
         float best = VOX_FMUL(lo, lo);
