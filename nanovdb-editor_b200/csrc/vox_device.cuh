@@ -787,25 +787,31 @@ __device__ __forceinline__ LbControl lb_control(const int* err)
     return o;
 }
 
-// Publishes `aggregate` for `tile`, walks predecessors and returns the
-// exclusive prefix.  Every wait is bounded; on timeout *err is set and the
-// partial prefix (never larger than the true one) is returned, and the host
-// treats the call as failed.
+// Decoupled look-back over 64-bit status words (epoch << 56 | flag | value).
+// lookback_publish stores `aggregate` for `tile` (tile 0: as its inclusive
+// prefix); lookback_walk walks the predecessors, returns the exclusive prefix
+// and publishes the inclusive one.  Publishing early and walking late (after
+// other tile work) lets the predecessors' inclusive prefixes land meanwhile.
+// Every wait is bounded; on timeout *err is set and the partial prefix (never
+// larger than the true one) is returned, and the host treats the call as failed.
 // max_op: combine predecessors by maximum instead of sum (a running-max scan)
-__device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_t tile, uint64_t aggregate,
-                                                       uint32_t epoch, int* err, size_t stride = 1,
-                                                       bool max_op = false)
+__device__ __forceinline__ void lookback_publish(uint64_t* status, uint64_t tile, uint64_t aggregate, uint32_t epoch,
+                                                 int* err, size_t stride = 1)
 {
     const LbControl ctl = lb_control(err);
+    if (ctl.withhold)
+        return;
     const uint64_t tag = (uint64_t)epoch << 56;
+    st_release_u64(&status[tile * stride], tag | (tile == 0 ? LB_INCL : 0ull) | (aggregate & LB_VALUE_MASK));
+}
+
+__device__ __forceinline__ uint64_t lookback_walk(uint64_t* status, uint64_t tile, uint64_t aggregate, uint32_t epoch,
+                                                  int* err, size_t stride = 1, bool max_op = false)
+{
     if (tile == 0)
-    {
-        if (!ctl.withhold)
-            st_release_u64(&status[0], tag | LB_INCL | (aggregate & LB_VALUE_MASK));
         return 0;
-    }
-    if (!ctl.withhold)
-        st_release_u64(&status[tile * stride], tag | (aggregate & LB_VALUE_MASK));
+    const LbControl ctl = lb_control(err);
+    const uint64_t tag = (uint64_t)epoch << 56;
     uint64_t excl = 0;
     int64_t p = (int64_t)tile - 1;
     uint32_t spins = 0;
@@ -832,6 +838,15 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_
     if (!ctl.withhold)
         st_release_u64(&status[tile * stride], tag | LB_INCL | (incl & LB_VALUE_MASK));
     return excl;
+}
+
+// publish and walk at once
+__device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint64_t tile, uint64_t aggregate,
+                                                       uint32_t epoch, int* err, size_t stride = 1,
+                                                       bool max_op = false)
+{
+    lookback_publish(status, tile, aggregate, epoch, err, stride);
+    return lookback_walk(status, tile, aggregate, epoch, err, stride, max_op);
 }
 
 // The same walk for sums that may use all 64 bits (the prefix is exact mod

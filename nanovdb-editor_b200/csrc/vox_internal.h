@@ -78,19 +78,23 @@ void dual_gather(const uint32_t* sidx, int64_t n, const uint32_t* low_c, const u
                  uint32_t* low, uint32_t* high, uint32_t* val, int* err, int num_sms, cudaStream_t s);
 
 // Online choice among launch variants that give identical results.  Per size
-// class (floor(log2) of the work), each call of a class that has untried
-// variants runs the next one and reports its time per unit of work; later
-// calls run the fastest.  No extra work is launched to tune.
+// class (floor(log2) of the work), the first call of a class is a warm-up
+// (its time, taken on freshly mapped buffers, is not used), then each call of
+// a class that has untried variants runs the next one and reports its time per
+// unit of work; later calls run the fastest.  No extra work is launched to tune.
 struct OnlineChoice
 {
     static const int kClasses = 40, kMax = 4;
     int variants = 1;
     float cost[kClasses][kMax];
+    bool warm[kClasses];
     explicit OnlineChoice(int n = 1) : variants(n)
     {
         for (auto& r : cost)
             for (float& c : r)
                 c = -1.f;
+        for (bool& w : warm)
+            w = false;
     }
     static int size_class(int64_t work)
     {
@@ -115,6 +119,11 @@ struct OnlineChoice
     void report(int64_t work, int v, float ms)
     {
         const int c = size_class(work);
+        if (!warm[c])
+        {
+            warm[c] = true;
+            return;
+        }
         if (v >= 0 && v < variants && work > 0 && cost[c][v] < 0.f && ms > 0.f)
             cost[c][v] = ms / (float)work;
     }

@@ -459,7 +459,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_onesweep(const K* __restrict__ 
         const int d = threadIdx.x;
         if (d < radix)
         {
-            // count of digit d in all earlier tiles
+            // count of digit d in all earlier tiles.  Walked before the shared-memory
+            // scatter: the inclusive prefix this tile publishes is what shortens its
+            // successors' walks (publishing it after the scatter measured slower)
             uint64_t excl = lookback_exclusive(status + d, (uint64_t)tile, total, epoch, err, 256);
             S.gbase[d] = base[d] + excl - dexcl;
         }
