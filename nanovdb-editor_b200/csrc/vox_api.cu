@@ -86,7 +86,8 @@ struct vox_context_t
     vox_stats_t stats{};
     Timers timers;
     SortTuning tuning;
-    OnlineChoice walk_choice{ 2 };     // leaf walk: 4 or 3 CTAs per SM
+    OnlineChoice walk_choice[4] = { OnlineChoice(2), OnlineChoice(2), OnlineChoice(2), OnlineChoice(2) }; // leaf walk: 4 or 3 CTAs per SM, per mode (window | smooth << 1)
+    int walk_mode = 0;
     OnlineChoice vb_search_choice{ 2 }; // VoxelBVH level search: lane-balanced or thread per Gaussian
     int walk_variant = 0, vb_variant = 0;
     // last result
@@ -628,7 +629,8 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     LP.cand_vbase = (const uint64_t*)ctx->cand_vbase.p;
     LP.cand_voff = (const uint64_t*)ctx->cand_voff.p;
     LP.key64 = key64;
-    ctx->walk_variant = ctx->walk_choice.pick((int64_t)Q);
+    ctx->walk_mode = (LP.window ? 1 : 0) | (LP.smooth ? 2 : 0); // the modes differ in cost per pair
+    ctx->walk_variant = ctx->walk_choice[ctx->walk_mode].pick((int64_t)Q);
     ctx->stats.walk_ctas_per_sm = launch_leaf_pass(LP, d_counter, ctx->num_sms, s, ctx->walk_variant);
     cudaEventRecord(ctx->timers.ev[4], s);
     launch_leaf_popc(LP.cand_mask, NCL, (uint64_t*)ctx->cand_cnt.p, s);
@@ -837,7 +839,7 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     st.ms_emit = elapsed(ctx->timers.ev[1], ctx->timers.ev[2]);       // (leaf, Gaussian) pairs
     st.ms_sort = elapsed(ctx->timers.ev[2], ctx->timers.ev[3]);       // sort + candidate leaves
     st.ms_accumulate = elapsed(ctx->timers.ev[3], ctx->timers.ev[4]); // leaf walk: test, RGBA8, float sums
-    ctx->walk_choice.report((int64_t)Q, ctx->walk_variant, st.ms_accumulate);
+    ctx->walk_choice[ctx->walk_mode].report((int64_t)Q, ctx->walk_variant, st.ms_accumulate);
     st.ms_build = elapsed(ctx->timers.ev[4], ctx->timers.ev[6]);      // topology, values, node2
     st.ms_total = elapsed(ctx->timers.ev[0], ctx->timers.ev[6]);
     st.kernel_launches = launch_count() - launches0;
