@@ -480,10 +480,11 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
 // rounding adds 0.5 ulp(E_a), its other roundings (the chain 3, k and base 2,
 // the steps' 3 times |t| <= 7 with 8 vs <= E, lo0 3, the per-voxel fma 3, W and
 // the hi sum about 1.3, in units of 2^-24 sum_a |m_ra| E_a) at most
-// 2^-20 sum_a |m_ra| E_a; all scaled by il is_r.  The linear z classification of the leaf test (leaf_test_chunk)
-// needs only the reference's z terms: dz_r = il is_r |m_r2| (0.5 ulp(W_z) +
-// 0.5 ulp(Cm_z) + 2^-21 Cm_z), and the leaf's largest scaled bound magnitude
-// Bl_r = il is_r sum_a |m_ra| Cm_a; from them its thresholds lo_t / hi_t.
+// 2^-20 sum_a |m_ra| E_a; all scaled by il is_r.  The leaf test
+// (leaf_test_chunk) classifies voxels from this AABB: per row it is within
+// delta_r = dab_r + 2^-20 2 Bl_r of the reference's, Bl_r = il is_r sum_a
+// |m_ra| Cm_a bounding the bounds' magnitudes in the leaf, and Delta = sum_r
+// delta_r gives its thresholds lo_t / hi_t.
 struct LeafPairConst
 {
     float lo0[3], W[3]; // per row: the scaled lower bound of the anchor voxel, the scaled voxel width
@@ -545,9 +546,8 @@ __device__ __forceinline__ LeafPairConst leaf_pair_consts(const GaussRec& R, flo
         const float s = (1.f + 0x1p-20f) * il * is[r];
         const float m0 = fabsf(M.m[r][0]), m1 = fabsf(M.m[r][1]), m2 = fabsf(M.m[r][2]);
         c.dab[r] = s * (m0 * G[0] + m1 * G[1] + m2 * G[2]);
-        const float dz = s * m2 * Gr[2];
         const float Bl = s * (m0 * Cm[0] + m1 * Cm[1] + m2 * Cm[2]);
-        Dl += 2.f * dz + 0x1p-20f * (2.f * Bl + 8.f * fabsf(c.A[r][2]));
+        Dl += c.dab[r] + 0x1p-20f * 2.f * Bl;
     }
     Dl *= 1.f + 0x1p-20f;
     if (Dl <= 0.0625f) // false for NaN
@@ -590,6 +590,7 @@ struct AlphaF
     float d;    // smallest lattice |p|^2
     float a;    // op exp(-ls d), before the opacity transform
     float B[3]; // max(|lo|, |hi|) per axis
+    float m[3]; // the smallest lattice square per axis
 };
 __device__ __forceinline__ AlphaF pair_alpha_f_ex(const GaussRec& R, const Aabb& b)
 {
@@ -604,6 +605,7 @@ __device__ __forceinline__ AlphaF pair_alpha_f_ex(const GaussRec& R, const Aabb&
                     s3 = VOX_FMUL(b.hi[a], b.hi[a]);
         m[a] = fminf(fminf(s0, s1), fminf(s2, s3)); // squares: no NaN, no signed zero
         f.B[a] = fmaxf(fabsf(b.lo[a]), fabsf(b.hi[a]));
+        f.m[a] = m[a];
     }
     f.d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
     float a = VOX_FMUL(R.q6.x, vox_expf(-VOX_FMUL(R.q6.y, f.d)));
@@ -624,10 +626,14 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
 // The RGBA8 alpha byte of a passing pair, rgba8_byte(pair_alpha(R, b_ref))
 // with b_ref = voxel_local_aabb(...), decided where possible from the float
 // channel's alpha f (same formula, evaluated from stable_leaf_aabb).
-// Per row the two AABBs' bounds differ by at most D_r = dab_r + 2^-20 B_r
-// (leaf_pair_consts, plus the scalings' and lattice points' roundings),
-// so their lattice minima d differ by at most md = sum_r (2 B'_r D_r + D_r^2 +
-// 2^-22 B'_r^2) + 2^-21 d (B' = B + D; squares and sums rounded), and the
+// Per row the two AABBs' bounds, and so their four lattice points, differ by at
+// most D_r = dab_r + 2^-20 B_r (leaf_pair_consts, plus the scalings' and
+// lattice points' roundings proportional to B_r = max(|lo|, |hi|)).  With m_r
+// the float evaluation's smallest lattice square, either evaluation's
+// minimizing point is within u_r = sqrt(m_r) + D_r of zero, so the row minima
+// differ by at most 2 sqrt(m_r) D_r + D_r^2 + 2^-22 u_r^2 (rounded squares) and
+// the lattice minima d by md = sum_r of that (times 1 + 2^-20) + 2^-21 d (the
+// two rounded sums); and the
 // alpha a' = 1 - (1 - op e^-ls d)^e, whose slope in d is at most
 // e ls a_hi (times 1 / (1 - a_hi) when e < 1) for a_hi >= op e^-ls (d - md),
 // by at most that slope times md, plus both evaluations' own error (a few ulp
@@ -636,39 +642,42 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
 // decided is set; otherwise the caller runs the reference's evaluation
 // (ref_alpha_byte).  VOX_CHECK_EMIT=1 compares every decided byte with the
 // reference's evaluation.
+// an upper bound of sqrt(x) for x >= 0: the hardware approximation (relative
+// error far below 2^-20) raised by 2^-18, plus 2^-60 for subnormal inputs
+__device__ __forceinline__ float sqrt_upper(float x)
+{
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y * (1.f + 0x1p-18f) + 0x1p-60f;
+}
+
 __device__ __forceinline__ uint32_t alpha_byte_bound(const GaussRec& R, const AlphaF& f, const float dab[3],
                                                      bool& decided)
 {
-    decided = true;
-    if (R.q7.w != 0.f)
-        return 0u; // culled by scale: both alphas are 0
+    // branch-free (the pairs of a warp take different cases): every quantity is
+    // computed and the cases are combined at the end
     float md = 0.f;
 #pragma unroll
     for (int r = 0; r < 3; r++)
     {
         const float D = dab[r] + 0x1p-20f * f.B[r];
-        const float Bp = f.B[r] + D;
-        md += (2.f * Bp + D) * D + 0x1p-22f * Bp * Bp;
+        const float u = sqrt_upper(f.m[r]) + D; // bounds both evaluations' minimizing lattice point
+        md += (2.f * u - D) * D + 0x1p-22f * u * u;
     }
     md = md * (1.f + 0x1p-20f) + 0x1p-21f * f.d;
     const float ls = R.q6.y, e = R.q6.z;
     const float x = ls * md;
-    if (x < 0.25f)
-    {
-        const float a_hi = f.a * (1.f + 2.f * x) * (1.f + 1e-6f); // e^x <= 1 + 2x for x <= 1
-        if (a_hi < 1.f)
-        {
-            float slope = e * ls * a_hi;
-            if (e < 1.f)
-                slope = slope / (1.f - a_hi);
-            const float delta = 1.25f * slope * md + 4e-6f * (1.f + e) + 1e-6f;
-            const uint32_t lo = rgba8_byte(f.a1 - delta), hi = rgba8_byte(f.a1 + delta);
-            if (lo == hi)
-                return lo;
-        }
-    }
-    decided = false;
-    return 0u;
+    const float a_hi = f.a * (1.f + 2.f * x) * (1.f + 1e-6f); // e^x <= 1 + 2x for x <= 1
+    // 1 / (1 - a_hi) from the fast reciprocal (within 2 ulp for 1 - a_hi >= 2^-24,
+    // as it is when a_hi < 1), raised by 2^-20 so it stays an upper bound
+    const float inv = __fdividef(1.f, 1.f - a_hi) * (1.f + 0x1p-20f);
+    float slope = e * ls * a_hi;
+    slope = e < 1.f ? slope * inv : slope;
+    const float delta = 1.25f * slope * md + 4e-6f * (1.f + e) + 1e-6f;
+    const uint32_t lo = rgba8_byte(f.a1 - delta), hi = rgba8_byte(f.a1 + delta);
+    const bool culled = R.q7.w != 0.f; // culled by scale: both alphas are 0
+    decided = culled || (x < 0.25f && a_hi < 1.f && lo == hi);
+    return culled ? 0u : lo;
 }
 
 // the reference's RGBA8 alpha byte of voxel (i, j, k) and the record's Gaussian

@@ -380,27 +380,23 @@ struct LeafQSmem
 // shared atomic per warp and round.
 //
 // APPROX (a LeafChunk, carrying the leaf_pair_consts of each Gaussian): each
-// voxel of the column is first classified from bounds linear in k - the
-// reference's scaled bounds of the column's first voxel, sl / sh, plus k times
-// the scaled z step st = fl(fl(vs m_r2) fl(il is_r)) - and only voxels near the
-// sphere run the reference test.  Per row, the reference's bound of voxel k
-// differs from the exact-arithmetic one by at most dz_r + 2^-22 Bl_r (the z
-// corner offset, product and sum roundings; the x + y share is common to both;
-// the sum and two scalings relative), and so does sl; the step's three
-// roundings times k <= 8 and the fma's rounding add at most 2^-21 (Bl_r +
-// 8 |st_r|).  The selected values (max(lo, min(hi, 0)), 1-Lipschitz in both
-// bounds) therefore differ by at most delta_r = 2 dz_r + 2^-20 (2 Bl_r +
-// 8 |st_r|), and the vectors of the three by eta <= Delta = sum delta_r in
-// norm.  The reference passes a voxel when its fl-evaluated 1 - S > 0: surely
-// if S < 1 - 2^-22 (three subtractions and squares of values below 1) and
-// surely not if S > 1 + 2^-20.  With D the fma-summed squares of the linear
-// values (relative error <= 3 2^-24) and Delta <= 1/16, (sqrt(D) + eta)^2 <
-// 1 - 2^-22 holds when D < lo_t = 1 - (2 Delta + 2^-19), and (sqrt(D) - eta)^2
-// > 1 + 2^-20 when D > hi_t = 1 + (2 Delta + Delta^2 + 2^-18) (the slack
-// covers the roundings of the thresholds themselves).  Voxels with D in
-// [lo_t, hi_t] (or NaN), and every voxel of a (leaf, Gaussian) with Delta >
-// 1/16 (lo_t = -1, hi_t = inf), take the reference test.  In CHECK mode every
-// voxel also takes it and a difference sets ERR_BOUNDS.
+// voxel of the column is first classified from the float channels' local AABB
+// (stable_leaf_aabb: per column the x / y terms once, then one fma per row
+// and voxel), and only voxels near the sphere run the reference test.  Per
+// row that AABB is within delta_r = dab_r + 2^-20 2 Bl_r of the reference's
+// (leaf_pair_consts), so the selected values (max(lo, min(hi, 0)),
+// 1-Lipschitz in both bounds) differ by at most delta_r and the vectors of the
+// three by eta <= Delta = sum delta_r in norm.  The reference passes a voxel
+// when its fl-evaluated 1 - S > 0: surely if S < 1 - 2^-22 (three subtractions
+// and squares of values below 1) and surely not if S > 1 + 2^-20.  With D the
+// fma-summed squares of the float values (relative error <= 3 2^-24) and
+// Delta <= 1/16, (sqrt(D) + eta)^2 < 1 - 2^-22 holds when D < lo_t = 1 -
+// (2 Delta + 2^-19), and (sqrt(D) - eta)^2 > 1 + 2^-20 when D > hi_t = 1 +
+// (2 Delta + Delta^2 + 2^-18) (the slack covers the roundings of the
+// thresholds themselves).  Voxels with D in [lo_t, hi_t] (or NaN), and every
+// voxel of a (leaf, Gaussian) with Delta > 1/16 (lo_t = -1, hi_t = inf), take
+// the reference test.  In CHECK mode every voxel also takes it and a
+// difference sets ERR_BOUNDS.
 template <bool CHECK, bool PER_WARP = false, bool APPROX = false, class Chunk>
 __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const Chunk& C, uint32_t cnt,
                                                 const int32_t o[3], uint16_t* queue, uint32_t* qcount, int t, int lane)
@@ -452,78 +448,28 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
             const uint32_t dy = local - dx * C.bny[j];
             const int32_t rx = C.bx0[j] + (int32_t)dx, ry = C.by0[j] + (int32_t)dy, rz0 = C.bz0[j];
             const GaussRec& R = C.rec[j].r;
-            const RInv M = rinv_of(R);
-            const float vsf = C.vs[j], il = R.q0.w, pz = R.q0.z;
-            const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
-            float cx0, cx1, cy0, cy1;
-            axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
-            axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
-            float slo[3], shi[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-            {
-                float xn, xx, yn, yx;
-                minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
-                minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
-                slo[r] = VOX_FADD(xn, yn);
-                shi[r] = VOX_FADD(xx, yx);
-            }
+            const float vsf = C.vs[j];
             const uint32_t nz = C.bnz[j];
-            // the reference test of the column's voxels, z run from k0 (mask bits from k0)
-            auto exact_run = [&](uint32_t k0, uint32_t k1) -> uint32_t {
-                uint32_t mk = 0;
-                float v = (float)(o[2] + rz0 + (int32_t)k0);
-                float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-                float pa[3];
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-                    pa[r] = VOX_FMUL(cz, M.m[r][2]);
-#pragma unroll 2
-                for (uint32_t k = k0; k < k1; k++)
-                {
-                    v = VOX_FADD(v, 1.f);
-                    cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
-                    float d2 = 1.f;
-#pragma unroll
-                    for (int r = 0; r < 3; r++)
-                    {
-                        // the corner offsets grow with z: per row the smaller product is the
-                        // lower corner's when the matrix entry is >= 0 (fl(c m) is monotone
-                        // in c; a tie differs at most in the sign of a zero, which is squared)
-                        const float pb = VOX_FMUL(cz, M.m[r][2]);
-                        const bool up = M.m[r][2] >= 0.f;
-                        const float zn = up ? pa[r] : pb, zx = up ? pb : pa[r];
-                        pa[r] = pb;
-                        const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
-                        // xl <= xh: the bound of the row's interval nearest to zero, or zero
-                        const float xs = VOX_FADD(fmaxf(xl, 0.f), fminf(xh, 0.f));
-                        const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
-                        d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
-                    }
-                    mk |= (d2 > 0.f ? 1u : 0u) << k;
-                }
-                return mk;
-            };
             if constexpr (APPROX)
             {
-                // the reference's scaled bounds of voxel 0 of the run, the scaled z step
-                const float v0 = (float)(o[2] + rz0);
-                const float cz0 = VOX_FSUB(VOX_FMUL(v0, vsf), pz);
-                const float cz1 = VOX_FSUB(VOX_FMUL(VOX_FADD(v0, 1.f), vsf), pz);
-                float sl[3], sh[3], st[3];
+                // the float channels' AABB of the run's voxels (stable_leaf_aabb: the
+                // column's x / y terms once, then one fma per row and voxel), within
+                // delta_r of the reference's for every voxel of the leaf
+                const uint32_t anc = C.anchor[j];
+                const float tx = (float)(rx - (int32_t)(anc & 255u)), ty = (float)(ry - (int32_t)((anc >> 8) & 255u)),
+                            tz0 = (float)(rz0 - (int32_t)(anc >> 16));
+                float base[3], wid[3], st[3];
 #pragma unroll
                 for (int r = 0; r < 3; r++)
                 {
-                    float zn, zx;
-                    minmax_prod(cz0, cz1, M.m[r][2], zn, zx);
-                    sl[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(slo[r], zn), il), is[r]);
-                    sh[r] = VOX_FMUL(VOX_FMUL(VOX_FADD(shi[r], zx), il), is[r]);
+                    base[r] = VOX_FFMA(ty, C.stp[r][1][j], VOX_FFMA(tx, C.stp[r][0][j], C.lo0[r][j]));
+                    wid[r] = C.wid[r][j];
                     st[r] = C.stp[r][2][j];
                 }
                 const float lo_t = C.lo_t[j], hi_t = C.hi_t[j];
                 uint32_t unc = 0;
                 {
-                    float kf = 0.f;
+                    float kf = tz0;
 #pragma unroll 2
                     for (uint32_t k = 0; k < nz; k++, kf += 1.f)
                     {
@@ -531,7 +477,7 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
 #pragma unroll
                         for (int r = 0; r < 3; r++)
                         {
-                            const float a = __fmaf_rn(kf, st[r], sl[r]), b = __fmaf_rn(kf, st[r], sh[r]);
+                            const float a = VOX_FFMA(kf, st[r], base[r]), b = VOX_FADD(a, wid[r]);
                             const float xs = fmaxf(a, fminf(b, 0.f));
                             D = __fmaf_rn(xs, xs, D);
                         }
@@ -556,7 +502,52 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
                 }
             }
             else
-                zmask = exact_run(0, nz);
+            {
+                const RInv M = rinv_of(R);
+                const float il = R.q0.w, pz = R.q0.z;
+                const float is[3] = { R.q3.y, R.q3.z, R.q3.w };
+                float cx0, cx1, cy0, cy1;
+                axis_corners(vsf, R.q0.x, o[0] + rx, cx0, cx1);
+                axis_corners(vsf, R.q0.y, o[1] + ry, cy0, cy1);
+                float slo[3], shi[3], pa[3];
+                float v = (float)(o[2] + rz0);
+                float cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                {
+                    float xn, xx, yn, yx;
+                    minmax_prod(cx0, cx1, M.m[r][0], xn, xx);
+                    minmax_prod(cy0, cy1, M.m[r][1], yn, yx);
+                    slo[r] = VOX_FADD(xn, yn);
+                    shi[r] = VOX_FADD(xx, yx);
+                    pa[r] = VOX_FMUL(cz, M.m[r][2]);
+                }
+                // the reference test along the z run
+#pragma unroll 2
+                for (uint32_t k = 0; k < nz; k++)
+                {
+                    v = VOX_FADD(v, 1.f);
+                    cz = VOX_FSUB(VOX_FMUL(v, vsf), pz);
+                    float d2 = 1.f;
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        // the corner offsets grow with z: per row the smaller product is the
+                        // lower corner's when the matrix entry is >= 0 (fl(c m) is monotone
+                        // in c; a tie differs at most in the sign of a zero, which is squared)
+                        const float pb = VOX_FMUL(cz, M.m[r][2]);
+                        const bool up = M.m[r][2] >= 0.f;
+                        const float zn = up ? pa[r] : pb, zx = up ? pb : pa[r];
+                        pa[r] = pb;
+                        const float xl = VOX_FADD(slo[r], zn), xh = VOX_FADD(shi[r], zx);
+                        // xl <= xh: the bound of the row's interval nearest to zero, or zero
+                        const float xs = VOX_FADD(fmaxf(xl, 0.f), fminf(xh, 0.f));
+                        const float sv = VOX_FMUL(VOX_FMUL(xs, il), is[r]);
+                        d2 = VOX_FSUB(d2, VOX_FMUL(sv, sv));
+                    }
+                    zmask |= (d2 > 0.f ? 1u : 0u) << k;
+                }
+            }
             ebase = ((uint32_t)j << 9) | (uint32_t)((rx << 6) | (ry << 3) | rz0);
             if (CHECK && zmask && C.flag[j])
                 atomicOr(P.err, ERR_BOUNDS); // the leaf test would have dropped a passing voxel
