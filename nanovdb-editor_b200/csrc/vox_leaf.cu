@@ -399,7 +399,8 @@ struct LeafQSmem
 // difference sets ERR_BOUNDS.
 template <bool CHECK, bool PER_WARP = false, bool APPROX = false, class Chunk>
 __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const Chunk& C, uint32_t cnt,
-                                                const int32_t o[3], uint16_t* queue, uint32_t* qcount, int t, int lane)
+                                                const int32_t o[3], uint16_t* queue, uint32_t* qcount, int t, int lane,
+                                                uint32_t rot = 0)
 {
     uint32_t wbase = 0; // PER_WARP: entries this warp has written
     if (PER_WARP)
@@ -416,9 +417,13 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
             start[j + 1] = start[j] + (j < (int)cnt ? C.bcol[j] : 0u);
         T = start[LQ_CHUNK];
     }
-    for (uint32_t b0 = 0; b0 < T; b0 += LP_THREADS)
+    // rounds of 32 columns dealt to the warps in turn, starting at warp rot (mod 8):
+    // the forward continues the deal where the alpha's rounds of 32 pairs stopped,
+    // so the warps' loads in a phase differ by at most one round
+    const uint32_t first = (uint32_t)(((t >> 5) - (int)(rot & 7u)) & 7);
+    for (uint32_t tu = first; tu * 32u < T; tu += LP_THREADS / 32)
     {
-        const uint32_t e = b0 + (uint32_t)t;
+        const uint32_t e = tu * 32u + (uint32_t)lane;
         uint32_t zmask = 0, ebase = 0;
         if (e < T)
         {
@@ -817,6 +822,7 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
             }
             __syncthreads(); // the next leaf's alpha reuses the accumulators
         }
+        const uint32_t a_rounds = a_valid ? (S.qn[ab] + 31u) / 32u : 0u; // the alpha's rounds of 32 pairs
         // ---- alpha of the previous chunk, one queued pair per thread.  A pair
         // whose RGBA8 byte the bound leaves open (a few percent) is deferred to
         // its warp's list and the reference's byte is evaluated 32 pairs at a
@@ -924,8 +930,8 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
         }
         // ---- test of this chunk
         if (t_valid)
-            leaf_test_chunk<CHECK, false, true>(P, S.ch[tb], min((uint32_t)LQ_CHUNK, tp1 - tq0), to, S.queue[i & 1u], &S.qn[tb], t,
-                                   lane);
+            leaf_test_chunk<CHECK, false, true>(P, S.ch[tb], min((uint32_t)LQ_CHUNK, tp1 - tq0), to, S.queue[i & 1u],
+                                                &S.qn[tb], t, lane, a_rounds);
         // the counter the test of phase i + 1 fills: last read by the alpha of phase i - 1
         if (t == 0)
             S.qn[nb] = 0;
