@@ -334,7 +334,7 @@ typedef struct vox_stats_t
     float ms_prep, ms_emit, ms_sort, ms_build, ms_accumulate, ms_total;
     int64_t kernel_launches; /* kernels this library launched in the call */
     float ms_backward;       /* last vox_backward */
-    int32_t sort_shape;      /* onesweep tile shape the sort used (tuned) */
+    int32_t sort_shape;      /* the sort's tuned candidate: 0-4 onesweep tile shapes, 5-9 the same as three-kernel passes */
     int64_t leaf_pairs;      /* (leaf, Gaussian) pairs sorted */
     int64_t candidate_leaves; /* leaves walked (some end up empty) */
     /* last vox_voxelbvh_ijkl_from_gaussians */

@@ -1000,6 +1000,11 @@ vox_context_t* vox_context_create(int device)
     ctx->check_sort = (chk && chk[0] == '1') ? 1 : 0;
     const char* chk_emit = getenv("VOX_CHECK_EMIT");
     ctx->check_emit = (chk_emit && chk_emit[0] == '1') ? 1 : 0;
+    // VOX_SORT_SHAPE=c fixes the sort's tuner candidate (0-4: onesweep tile
+    // shapes, 5-9: the same shapes as three-kernel passes), for tests and timing
+    const char* shp = getenv("VOX_SORT_SHAPE");
+    if (shp && shp[0] >= '0' && shp[0] <= '9' && shp[1] == 0)
+        ctx->tuning.shape = shp[0] - '0';
     return ctx;
 }
 

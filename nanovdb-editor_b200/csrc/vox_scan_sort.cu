@@ -278,10 +278,11 @@ constexpr int SORT_TILE_MIN = 2048; // status words are sized for the smallest t
 
 struct SortWs
 {
-    uint32_t* hist;     // [passes][256]
-    uint64_t* base;     // [passes][256]
-    uint32_t* counters; // [passes]
-    uint64_t* status;   // [tiles][256]
+    uint32_t* hist;      // [passes][256]
+    uint64_t* base;      // [passes][256]
+    uint32_t* counters;  // [passes]
+    uint64_t* status;    // [tiles][256]
+    uint32_t* tile_hist; // [256][tiles]: per-tile digit counts, then their global offsets (three-kernel passes)
     int64_t tiles;
 };
 
@@ -302,6 +303,8 @@ static SortWs carve(void* ws, int64_t n)
     w.counters = (uint32_t*)p;
     p += align256(sizeof(uint32_t) * (SORT_MAX_PASSES + 1));
     w.status = (uint64_t*)p;
+    p += align256(sizeof(uint64_t) * (w.tiles + 1) * 256);
+    w.tile_hist = (uint32_t*)p;
     return w;
 }
 
@@ -310,7 +313,8 @@ size_t sort_workspace_bytes(int64_t n, int key_bytes)
     (void)key_bytes;
     int64_t tiles = (n + SORT_TILE_MIN - 1) / SORT_TILE_MIN;
     return align256(sizeof(uint32_t) * SORT_MAX_PASSES * 256) + align256(sizeof(uint64_t) * SORT_MAX_PASSES * 256) +
-           align256(sizeof(uint32_t) * (SORT_MAX_PASSES + 1)) + align256(sizeof(uint64_t) * (tiles + 1) * 256);
+           align256(sizeof(uint32_t) * (SORT_MAX_PASSES + 1)) + align256(sizeof(uint64_t) * (tiles + 1) * 256) +
+           align256(sizeof(uint32_t) * (tiles + 1) * 256);
 }
 
 size_t sort_status_words(int64_t n)
@@ -381,11 +385,15 @@ struct SortSmem
     uint32_t tile;
 };
 
-template <class K, int BLOCK, int ITEMS, int MINB>
+// LB: the tile's digit offsets from a decoupled look-back over the tiles before
+// it (tiles claimed in order by an atomic ticket); otherwise from offsets, the
+// digit-major exclusive scan of every tile's digit counts (tile = block index)
+template <class K, int BLOCK, int ITEMS, int MINB, bool LB = true>
 __global__ void __launch_bounds__(BLOCK, MINB) k_onesweep(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                                                           K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                                                           int64_t n, int shift, int bits, const uint64_t* base,
-                                                          uint64_t* status, uint32_t epoch, uint32_t* counter, int* err)
+                                                          uint64_t* status, uint32_t epoch, uint32_t* counter, int* err,
+                                                          const uint32_t* offsets = nullptr, int64_t ntiles = 0)
 {
     constexpr int TILE = BLOCK * ITEMS;
     constexpr int WARPS = BLOCK / 32;
@@ -396,7 +404,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_onesweep(const K* __restrict__ 
     const int radix = 1 << bits;
 
     if (threadIdx.x == 0)
-        S.tile = atomicAdd(counter, 1u);
+        S.tile = LB ? atomicAdd(counter, 1u) : blockIdx.x;
     for (int i = lane; i < 256; i += 32)
         S.warp_hist[warp][i] = 0;
     __syncthreads();
@@ -462,8 +470,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_onesweep(const K* __restrict__ 
             // count of digit d in all earlier tiles.  Walked before the shared-memory
             // scatter: the inclusive prefix this tile publishes is what shortens its
             // successors' walks (publishing it after the scatter measured slower)
-            uint64_t excl = lookback_exclusive(status + d, (uint64_t)tile, total, epoch, err, 256);
-            S.gbase[d] = base[d] + excl - dexcl;
+            if constexpr (LB)
+            {
+                uint64_t excl = lookback_exclusive(status + d, (uint64_t)tile, total, epoch, err, 256);
+                S.gbase[d] = base[d] + excl - dexcl;
+            }
+            else
+                S.gbase[d] = (uint64_t)offsets[(int64_t)d * ntiles + tile] - dexcl;
         }
     }
     __syncthreads();
@@ -528,6 +541,118 @@ static void onesweep_pass(int shape, const K* src_k, const uint32_t* src_v, K* d
 #undef VOX_ONESWEEP
 }
 
+// Three-kernel pass (no look-back chain): per-tile digit counts, then per digit
+// an exclusive scan over the tiles plus the digit's global base, then the
+// onesweep tile ranking and scatter with those offsets.  The same stable result
+// as the onesweep pass; it reads the keys once more but no tile waits on
+// another, which wins where the look-back chain's latency bounds the pass.
+template <class K, int BLOCK, int ITEMS>
+__global__ void __launch_bounds__(BLOCK) k_tile_hist(const K* __restrict__ keys, int64_t n, int shift, int bits,
+                                                     uint32_t* __restrict__ tile_hist, int64_t ntiles)
+{
+    __shared__ uint32_t h[BLOCK / 32][256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t mask = (1u << bits) - 1u;
+    for (int i = lane; i < 256; i += 32)
+        h[warp][i] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * (BLOCK * ITEMS);
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+    {
+        const int64_t idx = base + (int64_t)i * BLOCK + threadIdx.x;
+        if (idx < n)
+            atomicAdd(&h[warp][digit_of(keys[idx], shift, mask)], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d <= (int)mask; d += BLOCK)
+    {
+        uint32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < BLOCK / 32; w++)
+            c += h[w][d];
+        tile_hist[(int64_t)d * ntiles + blockIdx.x] = c;
+    }
+}
+
+// one block per digit: the row of tile counts -> base[d] + exclusive prefix, in place
+__global__ void __launch_bounds__(256) k_tile_offsets(uint32_t* tile_hist, int64_t ntiles, const uint64_t* base)
+{
+    __shared__ uint64_t s_warp[33];
+    uint32_t* row = tile_hist + (int64_t)blockIdx.x * ntiles;
+    uint64_t running = base[blockIdx.x];
+    for (int64_t c0 = 0; c0 < ntiles; c0 += 256 * 4)
+    {
+        const int64_t t0 = c0 + (int64_t)threadIdx.x * 4;
+        uint32_t v[4];
+        uint64_t sum = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+            v[q] = t0 + q < ntiles ? row[t0 + q] : 0u;
+            sum += v[q];
+        }
+        uint64_t all;
+        uint64_t ex = running + block_excl_scan_u64(sum, s_warp, all);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (t0 + q < ntiles)
+            {
+                row[t0 + q] = (uint32_t)ex;
+                ex += v[q];
+            }
+        running += all;
+    }
+}
+
+template <class K>
+static void three_kernel_pass(int shape, const K* src_k, const uint32_t* src_v, K* dst_k, uint32_t* dst_v, int64_t n,
+                              int shift, int bits, const uint64_t* base, uint32_t* tile_hist, int* err, cudaStream_t s)
+{
+    const int64_t tiles = (n + SORT_SHAPES[shape].tile - 1) / SORT_SHAPES[shape].tile;
+#define VOX_THREEK(B, I, M)                                                                                        \
+    {                                                                                                              \
+        k_tile_hist<K, B, I><<<(unsigned)tiles, B, 0, s>>>(src_k, n, shift, bits, tile_hist, tiles);               \
+        count_launch();                                                                                            \
+        k_tile_offsets<<<1u << bits, 256, 0, s>>>(tile_hist, tiles, base);                                         \
+        count_launch();                                                                                            \
+        const size_t smem = sizeof(SortSmem<K, B, I>);                                                             \
+        cudaFuncSetAttribute(k_onesweep<K, B, I, M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        k_onesweep<K, B, I, M, false><<<(unsigned)tiles, B, smem, s>>>(src_k, src_v, dst_k, dst_v, n, shift, bits,   \
+                                                                        base, nullptr, 0u, nullptr, err, tile_hist, \
+                                                                        tiles);                                    \
+        count_launch();                                                                                            \
+    }
+    switch (shape)
+    {
+    case 0: VOX_THREEK(512, 16, 1) break;
+    case 1: VOX_THREEK(256, 16, 2) break;
+    case 2: VOX_THREEK(256, 12, 3) break;
+    case 3: VOX_THREEK(256, 8, 4) break;
+    default: VOX_THREEK(512, 8, 2) break;
+    }
+#undef VOX_THREEK
+}
+
+// candidate c of the tuner: tile shape c % SORT_NSHAPES, onesweep (c < SORT_NSHAPES) or three kernels
+constexpr int SORT_NCAND = 2 * SORT_NSHAPES;
+
+template <class K>
+static void sort_pass(int cand, const K* src_k, const uint32_t* src_v, K* dst_k, uint32_t* dst_v, int64_t n, int shift,
+                      int bits, const uint64_t* base, const SortWs& w, Epochs* epochs, size_t words, uint32_t* counter,
+                      int* err, cudaStream_t s)
+{
+    // the three-kernel offsets are 32-bit: n < 2^32 (every caller's limit; onesweep otherwise)
+    if (cand < SORT_NSHAPES || n >= (1ll << 32))
+    {
+        cand %= SORT_NSHAPES;
+        const uint32_t epoch = epochs->next(w.status, words, s);
+        onesweep_pass<K>(cand, src_k, src_v, dst_k, dst_v, n, shift, bits, base, w.status, epoch, counter, err, s);
+    }
+    else
+        three_kernel_pass<K>(cand - SORT_NSHAPES, src_k, src_v, dst_k, dst_v, n, shift, bits, base, w.tile_hist, err, s);
+}
+
 static int size_class(int64_t n)
 {
     int c = 0;
@@ -557,22 +682,21 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     { k_sort_bases<<<1, 256, 0, s>>>(w.hist, w.base, passes); count_launch(); }
     const size_t words = sort_status_words(n);
     const int kw = sizeof(K) == 8 ? 1 : 0, sc = size_class(n);
-    int shape = tune.shape >= 0 && tune.shape < SORT_NSHAPES ? tune.shape : tune.best[kw][sc];
+    int shape = tune.shape >= 0 && tune.shape < SORT_NCAND ? tune.shape : tune.best[kw][sc];
     if (shape < 0)
     {
-        // tuner: time pass 0 of every shape on this data (the output is rewritten below)
+        // tuner: time pass 0 of every candidate on this data (the output is rewritten below)
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         float best_ms = 1e30f;
         shape = 0;
-        for (int t = 0; t < SORT_NSHAPES; t++)
+        for (int t = 0; t < SORT_NCAND; t++)
         {
-            uint32_t epoch = epochs->next(w.status, words, s);
             cudaMemsetAsync(w.counters + SORT_MAX_PASSES, 0, sizeof(uint32_t), s);
             cudaEventRecord(e0, s);
-            onesweep_pass<K>(t, keys, vals, keys_alt, vals_alt, n, 0, pass_bits(0, bits, key_bits), w.base, w.status,
-                             epoch, w.counters + SORT_MAX_PASSES, err, s);
+            sort_pass<K>(t, keys, vals, keys_alt, vals_alt, n, 0, pass_bits(0, bits, key_bits), w.base, w, epochs, words,
+                         w.counters + SORT_MAX_PASSES, err, s);
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             float ms = 0.f;
@@ -593,9 +717,8 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
     uint32_t* dst_v = vals_alt;
     for (int p = 0; p < passes; p++)
     {
-        uint32_t epoch = epochs->next(w.status, words, s);
-        onesweep_pass<K>(shape, src_k, src_v, dst_k, dst_v, n, p * bits, pass_bits(p, bits, key_bits),
-                         w.base + p * 256, w.status, epoch, w.counters + p, err, s);
+        sort_pass<K>(shape, src_k, src_v, dst_k, dst_v, n, p * bits, pass_bits(p, bits, key_bits), w.base + p * 256, w,
+                     epochs, words, w.counters + p, err, s);
         K* tk = src_k;
         src_k = dst_k;
         dst_k = tk;
@@ -608,7 +731,7 @@ static int sort_pairs_impl(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_
 
 int sort_shape_used(int64_t n, int key64, const SortTuning& tune)
 {
-    if (tune.shape >= 0 && tune.shape < SORT_NSHAPES)
+    if (tune.shape >= 0 && tune.shape < SORT_NCAND)
         return tune.shape;
     return n > 1 ? tune.best[key64 ? 1 : 0][size_class(n)] : -1;
 }

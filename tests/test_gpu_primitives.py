@@ -177,3 +177,43 @@ def test_radix_sort_dual_key(vox_ctx, n, low_bits, high_bits):
     np.testing.assert_array_equal(dl.cpu().numpy().view(np.uint32), low[order])
     np.testing.assert_array_equal(dh.cpu().numpy().view(np.uint32), high[order])
     np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[order])
+
+
+@pytest.mark.parametrize("cand", list(range(10)))
+def test_every_sort_candidate_is_the_same_stable_sort(cand):
+    # VOX_SORT_SHAPE fixes the tuner's candidate: 0-4 onesweep tile shapes
+    # (decoupled look-back), 5-9 the same tiles as three-kernel passes (tile
+    # digit counts, per-digit offsets, scatter); all are the same stable sort
+    import os
+
+    import torch
+
+    from nanovdb_editor.vox import VoxContext
+
+    os.environ["VOX_SORT_SHAPE"] = str(cand)
+    try:
+        ctx = VoxContext(0)
+    finally:
+        del os.environ["VOX_SORT_SHAPE"]
+    try:
+        for n, bits in ((1, 32), (4097, 20), (300_001, 31), (2_000_003, 64)):
+            rng = np.random.default_rng(1000 * cand + n)
+            if bits == 64:
+                keys = rng.integers(0, np.iinfo(np.uint64).max, n, dtype=np.uint64, endpoint=True)
+                vals = np.arange(n, dtype=np.uint32)
+                dk, dv = _dev(keys, np.int64), _dev(vals, np.int32)
+                ctx.radix_sort_key64(dk, dv, bits)
+                gk = dk.cpu().numpy().view(np.uint64)
+            else:
+                keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
+                keys[: n // 3] = keys[0]  # long runs of equal keys: stability
+                vals = np.arange(n, dtype=np.uint32)
+                dk, dv = _dev(keys, np.int32), _dev(vals, np.int32)
+                ctx.radix_sort_u32(dk, dv, bits)
+                gk = dk.cpu().numpy().view(np.uint32)
+            torch.cuda.synchronize()
+            order = np.argsort(keys, kind="stable")
+            np.testing.assert_array_equal(gk, keys[order])
+            np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[order])
+    finally:
+        ctx.close()
