@@ -359,6 +359,8 @@ struct LeafQSmem
     LeafAcc acc[1];
     uint16_t queue[2][LQ_CHUNK * 512];
     uint16_t defer[LP_THREADS / 32][64]; // per warp: queued pairs whose RGBA8 byte the bound left open
+    uint32_t dcount[LP_THREADS / 32];     // per warp: the open pairs left at the end of its alpha
+    uint32_t dfin;                        // warps done with this phase's alpha
     uint32_t qn[3];
     int32_t nxt_o[2][3]; // the next chunk (by phase parity): leaf origin and sorted pair range
     uint32_t nxt_q0[2], nxt_p1[2];
@@ -689,6 +691,7 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
         S.cand_next[0] = atomicAdd(counter, 1u);
         S.pairs = 0;
         S.qn[0] = S.qn[1] = S.qn[2] = 0;
+        S.dfin = 0;
         S.acc[0].wmin = ~0ull;
     }
 #pragma unroll
@@ -921,11 +924,48 @@ __global__ void __launch_bounds__(LP_THREADS, MINB) k_leaf_pass(LeafPassParams P
                     }
                 }
             }
-            if (dn)
+            // the open pairs left in every warp's list (fewer than 32 each): the last
+            // warp to finish this phase's alpha evaluates all of them, 32 at a time
+            // (the chunk's records stay in place until the next phase's staging)
+            uint32_t fin = 0;
+            if (lane == 0)
             {
-                __syncwarp();
-                if ((uint32_t)lane < dn)
-                    ref_byte(dq[lane]);
+                S.dcount[warp] = dn;
+                __threadfence_block();
+                fin = atomicAdd(&S.dfin, 1u);
+            }
+            fin = __shfl_sync(0xffffffffu, fin, 0);
+            if (fin == LP_THREADS / 32 - 1)
+            {
+                __threadfence_block();
+                const uint32_t c = (uint32_t)lane < LP_THREADS / 32 ? *(volatile uint32_t*)&S.dcount[lane] : 0u;
+                uint32_t incl = c;
+#pragma unroll
+                for (int off = 1; off < LP_THREADS / 32; off <<= 1)
+                {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+                    if (lane >= off)
+                        incl += y;
+                }
+                const uint32_t total = __shfl_sync(0xffffffffu, incl, LP_THREADS / 32 - 1);
+                for (uint32_t b = 0; b < total; b += 32)
+                {
+                    const uint32_t item = b + (uint32_t)lane;
+                    // the warp list holding item: the first w whose inclusive count exceeds it
+                    uint32_t w = 0, before = 0;
+#pragma unroll
+                    for (int v = 0; v < LP_THREADS / 32; v++)
+                    {
+                        const uint32_t iv = __shfl_sync(0xffffffffu, incl, v);
+                        const bool past = item >= iv;
+                        w += past ? 1u : 0u;
+                        before = past ? iv : before;
+                    }
+                    if (item < total)
+                        ref_byte(*(volatile uint16_t*)&S.defer[w][item - before]);
+                }
+                if (lane == 0)
+                    S.dfin = 0;
             }
         }
         // ---- test of this chunk
