@@ -580,7 +580,8 @@ __device__ __forceinline__ Aabb stable_leaf_aabb(const float lo0[3], const float
 }
 
 // Alpha of the float density / colour channels from their local AABB
-// (stable_leaf_aabb): the lattice points lo + w (hi - lo), float exp / pow.  The oracle's
+// (stable_leaf_aabb): the lattice points lo + w (hi - lo), float exp / pow
+// (vox_expf_ch / vox_powf_ch: about 2 ulp, no division).  The oracle's
 // frag_alpha_f evaluates the same operations in the same order.  Also keeps
 // what alpha_byte_bound needs: the lattice minimum d, op exp(-ls d) and
 // the largest bound magnitude per axis.
@@ -608,10 +609,10 @@ __device__ __forceinline__ AlphaF pair_alpha_f_ex(const GaussRec& R, const Aabb&
         f.m[a] = m[a];
     }
     f.d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
-    float a = VOX_FMUL(R.q6.x, vox_expf(-VOX_FMUL(R.q6.y, f.d)));
+    float a = VOX_FMUL(R.q6.x, vox_expf_ch(-VOX_FMUL(R.q6.y, f.d)));
     a = a > 0.f ? a : 0.f;
     f.a = a;
-    a = VOX_FSUB(1.f, vox_powf_unit(VOX_FSUB(1.f, a), R.q6.z));
+    a = VOX_FSUB(1.f, vox_powf_ch(VOX_FSUB(1.f, a), R.q6.z));
     if (R.q7.w != 0.f)
         a = 0.f;
     f.a1 = a;

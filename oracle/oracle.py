@@ -52,6 +52,8 @@ def lib():
         L.ov_run.argtypes = [c_int64] + [c_void_p] * 5 + [c_float, c_float, c_int, c_int]
         L.ov_destroy.argtypes = [c_void_p]
         L.ov_counts.argtypes = [c_void_p, c_void_p]
+        L.ov_chan_math.argtypes = [c_int64] + [c_void_p] * 6
+        L.ov_chan_math.restype = None
         L.ov_node2_bytes.restype = c_int64
         L.ov_node2_bytes.argtypes = [c_void_p, c_void_p]
         L.ov_pairs.argtypes = [c_void_p, c_void_p, c_void_p]
@@ -209,3 +211,12 @@ def voxelbvh_ijkl(cloud, resolution: int, transform=None, transform_inv=None, nt
                                keys.ctypes.data, ids.ctypes.data, rng.ctypes.data, box.ctypes.data,
                                int(nthreads or max(1, min(16, os.cpu_count() or 1))))
     return {"ijkl": keys, "prim_id": ids, "range": rng, "ranges": int(r), "world_bbox": box}
+
+
+def chan_math(x, b, e):
+    """The float channels' exp(x), log(b), b^e (float32 arrays of one length)."""
+    x, b, e = (np.ascontiguousarray(a, dtype=np.float32) for a in (x, b, e))
+    n = x.shape[0]
+    out = [np.empty(n, np.float32) for _ in range(3)]
+    lib().ov_chan_math(n, x.ctypes.data, b.ctypes.data, e.ctypes.data, *(o.ctypes.data for o in out))
+    return out

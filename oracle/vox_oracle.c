@@ -316,7 +316,7 @@ static float fx_to_float(int64_t s)
  *     fma(t_z, A_r2, fma(t_y, A_r1, fma(t_x, A_r0, lo0_r))), hi_r = fl(lo_r + W_r);
  *   lattice points lo + w (hi - lo), w = 0, 1/3, 2/3, 1; the maximum of the
  *     decreasing exp is at the per-axis smallest square;
- *   float exp / pow (vox_expf, vox_powf).
+ *   float exp / pow (vox_expf_ch, vox_powf_ch).
  * The device evaluates the same operations in the same order (leaf_pair_consts,
  * stable_leaf_aabb); the signs of zero sums may differ, which the squares hide. */
 static float frag_alpha_f(const prim_t* P, const float rinv[3][3], float vs, const int32_t* ijk, float cull_scale)
@@ -355,11 +355,11 @@ static float frag_alpha_f(const prim_t* P, const float rinv[3][3], float vs, con
         m[r] = best;
     }
     const float d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
-    float a = VOX_FMUL(P->op, vox_expf(-VOX_FMUL(P->ls, d)));
+    float a = VOX_FMUL(P->op, vox_expf_ch(-VOX_FMUL(P->ls, d)));
     a = a > 0.f ? a : 0.f;
     const float scale1d = VOX_FSQRT(dot3(P->s, P->s));
     const float vrs = VOX_FDIV(VOX_FMUL(0.1f, scale1d), vs);
-    a = VOX_FSUB(1.f, vox_powf(VOX_FSUB(1.f, a), VOX_FDIV(1.f, vrs)));
+    a = VOX_FSUB(1.f, vox_powf_ch(VOX_FSUB(1.f, a), VOX_FDIV(1.f, vrs)));
     const float cull = cull_scale > 0.f ? cull_scale : 0.05f;
     if (scale1d > cull)
         a = 0.f;
@@ -1878,4 +1878,17 @@ double ov_smooth_loss64(void* h, const double* theta, int raw, const double* gra
                 L += K * t;
             }
     return L;
+}
+
+/* The float channels' exp / log / pow (vox_expf_ch, vox_logf_ch, vox_powf_ch)
+ * on arrays, for their accuracy test against double precision. */
+void ov_chan_math(int64_t n, const float* x, const float* b, const float* e, float* exp_out, float* log_out,
+                  float* pow_out)
+{
+    for (int64_t i = 0; i < n; i++)
+    {
+        exp_out[i] = vox_expf_ch(x[i]);
+        log_out[i] = vox_logf_ch(b[i]);
+        pow_out[i] = vox_powf_ch(b[i], e[i]);
+    }
 }

@@ -66,6 +66,9 @@ void* ov_run(int64_t n, const float* means, const float* quats_wxyz, const float
              const float* opacities, float voxel_size, float cull_scale, int window_mode, int nthreads);
 void ov_destroy(void* h);
 void ov_counts(void* h, int64_t* out);
+/* the float channels' exp / log / pow on arrays (accuracy test) */
+void ov_chan_math(int64_t n, const float* x, const float* b, const float* e, float* exp_out, float* log_out,
+                  float* pow_out);
 int64_t ov_node2_bytes(void* h, uint8_t* dst); /* node2 region starting at the root */
 void ov_pairs(void* h, uint64_t* keys, uint32_t* ids); /* sorted by (hierarchical key, Gaussian id) */
 void ov_values(void* h, uint32_t* rgba8, float* density, float* color, double* density64, double* color64);

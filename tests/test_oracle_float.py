@@ -44,3 +44,29 @@ def test_float_channels_within_tolerance_of_fp64(oracle_mod, make, vs):
     err_c = float(np.abs(v["color"].astype(np.float64)[w] - v["color64"][w]).max())
     assert err_c <= 1e-4, err_c
     ref.close()
+
+
+def _ulp(y):
+    y = np.abs(y).astype(np.float32)
+    return np.maximum(np.spacing(y).astype(np.float64), 2.0 ** -149)
+
+
+def test_channel_math_accuracy(oracle_mod):
+    # vox_expf_ch / vox_logf_ch / vox_powf_ch against double precision over their
+    # domain (x <= 0, b in (0, 1], e > 0): exp within 1.5 ulp, log within 1.5 ulp
+    # of max(|log b|, 1/2), b^e within 1.2e-7 absolute (what the alpha 1 - b^e sees)
+    rng = np.random.default_rng(77)
+    n = 2_000_000
+    u = rng.random(n)
+    x = (-87.0 * u * u).astype(np.float32)
+    b = np.where(u < 0.5, np.ldexp(1.0 + u, -(48 * u).astype(np.int64)), u).clip(2.0 ** -24, 1.0).astype(np.float32)
+    e = (0.05 + 20.0 * rng.random(n) ** 2).astype(np.float32)
+    ex, lg, pw = oracle_mod.chan_math(x, b, e)
+    ref_e = np.exp(x.astype(np.float64))
+    assert float(np.max(np.abs(ex - ref_e) / _ulp(ref_e))) <= 1.5
+    ref_l = np.log(b.astype(np.float64))
+    assert float(np.max(np.abs(lg - ref_l) / _ulp(np.maximum(np.abs(ref_l), 0.5)))) <= 1.5
+    ref_p = np.power(b.astype(np.float64), e.astype(np.float64))
+    assert float(np.max(np.abs(pw - ref_p))) <= 1.2e-7
+    assert oracle_mod.chan_math(np.zeros(1), np.zeros(1), np.ones(1))[2][0] == 0.0  # 0^e
+    assert oracle_mod.chan_math(np.zeros(1), np.ones(1), np.ones(1) * 3)[2][0] == 1.0  # 1^e
