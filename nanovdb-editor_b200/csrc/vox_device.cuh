@@ -637,8 +637,13 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
 // two rounded sums); and the
 // alpha a' = 1 - (1 - op e^-ls d)^e, whose slope in d is at most
 // e ls a_hi (times 1 / (1 - a_hi) when e < 1) for a_hi >= op e^-ls (d - md),
-// by at most that slope times md, plus both evaluations' own error (a few ulp
-// of the exp and pow: 4e-6 (1 + e) bounds it).  When a' +- that margin falls
+// by at most that slope times md, plus both evaluations' own error: the exps
+// within 0.5 and 1.5 ulp (vox_expf_cr, vox_expf_ch) and two roundings of op e
+// give |delta a| <= 3.6e-7 a, so the bases 1 - a differ by at most 3.6e-7 a +
+// 6e-8; through the pow's slope (e, or e / (1 - a_hi) when e < 1) plus the two
+// pows' own errors (within 1.0e-7 and 0.82e-7, tests/test_oracle_float.py) and
+// the final roundings (6e-8) that is slope_e (3.6e-7 a + 6e-8) + 3.1e-7, taken
+// three times over.  When a' +- that margin falls
 // in one byte (rgba8_byte is monotone) the byte is the reference's and
 // decided is set; otherwise the caller runs the reference's evaluation
 // (ref_alpha_byte).  VOX_CHECK_EMIT=1 compares every decided byte with the
@@ -672,9 +677,9 @@ __device__ __forceinline__ uint32_t alpha_byte_bound(const GaussRec& R, const Al
     // 1 / (1 - a_hi) from the fast reciprocal (within 2 ulp for 1 - a_hi >= 2^-24,
     // as it is when a_hi < 1), raised by 2^-20 so it stays an upper bound
     const float inv = __fdividef(1.f, 1.f - a_hi) * (1.f + 0x1p-20f);
-    float slope = e * ls * a_hi;
-    slope = e < 1.f ? slope * inv : slope;
-    const float delta = 1.25f * slope * md + 4e-6f * (1.f + e) + 1e-6f;
+    const float slope_e = e < 1.f ? e * inv : e; // the pow's slope bound
+    const float slope = slope_e * ls * a_hi;
+    const float delta = 1.25f * slope * md + slope_e * (1.1e-6f * a_hi + 1.8e-7f) + 9.3e-7f;
     const uint32_t lo = rgba8_byte(f.a1 - delta), hi = rgba8_byte(f.a1 + delta);
     const bool culled = R.q7.w != 0.f; // culled by scale: both alphas are 0
     decided = culled || (x < 0.25f && a_hi < 1.f && lo == hi);
