@@ -49,6 +49,18 @@ struct vox_context_t
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = true;
+    // host-array calls: the attribute upload runs in chunks on its own stream,
+    // each chunk's k_prep launch waiting only for that chunk's copies
+    struct Upload
+    {
+        bool active = false;
+        const void* host[5] = {};     // means, quats, scales, opacities, colors
+        char* dev[5] = {};
+        int width[5] = { 3, 4, 3, 1, 3 }; // values per Gaussian
+        size_t es = 4;                   // bytes per value
+    } upload;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t up_ev[5] = {};           // [0]: the call's start on the stream, [1..4]: chunks landed
     uint32_t wait_ctl = 0; // look-back wait control (0: default limit), see vox_context_set_wait_limit
     std::string last_error;
     std::vector<DevBuf*> bufs;
@@ -413,7 +425,37 @@ static int run_voxelize(vox_context_t* ctx, const vox_gaussians_t* gs, float vox
     P.cloud_start = d_cloud_start;
     P.cloud_vs = d_cloud_vs;
     P.clouds = B;
-    launch_prep(P, recs, footprints, root_bits, d_err, s);
+    if (ctx->upload.active && G >= (1 << 20))
+    {
+        // four chunks: the copies of chunk c + 1 overlap the prep of chunk c
+        const int NC = 4;
+        cudaEventRecord(ctx->up_ev[0], s);
+        cudaStreamWaitEvent(ctx->copy_stream, ctx->up_ev[0], 0);
+        for (int c = 0; c < NC; c++)
+        {
+            const int64_t g0 = G * c / NC, g1 = G * (c + 1) / NC;
+            for (int a = 0; a < 5; a++)
+            {
+                const size_t row = (size_t)ctx->upload.width[a] * ctx->upload.es;
+                cudaMemcpyAsync(ctx->upload.dev[a] + row * g0, (const char*)ctx->upload.host[a] + row * g0,
+                                row * (size_t)(g1 - g0), cudaMemcpyHostToDevice, ctx->copy_stream);
+            }
+            cudaEventRecord(ctx->up_ev[1 + c], ctx->copy_stream);
+            cudaStreamWaitEvent(s, ctx->up_ev[1 + c], 0);
+            P.g0 = g0;
+            P.g1 = g1;
+            launch_prep(P, recs, footprints, root_bits, d_err, s);
+        }
+    }
+    else
+    {
+        if (ctx->upload.active)
+            for (int a = 0; a < 5; a++)
+                cudaMemcpyAsync(ctx->upload.dev[a], ctx->upload.host[a],
+                                (size_t)ctx->upload.width[a] * ctx->upload.es * (size_t)G, cudaMemcpyHostToDevice, s);
+        launch_prep(P, recs, footprints, root_bits, d_err, s);
+    }
+    ctx->upload.active = false;
     uint64_t* scan_status = (uint64_t*)ctx->scan_status.p;
     size_t scan_words = ctx->scan_status.cap / sizeof(uint64_t);
     scan_exclusive_u64(footprints, frag_off, G, 0, sc + SC_F, scan_status, ctx->scan_epochs.next(scan_status, scan_words, s),
@@ -996,6 +1038,9 @@ vox_context_t* vox_context_create(int device)
     }
     for (auto& e : ctx->timers.ev)
         cudaEventCreate(&e);
+    cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+    for (auto& e : ctx->up_ev)
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     const char* chk = getenv("VOX_CHECK_SORT");
     ctx->check_sort = (chk && chk[0] == '1') ? 1 : 0;
     const char* chk_emit = getenv("VOX_CHECK_EMIT");
@@ -1037,6 +1082,14 @@ void vox_context_destroy(vox_context_t* ctx)
     for (auto& e : ctx->timers.ev)
         if (e)
             cudaEventDestroy(e);
+    for (auto& e : ctx->up_ev)
+        if (e)
+            cudaEventDestroy(e);
+    if (ctx->copy_stream)
+    {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
     if (ctx->hscal)
         cudaFreeHost(ctx->hscal);
     if (ctx->stream)
@@ -1131,15 +1184,18 @@ int vox_voxelize_host(vox_context_t* ctx, const vox_gaussians_t* gaussians, floa
     dg.scales = (const float*)(db + 7 * n * es);
     dg.opacities = (const float*)(db + 10 * n * es);
     dg.colors = (const float*)(db + 11 * n * es);
-    if (n > 0)
+    // the copies are issued by run_voxelize's prep step (chunked, overlapping k_prep)
+    const void* hs[5] = { gaussians->means, gaussians->quats, gaussians->scales, gaussians->opacities, gaussians->colors };
+    const void* ds[5] = { dg.means, dg.quats, dg.scales, dg.opacities, dg.colors };
+    for (int a = 0; a < 5; a++)
     {
-        cudaMemcpyAsync((void*)dg.means, gaussians->means, 3 * n * es, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.quats, gaussians->quats, 4 * n * es, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.scales, gaussians->scales, 3 * n * es, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.opacities, gaussians->opacities, n * es, cudaMemcpyHostToDevice, ctx->stream);
-        cudaMemcpyAsync((void*)dg.colors, gaussians->colors, 3 * n * es, cudaMemcpyHostToDevice, ctx->stream);
+        ctx->upload.host[a] = hs[a];
+        ctx->upload.dev[a] = (char*)ds[a];
     }
+    ctx->upload.es = es;
+    ctx->upload.active = n > 0;
     int rc = run_voxelize(ctx, &dg, voxel_size, cull_scale, flags);
+    ctx->upload.active = false;
     if (rc)
         return rc;
     if (grid_bytes)

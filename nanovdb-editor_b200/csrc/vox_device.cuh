@@ -123,6 +123,7 @@ struct PrepParams
     const int64_t* cloud_start;
     const float* cloud_vs;
     int64_t clouds;
+    int64_t g0 = 0, g1 = -1; // the Gaussians [g0, g1) this launch builds (g1 < 0: up to count)
 };
 
 

@@ -29,8 +29,8 @@ namespace vox
 __global__ void __launch_bounds__(256) k_prep(PrepParams P, GaussRec* recs, uint64_t* footprints,
                                               unsigned long long* root_bits, int* err)
 {
-    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= P.count)
+    const int64_t g = P.g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (P.g1 < 0 ? P.count : P.g1))
         return;
     GaussRec R;
     int32_t bmax[3];
@@ -728,9 +728,10 @@ __global__ void __launch_bounds__(256) k_write_leaf(NodeParams N, uint8_t* node2
 void launch_prep(const PrepParams& P, GaussRec* recs, uint64_t* footprints, uint64_t* root_bits, int* err,
                  cudaStream_t s)
 {
-    if (P.count <= 0)
+    const int64_t n = (P.g1 < 0 ? P.count : P.g1) - P.g0;
+    if (n <= 0)
         return;
-    { k_prep<<<(unsigned)((P.count + 255) / 256), 256, 0, s>>>(P, recs, footprints, (unsigned long long*)root_bits, err); count_launch(); }
+    { k_prep<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, recs, footprints, (unsigned long long*)root_bits, err); count_launch(); }
 }
 
 void launch_mark_lower(const GaussRec* recs, int64_t G, const uint64_t* root_bits, const uint64_t* root_prefix,
