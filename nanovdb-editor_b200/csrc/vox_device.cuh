@@ -481,11 +481,13 @@ __device__ __forceinline__ float pair_alpha(const GaussRec& R, const Aabb& b)
 // rounding adds 0.5 ulp(E_a), its other roundings (the chain 3, k and base 2,
 // the steps' 3 times |t| <= 7 with 8 vs <= E, lo0 3, the per-voxel fma 3, W and
 // the hi sum about 1.3, in units of 2^-24 sum_a |m_ra| E_a) at most
-// 2^-20 sum_a |m_ra| E_a; all scaled by il is_r.  The leaf test
-// (leaf_test_chunk) classifies voxels from this AABB: per row it is within
-// delta_r = dab_r + 2^-20 2 Bl_r of the reference's, Bl_r = il is_r sum_a
-// |m_ra| Cm_a bounding the bounds' magnitudes in the leaf, and Delta = sum_r
-// delta_r gives its thresholds lo_t / hi_t.
+// 2^-20 sum_a |m_ra| E_a; all scaled by il is_r.  dab_r also carries the
+// roundings proportional to the bound magnitude (the sum and scalings of the
+// reference, the lattice points): 2^-20 2 Bl_r, Bl_r = il is_r sum_a |m_ra|
+// Cm_a bounding every bound's magnitude in the leaf.  So per row this AABB,
+// and its four lattice points, are within dab_r of the reference's for every
+// voxel of the leaf.  The leaf test (leaf_test_chunk) classifies voxels from
+// it, Delta = sum_r dab_r giving its thresholds lo_t / hi_t.
 struct LeafPairConst
 {
     float lo0[3], W[3]; // per row: the scaled lower bound of the anchor voxel, the scaled voxel width
@@ -546,9 +548,10 @@ __device__ __forceinline__ LeafPairConst leaf_pair_consts(const GaussRec& R, flo
         c.W[r] = VOX_FADD(VOX_FADD(fabsf(c.A[r][0]), fabsf(c.A[r][1])), fabsf(c.A[r][2]));
         const float s = (1.f + 0x1p-20f) * il * is[r];
         const float m0 = fabsf(M.m[r][0]), m1 = fabsf(M.m[r][1]), m2 = fabsf(M.m[r][2]);
-        c.dab[r] = s * (m0 * G[0] + m1 * G[1] + m2 * G[2]);
         const float Bl = s * (m0 * Cm[0] + m1 * Cm[1] + m2 * Cm[2]);
-        Dl += c.dab[r] + 0x1p-20f * 2.f * Bl;
+        // with the scalings' and lattice points' roundings, 2^-20 B_r <= 2^-20 2 Bl_r
+        c.dab[r] = s * (m0 * G[0] + m1 * G[1] + m2 * G[2]) + 0x1p-20f * 2.f * Bl;
+        Dl += c.dab[r];
     }
     Dl *= 1.f + 0x1p-20f;
     if (Dl <= 0.0625f) // false for NaN
@@ -584,14 +587,13 @@ __device__ __forceinline__ Aabb stable_leaf_aabb(const float lo0[3], const float
 // (stable_leaf_aabb): the lattice points lo + w (hi - lo), float exp / pow
 // (vox_expf_ch / vox_powf_ch: about 2 ulp, no division).  The oracle's
 // frag_alpha_f evaluates the same operations in the same order.  Also keeps
-// what alpha_byte_bound needs: the lattice minimum d, op exp(-ls d) and
-// the largest bound magnitude per axis.
+// what alpha_byte_bound needs: the lattice minimum d, op exp(-ls d) and the
+// smallest lattice square per axis.
 struct AlphaF
 {
     float a1;   // the channel's alpha
     float d;    // smallest lattice |p|^2
     float a;    // op exp(-ls d), before the opacity transform
-    float B[3]; // max(|lo|, |hi|) per axis
     float m[3]; // the smallest lattice square per axis
 };
 __device__ __forceinline__ AlphaF pair_alpha_f_ex(const GaussRec& R, const Aabb& b)
@@ -606,7 +608,6 @@ __device__ __forceinline__ AlphaF pair_alpha_f_ex(const GaussRec& R, const Aabb&
         const float s0 = VOX_FMUL(b.lo[a], b.lo[a]), s1 = VOX_FMUL(p1, p1), s2 = VOX_FMUL(p2, p2),
                     s3 = VOX_FMUL(b.hi[a], b.hi[a]);
         m[a] = fminf(fminf(s0, s1), fminf(s2, s3)); // squares: no NaN, no signed zero
-        f.B[a] = fmaxf(fabsf(b.lo[a]), fabsf(b.hi[a]));
         f.m[a] = m[a];
     }
     f.d = VOX_FADD(VOX_FADD(m[0], m[1]), m[2]);
@@ -629,8 +630,8 @@ __device__ __forceinline__ float pair_alpha_f(const GaussRec& R, const Aabb& b)
 // with b_ref = voxel_local_aabb(...), decided where possible from the float
 // channel's alpha f (same formula, evaluated from stable_leaf_aabb).
 // Per row the two AABBs' bounds, and so their four lattice points, differ by at
-// most D_r = dab_r + 2^-20 B_r (leaf_pair_consts, plus the scalings' and
-// lattice points' roundings proportional to B_r = max(|lo|, |hi|)).  With m_r
+// most D_r = dab_r (leaf_pair_consts: the scalings' and lattice points'
+// roundings included).  With m_r
 // the float evaluation's smallest lattice square, either evaluation's
 // minimizing point is within u_r = sqrt(m_r) + D_r of zero, so the row minima
 // differ by at most 2 sqrt(m_r) D_r + D_r^2 + 2^-22 u_r^2 (rounded squares) and
@@ -667,7 +668,7 @@ __device__ __forceinline__ uint32_t alpha_byte_bound(const GaussRec& R, const Al
 #pragma unroll
     for (int r = 0; r < 3; r++)
     {
-        const float D = dab[r] + 0x1p-20f * f.B[r];
+        const float D = dab[r]; // dab_r + 2^-20 B_r, folded per leaf (leaf_pair_consts)
         const float u = sqrt_upper(f.m[r]) + D; // bounds both evaluations' minimizing lattice point
         md += (2.f * u - D) * D + 0x1p-22f * u * u;
     }

@@ -385,7 +385,7 @@ struct LeafQSmem
 // voxel of the column is first classified from the float channels' local AABB
 // (stable_leaf_aabb: per column the x / y terms once, then one fma per row
 // and voxel), and only voxels near the sphere run the reference test.  Per
-// row that AABB is within delta_r = dab_r + 2^-20 2 Bl_r of the reference's
+// row that AABB is within delta_r = dab_r of the reference's
 // (leaf_pair_consts), so the selected values (max(lo, min(hi, 0)),
 // 1-Lipschitz in both bounds) differ by at most delta_r and the vectors of the
 // three by eta <= Delta = sum delta_r in norm.  The reference passes a voxel
@@ -489,8 +489,9 @@ __device__ __forceinline__ void leaf_test_chunk(const LeafPassParams& P, const C
                             D = __fmaf_rn(xs, xs, D);
                         }
                         zmask |= (D < lo_t ? 1u : 0u) << k;
-                        unc |= (!(D < lo_t) && !(D > hi_t) ? 1u : 0u) << k;
+                        unc |= (D > hi_t ? 0u : 1u) << k; // not surely failing (NaN included)
                     }
+                    unc &= ~zmask; // neither surely passing nor surely failing
                 }
                 // the reference test of one voxel, from the record (nothing of the column kept live)
                 auto exact_voxel = [&](uint32_t k) -> uint32_t {
