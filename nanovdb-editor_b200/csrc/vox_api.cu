@@ -86,7 +86,7 @@ struct vox_context_t
     DevBuf hier_keys;
     DevBuf prim_keys_alt, prim_vals_alt; // ping-pong buffers of vox_radix_sort_key64
     DevBuf vb_work; // VoxelBVH ingestion: world-box keys, range tile counts
-    DevBuf vb_keys; // VoxelBVH ingestion: compressed sort keys (also the dual-key sort's keys)
+    DevBuf vb_keys, vb_ids_c, vb_used; // VoxelBVH ingestion: compressed sort keys (also the dual-key sort's keys)
     DevBuf dual_idx; // dual-key sort: original indices
     DevBuf vb_rec;   // VoxelBVH ingestion: per-Gaussian search records
     uint64_t* hscal = nullptr; // pinned mirror
@@ -137,6 +137,7 @@ enum
     SC_NCL,  // candidate leaves
     SC_NVOX, // active voxels from the leaf masks
     SC_NWIN, // reference fragment windows (window order)
+    SC_VBU,  // VoxelBVH: used key slots
     SC_BBOX, // 3 words (6 int32)
     SC_COUNT = SC_BBOX + 3,
     SC_SCRATCH = 24
@@ -1067,7 +1068,7 @@ void vox_context_destroy(vox_context_t* ctx)
                       &ctx->lower_parent, &ctx->upper_root_n, &ctx->upper_lostart, &ctx->leaf_lower,
                       &ctx->leaf_lower_n, &ctx->leaf_mask, &ctx->leaf_origin, &ctx->order, &ctx->grid, &ctx->scal,
                       &ctx->vox_leaf, &ctx->vox_n, &ctx->rank_to_lower,
-                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->vb_keys, &ctx->dual_idx, &ctx->vb_rec, &ctx->cloud_start,
+                      &ctx->hier_keys, &ctx->prim_keys_alt, &ctx->prim_vals_alt, &ctx->vb_work, &ctx->vb_keys, &ctx->vb_ids_c, &ctx->vb_used, &ctx->dual_idx, &ctx->vb_rec, &ctx->cloud_start,
                       &ctx->cloud_vs, &ctx->clouds, &ctx->lcols, &ctx->lcol_off, &ctx->lc_count, &ctx->lc_mask, &ctx->lc_off,
                       &ctx->cand_org, &ctx->tile_g0, &ctx->emit_gid, &ctx->emit_flag, &ctx->lflags, &ctx->lpos, &ctx->cand_key, &ctx->cand_start,
                       &ctx->cand_mask, &ctx->pair_gid, &ctx->s_rgba, &ctx->s_dens, &ctx->s_col, &ctx->s_pairs, &ctx->cand_cnt,
@@ -1639,6 +1640,7 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
     R.keys_out = d_ijkl;
     R.ids_out = d_prim_id;
     int key32 = 0, sort_bits = 0;
+    int64_t n_sorted = N; // the slots the sort and the range kernels cover (the used ones when compacted)
     const void* sorted_keys = d_ijkl;
     const bool any_cell = mm[3] >= mm[0];
     // VOX_VB_SORT64=1 sorts the 64-bit keys even when they compress (testing)
@@ -1659,14 +1661,32 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
             key32 = sort_bits <= 32;
             R.sentinel = sort_bits >= 64 ? ~0ull : (1ull << sort_bits) - 1;
             R.expand = 1;
-            launch_vb_compress(d_ijkl, N, R, ctx->vb_keys.p, key32, ctx->num_sms, s);
+            // only the used slots are sorted: per-Gaussian counts, their scan (the total U
+            // read back to size the sort), then the compressed keys and ids compacted
+            if (!ensure(ctx, ctx->vb_ids_c, 4 * (size_t)N) || !ensure(ctx, ctx->vb_used, 8 * (size_t)(count + 1)))
+                return VOX_ERR_MEMORY;
+            uint32_t* used = (uint32_t*)ctx->vb_used.p;
+            uint32_t* uoff = used + count + 1;
+            uint32_t* ids_c = (uint32_t*)ctx->vb_ids_c.p;
+            launch_vb_used(d_prim_id, count, used, s);
+            uint64_t* status = (uint64_t*)ctx->scan_status.p;
+            scan_u32(used, uoff, count, 0, 0, sc + SC_VBU, status,
+                     ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s),
+                     (uint32_t*)(sc + SC_SCRATCH), err, s);
+            rc = sync_scalars(ctx, "vox_voxelbvh_ijkl_from_gaussians");
+            if (rc != VOX_OK)
+                return rc;
+            n_sorted = (int64_t)ctx->hscal[SC_VBU];
+            launch_vb_compress_used(d_ijkl, d_prim_id, count, used, uoff, R, ctx->vb_keys.p, ids_c, key32, ctx->num_sms,
+                                    s);
             if (key32)
-                in_alt = sort_pairs_u32((uint32_t*)ctx->vb_keys.p, d_prim_id, (uint32_t*)alt_k, alt_v, N, sort_bits,
+                in_alt = sort_pairs_u32((uint32_t*)ctx->vb_keys.p, ids_c, (uint32_t*)alt_k, alt_v, n_sorted, sort_bits,
                                         ctx->sort_ws.p, &ctx->sort_epochs, err, ctx->num_sms, s, ctx->tuning);
             else
-                in_alt = sort_pairs_u64((uint64_t*)ctx->vb_keys.p, d_prim_id, alt_k, alt_v, N, sort_bits,
+                in_alt = sort_pairs_u64((uint64_t*)ctx->vb_keys.p, ids_c, alt_k, alt_v, n_sorted, sort_bits,
                                         ctx->sort_ws.p, &ctx->sort_epochs, err, ctx->num_sms, s, ctx->tuning);
             sorted_keys = in_alt ? (const void*)alt_k : (const void*)ctx->vb_keys.p;
+            R.ids_src = in_alt ? alt_v : ids_c;
         }
         else
         {
@@ -1676,19 +1696,23 @@ int vox_voxelbvh_ijkl_from_gaussians(vox_context_t* ctx, const float* d_means, c
             if (in_alt)
                 cudaMemcpyAsync(d_ijkl, alt_k, 8 * (size_t)N, cudaMemcpyDeviceToDevice, s);
         }
-        if (in_alt)
+        if (in_alt && !compress)
             R.ids_src = alt_v;
     }
     cudaEventRecord(ctx->timers.ev[3], s);
-    if (N > 0)
+    if (n_sorted > 0)
     {
-        launch_vb_range_count(sorted_keys, key32, N, tile_cnt, s);
+        const int64_t rtiles = vb_range_tiles(n_sorted);
+        launch_vb_range_count(sorted_keys, key32, n_sorted, tile_cnt, s);
         uint64_t* status = (uint64_t*)ctx->scan_status.p;
-        scan_exclusive_u64(tile_cnt, tile_off, tiles, 0, d_total, status,
+        scan_exclusive_u64(tile_cnt, tile_off, rtiles, 0, d_total, status,
                            ctx->scan_epochs.next(status, ctx->scan_status.cap / sizeof(uint64_t), s),
                            (uint32_t*)(sc + SC_SCRATCH), err, ctx->num_sms, s);
-        launch_vb_range_scatter(sorted_keys, key32, N, tile_off, d_total, R, s);
-        cudaMemcpyAsync(sc + SC_F, d_total, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+        launch_vb_range_scatter(sorted_keys, key32, n_sorted, tile_off, d_total, R, s);
+        if (n_sorted < N) // compacted: the unused run [U, N) is the last range
+            launch_vb_tail(n_sorted, N, d_total, sc + SC_F, R, ctx->num_sms, s);
+        else
+            cudaMemcpyAsync(sc + SC_F, d_total, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
     }
     cudaEventRecord(ctx->timers.ev[4], s);
     rc = check_cuda(ctx, "vox_voxelbvh_ijkl_from_gaussians");

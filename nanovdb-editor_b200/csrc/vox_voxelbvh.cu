@@ -20,17 +20,21 @@
 //                       (voxelbvh_gaussians_to_ijkl.slang:25-250)
 //   k_vb_ijkl           the same search, one thread per Gaussian with the
 //                       per-axis reuse below (VOX_VB_SEARCH=thread)
-//   k_vb_compress       keys -> compressed keys of 4 + bits(i) + bits(j) +
+//   k_vb_used,          the used slots (a prefix of each Gaussian's 8) counted and
+//   k_vb_compress_used  scanned, their keys compressed to 4 + bits(i) + bits(j) +
 //                       bits(k) bits (32-bit when they fit), sized by the
 //                       emitted cells' range the search reduces: the same
-//                       order in fewer radix passes
-//   (sort)              stable onesweep LSD sort of the compressed keys (of
-//                       the 64-bit keys when a cell lies outside [0, 2^15))
+//                       order in fewer radix passes, and compacted (the
+//                       unused slots, all-ones key and id, are the sorted tail)
+//   (sort)              stable LSD sort of the used compressed keys (of all
+//                       64-bit keys when a cell lies outside [0, 2^15))
 //   k_vb_range_count    starts per 2048-key tile
 //   (scan)              exclusive scan of the tile counts
 //   k_vb_range_scatter  headers [2r] = start, [2r + 1] = end; every header
 //                       slot at or past the range count is zeroed; writes
 //                       the sorted keys back as 64-bit keys
+//   k_vb_tail           the unused tail: keys and ids all ones, its run as
+//                       the last range, the other headers zeroed
 //                       (voxelbvh_find_range_starts.slang,
 //                       voxelbvh_scatter_range_headers.slang)
 //
@@ -950,7 +954,109 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_compress(const uint64_t* keys
     }
 }
 
+// Compaction of the used slots before the sort: a Gaussian's used slots are
+// the first of its 8 (the unused ones carry key ~0 and id ~0, identical pairs,
+// so after a stable sort they simply fill the tail).  k_vb_used: each
+// Gaussian's used count; k_vb_compress_used: the used slots' compressed keys
+// and ids at their scanned positions; k_vb_tail: the tail's keys, ids and
+// headers (the unused run [U, N) is the last range).
+__global__ void __launch_bounds__(VB_THREADS) k_vb_used(const uint32_t* __restrict__ ids, int64_t count,
+                                                        uint32_t* __restrict__ used)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= count)
+        return;
+    const uint4* p = reinterpret_cast<const uint4*>(ids + 8 * g);
+    const uint4 a = p[0], b = p[1];
+    used[g] = (uint32_t)(a.x != ~0u) + (a.y != ~0u) + (a.z != ~0u) + (a.w != ~0u) + (b.x != ~0u) + (b.y != ~0u) +
+              (b.z != ~0u) + (b.w != ~0u);
+}
+
+template <class K>
+__global__ void __launch_bounds__(VB_THREADS) k_vb_compress_used(const uint64_t* __restrict__ keys,
+                                                                   const uint32_t* __restrict__ ids, int64_t count,
+                                                                   const uint32_t* __restrict__ used,
+                                                                   const uint32_t* __restrict__ off, VbRangeParams R,
+                                                                   K* __restrict__ out_keys, uint32_t* __restrict__ out_ids)
+{
+    const int64_t N = 8 * count;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t g = t >> 3;
+        const uint32_t slot = (uint32_t)(t & 7);
+        if (slot >= used[g])
+            continue;
+        const uint64_t u = keys[t];
+        const uint64_t i = (u >> 48) & 0xffffu, j = (u >> 32) & 0xffffu, k = (u >> 16) & 0xffffu, level = u & 15u;
+        const int64_t dst = (int64_t)off[g] + slot;
+        out_keys[dst] = (K)((((i << R.bits[1] | j) << R.bits[2] | k) << 4) | level);
+        out_ids[dst] = ids[t];
+    }
+}
+
+__global__ void __launch_bounds__(VB_THREADS) k_vb_tail(int64_t U, int64_t N, const uint64_t* __restrict__ nr_used,
+                                                        uint64_t* __restrict__ ranges_out, VbRangeParams R)
+{
+    const uint64_t nr = *nr_used;
+    for (int64_t i = U + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+    {
+        R.keys_out[i] = ~0ull;
+        R.ids_out[i] = ~0u;
+        if ((uint64_t)i != nr)
+        {
+            R.range[2 * i] = 0u;
+            R.range[2 * i + 1] = 0u;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        R.range[2 * nr] = (uint32_t)U;
+        R.range[2 * nr + 1] = (uint32_t)N;
+        *ranges_out = nr + 1;
+    }
+}
+
 } // namespace
+
+void launch_vb_used(const uint32_t* ids, int64_t count, uint32_t* used, cudaStream_t s)
+{
+    if (count <= 0)
+        return;
+    k_vb_used<<<(unsigned)((count + VB_THREADS - 1) / VB_THREADS), VB_THREADS, 0, s>>>(ids, count, used);
+    count_launch();
+}
+
+void launch_vb_compress_used(const uint64_t* keys, const uint32_t* ids, int64_t count, const uint32_t* used,
+                             const uint32_t* off, const VbRangeParams& R, void* out_keys, uint32_t* out_ids, int key32,
+                             int num_sms, cudaStream_t s)
+{
+    if (count <= 0)
+        return;
+    int64_t grid = (8 * count + VB_THREADS - 1) / VB_THREADS;
+    const int64_t cap = (int64_t)num_sms * 16;
+    if (grid > cap)
+        grid = cap;
+    if (key32)
+        k_vb_compress_used<uint32_t><<<(unsigned)grid, VB_THREADS, 0, s>>>(keys, ids, count, used, off, R,
+                                                                           (uint32_t*)out_keys, out_ids);
+    else
+        k_vb_compress_used<uint64_t><<<(unsigned)grid, VB_THREADS, 0, s>>>(keys, ids, count, used, off, R,
+                                                                           (uint64_t*)out_keys, out_ids);
+    count_launch();
+}
+
+void launch_vb_tail(int64_t U, int64_t N, const uint64_t* nr_used, uint64_t* ranges_out, const VbRangeParams& R,
+                    int num_sms, cudaStream_t s)
+{
+    int64_t grid = (N - U + VB_THREADS - 1) / VB_THREADS;
+    const int64_t cap = (int64_t)num_sms * 8;
+    if (grid > cap)
+        grid = cap;
+    if (grid < 1)
+        grid = 1;
+    k_vb_tail<<<(unsigned)grid, VB_THREADS, 0, s>>>(U, N, nr_used, ranges_out, R);
+    count_launch();
+}
 
 void launch_vb_init(uint32_t* box_keys, int* cell_minmax, cudaStream_t s)
 {
