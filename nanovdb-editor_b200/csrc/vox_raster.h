@@ -288,8 +288,6 @@ void launch_vb_box(const VoxelBvhParams& P, int num_sms, cudaStream_t s);
 void launch_vb_ijkl(const VoxelBvhParams& P, cudaStream_t s);
 void launch_vb_search(const VoxelBvhParams& P, int num_sms, cudaStream_t s);
 int64_t vb_range_tiles(int64_t N);
-void launch_vb_compress(const uint64_t* keys, int64_t N, const VbRangeParams& R, void* out, int key32, int num_sms,
-                        cudaStream_t s);
 void launch_vb_used(const uint32_t* ids, int64_t count, uint32_t* used, cudaStream_t s);
 void launch_vb_compress_used(const uint64_t* keys, const uint32_t* ids, int64_t count, const uint32_t* used,
                              const uint32_t* off, const VbRangeParams& R, void* out_keys, uint32_t* out_ids, int key32,

@@ -932,31 +932,11 @@ __global__ void __launch_bounds__(VB_THREADS) k_vb_range_scatter(const K* keys, 
     }
 }
 
-// 64-bit keys -> compressed keys: i, j, k in bits[0], bits[1], bits[2] bits
-// above a 4-bit level, the unused slot as all ones (above every cell key,
-// whose level is at most 11).  Order-preserving for cells in [0, 2^bits).
-template <class K>
-__global__ void __launch_bounds__(VB_THREADS) k_vb_compress(const uint64_t* keys, int64_t N, VbRangeParams R,
-                                                              K* out)
-{
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (int64_t)gridDim.x * blockDim.x)
-    {
-        const uint64_t u = keys[t];
-        uint64_t c;
-        if (u == ~0ull)
-            c = R.sentinel;
-        else
-        {
-            const uint64_t i = (u >> 48) & 0xffffu, j = (u >> 32) & 0xffffu, k = (u >> 16) & 0xffffu, level = u & 15u;
-            c = (((i << R.bits[1] | j) << R.bits[2] | k) << 4) | level;
-        }
-        out[t] = (K)c;
-    }
-}
-
 // Compaction of the used slots before the sort: a Gaussian's used slots are
 // the first of its 8 (the unused ones carry key ~0 and id ~0, identical pairs,
-// so after a stable sort they simply fill the tail).  k_vb_used: each
+// so after a stable sort they simply fill the tail).  The compressed key
+// holds i, j, k in bits[0], bits[1], bits[2] bits above a 4-bit level, in the
+// order of the 64-bit key for cells in [0, 2^bits).  k_vb_used: each
 // Gaussian's used count; k_vb_compress_used: the used slots' compressed keys
 // and ids at their scanned positions; k_vb_tail: the tail's keys, ids and
 // headers (the unused run [U, N) is the last range).
@@ -1112,22 +1092,6 @@ void launch_vb_ijkl(const VoxelBvhParams& P, cudaStream_t s)
 int64_t vb_range_tiles(int64_t N)
 {
     return (N + VB_TILE - 1) / VB_TILE;
-}
-
-void launch_vb_compress(const uint64_t* keys, int64_t N, const VbRangeParams& R, void* out, int key32, int num_sms,
-                        cudaStream_t s)
-{
-    if (N <= 0)
-        return;
-    int64_t grid = (N + VB_THREADS - 1) / VB_THREADS;
-    const int64_t cap = (int64_t)num_sms * 16;
-    if (grid > cap)
-        grid = cap;
-    if (key32)
-        k_vb_compress<uint32_t><<<(unsigned)grid, VB_THREADS, 0, s>>>(keys, N, R, (uint32_t*)out);
-    else
-        k_vb_compress<uint64_t><<<(unsigned)grid, VB_THREADS, 0, s>>>(keys, N, R, (uint64_t*)out);
-    count_launch();
 }
 
 void launch_vb_range_count(const void* keys, int key32, int64_t N, uint64_t* counts, cudaStream_t s)
