@@ -228,6 +228,21 @@ __device__ __forceinline__ uint32_t vb_scan_level(const VoxelBvhParams& P, const
                             s01[r][b0][b1] = __fadd_rn(__fmul_rn(__fsub_rn(pi[b0], G.mu[0]), G.R[0][r]),
                                                        __fmul_rn(__fsub_rn(pj[b1], G.mu[1]), G.R[1][r]));
                     }
+            // without a transform a corner's row value is fl(fl(s01 + z term) inv_r); rounded
+            // addition and a positive finite multiplier are monotone, so the minimum
+            // (maximum) over the 8 corners is that expression over the smallest
+            // (largest) s01 and z term - the shader's 8-corner result, bit for bit (a tie
+            // differs at most in the sign of a zero, which the test compares with zero)
+            const bool mono = !XF && G.inv[0] > 0.f && G.inv[1] > 0.f && G.inv[2] > 0.f &&
+                              G.inv[0] < __int_as_float(0x7f800000) && G.inv[1] < __int_as_float(0x7f800000) &&
+                              G.inv[2] < __int_as_float(0x7f800000);
+            float smin[3], smax[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+            {
+                smin[r] = fminf(fminf(s01[r][0][0], s01[r][0][1]), fminf(s01[r][1][0], s01[r][1][1]));
+                smax[r] = fmaxf(fmaxf(s01[r][0][0], s01[r][0][1]), fmaxf(s01[r][1][0], s01[r][1][1]));
+            }
             int k = lo[2] & msk;
             float pk0 = vb_lp(w2v, (float)k, 2);
             for (; k <= (hi[2] & msk); k += st)
@@ -236,6 +251,18 @@ __device__ __forceinline__ uint32_t vb_scan_level(const VoxelBvhParams& P, const
                 const float pk[2] = { pk0, pk1 };
                 pk0 = pk1;
                 float vmin[3] = { 0.f, 0.f, 0.f }, vmax[3] = { 0.f, 0.f, 0.f };
+                if (mono)
+                {
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                    {
+                        const float za = __fmul_rn(__fsub_rn(pk[0], G.mu[2]), G.R[2][r]);
+                        const float zb = __fmul_rn(__fsub_rn(pk[1], G.mu[2]), G.R[2][r]);
+                        vmin[r] = __fmul_rn(__fadd_rn(smin[r], fminf(za, zb)), G.inv[r]);
+                        vmax[r] = __fmul_rn(__fadd_rn(smax[r], fmaxf(za, zb)), G.inv[r]);
+                    }
+                }
+                else
 #pragma unroll
                 for (int v = 0; v < 8; v++)
                 {
@@ -553,6 +580,27 @@ __device__ __forceinline__ bool vb_overlap_cell(const VoxelBvhParams& P, const f
             }
     }
     float vmin[3] = { 0.f, 0.f, 0.f }, vmax[3] = { 0.f, 0.f, 0.f };
+    // Without a transform the corner value of row r is fl(fl(fl(q0 + q1) + q2) inv_r)
+    // over one product per axis; rounded addition and a positive finite
+    // multiplier are monotone, so the minimum (maximum) over the 8 corners is
+    // the same expression over the per-axis minimum (maximum) products - the
+    // shader's 8-corner loop's result, bit for bit (a tie differs at most in the
+    // sign of a zero, which the test below compares with zero)
+    if (!XF && inv[0] > 0.f && inv[1] > 0.f && inv[2] > 0.f && inv[0] < __int_as_float(0x7f800000) &&
+        inv[1] < __int_as_float(0x7f800000) && inv[2] < __int_as_float(0x7f800000))
+    {
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+        {
+            const float lo = __fadd_rn(__fadd_rn(fminf(q[r][0][0], q[r][0][1]), fminf(q[r][1][0], q[r][1][1])),
+                                       fminf(q[r][2][0], q[r][2][1]));
+            const float hi = __fadd_rn(__fadd_rn(fmaxf(q[r][0][0], q[r][0][1]), fmaxf(q[r][1][0], q[r][1][1])),
+                                       fmaxf(q[r][2][0], q[r][2][1]));
+            vmin[r] = __fmul_rn(lo, inv[r]);
+            vmax[r] = __fmul_rn(hi, inv[r]);
+        }
+    }
+    else
 #pragma unroll
     for (int v = 0; v < 8; v++)
     {
